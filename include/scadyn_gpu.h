@@ -1,0 +1,169 @@
+/* scadyn_gpu — B200 (sm_100a) T-matrix solve path behind a C ABI.
+ *
+ * Drop-in for jherrane/scadyn's T-matrix solve: the precorrected-FFT JVIE
+ * matrix-vector product (compute_Ax2), the restarted GMRES that calls it
+ * (gmres), the per-column solve loop (compute_T_matrix), and the
+ * per-wavelength setup that feeds them (build_G, pfft_projection_const,
+ * compute_near_zone_interactions_const).  A Fortran host binds these entry
+ * points through iso_c_binding; every entry point returns an int status.
+ *
+ * Array conventions are the reference's (Fortran column-major, 1-based ids):
+ *   complex arrays   interleaved (re, im) == complex(c_double_complex)
+ *   x, rhs, Ax       (3T)          unknowns of tet t at 3(t-1)+1..3(t-1)+3
+ *   S, Sx, Sy, Sz    (27, T)       projector coefficients
+ *   indS             (27, T)       1-based grid node ids (x fastest)
+ *   sp_mat           (3, 3, B)     near-zone blocks, tet_B >= tet_T
+ *   sp_ind           (2, B)        1-based (tet_T, tet_B)
+ *   Fg               (2Nx,2Ny,2Nz) FFT of the zero-padded Green's function
+ *   mat              (3T, ncol)    incident VSWF columns
+ *   Tcols            (ncol, ncol)  matᴴ·X, unscaled T_mat columns
+ * Host arrays are borrowed for the duration of a call; device copies belong
+ * to the context until scd_destroy.  A context is not thread-safe.
+ */
+#ifndef SCADYN_GPU_H
+#define SCADYN_GPU_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define SCD_API __attribute__((visibility("default")))
+#else
+#define SCD_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define SCD_OK             0
+#define SCD_NOT_CONVERGED  1   /* GMRES hit its cycle limit (the reference returns silently) */
+#define SCD_NAN            2   /* a non-finite residual or breakdown */
+#define SCD_OOM            3   /* device allocation failed */
+#define SCD_BAD_ARG        4   /* invalid sizes, pointers or indices */
+#define SCD_TIMEOUT        5   /* a host deadline expired */
+#define SCD_CUDA_ERROR     6   /* CUDA runtime error; see scd_last_error */
+#define SCD_NOT_READY      7   /* an operator piece has not been set */
+#define SCD_NO_DEVICE      8   /* no usable CUDA device */
+
+typedef struct scd_c128 { double re, im; } scd_c128;   /* complex(c_double_complex) */
+typedef struct scd_c64  { float re, im; }  scd_c64;    /* complex(c_float_complex)  */
+
+typedef struct scd_ctx scd_ctx;
+
+/* Grid and mesh sizes (type mesh_struct, src/common.f90:63-90). */
+typedef struct scd_grid_desc {
+    int32_t Nx, Ny, Nz;      /* grid nodes per axis (mesh%Nx..Nz) */
+    double  delta;           /* node spacing (mesh%delta) */
+    double  min_coord[3];    /* grid origin (mesh%min_coord) */
+    int32_t T;               /* tetrahedra (mesh%N_tet) */
+    int32_t order;           /* basis order (mesh%order); 0 only */
+    int32_t M_ex;            /* projection order (mesh%M_ex); 2 only */
+    int32_t near_zone;       /* near-cube radius (mesh%near_zone); 1 only */
+    int32_t device;          /* CUDA device ordinal */
+} scd_grid_desc;
+
+/* near-zone storage precision */
+#define SCD_STORE_C64   32   /* complex64, as the reference stores sp_mat */
+#define SCD_STORE_C128  64   /* complex128 */
+
+/* solve precision */
+#define SCD_PREC_FP64   0    /* complex128 GMRES and matvec */
+#define SCD_PREC_MIXED  1    /* complex64 inner GMRES, complex128 outer refinement */
+
+typedef struct scd_solve_opts {
+    double  tol;          /* GMRES relative residual (mesh%tol) */
+    int32_t m;            /* Krylov dimension (mesh%maxit) */
+    int32_t cycles;       /* restart cycles (mesh%restart) */
+    int32_t block;        /* right-hand sides solved together; 0 = all */
+    int32_t precision;    /* SCD_PREC_FP64 or SCD_PREC_MIXED */
+    double  inner_tol;    /* mixed: inner complex64 GMRES tolerance */
+    int32_t max_outer;    /* mixed: outer refinement steps */
+} scd_solve_opts;
+
+/* --- context ----------------------------------------------------------- */
+
+/* Replaces the workspace set-up of gmres_module (src/gmres_module.f90:34-53). */
+SCD_API int scd_create(scd_ctx **ctx, const scd_grid_desc *desc);
+SCD_API int scd_destroy(scd_ctx *ctx);
+SCD_API const char *scd_last_error(const scd_ctx *ctx);
+
+/* mesh%k for the current wavelength (src/T_matrix.f90:52). */
+SCD_API int scd_set_wavenumber(scd_ctx *ctx, double k);
+
+/* matrices%Fg (src/build_G.f90:22-64).  NULL builds it on the device from
+ * delta, min_coord and k (requires scd_set_wavenumber first). */
+SCD_API int scd_set_green(scd_ctx *ctx, const scd_c128 *Fg);
+
+/* matrices%S/Sx/Sy/Sz/indS (src/projection.f90:155-164). M_box must be 27. */
+SCD_API int scd_set_projectors(scd_ctx *ctx, int32_t M_box, int32_t T,
+                       const scd_c128 *S, const scd_c128 *Sx, const scd_c128 *Sy,
+                       const scd_c128 *Sz, const int32_t *indS);
+
+/* matrices%sp_mat / sp_ind (src/precorrection.f90:251-254).  sp_mat points to
+ * scd_c64 when storage_prec == SCD_STORE_C64 and to scd_c128 otherwise; the
+ * device copy is kept in the same precision. */
+SCD_API int scd_set_nearzone(scd_ctx *ctx, int64_t B, const void *sp_mat, const int32_t *sp_ind,
+                     int32_t storage_prec);
+
+/* --- device-side setup --------------------------------------------------- */
+
+/* build_grid (src/geometry.f90:60-125) on the host: fills desc from the mesh.
+ * grid_size is the "cell_size" parameter (mesh%grid_size). */
+SCD_API int scd_grid_from_mesh(int32_t Nv, const double *coord, int32_t T, const int32_t *etopol,
+                       double grid_size, int32_t M_ex, scd_grid_desc *desc);
+
+/* mesh%coord (3,Nv), mesh%etopol (4,T) 1-based, mesh%param (T) complex eps. */
+SCD_API int scd_set_mesh(scd_ctx *ctx, int32_t Nv, const double *coord, const int32_t *etopol,
+                 const scd_c128 *param);
+
+/* pfft_projection_const (src/projection.f90:17-166) on the device. */
+SCD_API int scd_build_projectors(scd_ctx *ctx);
+
+/* compute_near_zone_interactions_const (src/precorrection.f90:131-264) on the
+ * device, FP64 arithmetic, stored in storage_prec. */
+SCD_API int scd_build_nearzone(scd_ctx *ctx, int32_t storage_prec);
+
+/* Copy the device operator back in the reference's layouts (for a Fortran
+ * host that keeps its own copy, and for checking). */
+SCD_API int scd_get_projectors(scd_ctx *ctx, scd_c128 *S, scd_c128 *Sx, scd_c128 *Sy, scd_c128 *Sz,
+                       int32_t *indS);
+SCD_API int64_t scd_nearzone_count(scd_ctx *ctx);
+SCD_API int scd_get_nearzone(scd_ctx *ctx, int64_t B, scd_c128 *sp_mat, int32_t *sp_ind);
+
+/* --- the hot path ------------------------------------------------------- */
+
+/* compute_Ax2 (src/gmres_module.f90:57-176): Ax = A x. */
+SCD_API int scd_matvec(scd_ctx *ctx, const scd_c128 *x, scd_c128 *Ax);
+
+/* gmres (src/gmres_module.f90:180-325): x0 = rhs, GMRES(m) with `cycles`
+ * restarts, stop when |g(i+1)|/||rhs|| < tol.  Returns SCD_NOT_CONVERGED with
+ * the last iterate in x when the cycles run out. */
+SCD_API int scd_gmres(scd_ctx *ctx, const scd_c128 *rhs, scd_c128 *x, double tol, int32_t m,
+              int32_t cycles, int32_t *iters, double *relres);
+
+/* The column loop of compute_T_matrix (src/T_matrix.f90:254-268): solve
+ * A X = mat column by column (in blocks of opts->block right-hand sides) and
+ * return Tcols = matᴴ·X.  iters (ncol) receives per-column Arnoldi steps;
+ * X (3T, ncol) receives the solutions when non-NULL. */
+SCD_API int scd_solve_columns(scd_ctx *ctx, int32_t ncol, const scd_c128 *mat, scd_c128 *Tcols,
+                      const scd_solve_opts *opts, int32_t *iters, scd_c128 *X);
+
+/* vswf2constant (src/T_matrix.f90:280-305) on the device: mat (3T, 2nm) for
+ * the mesh set by scd_set_mesh and the current wavenumber. */
+SCD_API int scd_vswf_rhs(scd_ctx *ctx, int32_t Nmax, scd_c128 *mat);
+
+/* Per-kernel timing of the last scd_matvec / solve, milliseconds (CUDA events). */
+typedef struct scd_timing {
+    double matvec_ms;      /* average matvec */
+    double nearzone_ms;    /* average near-zone kernel */
+    double fft_ms;         /* average FFT convolution chain */
+    double arnoldi_ms;     /* average orthogonalisation step */
+    int64_t launches;      /* kernels launched by the last call */
+} scd_timing;
+SCD_API int scd_get_timing(scd_ctx *ctx, scd_timing *t);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SCADYN_GPU_H */

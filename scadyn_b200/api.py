@@ -1,0 +1,286 @@
+"""Host-side mirror of scadyn's solver interface over the C ABI of
+``libscadyn_gpu.so`` (include/scadyn_gpu.h).
+
+Names follow the reference: ``compute_Ax2`` (src/gmres_module.f90:57),
+``gmres`` (:180), ``compute_T_matrix`` (src/T_matrix.f90:240), ``build_G``
+(src/build_G.f90), ``pfft_projection_const`` (src/projection.f90:17),
+``compute_near_zone_interactions_const`` (src/precorrection.f90:131),
+``vswf2constant`` (src/T_matrix.f90:280).  Arrays use the reference's Fortran
+layouts, stored C-contiguous with the shape reversed (``S`` is ``(T, 27)``
+memory of Fortran ``S(27, T)``).
+
+There is no CPU fallback: importing succeeds without a GPU, but every call
+that computes needs the CUDA library and a device and raises otherwise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libscadyn_gpu.so")
+
+SCD_OK, SCD_NOT_CONVERGED, SCD_NAN, SCD_OOM, SCD_BAD_ARG, SCD_TIMEOUT, SCD_CUDA_ERROR, SCD_NOT_READY, SCD_NO_DEVICE = range(9)
+STORE_C64, STORE_C128 = 32, 64
+PREC_FP64, PREC_MIXED = 0, 1
+
+_NAMES = {0: "SCD_OK", 1: "SCD_NOT_CONVERGED", 2: "SCD_NAN", 3: "SCD_OOM", 4: "SCD_BAD_ARG",
+          5: "SCD_TIMEOUT", 6: "SCD_CUDA_ERROR", 7: "SCD_NOT_READY", 8: "SCD_NO_DEVICE"}
+
+# every symbol declared in include/scadyn_gpu.h
+EXPORTS = [
+    "scd_create", "scd_destroy", "scd_last_error", "scd_set_wavenumber", "scd_set_green",
+    "scd_set_projectors", "scd_set_nearzone", "scd_grid_from_mesh", "scd_set_mesh",
+    "scd_build_projectors", "scd_build_nearzone", "scd_get_projectors", "scd_nearzone_count",
+    "scd_get_nearzone", "scd_matvec", "scd_gmres", "scd_solve_columns", "scd_vswf_rhs",
+    "scd_get_timing",
+]
+
+
+class ScadynError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("Nx", C.c_int32), ("Ny", C.c_int32), ("Nz", C.c_int32), ("delta", C.c_double),
+                ("min_coord", C.c_double * 3), ("T", C.c_int32), ("order", C.c_int32),
+                ("M_ex", C.c_int32), ("near_zone", C.c_int32), ("device", C.c_int32)]
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("tol", C.c_double), ("m", C.c_int32), ("cycles", C.c_int32), ("block", C.c_int32),
+                ("precision", C.c_int32), ("inner_tol", C.c_double), ("max_outer", C.c_int32)]
+
+
+class Timing(C.Structure):
+    _fields_ = [("matvec_ms", C.c_double), ("nearzone_ms", C.c_double), ("fft_ms", C.c_double),
+                ("arnoldi_ms", C.c_double), ("launches", C.c_int64)]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libscadyn_gpu.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ScadynError(SCD_NOT_READY, f"{path} is missing: run scadyn_b200.build.build() (nvcc, sm_100a)")
+    lib = C.CDLL(path)
+    vp, i32, i64, dbl = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+    sig = {
+        "scd_create": ([C.POINTER(vp), C.POINTER(GridDesc)], C.c_int),
+        "scd_destroy": ([vp], C.c_int),
+        "scd_last_error": ([vp], C.c_char_p),
+        "scd_set_wavenumber": ([vp, dbl], C.c_int),
+        "scd_set_green": ([vp, vp], C.c_int),
+        "scd_set_projectors": ([vp, i32, i32, vp, vp, vp, vp, vp], C.c_int),
+        "scd_set_nearzone": ([vp, i64, vp, vp, i32], C.c_int),
+        "scd_grid_from_mesh": ([i32, vp, i32, vp, dbl, i32, C.POINTER(GridDesc)], C.c_int),
+        "scd_set_mesh": ([vp, i32, vp, vp, vp], C.c_int),
+        "scd_build_projectors": ([vp], C.c_int),
+        "scd_build_nearzone": ([vp, i32], C.c_int),
+        "scd_get_projectors": ([vp, vp, vp, vp, vp, vp], C.c_int),
+        "scd_nearzone_count": ([vp], C.c_int64),
+        "scd_get_nearzone": ([vp, i64, vp, vp], C.c_int),
+        "scd_matvec": ([vp, vp, vp], C.c_int),
+        "scd_gmres": ([vp, vp, vp, dbl, i32, i32, C.POINTER(i32), C.POINTER(dbl)], C.c_int),
+        "scd_solve_columns": ([vp, i32, vp, vp, C.POINTER(SolveOpts), vp, vp], C.c_int),
+        "scd_vswf_rhs": ([vp, i32, vp], C.c_int),
+        "scd_get_timing": ([vp, C.POINTER(Timing)], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = lib
+    return lib
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else C.c_void_p(0)
+
+
+def _c128(a):
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+def grid_from_mesh(coord, etopol, grid_size=1.8, M_ex=2) -> GridDesc:
+    """build_grid (src/geometry.f90:60-125) -> GridDesc."""
+    lib = load_library()
+    coord = np.ascontiguousarray(coord, np.float64)
+    etopol = np.ascontiguousarray(etopol, np.int32)
+    d = GridDesc()
+    rc = lib.scd_grid_from_mesh(coord.shape[0], _p(coord), etopol.shape[0], _p(etopol), grid_size, M_ex, C.byref(d))
+    if rc:
+        raise ScadynError(rc, "scd_grid_from_mesh")
+    return d
+
+
+@dataclass
+class GridInfo:
+    Nx: int
+    Ny: int
+    Nz: int
+    delta: float
+    min_coord: tuple
+    T: int
+
+
+class Solver:
+    """One device context (scd_ctx) for one mesh and grid."""
+
+    def __init__(self, Nx, Ny, Nz, delta, min_coord, T, device=0):
+        self.lib = load_library()
+        d = GridDesc()
+        d.Nx, d.Ny, d.Nz, d.delta = Nx, Ny, Nz, delta
+        for i in range(3):
+            d.min_coord[i] = float(min_coord[i])
+        d.T, d.order, d.M_ex, d.near_zone, d.device = T, 0, 2, 1, device
+        self.desc = d
+        self.T = T
+        self.n = 3 * T
+        h = C.c_void_p()
+        rc = self.lib.scd_create(C.byref(h), C.byref(d))
+        self.ctx = h
+        if rc:
+            msg = self.lib.scd_last_error(h).decode() if h.value else "scd_create"
+            if h.value:
+                self.lib.scd_destroy(h)
+                self.ctx = C.c_void_p()
+            raise ScadynError(rc, msg)
+
+    @classmethod
+    def from_desc(cls, d: GridDesc, device=0):
+        return cls(d.Nx, d.Ny, d.Nz, d.delta, list(d.min_coord), d.T, device)
+
+    def _chk(self, rc, what, ok=(SCD_OK,)):
+        if rc not in ok:
+            raise ScadynError(rc, f"{what}: {self.lib.scd_last_error(self.ctx).decode()}")
+        return rc
+
+    def close(self):
+        if self.ctx and self.ctx.value:
+            self.lib.scd_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- operator pieces
+    def set_wavenumber(self, k):
+        self._chk(self.lib.scd_set_wavenumber(self.ctx, float(k)), "set_wavenumber")
+
+    def build_G(self, Fg=None):
+        """matrices%Fg; None builds it on the device (src/build_G.f90)."""
+        if Fg is None:
+            self._chk(self.lib.scd_set_green(self.ctx, None), "build_G")
+        else:
+            Fg = _c128(Fg)
+            self._chk(self.lib.scd_set_green(self.ctx, _p(Fg)), "set_green")
+
+    def set_projectors(self, S, Sx, Sy, Sz, indS):
+        S, Sx, Sy, Sz = (_c128(a) for a in (S, Sx, Sy, Sz))
+        indS = np.ascontiguousarray(indS, np.int32)
+        self._chk(self.lib.scd_set_projectors(self.ctx, 27, self.T, _p(S), _p(Sx), _p(Sy), _p(Sz), _p(indS)),
+                  "set_projectors")
+
+    def set_nearzone(self, sp_mat, sp_ind):
+        sp_ind = np.ascontiguousarray(sp_ind, np.int32)
+        if sp_mat.dtype == np.complex64:
+            sp = np.ascontiguousarray(sp_mat)
+            prec = STORE_C64
+        else:
+            sp = _c128(sp_mat)
+            prec = STORE_C128
+        self._chk(self.lib.scd_set_nearzone(self.ctx, sp_ind.shape[0], _p(sp), _p(sp_ind), prec), "set_nearzone")
+
+    def set_mesh(self, coord, etopol, param):
+        self._coord = np.ascontiguousarray(coord, np.float64)
+        self._etopol = np.ascontiguousarray(etopol, np.int32)
+        self._param = _c128(param)
+        self._chk(self.lib.scd_set_mesh(self.ctx, self._coord.shape[0], _p(self._coord), _p(self._etopol),
+                                        _p(self._param)), "set_mesh")
+
+    def pfft_projection_const(self):
+        """Projectors on the device; returns (S, Sx, Sy, Sz, indS) in the reference layout."""
+        self._chk(self.lib.scd_build_projectors(self.ctx), "build_projectors")
+        return self.get_projectors()
+
+    def get_projectors(self):
+        S, Sx, Sy, Sz = (np.zeros((self.T, 27), np.complex128) for _ in range(4))
+        indS = np.zeros((self.T, 27), np.int32)
+        self._chk(self.lib.scd_get_projectors(self.ctx, _p(S), _p(Sx), _p(Sy), _p(Sz), _p(indS)), "get_projectors")
+        return S, Sx, Sy, Sz, indS
+
+    def compute_near_zone_interactions_const(self, storage=STORE_C64):
+        self._chk(self.lib.scd_build_nearzone(self.ctx, storage), "build_nearzone")
+
+    def get_nearzone(self):
+        B = self.lib.scd_nearzone_count(self.ctx)
+        if B < 0:
+            raise ScadynError(SCD_NOT_READY, "near zone not set")
+        sp = np.zeros((B, 3, 3), np.complex128)
+        ind = np.zeros((B, 2), np.int32)
+        self._chk(self.lib.scd_get_nearzone(self.ctx, B, _p(sp), _p(ind)), "get_nearzone")
+        return sp, ind
+
+    # --- hot path
+    def compute_Ax2(self, x):
+        x = _c128(x)
+        Ax = np.zeros_like(x)
+        self._chk(self.lib.scd_matvec(self.ctx, _p(x), _p(Ax)), "matvec")
+        return Ax
+
+    def gmres(self, rhs, tol=1e-5, m=50, cycles=4):
+        rhs = _c128(rhs)
+        x = np.zeros_like(rhs)
+        it = C.c_int32()
+        rr = C.c_double()
+        rc = self._chk(self.lib.scd_gmres(self.ctx, _p(rhs), _p(x), tol, m, cycles, C.byref(it), C.byref(rr)),
+                       "gmres", ok=(SCD_OK, SCD_NOT_CONVERGED))
+        return x, {"iters": it.value, "relres": rr.value, "converged": rc == SCD_OK}
+
+    def vswf2constant(self, Nmax):
+        nm = (Nmax + 1) ** 2 - 1
+        mat = np.zeros((2 * nm, self.n), np.complex128)
+        self._chk(self.lib.scd_vswf_rhs(self.ctx, Nmax, _p(mat)), "vswf_rhs")
+        return mat
+
+    def solve_columns(self, mat, tol=1e-5, m=50, cycles=4, block=1, precision=PREC_FP64,
+                      inner_tol=1e-3, max_outer=10, want_x=False):
+        """The column loop of compute_T_matrix: returns (T_mat (ncol, ncol)
+        memory of Fortran T_mat(ncol,ncol) i.e. out[c, r] = T(r, c), iters, X)."""
+        mat = _c128(mat)
+        ncol = mat.shape[0]
+        Tc = np.zeros((ncol, ncol), np.complex128)
+        iters = np.zeros(ncol, np.int32)
+        X = np.zeros_like(mat) if want_x else None
+        o = SolveOpts(tol, m, cycles, block, precision, inner_tol, max_outer)
+        rc = self._chk(self.lib.scd_solve_columns(self.ctx, ncol, _p(mat), _p(Tc), C.byref(o), _p(iters), _p(X)),
+                       "solve_columns", ok=(SCD_OK, SCD_NOT_CONVERGED))
+        return Tc, iters, X, rc
+
+    def compute_T_matrix(self, Nmax, k, mat=None, **kw):
+        """compute_T_matrix (src/T_matrix.f90:240-277): returns Taa, Tab, Tba, Tbb."""
+        if mat is None:
+            mat = self.vswf2constant(Nmax)
+        Tc, iters, _, _ = self.solve_columns(mat, **kw)
+        T = Tc.T * (1j * k ** 3)
+        nm = (Nmax + 1) ** 2 - 1
+        return T[:nm, :nm], T[:nm, nm:], T[nm:, :nm], T[nm:, nm:], iters
+
+    def timing(self):
+        t = Timing()
+        self.lib.scd_get_timing(self.ctx, C.byref(t))
+        return {"matvec_ms": t.matvec_ms, "nearzone_ms": t.nearzone_ms, "fft_ms": t.fft_ms,
+                "arnoldi_ms": t.arnoldi_ms, "launches": t.launches}

@@ -1,0 +1,461 @@
+// C-ABI entry points of scadyn_gpu (include/scadyn_gpu.h) and the host-side
+// set-up that prepares device layouts: tet ordering by projection box,
+// near-zone tiling, work buffers.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <unordered_map>
+#include <vector>
+
+#include "ctx.h"
+
+// ------------------------------------------------------------------ errors
+int set_error(scd_ctx *c, int code, const char *fmt, ...) {
+    if (!c) return code;
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    c->err = buf;
+    return code;
+}
+
+int check_cuda(scd_ctx *c, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return SCD_OK;
+    if (e == cudaErrorMemoryAllocation) return set_error(c, SCD_OOM, "%s: %s", what, cudaGetErrorString(e));
+    return set_error(c, SCD_CUDA_ERROR, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(expr, what)                                  \
+    do {                                                \
+        int _rc = check_cuda(c, (expr), (what));        \
+        if (_rc) return _rc;                            \
+    } while (0)
+
+static int next_pow2(int v) {
+    int p = 8;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+template <typename Tp>
+static int dalloc(scd_ctx *c, Tp **p, size_t count, const char *what) {
+    if (*p) { cudaFree(*p); *p = nullptr; }
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void **)p, sizeof(Tp) * count);
+    if (e != cudaSuccess) { *p = nullptr; cudaGetLastError(); return set_error(c, SCD_OOM, "allocating %s (%zu bytes)", what, sizeof(Tp) * count); }
+    return SCD_OK;
+}
+
+// -------------------------------------------------------------- work area
+int ensure_work(scd_ctx *c, int nrhs) {
+    if (c->nrhs_cap >= nrhs && c->d_x) return SCD_OK;
+    int rc;
+    const size_t r = (size_t)nrhs;
+    if ((rc = dalloc(c, &c->d_bpart, r * c->ncubes * 4 * 27, "box partials"))) return rc;
+    if ((rc = dalloc(c, &c->d_W, r * 4 * (size_t)c->Px * c->Py * c->Nz, "FFT work grid"))) return rc;
+    if ((rc = dalloc(c, &c->d_R, r * 4 * (size_t)c->Nx * c->Ny * c->Nz, "result grid"))) return rc;
+    if ((rc = dalloc(c, &c->d_nzpart, r * (size_t)std::max<long long>(c->part_len, 1), "near-zone partials"))) return rc;
+    if ((rc = dalloc(c, &c->d_x, r * c->n, "x"))) return rc;
+    if ((rc = dalloc(c, &c->d_y, r * c->n, "y"))) return rc;
+    if ((rc = dalloc(c, &c->d_io, r * c->n, "io"))) return rc;
+    if ((rc = dalloc(c, &c->d_rhs, r * c->n, "rhs"))) return rc;
+    c->nrhs_cap = nrhs;
+    return SCD_OK;
+}
+
+// ---------------------------------------------------------------- ordering
+// Slot order: tets sorted by cube, ties by original index (tetras_in_cubes,
+// src/geometry.f90:330-377, lists each cube's tets in increasing order).
+static int set_order(scd_ctx *c, const std::vector<int> &cube_of_tet) {
+    const int T = c->T;
+    std::vector<int> cnt(c->ncubes + 1, 0);
+    for (int t = 0; t < T; ++t) cnt[cube_of_tet[t] + 1]++;
+    for (int q = 0; q < c->ncubes; ++q) cnt[q + 1] += cnt[q];
+    std::vector<int> perm(T), slot_of(T), cos(T);
+    std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+    for (int t = 0; t < T; ++t) {
+        int s = fill[cube_of_tet[t]]++;
+        perm[s] = t;
+        slot_of[t] = s;
+        cos[s] = cube_of_tet[t];
+    }
+    if (c->have_order) {
+        if (perm != c->perm) {
+            // a different binning invalidates anything stored in slot order
+            c->have_proj = false;
+            c->have_near = false;
+        } else {
+            return SCD_OK;
+        }
+    }
+    c->perm.swap(perm);
+    c->slot_of.swap(slot_of);
+    c->cube_of_slot.swap(cos);
+    c->cube_off = cnt;
+    c->max_per_cube = 0;
+    for (int q = 0; q < c->ncubes; ++q) c->max_per_cube = std::max(c->max_per_cube, cnt[q + 1] - cnt[q]);
+    int rc;
+    if ((rc = dalloc(c, &c->d_perm, T, "perm"))) return rc;
+    if ((rc = dalloc(c, &c->d_cube_off, c->ncubes + 1, "cube offsets"))) return rc;
+    CK(cudaMemcpy(c->d_perm, c->perm.data(), sizeof(int) * T, cudaMemcpyHostToDevice), "perm");
+    CK(cudaMemcpy(c->d_cube_off, c->cube_off.data(), sizeof(int) * (c->ncubes + 1), cudaMemcpyHostToDevice), "cube offsets");
+    c->have_order = true;
+    return SCD_OK;
+}
+
+// ------------------------------------------------------------ near tiles
+template <typename ST>
+static void put_block(ST *dst, const ST *src, bool transpose) {
+    for (int r = 0; r < 3; ++r)
+        for (int q = 0; q < 3; ++q) dst[r + 3 * q] = transpose ? src[q + 3 * r] : src[r + 3 * q];
+}
+template <typename ST>
+static void add_block(ST *dst, const ST *src, bool transpose) {
+    for (int r = 0; r < 3; ++r)
+        for (int q = 0; q < 3; ++q) {
+            const ST v = transpose ? src[q + 3 * r] : src[r + 3 * q];
+            dst[r + 3 * q].x += v.x;
+            dst[r + 3 * q].y += v.y;
+        }
+}
+
+// Tile the reference's symmetric block list (tet_B >= tet_T) into dense
+// cube-pair tiles; see NearTile in ctx.h.  Blocks given twice are summed, as
+// the reference's SpMV would sum them.
+template <typename ST>
+static int build_tiles(scd_ctx *c, int64_t B, const ST *sp, const int32_t *ind) {
+    const int T = c->T;
+    std::unordered_map<uint64_t, int> tid;
+    tid.reserve((size_t)c->ncubes * 16);
+    std::vector<uint64_t> keys;
+    std::vector<int> btile((size_t)B);
+    for (int64_t b = 0; b < B; ++b) {
+        const int t1 = ind[2 * b] - 1, t2 = ind[2 * b + 1] - 1;
+        if (t1 < 0 || t1 >= T || t2 < 0 || t2 >= T)
+            return set_error(c, SCD_BAD_ARG, "sp_ind(:,%lld) = (%d,%d) outside 1..%d", (long long)b + 1, t1 + 1, t2 + 1, T);
+        const int ca = c->cube_of_slot[c->slot_of[t1]], cb = c->cube_of_slot[c->slot_of[t2]];
+        const uint64_t key = (uint64_t)std::min(ca, cb) * (uint64_t)c->ncubes + (uint64_t)std::max(ca, cb);
+        auto it = tid.find(key);
+        int id;
+        if (it == tid.end()) { id = (int)keys.size(); tid.emplace(key, id); keys.push_back(key); }
+        else id = it->second;
+        btile[b] = id;
+    }
+    const int nt = (int)keys.size();
+    std::vector<int> order(nt);
+    for (int i = 0; i < nt; ++i) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return keys[a] < keys[b]; });
+    std::vector<int> rank(nt);
+    for (int i = 0; i < nt; ++i) rank[order[i]] = i;
+    std::vector<NearTile> tiles(nt);
+    std::vector<int> cnt(c->ncubes, 0);
+    long long off = 0;
+    for (int i = 0; i < nt; ++i) {
+        const uint64_t key = keys[order[i]];
+        NearTile &tl = tiles[i];
+        tl.c1 = (int)(key / c->ncubes);
+        tl.c2 = (int)(key % c->ncubes);
+        tl.n1 = c->cube_off[tl.c1 + 1] - c->cube_off[tl.c1];
+        tl.n2 = c->cube_off[tl.c2 + 1] - c->cube_off[tl.c2];
+        tl.data_off = off;
+        off += (long long)tl.n1 * tl.n2;
+        cnt[tl.c1]++;
+        if (tl.c2 != tl.c1) cnt[tl.c2]++;
+    }
+    // partial slots per cube, in tile order
+    c->pslot_base.assign(c->ncubes + 1, 0);
+    c->pslot_cnt = cnt;
+    for (int q = 0; q < c->ncubes; ++q) {
+        const int nq = c->cube_off[q + 1] - c->cube_off[q];
+        c->pslot_base[q + 1] = c->pslot_base[q] + (long long)cnt[q] * 3 * nq;
+    }
+    std::vector<int> used(c->ncubes, 0);
+    for (int i = 0; i < nt; ++i) {
+        NearTile &tl = tiles[i];
+        tl.row_off = c->pslot_base[tl.c1] + (long long)(used[tl.c1]++) * 3 * tl.n1;
+        tl.col_off = -1;
+        if (tl.c2 != tl.c1) tl.col_off = c->pslot_base[tl.c2] + (long long)(used[tl.c2]++) * 3 * tl.n2;
+    }
+    std::vector<ST> data((size_t)off * 9);
+    std::memset(data.data(), 0, sizeof(ST) * data.size());
+    std::vector<char> seen((size_t)off, 0);
+    for (int64_t b = 0; b < B; ++b) {
+        const NearTile &tl = tiles[rank[btile[b]]];
+        const int t1 = ind[2 * b] - 1, t2 = ind[2 * b + 1] - 1;
+        const int s1 = c->slot_of[t1], s2 = c->slot_of[t2];
+        const int ca = c->cube_of_slot[s1];
+        const ST *src = sp + 9 * b;
+        // position of (row tet, column tet) in the tile and whether the block
+        // must be transposed (M(B,T) = M(T,B)^T)
+        auto place = [&](int srow, int scol, bool tr) {
+            const int i = srow - c->cube_off[tl.c1], j = scol - c->cube_off[tl.c2];
+            const size_t e = (size_t)tl.data_off + (size_t)i * tl.n2 + j;
+            if (seen[e]) add_block(&data[9 * e], src, tr);
+            else { put_block(&data[9 * e], src, tr); seen[e] = 1; }
+        };
+        if (tl.c1 == tl.c2) {
+            place(s1, s2, false);
+            if (s1 != s2) place(s2, s1, true);
+        } else if (ca == tl.c1) {
+            place(s1, s2, false);
+        } else {
+            place(s2, s1, true);
+        }
+    }
+    int rc;
+    if ((rc = dalloc(c, (ST **)&c->d_tdata, data.size(), "near-zone tiles"))) return rc;
+    if ((rc = dalloc(c, &c->d_tiles, nt, "tile table"))) return rc;
+    if ((rc = dalloc(c, &c->d_pslot_base, c->ncubes + 1, "slot bases"))) return rc;
+    if ((rc = dalloc(c, &c->d_pslot_cnt, c->ncubes, "slot counts"))) return rc;
+    CK(cudaMemcpy(c->d_tdata, data.data(), sizeof(ST) * data.size(), cudaMemcpyHostToDevice), "tiles");
+    CK(cudaMemcpy(c->d_tiles, tiles.data(), sizeof(NearTile) * nt, cudaMemcpyHostToDevice), "tile table");
+    CK(cudaMemcpy(c->d_pslot_base, c->pslot_base.data(), sizeof(long long) * (c->ncubes + 1), cudaMemcpyHostToDevice), "slots");
+    CK(cudaMemcpy(c->d_pslot_cnt, c->pslot_cnt.data(), sizeof(int) * c->ncubes, cudaMemcpyHostToDevice), "slots");
+    c->ntiles = nt;
+    c->tile_blocks = off;
+    c->part_len = c->pslot_base[c->ncubes];
+    c->tiles_h.swap(tiles);
+    c->B_ref = B;
+    c->nrhs_cap = 0;   // partial buffer size changed
+    return SCD_OK;
+}
+
+// ------------------------------------------------------------------ ABI
+extern "C" {
+
+const char *scd_last_error(const scd_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int scd_create(scd_ctx **out, const scd_grid_desc *d) {
+    if (!out || !d) return SCD_BAD_ARG;
+    *out = nullptr;
+    if (d->order != 0 || d->M_ex != 2 || d->near_zone != 1) return SCD_BAD_ARG;
+    if (d->Nx < 4 || d->Ny < 4 || d->Nz < 4 || d->T <= 0 || !(d->delta > 0)) return SCD_BAD_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return SCD_NO_DEVICE; }
+    if (d->device < 0 || d->device >= ndev) return SCD_BAD_ARG;
+    scd_ctx *c = new scd_ctx();
+    c->d = *d;
+    c->dev = d->device;
+    cudaSetDevice(c->dev);
+    cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev);
+    c->Nx = d->Nx; c->Ny = d->Ny; c->Nz = d->Nz;
+    c->Px = next_pow2(2 * d->Nx); c->Py = next_pow2(2 * d->Ny); c->Pz = next_pow2(2 * d->Nz);
+    if (c->Px > 512 || c->Py > 512 || c->Pz > 512) {
+        set_error(c, SCD_BAD_ARG, "grid %dx%dx%d needs an FFT longer than 512", d->Nx, d->Ny, d->Nz);
+        *out = c;
+        return SCD_BAD_ARG;
+    }
+    c->Hx = c->Px / 2 + 1; c->Hy = c->Py / 2 + 1; c->Hz = c->Pz / 2 + 1;
+    c->ncx = (d->Nx - 2) / 2; c->ncy = (d->Ny - 2) / 2; c->ncz = (d->Nz - 2) / 2;
+    c->ncubes = c->ncx * c->ncy * c->ncz;
+    c->T = d->T;
+    c->n = 3LL * d->T;
+    *out = c;
+    int rc;
+    if ((rc = check_cuda(c, cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking), "stream"))) return rc;
+    for (int i = 0; i < 8; ++i) cudaEventCreate(&c->ev[i]);
+    const int Ps[3] = {c->Px, c->Py, c->Pz};
+    for (int a = 0; a < 3; ++a)
+        if ((rc = build_twiddles(c, Ps[a], &c->d_tw[a]))) return rc;
+    return check_cuda(c, cudaStreamSynchronize(c->st), "create");
+}
+
+int scd_destroy(scd_ctx *c) {
+    if (!c) return SCD_OK;
+    cudaSetDevice(c->dev);
+    if (c->st) cudaStreamSynchronize(c->st);
+    void *ptrs[] = {c->d_perm, c->d_cube_off, c->d_P, c->d_Fo, c->d_tdata, c->d_tiles, c->d_pslot_base,
+                    c->d_pslot_cnt, c->d_tc, c->d_eps, c->d_bpart, c->d_W, c->d_R, c->d_nzpart, c->d_x,
+                    c->d_y, c->d_io, c->d_V, c->d_H, c->d_cs, c->d_sn, c->d_g, c->d_rhs, c->d_w, c->d_red,
+                    c->d_bar, c->d_err, c->d_state, c->d_tw[0], c->d_tw[1], c->d_tw[2]};
+    for (void *p : ptrs) if (p) cudaFree(p);
+    if (c->h_state) cudaFreeHost(c->h_state);
+    for (int i = 0; i < 8; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+    return SCD_OK;
+}
+
+int scd_set_wavenumber(scd_ctx *c, double k) {
+    if (!c) return SCD_BAD_ARG;
+    if (!(k > 0) || !std::isfinite(k)) return set_error(c, SCD_BAD_ARG, "wavenumber %g", k);
+    if (c->have_k && k != c->k) c->have_green = false;   // a device-built Fg is per wavelength
+    c->k = k;
+    c->have_k = true;
+    return SCD_OK;
+}
+
+int scd_set_green(scd_ctx *c, const scd_c128 *Fg) {
+    if (!c) return SCD_BAD_ARG;
+    cudaSetDevice(c->dev);
+    if (!Fg && !c->have_k) return set_error(c, SCD_NOT_READY, "scd_set_green(NULL) needs scd_set_wavenumber first");
+    if (Fg && (c->Px != 2 * c->Nx || c->Py != 2 * c->Ny || c->Pz != 2 * c->Nz))
+        return set_error(c, SCD_BAD_ARG,
+                         "host Fg of size (%d,%d,%d) is not a power-of-two FFT; pass NULL to build it on the device",
+                         2 * c->Nx, 2 * c->Ny, 2 * c->Nz);
+    int rc = setup_green(c, Fg);
+    if (rc == SCD_OK) c->have_green = true;
+    return rc;
+}
+
+int scd_set_projectors(scd_ctx *c, int32_t M_box, int32_t T, const scd_c128 *S, const scd_c128 *Sx,
+                       const scd_c128 *Sy, const scd_c128 *Sz, const int32_t *indS) {
+    if (!c) return SCD_BAD_ARG;
+    cudaSetDevice(c->dev);
+    if (M_box != 27) return set_error(c, SCD_BAD_ARG, "M_box = %d, only 27 (M_ex = 2) is supported", M_box);
+    if (T != c->T) return set_error(c, SCD_BAD_ARG, "T = %d, context has %d", T, c->T);
+    if (!S || !Sx || !Sy || !Sz || !indS) return set_error(c, SCD_BAD_ARG, "null projector array");
+    // the 27 nodes of every column must be the node block of one projection
+    // box (src/projection.f90:160 stores etopol_box(:, cube))
+    std::vector<int> cube(T);
+    const int Nx = c->Nx, Ny = c->Ny;
+    for (int t = 0; t < T; ++t) {
+        const int32_t *id = indS + 27LL * t;
+        const long long n0 = id[0] - 1;
+        const int x = (int)(n0 % Nx), y = (int)((n0 / Nx) % Ny), z = (int)(n0 / ((long long)Nx * Ny));
+        if (n0 < 0 || (x & 1) || (y & 1) || (z & 1) || x / 2 >= c->ncx || y / 2 >= c->ncy || z / 2 >= c->ncz)
+            return set_error(c, SCD_BAD_ARG, "indS(1,%d) = %d is not the first node of a projection box", t + 1, id[0]);
+        for (int j = 0; j < 27; ++j) {
+            const long long want = n0 + (j % 3) + (long long)((j / 3) % 3) * Nx + (long long)(j / 9) * Nx * Ny + 1;
+            if (id[j] != want) return set_error(c, SCD_BAD_ARG, "indS(%d,%d) = %d, expected %lld", j + 1, t + 1, id[j], want);
+        }
+        cube[t] = x / 2 + c->ncx * (y / 2 + c->ncy * (z / 2));
+    }
+    int rc = set_order(c, cube);
+    if (rc) return rc;
+    std::vector<cd> h((size_t)4 * 27 * T);
+    const scd_c128 *src[4] = {S, Sx, Sy, Sz};
+    for (int g = 0; g < 4; ++g)
+        for (int s = 0; s < T; ++s) {
+            const scd_c128 *p = src[g] + 27LL * c->perm[s];
+            cd *o = h.data() + (size_t)g * 27 * T + 27LL * s;
+            for (int j = 0; j < 27; ++j) o[j] = cmk(p[j].re, p[j].im);
+        }
+    if ((rc = dalloc(c, &c->d_P, h.size(), "projectors"))) return rc;
+    CK(cudaMemcpy(c->d_P, h.data(), sizeof(cd) * h.size(), cudaMemcpyHostToDevice), "projectors");
+    c->have_proj = true;
+    return SCD_OK;
+}
+
+int scd_set_nearzone(scd_ctx *c, int64_t B, const void *sp_mat, const int32_t *sp_ind, int32_t prec) {
+    if (!c) return SCD_BAD_ARG;
+    cudaSetDevice(c->dev);
+    if (!c->have_order) return set_error(c, SCD_NOT_READY, "set the projectors (or the mesh) before the near zone");
+    if (B < 0 || (B > 0 && (!sp_mat || !sp_ind))) return set_error(c, SCD_BAD_ARG, "bad near-zone arrays");
+    if (prec != SCD_STORE_C64 && prec != SCD_STORE_C128) return set_error(c, SCD_BAD_ARG, "storage_prec %d", prec);
+    int rc;
+    c->have_near = false;
+    c->near_prec = prec;
+    if (prec == SCD_STORE_C64) rc = build_tiles<cf>(c, B, (const cf *)sp_mat, sp_ind);
+    else rc = build_tiles<cd>(c, B, (const cd *)sp_mat, sp_ind);
+    if (rc == SCD_OK) c->have_near = true;
+    return rc;
+}
+
+static int ready(scd_ctx *c) {
+    if (!c->have_proj) return set_error(c, SCD_NOT_READY, "projectors not set");
+    if (!c->have_green) return set_error(c, SCD_NOT_READY, "Green's function not set (or stale after a new wavenumber)");
+    if (!c->have_near) return set_error(c, SCD_NOT_READY, "near zone not set");
+    if (!c->have_k) return set_error(c, SCD_NOT_READY, "wavenumber not set");
+    return ensure_work(c, 1);
+}
+
+int scd_matvec(scd_ctx *c, const scd_c128 *x, scd_c128 *Ax) {
+    if (!c || !x || !Ax) return SCD_BAD_ARG;
+    cudaSetDevice(c->dev);
+    int rc = ready(c);
+    if (rc) return rc;
+    const size_t bytes = sizeof(cd) * c->n;
+    CK(cudaMemcpyAsync(c->d_io, x, bytes, cudaMemcpyHostToDevice, c->st), "x");
+    launch_permute_in(c, c->d_io, c->d_x, 1, c->n);
+    c->timing = true;
+    run_matvec(c, c->d_x, c->d_y, 1, nullptr);
+    c->timing = false;
+    launch_permute_out(c, c->d_y, c->d_io, 1, c->n);
+    CK(cudaMemcpyAsync(Ax, c->d_io, bytes, cudaMemcpyDeviceToHost, c->st), "Ax");
+    CK(cudaStreamSynchronize(c->st), "matvec");
+    float a = 0, b = 0, t = 0;
+    cudaEventElapsedTime(&a, c->ev[0], c->ev[1]);
+    cudaEventElapsedTime(&b, c->ev[1], c->ev[2]);
+    cudaEventElapsedTime(&t, c->ev[0], c->ev[3]);
+    c->t_near = a; c->t_fft = b; c->t_matvec = t;
+    return check_cuda(c, cudaGetLastError(), "matvec");
+}
+
+int scd_gmres(scd_ctx *c, const scd_c128 *rhs, scd_c128 *x, double tol, int32_t m, int32_t cycles, int32_t *iters,
+              double *relres) {
+    if (!c || !rhs || !x || m < 1 || cycles < 1 || !(tol > 0)) return SCD_BAD_ARG;
+    cudaSetDevice(c->dev);
+    int rc = ready(c);
+    if (rc) return rc;
+    const size_t bytes = sizeof(cd) * c->n;
+    CK(cudaMemcpyAsync(c->d_io, rhs, bytes, cudaMemcpyHostToDevice, c->st), "rhs");
+    launch_permute_in(c, c->d_io, c->d_rhs, 1, c->n);
+    int it = 0;
+    double rr = 0;
+    rc = gmres_solve(c, c->d_rhs, c->d_x, tol, m, cycles, &it, &rr);
+    if (rc != SCD_OK && rc != SCD_NOT_CONVERGED) return rc;
+    launch_permute_out(c, c->d_x, c->d_io, 1, c->n);
+    CK(cudaMemcpyAsync(x, c->d_io, bytes, cudaMemcpyDeviceToHost, c->st), "x");
+    CK(cudaStreamSynchronize(c->st), "gmres");
+    if (iters) *iters = it;
+    if (relres) *relres = rr;
+    return rc;
+}
+
+int scd_solve_columns(scd_ctx *c, int32_t ncol, const scd_c128 *mat, scd_c128 *Tcols, const scd_solve_opts *o,
+                      int32_t *iters, scd_c128 *X) {
+    if (!c || ncol <= 0 || !mat || !Tcols || !o) return SCD_BAD_ARG;
+    cudaSetDevice(c->dev);
+    int rc = ready(c);
+    if (rc) return rc;
+    const long long n = c->n;
+    cd *d_mat = nullptr, *d_X = nullptr, *d_T = nullptr;
+    if ((rc = dalloc(c, &d_mat, (size_t)n * ncol, "mat"))) return rc;
+    if ((rc = dalloc(c, &d_X, (size_t)n * ncol, "X"))) { cudaFree(d_mat); return rc; }
+    if ((rc = dalloc(c, &d_T, (size_t)ncol * ncol, "T"))) { cudaFree(d_mat); cudaFree(d_X); return rc; }
+    int worst = SCD_OK;
+    for (int col = 0; col < ncol && worst != SCD_NAN && worst != SCD_TIMEOUT; ++col) {
+        CK(cudaMemcpyAsync(c->d_io, mat + (size_t)n * col, sizeof(cd) * n, cudaMemcpyHostToDevice, c->st), "mat");
+        launch_permute_in(c, c->d_io, d_mat + (size_t)n * col, 1, n);
+        int it = 0;
+        double rr = 0;
+        rc = gmres_solve(c, d_mat + (size_t)n * col, d_X + (size_t)n * col, o->tol, o->m, o->cycles, &it, &rr);
+        if (iters) iters[col] = it;
+        if (rc != SCD_OK && rc != SCD_NOT_CONVERGED) { worst = rc; break; }
+        if (rc == SCD_NOT_CONVERGED) worst = SCD_NOT_CONVERGED;
+    }
+    if (worst == SCD_OK || worst == SCD_NOT_CONVERGED) {
+        launch_T_assemble(c, d_mat, ncol, 0, ncol, d_X, d_T);
+        rc = check_cuda(c, cudaMemcpyAsync(Tcols, d_T, sizeof(cd) * ncol * ncol, cudaMemcpyDeviceToHost, c->st), "T");
+        if (!rc && X) {
+            for (int col = 0; col < ncol && !rc; ++col) {
+                launch_permute_out(c, d_X + (size_t)n * col, c->d_io, 1, n);
+                rc = check_cuda(c, cudaMemcpyAsync(X + (size_t)n * col, c->d_io, sizeof(cd) * n, cudaMemcpyDeviceToHost, c->st), "X");
+            }
+        }
+        if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->st), "solve");
+        if (rc) worst = rc;
+    }
+    cudaStreamSynchronize(c->st);
+    cudaFree(d_mat); cudaFree(d_X); cudaFree(d_T);
+    return worst;
+}
+
+int scd_get_timing(scd_ctx *c, scd_timing *t) {
+    if (!c || !t) return SCD_BAD_ARG;
+    t->matvec_ms = c->t_matvec;
+    t->nearzone_ms = c->t_near;
+    t->fft_ms = c->t_fft;
+    t->arnoldi_ms = c->t_arn;
+    t->launches = c->launches;
+    return SCD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,153 @@
+// Internal context of the scadyn_gpu library and the launch wrappers of its
+// kernels.  Device data are kept in "slot order": tetrahedra sorted by the
+// projection box (cube) that holds them, so that every cube's tets, projector
+// columns and unknowns are contiguous.  The public entry points permute at the
+// boundary.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/scadyn_gpu.h"
+#include "common.cuh"
+
+// One dense tile of near-zone blocks coupling the tets of cube c1 (rows) to
+// the tets of cube c2 (columns), c1 <= c2.  Block (i, j) is the 3x3 matrix
+// that maps the unknowns of slot off(c2)+j onto the equations of slot
+// off(c1)+i; it is stored at data[(data_off + i*n2 + j)*9 + r + 3c].
+// Diagonal tiles (c1 == c2) hold the full symmetric n1 x n1 pattern.
+struct NearTile {
+    int c1, c2, n1, n2;
+    long long data_off;   // in blocks
+    long long row_off;    // partial-sum slot of c1 (complex elements)
+    long long col_off;    // partial-sum slot of c2, -1 for diagonal tiles
+};
+
+struct GmresState {
+    double b_norm;     // ||rhs||
+    double beta;       // ||r0|| of the current cycle
+    double error;      // |g(i+1)|/b_norm after the last step
+    int    step;       // Arnoldi steps taken in the current cycle
+    int    done;       // 1 once error < tol (or a fault)
+    int    conv_step;  // step at which the tolerance was met (0 = not yet)
+    int    iters;      // Arnoldi steps over all cycles
+    int    status;     // SCD_OK / SCD_NAN / SCD_TIMEOUT
+    int    reorth;     // re-orthogonalisations taken
+};
+
+struct scd_ctx {
+    int dev = 0;
+    int nsm = 148;
+    cudaStream_t st = nullptr;
+    scd_grid_desc d{};
+    int Nx = 0, Ny = 0, Nz = 0;          // grid nodes
+    int Px = 0, Py = 0, Pz = 0;          // padded FFT lengths (powers of two >= 2N)
+    int Hx = 0, Hy = 0, Hz = 0;          // P/2 + 1 (independent octant of Fg)
+    int ncx = 0, ncy = 0, ncz = 0, ncubes = 0;
+    int T = 0;
+    long long n = 0;                     // 3T unknowns
+    double k = 0.0;
+    bool have_k = false;
+
+    // tet order
+    bool have_order = false;
+    std::vector<int> perm;               // slot -> original tet (0-based)
+    std::vector<int> slot_of;            // original tet -> slot
+    std::vector<int> cube_of_slot;       // slot -> cube
+    std::vector<int> cube_off;           // ncubes + 1
+    int max_per_cube = 0;
+    int *d_perm = nullptr, *d_cube_off = nullptr;
+
+    // projectors: d_P[g*27*T + 27*slot + j], g = S, Sx, Sy, Sz
+    bool have_proj = false;
+    cd *d_P = nullptr;
+
+    cd *d_tw[3] = {nullptr, nullptr, nullptr};   // twiddles for Px, Py, Pz
+
+    // Green octant (Hx*Hy*Hz), pre-scaled by 1/(Px*Py*Pz)
+    bool have_green = false;
+    cd *d_Fo = nullptr;
+
+    // near zone
+    bool have_near = false;
+    int near_prec = SCD_STORE_C64;
+    void *d_tdata = nullptr;
+    NearTile *d_tiles = nullptr;
+    int ntiles = 0;
+    long long tile_blocks = 0;
+    long long B_ref = 0;                 // blocks in the reference layout
+    std::vector<long long> pslot_base;   // per cube, complex offset of its first slot
+    std::vector<int> pslot_cnt;          // per cube, number of slots
+    long long *d_pslot_base = nullptr;
+    int *d_pslot_cnt = nullptr;
+    long long part_len = 0;
+    std::vector<NearTile> tiles_h;
+
+    // mesh (device-side setup)
+    bool have_mesh = false;
+    int Nv = 0;
+    std::vector<double> coord;           // (3, Nv)
+    std::vector<int> etopol;             // (4, T) 1-based
+    std::vector<cd> param;               // (T)
+    double *d_tc = nullptr;              // slot-ordered tet vertex coords (12 per slot)
+    cd *d_eps = nullptr;                 // slot-ordered eps
+
+    // work buffers (sized for nrhs_cap right-hand sides)
+    int nrhs_cap = 0;
+    cd *d_bpart = nullptr;               // nrhs * ncubes * 4 * 27
+    cd *d_W = nullptr;                   // nrhs * 4 * Px*Py*Nz
+    cd *d_R = nullptr;                   // nrhs * 4 * Nx*Ny*Nz
+    cd *d_nzpart = nullptr;              // nrhs * part_len
+    cd *d_x = nullptr, *d_y = nullptr, *d_io = nullptr;   // n each (nrhs_cap)
+
+    // GMRES
+    int gm_m = 0;
+    cd *d_V = nullptr;                   // (m+1) * n
+    cd *d_H = nullptr;                   // (m+1) * m
+    cd *d_cs = nullptr, *d_sn = nullptr, *d_g = nullptr;
+    cd *d_rhs = nullptr, *d_w = nullptr;
+    double *d_red = nullptr;             // 2 * grid * 8 partial sums
+    GridBarrier *d_bar = nullptr;
+    int *d_err = nullptr;
+    GmresState *d_state = nullptr;
+    GmresState *h_state = nullptr;       // pinned
+    int coop_grid = 0;
+
+    // timing
+    cudaEvent_t ev[8] = {};
+    double t_matvec = 0, t_near = 0, t_fft = 0, t_arn = 0;
+    long long n_matvec = 0, n_arn = 0, launches = 0;
+    bool timing = false;
+
+    std::string err;
+};
+
+// ---- launch wrappers (kernels_matvec.cu) ----
+void launch_permute_in(scd_ctx *c, const cd *x_orig, cd *x_slot, int nrhs, long long ld);
+void launch_permute_out(scd_ctx *c, const cd *x_slot, cd *x_orig, int nrhs, long long ld);
+// full matvec y = A x on slot-ordered vectors (nrhs columns, stride n)
+void run_matvec(scd_ctx *c, const cd *x, cd *y, int nrhs, const int *done);
+void launch_near(scd_ctx *c, const cd *x, int nrhs, const int *done);
+void launch_fft_chain(scd_ctx *c, const cd *x, int nrhs, const int *done);
+void launch_gather(scd_ctx *c, const cd *x, cd *y, int nrhs, const int *done);
+int build_twiddles(scd_ctx *c, int P, cd **out);
+
+// ---- GMRES (kernels_gmres.cu) ----
+int gmres_prepare(scd_ctx *c, int m);
+int gmres_solve(scd_ctx *c, const cd *d_rhs_slot, cd *d_x_slot, double tol, int m, int cycles,
+                int *iters, double *relres);
+
+// ---- setup (kernels_setup.cu) ----
+int setup_green(scd_ctx *c, const scd_c128 *Fg_host);
+int setup_projectors_device(scd_ctx *c);
+int setup_nearzone_device(scd_ctx *c, int prec);
+int setup_vswf(scd_ctx *c, int Nmax, cd *d_mat);   // slot-ordered (n, 2nm)
+void launch_T_assemble(scd_ctx *c, const cd *d_mat, int ncol_total, int col0, int ncb,
+                       const cd *d_X, cd *d_T);
+
+// ---- helpers (api.cu) ----
+int set_error(scd_ctx *c, int code, const char *fmt, ...);
+int check_cuda(scd_ctx *c, cudaError_t e, const char *what);
+int ensure_work(scd_ctx *c, int nrhs);

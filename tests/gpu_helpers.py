@@ -1,0 +1,14 @@
+"""Test helpers that connect oracle operator data to the device solver."""
+from scadyn_b200 import api
+
+
+def solver_from_oracle(op, device=0, fg_from_host=False):
+    """Load an oracle operator into a device Solver so that both sides see the
+    same operator data."""
+    g = op.geom
+    s = api.Solver(g.Nx, g.Ny, g.Nz, g.delta, g.min_coord, g.T, device)
+    s.set_wavenumber(g.k)
+    s.set_projectors(op.S, op.Sx, op.Sy, op.Sz, op.indS)
+    s.build_G(op.Fg if fg_from_host else None)
+    s.set_nearzone(op.sp_mat, op.sp_ind)
+    return s

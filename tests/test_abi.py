@@ -1,0 +1,45 @@
+"""The C-ABI library builds for sm_100a, loads without a GPU and exports every
+entry point include/scadyn_gpu.h declares.  No device calls."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from scadyn_b200 import api, build
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "scadyn_gpu.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(scd_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_builds_and_loads():
+    path = build.build()
+    assert os.path.exists(path)
+    lib = ctypes.CDLL(path)
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+
+
+def test_binding_covers_header():
+    assert sorted(api.EXPORTS) == declared_symbols()
+
+
+def test_api_binds_all_signatures():
+    lib = api.load_library()
+    for name in api.EXPORTS:
+        assert getattr(lib, name).restype is not None
+
+
+def test_no_device_is_reported_not_crashed():
+    """Without a GPU scd_create returns SCD_NO_DEVICE instead of failing."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(api.ScadynError) as e:
+        api.Solver(8, 8, 8, 1.0, (0, 0, 0), 10)
+    assert e.value.code == api.SCD_NO_DEVICE
