@@ -125,6 +125,85 @@ static void add_block(ST *dst, const ST *src, bool transpose) {
         }
 }
 
+// Dense tile layout for a sorted list of cube pairs key = c1*ncubes + c2
+// (c1 <= c2): data offsets and per-cube partial-sum slots in tile order.
+static long long layout_tiles(scd_ctx *c, const std::vector<uint64_t> &keys, std::vector<NearTile> &tiles) {
+    const int nt = (int)keys.size();
+    tiles.assign(nt, NearTile{});
+    std::vector<int> cnt(c->ncubes, 0);
+    long long off = 0;
+    for (int i = 0; i < nt; ++i) {
+        NearTile &tl = tiles[i];
+        tl.c1 = (int)(keys[i] / c->ncubes);
+        tl.c2 = (int)(keys[i] % c->ncubes);
+        tl.n1 = c->cube_off[tl.c1 + 1] - c->cube_off[tl.c1];
+        tl.n2 = c->cube_off[tl.c2 + 1] - c->cube_off[tl.c2];
+        tl.data_off = off;
+        off += (long long)tl.n1 * tl.n2;
+        cnt[tl.c1]++;
+        if (tl.c2 != tl.c1) cnt[tl.c2]++;
+    }
+    c->pslot_base.assign(c->ncubes + 1, 0);
+    c->pslot_cnt = cnt;
+    for (int q = 0; q < c->ncubes; ++q) {
+        const int nq = c->cube_off[q + 1] - c->cube_off[q];
+        c->pslot_base[q + 1] = c->pslot_base[q] + (long long)cnt[q] * 3 * nq;
+    }
+    std::vector<int> used(c->ncubes, 0);
+    for (int i = 0; i < nt; ++i) {
+        NearTile &tl = tiles[i];
+        tl.row_off = c->pslot_base[tl.c1] + (long long)(used[tl.c1]++) * 3 * tl.n1;
+        tl.col_off = -1;
+        if (tl.c2 != tl.c1) tl.col_off = c->pslot_base[tl.c2] + (long long)(used[tl.c2]++) * 3 * tl.n2;
+    }
+    return off;
+}
+
+static int upload_layout(scd_ctx *c, std::vector<NearTile> &tiles, long long off) {
+    const int nt = (int)tiles.size();
+    int rc;
+    if ((rc = dalloc(c, &c->d_tiles, nt, "tile table"))) return rc;
+    if ((rc = dalloc(c, &c->d_pslot_base, c->ncubes + 1, "slot bases"))) return rc;
+    if ((rc = dalloc(c, &c->d_pslot_cnt, c->ncubes, "slot counts"))) return rc;
+    CK(cudaMemcpy(c->d_tiles, tiles.data(), sizeof(NearTile) * nt, cudaMemcpyHostToDevice), "tile table");
+    CK(cudaMemcpy(c->d_pslot_base, c->pslot_base.data(), sizeof(long long) * (c->ncubes + 1), cudaMemcpyHostToDevice), "slots");
+    CK(cudaMemcpy(c->d_pslot_cnt, c->pslot_cnt.data(), sizeof(int) * c->ncubes, cudaMemcpyHostToDevice), "slots");
+    c->ntiles = nt;
+    c->tile_blocks = off;
+    c->part_len = c->pslot_base[c->ncubes];
+    c->tiles_h.swap(tiles);
+    c->nrhs_cap = 0;   // partial buffer size changed
+    return SCD_OK;
+}
+
+// Tiles from the geometry: every non-empty cube c1 with each non-empty cube
+// c2 >= c1 of its 27-neighbourhood (find_near_cubes, src/geometry.f90:275-326)
+// — the same tet pairs compute_near_zone_interactions_const visits.
+int build_tile_layout(scd_ctx *c) {
+    std::vector<uint64_t> keys;
+    for (int z = 0; z < c->ncz; ++z)
+        for (int y = 0; y < c->ncy; ++y)
+            for (int x = 0; x < c->ncx; ++x) {
+                const int c1 = x + c->ncx * (y + c->ncy * z);
+                if (c->cube_off[c1 + 1] == c->cube_off[c1]) continue;
+                for (int dz = -1; dz <= 1; ++dz)
+                    for (int dy = -1; dy <= 1; ++dy)
+                        for (int dx = -1; dx <= 1; ++dx) {
+                            const int xx = x + dx, yy = y + dy, zz = z + dz;
+                            if (xx < 0 || yy < 0 || zz < 0 || xx >= c->ncx || yy >= c->ncy || zz >= c->ncz) continue;
+                            const int c2 = xx + c->ncx * (yy + c->ncy * zz);
+                            if (c2 < c1 || c->cube_off[c2 + 1] == c->cube_off[c2]) continue;
+                            keys.push_back((uint64_t)c1 * (uint64_t)c->ncubes + (uint64_t)c2);
+                        }
+            }
+    std::sort(keys.begin(), keys.end());
+    std::vector<NearTile> tiles;
+    const long long off = layout_tiles(c, keys, tiles);
+    return upload_layout(c, tiles, off);
+}
+
+int set_order_from_cubes(scd_ctx *c, const std::vector<int> &cube_of_tet) { return set_order(c, cube_of_tet); }
+
 // Tile the reference's symmetric block list (tet_B >= tet_T) into dense
 // cube-pair tiles; see NearTile in ctx.h.  Blocks given twice are summed, as
 // the reference's SpMV would sum them.
@@ -153,35 +232,10 @@ static int build_tiles(scd_ctx *c, int64_t B, const ST *sp, const int32_t *ind) 
     std::sort(order.begin(), order.end(), [&](int a, int b) { return keys[a] < keys[b]; });
     std::vector<int> rank(nt);
     for (int i = 0; i < nt; ++i) rank[order[i]] = i;
-    std::vector<NearTile> tiles(nt);
-    std::vector<int> cnt(c->ncubes, 0);
-    long long off = 0;
-    for (int i = 0; i < nt; ++i) {
-        const uint64_t key = keys[order[i]];
-        NearTile &tl = tiles[i];
-        tl.c1 = (int)(key / c->ncubes);
-        tl.c2 = (int)(key % c->ncubes);
-        tl.n1 = c->cube_off[tl.c1 + 1] - c->cube_off[tl.c1];
-        tl.n2 = c->cube_off[tl.c2 + 1] - c->cube_off[tl.c2];
-        tl.data_off = off;
-        off += (long long)tl.n1 * tl.n2;
-        cnt[tl.c1]++;
-        if (tl.c2 != tl.c1) cnt[tl.c2]++;
-    }
-    // partial slots per cube, in tile order
-    c->pslot_base.assign(c->ncubes + 1, 0);
-    c->pslot_cnt = cnt;
-    for (int q = 0; q < c->ncubes; ++q) {
-        const int nq = c->cube_off[q + 1] - c->cube_off[q];
-        c->pslot_base[q + 1] = c->pslot_base[q] + (long long)cnt[q] * 3 * nq;
-    }
-    std::vector<int> used(c->ncubes, 0);
-    for (int i = 0; i < nt; ++i) {
-        NearTile &tl = tiles[i];
-        tl.row_off = c->pslot_base[tl.c1] + (long long)(used[tl.c1]++) * 3 * tl.n1;
-        tl.col_off = -1;
-        if (tl.c2 != tl.c1) tl.col_off = c->pslot_base[tl.c2] + (long long)(used[tl.c2]++) * 3 * tl.n2;
-    }
+    std::vector<uint64_t> skeys(nt);
+    for (int i = 0; i < nt; ++i) skeys[i] = keys[order[i]];
+    std::vector<NearTile> tiles;
+    const long long off = layout_tiles(c, skeys, tiles);
     std::vector<ST> data((size_t)off * 9);
     std::memset(data.data(), 0, sizeof(ST) * data.size());
     std::vector<char> seen((size_t)off, 0);
@@ -210,19 +264,9 @@ static int build_tiles(scd_ctx *c, int64_t B, const ST *sp, const int32_t *ind) 
     }
     int rc;
     if ((rc = dalloc(c, (ST **)&c->d_tdata, data.size(), "near-zone tiles"))) return rc;
-    if ((rc = dalloc(c, &c->d_tiles, nt, "tile table"))) return rc;
-    if ((rc = dalloc(c, &c->d_pslot_base, c->ncubes + 1, "slot bases"))) return rc;
-    if ((rc = dalloc(c, &c->d_pslot_cnt, c->ncubes, "slot counts"))) return rc;
     CK(cudaMemcpy(c->d_tdata, data.data(), sizeof(ST) * data.size(), cudaMemcpyHostToDevice), "tiles");
-    CK(cudaMemcpy(c->d_tiles, tiles.data(), sizeof(NearTile) * nt, cudaMemcpyHostToDevice), "tile table");
-    CK(cudaMemcpy(c->d_pslot_base, c->pslot_base.data(), sizeof(long long) * (c->ncubes + 1), cudaMemcpyHostToDevice), "slots");
-    CK(cudaMemcpy(c->d_pslot_cnt, c->pslot_cnt.data(), sizeof(int) * c->ncubes, cudaMemcpyHostToDevice), "slots");
-    c->ntiles = nt;
-    c->tile_blocks = off;
-    c->part_len = c->pslot_base[c->ncubes];
-    c->tiles_h.swap(tiles);
+    if ((rc = upload_layout(c, tiles, off))) return rc;
     c->B_ref = B;
-    c->nrhs_cap = 0;   // partial buffer size changed
     return SCD_OK;
 }
 
@@ -271,7 +315,7 @@ int scd_destroy(scd_ctx *c) {
     cudaSetDevice(c->dev);
     if (c->st) cudaStreamSynchronize(c->st);
     void *ptrs[] = {c->d_perm, c->d_cube_off, c->d_P, c->d_Fo, c->d_tdata, c->d_tiles, c->d_pslot_base,
-                    c->d_pslot_cnt, c->d_tc, c->d_eps, c->d_bpart, c->d_W, c->d_R, c->d_nzpart, c->d_x,
+                    c->d_pslot_cnt, c->d_tc, c->d_tvol, c->d_eps, c->d_bpart, c->d_W, c->d_R, c->d_nzpart, c->d_x,
                     c->d_y, c->d_io, c->d_V, c->d_H, c->d_cs, c->d_sn, c->d_g, c->d_rhs, c->d_w, c->d_red,
                     c->d_bar, c->d_err, c->d_state, c->d_tw[0], c->d_tw[1], c->d_tw[2]};
     for (void *p : ptrs) if (p) cudaFree(p);

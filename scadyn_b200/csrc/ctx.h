@@ -92,6 +92,7 @@ struct scd_ctx {
     std::vector<int> etopol;             // (4, T) 1-based
     std::vector<cd> param;               // (T)
     double *d_tc = nullptr;              // slot-ordered tet vertex coords (12 per slot)
+    double *d_tvol = nullptr;            // slot-ordered tet volumes
     cd *d_eps = nullptr;                 // slot-ordered eps
 
     // work buffers (sized for nrhs_cap right-hand sides)

@@ -1,0 +1,113 @@
+"""Device-side operator construction (build_grid, build_G, projectors, near
+zone, VSWF right-hand sides) against the CPU oracle, complex FP64."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from scadyn_b200 import api
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.fixture(scope="module")
+def dev_setup(small_sphere, small_op):
+    m = small_sphere
+    d = api.grid_from_mesh(m.coord, m.etopol, grid_size=1.8)
+    s = api.Solver.from_desc(d)
+    s.set_wavenumber(small_op.geom.k)
+    s.set_mesh(m.coord, m.etopol, m.param)
+    s.build_G()
+    proj = s.pfft_projection_const()
+    s.compute_near_zone_interactions_const(api.STORE_C128)
+    yield s, proj
+    s.close()
+
+
+def test_grid_from_mesh_matches_build_grid(small_sphere, small_op):
+    d = api.grid_from_mesh(small_sphere.coord, small_sphere.etopol, grid_size=1.8)
+    g = small_op.geom
+    assert (d.Nx, d.Ny, d.Nz) == (g.Nx, g.Ny, g.Nz)
+    assert d.delta == g.delta
+    assert tuple(d.min_coord) == tuple(g.min_coord)
+
+
+def test_projectors_match_oracle(dev_setup, small_op):
+    s, (S, Sx, Sy, Sz, indS) = dev_setup
+    np.testing.assert_array_equal(indS, small_op.indS)
+    for a, b in ((S, small_op.S), (Sx, small_op.Sx), (Sy, small_op.Sy), (Sz, small_op.Sz)):
+        assert rel(a, b) < 1e-9
+
+
+def test_near_zone_matches_oracle(dev_setup, small_op):
+    s, _ = dev_setup
+    sp, ind = s.get_nearzone()
+    sp64, ind64 = small_op.geom.nearzone(small_op.S, small_op.Sx, small_op.Sy, small_op.Sz, fp64=True)
+    o = np.lexsort((ind64[:, 1], ind64[:, 0]))
+    np.testing.assert_array_equal(ind, ind64[o])
+    ref = sp64[o]
+    err = np.abs(sp - ref).max() / np.abs(ref).max()
+    assert err < 1e-9, err
+
+
+def test_device_operator_matvec_matches_oracle(dev_setup, small_op, rng):
+    s, _ = dev_setup
+    x = rng.standard_normal(3 * small_op.geom.T) + 1j * rng.standard_normal(3 * small_op.geom.T)
+    small_op.merged = False
+    # the oracle operator with FP64 near zone
+    sp64, ind64 = small_op.geom.nearzone(small_op.S, small_op.Sx, small_op.Sy, small_op.Sz, fp64=True)
+    op64 = O.Operator(small_op.geom, small_op.S, small_op.Sx, small_op.Sy, small_op.Sz, small_op.indS,
+                      small_op.Fg, sp64, ind64)
+    assert rel(s.compute_Ax2(x), op64.compute_Ax2(x)) < 1e-9
+
+
+def test_vswf_rhs_matches_oracle(dev_setup, small_sphere, small_op):
+    s, _ = dev_setup
+    for Nmax in (1, 3, 6):
+        mat = s.vswf2constant(Nmax)
+        ref = O.vswf2constant(small_sphere.coord, small_sphere.etopol, small_op.geom.k, Nmax)
+        assert rel(mat, ref) < 1e-12, Nmax
+
+
+def test_green_host_and_device_agree(small_sphere):
+    """Fg passed from the host (power-of-two 2N) equals the device-built one."""
+    from scadyn_b200 import geometry
+    m = small_sphere
+    gs = geometry.cell_size_for_grid(m.coord, m.etopol, 16)
+    g = O.Geometry(m.coord, m.etopol, m.param, k=1.0 / m.a, grid_size=gs)
+    assert max(g.Nx, g.Ny, g.Nz) == 16
+    S, Sx, Sy, Sz, indS = g.projectors()
+    Fg = g.build_G()
+    sp, ind = g.nearzone(S, Sx, Sy, Sz)
+    op = O.Operator(g, S, Sx, Sy, Sz, indS, Fg, sp, ind)
+    from tests.gpu_helpers import solver_from_oracle
+    a = solver_from_oracle(op, fg_from_host=True)
+    b = solver_from_oracle(op, fg_from_host=False)
+    x = np.random.default_rng(5).standard_normal(3 * g.T) + 0j
+    ya, yb, yr = a.compute_Ax2(x), b.compute_Ax2(x), op.compute_Ax2(x)
+    assert rel(ya, yr) < 1e-11
+    assert rel(yb, yr) < 1e-11
+    a.close()
+    b.close()
+
+
+def test_full_device_T_matrix_matches_oracle(dev_setup, small_sphere, small_op):
+    """T from the device-built operator and device RHS vs the oracle's own
+    setup and solve: agreement to the GMRES tolerance."""
+    s, _ = dev_setup
+    k = small_op.geom.k
+    Taa, Tab, Tba, Tbb, iters = s.compute_T_matrix(1, k, tol=1e-10)
+    mat = O.vswf2constant(small_sphere.coord, small_sphere.etopol, k, 1)
+    sp64, ind64 = small_op.geom.nearzone(small_op.S, small_op.Sx, small_op.Sy, small_op.Sz, fp64=True)
+    op64 = O.Operator(small_op.geom, small_op.S, small_op.Sx, small_op.Sy, small_op.Sz, small_op.indS,
+                      small_op.Fg, sp64, ind64)
+    X = np.zeros_like(mat)
+    for c in range(mat.shape[0]):
+        X[c], _ = op64.gmres(mat[c], tol=1e-10)
+    T = O.T_assemble(mat, X).T * (1j * k ** 3)
+    nm = 3
+    Td = np.block([[Taa, Tab], [Tba, Tbb]])
+    assert rel(Td, T) < 1e-8
