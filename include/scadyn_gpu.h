@@ -153,15 +153,37 @@ SCD_API int scd_solve_columns(scd_ctx *ctx, int32_t ncol, const scd_c128 *mat, s
  * the mesh set by scd_set_mesh and the current wavenumber. */
 SCD_API int scd_vswf_rhs(scd_ctx *ctx, int32_t Nmax, scd_c128 *mat);
 
-/* Per-kernel timing of the last scd_matvec / solve, milliseconds (CUDA events). */
+/* compute_T_matrix (src/T_matrix.f90:240-277) with device-resident data:
+ * the incident VSWF columns are built on the device (vswf2constant, kept for
+ * the current Nmax and wavenumber), columns col0 .. col0+ncol-1 are solved,
+ * and T(:, col0+j) = i k^3 mat^H x_j is returned in T (2nm, ncol).  With
+ * col0 = 0 and ncol = 2nm, T holds [Taa Tab; Tba Tbb] (src/T_matrix.f90:271-275).
+ * Needs scd_set_mesh (for the VSWF points) and the operator. */
+SCD_API int scd_compute_T_matrix(scd_ctx *ctx, int32_t Nmax, const scd_solve_opts *opts, int32_t col0,
+                                 int32_t ncol, scd_c128 *T, int32_t *iters);
+
+/* Device timing, milliseconds, from CUDA events on the context's stream. */
 typedef struct scd_timing {
-    double matvec_ms;      /* average matvec */
+    double matvec_ms;      /* average matvec (scd_profile_matvec) */
     double nearzone_ms;    /* average near-zone kernel */
-    double fft_ms;         /* average FFT convolution chain */
+    double fft_ms;         /* average scatter + FFT convolution chain */
+    double gather_ms;      /* average interpolation / assembly kernel */
     double arnoldi_ms;     /* average orthogonalisation step */
-    int64_t launches;      /* kernels launched by the last call */
+    double last_call_ms;   /* last scd_solve_columns / scd_compute_T_matrix / scd_gmres */
+    double accum_ms;       /* sum of last_call_ms since the last reset */
+    int64_t launches;      /* kernels launched since the last reset */
+    int64_t matvecs;       /* operator applications since the last reset */
+    int64_t arnoldi_steps; /* Arnoldi steps since the last reset */
 } scd_timing;
-SCD_API int scd_get_timing(scd_ctx *ctx, scd_timing *t);
+SCD_API int scd_get_timing(scd_ctx *ctx, scd_timing *t, int32_t reset);
+
+/* Run `reps` device-resident matvecs on a fixed vector and record per-kernel
+ * averages in the timing block (matvec_ms, nearzone_ms, fft_ms, gather_ms). */
+SCD_API int scd_profile_matvec(scd_ctx *ctx, int32_t reps);
+
+/* Near-zone blocks in the reference layout (tet_B >= tet_T) and the bytes of
+ * the device tile storage. */
+SCD_API int64_t scd_nearzone_bytes(scd_ctx *ctx);
 
 #ifdef __cplusplus
 }

@@ -676,49 +676,79 @@ int orc_fft1d(int L, zc *x, int sign) {
     return 0;
 }
 
-typedef struct { int L; zc *w, *o, *t, *line; } fft_plan;
+/* Line transforms: iterative radix-2 for power-of-two lengths (bit-reversal
+ * then butterflies with a precomputed root table), the recursive mixed-radix
+ * routine otherwise.  3D passes run their line loops with OpenMP, like the
+ * reference's `!$OMP` regions in FFT3d_2/IFFT3d_2. */
+typedef struct { int L, pow2; zc *w, *o, *t, *line; int *rev; } fft_plan;
 static void plan_init(fft_plan *p, int L, int sign) {
     p->L = L;
+    p->pow2 = (L & (L - 1)) == 0;
     p->w = (zc *)malloc(sizeof(zc)*(size_t)L); p->o = (zc *)malloc(sizeof(zc)*(size_t)L);
     p->t = (zc *)malloc(sizeof(zc)*(size_t)L); p->line = (zc *)malloc(sizeof(zc)*(size_t)L);
+    p->rev = (int *)malloc(sizeof(int)*(size_t)L);
     for (int j = 0; j < L; ++j) { double a = 2.0*PI*(double)j/(double)L; p->w[j] = CMPLX(cos(a), sign*sin(a)); }
+    if (p->pow2) {
+        int lg = 0; while ((1 << lg) < L) ++lg;
+        for (int i = 0; i < L; ++i) { int r = 0; for (int b = 0; b < lg; ++b) if (i & (1 << b)) r |= 1 << (lg - 1 - b); p->rev[i] = r; }
+    }
 }
-static void plan_free(fft_plan *p) { free(p->w); free(p->o); free(p->t); free(p->line); }
+static void plan_free(fft_plan *p) { free(p->w); free(p->o); free(p->t); free(p->line); free(p->rev); }
+static void fft_pow2(fft_plan *p, zc *x) {
+    const int L = p->L;
+    for (int i = 0; i < L; ++i) p->o[p->rev[i]] = x[i];
+    for (int len = 2; len <= L; len <<= 1) {
+        const int half = len >> 1, step = L/len;
+        for (int b = 0; b < L; b += len)
+            for (int j = 0; j < half; ++j) {
+                zc u = p->o[b + j], v = p->o[b + j + half]*p->w[j*step];
+                p->o[b + j] = u + v;
+                p->o[b + j + half] = u - v;
+            }
+    }
+    memcpy(x, p->o, sizeof(zc)*(size_t)L);
+}
 /* transform the line A[base + i*stride], i < L, in place */
 static void plan_line(fft_plan *p, zc *A, size_t base, size_t stride) {
     for (int i = 0; i < p->L; ++i) p->line[i] = A[base + i*stride];
-    fft_rec(p->line, 1, p->o, p->L, p->w, 1, p->L, p->t);
-    for (int i = 0; i < p->L; ++i) A[base + i*stride] = p->o[i];
+    if (p->pow2) fft_pow2(p, p->line);
+    else { fft_rec(p->line, 1, p->o, p->L, p->w, 1, p->L, p->t); memcpy(p->line, p->o, sizeof(zc)*(size_t)p->L); }
+    for (int i = 0; i < p->L; ++i) A[base + i*stride] = p->line[i];
+}
+
+/* pass over lines (i1 < n1, i2 < n2) with base = i1*s1 + i2*s2 */
+static void pass_lines(int L, int sign, zc *A, int n1, size_t s1, int n2, size_t s2, size_t stride) {
+#pragma omp parallel
+    {
+        fft_plan p; plan_init(&p, L, sign);
+#pragma omp for collapse(2) schedule(static)
+        for (int i1 = 0; i1 < n1; ++i1) for (int i2 = 0; i2 < n2; ++i2) plan_line(&p, A, i1*s1 + i2*s2, stride);
+        plan_free(&p);
+    }
 }
 
 /* FFT3d / IFFT3d: full unnormalised 3D transform (src/possu.f90:124-136,209-221) */
 int orc_fft3d(int Px, int Py, int Pz, zc *A, int sign) {
-    fft_plan px, py, pz;
-    plan_init(&px, Px, sign); plan_init(&py, Py, sign); plan_init(&pz, Pz, sign);
-    size_t sx = 1, sy = (size_t)Px, sz = (size_t)Px*Py;
-    for (int z = 0; z < Pz; ++z) for (int y = 0; y < Py; ++y) plan_line(&px, A, y*sy + z*sz, sx);
-    for (int z = 0; z < Pz; ++z) for (int x = 0; x < Px; ++x) plan_line(&py, A, x*sx + z*sz, sy);
-    for (int y = 0; y < Py; ++y) for (int x = 0; x < Px; ++x) plan_line(&pz, A, x*sx + y*sy, sz);
-    plan_free(&px); plan_free(&py); plan_free(&pz);
+    size_t sy = (size_t)Px, sz = (size_t)Px*Py;
+    pass_lines(Px, sign, A, Pz, sz, Py, sy, 1);
+    pass_lines(Py, sign, A, Pz, sz, Px, 1, sy);
+    pass_lines(Pz, sign, A, Py, sy, Px, 1, sz);
     return 0;
 }
 
 /* FFT3d_2 / IFFT3d_2: the zero-padding-pruned passes (src/possu.f90:140-204,225-289) */
 int orc_fft3d_pruned(int Px, int Py, int Pz, zc *A, int inverse) {
     int sign = inverse ? 1 : -1;
-    fft_plan px, py, pz;
-    plan_init(&px, Px, sign); plan_init(&py, Py, sign); plan_init(&pz, Pz, sign);
     size_t sy = (size_t)Px, sz = (size_t)Px*Py;
     if (!inverse) {
-        for (int i1 = 0; i1 < Pz/2; ++i1) for (int i2 = 0; i2 < Py/2; ++i2) plan_line(&px, A, i2*sy + i1*sz, 1);
-        for (int i1 = 0; i1 < Pz/2; ++i1) for (int i2 = 0; i2 < Px; ++i2) plan_line(&py, A, i2 + i1*sz, sy);
-        for (int i1 = 0; i1 < Py; ++i1) for (int i2 = 0; i2 < Px; ++i2) plan_line(&pz, A, i2 + i1*sy, sz);
+        pass_lines(Px, sign, A, Pz/2, sz, Py/2, sy, 1);
+        pass_lines(Py, sign, A, Pz/2, sz, Px, 1, sy);
+        pass_lines(Pz, sign, A, Py, sy, Px, 1, sz);
     } else {
-        for (int i1 = 0; i1 < Py; ++i1) for (int i2 = 0; i2 < Px; ++i2) plan_line(&pz, A, i2 + i1*sy, sz);
-        for (int i1 = 0; i1 < Pz/2; ++i1) for (int i2 = 0; i2 < Px; ++i2) plan_line(&py, A, i2 + i1*sz, sy);
-        for (int i1 = 0; i1 < Pz/2; ++i1) for (int i2 = 0; i2 < Py/2; ++i2) plan_line(&px, A, i2*sy + i1*sz, 1);
+        pass_lines(Pz, sign, A, Py, sy, Px, 1, sz);
+        pass_lines(Py, sign, A, Pz/2, sz, Px, 1, sy);
+        pass_lines(Px, sign, A, Pz/2, sz, Py/2, sy, 1);
     }
-    plan_free(&px); plan_free(&py); plan_free(&pz);
     return 0;
 }
 
@@ -846,6 +876,7 @@ static void convolve(const orc_op *op, zc *grid_src /* N^3 */, zc *SS, zc *out /
     for (int m = 0; m < Nz; ++m) for (int l = 0; l < Ny; ++l) for (int k = 0; k < Nx; ++k)
         SS[k + (size_t)Px*(l + (size_t)Py*m)] = grid_src[k + (size_t)Nx*(l + (size_t)Ny*m)];
     orc_fft3d_pruned(Px, Py, Pz, SS, 0);
+#pragma omp parallel for schedule(static)
     for (size_t i = 0; i < tot; ++i) SS[i] = op->Fg[i]*SS[i];
     orc_fft3d_pruned(Px, Py, Pz, SS, 1);
     /* arr2vec, src/common.f90:417-438 */

@@ -36,7 +36,7 @@ EXPORTS = [
     "scd_set_projectors", "scd_set_nearzone", "scd_grid_from_mesh", "scd_set_mesh",
     "scd_build_projectors", "scd_build_nearzone", "scd_get_projectors", "scd_nearzone_count",
     "scd_get_nearzone", "scd_matvec", "scd_gmres", "scd_solve_columns", "scd_vswf_rhs",
-    "scd_get_timing",
+    "scd_get_timing", "scd_compute_T_matrix", "scd_profile_matvec", "scd_nearzone_bytes",
 ]
 
 
@@ -59,7 +59,9 @@ class SolveOpts(C.Structure):
 
 class Timing(C.Structure):
     _fields_ = [("matvec_ms", C.c_double), ("nearzone_ms", C.c_double), ("fft_ms", C.c_double),
-                ("arnoldi_ms", C.c_double), ("launches", C.c_int64)]
+                ("gather_ms", C.c_double), ("arnoldi_ms", C.c_double), ("last_call_ms", C.c_double),
+                ("accum_ms", C.c_double), ("launches", C.c_int64), ("matvecs", C.c_int64),
+                ("arnoldi_steps", C.c_int64)]
 
 
 _lib = None
@@ -93,7 +95,10 @@ def load_library(path: str = LIB_PATH):
         "scd_gmres": ([vp, vp, vp, dbl, i32, i32, C.POINTER(i32), C.POINTER(dbl)], C.c_int),
         "scd_solve_columns": ([vp, i32, vp, vp, C.POINTER(SolveOpts), vp, vp], C.c_int),
         "scd_vswf_rhs": ([vp, i32, vp], C.c_int),
-        "scd_get_timing": ([vp, C.POINTER(Timing)], C.c_int),
+        "scd_get_timing": ([vp, C.POINTER(Timing), i32], C.c_int),
+        "scd_compute_T_matrix": ([vp, i32, C.POINTER(SolveOpts), i32, i32, vp, vp], C.c_int),
+        "scd_profile_matvec": ([vp, i32], C.c_int),
+        "scd_nearzone_bytes": ([vp], C.c_int64),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -270,17 +275,32 @@ class Solver:
                        "solve_columns", ok=(SCD_OK, SCD_NOT_CONVERGED))
         return Tc, iters, X, rc
 
-    def compute_T_matrix(self, Nmax, k, mat=None, **kw):
-        """compute_T_matrix (src/T_matrix.f90:240-277): returns Taa, Tab, Tba, Tbb."""
-        if mat is None:
-            mat = self.vswf2constant(Nmax)
-        Tc, iters, _, _ = self.solve_columns(mat, **kw)
-        T = Tc.T * (1j * k ** 3)
+    def compute_T_matrix(self, Nmax, col0=0, ncol=None, tol=1e-5, m=50, cycles=4, block=1,
+                         precision=PREC_FP64, inner_tol=1e-3, max_outer=10):
+        """compute_T_matrix (src/T_matrix.f90:240-277) on device-resident data:
+        returns (T (2nm, ncol) with T[:, j] the scaled T column col0+j, iters).
+        With all columns, T = [[Taa, Tab], [Tba, Tbb]]."""
         nm = (Nmax + 1) ** 2 - 1
-        return T[:nm, :nm], T[:nm, nm:], T[nm:, :nm], T[nm:, nm:], iters
+        if ncol is None:
+            ncol = 2 * nm - col0
+        Tf = np.zeros((ncol, 2 * nm), np.complex128)       # memory of Fortran T(2nm, ncol)
+        iters = np.zeros(ncol, np.int32)
+        o = SolveOpts(tol, m, cycles, block, precision, inner_tol, max_outer)
+        self._chk(self.lib.scd_compute_T_matrix(self.ctx, Nmax, C.byref(o), col0, ncol, _p(Tf), _p(iters)),
+                  "compute_T_matrix", ok=(SCD_OK, SCD_NOT_CONVERGED))
+        return Tf.T, iters
 
-    def timing(self):
+    def profile_matvec(self, reps=10):
+        self._chk(self.lib.scd_profile_matvec(self.ctx, reps), "profile_matvec")
+        return self.timing()
+
+    def nearzone_bytes(self):
+        return int(self.lib.scd_nearzone_bytes(self.ctx))
+
+    def nearzone_count(self):
+        return int(self.lib.scd_nearzone_count(self.ctx))
+
+    def timing(self, reset=False):
         t = Timing()
-        self.lib.scd_get_timing(self.ctx, C.byref(t))
-        return {"matvec_ms": t.matvec_ms, "nearzone_ms": t.nearzone_ms, "fft_ms": t.fft_ms,
-                "arnoldi_ms": t.arnoldi_ms, "launches": t.launches}
+        self.lib.scd_get_timing(self.ctx, C.byref(t), int(reset))
+        return {f: getattr(t, f) for f, _ in Timing._fields_}

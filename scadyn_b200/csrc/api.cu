@@ -418,17 +418,11 @@ int scd_matvec(scd_ctx *c, const scd_c128 *x, scd_c128 *Ax) {
     const size_t bytes = sizeof(cd) * c->n;
     CK(cudaMemcpyAsync(c->d_io, x, bytes, cudaMemcpyHostToDevice, c->st), "x");
     launch_permute_in(c, c->d_io, c->d_x, 1, c->n);
-    c->timing = true;
     run_matvec(c, c->d_x, c->d_y, 1, nullptr);
-    c->timing = false;
     launch_permute_out(c, c->d_y, c->d_io, 1, c->n);
     CK(cudaMemcpyAsync(Ax, c->d_io, bytes, cudaMemcpyDeviceToHost, c->st), "Ax");
     CK(cudaStreamSynchronize(c->st), "matvec");
-    float a = 0, b = 0, t = 0;
-    cudaEventElapsedTime(&a, c->ev[0], c->ev[1]);
-    cudaEventElapsedTime(&b, c->ev[1], c->ev[2]);
-    cudaEventElapsedTime(&t, c->ev[0], c->ev[3]);
-    c->t_near = a; c->t_fft = b; c->t_matvec = t;
+    c->n_matvec += 1;
     return check_cuda(c, cudaGetLastError(), "matvec");
 }
 
@@ -443,11 +437,19 @@ int scd_gmres(scd_ctx *c, const scd_c128 *rhs, scd_c128 *x, double tol, int32_t 
     launch_permute_in(c, c->d_io, c->d_rhs, 1, c->n);
     int it = 0;
     double rr = 0;
+    cudaEventRecord(c->ev[4], c->st);
     rc = gmres_solve(c, c->d_rhs, c->d_x, tol, m, cycles, &it, &rr);
     if (rc != SCD_OK && rc != SCD_NOT_CONVERGED) return rc;
+    cudaEventRecord(c->ev[5], c->st);
     launch_permute_out(c, c->d_x, c->d_io, 1, c->n);
     CK(cudaMemcpyAsync(x, c->d_io, bytes, cudaMemcpyDeviceToHost, c->st), "x");
     CK(cudaStreamSynchronize(c->st), "gmres");
+    {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]);
+        c->last_call_ms = ms;
+        c->accum_ms += ms;
+    }
     if (iters) *iters = it;
     if (relres) *relres = rr;
     return rc;
@@ -465,6 +467,7 @@ int scd_solve_columns(scd_ctx *c, int32_t ncol, const scd_c128 *mat, scd_c128 *T
     if ((rc = dalloc(c, &d_X, (size_t)n * ncol, "X"))) { cudaFree(d_mat); return rc; }
     if ((rc = dalloc(c, &d_T, (size_t)ncol * ncol, "T"))) { cudaFree(d_mat); cudaFree(d_X); return rc; }
     int worst = SCD_OK;
+    cudaEventRecord(c->ev[4], c->st);
     for (int col = 0; col < ncol && worst != SCD_NAN && worst != SCD_TIMEOUT; ++col) {
         CK(cudaMemcpyAsync(c->d_io, mat + (size_t)n * col, sizeof(cd) * n, cudaMemcpyHostToDevice, c->st), "mat");
         launch_permute_in(c, c->d_io, d_mat + (size_t)n * col, 1, n);
@@ -484,22 +487,131 @@ int scd_solve_columns(scd_ctx *c, int32_t ncol, const scd_c128 *mat, scd_c128 *T
                 rc = check_cuda(c, cudaMemcpyAsync(X + (size_t)n * col, c->d_io, sizeof(cd) * n, cudaMemcpyDeviceToHost, c->st), "X");
             }
         }
+        cudaEventRecord(c->ev[5], c->st);
         if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->st), "solve");
         if (rc) worst = rc;
+        else {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]);
+            c->last_call_ms = ms;
+            c->accum_ms += ms;
+        }
     }
     cudaStreamSynchronize(c->st);
     cudaFree(d_mat); cudaFree(d_X); cudaFree(d_T);
     return worst;
 }
 
-int scd_get_timing(scd_ctx *c, scd_timing *t) {
+int scd_get_timing(scd_ctx *c, scd_timing *t, int32_t reset) {
     if (!c || !t) return SCD_BAD_ARG;
     t->matvec_ms = c->t_matvec;
     t->nearzone_ms = c->t_near;
     t->fft_ms = c->t_fft;
+    t->gather_ms = c->t_gather;
     t->arnoldi_ms = c->t_arn;
+    t->last_call_ms = c->last_call_ms;
+    t->accum_ms = c->accum_ms;
     t->launches = c->launches;
+    t->matvecs = c->n_matvec;
+    t->arnoldi_steps = c->n_arn;
+    if (reset) {
+        c->accum_ms = 0;
+        c->launches = 0;
+        c->n_matvec = 0;
+        c->n_arn = 0;
+    }
     return SCD_OK;
+}
+
+int scd_profile_matvec(scd_ctx *c, int32_t reps) {
+    if (!c || reps < 1) return SCD_BAD_ARG;
+    cudaSetDevice(c->dev);
+    int rc = ready(c);
+    if (rc) return rc;
+    // a fixed non-trivial vector: the first VSWF-like pattern is not needed,
+    // any dense vector exercises the same memory traffic
+    std::vector<cd> h((size_t)c->n);
+    for (long long i = 0; i < c->n; ++i) h[i] = cmk(std::sin(0.37 * (double)i), std::cos(0.11 * (double)i));
+    CK(cudaMemcpy(c->d_x, h.data(), sizeof(cd) * c->n, cudaMemcpyHostToDevice), "profile x");
+    double sn = 0, sf = 0, sg = 0, st = 0;
+    c->timing = true;
+    for (int r = 0; r < reps + 1; ++r) {
+        run_matvec(c, c->d_x, c->d_y, 1, nullptr);
+        CK(cudaStreamSynchronize(c->st), "profile");
+        float a = 0, b = 0, g = 0, t = 0;
+        cudaEventElapsedTime(&a, c->ev[0], c->ev[1]);
+        cudaEventElapsedTime(&b, c->ev[1], c->ev[2]);
+        cudaEventElapsedTime(&g, c->ev[2], c->ev[3]);
+        cudaEventElapsedTime(&t, c->ev[0], c->ev[3]);
+        if (r == 0) continue;   // warm-up
+        sn += a; sf += b; sg += g; st += t;
+    }
+    c->timing = false;
+    c->t_near = sn / reps;
+    c->t_fft = sf / reps;
+    c->t_gather = sg / reps;
+    c->t_matvec = st / reps;
+    return check_cuda(c, cudaGetLastError(), "profile");
+}
+
+int64_t scd_nearzone_bytes(scd_ctx *c) {
+    if (!c || !c->have_near) return -1;
+    return (int64_t)c->tile_blocks * 9 * (c->near_prec == SCD_STORE_C64 ? 8 : 16);
+}
+
+int scd_compute_T_matrix(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int32_t col0, int32_t ncol,
+                         scd_c128 *T, int32_t *iters) {
+    if (!c || !o || !T || Nmax < 1) return SCD_BAD_ARG;
+    cudaSetDevice(c->dev);
+    int rc = ready(c);
+    if (rc) return rc;
+    const int nm = (Nmax + 1) * (Nmax + 1) - 1, ntot = 2 * nm;
+    if (col0 < 0 || ncol < 1 || col0 + ncol > ntot)
+        return set_error(c, SCD_BAD_ARG, "columns %d..%d outside 1..%d", col0 + 1, col0 + ncol, ntot);
+    const long long n = c->n;
+    if (!c->d_mat || c->mat_Nmax != Nmax || c->mat_k != c->k) {
+        cudaFree(c->d_mat);
+        c->d_mat = nullptr;
+        if ((rc = dalloc(c, &c->d_mat, (size_t)n * ntot, "resident VSWF columns"))) return rc;
+        if ((rc = setup_vswf(c, Nmax, c->d_mat))) return rc;
+        c->mat_Nmax = Nmax;
+        c->mat_k = c->k;
+    }
+    cd *d_X = nullptr, *d_T = nullptr;
+    if ((rc = dalloc(c, &d_X, (size_t)n * ncol, "X"))) return rc;
+    if ((rc = dalloc(c, &d_T, (size_t)ntot * ncol, "T"))) { cudaFree(d_X); return rc; }
+    cudaEventRecord(c->ev[4], c->st);
+    int worst = SCD_OK;
+    for (int j = 0; j < ncol; ++j) {
+        int it = 0;
+        double rr = 0;
+        rc = gmres_solve(c, c->d_mat + (size_t)n * (col0 + j), d_X + (size_t)n * j, o->tol, o->m, o->cycles, &it, &rr);
+        if (iters) iters[j] = it;
+        if (rc != SCD_OK && rc != SCD_NOT_CONVERGED) { worst = rc; break; }
+        if (rc == SCD_NOT_CONVERGED) worst = rc;
+    }
+    if (worst == SCD_OK || worst == SCD_NOT_CONVERGED) {
+        launch_T_assemble(c, c->d_mat, ntot, 0, ncol, d_X, d_T);
+        cudaEventRecord(c->ev[5], c->st);
+        std::vector<cd> h((size_t)ntot * ncol);
+        rc = check_cuda(c, cudaMemcpyAsync(h.data(), d_T, sizeof(cd) * h.size(), cudaMemcpyDeviceToHost, c->st), "T");
+        if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->st), "compute_T_matrix");
+        if (!rc) {
+            // T_mat * i k^3 (src/T_matrix.f90:270-275)
+            const double k3 = std::pow(c->k, 3.0);
+            for (size_t i = 0; i < h.size(); ++i) T[i] = scd_c128{-k3 * h[i].y, k3 * h[i].x};
+            float ms = 0;
+            cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]);
+            c->last_call_ms = ms;
+            c->accum_ms += ms;
+        } else {
+            worst = rc;
+        }
+    }
+    cudaStreamSynchronize(c->st);
+    cudaFree(d_X);
+    cudaFree(d_T);
+    return worst;
 }
 
 }  // extern "C"

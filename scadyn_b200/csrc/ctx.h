@@ -118,9 +118,15 @@ struct scd_ctx {
 
     // timing
     cudaEvent_t ev[8] = {};
-    double t_matvec = 0, t_near = 0, t_fft = 0, t_arn = 0;
+    double t_matvec = 0, t_near = 0, t_fft = 0, t_gather = 0, t_arn = 0;
+    double last_call_ms = 0, accum_ms = 0;
     long long n_matvec = 0, n_arn = 0, launches = 0;
     bool timing = false;
+
+    // resident right-hand sides (vswf2constant for mat_Nmax, mat_k)
+    cd *d_mat = nullptr;
+    int mat_Nmax = 0;
+    double mat_k = 0.0;
 
     std::string err;
 };

@@ -329,7 +329,9 @@ int gmres_solve(scd_ctx *c, const cd *d_rhs, cd *d_x, double tol, int m, int cyc
     cudaMemcpyAsync(d_x, d_rhs, sizeof(cd) * c->n, cudaMemcpyDeviceToDevice, c->st);   // x0 = rhs
     const int check_every = 4;
     bool done = false;
+    int cycles_run = 0;
     for (int cyc = 0; cyc < cycles && !done; ++cyc) {
+        ++cycles_run;
         run_matvec(c, d_x, c->d_w, 1, nullptr);
         int first = cyc == 0;
         void *args_init[] = {&a, &first};
@@ -353,6 +355,8 @@ int gmres_solve(scd_ctx *c, const cd *d_rhs, cd *d_x, double tol, int m, int cyc
     }
     if (iters) *iters = c->h_state->iters;
     if (relres) *relres = c->h_state->error;
+    c->n_arn += c->h_state->iters;
+    c->n_matvec += c->h_state->iters + cycles_run;
     if (c->h_state->status == SCD_TIMEOUT) return set_error(c, SCD_TIMEOUT, "grid barrier wait expired in GMRES");
     if (c->h_state->status == SCD_NAN) return set_error(c, SCD_NAN, "non-finite residual in GMRES");
     if (!(c->h_state->error < tol)) return SCD_NOT_CONVERGED;

@@ -99,7 +99,7 @@ def test_full_device_T_matrix_matches_oracle(dev_setup, small_sphere, small_op):
     setup and solve: agreement to the GMRES tolerance."""
     s, _ = dev_setup
     k = small_op.geom.k
-    Taa, Tab, Tba, Tbb, iters = s.compute_T_matrix(1, k, tol=1e-10)
+    Td, iters = s.compute_T_matrix(1, tol=1e-10)
     mat = O.vswf2constant(small_sphere.coord, small_sphere.etopol, k, 1)
     sp64, ind64 = small_op.geom.nearzone(small_op.S, small_op.Sx, small_op.Sy, small_op.Sz, fp64=True)
     op64 = O.Operator(small_op.geom, small_op.S, small_op.Sx, small_op.Sy, small_op.Sz, small_op.indS,
@@ -108,6 +108,7 @@ def test_full_device_T_matrix_matches_oracle(dev_setup, small_sphere, small_op):
     for c in range(mat.shape[0]):
         X[c], _ = op64.gmres(mat[c], tol=1e-10)
     T = O.T_assemble(mat, X).T * (1j * k ** 3)
-    nm = 3
-    Td = np.block([[Taa, Tab], [Tba, Tbb]])
     assert rel(Td, T) < 1e-8
+    # a column range returns the same columns
+    Tpart, _ = s.compute_T_matrix(1, col0=2, ncol=3, tol=1e-10)
+    assert rel(Tpart, Td[:, 2:5]) < 1e-12
