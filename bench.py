@@ -40,7 +40,7 @@ CONFIGS = {
     "c2": dict(workload="C2: ellipsoid 1:0.8:0.6, ka=8 (~150k tets), per-tet eps Re U(2,3) Im U(0.01,0.1), "
                         "Nmax=14 (448 columns), padded pFFT grid 128^3, GMRES(50) tol 1e-6",
                body="ellipsoid", n_major=23.2, axes=(1.0, 0.8, 0.6), ka=8.0, eps=None,
-               Nmax=14, N=64, tol=1e-6, m=50, cycles=4, seed=1002, eps_seed=2002),
+               Nmax=14, N=64, tol=1e-6, m=50, cycles=12, seed=1002, eps_seed=2002),
 }
 
 L2_BYTES = 126 * 1024 * 1024
@@ -210,7 +210,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
-    ap.add_argument("--block", type=int, default=8, help="columns per step")
+    ap.add_argument("--block", type=int, default=32, help="columns per step")
+    ap.add_argument("--slots", type=int, default=16, help="columns solved concurrently (batched GMRES slots)")
+    ap.add_argument("--plain-sample", type=int, default=2, help="columns timed in the plain one-at-a-time form")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
@@ -272,8 +274,9 @@ def main():
 
     # ---------------------------------------------------------------- ours
     opts = dict(tol=cfg["tol"], m=cfg["m"], cycles=cfg["cycles"])
+    S = min(args.slots, B)
     for st in range(args.warmup):
-        solver.compute_T_matrix(Nmax, col0=cols_for(st), ncol=B, **opts)
+        solver.compute_T_matrix(Nmax, col0=cols_for(st), ncol=B, block=S, **opts)
 
     def barrier():
         if dist:
@@ -288,11 +291,10 @@ def main():
     with Clocks(local) as clk:
         for st in range(args.warmup, args.warmup + args.steps):
             c0 = cols_for(st)
-            for j in range(B):
-                _, it = solver.compute_T_matrix(Nmax, col0=c0 + j, ncol=1, **opts)
-                lat.append(solver.timing()["last_call_ms"])
-                iters.append(int(it[0]))
-                cycles.append(max(1, -(-int(it[0]) // cfg["m"])))
+            _, it = solver.compute_T_matrix(Nmax, col0=c0, ncol=B, block=S, **opts)
+            lat += list(solver.column_latency(B))
+            iters += [int(v) for v in it]
+            cycles += [max(1, -(-int(v) // cfg["m"])) for v in it]
     barrier()
     wall = time.time() - t_wall
     tm = solver.timing(reset=True)
@@ -306,6 +308,17 @@ def main():
         dev_ms = float(tt.item())
     value = world * cols / (dev_ms / 1e3)
 
+    # the plain form: one column at a time (no batching), same columns
+    forms = {}
+    if args.plain_sample > 0:
+        solver.timing(reset=True)
+        c0 = cols_for(args.warmup)
+        for j in range(args.plain_sample):
+            solver.compute_T_matrix(Nmax, col0=c0 + j, ncol=1, block=1, **opts)
+        pm = solver.timing(reset=True)["accum_ms"]
+        forms["plain_fp64_one_column"] = round(args.plain_sample / (pm / 1e3), 4)
+    forms["batched_fp64_%d_slots" % S] = round(value / world, 4)
+
     # e2e: the same columns through scd_solve_columns with host buffers
     mat_all = solver.vswf2constant(Nmax)
     e2e_ms = 0.0
@@ -315,7 +328,7 @@ def main():
         blk = np.ascontiguousarray(mat_all[c0:c0 + B])
         solver.timing(reset=True)
         t = time.time()
-        Tc, its, _, _ = solver.solve_columns(blk, **opts)
+        Tc, its, _, _ = solver.solve_columns(blk, block=S, **opts)
         e2e_ms += (time.time() - t) * 1e3
         h2d = blk.nbytes
         d2h = Tc.nbytes + its.nbytes
@@ -326,8 +339,13 @@ def main():
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_val = world * cols / (float(tt.item()) / 1e3)
 
-    # roofline of the dominant kernel (near-zone tiles) from live CUDA events
-    prof = solver.profile_matvec(20)
+    # per-kernel times of the batched matvec (the timed region's shape)
+    profb = solver.profile_matvec(5, S)
+    batched = {"nrhs": S, "matvec_ms": profb["matvec_ms"], "nearzone_ms": profb["nearzone_ms"],
+               "fft_chain_ms": profb["fft_ms"], "gather_ms": profb["gather_ms"]}
+    # roofline of the dominant kernel of the memory-bound single-column form
+    # (near-zone tiles) from live CUDA events
+    prof = solver.profile_matvec(20, 1)
     Bref = solver.nearzone_count()
     alg_bytes = Bref * (9 * 8 + 8)                 # complex64 blocks + index pair, per matvec
     near_ms = prof["nearzone_ms"]
@@ -350,19 +368,22 @@ def main():
     if rank == 0:
         lat_s = sorted(lat)
         line = {
-            "metric": "T-matrix columns/s (plain FP64 GMRES(50), tol 1e-6)",
+            "metric": "T-matrix columns/s (FP64 GMRES(50), tol 1e-6, batched columns)",
             "value": round(value, 4), "unit": "columns/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(dev_ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded jittered cube-lattice mesh)",
             "config": {"workload": cfg["workload"], "tets": mesh.n_tet,
                        "grid_nodes": [desc.Nx, desc.Ny, desc.Nz], "near_blocks": Bref,
-                       "near_bytes": solver.nearzone_bytes(), "columns_per_step": B, "precision": "plain FP64",
+                       "near_bytes": solver.nearzone_bytes(), "columns_per_step": B, "slots": S,
+                       "precision": "complex FP64 (near zone stored complex64 as the reference)",
                        "l2": "inputs larger than L2 (near-zone tiles %.2f GB per matvec)" % (solver.nearzone_bytes() / 1e9),
                        "parallelism": f"replicas x{world}"},
             "p50_ms": round(float(np.percentile(lat_s, 50)), 3),
             "p99_ms": round(float(np.percentile(lat_s, 99)), 3),
             "iters_mean": float(np.mean(iters)),
+            "forms": forms,
+            "batched_matvec": batched,
             "e2e": {"value": round(e2e_val, 4), "unit": "columns/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "roofline": roof,

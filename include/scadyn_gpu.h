@@ -177,9 +177,15 @@ typedef struct scd_timing {
 } scd_timing;
 SCD_API int scd_get_timing(scd_ctx *ctx, scd_timing *t, int32_t reset);
 
-/* Run `reps` device-resident matvecs on a fixed vector and record per-kernel
- * averages in the timing block (matvec_ms, nearzone_ms, fft_ms, gather_ms). */
-SCD_API int scd_profile_matvec(scd_ctx *ctx, int32_t reps);
+/* Run `reps` device-resident matvecs on `nrhs` fixed vectors at once and
+ * record per-kernel averages per call in the timing block (matvec_ms,
+ * nearzone_ms, fft_ms, gather_ms). */
+SCD_API int scd_profile_matvec(scd_ctx *ctx, int32_t reps, int32_t nrhs);
+
+/* Per-column solve latency (admission to completion, milliseconds on the
+ * host clock, each tick ending in a stream synchronisation) of the last
+ * scd_solve_columns / scd_compute_T_matrix call; ncol must match it. */
+SCD_API int scd_column_latency(scd_ctx *ctx, int32_t ncol, double *ms);
 
 /* Near-zone blocks in the reference layout (tet_B >= tet_T) and the bytes of
  * the device tile storage. */

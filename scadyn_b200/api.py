@@ -37,6 +37,7 @@ EXPORTS = [
     "scd_build_projectors", "scd_build_nearzone", "scd_get_projectors", "scd_nearzone_count",
     "scd_get_nearzone", "scd_matvec", "scd_gmres", "scd_solve_columns", "scd_vswf_rhs",
     "scd_get_timing", "scd_compute_T_matrix", "scd_profile_matvec", "scd_nearzone_bytes",
+    "scd_column_latency",
 ]
 
 
@@ -97,8 +98,9 @@ def load_library(path: str = LIB_PATH):
         "scd_vswf_rhs": ([vp, i32, vp], C.c_int),
         "scd_get_timing": ([vp, C.POINTER(Timing), i32], C.c_int),
         "scd_compute_T_matrix": ([vp, i32, C.POINTER(SolveOpts), i32, i32, vp, vp], C.c_int),
-        "scd_profile_matvec": ([vp, i32], C.c_int),
+        "scd_profile_matvec": ([vp, i32, i32], C.c_int),
         "scd_nearzone_bytes": ([vp], C.c_int64),
+        "scd_column_latency": ([vp, i32, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -290,9 +292,14 @@ class Solver:
                   "compute_T_matrix", ok=(SCD_OK, SCD_NOT_CONVERGED))
         return Tf.T, iters
 
-    def profile_matvec(self, reps=10):
-        self._chk(self.lib.scd_profile_matvec(self.ctx, reps), "profile_matvec")
+    def profile_matvec(self, reps=10, nrhs=1):
+        self._chk(self.lib.scd_profile_matvec(self.ctx, reps, nrhs), "profile_matvec")
         return self.timing()
+
+    def column_latency(self, ncol):
+        ms = np.zeros(ncol, np.float64)
+        self._chk(self.lib.scd_column_latency(self.ctx, ncol, _p(ms)), "column_latency")
+        return ms
 
     def nearzone_bytes(self):
         return int(self.lib.scd_nearzone_bytes(self.ctx))

@@ -320,6 +320,8 @@ int scd_destroy(scd_ctx *c) {
                     c->d_bar, c->d_err, c->d_state, c->d_tw[0], c->d_tw[1], c->d_tw[2]};
     for (void *p : ptrs) if (p) cudaFree(p);
     if (c->h_state) cudaFreeHost(c->h_state);
+    batch_free(c);
+    if (c->d_mat) cudaFree(c->d_mat);
     for (int i = 0; i < 8; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
@@ -378,8 +380,7 @@ int scd_set_projectors(scd_ctx *c, int32_t M_box, int32_t T, const scd_c128 *S, 
     for (int g = 0; g < 4; ++g)
         for (int s = 0; s < T; ++s) {
             const scd_c128 *p = src[g] + 27LL * c->perm[s];
-            cd *o = h.data() + (size_t)g * 27 * T + 27LL * s;
-            for (int j = 0; j < 27; ++j) o[j] = cmk(p[j].re, p[j].im);
+            for (int j = 0; j < 27; ++j) h[(size_t)(g * 27 + j) * T + s] = cmk(p[j].re, p[j].im);
         }
     if ((rc = dalloc(c, &c->d_P, h.size(), "projectors"))) return rc;
     CK(cudaMemcpy(c->d_P, h.data(), sizeof(cd) * h.size(), cudaMemcpyHostToDevice), "projectors");
@@ -393,6 +394,9 @@ int scd_set_nearzone(scd_ctx *c, int64_t B, const void *sp_mat, const int32_t *s
     if (!c->have_order) return set_error(c, SCD_NOT_READY, "set the projectors (or the mesh) before the near zone");
     if (B < 0 || (B > 0 && (!sp_mat || !sp_ind))) return set_error(c, SCD_BAD_ARG, "bad near-zone arrays");
     if (prec != SCD_STORE_C64 && prec != SCD_STORE_C128) return set_error(c, SCD_BAD_ARG, "storage_prec %d", prec);
+    if (c->max_per_cube > SCD_NEAR_MAXN)
+        return set_error(c, SCD_BAD_ARG, "%d tets in one projection box; the near-zone kernels support %d",
+                         c->max_per_cube, SCD_NEAR_MAXN);
     int rc;
     c->have_near = false;
     c->near_prec = prec;
@@ -466,18 +470,17 @@ int scd_solve_columns(scd_ctx *c, int32_t ncol, const scd_c128 *mat, scd_c128 *T
     if ((rc = dalloc(c, &d_mat, (size_t)n * ncol, "mat"))) return rc;
     if ((rc = dalloc(c, &d_X, (size_t)n * ncol, "X"))) { cudaFree(d_mat); return rc; }
     if ((rc = dalloc(c, &d_T, (size_t)ncol * ncol, "T"))) { cudaFree(d_mat); cudaFree(d_X); return rc; }
-    int worst = SCD_OK;
     cudaEventRecord(c->ev[4], c->st);
-    for (int col = 0; col < ncol && worst != SCD_NAN && worst != SCD_TIMEOUT; ++col) {
+    for (int col = 0; col < ncol; ++col) {
         CK(cudaMemcpyAsync(c->d_io, mat + (size_t)n * col, sizeof(cd) * n, cudaMemcpyHostToDevice, c->st), "mat");
         launch_permute_in(c, c->d_io, d_mat + (size_t)n * col, 1, n);
-        int it = 0;
-        double rr = 0;
-        rc = gmres_solve(c, d_mat + (size_t)n * col, d_X + (size_t)n * col, o->tol, o->m, o->cycles, &it, &rr);
-        if (iters) iters[col] = it;
-        if (rc != SCD_OK && rc != SCD_NOT_CONVERGED) { worst = rc; break; }
-        if (rc == SCD_NOT_CONVERGED) worst = SCD_NOT_CONVERGED;
     }
+    std::vector<const cd *> cols(ncol);
+    for (int j = 0; j < ncol; ++j) cols[j] = d_mat + (size_t)n * j;
+    const int ns = o->block > 0 ? o->block : ncol;
+    std::vector<int> it(ncol, 0);
+    int worst = batch_solve(c, ncol, cols.data(), d_X, o->tol, o->m, o->cycles, ns, it.data(), nullptr, nullptr);
+    if (iters) for (int j = 0; j < ncol; ++j) iters[j] = it[j];
     if (worst == SCD_OK || worst == SCD_NOT_CONVERGED) {
         launch_T_assemble(c, d_mat, ncol, 0, ncol, d_X, d_T);
         rc = check_cuda(c, cudaMemcpyAsync(Tcols, d_T, sizeof(cd) * ncol * ncol, cudaMemcpyDeviceToHost, c->st), "T");
@@ -523,20 +526,22 @@ int scd_get_timing(scd_ctx *c, scd_timing *t, int32_t reset) {
     return SCD_OK;
 }
 
-int scd_profile_matvec(scd_ctx *c, int32_t reps) {
-    if (!c || reps < 1) return SCD_BAD_ARG;
+int scd_profile_matvec(scd_ctx *c, int32_t reps, int32_t nrhs) {
+    if (!c || reps < 1 || nrhs < 1) return SCD_BAD_ARG;
     cudaSetDevice(c->dev);
     int rc = ready(c);
     if (rc) return rc;
+    if ((rc = ensure_work(c, nrhs))) return rc;
     // a fixed non-trivial vector: the first VSWF-like pattern is not needed,
     // any dense vector exercises the same memory traffic
     std::vector<cd> h((size_t)c->n);
     for (long long i = 0; i < c->n; ++i) h[i] = cmk(std::sin(0.37 * (double)i), std::cos(0.11 * (double)i));
-    CK(cudaMemcpy(c->d_x, h.data(), sizeof(cd) * c->n, cudaMemcpyHostToDevice), "profile x");
+    for (int r = 0; r < nrhs; ++r)
+        CK(cudaMemcpy(c->d_x + (size_t)r * c->n, h.data(), sizeof(cd) * c->n, cudaMemcpyHostToDevice), "profile x");
     double sn = 0, sf = 0, sg = 0, st = 0;
     c->timing = true;
     for (int r = 0; r < reps + 1; ++r) {
-        run_matvec(c, c->d_x, c->d_y, 1, nullptr);
+        run_matvec(c, c->d_x, c->d_y, nrhs, nullptr);
         CK(cudaStreamSynchronize(c->st), "profile");
         float a = 0, b = 0, g = 0, t = 0;
         cudaEventElapsedTime(&a, c->ev[0], c->ev[1]);
@@ -552,6 +557,14 @@ int scd_profile_matvec(scd_ctx *c, int32_t reps) {
     c->t_gather = sg / reps;
     c->t_matvec = st / reps;
     return check_cuda(c, cudaGetLastError(), "profile");
+}
+
+int scd_column_latency(scd_ctx *c, int32_t ncol, double *ms) {
+    if (!c || !ms) return SCD_BAD_ARG;
+    if ((size_t)ncol != c->col_latency_ms.size())
+        return set_error(c, SCD_BAD_ARG, "ncol = %d, last solve had %zu columns", ncol, c->col_latency_ms.size());
+    for (int i = 0; i < ncol; ++i) ms[i] = c->col_latency_ms[i];
+    return SCD_OK;
 }
 
 int64_t scd_nearzone_bytes(scd_ctx *c) {
@@ -581,15 +594,12 @@ int scd_compute_T_matrix(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int3
     if ((rc = dalloc(c, &d_X, (size_t)n * ncol, "X"))) return rc;
     if ((rc = dalloc(c, &d_T, (size_t)ntot * ncol, "T"))) { cudaFree(d_X); return rc; }
     cudaEventRecord(c->ev[4], c->st);
-    int worst = SCD_OK;
-    for (int j = 0; j < ncol; ++j) {
-        int it = 0;
-        double rr = 0;
-        rc = gmres_solve(c, c->d_mat + (size_t)n * (col0 + j), d_X + (size_t)n * j, o->tol, o->m, o->cycles, &it, &rr);
-        if (iters) iters[j] = it;
-        if (rc != SCD_OK && rc != SCD_NOT_CONVERGED) { worst = rc; break; }
-        if (rc == SCD_NOT_CONVERGED) worst = rc;
-    }
+    std::vector<const cd *> cols(ncol);
+    for (int j = 0; j < ncol; ++j) cols[j] = c->d_mat + (size_t)n * (col0 + j);
+    const int ns = o->block > 0 ? o->block : ncol;
+    std::vector<int> it(ncol, 0);
+    int worst = batch_solve(c, ncol, cols.data(), d_X, o->tol, o->m, o->cycles, ns, it.data(), nullptr, nullptr);
+    if (iters) for (int j = 0; j < ncol; ++j) iters[j] = it[j];
     if (worst == SCD_OK || worst == SCD_NOT_CONVERGED) {
         launch_T_assemble(c, c->d_mat, ntot, 0, ncol, d_X, d_T);
         cudaEventRecord(c->ev[5], c->st);

@@ -1,0 +1,507 @@
+// Batched T-matrix column solves: `nslots` GMRES solves advance together,
+// one Arnoldi step per tick, sharing every read of the operator (projectors,
+// Green octant, near-zone tiles) and every grid barrier.  Each slot runs its
+// own restarted GMRES exactly as gmres (src/gmres_module.f90:180-325): x0 =
+// rhs, MGS with the conditional re-orthogonalisation, complex Givens, y =
+// H^-1 g, x += V y.  A slot's arithmetic does not depend on what the other
+// slots hold (per-slot reductions over a fixed CTA partition, summed in a
+// fixed order), so a column's result is bit-identical whether it is solved
+// alone or in a batch.  A slot whose column converged (or ran out of cycles)
+// is refilled with the next column on the following tick (continuous
+// batching).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "ctx.h"
+
+namespace {
+
+constexpr int BT = 256;             // threads per CTA of the tick kernel
+constexpr int NSMAX = 64;           // slot limit (partial buffer sizing)
+
+enum { SLOT_FREE = 0, SLOT_START = 1, SLOT_ARNOLDI = 2, SLOT_DONE = 3 };
+
+struct Slot {
+    int mode, col, cycle, step, iters, conv, status, reorth, finish, pad;
+    double b_norm, beta, error;
+};
+
+struct TickArgs {
+    Slot *slots;
+    int ns;
+    cd *V;          // [slot][m+1][n]
+    cd *H;          // [slot][(m+1) m]
+    cd *cs, *sn, *g, *y;   // [slot][m+1]
+    cd *x, *rhs, *w;       // [slot][n]
+    double *red;    // [2][grid][NSMAX*4]
+    GridBarrier *bar;
+    int *err;
+    long long n;
+    int m, max_cycles;
+    double tol;
+};
+
+__device__ __forceinline__ double *partial_slot(const TickArgs &a, int parity, int s) {
+    return a.red + ((size_t)parity * gridDim.x + blockIdx.x) * (NSMAX * 4) + s * 4;
+}
+
+// totals of the per-CTA partials of every slot: warp w reduces slots w,
+// w + nwarps, ...; lanes stride over CTAs; fixed order, deterministic
+__device__ void read_totals(const TickArgs &a, int parity, int nv, double (*tot)[4]) {
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int s = wp; s < a.ns; s += nw) {
+        double acc[4] = {0, 0, 0, 0};
+        for (int b = lane; b < (int)gridDim.x; b += 32) {
+            const double *p = a.red + ((size_t)parity * gridDim.x + b) * (NSMAX * 4) + s * 4;
+            for (int q = 0; q < nv; ++q) acc[q] += __ldcg(p + q);
+        }
+        for (int q = 0; q < nv; ++q) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+        }
+        if (lane == 0)
+            for (int q = 0; q < nv; ++q) tot[s][q] = acc[q];
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void put_partial(const TickArgs &a, int parity, int s, const double *v, int nv) {
+    if (threadIdx.x == 0) {
+        double *p = partial_slot(a, parity, s);
+        for (int q = 0; q < nv; ++q) p[q] = v[q];
+    }
+}
+
+// One tick: cycle starts (r = rhs - A x, V0 = r/||r||) and Arnoldi steps
+// (MGS, normalisation, Givens) for every active slot; cycle ends update x.
+__global__ void __launch_bounds__(BT) k_tick(TickArgs a) {
+    __shared__ double bsh[64];
+    __shared__ double tot[NSMAX][4];
+    __shared__ int smode[NSMAX], sstep[NSMAX];
+    __shared__ double snormav[NSMAX], shn[NSMAX];
+    __shared__ cd sh_h[NSMAX];
+    __shared__ cd ysm[64];
+    const long long n = a.n;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long q0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int ldh = a.m + 1;
+    for (int s = threadIdx.x; s < a.ns; s += blockDim.x) {
+        smode[s] = a.slots[s].mode;
+        sstep[s] = a.slots[s].step;
+    }
+    __syncthreads();
+    int parity = 0;
+    // ---- phase A: first reduction of every active slot
+    for (int s = 0; s < a.ns; ++s) {
+        const int md = smode[s];
+        double v[3] = {0, 0, 0};
+        const cd *ws = a.w + (size_t)s * n;
+        cd *V0 = a.V + (size_t)s * (a.m + 1) * n;
+        if (md == SLOT_START) {
+            const cd *bs = a.rhs + (size_t)s * n;
+            for (long long q = q0; q < n; q += stride) {
+                const cd b = bs[q];
+                const cd r = csub(b, ws[q]);
+                V0[q] = r;
+                v[0] += cabs2(r);
+                v[1] += cabs2(b);
+            }
+        } else if (md == SLOT_ARNOLDI) {
+            for (long long q = q0; q < n; q += stride) {
+                const cd w = ws[q], z = V0[q];
+                v[0] += cabs2(w);
+                cdot_acc(v[1], v[2], z, w);
+            }
+        } else {
+            continue;
+        }
+        block_sum<3>(v, bsh);
+        put_partial(a, parity, s, v, 3);
+    }
+    grid_barrier(a.bar, gridDim.x, a.err);
+    read_totals(a, parity, 3, tot);
+    int kmax = 0;
+    for (int s = 0; s < a.ns; ++s) {
+        if (smode[s] == SLOT_ARNOLDI) kmax = max(kmax, sstep[s] + 1);
+        if (threadIdx.x == 0) {
+            snormav[s] = sqrt(tot[s][0]);
+            sh_h[s] = cmk(tot[s][1], tot[s][2]);
+        }
+    }
+    __syncthreads();
+    // cycle starts: normalise V0, set g, b_norm
+    for (int s = 0; s < a.ns; ++s) {
+        if (smode[s] != SLOT_START) continue;
+        const double beta = sqrt(tot[s][0]);
+        cd *V0 = a.V + (size_t)s * (a.m + 1) * n;
+        for (long long q = q0; q < n; q += stride) {
+            const cd r = V0[q];
+            V0[q] = cmk(r.x / beta, r.y / beta);
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            Slot &sl = a.slots[s];
+            cd *gs = a.g + (size_t)s * (a.m + 1);
+            for (int i = 0; i <= a.m; ++i) gs[i] = cmk(0, 0);
+            gs[0] = cmk(beta, 0.0);
+            sl.beta = beta;
+            if (sl.cycle == 0) sl.b_norm = sqrt(tot[s][1]);
+            sl.cycle += 1;
+            sl.step = 0;
+            sl.mode = SLOT_ARNOLDI;
+            if (sl.cycle == 1 && sl.b_norm == 0.0) { sl.error = 0.0; sl.conv = 1; sl.mode = SLOT_DONE; }
+            else if (!(beta == beta)) { sl.status = SCD_NAN; sl.mode = SLOT_DONE; }
+        }
+    }
+    // ---- MGS for the Arnoldi slots: one barrier per term
+    for (int k = 1; k <= kmax; ++k) {
+        for (int s = 0; s < a.ns; ++s) {
+            if (smode[s] != SLOT_ARNOLDI) continue;
+            const int i = sstep[s] + 1;
+            if (k > i) continue;
+            const cd h = sh_h[s];
+            if (blockIdx.x == 0 && threadIdx.x == 0) a.H[(size_t)s * ldh * a.m + (size_t)ldh * (i - 1) + (k - 1)] = h;
+            cd *ws = a.w + (size_t)s * n;
+            const cd *Vs = a.V + (size_t)s * (a.m + 1) * n;
+            const cd *vk = Vs + (size_t)(k - 1) * n;
+            const cd *vn = (k < i) ? Vs + (size_t)k * n : nullptr;
+            double u[2] = {0, 0};
+            for (long long q = q0; q < n; q += stride) {
+                cd w = ws[q];
+                const cd p = vk[q];
+                csub_mul(w, h, p);
+                ws[q] = w;
+                if (vn) {
+                    const cd z = vn[q];
+                    cdot_acc(u[0], u[1], z, w);
+                } else {
+                    u[0] += cabs2(w);
+                }
+            }
+            block_sum<2>(u, bsh);
+            put_partial(a, parity ^ 1, s, u, 2);
+        }
+        parity ^= 1;
+        grid_barrier(a.bar, gridDim.x, a.err);
+        read_totals(a, parity, 2, tot);
+        if (threadIdx.x == 0) {
+            for (int s = 0; s < a.ns; ++s) {
+                if (smode[s] != SLOT_ARNOLDI) continue;
+                const int i = sstep[s] + 1;
+                if (k > i) continue;
+                sh_h[s] = cmk(tot[s][0], tot[s][1]);
+                if (k == i) shn[s] = sqrt(tot[s][0]);
+            }
+        }
+        __syncthreads();
+    }
+    // ---- conditional re-orthogonalisation (src/gmres_module.f90:251-258)
+    int jmax = 0;
+    for (int s = 0; s < a.ns; ++s)
+        if (smode[s] == SLOT_ARNOLDI && snormav[s] + (double)0.001f * shn[s] == snormav[s]) jmax = max(jmax, sstep[s] + 1);
+    for (int j = 1; j <= jmax; ++j) {
+        for (int s = 0; s < a.ns; ++s) {
+            if (smode[s] != SLOT_ARNOLDI || !(snormav[s] + (double)0.001f * shn[s] == snormav[s]) || j > sstep[s] + 1) continue;
+            const cd *vj = a.V + (size_t)s * (a.m + 1) * n + (size_t)(j - 1) * n;
+            const cd *ws = a.w + (size_t)s * n;
+            double u[2] = {0, 0};
+            for (long long q = q0; q < n; q += stride) {
+                const cd z = vj[q], w = ws[q];
+                cdot_acc(u[0], u[1], z, w);
+            }
+            block_sum<2>(u, bsh);
+            put_partial(a, parity ^ 1, s, u, 2);
+        }
+        parity ^= 1;
+        grid_barrier(a.bar, gridDim.x, a.err);
+        read_totals(a, parity, 2, tot);
+        for (int s = 0; s < a.ns; ++s) {
+            if (smode[s] != SLOT_ARNOLDI || !(snormav[s] + (double)0.001f * shn[s] == snormav[s]) || j > sstep[s] + 1) continue;
+            const int i = sstep[s] + 1;
+            const cd hr = cmk(tot[s][0], tot[s][1]);
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                cd *Hc = a.H + (size_t)s * ldh * a.m + (size_t)ldh * (i - 1);
+                Hc[j - 1] = cadd(Hc[j - 1], hr);
+            }
+            const cd *vj = a.V + (size_t)s * (a.m + 1) * n + (size_t)(j - 1) * n;
+            cd *ws = a.w + (size_t)s * n;
+            for (long long q = q0; q < n; q += stride) {
+                cd w = ws[q];
+                const cd p = vj[q];
+                csub_mul(w, hr, p);
+                ws[q] = w;
+            }
+        }
+    }
+    if (jmax > 0) {
+        for (int s = 0; s < a.ns; ++s) {
+            if (smode[s] != SLOT_ARNOLDI || !(snormav[s] + (double)0.001f * shn[s] == snormav[s])) continue;
+            const cd *ws = a.w + (size_t)s * n;
+            double u[1] = {0};
+            for (long long q = q0; q < n; q += stride) u[0] += cabs2(ws[q]);
+            block_sum<1>(u, bsh);
+            put_partial(a, parity ^ 1, s, u, 1);
+        }
+        parity ^= 1;
+        grid_barrier(a.bar, gridDim.x, a.err);
+        read_totals(a, parity, 1, tot);
+        if (threadIdx.x == 0)
+            for (int s = 0; s < a.ns; ++s)
+                if (smode[s] == SLOT_ARNOLDI && snormav[s] + (double)0.001f * shn[s] == snormav[s]) shn[s] = sqrt(tot[s][0]);
+        __syncthreads();
+    }
+    // ---- v_i = w / h(i+1,i) and the Givens update
+    for (int s = 0; s < a.ns; ++s) {
+        if (smode[s] != SLOT_ARNOLDI) continue;
+        const int i = sstep[s] + 1;
+        const double hn = shn[s];
+        const cd *ws = a.w + (size_t)s * n;
+        cd *vi = a.V + (size_t)s * (a.m + 1) * n + (size_t)i * n;
+        for (long long q = q0; q < n; q += stride) {
+            const cd w = ws[q];
+            vi[q] = (hn != 0.0) ? cmk(w.x / hn, w.y / hn) : w;
+        }
+    }
+    if (blockIdx.x == 0) {
+        for (int s = threadIdx.x; s < a.ns; s += blockDim.x) {
+            if (smode[s] != SLOT_ARNOLDI) continue;
+            Slot &sl = a.slots[s];
+            const int i = sstep[s] + 1;
+            cd *Hc = a.H + (size_t)s * ldh * a.m + (size_t)ldh * (i - 1);
+            cd *cs = a.cs + (size_t)s * (a.m + 1), *sn = a.sn + (size_t)s * (a.m + 1), *g = a.g + (size_t)s * (a.m + 1);
+            Hc[i] = cmk(shn[s], 0.0);
+            for (int k = 1; k <= i - 1; ++k) {
+                const cd c = cs[k - 1], sv = sn[k - 1];
+                const cd tmp = csub(cmul(c, Hc[k - 1]), cmul(sv, Hc[k]));
+                Hc[k] = cadd(cmul(sv, Hc[k - 1]), cmul(cconj(c), Hc[k]));
+                Hc[k - 1] = tmp;
+            }
+            const double nu = sqrt(cabs2(Hc[i - 1]) + cabs2(Hc[i]));
+            if (nu != 0.0) {
+                const cd c = cconj(cmk(Hc[i - 1].x / nu, Hc[i - 1].y / nu));
+                const cd sv = cmk(-Hc[i].x / nu, -Hc[i].y / nu);
+                cs[i - 1] = c;
+                sn[i - 1] = sv;
+                Hc[i - 1] = csub(cmul(c, Hc[i - 1]), cmul(sv, Hc[i]));
+                Hc[i] = cmk(0, 0);
+                const cd t1 = g[i - 1], t2 = g[i];
+                g[i - 1] = csub(cmul(c, t1), cmul(sv, t2));
+                g[i] = cadd(cmul(sv, t1), cmul(cconj(c), t2));
+            }
+            const double error = sqrt(cabs2(g[i])) / sl.b_norm;
+            sl.error = error;
+            sl.step = i;
+            sl.iters += 1;
+            if (snormav[s] + (double)0.001f * shn[s] == snormav[s]) sl.reorth += 1;
+            sl.finish = 0;
+            if (error < a.tol) { sl.conv = 1; sl.finish = 1; }
+            else if (i == a.m) sl.finish = 1;
+            if (!(error == error)) { sl.status = SCD_NAN; sl.finish = 0; sl.mode = SLOT_DONE; }
+            if (*a.err) { sl.status = SCD_TIMEOUT; sl.finish = 0; sl.mode = SLOT_DONE; }
+            if (sl.finish) {
+                // y = H(1:i,1:i)^-1 g(1:i), back substitution
+                cd *ys = a.y + (size_t)s * (a.m + 1);
+                const cd *Hs = a.H + (size_t)s * ldh * a.m;
+                for (int r = i - 1; r >= 0; --r) {
+                    cd acc = g[r];
+                    for (int cc = r + 1; cc < i; ++cc) acc = csub(acc, cmul(Hs[r + (size_t)ldh * cc], ys[cc]));
+                    ys[r] = cdiv(acc, Hs[r + (size_t)ldh * r]);
+                }
+            }
+        }
+    }
+    grid_barrier(a.bar, gridDim.x, a.err);
+    // ---- cycle end: x += V(:,1:i) y; next cycle or done
+    for (int s = 0; s < a.ns; ++s) {
+        if (smode[s] != SLOT_ARNOLDI) continue;
+        const Slot *sl = a.slots + s;
+        if (!__ldcg(&sl->finish)) continue;      // uniform across the CTA (L2 read after the barrier)
+        const int kd = __ldcg(&sl->step);
+        const cd *ys = a.y + (size_t)s * (a.m + 1);
+        for (int c = threadIdx.x; c < kd; c += blockDim.x) ysm[c] = make_double2(__ldcg(&ys[c].x), __ldcg(&ys[c].y));
+        __syncthreads();
+        const cd *Vs = a.V + (size_t)s * (a.m + 1) * n;
+        cd *xs = a.x + (size_t)s * n;
+        for (long long q = q0; q < n; q += stride) {
+            cd acc = cmk(0, 0);
+            for (int c = 0; c < kd; ++c) cfma(acc, Vs[(size_t)c * n + q], ysm[c]);
+            xs[q] = cadd(xs[q], acc);
+        }
+        __syncthreads();
+    }
+    if (blockIdx.x == 0) {
+        // `finish` stays set: other CTAs may still be reading it; the next
+        // Givens update of the slot overwrites it
+        for (int s = threadIdx.x; s < a.ns; s += blockDim.x) {
+            if (smode[s] != SLOT_ARNOLDI) continue;
+            Slot &sl = a.slots[s];
+            if (!sl.finish) continue;
+            if (sl.conv) sl.mode = SLOT_DONE;
+            else if (sl.cycle < a.max_cycles) sl.mode = SLOT_START;
+            else sl.mode = SLOT_DONE;
+        }
+    }
+}
+
+// matvec input per slot: x at a cycle start, v_step during Arnoldi; idle
+// slots are skipped by every matvec kernel
+__global__ void k_stage(const Slot *slots, int ns, const cd *V, const cd *x, cd *Xin, int *skip, long long n, int m) {
+    const int s = blockIdx.y;
+    const int md = slots[s].mode;
+    const bool act = md == SLOT_START || md == SLOT_ARNOLDI;
+    if (blockIdx.x == 0 && threadIdx.x == 0) skip[s] = act ? 0 : 1;
+    if (!act) return;
+    const cd *src = md == SLOT_START ? x + (size_t)s * n : V + ((size_t)s * (m + 1) + slots[s].step) * n;
+    cd *dst = Xin + (size_t)s * n;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        dst[q] = src[q];
+}
+
+}  // namespace
+
+struct BatchBuffers {
+    int ns = 0, m = 0;
+    long long n = 0;
+    cd *V = nullptr, *H = nullptr, *cs = nullptr, *sn = nullptr, *g = nullptr, *y = nullptr;
+    cd *x = nullptr, *rhs = nullptr, *Xin = nullptr, *W = nullptr;
+    Slot *slots = nullptr;
+    Slot *h_slots = nullptr;
+    int *skip = nullptr;
+    double *red = nullptr;
+    int grid = 0;
+};
+
+static void free_bb(BatchBuffers &b) {
+    void *p[] = {b.V, b.H, b.cs, b.sn, b.g, b.y, b.x, b.rhs, b.Xin, b.W, b.slots, b.skip, b.red};
+    for (void *q : p) if (q) cudaFree(q);
+    if (b.h_slots) cudaFreeHost(b.h_slots);
+    b = BatchBuffers();
+}
+
+void batch_free(scd_ctx *c) {
+    if (!c->batch) return;
+    free_bb(*(BatchBuffers *)c->batch);
+    delete (BatchBuffers *)c->batch;
+    c->batch = nullptr;
+}
+
+int batch_prepare(scd_ctx *c, int ns, int m, BatchBuffers &b) {
+    if (b.ns >= ns && b.m >= m && b.n == c->n && b.V) return SCD_OK;
+    free_bb(b);
+    const long long n = c->n;
+    auto al = [&](void **p, size_t bytes, const char *what) -> int {
+        if (cudaMalloc(p, bytes) != cudaSuccess) { cudaGetLastError(); return set_error(c, SCD_OOM, "batch %s (%zu bytes)", what, bytes); }
+        return SCD_OK;
+    };
+    int rc;
+    if ((rc = al((void **)&b.V, sizeof(cd) * (size_t)ns * (m + 1) * n, "Krylov bases"))) return rc;
+    if ((rc = al((void **)&b.H, sizeof(cd) * (size_t)ns * (m + 1) * m, "H"))) return rc;
+    if ((rc = al((void **)&b.cs, sizeof(cd) * (size_t)ns * (m + 1), "cs"))) return rc;
+    if ((rc = al((void **)&b.sn, sizeof(cd) * (size_t)ns * (m + 1), "sn"))) return rc;
+    if ((rc = al((void **)&b.g, sizeof(cd) * (size_t)ns * (m + 1), "g"))) return rc;
+    if ((rc = al((void **)&b.y, sizeof(cd) * (size_t)ns * (m + 1), "y"))) return rc;
+    if ((rc = al((void **)&b.x, sizeof(cd) * (size_t)ns * n, "x"))) return rc;
+    if ((rc = al((void **)&b.rhs, sizeof(cd) * (size_t)ns * n, "rhs"))) return rc;
+    if ((rc = al((void **)&b.Xin, sizeof(cd) * (size_t)ns * n, "Xin"))) return rc;
+    if ((rc = al((void **)&b.W, sizeof(cd) * (size_t)ns * n, "W"))) return rc;
+    if ((rc = al((void **)&b.slots, sizeof(Slot) * ns, "slots"))) return rc;
+    if ((rc = al((void **)&b.skip, sizeof(int) * ns, "skip"))) return rc;
+    if (cudaMallocHost((void **)&b.h_slots, sizeof(Slot) * ns) != cudaSuccess) return set_error(c, SCD_OOM, "pinned slots");
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tick, BT, 0);
+    if (per_sm < 1) return set_error(c, SCD_CUDA_ERROR, "tick kernel cannot be resident");
+    per_sm = std::min(per_sm, 2);
+    b.grid = per_sm * c->nsm;
+    if ((rc = al((void **)&b.red, sizeof(double) * 2 * (size_t)b.grid * NSMAX * 4, "partials"))) return rc;
+    b.ns = ns;
+    b.m = m;
+    b.n = n;
+    return SCD_OK;
+}
+
+// Solve columns `cols` (device pointers to slot-ordered right-hand sides)
+// with up to `ns` slots; solutions go to X[j] (slot-ordered, stride n).
+int batch_solve(scd_ctx *c, int ncol, const cd *const *rhs_cols, cd *X, double tol, int m, int cycles, int ns,
+                int *iters, int *conv_out, int *status_out) {
+    if (!c->batch) c->batch = new BatchBuffers();
+    BatchBuffers &bb = *(BatchBuffers *)c->batch;
+    if (ns > NSMAX) ns = NSMAX;
+    if (ns > ncol) ns = ncol;
+    int rc = batch_prepare(c, ns, m, bb);
+    if (rc) return rc;
+    if ((rc = ensure_work(c, ns))) return rc;
+    if (!c->d_bar) {
+        if (cudaMalloc(&c->d_bar, sizeof(GridBarrier)) != cudaSuccess || cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess)
+            return set_error(c, SCD_OOM, "barrier");
+    }
+    cudaMemsetAsync(c->d_bar, 0, sizeof(GridBarrier), c->st);
+    cudaMemsetAsync(c->d_err, 0, sizeof(int), c->st);
+    const long long n = c->n;
+    Slot *hs = bb.h_slots;
+    std::memset(hs, 0, sizeof(Slot) * ns);
+    for (int s = 0; s < ns; ++s) { hs[s].mode = SLOT_FREE; hs[s].col = -1; }
+    int next = 0, finished = 0, worst = SCD_OK;
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
+    auto now_ms = [&]() { return std::chrono::duration<double, std::milli>(clk::now() - t0).count(); };
+    std::vector<double> t_in(ncol, 0.0);
+    c->col_latency_ms.assign(ncol, 0.0);
+    TickArgs a;
+    a.slots = bb.slots; a.ns = ns; a.V = bb.V; a.H = bb.H; a.cs = bb.cs; a.sn = bb.sn; a.g = bb.g; a.y = bb.y;
+    a.x = bb.x; a.rhs = bb.rhs; a.w = bb.W; a.red = bb.red; a.bar = c->d_bar; a.err = c->d_err; a.n = n;
+    a.m = m; a.max_cycles = cycles; a.tol = tol;
+    long long ticks = 0;
+    while (finished < ncol) {
+        // refill free slots
+        bool any = false;
+        for (int s = 0; s < ns; ++s) {
+            if (hs[s].mode == SLOT_DONE) {
+                const int col = hs[s].col;
+                cudaMemcpyAsync(X + (size_t)col * n, bb.x + (size_t)s * n, sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
+                if (iters) iters[col] = hs[s].iters;
+                c->col_latency_ms[col] = now_ms() - t_in[col];
+                if (conv_out) conv_out[col] = hs[s].conv;
+                if (status_out) status_out[col] = hs[s].status;
+                if (hs[s].status != SCD_OK) worst = hs[s].status;
+                else if (!hs[s].conv && worst == SCD_OK) worst = SCD_NOT_CONVERGED;
+                c->n_arn += hs[s].iters;
+                c->n_matvec += hs[s].iters + hs[s].cycle;
+                ++finished;
+                std::memset(&hs[s], 0, sizeof(Slot));
+                hs[s].mode = SLOT_FREE;
+                hs[s].col = -1;
+            }
+            if (hs[s].mode == SLOT_FREE && next < ncol) {
+                cudaMemcpyAsync(bb.rhs + (size_t)s * n, rhs_cols[next], sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
+                cudaMemcpyAsync(bb.x + (size_t)s * n, rhs_cols[next], sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
+                std::memset(&hs[s], 0, sizeof(Slot));
+                hs[s].mode = SLOT_START;
+                t_in[next] = now_ms();
+                hs[s].col = next++;
+            }
+            if (hs[s].mode == SLOT_START || hs[s].mode == SLOT_ARNOLDI) any = true;
+        }
+        if (finished >= ncol) break;
+        if (!any) return set_error(c, SCD_CUDA_ERROR, "batch solver stalled");
+        cudaMemcpyAsync(bb.slots, hs, sizeof(Slot) * ns, cudaMemcpyHostToDevice, c->st);
+        k_stage<<<dim3(std::min<long long>((n + 255) / 256, 1024), ns), 256, 0, c->st>>>(bb.slots, ns, bb.V, bb.x, bb.Xin,
+                                                                                         bb.skip, n, m);
+        run_matvec(c, bb.Xin, bb.W, ns, bb.skip);
+        void *args[] = {&a};
+        cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_tick, dim3(bb.grid), dim3(BT), args, 0, c->st);
+        c->launches += 2;
+        if ((rc = check_cuda(c, e, "tick launch"))) return rc;
+        cudaMemcpyAsync(hs, bb.slots, sizeof(Slot) * ns, cudaMemcpyDeviceToHost, c->st);
+        if ((rc = check_cuda(c, cudaStreamSynchronize(c->st), "tick"))) return rc;
+        ++ticks;
+        for (int s = 0; s < ns; ++s)
+            if (hs[s].status == SCD_TIMEOUT) return set_error(c, SCD_TIMEOUT, "grid barrier wait expired in the batch solver");
+    }
+    rc = check_cuda(c, cudaStreamSynchronize(c->st), "batch end");
+    if (rc) return rc;
+    return worst;
+}

@@ -11,19 +11,55 @@
 typedef double2 cd;     // complex double, (x, y) = (re, im)
 typedef float2  cf;     // complex float
 
+// Complex arithmetic with a pinned operation sequence: device code uses
+// explicit round-to-nearest intrinsics so that the compiler cannot contract
+// or reorder differently in different kernels (results of a column are
+// bit-identical whichever kernel variant computes them).
+#ifdef __CUDA_ARCH__
+#define SCD_FMA(a, b, c) __fma_rn((a), (b), (c))
+#define SCD_MUL(a, b) __dmul_rn((a), (b))
+#define SCD_ADD(a, b) __dadd_rn((a), (b))
+#define SCD_SUB(a, b) __dsub_rn((a), (b))
+#else
+#define SCD_FMA(a, b, c) fma((a), (b), (c))
+#define SCD_MUL(a, b) ((a) * (b))
+#define SCD_ADD(a, b) ((a) + (b))
+#define SCD_SUB(a, b) ((a) - (b))
+#endif
+
 SCD_HD cd  cmk(double r, double i) { return make_double2(r, i); }
-SCD_HD cd  cadd(cd a, cd b) { return make_double2(a.x + b.x, a.y + b.y); }
-SCD_HD cd  csub(cd a, cd b) { return make_double2(a.x - b.x, a.y - b.y); }
-SCD_HD cd  cmul(cd a, cd b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+SCD_HD cd  cadd(cd a, cd b) { return make_double2(SCD_ADD(a.x, b.x), SCD_ADD(a.y, b.y)); }
+SCD_HD cd  csub(cd a, cd b) { return make_double2(SCD_SUB(a.x, b.x), SCD_SUB(a.y, b.y)); }
+SCD_HD cd  cmul(cd a, cd b) {
+    return make_double2(SCD_FMA(a.x, b.x, SCD_MUL(-a.y, b.y)), SCD_FMA(a.x, b.y, SCD_MUL(a.y, b.x)));
+}
 SCD_HD cd  cconj(cd a) { return make_double2(a.x, -a.y); }
-SCD_HD cd  cscale(cd a, double s) { return make_double2(a.x * s, a.y * s); }
+SCD_HD cd  cscale(cd a, double s) { return make_double2(SCD_MUL(a.x, s), SCD_MUL(a.y, s)); }
 // a += b * c
-SCD_HD void cfma(cd &a, cd b, cd c) { a.x += b.x * c.x - b.y * c.y; a.y += b.x * c.y + b.y * c.x; }
+SCD_HD void cfma(cd &a, cd b, cd c) {
+    a.x = SCD_FMA(-b.y, c.y, SCD_FMA(b.x, c.x, a.x));
+    a.y = SCD_FMA(b.y, c.x, SCD_FMA(b.x, c.y, a.y));
+}
 // a += conj(b) * c
-SCD_HD void cfma_conj(cd &a, cd b, cd c) { a.x += b.x * c.x + b.y * c.y; a.y += b.x * c.y - b.y * c.x; }
-SCD_HD double cabs2(cd a) { return a.x * a.x + a.y * a.y; }
+SCD_HD void cfma_conj(cd &a, cd b, cd c) {
+    a.x = SCD_FMA(b.y, c.y, SCD_FMA(b.x, c.x, a.x));
+    a.y = SCD_FMA(-b.y, c.x, SCD_FMA(b.x, c.y, a.y));
+}
+SCD_HD double cabs2(cd a) { return SCD_FMA(a.x, a.x, SCD_MUL(a.y, a.y)); }
+// w -= h * p
+SCD_HD void csub_mul(cd &w, cd h, cd p) {
+    w.x = SCD_FMA(h.y, p.y, SCD_FMA(-h.x, p.x, w.x));
+    w.y = SCD_FMA(-h.y, p.x, SCD_FMA(-h.x, p.y, w.y));
+}
+// (re, im) += conj(z) * w
+SCD_HD void cdot_acc(double &re, double &im, cd z, cd w) {
+    re = SCD_FMA(z.y, w.y, SCD_FMA(z.x, w.x, re));
+    im = SCD_FMA(-z.y, w.x, SCD_FMA(z.x, w.y, im));
+}
+// a - k2 * b
+SCD_HD cd csub_scaled(cd a, double k2, cd b) { return make_double2(SCD_FMA(-k2, b.x, a.x), SCD_FMA(-k2, b.y, a.y)); }
 SCD_HD cd cdiv(cd a, cd b) {
-    double d = b.x * b.x + b.y * b.y;
+    double d = SCD_FMA(b.x, b.x, SCD_MUL(b.y, b.y));
     return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
 }
 

@@ -13,6 +13,10 @@
 #include "../../include/scadyn_gpu.h"
 #include "common.cuh"
 
+// largest number of tets in one projection box that the near-zone kernels
+// handle (register-resident column accumulators)
+#define SCD_NEAR_MAXN 64
+
 // One dense tile of near-zone blocks coupling the tets of cube c1 (rows) to
 // the tets of cube c2 (columns), c1 <= c2.  Block (i, j) is the 3x3 matrix
 // that maps the unknowns of slot off(c2)+j onto the equations of slot
@@ -60,7 +64,7 @@ struct scd_ctx {
     int max_per_cube = 0;
     int *d_perm = nullptr, *d_cube_off = nullptr;
 
-    // projectors: d_P[g*27*T + 27*slot + j], g = S, Sx, Sy, Sz
+    // projectors: d_P[(g*27 + j)*T + slot], g = S, Sx, Sy, Sz
     bool have_proj = false;
     cd *d_P = nullptr;
 
@@ -123,6 +127,9 @@ struct scd_ctx {
     long long n_matvec = 0, n_arn = 0, launches = 0;
     bool timing = false;
 
+    void *batch = nullptr;               // batch-solver buffers (batch.cu)
+    std::vector<double> col_latency_ms;  // admission -> completion, last batch solve
+
     // resident right-hand sides (vswf2constant for mat_Nmax, mat_k)
     cd *d_mat = nullptr;
     int mat_Nmax = 0;
@@ -145,6 +152,11 @@ int build_twiddles(scd_ctx *c, int P, cd **out);
 int gmres_prepare(scd_ctx *c, int m);
 int gmres_solve(scd_ctx *c, const cd *d_rhs_slot, cd *d_x_slot, double tol, int m, int cycles,
                 int *iters, double *relres);
+
+// ---- batched column solves (batch.cu) ----
+void batch_free(scd_ctx *c);
+int batch_solve(scd_ctx *c, int ncol, const cd *const *rhs_cols, cd *X, double tol, int m, int cycles, int ns,
+                int *iters, int *conv, int *status);
 
 // ---- setup (kernels_setup.cu) ----
 int setup_green(scd_ctx *c, const scd_c128 *Fg_host);

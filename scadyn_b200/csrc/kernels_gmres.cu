@@ -121,8 +121,7 @@ __global__ void __launch_bounds__(GT) k_arnoldi(GmArgs a, int i) {
     for (long long q = q0; q < n; q += stride) {
         cd w = a.w[q], z = a.V[q];
         v[0] += cabs2(w);
-        v[1] += z.x * w.x + z.y * w.y;
-        v[2] += z.x * w.y - z.y * w.x;
+        cdot_acc(v[1], v[2], z, w);
     }
     block_sum<3>(v, sh);
     write_partial(a.red, parity, 3, v);
@@ -140,13 +139,11 @@ __global__ void __launch_bounds__(GT) k_arnoldi(GmArgs a, int i) {
         for (long long q = q0; q < n; q += stride) {
             cd w = a.w[q];
             cd p = vk[q];
-            w.x -= h.x * p.x - h.y * p.y;
-            w.y -= h.x * p.y + h.y * p.x;
+            csub_mul(w, h, p);
             a.w[q] = w;
             if (vn) {
                 cd z = vn[q];
-                u[0] += z.x * w.x + z.y * w.y;
-                u[1] += z.x * w.y - z.y * w.x;
+                cdot_acc(u[0], u[1], z, w);
             } else {
                 u[0] += cabs2(w);
             }
@@ -168,8 +165,7 @@ __global__ void __launch_bounds__(GT) k_arnoldi(GmArgs a, int i) {
             double u[2] = {0, 0};
             for (long long q = q0; q < n; q += stride) {
                 cd z = vj[q], w = a.w[q];
-                u[0] += z.x * w.x + z.y * w.y;
-                u[1] += z.x * w.y - z.y * w.x;
+                cdot_acc(u[0], u[1], z, w);
             }
             parity ^= 1;
             block_sum<2>(u, sh);
@@ -181,8 +177,7 @@ __global__ void __launch_bounds__(GT) k_arnoldi(GmArgs a, int i) {
             if (blockIdx.x == 0 && threadIdx.x == 0) Hc[j - 1] = cadd(Hc[j - 1], hr);
             for (long long q = q0; q < n; q += stride) {
                 cd w = a.w[q], p = vj[q];
-                w.x -= hr.x * p.x - hr.y * p.y;
-                w.y -= hr.x * p.y + hr.y * p.x;
+                csub_mul(w, hr, p);
                 a.w[q] = w;
             }
         }

@@ -9,6 +9,9 @@
 // All vectors are slot ordered (tets sorted by cube); see ctx.h.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cstdint>
+
 #include "ctx.h"
 
 namespace {
@@ -36,36 +39,52 @@ __global__ void k_permute_out(const cd *__restrict__ xs, cd *__restrict__ xo, co
 // ---------------------------------------------------------------- scatter
 // Anterpolation (sparse_T_matmul, src/sparse.f90:13-43), one warp per cube:
 // lane j < 27 accumulates the four box-node sums of node j over the cube's
-// tets.  bpart[((r*ncubes + c)*4 + g)*27 + j].
-__global__ void k_scatter(const cd *__restrict__ x, long long ld, const cd *__restrict__ P, int T,
-                          const int *__restrict__ cube_off, int ncubes, cd *__restrict__ bpart,
-                          const int *done) {
-    if (done && *done) return;
+// tets, for a group of right-hand sides at a time (projector values are read
+// once per group).  Projectors are stored P[(g*27 + j)*T + slot].
+// bpart[((r*ncubes + c)*4 + g)*27 + j].
+template <int SC_RG>
+__global__ void __launch_bounds__(32 * WARPS_PER_CTA)
+k_scatter(const cd *__restrict__ x, long long ld, const cd *__restrict__ P, int T,
+          const int *__restrict__ cube_off, int ncubes, cd *__restrict__ bpart, const int *skip, int nrhs) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c = blockIdx.x * WARPS_PER_CTA + warp;
-    const int r = blockIdx.y;
-    if (c >= ncubes) return;
-    const cd *xr = x + r * ld;
-    const long long TT = 27LL * T;
-    cd a0 = cmk(0, 0), a1 = a0, a2 = a0, a3 = a0;
-    if (lane < 27) {
-        const int s0 = cube_off[c], s1 = cube_off[c + 1];
+    if (c >= ncubes || lane >= 27) return;
+    const int s0 = cube_off[c], s1 = cube_off[c + 1];
+    const cd *P0 = P + (size_t)lane * T, *PX = P + (size_t)(27 + lane) * T;
+    const cd *PY = P + (size_t)(54 + lane) * T, *PZ = P + (size_t)(81 + lane) * T;
+    for (int r0 = 0; r0 < nrhs; r0 += SC_RG) {
+        cd acc[SC_RG][4];
+#pragma unroll
+        for (int q = 0; q < SC_RG; ++q) acc[q][0] = acc[q][1] = acc[q][2] = acc[q][3] = cmk(0, 0);
+#pragma unroll 4
         for (int s = s0; s < s1; ++s) {
-            const cd x0 = xr[3LL * s], x1 = xr[3LL * s + 1], x2 = xr[3LL * s + 2];
-            const long long o = 27LL * s + lane;
-            const cd p0 = P[o], px = P[TT + o], py = P[2 * TT + o], pz = P[3 * TT + o];
-            cfma(a0, p0, x0);
-            cfma(a1, p0, x1);
-            cfma(a2, p0, x2);
-            cfma(a3, px, x0);
-            cfma(a3, py, x1);
-            cfma(a3, pz, x2);
+            const cd p0 = P0[s], px = PX[s], py = PY[s], pz = PZ[s];
+#pragma unroll
+            for (int q = 0; q < SC_RG; ++q) {
+                const int r = r0 + q;
+                if (r < nrhs) {
+                    const cd *xr = x + r * ld + 3LL * s;
+                    const cd x0 = xr[0], x1 = xr[1], x2 = xr[2];
+                    cfma(acc[q][0], p0, x0);
+                    cfma(acc[q][1], p0, x1);
+                    cfma(acc[q][2], p0, x2);
+                    cfma(acc[q][3], px, x0);
+                    cfma(acc[q][3], py, x1);
+                    cfma(acc[q][3], pz, x2);
+                }
+            }
         }
-        cd *o = bpart + ((long long)r * ncubes + c) * 4 * 27 + lane;
-        o[0] = a0;
-        o[27] = a1;
-        o[54] = a2;
-        o[81] = a3;
+#pragma unroll
+        for (int q = 0; q < SC_RG; ++q) {
+            const int r = r0 + q;
+            if (r < nrhs && !(skip && skip[r])) {
+                cd *o = bpart + ((long long)r * ncubes + c) * 4 * 27 + lane;
+                o[0] = acc[q][0];
+                o[27] = acc[q][1];
+                o[54] = acc[q][2];
+                o[81] = acc[q][3];
+            }
+        }
     }
 }
 
@@ -87,6 +106,10 @@ __device__ __forceinline__ void radix4(cd &v0, cd &v1, cd &v2, cd &v3) {
     v3 = csub(a1, ia3);
 }
 
+// in-line padding: one spare slot per 16 complex values spreads the
+// strided Stockham writes over the shared-memory banks
+__device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
+
 template <bool INV>
 __device__ __forceinline__ cd twid(const cd *tw, int i) {
     cd w = tw[i];
@@ -101,7 +124,7 @@ __device__ __forceinline__ void fft_line(cd *s, const cd *tw, int t) {
 #pragma unroll
     for (int st = 0; st < L / 2; ++st) {
         const int j = t;
-        cd v0 = s[j], v1 = s[j + NB], v2 = s[j + 2 * NB], v3 = s[j + 3 * NB];
+        cd v0 = s[pidx(j)], v1 = s[pidx(j + NB)], v2 = s[pidx(j + 2 * NB)], v3 = s[pidx(j + 3 * NB)];
         const int kk = j & (Ns - 1);
         if (Ns > 1) {
             const int step = P / (Ns * 4);
@@ -112,10 +135,10 @@ __device__ __forceinline__ void fft_line(cd *s, const cd *tw, int t) {
         radix4<INV>(v0, v1, v2, v3);
         __syncthreads();
         const int idx = (j / Ns) * Ns * 4 + kk;
-        s[idx] = v0;
-        s[idx + Ns] = v1;
-        s[idx + 2 * Ns] = v2;
-        s[idx + 3 * Ns] = v3;
+        s[pidx(idx)] = v0;
+        s[pidx(idx + Ns)] = v1;
+        s[pidx(idx + 2 * Ns)] = v2;
+        s[pidx(idx + 3 * Ns)] = v3;
         __syncthreads();
         Ns *= 4;
     }
@@ -124,15 +147,15 @@ __device__ __forceinline__ void fft_line(cd *s, const cd *tw, int t) {
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
             const int j = t + q * NB;
-            a[q] = s[j];
-            b[q] = cmul(s[j + P / 2], twid<INV>(tw, j));
+            a[q] = s[pidx(j)];
+            b[q] = cmul(s[pidx(j + P / 2)], twid<INV>(tw, j));
         }
         __syncthreads();
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
             const int j = t + q * NB;
-            s[j] = cadd(a[q], b[q]);
-            s[j + P / 2] = csub(a[q], b[q]);
+            s[pidx(j)] = cadd(a[q], b[q]);
+            s[pidx(j + P / 2)] = csub(a[q], b[q]);
         }
         __syncthreads();
     }
@@ -142,7 +165,7 @@ template <int P> struct FftCfg {
     static constexpr int TPL = P / 4;                        // threads per line
     static constexpr int LPB = (256 / TPL) > 0 ? 256 / TPL : 1;   // lines per CTA
     static constexpr int THREADS = TPL * LPB;
-    static constexpr int LS = P + 1;                         // padded line stride (bank spread)
+    static constexpr int LS = P + (P >> 4) + 1;              // padded line stride (bank spread)
 };
 
 struct GridDims {
@@ -180,7 +203,7 @@ __device__ __forceinline__ cd node_value(const cd *__restrict__ bp, const GridDi
 template <int P>
 __global__ void __launch_bounds__(FftCfg<P>::THREADS)
 k_fft_x_fwd(const cd *__restrict__ bpart, cd *__restrict__ W, const cd *__restrict__ twg, GridDims G, const int *done) {
-    if (done && *done) return;
+    if (done && done[blockIdx.y >> 2]) return;
     using C = FftCfg<P>;
     __shared__ cd sh[C::LPB * C::LS];
     __shared__ cd tw[P];
@@ -197,7 +220,7 @@ k_fft_x_fwd(const cd *__restrict__ bpart, cd *__restrict__ W, const cd *__restri
             const int y = line % G.Ny, z = line / G.Ny;
             v = node_value(bp, G, g, x, y, z);
         }
-        sh[l * C::LS + x] = v;
+        sh[l * C::LS + pidx(x)] = v;
     }
     __syncthreads();
     const int l = threadIdx.x / C::TPL, t = threadIdx.x - l * C::TPL;
@@ -207,7 +230,7 @@ k_fft_x_fwd(const cd *__restrict__ bpart, cd *__restrict__ W, const cd *__restri
         const int ll = e / P, x = e - ll * P, line = line0 + ll;
         if (line < nlines) {
             const int y = line % G.Ny, z = line / G.Ny;
-            Wr[((long long)z * G.Py + y) * G.Px + x] = sh[ll * C::LS + x];
+            Wr[((long long)z * G.Py + y) * G.Px + x] = sh[ll * C::LS + pidx(x)];
         }
     }
 }
@@ -217,7 +240,7 @@ k_fft_x_fwd(const cd *__restrict__ bpart, cd *__restrict__ W, const cd *__restri
 template <int P, bool INV>
 __global__ void __launch_bounds__(FftCfg<P>::THREADS)
 k_fft_y(cd *__restrict__ W, const cd *__restrict__ twg, GridDims G, const int *done) {
-    if (done && *done) return;
+    if (done && done[blockIdx.y >> 2]) return;
     using C = FftCfg<P>;
     __shared__ cd sh[C::LPB * C::LS];
     __shared__ cd tw[P];
@@ -232,14 +255,14 @@ k_fft_y(cd *__restrict__ W, const cd *__restrict__ twg, GridDims G, const int *d
         const int y = e / C::LPB, l = e - y * C::LPB, x = x0 + l;
         cd v = cmk(0, 0);
         if (y < nin && x < G.Px) v = Wr[(long long)y * G.Px + x];
-        sh[l * C::LS + y] = v;
+        sh[l * C::LS + pidx(y)] = v;
     }
     __syncthreads();
     const int l = threadIdx.x / C::TPL, t = threadIdx.x - l * C::TPL;
     fft_line<P, INV>(sh + l * C::LS, tw, t);
     for (int e = threadIdx.x; e < C::LPB * P; e += blockDim.x) {
         const int y = e / C::LPB, ll = e - y * C::LPB, x = x0 + ll;
-        if (y < nout && x < G.Px) Wr[(long long)y * G.Px + x] = sh[ll * C::LS + y];
+        if (y < nout && x < G.Px) Wr[(long long)y * G.Px + x] = sh[ll * C::LS + pidx(y)];
     }
 }
 
@@ -248,7 +271,7 @@ k_fft_y(cd *__restrict__ W, const cd *__restrict__ twg, GridDims G, const int *d
 template <int P>
 __global__ void __launch_bounds__(FftCfg<P>::THREADS)
 k_fft_z(cd *__restrict__ W, const cd *__restrict__ Fo, const cd *__restrict__ twg, GridDims G, const int *done) {
-    if (done && *done) return;
+    if (done && done[blockIdx.y >> 2]) return;
     using C = FftCfg<P>;
     __shared__ cd sh[C::LPB * C::LS];
     __shared__ cd tw[P];
@@ -262,24 +285,26 @@ k_fft_z(cd *__restrict__ W, const cd *__restrict__ Fo, const cd *__restrict__ tw
         const int z = e / C::LPB, l = e - z * C::LPB, x = x0 + l;
         cd v = cmk(0, 0);
         if (z < G.Nz && x < G.Px) v = Wr[(long long)z * plane + x];
-        sh[l * C::LS + z] = v;
+        sh[l * C::LS + pidx(z)] = v;
     }
     __syncthreads();
     const int l = threadIdx.x / C::TPL, t = threadIdx.x - l * C::TPL;
     fft_line<P, false>(sh + l * C::LS, tw, t);
     const int fy = fold(y, G.Py);
+    // consecutive threads take consecutive lines (x), so the octant reads of
+    // one z plane are contiguous
     for (int e = threadIdx.x; e < C::LPB * P; e += blockDim.x) {
-        const int ll = e / P, z = e - ll * P, x = x0 + ll;
+        const int z = e / C::LPB, ll = e - z * C::LPB, x = x0 + ll;
         if (x < G.Px) {
-            const cd f = Fo[((long long)fold(z, G.Pz) * G.Hy + fy) * G.Hx + fold(x, G.Px)];
-            sh[ll * C::LS + z] = cmul(f, sh[ll * C::LS + z]);
+            const cd f = __ldg(&Fo[((long long)fold(z, G.Pz) * G.Hy + fy) * G.Hx + fold(x, G.Px)]);
+            sh[ll * C::LS + pidx(z)] = cmul(f, sh[ll * C::LS + pidx(z)]);
         }
     }
     __syncthreads();
     fft_line<P, true>(sh + l * C::LS, tw, t);
     for (int e = threadIdx.x; e < C::LPB * P; e += blockDim.x) {
         const int z = e / C::LPB, ll = e - z * C::LPB, x = x0 + ll;
-        if (z < G.Nz && x < G.Px) Wr[(long long)z * plane + x] = sh[ll * C::LS + z];
+        if (z < G.Nz && x < G.Px) Wr[(long long)z * plane + x] = sh[ll * C::LS + pidx(z)];
     }
 }
 
@@ -288,7 +313,7 @@ k_fft_z(cd *__restrict__ W, const cd *__restrict__ Fo, const cd *__restrict__ tw
 template <int P>
 __global__ void __launch_bounds__(FftCfg<P>::THREADS)
 k_fft_x_inv(const cd *__restrict__ W, cd *__restrict__ R, const cd *__restrict__ twg, GridDims G, const int *done) {
-    if (done && *done) return;
+    if (done && done[blockIdx.y >> 2]) return;
     using C = FftCfg<P>;
     __shared__ cd sh[C::LPB * C::LS];
     __shared__ cd tw[P];
@@ -304,7 +329,7 @@ k_fft_x_inv(const cd *__restrict__ W, cd *__restrict__ R, const cd *__restrict__
             const int y = line % G.Ny, z = line / G.Ny;
             v = Wr[((long long)z * G.Py + y) * G.Px + x];
         }
-        sh[l * C::LS + x] = v;
+        sh[l * C::LS + pidx(x)] = v;
     }
     __syncthreads();
     const int l = threadIdx.x / C::TPL, t = threadIdx.x - l * C::TPL;
@@ -314,121 +339,231 @@ k_fft_x_inv(const cd *__restrict__ W, cd *__restrict__ R, const cd *__restrict__
         const int ll = e / P, x = e - ll * P, line = line0 + ll;
         if (line < nlines && x < G.Nx) {
             const int y = line % G.Ny, z = line / G.Ny;
-            Rr[((long long)z * G.Ny + y) * G.Nx + x] = sh[ll * C::LS + x];
+            Rr[((long long)z * G.Ny + y) * G.Nx + x] = sh[ll * C::LS + pidx(x)];
         }
     }
 }
 
 // ------------------------------------------------------------ near zone
-// One CTA per tile: row sums y(c1) += M x(c2) and, for off-diagonal tiles,
-// column sums y(c2) += M^T x(c1) (transpose, not conjugate: the operator is
-// complex symmetric, src/sparse_mat.f90:113-116).  Results go to per-cube
-// partial slots; k_gather adds them in a fixed order (deterministic).
+// Row sums y(c1) += M x(c2) and, for off-diagonal tiles, column sums
+// y(c2) += M^T x(c1) (transpose, not conjugate: the operator is complex
+// symmetric, src/sparse_mat.f90:113-116).  M(3i+a, 3j+b) is entry (a,b) of
+// block (i,j), stored at D[(i*n2 + j)*9 + a + 3b].  Results go to per-cube
+// partial slots that k_gather adds in a fixed order (deterministic).
+constexpr int NZ_MAXN = 64;            // tets per cube supported (two lanes' worth)
+
+// One warp per tile (4 tiles per CTA).  Tile rows stream through a
+// two-row shared-memory ring with cp.async (coalesced 8/16-byte copies): row
+// i+1 is in flight while row i is used.  Lane j takes block (i, j) from
+// shared memory and applies it to RG right-hand sides; each row sum is
+// reduced across the warp (xor tree), column j accumulates in lane j over the
+// rows in order.  The arithmetic of one right-hand side is the same for every
+// RG, so a column's result does not depend on the batch it is solved in.
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
 template <typename ST>
-__global__ void __launch_bounds__(128)
-k_near_tiles(const NearTile *__restrict__ tiles, const ST *__restrict__ data, const cd *__restrict__ x,
-             long long ld, const int *__restrict__ cube_off, cd *__restrict__ part, long long part_len,
-             const int *done) {
-    if (done && *done) return;
-    extern __shared__ cd xs_sh[];
-    const NearTile tl = tiles[blockIdx.x];
-    const int r = blockIdx.y;
-    const cd *xr = x + r * ld;
-    cd *pr = part + r * part_len;
-    const int s1 = cube_off[tl.c1], s2 = cube_off[tl.c2];
-    cd *x1 = xs_sh, *x2 = xs_sh + 3 * tl.n1;
-    for (int i = threadIdx.x; i < 3 * tl.n1; i += blockDim.x) x1[i] = xr[3LL * s1 + i];
-    for (int i = threadIdx.x; i < 3 * tl.n2; i += blockDim.x) x2[i] = xr[3LL * s2 + i];
-    __syncthreads();
-    const ST *D = data + tl.data_off * 9;
-    for (int row = threadIdx.x; row < 3 * tl.n1; row += blockDim.x) {
-        const int i = row / 3, a = row - 3 * i;
-        cd acc = cmk(0, 0);
-        const ST *Bi = D + (long long)i * tl.n2 * 9 + a;
-        for (int j = 0; j < tl.n2; ++j) {
-            const ST *b = Bi + 9 * j;
-            cfma(acc, widen(b[0]), x2[3 * j]);
-            cfma(acc, widen(b[3]), x2[3 * j + 1]);
-            cfma(acc, widen(b[6]), x2[3 * j + 2]);
-        }
-        pr[tl.row_off + row] = acc;
+__device__ __forceinline__ void copy_row_async(ST *dst, const ST *src, int nel, int lane) {
+    for (int e = lane; e < nel; e += 32) {
+        if (sizeof(ST) == 8) cp_async8(dst + e, src + e);
+        else cp_async16(dst + e, src + e);
     }
-    if (tl.col_off >= 0) {
-        for (int col = threadIdx.x; col < 3 * tl.n2; col += blockDim.x) {
-            const int j = col / 3, b = col - 3 * j;
-            cd acc = cmk(0, 0);
-            const ST *Bj = D + (long long)j * 9 + 3 * b;
-            for (int i = 0; i < tl.n1; ++i) {
-                const ST *q = Bj + (long long)i * tl.n2 * 9;
-                cfma(acc, widen(q[0]), x1[3 * i]);
-                cfma(acc, widen(q[1]), x1[3 * i + 1]);
-                cfma(acc, widen(q[2]), x1[3 * i + 2]);
+    cp_async_commit();
+}
+
+constexpr int NZ_WARPS = 4;
+
+template <typename ST, int U, int RG>
+__global__ void __launch_bounds__(32 * NZ_WARPS)
+k_near_warp(const NearTile *__restrict__ tiles, int ntiles, const ST *__restrict__ data, const cd *__restrict__ x,
+            long long ld, const int *__restrict__ cube_off, cd *__restrict__ part, long long part_len,
+            const int *skip, int nrhs, int row_cap) {
+    extern __shared__ __align__(16) unsigned char nz_sh[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t = blockIdx.x * NZ_WARPS + warp;
+    if (t >= ntiles) return;
+    ST *ring = (ST *)nz_sh + (size_t)warp * 2 * row_cap;       // two rows of this warp
+    const NearTile tl = tiles[t];
+    const int n1 = tl.n1, n2 = tl.n2;
+    const int s1 = cube_off[tl.c1], s2 = cube_off[tl.c2];
+    const ST *D = data + tl.data_off * 9;
+    const bool offd = tl.col_off >= 0;
+    const int nel = 9 * n2;
+    for (int r0 = 0; r0 < nrhs; r0 += RG) {
+        bool act[RG];
+        cd y[RG][U][3], ca[RG][U][3];
+#pragma unroll
+        for (int rr = 0; rr < RG; ++rr) {
+            const int r = r0 + rr;
+            act[rr] = r < nrhs && !(skip && skip[r]);
+            const cd *x2 = x + r * ld + 3LL * s2;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int j = lane + 32 * u;
+                ca[rr][u][0] = ca[rr][u][1] = ca[rr][u][2] = cmk(0, 0);
+                y[rr][u][0] = y[rr][u][1] = y[rr][u][2] = cmk(0, 0);
+                if (act[rr] && j < n2) { y[rr][u][0] = x2[3 * j]; y[rr][u][1] = x2[3 * j + 1]; y[rr][u][2] = x2[3 * j + 2]; }
             }
-            pr[tl.col_off + col] = acc;
+        }
+        __syncwarp();
+        copy_row_async(ring, D, nel, lane);
+        for (int i = 0; i < n1; ++i) {
+            ST *cur = ring + (size_t)(i & 1) * row_cap;
+            if (i + 1 < n1) {
+                copy_row_async(ring + (size_t)((i + 1) & 1) * row_cap, D + (size_t)(i + 1) * nel, nel, lane);
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncwarp();
+            cd m[U][9];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int j = lane + 32 * u;
+#pragma unroll
+                for (int q = 0; q < 9; ++q) m[u][q] = (j < n2) ? widen(cur[9 * j + q]) : cmk(0, 0);
+            }
+            __syncwarp();      // the ring slot may be refilled after this
+#pragma unroll
+            for (int rr = 0; rr < RG; ++rr) {
+                if (!act[rr]) continue;           // uniform across the warp
+                const cd *x1 = x + (r0 + rr) * ld + 3LL * s1;
+                const cd xa0 = x1[3 * i], xa1 = x1[3 * i + 1], xa2 = x1[3 * i + 2];
+                cd t0 = cmk(0, 0), t1 = t0, t2 = t0;
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    cfma(t0, m[u][0], y[rr][u][0]); cfma(t1, m[u][1], y[rr][u][0]); cfma(t2, m[u][2], y[rr][u][0]);
+                    cfma(t0, m[u][3], y[rr][u][1]); cfma(t1, m[u][4], y[rr][u][1]); cfma(t2, m[u][5], y[rr][u][1]);
+                    cfma(t0, m[u][6], y[rr][u][2]); cfma(t1, m[u][7], y[rr][u][2]); cfma(t2, m[u][8], y[rr][u][2]);
+                    if (offd) {
+                        cfma(ca[rr][u][0], m[u][0], xa0); cfma(ca[rr][u][0], m[u][1], xa1); cfma(ca[rr][u][0], m[u][2], xa2);
+                        cfma(ca[rr][u][1], m[u][3], xa0); cfma(ca[rr][u][1], m[u][4], xa1); cfma(ca[rr][u][1], m[u][5], xa2);
+                        cfma(ca[rr][u][2], m[u][6], xa0); cfma(ca[rr][u][2], m[u][7], xa1); cfma(ca[rr][u][2], m[u][8], xa2);
+                    }
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    t0.x += __shfl_xor_sync(0xffffffffu, t0.x, o);
+                    t0.y += __shfl_xor_sync(0xffffffffu, t0.y, o);
+                    t1.x += __shfl_xor_sync(0xffffffffu, t1.x, o);
+                    t1.y += __shfl_xor_sync(0xffffffffu, t1.y, o);
+                    t2.x += __shfl_xor_sync(0xffffffffu, t2.x, o);
+                    t2.y += __shfl_xor_sync(0xffffffffu, t2.y, o);
+                }
+                cd *pr = part + (r0 + rr) * part_len + tl.row_off + 3 * i;
+                if (lane == 0) pr[0] = t0;
+                else if (lane == 1) pr[1] = t1;
+                else if (lane == 2) pr[2] = t2;
+            }
+        }
+        if (offd) {
+#pragma unroll
+            for (int rr = 0; rr < RG; ++rr) {
+                if (!act[rr]) continue;
+                cd *pc = part + (r0 + rr) * part_len + tl.col_off;
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int j = lane + 32 * u;
+                    if (j < n2) {
+                        pc[3 * j] = ca[rr][u][0];
+                        pc[3 * j + 1] = ca[rr][u][1];
+                        pc[3 * j + 2] = ca[rr][u][2];
+                    }
+                }
+            }
         }
     }
 }
 
 // ---------------------------------------------------------------- gather
 // Interpolation (sparse_eps_matmul, src/sparse.f90:47-77) and final
-// assembly (src/gmres_module.f90:148-170), one warp per cube: lane j < 27
-// holds the four result-grid values at node j of the cube's box; per tet the
-// six 27-term dot products are reduced across the warp.  The near-zone
-// partial slots of the cube are added in slot order.
-__global__ void k_gather(const cd *__restrict__ Rg, const cd *__restrict__ P, int T,
-                         const int *__restrict__ cube_off, GridDims G, double k2,
-                         const cd *__restrict__ part, long long part_len,
-                         const long long *__restrict__ pslot_base, const int *__restrict__ pslot_cnt,
-                         cd *__restrict__ y, long long ld, const int *done) {
-    if (done && *done) return;
+// assembly (src/gmres_module.f90:148-170), one warp per cube, one lane per
+// tet: the 27 box-node values of the four result grids are staged in shared
+// memory for a group of right-hand sides, each lane forms its tet's six
+// 27-term sums from the projector rows P[(g*27 + j)*T + slot] (coalesced
+// across lanes), adds the cube's near-zone partial slots in slot order and
+// writes Ax = near + (Y2 - k^2 Y).
+template <int GA_RG>
+__global__ void __launch_bounds__(32 * WARPS_PER_CTA)
+k_gather(const cd *__restrict__ Rg, const cd *__restrict__ P, int T, const int *__restrict__ cube_off, GridDims G,
+         double k2, const cd *__restrict__ part, long long part_len, const long long *__restrict__ pslot_base,
+         const int *__restrict__ pslot_cnt, cd *__restrict__ y, long long ld, const int *skip, int nrhs) {
+    __shared__ cd Rs[WARPS_PER_CTA][GA_RG][4][27];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c = blockIdx.x * WARPS_PER_CTA + warp;
-    const int r = blockIdx.y;
     if (c >= G.ncubes) return;
     const int s0 = cube_off[c], s1 = cube_off[c + 1];
     if (s0 == s1) return;
+    const int nc = s1 - s0;
     const int bx = c % G.ncx, by = (c / G.ncx) % G.ncy, bz = c / (G.ncx * G.ncy);
     const long long NN = (long long)G.Nx * G.Ny * G.Nz;
-    const cd *Rr = Rg + (long long)r * 4 * NN;
-    cd R0 = cmk(0, 0), R1 = R0, R2 = R0, R3 = R0;
+    const long long pbase = pslot_base[c];
+    const int nslot = pslot_cnt[c];
+    long long node = 0;
     if (lane < 27) {
         const int a = lane % 3, b = (lane / 3) % 3, cc = lane / 9;
-        const long long node = ((long long)(2 * bz + cc) * G.Ny + (2 * by + b)) * G.Nx + (2 * bx + a);
-        R0 = Rr[node];
-        R1 = Rr[NN + node];
-        R2 = Rr[2 * NN + node];
-        R3 = Rr[3 * NN + node];
+        node = ((long long)(2 * bz + cc) * G.Ny + (2 * by + b)) * G.Nx + (2 * bx + a);
     }
-    const long long TT = 27LL * T;
-    const int nc = s1 - s0;
-    const cd *pr = part + r * part_len + pslot_base[c];
-    const int nslot = pslot_cnt[c];
-    cd *yr = y + r * ld;
-    for (int s = s0; s < s1; ++s) {
-        double v[12];
+    for (int r0 = 0; r0 < nrhs; r0 += GA_RG) {
+        __syncwarp();
         if (lane < 27) {
-            const long long o = 27LL * s + lane;
-            const cd p0 = P[o], px = P[TT + o], py = P[2 * TT + o], pz = P[3 * TT + o];
-            const cd t0 = cmul(p0, R0), t1 = cmul(p0, R1), t2 = cmul(p0, R2);
-            const cd u0 = cmul(px, R3), u1 = cmul(py, R3), u2 = cmul(pz, R3);
-            v[0] = t0.x; v[1] = t0.y; v[2] = t1.x; v[3] = t1.y; v[4] = t2.x; v[5] = t2.y;
-            v[6] = u0.x; v[7] = u0.y; v[8] = u1.x; v[9] = u1.y; v[10] = u2.x; v[11] = u2.y;
-        } else {
 #pragma unroll
-            for (int q = 0; q < 12; ++q) v[q] = 0.0;
+            for (int q = 0; q < GA_RG; ++q) {
+                const int r = r0 + q;
+                if (r < nrhs) {
+                    const cd *Rr = Rg + (long long)r * 4 * NN;
+#pragma unroll
+                    for (int g = 0; g < 4; ++g) Rs[warp][q][g][lane] = Rr[g * NN + node];
+                }
+            }
         }
+        __syncwarp();
+        for (int sl = lane; sl < nc; sl += 32) {
+            const int s = s0 + sl;
+            cd acc[GA_RG][6];
 #pragma unroll
-        for (int q = 0; q < 12; ++q) {
+            for (int q = 0; q < GA_RG; ++q)
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
-        }
-        if (lane < 3) {
-            const int d = lane;
-            cd far = cmk(v[6 + 2 * d] - k2 * v[2 * d], v[7 + 2 * d] - k2 * v[2 * d + 1]);
-            cd nz = cmk(0, 0);
-            const int li = 3 * (s - s0) + d;
-            for (int q = 0; q < nslot; ++q) nz = cadd(nz, pr[(long long)q * 3 * nc + li]);
-            yr[3LL * s + d] = cadd(nz, far);
+                for (int v = 0; v < 6; ++v) acc[q][v] = cmk(0, 0);
+#pragma unroll 3
+            for (int j = 0; j < 27; ++j) {
+                const cd p0 = P[(size_t)j * T + s], px = P[(size_t)(27 + j) * T + s];
+                const cd py = P[(size_t)(54 + j) * T + s], pz = P[(size_t)(81 + j) * T + s];
+#pragma unroll
+                for (int q = 0; q < GA_RG; ++q) {
+                    cfma(acc[q][0], p0, Rs[warp][q][0][j]);
+                    cfma(acc[q][1], p0, Rs[warp][q][1][j]);
+                    cfma(acc[q][2], p0, Rs[warp][q][2][j]);
+                    const cd r3 = Rs[warp][q][3][j];
+                    cfma(acc[q][3], px, r3);
+                    cfma(acc[q][4], py, r3);
+                    cfma(acc[q][5], pz, r3);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < GA_RG; ++q) {
+                const int r = r0 + q;
+                if (r >= nrhs || (skip && skip[r])) continue;
+                const cd *pr = part + r * part_len + pbase + 3 * sl;
+                cd *yr = y + r * ld + 3LL * s;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    cd nz = cmk(0, 0);
+#pragma unroll 8
+                    for (int t = 0; t < nslot; ++t) nz = cadd(nz, pr[(long long)t * 3 * nc + d]);
+                    const cd far = csub_scaled(acc[q][3 + d], k2, acc[q][d]);
+                    yr[d] = cadd(nz, far);
+                }
+            }
         }
     }
 }
@@ -515,9 +650,16 @@ void launch_permute_out(scd_ctx *c, const cd *x_slot, cd *x_orig, int nrhs, long
 void launch_fft_chain(scd_ctx *c, const cd *x, int nrhs, const int *done) {
     const GridDims G = dims_of(c);
     {
-        dim3 grid((c->ncubes + WARPS_PER_CTA - 1) / WARPS_PER_CTA, nrhs);
-        k_scatter<<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(x, c->n, c->d_P, c->T, c->d_cube_off, c->ncubes,
-                                                          c->d_bpart, done);
+        dim3 grid((c->ncubes + WARPS_PER_CTA - 1) / WARPS_PER_CTA);
+        if (nrhs >= 8)
+            k_scatter<8><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(x, c->n, c->d_P, c->T, c->d_cube_off, c->ncubes,
+                                                                 c->d_bpart, done, nrhs);
+        else if (nrhs >= 4)
+            k_scatter<4><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(x, c->n, c->d_P, c->T, c->d_cube_off, c->ncubes,
+                                                                 c->d_bpart, done, nrhs);
+        else
+            k_scatter<1><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(x, c->n, c->d_P, c->T, c->d_cube_off, c->ncubes,
+                                                                 c->d_bpart, done, nrhs);
     }
     const int nrg = 4 * nrhs;
 #define XF(P) fft_x_fwd_t<P>(c, G, nrg, done, c->d_tw[0])
@@ -538,26 +680,51 @@ void launch_fft_chain(scd_ctx *c, const cd *x, int nrhs, const int *done) {
     c->launches += 6;
 }
 
+template <typename ST, int U>
+static void near_dispatch_u(scd_ctx *c, const ST *data, const cd *x, int nrhs, const int *done) {
+    const int row_cap = 9 * c->max_per_cube;
+    const size_t sh = sizeof(ST) * 2 * (size_t)row_cap * NZ_WARPS;
+    const int grid = (c->ntiles + NZ_WARPS - 1) / NZ_WARPS;
+    if (nrhs >= 4) {
+        cudaFuncSetAttribute(k_near_warp<ST, U, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+        k_near_warp<ST, U, 4><<<grid, 32 * NZ_WARPS, sh, c->st>>>(c->d_tiles, c->ntiles, data, x, c->n, c->d_cube_off,
+                                                                 c->d_nzpart, c->part_len, done, nrhs, row_cap);
+    } else if (nrhs >= 2) {
+        cudaFuncSetAttribute(k_near_warp<ST, U, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+        k_near_warp<ST, U, 2><<<grid, 32 * NZ_WARPS, sh, c->st>>>(c->d_tiles, c->ntiles, data, x, c->n, c->d_cube_off,
+                                                                 c->d_nzpart, c->part_len, done, nrhs, row_cap);
+    } else {
+        cudaFuncSetAttribute(k_near_warp<ST, U, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+        k_near_warp<ST, U, 1><<<grid, 32 * NZ_WARPS, sh, c->st>>>(c->d_tiles, c->ntiles, data, x, c->n, c->d_cube_off,
+                                                                 c->d_nzpart, c->part_len, done, nrhs, row_cap);
+    }
+}
+
+template <typename ST>
+static void near_dispatch(scd_ctx *c, const ST *data, const cd *x, int nrhs, const int *done) {
+    if (c->max_per_cube <= 32) near_dispatch_u<ST, 1>(c, data, x, nrhs, done);
+    else near_dispatch_u<ST, 2>(c, data, x, nrhs, done);
+}
+
 void launch_near(scd_ctx *c, const cd *x, int nrhs, const int *done) {
     if (c->ntiles == 0) return;
-    dim3 grid(c->ntiles, nrhs);
-    size_t sh = sizeof(cd) * 6 * (size_t)c->max_per_cube;
-    if (c->near_prec == SCD_STORE_C64)
-        k_near_tiles<cf><<<grid, 128, sh, c->st>>>(c->d_tiles, (const cf *)c->d_tdata, x, c->n, c->d_cube_off,
-                                                   c->d_nzpart, c->part_len, done);
-    else
-        k_near_tiles<cd><<<grid, 128, sh, c->st>>>(c->d_tiles, (const cd *)c->d_tdata, x, c->n, c->d_cube_off,
-                                                   c->d_nzpart, c->part_len, done);
+    if (c->near_prec == SCD_STORE_C64) near_dispatch(c, (const cf *)c->d_tdata, x, nrhs, done);
+    else near_dispatch(c, (const cd *)c->d_tdata, x, nrhs, done);
     c->launches += 1;
 }
 
 void launch_gather(scd_ctx *c, const cd *x, cd *y, int nrhs, const int *done) {
     (void)x;
     const GridDims G = dims_of(c);
-    dim3 grid((c->ncubes + WARPS_PER_CTA - 1) / WARPS_PER_CTA, nrhs);
-    k_gather<<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(c->d_R, c->d_P, c->T, c->d_cube_off, G, c->k * c->k,
-                                                     c->d_nzpart, c->part_len, c->d_pslot_base, c->d_pslot_cnt,
-                                                     y, c->n, done);
+    dim3 grid((c->ncubes + WARPS_PER_CTA - 1) / WARPS_PER_CTA);
+    if (nrhs >= 4)
+        k_gather<4><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(c->d_R, c->d_P, c->T, c->d_cube_off, G, c->k * c->k,
+                                                            c->d_nzpart, c->part_len, c->d_pslot_base, c->d_pslot_cnt,
+                                                            y, c->n, done, nrhs);
+    else
+        k_gather<1><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(c->d_R, c->d_P, c->T, c->d_cube_off, G, c->k * c->k,
+                                                            c->d_nzpart, c->part_len, c->d_pslot_base, c->d_pslot_cnt,
+                                                            y, c->n, done, nrhs);
     c->launches += 1;
 }
 

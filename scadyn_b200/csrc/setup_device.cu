@@ -243,15 +243,15 @@ struct TetGeo {
 };
 
 __device__ void near_block(const TetGeo &T, const TetGeo &B, bool self, cd eps_t, double k,
-                           const cd *St, const cd *Sxt, const cd *Syt, const cd *Szt,
+                           const cd *St, const cd *Sxt, const cd *Syt, const cd *Szt, long long ps,
                            const cd *gs, const cd *gx, const cd *gy, const cd *gz, cd out[9]) {
     // precorrection (linear in S; computed from G times basis projectors)
     cd acorr = cmk(0, 0);
     cd corr2[9];
     for (int q = 0; q < 9; ++q) corr2[q] = cmk(0, 0);
     for (int a = 0; a < 27; ++a) {
-        cfma(acorr, gs[a], St[a]);
-        const cd pt[3] = {Sxt[a], Syt[a], Szt[a]};
+        cfma(acorr, gs[a], St[a * ps]);
+        const cd pt[3] = {Sxt[a * ps], Syt[a * ps], Szt[a * ps]};
         const cd gb[3] = {gx[a], gy[a], gz[a]};
 #pragma unroll
         for (int r = 0; r < 3; ++r)
@@ -418,18 +418,18 @@ __global__ void __launch_bounds__(NEAR_THREADS) k_near_build(NearArgs a) {
     // GP2[j][g][row i of c1-box] = sum_q G[i][q] P_g(q, tet j of c2)   (test in c1, basis in c2)
     for (int e = threadIdx.x; e < tl.n2 * 108; e += blockDim.x) {
         const int j = e / 108, g = (e / 27) % 4, i = e % 27;
-        const cd *p = a.P + g * TT + 27LL * (s2 + j);
+        const cd *p = a.P + (size_t)g * TT + (s2 + j);
         cd acc = cmk(0, 0);
-        for (int q = 0; q < 27; ++q) cfma(acc, G[i * 27 + q], p[q]);
+        for (int q = 0; q < 27; ++q) cfma(acc, G[i * 27 + q], p[(size_t)q * a.T]);
         GP2[e] = acc;
     }
     // GP1[i][g][row q of c2-box] = sum_p G[p][q] P_g(p, tet i of c1)   (test in c2, basis in c1)
     if (tl.c1 != tl.c2) {
         for (int e = threadIdx.x; e < tl.n1 * 108; e += blockDim.x) {
             const int i = e / 108, g = (e / 27) % 4, q = e % 27;
-            const cd *p = a.P + g * TT + 27LL * (s1 + i);
+            const cd *p = a.P + (size_t)g * TT + (s1 + i);
             cd acc = cmk(0, 0);
-            for (int pp = 0; pp < 27; ++pp) cfma(acc, G[pp * 27 + q], p[pp]);
+            for (int pp = 0; pp < 27; ++pp) cfma(acc, G[pp * 27 + q], p[(size_t)pp * a.T]);
             GP1[e] = acc;
         }
     }
@@ -447,8 +447,8 @@ __global__ void __launch_bounds__(NEAR_THREADS) k_near_build(NearArgs a) {
         load_tet(a, st, Tt);
         load_tet(a, sbas, Bt);
         cd blk[9];
-        near_block(Tt, Bt, st == sbas, a.eps[st], a.k, a.P + 27LL * st, a.P + TT + 27LL * st,
-                   a.P + 2 * TT + 27LL * st, a.P + 3 * TT + 27LL * st, gp, gp + 27, gp + 54, gp + 81, blk);
+        near_block(Tt, Bt, st == sbas, a.eps[st], a.k, a.P + st, a.P + TT + st, a.P + 2 * TT + st, a.P + 3 * TT + st,
+                   a.T, gp, gp + 27, gp + 54, gp + 81, blk);
         store_block(a, tl.data_off + (long long)i * tl.n2 + j, blk, !fwd);
         if (diag && i != j) store_block(a, tl.data_off + (long long)j * tl.n2 + i, blk, true);
     }
@@ -511,7 +511,7 @@ __global__ void k_projectors(const double *tc, const double *vol, const int *cub
         }
         const double sv = sqrt(vb);
         const long long TT = 27LL * T;
-        for (int g = 0; g < 4; ++g) P[g * TT + 27LL * s + lane] = cmk(acc[g].x / sv, acc[g].y / sv);
+        for (int g = 0; g < 4; ++g) P[(size_t)(g * 27 + lane) * T + s] = cmk(acc[g].x / sv, acc[g].y / sv);
     }
 }
 
@@ -815,6 +815,9 @@ int setup_nearzone_device(scd_ctx *c, int prec) {
     if (rc) return rc;
     c->have_near = false;
     c->near_prec = prec;
+    if (c->max_per_cube > SCD_NEAR_MAXN)
+        return set_error(c, SCD_BAD_ARG, "%d tets in one projection box; the near-zone kernels support %d",
+                         c->max_per_cube, SCD_NEAR_MAXN);
     if ((rc = build_tile_layout(c))) return rc;
     const size_t esz = prec == SCD_STORE_C64 ? sizeof(cf) : sizeof(cd);
     if (c->d_tdata) { cudaFree(c->d_tdata); c->d_tdata = nullptr; }
@@ -957,7 +960,7 @@ int scd_get_projectors(scd_ctx *c, scd_c128 *S, scd_c128 *Sx, scd_c128 *Sy, scd_
         for (int j = 0; j < 27; ++j) {
             for (int g = 0; g < 4; ++g)
                 if (dst[g]) {
-                    const cd v = h[g * TT + 27LL * s + j];
+                    const cd v = h[(size_t)(g * 27 + j) * c->T + s];
                     dst[g][27LL * t + j] = scd_c128{v.x, v.y};
                 }
             if (indS) {

@@ -98,3 +98,29 @@ def test_solve_columns_T_matches_oracle(small_op, dev_small, small_sphere):
     Tr = O.T_assemble(mat, Xr)
     assert rel(Tc, Tr) < 1e-9
     assert rel(X, Xr) < 1e-9
+
+
+def test_batched_columns_bitwise_equal_single(small_op, dev_small, small_sphere):
+    """Slots solved together give the same bits as one column at a time and
+    as scd_gmres (per-column arithmetic does not depend on the batch)."""
+    mat = O.vswf2constant(small_sphere.coord, small_sphere.etopol, small_op.geom.k, 2)
+    T1, it1, X1, _ = dev_small.solve_columns(mat, tol=1e-8, block=1, want_x=True)
+    T4, it4, X4, _ = dev_small.solve_columns(mat, tol=1e-8, block=4, want_x=True)
+    T16, it16, X16, _ = dev_small.solve_columns(mat, tol=1e-8, block=16, want_x=True)
+    assert np.array_equal(it1, it4) and np.array_equal(it1, it16)
+    assert np.array_equal(X1, X4) and np.array_equal(X1, X16)
+    assert np.array_equal(T1, T4) and np.array_equal(T1, T16)
+    for c in (0, 7):
+        x, info = dev_small.gmres(mat[c], tol=1e-8, m=50, cycles=4)
+        assert info["iters"] == it1[c]
+        assert np.array_equal(x, X1[c])
+
+
+def test_batched_restarts_match_oracle(small_op, dev_small, small_sphere):
+    """Small Krylov dimension: slots restart at different ticks."""
+    mat = O.vswf2constant(small_sphere.coord, small_sphere.etopol, small_op.geom.k, 1)
+    Tc, it, X, rc = dev_small.solve_columns(mat, tol=1e-9, m=3, cycles=8, block=6, want_x=True)
+    for c in range(mat.shape[0]):
+        xr, info = small_op.gmres(mat[c], tol=1e-9, m=3, cycles=8)
+        assert it[c] == info["iters"]
+        assert rel(X[c], xr) < 1e-9
