@@ -182,6 +182,20 @@ SCD_API int scd_get_timing(scd_ctx *ctx, scd_timing *t, int32_t reset);
  * nearzone_ms, fft_ms, gather_ms). */
 SCD_API int scd_profile_matvec(scd_ctx *ctx, int32_t reps, int32_t nrhs);
 
+/* T = mat^H X without allocating: mat (n, ncol), X (n, ncb) and T (ncol, ncb)
+ * are DEVICE pointers owned by the caller; the kernels run on `stream`
+ * (a cudaStream_t, NULL = the legacy default stream) and the call returns
+ * after launching them.  No counterpart in the reference: it is for callers
+ * that cannot let a library call cudaMalloc (device memory owned by the
+ * host's own allocator; column loops recorded into CUDA graphs).  Scratch
+ * is a fixed 4 MiB per-device array, so ncol*ncb must not exceed 262144
+ * (SCD_BAD_ARG otherwise).  The first call on a device looks up that array's
+ * device address; make it before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU race and must be ordered by the
+ * caller (one stream, or events). */
+SCD_API int scd_T_assemble_noalloc(const scd_c128 *mat, int64_t n, int32_t ncol, const scd_c128 *X, int32_t ncb,
+                                   scd_c128 *T, void *stream);
+
 /* Per-column solve latency (admission to completion, milliseconds on the
  * host clock, each tick ending in a stream synchronisation) of the last
  * scd_solve_columns / scd_compute_T_matrix call; ncol must match it. */

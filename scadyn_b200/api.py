@@ -37,7 +37,7 @@ EXPORTS = [
     "scd_build_projectors", "scd_build_nearzone", "scd_get_projectors", "scd_nearzone_count",
     "scd_get_nearzone", "scd_matvec", "scd_gmres", "scd_solve_columns", "scd_vswf_rhs",
     "scd_get_timing", "scd_compute_T_matrix", "scd_profile_matvec", "scd_nearzone_bytes",
-    "scd_column_latency",
+    "scd_column_latency", "scd_T_assemble_noalloc",
 ]
 
 
@@ -101,6 +101,7 @@ def load_library(path: str = LIB_PATH):
         "scd_profile_matvec": ([vp, i32, i32], C.c_int),
         "scd_nearzone_bytes": ([vp], C.c_int64),
         "scd_column_latency": ([vp, i32, vp], C.c_int),
+        "scd_T_assemble_noalloc": ([vp, i64, i32, vp, i32, vp, vp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -128,6 +129,16 @@ def grid_from_mesh(coord, etopol, grid_size=1.8, M_ex=2) -> GridDesc:
     if rc:
         raise ScadynError(rc, "scd_grid_from_mesh")
     return d
+
+
+def T_assemble_noalloc(mat_ptr, n, ncol, X_ptr, ncb, T_ptr, stream=0):
+    """T = mat^H X on caller-owned device buffers, allocating nothing
+    (scd_T_assemble_noalloc).  Pointers are device addresses (ints)."""
+    lib = load_library()
+    rc = lib.scd_T_assemble_noalloc(C.c_void_p(mat_ptr), n, ncol, C.c_void_p(X_ptr), ncb, C.c_void_p(T_ptr),
+                                    C.c_void_p(stream))
+    if rc:
+        raise ScadynError(rc, "scd_T_assemble_noalloc")
 
 
 @dataclass

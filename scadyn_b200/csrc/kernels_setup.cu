@@ -3,6 +3,7 @@
 // T(:, c) = mat^H x_c (src/T_matrix.f90:260).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "ctx.h"
@@ -145,4 +146,47 @@ void launch_T_assemble(scd_ctx *c, const cd *d_mat, int ncol, int col0, int ncb,
     c->launches += 2;
 }
 
-// device-side operator construction: filled in by setup_device.cu
+
+// ------------------------------------------------------------ no allocation
+// scd_T_assemble_noalloc: the same split-K assembly T = mat^H X for callers
+// that must not allocate device memory -- e.g. a Fortran host whose device
+// arrays all come from its own allocator (CUDA Fortran `device` arrays,
+// OpenACC data regions) and which may record the column loop into a CUDA
+// graph, where a cudaMalloc inside the library would break the capture or
+// synchronise the device.  The split-K partial sums live in this fixed
+// file-scope array instead of a cudaMallocAsync buffer.
+#define SCD_NOALLOC_SCRATCH (1 << 18)   // complex doubles: 4 MiB per device
+static __device__ __align__(256) cd g_noalloc_scratch[SCD_NOALLOC_SCRATCH];
+
+// device address of g_noalloc_scratch per device; the symbol name in host
+// code is only a host-side stand-in, so the address is looked up once per
+// device with that device current (first call on the device)
+static cd *g_noalloc_ptr[128] = {nullptr};
+
+extern "C" SCD_API int scd_T_assemble_noalloc(const scd_c128 *mat, int64_t n, int32_t ncol, const scd_c128 *X,
+                                              int32_t ncb, scd_c128 *T, void *stream) {
+    if (!mat || !X || !T || n < 1 || ncol < 1 || ncb < 1) return SCD_BAD_ARG;
+    if ((int64_t)ncol * ncb > SCD_NOALLOC_SCRATCH) return SCD_BAD_ARG;   // one split must fit the scratch
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return SCD_NO_DEVICE;
+    if (!g_noalloc_ptr[dev]) {
+        cd *p = nullptr;
+        if (cudaGetSymbolAddress((void **)&p, g_noalloc_scratch) != cudaSuccess || !p) {
+            cudaGetLastError();
+            return SCD_CUDA_ERROR;
+        }
+        g_noalloc_ptr[dev] = p;
+    }
+    cd *part = g_noalloc_ptr[dev];
+    cudaStream_t st = (cudaStream_t)stream;
+    // as many K splits as the scratch holds (at most 64); every partial entry
+    // is written before it is read, so nothing needs clearing between calls
+    long long maxsplit = SCD_NOALLOC_SCRATCH / ((long long)ncol * ncb);
+    int nsplit = (int)std::min<long long>(std::min<long long>(64, maxsplit), std::max<long long>(1, n / 4096));
+    const long long kchunk = ((n + nsplit - 1) / nsplit + TB - 1) / TB * TB;
+    nsplit = (int)((n + kchunk - 1) / kchunk);
+    dim3 grid(nsplit, (ncol + TB - 1) / TB, (ncb + TB - 1) / TB);
+    k_tgemm_partial<<<grid, dim3(TB, TB), 0, st>>>((const cd *)mat, n, ncol, (const cd *)X, ncb, kchunk, part);
+    k_tgemm_reduce<<<(ncol * ncb + 255) / 256, 256, 0, st>>>(part, nsplit, ncol, ncb, (cd *)T, 0);
+    return cudaGetLastError() == cudaSuccess ? SCD_OK : SCD_CUDA_ERROR;
+}
