@@ -173,6 +173,7 @@ static int upload_layout(scd_ctx *c, std::vector<NearTile> &tiles, long long off
     c->part_len = c->pslot_base[c->ncubes];
     c->tiles_h.swap(tiles);
     c->nrhs_cap = 0;   // partial buffer size changed
+    c->f_cap = 0;
     return SCD_OK;
 }
 
@@ -317,7 +318,8 @@ int scd_destroy(scd_ctx *c) {
     void *ptrs[] = {c->d_perm, c->d_cube_off, c->d_P, c->d_Fo, c->d_tdata, c->d_tiles, c->d_pslot_base,
                     c->d_pslot_cnt, c->d_tc, c->d_tvol, c->d_eps, c->d_bpart, c->d_W, c->d_R, c->d_nzpart, c->d_x,
                     c->d_y, c->d_io, c->d_V, c->d_H, c->d_cs, c->d_sn, c->d_g, c->d_rhs, c->d_w, c->d_red,
-                    c->d_bar, c->d_err, c->d_state, c->d_tw[0], c->d_tw[1], c->d_tw[2]};
+                    c->d_bar, c->d_err, c->d_state, c->d_tw[0], c->d_tw[1], c->d_tw[2], c->f_P, c->f_Fo,
+                    c->f_tw[0], c->f_tw[1], c->f_tw[2], c->f_bpart, c->f_W, c->f_R, c->f_nzpart};
     for (void *p : ptrs) if (p) cudaFree(p);
     if (c->h_state) cudaFreeHost(c->h_state);
     batch_free(c);
@@ -347,6 +349,7 @@ int scd_set_green(scd_ctx *c, const scd_c128 *Fg) {
                          2 * c->Nx, 2 * c->Ny, 2 * c->Nz);
     int rc = setup_green(c, Fg);
     if (rc == SCD_OK) c->have_green = true;
+    c->f_ready = false;
     return rc;
 }
 
@@ -385,6 +388,7 @@ int scd_set_projectors(scd_ctx *c, int32_t M_box, int32_t T, const scd_c128 *S, 
     if ((rc = dalloc(c, &c->d_P, h.size(), "projectors"))) return rc;
     CK(cudaMemcpy(c->d_P, h.data(), sizeof(cd) * h.size(), cudaMemcpyHostToDevice), "projectors");
     c->have_proj = true;
+    c->f_ready = false;
     return SCD_OK;
 }
 
@@ -400,6 +404,7 @@ int scd_set_nearzone(scd_ctx *c, int64_t B, const void *sp_mat, const int32_t *s
     int rc;
     c->have_near = false;
     c->near_prec = prec;
+    c->f_cap = 0;
     if (prec == SCD_STORE_C64) rc = build_tiles<cf>(c, B, (const cf *)sp_mat, sp_ind);
     else rc = build_tiles<cd>(c, B, (const cd *)sp_mat, sp_ind);
     if (rc == SCD_OK) c->have_near = true;
@@ -479,7 +484,8 @@ int scd_solve_columns(scd_ctx *c, int32_t ncol, const scd_c128 *mat, scd_c128 *T
     for (int j = 0; j < ncol; ++j) cols[j] = d_mat + (size_t)n * j;
     const int ns = o->block > 0 ? o->block : ncol;
     std::vector<int> it(ncol, 0);
-    int worst = batch_solve(c, ncol, cols.data(), d_X, o->tol, o->m, o->cycles, ns, it.data(), nullptr, nullptr);
+    int worst = batch_solve(c, ncol, cols.data(), d_X, o->tol, o->m, o->cycles, ns, it.data(), nullptr, nullptr,
+                            o->precision, o->inner_tol, o->max_outer);
     if (iters) for (int j = 0; j < ncol; ++j) iters[j] = it[j];
     if (worst == SCD_OK || worst == SCD_NOT_CONVERGED) {
         launch_T_assemble(c, d_mat, ncol, 0, ncol, d_X, d_T);
@@ -598,7 +604,8 @@ int scd_compute_T_matrix(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int3
     for (int j = 0; j < ncol; ++j) cols[j] = c->d_mat + (size_t)n * (col0 + j);
     const int ns = o->block > 0 ? o->block : ncol;
     std::vector<int> it(ncol, 0);
-    int worst = batch_solve(c, ncol, cols.data(), d_X, o->tol, o->m, o->cycles, ns, it.data(), nullptr, nullptr);
+    int worst = batch_solve(c, ncol, cols.data(), d_X, o->tol, o->m, o->cycles, ns, it.data(), nullptr, nullptr,
+                            o->precision, o->inner_tol, o->max_outer);
     if (iters) for (int j = 0; j < ncol; ++j) iters[j] = it[j];
     if (worst == SCD_OK || worst == SCD_NOT_CONVERGED) {
         launch_T_assemble(c, c->d_mat, ntot, 0, ncol, d_X, d_T);

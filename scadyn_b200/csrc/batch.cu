@@ -24,35 +24,53 @@ namespace {
 constexpr int BT = 256;             // threads per CTA of the tick kernel
 constexpr int NSMAX = 64;           // slot limit (partial buffer sizing)
 
-enum { SLOT_FREE = 0, SLOT_START = 1, SLOT_ARNOLDI = 2, SLOT_DONE = 3 };
+enum { SLOT_FREE = 0, SLOT_START = 1, SLOT_ARNOLDI = 2, SLOT_DONE = 3, SLOT_RESID = 4, SLOT_INNER_DONE = 5 };
 
+// One column in flight.  Plain form: START/ARNOLDI until DONE.  Mixed form:
+// RESID (FP64 residual of the FP64 iterate) -> inner complex64 GMRES on the
+// normalised residual (START/ARNOLDI, zero initial guess) -> INNER_DONE
+// (x += rho d) -> RESID ... until the FP64 residual meets the tolerance.
 struct Slot {
-    int mode, col, cycle, step, iters, conv, status, reorth, finish, pad;
+    int mode, col, cycle, step, iters, conv, status, reorth, finish, zero_x;
+    int outer, upd;    // mixed: outer steps taken; x += rho d pending
     double b_norm, beta, error;
+    double rho;        // mixed: ||r|| of the residual the inner solve corrects
+    double b64;        // mixed: ||rhs|| in FP64
+    double relres;     // mixed: last FP64 relative residual
 };
 
+template <typename C>
 struct TickArgs {
     Slot *slots;
     int ns;
-    cd *V;          // [slot][m+1][n]
+    C *V;           // [slot][m+1][n]
     cd *H;          // [slot][(m+1) m]
     cd *cs, *sn, *g, *y;   // [slot][m+1]
-    cd *x, *rhs, *w;       // [slot][n]
+    C *x, *rhs, *w; // [slot][n]
     double *red;    // [2][grid][NSMAX*4]
     GridBarrier *bar;
     int *err;
     long long n;
     int m, max_cycles;
     double tol;
+    int mixed;      // inner solve of the mixed form: finish -> INNER_DONE
 };
 
-__device__ __forceinline__ double *partial_slot(const TickArgs &a, int parity, int s) {
+// vector elements in FP64 for arithmetic, rounded back on store
+__device__ __forceinline__ cd to_cd(cd a) { return a; }
+__device__ __forceinline__ cd to_cd(cf a) { return widen(a); }
+__device__ __forceinline__ void store_c(cd &d, cd v) { d = v; }
+__device__ __forceinline__ void store_c(cf &d, cd v) { d = make_float2((float)v.x, (float)v.y); }
+
+template <typename C>
+__device__ __forceinline__ double *partial_slot(const TickArgs<C> &a, int parity, int s) {
     return a.red + ((size_t)parity * gridDim.x + blockIdx.x) * (NSMAX * 4) + s * 4;
 }
 
 // totals of the per-CTA partials of every slot: warp w reduces slots w,
 // w + nwarps, ...; lanes stride over CTAs; fixed order, deterministic
-__device__ void read_totals(const TickArgs &a, int parity, int nv, double (*tot)[4]) {
+template <typename C>
+__device__ void read_totals(const TickArgs<C> &a, int parity, int nv, double (*tot)[4]) {
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for (int s = wp; s < a.ns; s += nw) {
         double acc[4] = {0, 0, 0, 0};
@@ -70,7 +88,8 @@ __device__ void read_totals(const TickArgs &a, int parity, int nv, double (*tot)
     __syncthreads();
 }
 
-__device__ __forceinline__ void put_partial(const TickArgs &a, int parity, int s, const double *v, int nv) {
+template <typename C>
+__device__ __forceinline__ void put_partial(const TickArgs<C> &a, int parity, int s, const double *v, int nv) {
     if (threadIdx.x == 0) {
         double *p = partial_slot(a, parity, s);
         for (int q = 0; q < nv; ++q) p[q] = v[q];
@@ -79,10 +98,11 @@ __device__ __forceinline__ void put_partial(const TickArgs &a, int parity, int s
 
 // One tick: cycle starts (r = rhs - A x, V0 = r/||r||) and Arnoldi steps
 // (MGS, normalisation, Givens) for every active slot; cycle ends update x.
-__global__ void __launch_bounds__(BT) k_tick(TickArgs a) {
+template <typename C>
+__global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
     __shared__ double bsh[64];
     __shared__ double tot[NSMAX][4];
-    __shared__ int smode[NSMAX], sstep[NSMAX];
+    __shared__ int smode[NSMAX], sstep[NSMAX], szero[NSMAX];
     __shared__ double snormav[NSMAX], shn[NSMAX];
     __shared__ cd sh_h[NSMAX];
     __shared__ cd ysm[64];
@@ -93,6 +113,7 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs a) {
     for (int s = threadIdx.x; s < a.ns; s += blockDim.x) {
         smode[s] = a.slots[s].mode;
         sstep[s] = a.slots[s].step;
+        szero[s] = a.slots[s].zero_x;
     }
     __syncthreads();
     int parity = 0;
@@ -100,20 +121,21 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs a) {
     for (int s = 0; s < a.ns; ++s) {
         const int md = smode[s];
         double v[3] = {0, 0, 0};
-        const cd *ws = a.w + (size_t)s * n;
-        cd *V0 = a.V + (size_t)s * (a.m + 1) * n;
+        const C *ws = a.w + (size_t)s * n;
+        C *V0 = a.V + (size_t)s * (a.m + 1) * n;
         if (md == SLOT_START) {
-            const cd *bs = a.rhs + (size_t)s * n;
+            const C *bs = a.rhs + (size_t)s * n;
+            const bool zx = szero[s] != 0;
             for (long long q = q0; q < n; q += stride) {
-                const cd b = bs[q];
-                const cd r = csub(b, ws[q]);
-                V0[q] = r;
+                const cd b = to_cd(bs[q]);
+                const cd r = zx ? b : csub(b, to_cd(ws[q]));
+                store_c(V0[q], r);
                 v[0] += cabs2(r);
                 v[1] += cabs2(b);
             }
         } else if (md == SLOT_ARNOLDI) {
             for (long long q = q0; q < n; q += stride) {
-                const cd w = ws[q], z = V0[q];
+                const cd w = to_cd(ws[q]), z = to_cd(V0[q]);
                 v[0] += cabs2(w);
                 cdot_acc(v[1], v[2], z, w);
             }
@@ -138,10 +160,10 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs a) {
     for (int s = 0; s < a.ns; ++s) {
         if (smode[s] != SLOT_START) continue;
         const double beta = sqrt(tot[s][0]);
-        cd *V0 = a.V + (size_t)s * (a.m + 1) * n;
+        C *V0 = a.V + (size_t)s * (a.m + 1) * n;
         for (long long q = q0; q < n; q += stride) {
-            const cd r = V0[q];
-            V0[q] = cmk(r.x / beta, r.y / beta);
+            const cd r = to_cd(V0[q]);
+            store_c(V0[q], cmk(r.x / beta, r.y / beta));
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             Slot &sl = a.slots[s];
@@ -165,18 +187,19 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs a) {
             if (k > i) continue;
             const cd h = sh_h[s];
             if (blockIdx.x == 0 && threadIdx.x == 0) a.H[(size_t)s * ldh * a.m + (size_t)ldh * (i - 1) + (k - 1)] = h;
-            cd *ws = a.w + (size_t)s * n;
-            const cd *Vs = a.V + (size_t)s * (a.m + 1) * n;
-            const cd *vk = Vs + (size_t)(k - 1) * n;
-            const cd *vn = (k < i) ? Vs + (size_t)k * n : nullptr;
+            C *ws = a.w + (size_t)s * n;
+            const C *Vs = a.V + (size_t)s * (a.m + 1) * n;
+            const C *vk = Vs + (size_t)(k - 1) * n;
+            const C *vn = (k < i) ? Vs + (size_t)k * n : nullptr;
             double u[2] = {0, 0};
             for (long long q = q0; q < n; q += stride) {
-                cd w = ws[q];
-                const cd p = vk[q];
+                cd w = to_cd(ws[q]);
+                const cd p = to_cd(vk[q]);
                 csub_mul(w, h, p);
-                ws[q] = w;
+                store_c(ws[q], w);
+                w = to_cd(ws[q]);
                 if (vn) {
-                    const cd z = vn[q];
+                    const cd z = to_cd(vn[q]);
                     cdot_acc(u[0], u[1], z, w);
                 } else {
                     u[0] += cabs2(w);
@@ -206,11 +229,11 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs a) {
     for (int j = 1; j <= jmax; ++j) {
         for (int s = 0; s < a.ns; ++s) {
             if (smode[s] != SLOT_ARNOLDI || !(snormav[s] + (double)0.001f * shn[s] == snormav[s]) || j > sstep[s] + 1) continue;
-            const cd *vj = a.V + (size_t)s * (a.m + 1) * n + (size_t)(j - 1) * n;
-            const cd *ws = a.w + (size_t)s * n;
+            const C *vj = a.V + (size_t)s * (a.m + 1) * n + (size_t)(j - 1) * n;
+            const C *ws = a.w + (size_t)s * n;
             double u[2] = {0, 0};
             for (long long q = q0; q < n; q += stride) {
-                const cd z = vj[q], w = ws[q];
+                const cd z = to_cd(vj[q]), w = to_cd(ws[q]);
                 cdot_acc(u[0], u[1], z, w);
             }
             block_sum<2>(u, bsh);
@@ -227,22 +250,22 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs a) {
                 cd *Hc = a.H + (size_t)s * ldh * a.m + (size_t)ldh * (i - 1);
                 Hc[j - 1] = cadd(Hc[j - 1], hr);
             }
-            const cd *vj = a.V + (size_t)s * (a.m + 1) * n + (size_t)(j - 1) * n;
-            cd *ws = a.w + (size_t)s * n;
+            const C *vj = a.V + (size_t)s * (a.m + 1) * n + (size_t)(j - 1) * n;
+            C *ws = a.w + (size_t)s * n;
             for (long long q = q0; q < n; q += stride) {
-                cd w = ws[q];
-                const cd p = vj[q];
+                cd w = to_cd(ws[q]);
+                const cd p = to_cd(vj[q]);
                 csub_mul(w, hr, p);
-                ws[q] = w;
+                store_c(ws[q], w);
             }
         }
     }
     if (jmax > 0) {
         for (int s = 0; s < a.ns; ++s) {
             if (smode[s] != SLOT_ARNOLDI || !(snormav[s] + (double)0.001f * shn[s] == snormav[s])) continue;
-            const cd *ws = a.w + (size_t)s * n;
+            const C *ws = a.w + (size_t)s * n;
             double u[1] = {0};
-            for (long long q = q0; q < n; q += stride) u[0] += cabs2(ws[q]);
+            for (long long q = q0; q < n; q += stride) u[0] += cabs2(to_cd(ws[q]));
             block_sum<1>(u, bsh);
             put_partial(a, parity ^ 1, s, u, 1);
         }
@@ -259,11 +282,11 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs a) {
         if (smode[s] != SLOT_ARNOLDI) continue;
         const int i = sstep[s] + 1;
         const double hn = shn[s];
-        const cd *ws = a.w + (size_t)s * n;
-        cd *vi = a.V + (size_t)s * (a.m + 1) * n + (size_t)i * n;
+        const C *ws = a.w + (size_t)s * n;
+        C *vi = a.V + (size_t)s * (a.m + 1) * n + (size_t)i * n;
         for (long long q = q0; q < n; q += stride) {
-            const cd w = ws[q];
-            vi[q] = (hn != 0.0) ? cmk(w.x / hn, w.y / hn) : w;
+            const cd w = to_cd(ws[q]);
+            store_c(vi[q], (hn != 0.0) ? cmk(w.x / hn, w.y / hn) : w);
         }
     }
     if (blockIdx.x == 0) {
@@ -324,12 +347,12 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs a) {
         const cd *ys = a.y + (size_t)s * (a.m + 1);
         for (int c = threadIdx.x; c < kd; c += blockDim.x) ysm[c] = make_double2(__ldcg(&ys[c].x), __ldcg(&ys[c].y));
         __syncthreads();
-        const cd *Vs = a.V + (size_t)s * (a.m + 1) * n;
-        cd *xs = a.x + (size_t)s * n;
+        const C *Vs = a.V + (size_t)s * (a.m + 1) * n;
+        C *xs = a.x + (size_t)s * n;
         for (long long q = q0; q < n; q += stride) {
             cd acc = cmk(0, 0);
-            for (int c = 0; c < kd; ++c) cfma(acc, Vs[(size_t)c * n + q], ysm[c]);
-            xs[q] = cadd(xs[q], acc);
+            for (int c = 0; c < kd; ++c) cfma(acc, to_cd(Vs[(size_t)c * n + q]), ysm[c]);
+            store_c(xs[q], cadd(to_cd(xs[q]), acc));
         }
         __syncthreads();
     }
@@ -340,43 +363,167 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs a) {
             if (smode[s] != SLOT_ARNOLDI) continue;
             Slot &sl = a.slots[s];
             if (!sl.finish) continue;
-            if (sl.conv) sl.mode = SLOT_DONE;
-            else if (sl.cycle < a.max_cycles) sl.mode = SLOT_START;
-            else sl.mode = SLOT_DONE;
+            if (sl.conv) sl.mode = a.mixed ? SLOT_INNER_DONE : SLOT_DONE;
+            else if (sl.cycle < a.max_cycles) { sl.mode = SLOT_START; sl.zero_x = 0; }
+            else sl.mode = a.mixed ? SLOT_INNER_DONE : SLOT_DONE;
         }
     }
 }
 
 // matvec input per slot: x at a cycle start, v_step during Arnoldi; idle
 // slots are skipped by every matvec kernel
-__global__ void k_stage(const Slot *slots, int ns, const cd *V, const cd *x, cd *Xin, int *skip, long long n, int m) {
+template <typename C>
+__global__ void k_stage(const Slot *slots, int ns, const C *V, const C *x, C *Xin, int *skip, long long n, int m) {
     const int s = blockIdx.y;
     const int md = slots[s].mode;
-    const bool act = md == SLOT_START || md == SLOT_ARNOLDI;
+    const bool act = (md == SLOT_START && !slots[s].zero_x) || md == SLOT_ARNOLDI;
     if (blockIdx.x == 0 && threadIdx.x == 0) skip[s] = act ? 0 : 1;
     if (!act) return;
-    const cd *src = md == SLOT_START ? x + (size_t)s * n : V + ((size_t)s * (m + 1) + slots[s].step) * n;
-    cd *dst = Xin + (size_t)s * n;
+    const C *src = md == SLOT_START ? x + (size_t)s * n : V + ((size_t)s * (m + 1) + slots[s].step) * n;
+    C *dst = Xin + (size_t)s * n;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
         dst[q] = src[q];
+}
+
+// ---- mixed form: the FP64 outer refinement
+// x64 += rho * d (the inner complex64 correction), for slots flagged upd
+__global__ void k_outer_update(const Slot *slots, cd *x64, const cf *d32, long long n) {
+    const int s = blockIdx.y;
+    if (!slots[s].upd) return;
+    const double rho = slots[s].rho;
+    cd *xs = x64 + (size_t)s * n;
+    const cf *ds = d32 + (size_t)s * n;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const cd d = widen(ds[q]);
+        xs[q] = cadd(xs[q], cmk(rho * d.x, rho * d.y));
+    }
+}
+
+__global__ void k_stage_resid(const Slot *slots, const cd *x64, cd *Xin, int *skip, long long n) {
+    const int s = blockIdx.y;
+    const bool act = slots[s].mode == SLOT_RESID;
+    if (blockIdx.x == 0 && threadIdx.x == 0) skip[s] = act ? 0 : 1;
+    if (!act) return;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+        Xin[(size_t)s * n + q] = x64[(size_t)s * n + q];
+}
+
+struct ResidArgs {
+    Slot *slots;
+    int ns;
+    const cd *b64, *w64;   // rhs and A x, FP64
+    cf *rhs32, *x32;       // inner right-hand side (r / rho) and initial guess (0)
+    double *red;
+    GridBarrier *bar;
+    int *err;
+    long long n;
+    double tol;
+    int max_outer;
+};
+
+// r = b - A x in FP64; stop when ||r||/||b|| < tol, else hand r/||r|| to an
+// inner complex64 solve with a zero initial guess
+__global__ void __launch_bounds__(BT) k_resid(ResidArgs a) {
+    __shared__ double bsh[64];
+    __shared__ double tot[NSMAX][4];
+    __shared__ int smode[NSMAX];
+    const long long n = a.n;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long q0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    for (int s = threadIdx.x; s < a.ns; s += blockDim.x) smode[s] = a.slots[s].mode;
+    __syncthreads();
+    for (int s = 0; s < a.ns; ++s) {
+        if (smode[s] != SLOT_RESID) continue;
+        double v[2] = {0, 0};
+        const cd *bs = a.b64 + (size_t)s * n, *ws = a.w64 + (size_t)s * n;
+        for (long long q = q0; q < n; q += stride) {
+            const cd b = bs[q], r = csub(b, ws[q]);
+            v[0] += cabs2(r);
+            v[1] += cabs2(b);
+        }
+        block_sum<2>(v, bsh);
+        if (threadIdx.x == 0) {
+            double *p = a.red + (size_t)blockIdx.x * (NSMAX * 4) + s * 4;
+            p[0] = v[0];
+            p[1] = v[1];
+        }
+    }
+    grid_barrier(a.bar, gridDim.x, a.err);
+    {
+        const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+        for (int s = wp; s < a.ns; s += nw) {
+            double acc[2] = {0, 0};
+            for (int b = lane; b < (int)gridDim.x; b += 32) {
+                const double *p = a.red + (size_t)b * (NSMAX * 4) + s * 4;
+                acc[0] += __ldcg(p);
+                acc[1] += __ldcg(p + 1);
+            }
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+            if (lane == 0) { tot[s][0] = acc[0]; tot[s][1] = acc[1]; }
+        }
+        __syncthreads();
+    }
+    for (int s = 0; s < a.ns; ++s) {
+        if (smode[s] != SLOT_RESID) continue;
+        const double rho = sqrt(tot[s][0]);
+        const double bn = a.slots[s].outer == 0 ? sqrt(tot[s][1]) : a.slots[s].b64;
+        const double rel = bn > 0.0 ? rho / bn : 0.0;
+        const bool stop = !(rel >= a.tol) || a.slots[s].outer >= a.max_outer;   // NaN stops too
+        if (!stop) {
+            const cd *bs = a.b64 + (size_t)s * n, *ws = a.w64 + (size_t)s * n;
+            cf *rs = a.rhs32 + (size_t)s * n, *xs = a.x32 + (size_t)s * n;
+            for (long long q = q0; q < n; q += stride) {
+                const cd r = csub(bs[q], ws[q]);
+                rs[q] = make_float2((float)(r.x / rho), (float)(r.y / rho));
+                xs[q] = make_float2(0.f, 0.f);
+            }
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            Slot &sl = a.slots[s];
+            if (sl.outer == 0) sl.b64 = bn;
+            sl.relres = rel;
+            sl.upd = 0;
+            if (stop) {
+                sl.mode = SLOT_DONE;
+                sl.conv = rel < a.tol;
+                sl.error = rel;
+                if (!(rel == rel)) sl.status = SCD_NAN;
+            } else {
+                sl.rho = rho;
+                sl.outer += 1;
+                sl.mode = SLOT_START;
+                sl.zero_x = 1;
+                sl.cycle = 0;
+                sl.step = 0;
+                sl.conv = 0;
+                sl.finish = 0;
+            }
+            if (*a.err) { sl.status = SCD_TIMEOUT; sl.mode = SLOT_DONE; }
+        }
+    }
 }
 
 }  // namespace
 
 struct BatchBuffers {
-    int ns = 0, m = 0;
+    int ns = 0, m = 0, mixed = 0;
     long long n = 0;
-    cd *V = nullptr, *H = nullptr, *cs = nullptr, *sn = nullptr, *g = nullptr, *y = nullptr;
-    cd *x = nullptr, *rhs = nullptr, *Xin = nullptr, *W = nullptr;
+    void *V = nullptr;                       // cd or cf bases
+    cd *H = nullptr, *cs = nullptr, *sn = nullptr, *g = nullptr, *y = nullptr;
+    void *x = nullptr, *rhs = nullptr, *Xin = nullptr, *W = nullptr;   // GMRES precision
+    cd *x64 = nullptr, *b64 = nullptr, *Xin64 = nullptr, *W64 = nullptr;   // mixed: FP64 outer vectors
     Slot *slots = nullptr;
     Slot *h_slots = nullptr;
-    int *skip = nullptr;
+    int *skip = nullptr, *skip64 = nullptr;
     double *red = nullptr;
     int grid = 0;
 };
 
 static void free_bb(BatchBuffers &b) {
-    void *p[] = {b.V, b.H, b.cs, b.sn, b.g, b.y, b.x, b.rhs, b.Xin, b.W, b.slots, b.skip, b.red};
+    void *p[] = {b.V, b.H, b.cs, b.sn, b.g, b.y, b.x, b.rhs, b.Xin, b.W, b.x64, b.b64, b.Xin64, b.W64,
+                 b.slots, b.skip, b.skip64, b.red};
     for (void *q : p) if (q) cudaFree(q);
     if (b.h_slots) cudaFreeHost(b.h_slots);
     b = BatchBuffers();
@@ -389,30 +536,42 @@ void batch_free(scd_ctx *c) {
     c->batch = nullptr;
 }
 
-int batch_prepare(scd_ctx *c, int ns, int m, BatchBuffers &b) {
-    if (b.ns >= ns && b.m >= m && b.n == c->n && b.V) return SCD_OK;
+int batch_prepare(scd_ctx *c, int ns, int m, int mixed, BatchBuffers &b) {
+    if (b.ns >= ns && b.m >= m && b.n == c->n && b.mixed == mixed && b.V) return SCD_OK;
     free_bb(b);
     const long long n = c->n;
+    const size_t es = mixed ? sizeof(cf) : sizeof(cd);
     auto al = [&](void **p, size_t bytes, const char *what) -> int {
         if (cudaMalloc(p, bytes) != cudaSuccess) { cudaGetLastError(); return set_error(c, SCD_OOM, "batch %s (%zu bytes)", what, bytes); }
         return SCD_OK;
     };
     int rc;
-    if ((rc = al((void **)&b.V, sizeof(cd) * (size_t)ns * (m + 1) * n, "Krylov bases"))) return rc;
+    if ((rc = al(&b.V, es * (size_t)ns * (m + 1) * n, "Krylov bases"))) return rc;
     if ((rc = al((void **)&b.H, sizeof(cd) * (size_t)ns * (m + 1) * m, "H"))) return rc;
     if ((rc = al((void **)&b.cs, sizeof(cd) * (size_t)ns * (m + 1), "cs"))) return rc;
     if ((rc = al((void **)&b.sn, sizeof(cd) * (size_t)ns * (m + 1), "sn"))) return rc;
     if ((rc = al((void **)&b.g, sizeof(cd) * (size_t)ns * (m + 1), "g"))) return rc;
     if ((rc = al((void **)&b.y, sizeof(cd) * (size_t)ns * (m + 1), "y"))) return rc;
-    if ((rc = al((void **)&b.x, sizeof(cd) * (size_t)ns * n, "x"))) return rc;
-    if ((rc = al((void **)&b.rhs, sizeof(cd) * (size_t)ns * n, "rhs"))) return rc;
-    if ((rc = al((void **)&b.Xin, sizeof(cd) * (size_t)ns * n, "Xin"))) return rc;
-    if ((rc = al((void **)&b.W, sizeof(cd) * (size_t)ns * n, "W"))) return rc;
+    if ((rc = al(&b.x, es * (size_t)ns * n, "x"))) return rc;
+    if ((rc = al(&b.rhs, es * (size_t)ns * n, "rhs"))) return rc;
+    if ((rc = al(&b.Xin, es * (size_t)ns * n, "Xin"))) return rc;
+    if ((rc = al(&b.W, es * (size_t)ns * n, "W"))) return rc;
+    if (mixed) {
+        if ((rc = al((void **)&b.x64, sizeof(cd) * (size_t)ns * n, "x64"))) return rc;
+        if ((rc = al((void **)&b.b64, sizeof(cd) * (size_t)ns * n, "b64"))) return rc;
+        if ((rc = al((void **)&b.Xin64, sizeof(cd) * (size_t)ns * n, "Xin64"))) return rc;
+        if ((rc = al((void **)&b.W64, sizeof(cd) * (size_t)ns * n, "W64"))) return rc;
+        if ((rc = al((void **)&b.skip64, sizeof(int) * ns, "skip64"))) return rc;
+    }
     if ((rc = al((void **)&b.slots, sizeof(Slot) * ns, "slots"))) return rc;
     if ((rc = al((void **)&b.skip, sizeof(int) * ns, "skip"))) return rc;
     if (cudaMallocHost((void **)&b.h_slots, sizeof(Slot) * ns) != cudaSuccess) return set_error(c, SCD_OOM, "pinned slots");
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tick, BT, 0);
+    int per_sm = 0, per_sm2 = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tick<cd>, BT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_tick<cf>, BT, 0);
+    per_sm = std::min(per_sm, per_sm2);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm2, k_resid, BT, 0);
+    per_sm = std::min(per_sm, per_sm2);
     if (per_sm < 1) return set_error(c, SCD_CUDA_ERROR, "tick kernel cannot be resident");
     per_sm = std::min(per_sm, 2);
     b.grid = per_sm * c->nsm;
@@ -420,20 +579,45 @@ int batch_prepare(scd_ctx *c, int ns, int m, BatchBuffers &b) {
     b.ns = ns;
     b.m = m;
     b.n = n;
+    b.mixed = mixed;
     return SCD_OK;
 }
 
-// Solve columns `cols` (device pointers to slot-ordered right-hand sides)
-// with up to `ns` slots; solutions go to X[j] (slot-ordered, stride n).
+template <typename C>
+static int launch_tick(scd_ctx *c, BatchBuffers &bb, int ns, int m, int cycles, double tol, int mixed) {
+    TickArgs<C> a;
+    a.slots = bb.slots; a.ns = ns; a.V = (C *)bb.V; a.H = bb.H; a.cs = bb.cs; a.sn = bb.sn; a.g = bb.g; a.y = bb.y;
+    a.x = (C *)bb.x; a.rhs = (C *)bb.rhs; a.w = (C *)bb.W; a.red = bb.red; a.bar = c->d_bar; a.err = c->d_err;
+    a.n = c->n; a.m = m; a.max_cycles = cycles; a.tol = tol; a.mixed = mixed;
+    const long long n = c->n;
+    k_stage<C><<<dim3(std::min<long long>((n + 255) / 256, 1024), ns), 256, 0, c->st>>>(bb.slots, ns, (C *)bb.V, (C *)bb.x,
+                                                                                       (C *)bb.Xin, bb.skip, n, m);
+    run_matvec(c, (const C *)bb.Xin, (C *)bb.W, ns, bb.skip);
+    void *args[] = {&a};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_tick<C>, dim3(bb.grid), dim3(BT), args, 0, c->st);
+    c->launches += 2;
+    return check_cuda(c, e, "tick launch");
+}
+
+// Solve columns `rhs_cols` (device pointers to slot-ordered right-hand
+// sides) with up to `ns` slots; FP64 solutions go to X[j] (stride n).
+// precision 0: restarted GMRES(m) in complex128 to `tol` (the reference's
+// algorithm); 1: FP64 iterative refinement to `tol` around complex64
+// GMRES(m) inner solves to `inner_tol`, at most `max_outer` outer steps.
 int batch_solve(scd_ctx *c, int ncol, const cd *const *rhs_cols, cd *X, double tol, int m, int cycles, int ns,
-                int *iters, int *conv_out, int *status_out) {
+                int *iters, int *conv_out, int *status_out, int precision, double inner_tol, int max_outer) {
     if (!c->batch) c->batch = new BatchBuffers();
     BatchBuffers &bb = *(BatchBuffers *)c->batch;
+    const int mixed = precision == SCD_PREC_MIXED ? 1 : 0;
     if (ns > NSMAX) ns = NSMAX;
     if (ns > ncol) ns = ncol;
-    int rc = batch_prepare(c, ns, m, bb);
+    int rc = batch_prepare(c, ns, m, mixed, bb);
     if (rc) return rc;
-    if ((rc = ensure_work(c, ns))) return rc;
+    if (mixed) {
+        if ((rc = ensure_single(c)) || (rc = ensure_work_single(c, ns)) || (rc = ensure_work(c, ns))) return rc;
+    } else if ((rc = ensure_work(c, ns))) {
+        return rc;
+    }
     if (!c->d_bar) {
         if (cudaMalloc(&c->d_bar, sizeof(GridBarrier)) != cudaSuccess || cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess)
             return set_error(c, SCD_OOM, "barrier");
@@ -450,22 +634,18 @@ int batch_solve(scd_ctx *c, int ncol, const cd *const *rhs_cols, cd *X, double t
     auto now_ms = [&]() { return std::chrono::duration<double, std::milli>(clk::now() - t0).count(); };
     std::vector<double> t_in(ncol, 0.0);
     c->col_latency_ms.assign(ncol, 0.0);
-    TickArgs a;
-    a.slots = bb.slots; a.ns = ns; a.V = bb.V; a.H = bb.H; a.cs = bb.cs; a.sn = bb.sn; a.g = bb.g; a.y = bb.y;
-    a.x = bb.x; a.rhs = bb.rhs; a.w = bb.W; a.red = bb.red; a.bar = c->d_bar; a.err = c->d_err; a.n = n;
-    a.m = m; a.max_cycles = cycles; a.tol = tol;
-    long long ticks = 0;
+    const double gm_tol = mixed ? inner_tol : tol;
     while (finished < ncol) {
-        // refill free slots
-        bool any = false;
+        bool inner = false, resid = false, upd = false;
         for (int s = 0; s < ns; ++s) {
             if (hs[s].mode == SLOT_DONE) {
                 const int col = hs[s].col;
-                cudaMemcpyAsync(X + (size_t)col * n, bb.x + (size_t)s * n, sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
+                const cd *xs = mixed ? bb.x64 + (size_t)s * n : (const cd *)bb.x + (size_t)s * n;
+                cudaMemcpyAsync(X + (size_t)col * n, xs, sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
                 if (iters) iters[col] = hs[s].iters;
-                c->col_latency_ms[col] = now_ms() - t_in[col];
                 if (conv_out) conv_out[col] = hs[s].conv;
                 if (status_out) status_out[col] = hs[s].status;
+                c->col_latency_ms[col] = now_ms() - t_in[col];
                 if (hs[s].status != SCD_OK) worst = hs[s].status;
                 else if (!hs[s].conv && worst == SCD_OK) worst = SCD_NOT_CONVERGED;
                 c->n_arn += hs[s].iters;
@@ -476,28 +656,47 @@ int batch_solve(scd_ctx *c, int ncol, const cd *const *rhs_cols, cd *X, double t
                 hs[s].col = -1;
             }
             if (hs[s].mode == SLOT_FREE && next < ncol) {
-                cudaMemcpyAsync(bb.rhs + (size_t)s * n, rhs_cols[next], sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
-                cudaMemcpyAsync(bb.x + (size_t)s * n, rhs_cols[next], sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
                 std::memset(&hs[s], 0, sizeof(Slot));
-                hs[s].mode = SLOT_START;
+                if (mixed) {
+                    cudaMemcpyAsync(bb.b64 + (size_t)s * n, rhs_cols[next], sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
+                    cudaMemcpyAsync(bb.x64 + (size_t)s * n, rhs_cols[next], sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
+                    hs[s].mode = SLOT_RESID;
+                } else {
+                    cudaMemcpyAsync((cd *)bb.rhs + (size_t)s * n, rhs_cols[next], sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
+                    cudaMemcpyAsync((cd *)bb.x + (size_t)s * n, rhs_cols[next], sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
+                    hs[s].mode = SLOT_START;
+                }
                 t_in[next] = now_ms();
                 hs[s].col = next++;
             }
-            if (hs[s].mode == SLOT_START || hs[s].mode == SLOT_ARNOLDI) any = true;
+            if (hs[s].mode == SLOT_INNER_DONE) { hs[s].mode = SLOT_RESID; hs[s].upd = 1; upd = true; }
+            if (hs[s].mode == SLOT_RESID) resid = true;
+            if (hs[s].mode == SLOT_START || hs[s].mode == SLOT_ARNOLDI) inner = true;
         }
         if (finished >= ncol) break;
-        if (!any) return set_error(c, SCD_CUDA_ERROR, "batch solver stalled");
+        if (!inner && !resid) return set_error(c, SCD_CUDA_ERROR, "batch solver stalled");
         cudaMemcpyAsync(bb.slots, hs, sizeof(Slot) * ns, cudaMemcpyHostToDevice, c->st);
-        k_stage<<<dim3(std::min<long long>((n + 255) / 256, 1024), ns), 256, 0, c->st>>>(bb.slots, ns, bb.V, bb.x, bb.Xin,
-                                                                                         bb.skip, n, m);
-        run_matvec(c, bb.Xin, bb.W, ns, bb.skip);
-        void *args[] = {&a};
-        cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_tick, dim3(bb.grid), dim3(BT), args, 0, c->st);
-        c->launches += 2;
-        if ((rc = check_cuda(c, e, "tick launch"))) return rc;
+        if (mixed) {
+            const dim3 g2(std::min<long long>((n + 255) / 256, 1024), ns);
+            if (upd) k_outer_update<<<g2, 256, 0, c->st>>>(bb.slots, bb.x64, (const cf *)bb.x, n);
+            if (resid) {
+                k_stage_resid<<<g2, 256, 0, c->st>>>(bb.slots, bb.x64, bb.Xin64, bb.skip64, n);
+                run_matvec(c, (const cd *)bb.Xin64, bb.W64, ns, bb.skip64);
+                ResidArgs ra;
+                ra.slots = bb.slots; ra.ns = ns; ra.b64 = bb.b64; ra.w64 = bb.W64; ra.rhs32 = (cf *)bb.rhs;
+                ra.x32 = (cf *)bb.x; ra.red = bb.red; ra.bar = c->d_bar; ra.err = c->d_err; ra.n = n; ra.tol = tol;
+                ra.max_outer = max_outer;
+                void *args[] = {&ra};
+                cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_resid, dim3(bb.grid), dim3(BT), args, 0, c->st);
+                c->launches += 3 + (upd ? 1 : 0);
+                if ((rc = check_cuda(c, e, "residual launch"))) return rc;
+            }
+            if ((rc = launch_tick<cf>(c, bb, ns, m, cycles, gm_tol, 1))) return rc;
+        } else {
+            if ((rc = launch_tick<cd>(c, bb, ns, m, cycles, gm_tol, 0))) return rc;
+        }
         cudaMemcpyAsync(hs, bb.slots, sizeof(Slot) * ns, cudaMemcpyDeviceToHost, c->st);
         if ((rc = check_cuda(c, cudaStreamSynchronize(c->st), "tick"))) return rc;
-        ++ticks;
         for (int s = 0; s < ns; ++s)
             if (hs[s].status == SCD_TIMEOUT) return set_error(c, SCD_TIMEOUT, "grid barrier wait expired in the batch solver");
     }

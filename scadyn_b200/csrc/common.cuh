@@ -63,14 +63,55 @@ SCD_HD cd cdiv(cd a, cd b) {
     return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
 }
 
+// complex float with pinned single-precision operations
+#ifdef __CUDA_ARCH__
+#define SCD_FMAF(a, b, c) __fmaf_rn((a), (b), (c))
+#define SCD_MULF(a, b) __fmul_rn((a), (b))
+#define SCD_ADDF(a, b) __fadd_rn((a), (b))
+#define SCD_SUBF(a, b) __fsub_rn((a), (b))
+#else
+#define SCD_FMAF(a, b, c) fmaf((a), (b), (c))
+#define SCD_MULF(a, b) ((a) * (b))
+#define SCD_ADDF(a, b) ((a) + (b))
+#define SCD_SUBF(a, b) ((a) - (b))
+#endif
 SCD_HD cf  fmk(float r, float i) { return make_float2(r, i); }
-SCD_HD cf  fadd(cf a, cf b) { return make_float2(a.x + b.x, a.y + b.y); }
-SCD_HD cf  fsub(cf a, cf b) { return make_float2(a.x - b.x, a.y - b.y); }
-SCD_HD cf  fmul(cf a, cf b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+SCD_HD cf  cadd(cf a, cf b) { return make_float2(SCD_ADDF(a.x, b.x), SCD_ADDF(a.y, b.y)); }
+SCD_HD cf  csub(cf a, cf b) { return make_float2(SCD_SUBF(a.x, b.x), SCD_SUBF(a.y, b.y)); }
+SCD_HD cf  cmul(cf a, cf b) {
+    return make_float2(SCD_FMAF(a.x, b.x, SCD_MULF(-a.y, b.y)), SCD_FMAF(a.x, b.y, SCD_MULF(a.y, b.x)));
+}
+SCD_HD cf  cconj(cf a) { return make_float2(a.x, -a.y); }
+SCD_HD void cfma(cf &a, cf b, cf c) {
+    a.x = SCD_FMAF(-b.y, c.y, SCD_FMAF(b.x, c.x, a.x));
+    a.y = SCD_FMAF(b.y, c.x, SCD_FMAF(b.x, c.y, a.y));
+}
+SCD_HD cf csub_scaled(cf a, float k2, cf b) { return make_float2(SCD_FMAF(-k2, b.x, a.x), SCD_FMAF(-k2, b.y, a.y)); }
+SCD_HD cf  fadd(cf a, cf b) { return cadd(a, b); }
+SCD_HD cf  fsub(cf a, cf b) { return csub(a, b); }
+SCD_HD cf  fmul(cf a, cf b) { return cmul(a, b); }
+
+// zero / construction for either complex type
+template <typename C> SCD_HD C czero();
+template <> SCD_HD cd czero<cd>() { return make_double2(0.0, 0.0); }
+template <> SCD_HD cf czero<cf>() { return make_float2(0.f, 0.f); }
+template <typename C> struct CReal;
+template <> struct CReal<cd> { typedef double type; };
+template <> struct CReal<cf> { typedef float type; };
+template <typename C> SCD_HD C cmake(double r, double i);
+template <> SCD_HD cd cmake<cd>(double r, double i) { return make_double2(r, i); }
+template <> SCD_HD cf cmake<cf>(double r, double i) { return make_float2((float)r, (float)i); }
 
 // widen a stored near-zone value to FP64 (dcmplx(val) in src/sparse_mat.f90:113)
 SCD_HD cd widen(cf a) { return make_double2((double)a.x, (double)a.y); }
 SCD_HD cd widen(cd a) { return a; }
+// stored value in the compute precision C
+template <typename C> SCD_HD C as_c(cf a);
+template <typename C> SCD_HD C as_c(cd a);
+template <> SCD_HD cd as_c<cd>(cf a) { return make_double2((double)a.x, (double)a.y); }
+template <> SCD_HD cd as_c<cd>(cd a) { return a; }
+template <> SCD_HD cf as_c<cf>(cf a) { return a; }
+template <> SCD_HD cf as_c<cf>(cd a) { return make_float2((float)a.x, (float)a.y); }
 
 // Grid-wide barrier for kernels launched with cudaLaunchCooperativeKernel
 // (all CTAs co-resident).  The spin is bounded: after `limit` polls the CTA

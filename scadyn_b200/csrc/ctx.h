@@ -127,6 +127,12 @@ struct scd_ctx {
     long long n_matvec = 0, n_arn = 0, launches = 0;
     bool timing = false;
 
+    // complex64 operator copies and work buffers (mixed-precision inner solves)
+    bool f_ready = false;
+    cf *f_P = nullptr, *f_Fo = nullptr, *f_tw[3] = {nullptr, nullptr, nullptr};
+    cf *f_bpart = nullptr, *f_W = nullptr, *f_R = nullptr, *f_nzpart = nullptr;
+    int f_cap = 0;
+
     void *batch = nullptr;               // batch-solver buffers (batch.cu)
     std::vector<double> col_latency_ms;  // admission -> completion, last batch solve
 
@@ -143,6 +149,9 @@ void launch_permute_in(scd_ctx *c, const cd *x_orig, cd *x_slot, int nrhs, long 
 void launch_permute_out(scd_ctx *c, const cd *x_slot, cd *x_orig, int nrhs, long long ld);
 // full matvec y = A x on slot-ordered vectors (nrhs columns, stride n)
 void run_matvec(scd_ctx *c, const cd *x, cd *y, int nrhs, const int *done);
+void run_matvec(scd_ctx *c, const cf *x, cf *y, int nrhs, const int *done);
+int ensure_single(scd_ctx *c);
+int ensure_work_single(scd_ctx *c, int nrhs);
 void launch_near(scd_ctx *c, const cd *x, int nrhs, const int *done);
 void launch_fft_chain(scd_ctx *c, const cd *x, int nrhs, const int *done);
 void launch_gather(scd_ctx *c, const cd *x, cd *y, int nrhs, const int *done);
@@ -156,7 +165,7 @@ int gmres_solve(scd_ctx *c, const cd *d_rhs_slot, cd *d_x_slot, double tol, int 
 // ---- batched column solves (batch.cu) ----
 void batch_free(scd_ctx *c);
 int batch_solve(scd_ctx *c, int ncol, const cd *const *rhs_cols, cd *X, double tol, int m, int cycles, int ns,
-                int *iters, int *conv, int *status);
+                int *iters, int *conv, int *status, int precision, double inner_tol, int max_outer);
 
 // ---- setup (kernels_setup.cu) ----
 int setup_green(scd_ctx *c, const scd_c128 *Fg_host);

@@ -42,29 +42,29 @@ __global__ void k_permute_out(const cd *__restrict__ xs, cd *__restrict__ xo, co
 // tets, for a group of right-hand sides at a time (projector values are read
 // once per group).  Projectors are stored P[(g*27 + j)*T + slot].
 // bpart[((r*ncubes + c)*4 + g)*27 + j].
-template <int SC_RG>
+template <typename C, int SC_RG>
 __global__ void __launch_bounds__(32 * WARPS_PER_CTA)
-k_scatter(const cd *__restrict__ x, long long ld, const cd *__restrict__ P, int T,
-          const int *__restrict__ cube_off, int ncubes, cd *__restrict__ bpart, const int *skip, int nrhs) {
+k_scatter(const C *__restrict__ x, long long ld, const C *__restrict__ P, int T,
+          const int *__restrict__ cube_off, int ncubes, C *__restrict__ bpart, const int *skip, int nrhs) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c = blockIdx.x * WARPS_PER_CTA + warp;
     if (c >= ncubes || lane >= 27) return;
     const int s0 = cube_off[c], s1 = cube_off[c + 1];
-    const cd *P0 = P + (size_t)lane * T, *PX = P + (size_t)(27 + lane) * T;
-    const cd *PY = P + (size_t)(54 + lane) * T, *PZ = P + (size_t)(81 + lane) * T;
+    const C *P0 = P + (size_t)lane * T, *PX = P + (size_t)(27 + lane) * T;
+    const C *PY = P + (size_t)(54 + lane) * T, *PZ = P + (size_t)(81 + lane) * T;
     for (int r0 = 0; r0 < nrhs; r0 += SC_RG) {
-        cd acc[SC_RG][4];
+        C acc[SC_RG][4];
 #pragma unroll
-        for (int q = 0; q < SC_RG; ++q) acc[q][0] = acc[q][1] = acc[q][2] = acc[q][3] = cmk(0, 0);
+        for (int q = 0; q < SC_RG; ++q) acc[q][0] = acc[q][1] = acc[q][2] = acc[q][3] = czero<C>();
 #pragma unroll 4
         for (int s = s0; s < s1; ++s) {
-            const cd p0 = P0[s], px = PX[s], py = PY[s], pz = PZ[s];
+            const C p0 = P0[s], px = PX[s], py = PY[s], pz = PZ[s];
 #pragma unroll
             for (int q = 0; q < SC_RG; ++q) {
                 const int r = r0 + q;
                 if (r < nrhs) {
-                    const cd *xr = x + r * ld + 3LL * s;
-                    const cd x0 = xr[0], x1 = xr[1], x2 = xr[2];
+                    const C *xr = x + r * ld + 3LL * s;
+                    const C x0 = xr[0], x1 = xr[1], x2 = xr[2];
                     cfma(acc[q][0], p0, x0);
                     cfma(acc[q][1], p0, x1);
                     cfma(acc[q][2], p0, x2);
@@ -78,7 +78,7 @@ k_scatter(const cd *__restrict__ x, long long ld, const cd *__restrict__ P, int 
         for (int q = 0; q < SC_RG; ++q) {
             const int r = r0 + q;
             if (r < nrhs && !(skip && skip[r])) {
-                cd *o = bpart + ((long long)r * ncubes + c) * 4 * 27 + lane;
+                C *o = bpart + ((long long)r * ncubes + c) * 4 * 27 + lane;
                 o[0] = acc[q][0];
                 o[27] = acc[q][1];
                 o[54] = acc[q][2];
@@ -95,11 +95,13 @@ k_scatter(const cd *__restrict__ x, long long ld, const cd *__restrict__ P, int 
 template <int P> struct Log2 { static constexpr int v = 1 + Log2<P / 2>::v; };
 template <> struct Log2<1> { static constexpr int v = 0; };
 
-template <bool INV>
-__device__ __forceinline__ void radix4(cd &v0, cd &v1, cd &v2, cd &v3) {
-    cd a0 = cadd(v0, v2), a1 = csub(v0, v2), a2 = cadd(v1, v3), a3 = csub(v1, v3);
+template <bool INV, typename C>
+__device__ __forceinline__ void radix4(C &v0, C &v1, C &v2, C &v3) {
+    C a0 = cadd(v0, v2), a1 = csub(v0, v2), a2 = cadd(v1, v3), a3 = csub(v1, v3);
     // forward: X1 = a1 - i a3 ; X3 = a1 + i a3
-    cd ia3 = INV ? cmk(-a3.y, a3.x) : cmk(a3.y, -a3.x);   // (+i or -i) * a3
+    C ia3;                                                 // (+i or -i) * a3
+    ia3.x = INV ? -a3.y : a3.y;
+    ia3.y = INV ? a3.x : -a3.x;
     v0 = cadd(a0, a2);
     v2 = csub(a0, a2);
     v1 = cadd(a1, ia3);
@@ -110,29 +112,29 @@ __device__ __forceinline__ void radix4(cd &v0, cd &v1, cd &v2, cd &v3) {
 // strided Stockham writes over the shared-memory banks
 __device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
 
-template <bool INV>
-__device__ __forceinline__ cd twid(const cd *tw, int i) {
-    cd w = tw[i];
+template <bool INV, typename C>
+__device__ __forceinline__ C twid(const C *tw, int i) {
+    C w = tw[i];
     return INV ? cconj(w) : w;
 }
 
-template <int P, bool INV>
-__device__ __forceinline__ void fft_line(cd *s, const cd *tw, int t) {
+template <int P, bool INV, typename C>
+__device__ __forceinline__ void fft_line(C *s, const C *tw, int t) {
     constexpr int L = Log2<P>::v;
     constexpr int NB = P / 4;
     int Ns = 1;
 #pragma unroll
     for (int st = 0; st < L / 2; ++st) {
         const int j = t;
-        cd v0 = s[pidx(j)], v1 = s[pidx(j + NB)], v2 = s[pidx(j + 2 * NB)], v3 = s[pidx(j + 3 * NB)];
+        C v0 = s[pidx(j)], v1 = s[pidx(j + NB)], v2 = s[pidx(j + 2 * NB)], v3 = s[pidx(j + 3 * NB)];
         const int kk = j & (Ns - 1);
         if (Ns > 1) {
             const int step = P / (Ns * 4);
-            v1 = cmul(v1, twid<INV>(tw, kk * step));
-            v2 = cmul(v2, twid<INV>(tw, 2 * kk * step));
-            v3 = cmul(v3, twid<INV>(tw, 3 * kk * step));
+            v1 = cmul(v1, twid<INV, C>(tw, kk * step));
+            v2 = cmul(v2, twid<INV, C>(tw, 2 * kk * step));
+            v3 = cmul(v3, twid<INV, C>(tw, 3 * kk * step));
         }
-        radix4<INV>(v0, v1, v2, v3);
+        radix4<INV, C>(v0, v1, v2, v3);
         __syncthreads();
         const int idx = (j / Ns) * Ns * 4 + kk;
         s[pidx(idx)] = v0;
@@ -143,12 +145,12 @@ __device__ __forceinline__ void fft_line(cd *s, const cd *tw, int t) {
         Ns *= 4;
     }
     if (L & 1) {   // radix-2 stage, Ns = P/2: butterflies j = t, t + NB
-        cd a[2], b[2];
+        C a[2], b[2];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
             const int j = t + q * NB;
             a[q] = s[pidx(j)];
-            b[q] = cmul(s[pidx(j + P / 2)], twid<INV>(tw, j));
+            b[q] = cmul(s[pidx(j + P / 2)], twid<INV, C>(tw, j));
         }
         __syncthreads();
 #pragma unroll
@@ -176,7 +178,8 @@ __device__ __forceinline__ int fold(int u, int P) { return u <= P - u ? u : P - 
 
 // node value of grid g at node (x,y,z) from the box partial sums: every box
 // whose 3x3x3 node block contains the node contributes its local sum
-__device__ __forceinline__ cd node_value(const cd *__restrict__ bp, const GridDims &G, int g, int x, int y, int z) {
+template <typename C>
+__device__ __forceinline__ C node_value(const C *__restrict__ bp, const GridDims &G, int g, int x, int y, int z) {
     int bxs[2], axs[2], nbx = 0, bys[2], ays[2], nby = 0, bzs[2], azs[2], nbz = 0;
     int b = x >> 1;
     if (b < G.ncx) { bxs[nbx] = b; axs[nbx++] = x - 2 * b; }
@@ -187,7 +190,7 @@ __device__ __forceinline__ cd node_value(const cd *__restrict__ bp, const GridDi
     b = z >> 1;
     if (b < G.ncz) { bzs[nbz] = b; azs[nbz++] = z - 2 * b; }
     if (!(z & 1) && z >= 2 && b - 1 < G.ncz) { bzs[nbz] = b - 1; azs[nbz++] = 2; }
-    cd v = cmk(0, 0);
+    C v = czero<C>();
     for (int iz = 0; iz < nbz; ++iz)
         for (int iy = 0; iy < nby; ++iy)
             for (int ix = 0; ix < nbx; ++ix) {
@@ -200,146 +203,146 @@ __device__ __forceinline__ cd node_value(const cd *__restrict__ bp, const GridDi
 
 // X forward: lines (y < Ny, z < Nz) of grid (g, r); node assembly on load,
 // zero padding x >= Nx.  W[(rg)][(z*Py + y)*Px + x]
-template <int P>
+template <int P, typename Cx>
 __global__ void __launch_bounds__(FftCfg<P>::THREADS)
-k_fft_x_fwd(const cd *__restrict__ bpart, cd *__restrict__ W, const cd *__restrict__ twg, GridDims G, const int *done) {
+k_fft_x_fwd(const Cx *__restrict__ bpart, Cx *__restrict__ W, const Cx *__restrict__ twg, GridDims G, const int *done) {
     if (done && done[blockIdx.y >> 2]) return;
-    using C = FftCfg<P>;
-    __shared__ cd sh[C::LPB * C::LS];
-    __shared__ cd tw[P];
+    using Cf = FftCfg<P>;
+    __shared__ Cx sh[Cf::LPB * Cf::LS];
+    __shared__ Cx tw[P];
     const int rg = blockIdx.y;                 // r*4 + g
     const int g = rg & 3, r = rg >> 2;
-    const cd *bp = bpart + (long long)r * G.ncubes * 4 * 27;
+    const Cx *bp = bpart + (long long)r * G.ncubes * 4 * 27;
     for (int i = threadIdx.x; i < P; i += blockDim.x) tw[i] = twg[i];
     const int nlines = G.Ny * G.Nz;
-    const int line0 = blockIdx.x * C::LPB;
-    for (int e = threadIdx.x; e < C::LPB * P; e += blockDim.x) {
+    const int line0 = blockIdx.x * Cf::LPB;
+    for (int e = threadIdx.x; e < Cf::LPB * P; e += blockDim.x) {
         const int l = e / P, x = e - l * P, line = line0 + l;
-        cd v = cmk(0, 0);
+        Cx v = czero<Cx>();
         if (line < nlines && x < G.Nx) {
             const int y = line % G.Ny, z = line / G.Ny;
-            v = node_value(bp, G, g, x, y, z);
+            v = node_value<Cx>(bp, G, g, x, y, z);
         }
-        sh[l * C::LS + pidx(x)] = v;
+        sh[l * Cf::LS + pidx(x)] = v;
     }
     __syncthreads();
-    const int l = threadIdx.x / C::TPL, t = threadIdx.x - l * C::TPL;
-    fft_line<P, false>(sh + l * C::LS, tw, t);
-    cd *Wr = W + (long long)rg * G.Px * G.Py * G.Nz;
-    for (int e = threadIdx.x; e < C::LPB * P; e += blockDim.x) {
+    const int l = threadIdx.x / Cf::TPL, t = threadIdx.x - l * Cf::TPL;
+    fft_line<P, false, Cx>(sh + l * Cf::LS, tw, t);
+    Cx *Wr = W + (long long)rg * G.Px * G.Py * G.Nz;
+    for (int e = threadIdx.x; e < Cf::LPB * P; e += blockDim.x) {
         const int ll = e / P, x = e - ll * P, line = line0 + ll;
         if (line < nlines) {
             const int y = line % G.Ny, z = line / G.Ny;
-            Wr[((long long)z * G.Py + y) * G.Px + x] = sh[ll * C::LS + pidx(x)];
+            Wr[((long long)z * G.Py + y) * G.Px + x] = sh[ll * Cf::LS + pidx(x)];
         }
     }
 }
 
 // Y pass: lines (x < Px, z < Nz); forward reads y < Ny and writes y < Py,
 // inverse reads y < Py and writes y < Ny.  A CTA takes LPB consecutive x.
-template <int P, bool INV>
+template <int P, bool INV, typename Cx>
 __global__ void __launch_bounds__(FftCfg<P>::THREADS)
-k_fft_y(cd *__restrict__ W, const cd *__restrict__ twg, GridDims G, const int *done) {
+k_fft_y(Cx *__restrict__ W, const Cx *__restrict__ twg, GridDims G, const int *done) {
     if (done && done[blockIdx.y >> 2]) return;
-    using C = FftCfg<P>;
-    __shared__ cd sh[C::LPB * C::LS];
-    __shared__ cd tw[P];
+    using Cf = FftCfg<P>;
+    __shared__ Cx sh[Cf::LPB * Cf::LS];
+    __shared__ Cx tw[P];
     const int rg = blockIdx.y;
     for (int i = threadIdx.x; i < P; i += blockDim.x) tw[i] = twg[i];
-    const int xblocks = (G.Px + C::LPB - 1) / C::LPB;
-    const int z = blockIdx.x / xblocks, x0 = (blockIdx.x - z * xblocks) * C::LPB;
-    cd *Wr = W + (long long)rg * G.Px * G.Py * G.Nz + (long long)z * G.Py * G.Px;
+    const int xblocks = (G.Px + Cf::LPB - 1) / Cf::LPB;
+    const int z = blockIdx.x / xblocks, x0 = (blockIdx.x - z * xblocks) * Cf::LPB;
+    Cx *Wr = W + (long long)rg * G.Px * G.Py * G.Nz + (long long)z * G.Py * G.Px;
     const int nin = INV ? G.Py : G.Ny, nout = INV ? G.Ny : G.Py;
     // sh layout [line][y]
-    for (int e = threadIdx.x; e < C::LPB * P; e += blockDim.x) {
-        const int y = e / C::LPB, l = e - y * C::LPB, x = x0 + l;
-        cd v = cmk(0, 0);
+    for (int e = threadIdx.x; e < Cf::LPB * P; e += blockDim.x) {
+        const int y = e / Cf::LPB, l = e - y * Cf::LPB, x = x0 + l;
+        Cx v = czero<Cx>();
         if (y < nin && x < G.Px) v = Wr[(long long)y * G.Px + x];
-        sh[l * C::LS + pidx(y)] = v;
+        sh[l * Cf::LS + pidx(y)] = v;
     }
     __syncthreads();
-    const int l = threadIdx.x / C::TPL, t = threadIdx.x - l * C::TPL;
-    fft_line<P, INV>(sh + l * C::LS, tw, t);
-    for (int e = threadIdx.x; e < C::LPB * P; e += blockDim.x) {
-        const int y = e / C::LPB, ll = e - y * C::LPB, x = x0 + ll;
-        if (y < nout && x < G.Px) Wr[(long long)y * G.Px + x] = sh[ll * C::LS + pidx(y)];
+    const int l = threadIdx.x / Cf::TPL, t = threadIdx.x - l * Cf::TPL;
+    fft_line<P, INV, Cx>(sh + l * Cf::LS, tw, t);
+    for (int e = threadIdx.x; e < Cf::LPB * P; e += blockDim.x) {
+        const int y = e / Cf::LPB, ll = e - y * Cf::LPB, x = x0 + ll;
+        if (y < nout && x < G.Px) Wr[(long long)y * G.Px + x] = sh[ll * Cf::LS + pidx(y)];
     }
 }
 
 // Z pass: lines (x < Px, y < Py), forward FFT of z < Nz (zero padded), times
 // the Green octant Fo (folded by evenness), inverse FFT, keep z < Nz.
-template <int P>
+template <int P, typename Cx>
 __global__ void __launch_bounds__(FftCfg<P>::THREADS)
-k_fft_z(cd *__restrict__ W, const cd *__restrict__ Fo, const cd *__restrict__ twg, GridDims G, const int *done) {
+k_fft_z(Cx *__restrict__ W, const Cx *__restrict__ Fo, const Cx *__restrict__ twg, GridDims G, const int *done) {
     if (done && done[blockIdx.y >> 2]) return;
-    using C = FftCfg<P>;
-    __shared__ cd sh[C::LPB * C::LS];
-    __shared__ cd tw[P];
+    using Cf = FftCfg<P>;
+    __shared__ Cx sh[Cf::LPB * Cf::LS];
+    __shared__ Cx tw[P];
     const int rg = blockIdx.y;
     for (int i = threadIdx.x; i < P; i += blockDim.x) tw[i] = twg[i];
-    const int xblocks = (G.Px + C::LPB - 1) / C::LPB;
-    const int y = blockIdx.x / xblocks, x0 = (blockIdx.x - y * xblocks) * C::LPB;
+    const int xblocks = (G.Px + Cf::LPB - 1) / Cf::LPB;
+    const int y = blockIdx.x / xblocks, x0 = (blockIdx.x - y * xblocks) * Cf::LPB;
     const long long plane = (long long)G.Px * G.Py;
-    cd *Wr = W + (long long)rg * plane * G.Nz + (long long)y * G.Px;
-    for (int e = threadIdx.x; e < C::LPB * P; e += blockDim.x) {
-        const int z = e / C::LPB, l = e - z * C::LPB, x = x0 + l;
-        cd v = cmk(0, 0);
+    Cx *Wr = W + (long long)rg * plane * G.Nz + (long long)y * G.Px;
+    for (int e = threadIdx.x; e < Cf::LPB * P; e += blockDim.x) {
+        const int z = e / Cf::LPB, l = e - z * Cf::LPB, x = x0 + l;
+        Cx v = czero<Cx>();
         if (z < G.Nz && x < G.Px) v = Wr[(long long)z * plane + x];
-        sh[l * C::LS + pidx(z)] = v;
+        sh[l * Cf::LS + pidx(z)] = v;
     }
     __syncthreads();
-    const int l = threadIdx.x / C::TPL, t = threadIdx.x - l * C::TPL;
-    fft_line<P, false>(sh + l * C::LS, tw, t);
+    const int l = threadIdx.x / Cf::TPL, t = threadIdx.x - l * Cf::TPL;
+    fft_line<P, false, Cx>(sh + l * Cf::LS, tw, t);
     const int fy = fold(y, G.Py);
     // consecutive threads take consecutive lines (x), so the octant reads of
     // one z plane are contiguous
-    for (int e = threadIdx.x; e < C::LPB * P; e += blockDim.x) {
-        const int z = e / C::LPB, ll = e - z * C::LPB, x = x0 + ll;
+    for (int e = threadIdx.x; e < Cf::LPB * P; e += blockDim.x) {
+        const int z = e / Cf::LPB, ll = e - z * Cf::LPB, x = x0 + ll;
         if (x < G.Px) {
-            const cd f = __ldg(&Fo[((long long)fold(z, G.Pz) * G.Hy + fy) * G.Hx + fold(x, G.Px)]);
-            sh[ll * C::LS + pidx(z)] = cmul(f, sh[ll * C::LS + pidx(z)]);
+            const Cx f = __ldg(&Fo[((long long)fold(z, G.Pz) * G.Hy + fy) * G.Hx + fold(x, G.Px)]);
+            sh[ll * Cf::LS + pidx(z)] = cmul(f, sh[ll * Cf::LS + pidx(z)]);
         }
     }
     __syncthreads();
-    fft_line<P, true>(sh + l * C::LS, tw, t);
-    for (int e = threadIdx.x; e < C::LPB * P; e += blockDim.x) {
-        const int z = e / C::LPB, ll = e - z * C::LPB, x = x0 + ll;
-        if (z < G.Nz && x < G.Px) Wr[(long long)z * plane + x] = sh[ll * C::LS + pidx(z)];
+    fft_line<P, true, Cx>(sh + l * Cf::LS, tw, t);
+    for (int e = threadIdx.x; e < Cf::LPB * P; e += blockDim.x) {
+        const int z = e / Cf::LPB, ll = e - z * Cf::LPB, x = x0 + ll;
+        if (z < G.Nz && x < G.Px) Wr[(long long)z * plane + x] = sh[ll * Cf::LS + pidx(z)];
     }
 }
 
 // X inverse: lines (y < Ny, z < Nz), keep x < Nx, write the result grid
 // R[(rg)][(z*Ny + y)*Nx + x]
-template <int P>
+template <int P, typename Cx>
 __global__ void __launch_bounds__(FftCfg<P>::THREADS)
-k_fft_x_inv(const cd *__restrict__ W, cd *__restrict__ R, const cd *__restrict__ twg, GridDims G, const int *done) {
+k_fft_x_inv(const Cx *__restrict__ W, Cx *__restrict__ R, const Cx *__restrict__ twg, GridDims G, const int *done) {
     if (done && done[blockIdx.y >> 2]) return;
-    using C = FftCfg<P>;
-    __shared__ cd sh[C::LPB * C::LS];
-    __shared__ cd tw[P];
+    using Cf = FftCfg<P>;
+    __shared__ Cx sh[Cf::LPB * Cf::LS];
+    __shared__ Cx tw[P];
     const int rg = blockIdx.y;
     for (int i = threadIdx.x; i < P; i += blockDim.x) tw[i] = twg[i];
     const int nlines = G.Ny * G.Nz;
-    const int line0 = blockIdx.x * C::LPB;
-    const cd *Wr = W + (long long)rg * G.Px * G.Py * G.Nz;
-    for (int e = threadIdx.x; e < C::LPB * P; e += blockDim.x) {
+    const int line0 = blockIdx.x * Cf::LPB;
+    const Cx *Wr = W + (long long)rg * G.Px * G.Py * G.Nz;
+    for (int e = threadIdx.x; e < Cf::LPB * P; e += blockDim.x) {
         const int l = e / P, x = e - l * P, line = line0 + l;
-        cd v = cmk(0, 0);
+        Cx v = czero<Cx>();
         if (line < nlines) {
             const int y = line % G.Ny, z = line / G.Ny;
             v = Wr[((long long)z * G.Py + y) * G.Px + x];
         }
-        sh[l * C::LS + pidx(x)] = v;
+        sh[l * Cf::LS + pidx(x)] = v;
     }
     __syncthreads();
-    const int l = threadIdx.x / C::TPL, t = threadIdx.x - l * C::TPL;
-    fft_line<P, true>(sh + l * C::LS, tw, t);
-    cd *Rr = R + (long long)rg * G.Nx * G.Ny * G.Nz;
-    for (int e = threadIdx.x; e < C::LPB * P; e += blockDim.x) {
+    const int l = threadIdx.x / Cf::TPL, t = threadIdx.x - l * Cf::TPL;
+    fft_line<P, true, Cx>(sh + l * Cf::LS, tw, t);
+    Cx *Rr = R + (long long)rg * G.Nx * G.Ny * G.Nz;
+    for (int e = threadIdx.x; e < Cf::LPB * P; e += blockDim.x) {
         const int ll = e / P, x = e - ll * P, line = line0 + ll;
         if (line < nlines && x < G.Nx) {
             const int y = line % G.Ny, z = line / G.Ny;
-            Rr[((long long)z * G.Ny + y) * G.Nx + x] = sh[ll * C::LS + pidx(x)];
+            Rr[((long long)z * G.Ny + y) * G.Nx + x] = sh[ll * Cf::LS + pidx(x)];
         }
     }
 }
@@ -382,10 +385,10 @@ __device__ __forceinline__ void copy_row_async(ST *dst, const ST *src, int nel, 
 
 constexpr int NZ_WARPS = 4;
 
-template <typename ST, int U, int RG>
+template <typename ST, typename C, int U, int RG>
 __global__ void __launch_bounds__(32 * NZ_WARPS)
-k_near_warp(const NearTile *__restrict__ tiles, int ntiles, const ST *__restrict__ data, const cd *__restrict__ x,
-            long long ld, const int *__restrict__ cube_off, cd *__restrict__ part, long long part_len,
+k_near_warp(const NearTile *__restrict__ tiles, int ntiles, const ST *__restrict__ data, const C *__restrict__ x,
+            long long ld, const int *__restrict__ cube_off, C *__restrict__ part, long long part_len,
             const int *skip, int nrhs, int row_cap) {
     extern __shared__ __align__(16) unsigned char nz_sh[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -400,17 +403,17 @@ k_near_warp(const NearTile *__restrict__ tiles, int ntiles, const ST *__restrict
     const int nel = 9 * n2;
     for (int r0 = 0; r0 < nrhs; r0 += RG) {
         bool act[RG];
-        cd y[RG][U][3], ca[RG][U][3];
+        C y[RG][U][3], ca[RG][U][3];
 #pragma unroll
         for (int rr = 0; rr < RG; ++rr) {
             const int r = r0 + rr;
             act[rr] = r < nrhs && !(skip && skip[r]);
-            const cd *x2 = x + r * ld + 3LL * s2;
+            const C *x2 = x + r * ld + 3LL * s2;
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int j = lane + 32 * u;
-                ca[rr][u][0] = ca[rr][u][1] = ca[rr][u][2] = cmk(0, 0);
-                y[rr][u][0] = y[rr][u][1] = y[rr][u][2] = cmk(0, 0);
+                ca[rr][u][0] = ca[rr][u][1] = ca[rr][u][2] = czero<C>();
+                y[rr][u][0] = y[rr][u][1] = y[rr][u][2] = czero<C>();
                 if (act[rr] && j < n2) { y[rr][u][0] = x2[3 * j]; y[rr][u][1] = x2[3 * j + 1]; y[rr][u][2] = x2[3 * j + 2]; }
             }
         }
@@ -425,20 +428,20 @@ k_near_warp(const NearTile *__restrict__ tiles, int ntiles, const ST *__restrict
                 cp_async_wait<0>();
             }
             __syncwarp();
-            cd m[U][9];
+            C m[U][9];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int j = lane + 32 * u;
 #pragma unroll
-                for (int q = 0; q < 9; ++q) m[u][q] = (j < n2) ? widen(cur[9 * j + q]) : cmk(0, 0);
+                for (int q = 0; q < 9; ++q) m[u][q] = (j < n2) ? as_c<C>(cur[9 * j + q]) : czero<C>();
             }
             __syncwarp();      // the ring slot may be refilled after this
 #pragma unroll
             for (int rr = 0; rr < RG; ++rr) {
                 if (!act[rr]) continue;           // uniform across the warp
-                const cd *x1 = x + (r0 + rr) * ld + 3LL * s1;
-                const cd xa0 = x1[3 * i], xa1 = x1[3 * i + 1], xa2 = x1[3 * i + 2];
-                cd t0 = cmk(0, 0), t1 = t0, t2 = t0;
+                const C *x1 = x + (r0 + rr) * ld + 3LL * s1;
+                const C xa0 = x1[3 * i], xa1 = x1[3 * i + 1], xa2 = x1[3 * i + 2];
+                C t0 = czero<C>(), t1 = t0, t2 = t0;
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
                     cfma(t0, m[u][0], y[rr][u][0]); cfma(t1, m[u][1], y[rr][u][0]); cfma(t2, m[u][2], y[rr][u][0]);
@@ -459,7 +462,7 @@ k_near_warp(const NearTile *__restrict__ tiles, int ntiles, const ST *__restrict
                     t2.x += __shfl_xor_sync(0xffffffffu, t2.x, o);
                     t2.y += __shfl_xor_sync(0xffffffffu, t2.y, o);
                 }
-                cd *pr = part + (r0 + rr) * part_len + tl.row_off + 3 * i;
+                C *pr = part + (r0 + rr) * part_len + tl.row_off + 3 * i;
                 if (lane == 0) pr[0] = t0;
                 else if (lane == 1) pr[1] = t1;
                 else if (lane == 2) pr[2] = t2;
@@ -469,7 +472,7 @@ k_near_warp(const NearTile *__restrict__ tiles, int ntiles, const ST *__restrict
 #pragma unroll
             for (int rr = 0; rr < RG; ++rr) {
                 if (!act[rr]) continue;
-                cd *pc = part + (r0 + rr) * part_len + tl.col_off;
+                C *pc = part + (r0 + rr) * part_len + tl.col_off;
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
                     const int j = lane + 32 * u;
@@ -492,12 +495,13 @@ k_near_warp(const NearTile *__restrict__ tiles, int ntiles, const ST *__restrict
 // 27-term sums from the projector rows P[(g*27 + j)*T + slot] (coalesced
 // across lanes), adds the cube's near-zone partial slots in slot order and
 // writes Ax = near + (Y2 - k^2 Y).
-template <int GA_RG>
+template <typename C, int GA_RG>
 __global__ void __launch_bounds__(32 * WARPS_PER_CTA)
-k_gather(const cd *__restrict__ Rg, const cd *__restrict__ P, int T, const int *__restrict__ cube_off, GridDims G,
-         double k2, const cd *__restrict__ part, long long part_len, const long long *__restrict__ pslot_base,
-         const int *__restrict__ pslot_cnt, cd *__restrict__ y, long long ld, const int *skip, int nrhs) {
-    __shared__ cd Rs[WARPS_PER_CTA][GA_RG][4][27];
+k_gather(const C *__restrict__ Rg, const C *__restrict__ P, int T, const int *__restrict__ cube_off, GridDims G,
+         typename CReal<C>::type k2, const C *__restrict__ part, long long part_len,
+         const long long *__restrict__ pslot_base, const int *__restrict__ pslot_cnt, C *__restrict__ y, long long ld,
+         const int *skip, int nrhs) {
+    __shared__ C Rs[WARPS_PER_CTA][GA_RG][4][27];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c = blockIdx.x * WARPS_PER_CTA + warp;
     if (c >= G.ncubes) return;
@@ -520,7 +524,7 @@ k_gather(const cd *__restrict__ Rg, const cd *__restrict__ P, int T, const int *
             for (int q = 0; q < GA_RG; ++q) {
                 const int r = r0 + q;
                 if (r < nrhs) {
-                    const cd *Rr = Rg + (long long)r * 4 * NN;
+                    const C *Rr = Rg + (long long)r * 4 * NN;
 #pragma unroll
                     for (int g = 0; g < 4; ++g) Rs[warp][q][g][lane] = Rr[g * NN + node];
                 }
@@ -529,21 +533,21 @@ k_gather(const cd *__restrict__ Rg, const cd *__restrict__ P, int T, const int *
         __syncwarp();
         for (int sl = lane; sl < nc; sl += 32) {
             const int s = s0 + sl;
-            cd acc[GA_RG][6];
+            C acc[GA_RG][6];
 #pragma unroll
             for (int q = 0; q < GA_RG; ++q)
 #pragma unroll
-                for (int v = 0; v < 6; ++v) acc[q][v] = cmk(0, 0);
+                for (int v = 0; v < 6; ++v) acc[q][v] = czero<C>();
 #pragma unroll 3
             for (int j = 0; j < 27; ++j) {
-                const cd p0 = P[(size_t)j * T + s], px = P[(size_t)(27 + j) * T + s];
-                const cd py = P[(size_t)(54 + j) * T + s], pz = P[(size_t)(81 + j) * T + s];
+                const C p0 = P[(size_t)j * T + s], px = P[(size_t)(27 + j) * T + s];
+                const C py = P[(size_t)(54 + j) * T + s], pz = P[(size_t)(81 + j) * T + s];
 #pragma unroll
                 for (int q = 0; q < GA_RG; ++q) {
                     cfma(acc[q][0], p0, Rs[warp][q][0][j]);
                     cfma(acc[q][1], p0, Rs[warp][q][1][j]);
                     cfma(acc[q][2], p0, Rs[warp][q][2][j]);
-                    const cd r3 = Rs[warp][q][3][j];
+                    const C r3 = Rs[warp][q][3][j];
                     cfma(acc[q][3], px, r3);
                     cfma(acc[q][4], py, r3);
                     cfma(acc[q][5], pz, r3);
@@ -553,14 +557,14 @@ k_gather(const cd *__restrict__ Rg, const cd *__restrict__ P, int T, const int *
             for (int q = 0; q < GA_RG; ++q) {
                 const int r = r0 + q;
                 if (r >= nrhs || (skip && skip[r])) continue;
-                const cd *pr = part + r * part_len + pbase + 3 * sl;
-                cd *yr = y + r * ld + 3LL * s;
+                const C *pr = part + r * part_len + pbase + 3 * sl;
+                C *yr = y + r * ld + 3LL * s;
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
-                    cd nz = cmk(0, 0);
+                    C nz = czero<C>();
 #pragma unroll 8
                     for (int t = 0; t < nslot; ++t) nz = cadd(nz, pr[(long long)t * 3 * nc + d]);
-                    const cd far = csub_scaled(acc[q][3 + d], k2, acc[q][d]);
+                    const C far = csub_scaled(acc[q][3 + d], k2, acc[q][d]);
                     yr[d] = cadd(nz, far);
                 }
             }
@@ -577,6 +581,11 @@ __global__ void k_twiddles(cd *tw, int P) {
     }
 }
 
+__global__ void k_narrow(const cd *in, cf *out, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = make_float2((float)in[i].x, (float)in[i].y);
+}
+
 GridDims dims_of(const scd_ctx *c) {
     GridDims G;
     G.Nx = c->Nx; G.Ny = c->Ny; G.Nz = c->Nz;
@@ -586,41 +595,50 @@ GridDims dims_of(const scd_ctx *c) {
     return G;
 }
 
-}  // namespace
+// operator copies and work buffers of one precision
+template <typename C> struct Res;
+template <> struct Res<cd> {
+    static const cd *P(scd_ctx *c) { return c->d_P; }
+    static const cd *Fo(scd_ctx *c) { return c->d_Fo; }
+    static const cd *tw(scd_ctx *c, int a) { return c->d_tw[a]; }
+    static cd *bpart(scd_ctx *c) { return c->d_bpart; }
+    static cd *W(scd_ctx *c) { return c->d_W; }
+    static cd *R(scd_ctx *c) { return c->d_R; }
+    static cd *part(scd_ctx *c) { return c->d_nzpart; }
+};
+template <> struct Res<cf> {
+    static const cf *P(scd_ctx *c) { return c->f_P; }
+    static const cf *Fo(scd_ctx *c) { return c->f_Fo; }
+    static const cf *tw(scd_ctx *c, int a) { return c->f_tw[a]; }
+    static cf *bpart(scd_ctx *c) { return c->f_bpart; }
+    static cf *W(scd_ctx *c) { return c->f_W; }
+    static cf *R(scd_ctx *c) { return c->f_R; }
+    static cf *part(scd_ctx *c) { return c->f_nzpart; }
+};
 
-// twiddle table exp(-2 pi i j / P), j < P
-int build_twiddles(scd_ctx *c, int P, cd **out) {
-    cudaError_t e = cudaMalloc(out, sizeof(cd) * P);
-    if (e != cudaSuccess) return check_cuda(c, e, "twiddles");
-    k_twiddles<<<(P + 255) / 256, 256, 0, c->st>>>(*out, P);
-    return check_cuda(c, cudaGetLastError(), "twiddles");
+template <int P, typename C>
+void fft_x_fwd_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const C *tw) {
+    using Cf = FftCfg<P>;
+    dim3 grid((G.Ny * G.Nz + Cf::LPB - 1) / Cf::LPB, nrg);
+    k_fft_x_fwd<P, C><<<grid, Cf::THREADS, 0, c->st>>>(Res<C>::bpart(c), Res<C>::W(c), tw, G, done);
 }
-
-namespace {
-
-template <int P>
-void fft_x_fwd_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const cd *tw) {
-    using C = FftCfg<P>;
-    dim3 grid((G.Ny * G.Nz + C::LPB - 1) / C::LPB, nrg);
-    k_fft_x_fwd<P><<<grid, C::THREADS, 0, c->st>>>(c->d_bpart, c->d_W, tw, G, done);
+template <int P, bool INV, typename C>
+void fft_y_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const C *tw) {
+    using Cf = FftCfg<P>;
+    dim3 grid(((G.Px + Cf::LPB - 1) / Cf::LPB) * G.Nz, nrg);
+    k_fft_y<P, INV, C><<<grid, Cf::THREADS, 0, c->st>>>(Res<C>::W(c), tw, G, done);
 }
-template <int P, bool INV>
-void fft_y_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const cd *tw) {
-    using C = FftCfg<P>;
-    dim3 grid(((G.Px + C::LPB - 1) / C::LPB) * G.Nz, nrg);
-    k_fft_y<P, INV><<<grid, C::THREADS, 0, c->st>>>(c->d_W, tw, G, done);
+template <int P, typename C>
+void fft_z_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const C *tw) {
+    using Cf = FftCfg<P>;
+    dim3 grid(((G.Px + Cf::LPB - 1) / Cf::LPB) * G.Py, nrg);
+    k_fft_z<P, C><<<grid, Cf::THREADS, 0, c->st>>>(Res<C>::W(c), Res<C>::Fo(c), tw, G, done);
 }
-template <int P>
-void fft_z_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const cd *tw) {
-    using C = FftCfg<P>;
-    dim3 grid(((G.Px + C::LPB - 1) / C::LPB) * G.Py, nrg);
-    k_fft_z<P><<<grid, C::THREADS, 0, c->st>>>(c->d_W, c->d_Fo, tw, G, done);
-}
-template <int P>
-void fft_x_inv_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const cd *tw) {
-    using C = FftCfg<P>;
-    dim3 grid((G.Ny * G.Nz + C::LPB - 1) / C::LPB, nrg);
-    k_fft_x_inv<P><<<grid, C::THREADS, 0, c->st>>>(c->d_W, c->d_R, tw, G, done);
+template <int P, typename C>
+void fft_x_inv_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const C *tw) {
+    using Cf = FftCfg<P>;
+    dim3 grid((G.Ny * G.Nz + Cf::LPB - 1) / Cf::LPB, nrg);
+    k_fft_x_inv<P, C><<<grid, Cf::THREADS, 0, c->st>>>(Res<C>::W(c), Res<C>::R(c), tw, G, done);
 }
 
 #define SCD_DISPATCH_P(PV, CALL)                     \
@@ -635,38 +653,28 @@ void fft_x_inv_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const 
         default: break;                              \
     }
 
-}  // namespace
-
-void launch_permute_in(scd_ctx *c, const cd *x_orig, cd *x_slot, int nrhs, long long ld) {
-    dim3 grid((unsigned)std::min<long long>((3LL * c->T + 255) / 256, 4096), nrhs);
-    k_permute_in<<<grid, 256, 0, c->st>>>(x_orig, x_slot, c->d_perm, c->T, ld);
-}
-
-void launch_permute_out(scd_ctx *c, const cd *x_slot, cd *x_orig, int nrhs, long long ld) {
-    dim3 grid((unsigned)std::min<long long>((3LL * c->T + 255) / 256, 4096), nrhs);
-    k_permute_out<<<grid, 256, 0, c->st>>>(x_slot, x_orig, c->d_perm, c->T, ld);
-}
-
-void launch_fft_chain(scd_ctx *c, const cd *x, int nrhs, const int *done) {
+template <typename C>
+void fft_chain_t(scd_ctx *c, const C *x, int nrhs, const int *done) {
     const GridDims G = dims_of(c);
     {
         dim3 grid((c->ncubes + WARPS_PER_CTA - 1) / WARPS_PER_CTA);
+        const C *P = Res<C>::P(c);
         if (nrhs >= 8)
-            k_scatter<8><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(x, c->n, c->d_P, c->T, c->d_cube_off, c->ncubes,
-                                                                 c->d_bpart, done, nrhs);
+            k_scatter<C, 8><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(x, c->n, P, c->T, c->d_cube_off, c->ncubes,
+                                                                    Res<C>::bpart(c), done, nrhs);
         else if (nrhs >= 4)
-            k_scatter<4><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(x, c->n, c->d_P, c->T, c->d_cube_off, c->ncubes,
-                                                                 c->d_bpart, done, nrhs);
+            k_scatter<C, 4><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(x, c->n, P, c->T, c->d_cube_off, c->ncubes,
+                                                                    Res<C>::bpart(c), done, nrhs);
         else
-            k_scatter<1><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(x, c->n, c->d_P, c->T, c->d_cube_off, c->ncubes,
-                                                                 c->d_bpart, done, nrhs);
+            k_scatter<C, 1><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(x, c->n, P, c->T, c->d_cube_off, c->ncubes,
+                                                                    Res<C>::bpart(c), done, nrhs);
     }
     const int nrg = 4 * nrhs;
-#define XF(P) fft_x_fwd_t<P>(c, G, nrg, done, c->d_tw[0])
-#define YF(P) fft_y_t<P, false>(c, G, nrg, done, c->d_tw[1])
-#define ZC(P) fft_z_t<P>(c, G, nrg, done, c->d_tw[2])
-#define YI(P) fft_y_t<P, true>(c, G, nrg, done, c->d_tw[1])
-#define XI(P) fft_x_inv_t<P>(c, G, nrg, done, c->d_tw[0])
+#define XF(PP) fft_x_fwd_t<PP, C>(c, G, nrg, done, Res<C>::tw(c, 0))
+#define YF(PP) fft_y_t<PP, false, C>(c, G, nrg, done, Res<C>::tw(c, 1))
+#define ZC(PP) fft_z_t<PP, C>(c, G, nrg, done, Res<C>::tw(c, 2))
+#define YI(PP) fft_y_t<PP, true, C>(c, G, nrg, done, Res<C>::tw(c, 1))
+#define XI(PP) fft_x_inv_t<PP, C>(c, G, nrg, done, Res<C>::tw(c, 0))
     SCD_DISPATCH_P(c->Px, XF)
     SCD_DISPATCH_P(c->Py, YF)
     SCD_DISPATCH_P(c->Pz, ZC)
@@ -680,60 +688,141 @@ void launch_fft_chain(scd_ctx *c, const cd *x, int nrhs, const int *done) {
     c->launches += 6;
 }
 
-template <typename ST, int U>
-static void near_dispatch_u(scd_ctx *c, const ST *data, const cd *x, int nrhs, const int *done) {
+template <typename ST, typename C, int U>
+void near_dispatch_u(scd_ctx *c, const ST *data, const C *x, int nrhs, const int *done) {
     const int row_cap = 9 * c->max_per_cube;
     const size_t sh = sizeof(ST) * 2 * (size_t)row_cap * NZ_WARPS;
     const int grid = (c->ntiles + NZ_WARPS - 1) / NZ_WARPS;
+    C *part = Res<C>::part(c);
     if (nrhs >= 4) {
-        cudaFuncSetAttribute(k_near_warp<ST, U, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-        k_near_warp<ST, U, 4><<<grid, 32 * NZ_WARPS, sh, c->st>>>(c->d_tiles, c->ntiles, data, x, c->n, c->d_cube_off,
-                                                                 c->d_nzpart, c->part_len, done, nrhs, row_cap);
+        cudaFuncSetAttribute(k_near_warp<ST, C, U, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+        k_near_warp<ST, C, U, 4><<<grid, 32 * NZ_WARPS, sh, c->st>>>(c->d_tiles, c->ntiles, data, x, c->n,
+                                                                    c->d_cube_off, part, c->part_len, done, nrhs, row_cap);
     } else if (nrhs >= 2) {
-        cudaFuncSetAttribute(k_near_warp<ST, U, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-        k_near_warp<ST, U, 2><<<grid, 32 * NZ_WARPS, sh, c->st>>>(c->d_tiles, c->ntiles, data, x, c->n, c->d_cube_off,
-                                                                 c->d_nzpart, c->part_len, done, nrhs, row_cap);
+        cudaFuncSetAttribute(k_near_warp<ST, C, U, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+        k_near_warp<ST, C, U, 2><<<grid, 32 * NZ_WARPS, sh, c->st>>>(c->d_tiles, c->ntiles, data, x, c->n,
+                                                                    c->d_cube_off, part, c->part_len, done, nrhs, row_cap);
     } else {
-        cudaFuncSetAttribute(k_near_warp<ST, U, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-        k_near_warp<ST, U, 1><<<grid, 32 * NZ_WARPS, sh, c->st>>>(c->d_tiles, c->ntiles, data, x, c->n, c->d_cube_off,
-                                                                 c->d_nzpart, c->part_len, done, nrhs, row_cap);
+        cudaFuncSetAttribute(k_near_warp<ST, C, U, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+        k_near_warp<ST, C, U, 1><<<grid, 32 * NZ_WARPS, sh, c->st>>>(c->d_tiles, c->ntiles, data, x, c->n,
+                                                                    c->d_cube_off, part, c->part_len, done, nrhs, row_cap);
     }
 }
 
-template <typename ST>
-static void near_dispatch(scd_ctx *c, const ST *data, const cd *x, int nrhs, const int *done) {
-    if (c->max_per_cube <= 32) near_dispatch_u<ST, 1>(c, data, x, nrhs, done);
-    else near_dispatch_u<ST, 2>(c, data, x, nrhs, done);
-}
-
-void launch_near(scd_ctx *c, const cd *x, int nrhs, const int *done) {
+template <typename C>
+void near_t(scd_ctx *c, const C *x, int nrhs, const int *done) {
     if (c->ntiles == 0) return;
-    if (c->near_prec == SCD_STORE_C64) near_dispatch(c, (const cf *)c->d_tdata, x, nrhs, done);
-    else near_dispatch(c, (const cd *)c->d_tdata, x, nrhs, done);
+    const bool u1 = c->max_per_cube <= 32;
+    if (c->near_prec == SCD_STORE_C64) {
+        if (u1) near_dispatch_u<cf, C, 1>(c, (const cf *)c->d_tdata, x, nrhs, done);
+        else near_dispatch_u<cf, C, 2>(c, (const cf *)c->d_tdata, x, nrhs, done);
+    } else {
+        if (u1) near_dispatch_u<cd, C, 1>(c, (const cd *)c->d_tdata, x, nrhs, done);
+        else near_dispatch_u<cd, C, 2>(c, (const cd *)c->d_tdata, x, nrhs, done);
+    }
     c->launches += 1;
 }
 
-void launch_gather(scd_ctx *c, const cd *x, cd *y, int nrhs, const int *done) {
-    (void)x;
+template <typename C>
+void gather_t(scd_ctx *c, C *y, int nrhs, const int *done) {
     const GridDims G = dims_of(c);
     dim3 grid((c->ncubes + WARPS_PER_CTA - 1) / WARPS_PER_CTA);
+    typedef typename CReal<C>::type R;
+    const R k2 = (R)(c->k * c->k);
     if (nrhs >= 4)
-        k_gather<4><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(c->d_R, c->d_P, c->T, c->d_cube_off, G, c->k * c->k,
-                                                            c->d_nzpart, c->part_len, c->d_pslot_base, c->d_pslot_cnt,
-                                                            y, c->n, done, nrhs);
+        k_gather<C, 4><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(Res<C>::R(c), Res<C>::P(c), c->T, c->d_cube_off, G, k2,
+                                                               Res<C>::part(c), c->part_len, c->d_pslot_base,
+                                                               c->d_pslot_cnt, y, c->n, done, nrhs);
     else
-        k_gather<1><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(c->d_R, c->d_P, c->T, c->d_cube_off, G, c->k * c->k,
-                                                            c->d_nzpart, c->part_len, c->d_pslot_base, c->d_pslot_cnt,
-                                                            y, c->n, done, nrhs);
+        k_gather<C, 1><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(Res<C>::R(c), Res<C>::P(c), c->T, c->d_cube_off, G, k2,
+                                                               Res<C>::part(c), c->part_len, c->d_pslot_base,
+                                                               c->d_pslot_cnt, y, c->n, done, nrhs);
     c->launches += 1;
 }
 
-void run_matvec(scd_ctx *c, const cd *x, cd *y, int nrhs, const int *done) {
+template <typename C>
+void run_matvec_t(scd_ctx *c, const C *x, C *y, int nrhs, const int *done) {
     if (c->timing) cudaEventRecord(c->ev[0], c->st);
-    launch_near(c, x, nrhs, done);
+    near_t<C>(c, x, nrhs, done);
     if (c->timing) cudaEventRecord(c->ev[1], c->st);
-    launch_fft_chain(c, x, nrhs, done);
+    fft_chain_t<C>(c, x, nrhs, done);
     if (c->timing) cudaEventRecord(c->ev[2], c->st);
-    launch_gather(c, x, y, nrhs, done);
+    gather_t<C>(c, y, nrhs, done);
     if (c->timing) cudaEventRecord(c->ev[3], c->st);
 }
+
+}  // namespace
+
+// twiddle table exp(-2 pi i j / P), j < P
+int build_twiddles(scd_ctx *c, int P, cd **out) {
+    cudaError_t e = cudaMalloc(out, sizeof(cd) * P);
+    if (e != cudaSuccess) return check_cuda(c, e, "twiddles");
+    k_twiddles<<<(P + 255) / 256, 256, 0, c->st>>>(*out, P);
+    return check_cuda(c, cudaGetLastError(), "twiddles");
+}
+
+// complex64 copies of the projectors, the Green octant and the twiddles for
+// the mixed-precision inner solves (rounded from the FP64 operator)
+int ensure_single(scd_ctx *c) {
+    if (c->f_ready) return SCD_OK;
+    const long long np = 4LL * 27 * c->T, no = (long long)c->Hx * c->Hy * c->Hz;
+    auto al = [&](cf **p, long long n) -> int {
+        if (*p) { cudaFree(*p); *p = nullptr; }
+        if (cudaMalloc(p, sizeof(cf) * (size_t)std::max<long long>(n, 1)) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(c, SCD_OOM, "complex64 operator copy");
+        }
+        return SCD_OK;
+    };
+    int rc;
+    if ((rc = al(&c->f_P, np)) || (rc = al(&c->f_Fo, no))) return rc;
+    k_narrow<<<1024, 256, 0, c->st>>>(c->d_P, c->f_P, np);
+    k_narrow<<<1024, 256, 0, c->st>>>(c->d_Fo, c->f_Fo, no);
+    const int Ps[3] = {c->Px, c->Py, c->Pz};
+    for (int a = 0; a < 3; ++a) {
+        if ((rc = al(&c->f_tw[a], Ps[a]))) return rc;
+        k_narrow<<<(Ps[a] + 255) / 256, 256, 0, c->st>>>(c->d_tw[a], c->f_tw[a], Ps[a]);
+    }
+    rc = check_cuda(c, cudaStreamSynchronize(c->st), "complex64 operator copy");
+    if (!rc) c->f_ready = true;
+    return rc;
+}
+
+int ensure_work_single(scd_ctx *c, int nrhs) {
+    if (c->f_cap >= nrhs && c->f_W) return SCD_OK;
+    const size_t r = (size_t)nrhs;
+    auto al = [&](cf **p, size_t n) -> int {
+        if (*p) { cudaFree(*p); *p = nullptr; }
+        if (cudaMalloc(p, sizeof(cf) * std::max<size_t>(n, 1)) != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(c, SCD_OOM, "complex64 work buffers (%d right-hand sides)", nrhs);
+        }
+        return SCD_OK;
+    };
+    int rc;
+    if ((rc = al(&c->f_bpart, r * c->ncubes * 4 * 27)) || (rc = al(&c->f_W, r * 4 * (size_t)c->Px * c->Py * c->Nz)) ||
+        (rc = al(&c->f_R, r * 4 * (size_t)c->Nx * c->Ny * c->Nz)) ||
+        (rc = al(&c->f_nzpart, r * (size_t)std::max<long long>(c->part_len, 1))))
+        return rc;
+    c->f_cap = nrhs;
+    return SCD_OK;
+}
+
+void launch_permute_in(scd_ctx *c, const cd *x_orig, cd *x_slot, int nrhs, long long ld) {
+    dim3 grid((unsigned)std::min<long long>((3LL * c->T + 255) / 256, 4096), nrhs);
+    k_permute_in<<<grid, 256, 0, c->st>>>(x_orig, x_slot, c->d_perm, c->T, ld);
+}
+
+void launch_permute_out(scd_ctx *c, const cd *x_slot, cd *x_orig, int nrhs, long long ld) {
+    dim3 grid((unsigned)std::min<long long>((3LL * c->T + 255) / 256, 4096), nrhs);
+    k_permute_out<<<grid, 256, 0, c->st>>>(x_slot, x_orig, c->d_perm, c->T, ld);
+}
+
+void launch_fft_chain(scd_ctx *c, const cd *x, int nrhs, const int *done) { fft_chain_t<cd>(c, x, nrhs, done); }
+void launch_near(scd_ctx *c, const cd *x, int nrhs, const int *done) { near_t<cd>(c, x, nrhs, done); }
+void launch_gather(scd_ctx *c, const cd *x, cd *y, int nrhs, const int *done) {
+    (void)x;
+    gather_t<cd>(c, y, nrhs, done);
+}
+void run_matvec(scd_ctx *c, const cd *x, cd *y, int nrhs, const int *done) { run_matvec_t<cd>(c, x, y, nrhs, done); }
+void run_matvec(scd_ctx *c, const cf *x, cf *y, int nrhs, const int *done) { run_matvec_t<cf>(c, x, y, nrhs, done); }

@@ -799,6 +799,7 @@ int setup_projectors_device(scd_ctx *c) {
     cudaFree(dWW);
     cudaFree(dcube);
     if (!rc) c->have_proj = true;
+    c->f_ready = false;
     return rc;
 }
 
@@ -837,7 +838,7 @@ int setup_nearzone_device(scd_ctx *c, int prec) {
     k_near_build<<<c->ntiles, NEAR_THREADS, sh, c->st>>>(a);
     rc = check_cuda(c, cudaGetLastError(), "near-zone launch");
     if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->st), "near-zone build");
-    if (!rc) { c->have_near = true; c->nrhs_cap = 0; }
+    if (!rc) { c->have_near = true; c->nrhs_cap = 0; c->f_cap = 0; }
     return rc;
 }
 

@@ -124,3 +124,33 @@ def test_batched_restarts_match_oracle(small_op, dev_small, small_sphere):
         xr, info = small_op.gmres(mat[c], tol=1e-9, m=3, cycles=8)
         assert it[c] == info["iters"]
         assert rel(X[c], xr) < 1e-9
+
+
+def test_mixed_precision_matches_fp64_oracle(small_op, dev_small, small_sphere):
+    """Complex64 inner GMRES + FP64 refinement reaches the FP64 answer: the
+    T-matrix relative error against the oracle's FP64 solve stays below 1e-6
+    (the target is <= 1e-5)."""
+    from scadyn_b200 import api
+    mat = O.vswf2constant(small_sphere.coord, small_sphere.etopol, small_op.geom.k, 2)
+    Tm, itm, Xm, rc = dev_small.solve_columns(mat, tol=1e-9, block=8, precision=api.PREC_MIXED,
+                                              inner_tol=1e-4, max_outer=10, want_x=True)
+    assert rc == api.SCD_OK
+    Xr = np.zeros_like(mat)
+    for c in range(mat.shape[0]):
+        Xr[c], _ = small_op.gmres(mat[c], tol=1e-11, m=50, cycles=8)
+    Tr = O.T_assemble(mat, Xr)
+    assert rel(Tm, Tr) < 1e-6
+    assert rel(Xm, Xr) < 1e-6
+    # the FP64 residual of every column meets the outer tolerance
+    for c in (0, 4):
+        r = mat[c] - small_op.compute_Ax2(Xm[c])
+        assert np.linalg.norm(r) / np.linalg.norm(mat[c]) < 1e-8
+
+
+def test_mixed_precision_batch_invariant(dev_small, small_op, small_sphere):
+    from scadyn_b200 import api
+    mat = O.vswf2constant(small_sphere.coord, small_sphere.etopol, small_op.geom.k, 1)
+    a = dev_small.solve_columns(mat, tol=1e-8, block=1, precision=api.PREC_MIXED, inner_tol=1e-3, want_x=True)
+    b = dev_small.solve_columns(mat, tol=1e-8, block=6, precision=api.PREC_MIXED, inner_tol=1e-3, want_x=True)
+    assert np.array_equal(a[1], b[1])
+    assert np.array_equal(a[2], b[2])
