@@ -354,7 +354,7 @@ def main():
     traffic = profile_traffic(f"near_tiles_{args.config}.txt")
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": kind,
-            "kernel": "k_near_tiles (near-zone block SpMV)", "alg_bytes_per_launch": alg_bytes,
+            "kernel": "k_near_groups (near-zone block SpMV)", "alg_bytes_per_launch": alg_bytes,
             "avg_launch_ms": near_ms, "matvec_ms": prof["matvec_ms"], "fft_chain_ms": prof["fft_ms"],
             "gather_ms": prof["gather_ms"]}
 

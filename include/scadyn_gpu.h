@@ -41,7 +41,7 @@ extern "C" {
 #define SCD_NAN            2   /* a non-finite residual or breakdown */
 #define SCD_OOM            3   /* device allocation failed */
 #define SCD_BAD_ARG        4   /* invalid sizes, pointers or indices */
-#define SCD_TIMEOUT        5   /* a host deadline expired */
+#define SCD_TIMEOUT        5   /* a deadline expired (host, or a bounded device wait) */
 #define SCD_CUDA_ERROR     6   /* CUDA runtime error; see scd_last_error */
 #define SCD_NOT_READY      7   /* an operator piece has not been set */
 #define SCD_NO_DEVICE      8   /* no usable CUDA device */
@@ -177,10 +177,11 @@ typedef struct scd_timing {
 } scd_timing;
 SCD_API int scd_get_timing(scd_ctx *ctx, scd_timing *t, int32_t reset);
 
-/* Run `reps` device-resident matvecs on `nrhs` fixed vectors at once and
- * record per-kernel averages per call in the timing block (matvec_ms,
- * nearzone_ms, fft_ms, gather_ms). */
-SCD_API int scd_profile_matvec(scd_ctx *ctx, int32_t reps, int32_t nrhs);
+/* Run `reps` device-resident matvecs on `nrhs` fixed vectors at once, in
+ * FP64 (SCD_PREC_FP64) or in the complex64 form the mixed-precision inner
+ * solves use (SCD_PREC_MIXED), and record per-kernel averages per call in
+ * the timing block (matvec_ms, nearzone_ms, fft_ms, gather_ms). */
+SCD_API int scd_profile_matvec(scd_ctx *ctx, int32_t reps, int32_t nrhs, int32_t precision);
 
 /* T = mat^H X without allocating: mat (n, ncol), X (n, ncb) and T (ncol, ncb)
  * are DEVICE pointers owned by the caller; the kernels run on `stream`

@@ -98,7 +98,7 @@ def load_library(path: str = LIB_PATH):
         "scd_vswf_rhs": ([vp, i32, vp], C.c_int),
         "scd_get_timing": ([vp, C.POINTER(Timing), i32], C.c_int),
         "scd_compute_T_matrix": ([vp, i32, C.POINTER(SolveOpts), i32, i32, vp, vp], C.c_int),
-        "scd_profile_matvec": ([vp, i32, i32], C.c_int),
+        "scd_profile_matvec": ([vp, i32, i32, i32], C.c_int),
         "scd_nearzone_bytes": ([vp], C.c_int64),
         "scd_column_latency": ([vp, i32, vp], C.c_int),
         "scd_T_assemble_noalloc": ([vp, i64, i32, vp, i32, vp, vp], C.c_int),
@@ -303,8 +303,8 @@ class Solver:
                   "compute_T_matrix", ok=(SCD_OK, SCD_NOT_CONVERGED))
         return Tf.T, iters
 
-    def profile_matvec(self, reps=10, nrhs=1):
-        self._chk(self.lib.scd_profile_matvec(self.ctx, reps, nrhs), "profile_matvec")
+    def profile_matvec(self, reps=10, nrhs=1, precision=PREC_FP64):
+        self._chk(self.lib.scd_profile_matvec(self.ctx, reps, nrhs, precision), "profile_matvec")
         return self.timing()
 
     def column_latency(self, ncol):

@@ -69,6 +69,16 @@ int ensure_work(scd_ctx *c, int nrhs) {
     return SCD_OK;
 }
 
+// error word of the near-zone kernel: a bounded wait that ran out
+int near_status(scd_ctx *c) {
+    if (!c->d_kerr) return SCD_OK;
+    int h = 0;
+    CK(cudaMemcpy(&h, c->d_kerr, sizeof(int), cudaMemcpyDeviceToHost), "near-zone status");
+    if (!h) return SCD_OK;
+    CK(cudaMemset(c->d_kerr, 0, sizeof(int)), "near-zone status");
+    return set_error(c, SCD_TIMEOUT, "near-zone kernel: a pipeline wait ran out");
+}
+
 // ---------------------------------------------------------------- ordering
 // Slot order: tets sorted by cube, ties by original index (tetras_in_cubes,
 // src/geometry.f90:330-377, lists each cube's tets in increasing order).
@@ -100,103 +110,151 @@ static int set_order(scd_ctx *c, const std::vector<int> &cube_of_tet) {
     c->cube_off = cnt;
     c->max_per_cube = 0;
     for (int q = 0; q < c->ncubes; ++q) c->max_per_cube = std::max(c->max_per_cube, cnt[q + 1] - cnt[q]);
+    // near-zone groups: each non-empty box split into ceil(n / SCD_GROUP_MAX)
+    // runs whose sizes differ by at most one
+    c->grp_off.assign(1, 0);
+    c->grp_cube.clear();
+    c->grp_of_slot.assign(T, 0);
+    c->max_per_group = 0;
+    for (int q = 0; q < c->ncubes; ++q) {
+        const int n = cnt[q + 1] - cnt[q];
+        if (n == 0) continue;
+        const int ng = (n + SCD_GROUP_MAX - 1) / SCD_GROUP_MAX;
+        int s = cnt[q];
+        for (int g = 0; g < ng; ++g) {
+            const int m = n / ng + (g < n % ng ? 1 : 0);
+            for (int k = 0; k < m; ++k) c->grp_of_slot[s + k] = (int)c->grp_cube.size();
+            s += m;
+            c->grp_off.push_back(s);
+            c->grp_cube.push_back(q);
+            c->max_per_group = std::max(c->max_per_group, m);
+        }
+    }
+    c->ngroups = (int)c->grp_cube.size();
     int rc;
     if ((rc = dalloc(c, &c->d_perm, T, "perm"))) return rc;
     if ((rc = dalloc(c, &c->d_cube_off, c->ncubes + 1, "cube offsets"))) return rc;
+    if ((rc = dalloc(c, &c->d_grp_off, c->ngroups + 1, "group offsets"))) return rc;
+    if ((rc = dalloc(c, &c->d_grp_cube, std::max(c->ngroups, 1), "group boxes"))) return rc;
     CK(cudaMemcpy(c->d_perm, c->perm.data(), sizeof(int) * T, cudaMemcpyHostToDevice), "perm");
     CK(cudaMemcpy(c->d_cube_off, c->cube_off.data(), sizeof(int) * (c->ncubes + 1), cudaMemcpyHostToDevice), "cube offsets");
+    CK(cudaMemcpy(c->d_grp_off, c->grp_off.data(), sizeof(int) * (c->ngroups + 1), cudaMemcpyHostToDevice), "groups");
+    if (c->ngroups)
+        CK(cudaMemcpy(c->d_grp_cube, c->grp_cube.data(), sizeof(int) * c->ngroups, cudaMemcpyHostToDevice), "groups");
     c->have_order = true;
     return SCD_OK;
 }
 
 // ------------------------------------------------------------ near tiles
+// write / accumulate a 3x3 block (column-major src, optionally transposed)
+// into its strided tile position
 template <typename ST>
-static void put_block(ST *dst, const ST *src, bool transpose) {
-    for (int r = 0; r < 3; ++r)
-        for (int q = 0; q < 3; ++q) dst[r + 3 * q] = transpose ? src[q + 3 * r] : src[r + 3 * q];
-}
-template <typename ST>
-static void add_block(ST *dst, const ST *src, bool transpose) {
+static void put_block(ST *tile, int n1, int i, int j, const ST *src, bool transpose, bool add) {
     for (int r = 0; r < 3; ++r)
         for (int q = 0; q < 3; ++q) {
             const ST v = transpose ? src[q + 3 * r] : src[r + 3 * q];
-            dst[r + 3 * q].x += v.x;
-            dst[r + 3 * q].y += v.y;
+            ST &d = tile[tile_at(n1, i, j, r + 3 * q)];
+            if (add) { d.x += v.x; d.y += v.y; }
+            else d = v;
         }
 }
 
-// Dense tile layout for a sorted list of cube pairs key = c1*ncubes + c2
-// (c1 <= c2): data offsets and per-cube partial-sum slots in tile order.
+// Tile layout for a sorted list of group pairs key = g1*ngroups + g2
+// (g1 <= g2): data offsets, the partial-sum slots of every group and the
+// tile range of every group.
 static long long layout_tiles(scd_ctx *c, const std::vector<uint64_t> &keys, std::vector<NearTile> &tiles) {
     const int nt = (int)keys.size();
+    const int ng = c->ngroups;
     tiles.assign(nt, NearTile{});
-    std::vector<int> cnt(c->ncubes, 0);
+    std::vector<int> cnt(ng, 1);           // slot 0: row sums
     long long off = 0;
+    c->tile_blocks = 0;
+    c->max_tile_store = 0;
+    c->grp_tile.assign(ng + 1, 0);
     for (int i = 0; i < nt; ++i) {
         NearTile &tl = tiles[i];
-        tl.c1 = (int)(keys[i] / c->ncubes);
-        tl.c2 = (int)(keys[i] % c->ncubes);
-        tl.n1 = c->cube_off[tl.c1 + 1] - c->cube_off[tl.c1];
-        tl.n2 = c->cube_off[tl.c2 + 1] - c->cube_off[tl.c2];
+        tl.g1 = (int)(keys[i] / ng);
+        tl.g2 = (int)(keys[i] % ng);
+        tl.c1 = c->grp_cube[tl.g1];
+        tl.c2 = c->grp_cube[tl.g2];
+        tl.s1 = c->grp_off[tl.g1];
+        tl.s2 = c->grp_off[tl.g2];
+        tl.n1 = c->grp_off[tl.g1 + 1] - tl.s1;
+        tl.n2 = c->grp_off[tl.g2 + 1] - tl.s2;
         tl.data_off = off;
-        off += (long long)tl.n1 * tl.n2;
-        cnt[tl.c1]++;
-        if (tl.c2 != tl.c1) cnt[tl.c2]++;
+        const long long te = tile_elems(tl.n1, tl.n2);
+        off += te;
+        c->max_tile_store = std::max(c->max_tile_store, te);
+        c->tile_blocks += (long long)tl.n1 * tl.n2;
+        if (tl.g2 != tl.g1) cnt[tl.g2]++;
+        c->grp_tile[tl.g1 + 1] = i + 1;
     }
-    c->pslot_base.assign(c->ncubes + 1, 0);
+    for (int g = 0; g < ng; ++g) c->grp_tile[g + 1] = std::max(c->grp_tile[g + 1], c->grp_tile[g]);
+    c->pslot_base.assign(ng + 1, 0);
     c->pslot_cnt = cnt;
-    for (int q = 0; q < c->ncubes; ++q) {
-        const int nq = c->cube_off[q + 1] - c->cube_off[q];
-        c->pslot_base[q + 1] = c->pslot_base[q] + (long long)cnt[q] * 3 * nq;
+    for (int g = 0; g < ng; ++g) {
+        const int n = c->grp_off[g + 1] - c->grp_off[g];
+        c->pslot_base[g + 1] = c->pslot_base[g] + (long long)cnt[g] * 3 * n;
     }
-    std::vector<int> used(c->ncubes, 0);
+    std::vector<int> used(ng, 1);
     for (int i = 0; i < nt; ++i) {
         NearTile &tl = tiles[i];
-        tl.row_off = c->pslot_base[tl.c1] + (long long)(used[tl.c1]++) * 3 * tl.n1;
         tl.col_off = -1;
-        if (tl.c2 != tl.c1) tl.col_off = c->pslot_base[tl.c2] + (long long)(used[tl.c2]++) * 3 * tl.n2;
+        if (tl.g2 != tl.g1) tl.col_off = c->pslot_base[tl.g2] + (long long)(used[tl.g2]++) * 3 * tl.n2;
     }
+    c->tile_store = off;
     return off;
 }
 
 static int upload_layout(scd_ctx *c, std::vector<NearTile> &tiles, long long off) {
+    (void)off;
     const int nt = (int)tiles.size();
+    const int ng = c->ngroups;
     int rc;
     if ((rc = dalloc(c, &c->d_tiles, nt, "tile table"))) return rc;
-    if ((rc = dalloc(c, &c->d_pslot_base, c->ncubes + 1, "slot bases"))) return rc;
-    if ((rc = dalloc(c, &c->d_pslot_cnt, c->ncubes, "slot counts"))) return rc;
-    CK(cudaMemcpy(c->d_tiles, tiles.data(), sizeof(NearTile) * nt, cudaMemcpyHostToDevice), "tile table");
-    CK(cudaMemcpy(c->d_pslot_base, c->pslot_base.data(), sizeof(long long) * (c->ncubes + 1), cudaMemcpyHostToDevice), "slots");
-    CK(cudaMemcpy(c->d_pslot_cnt, c->pslot_cnt.data(), sizeof(int) * c->ncubes, cudaMemcpyHostToDevice), "slots");
+    if ((rc = dalloc(c, &c->d_pslot_base, ng + 1, "slot bases"))) return rc;
+    if ((rc = dalloc(c, &c->d_pslot_cnt, std::max(ng, 1), "slot counts"))) return rc;
+    if ((rc = dalloc(c, &c->d_grp_tile, ng + 1, "group tiles"))) return rc;
+    if ((rc = dalloc(c, &c->d_kerr, 1, "error word"))) return rc;
+    CK(cudaMemset(c->d_kerr, 0, sizeof(int)), "error word");
+    if (nt) CK(cudaMemcpy(c->d_tiles, tiles.data(), sizeof(NearTile) * nt, cudaMemcpyHostToDevice), "tile table");
+    CK(cudaMemcpy(c->d_pslot_base, c->pslot_base.data(), sizeof(long long) * (ng + 1), cudaMemcpyHostToDevice), "slots");
+    if (ng) CK(cudaMemcpy(c->d_pslot_cnt, c->pslot_cnt.data(), sizeof(int) * ng, cudaMemcpyHostToDevice), "slots");
+    CK(cudaMemcpy(c->d_grp_tile, c->grp_tile.data(), sizeof(int) * (ng + 1), cudaMemcpyHostToDevice), "group tiles");
     c->ntiles = nt;
-    c->tile_blocks = off;
-    c->part_len = c->pslot_base[c->ncubes];
+    c->part_len = c->pslot_base[ng];
     c->tiles_h.swap(tiles);
     c->nrhs_cap = 0;   // partial buffer size changed
     c->f_cap = 0;
     return SCD_OK;
 }
 
-// Tiles from the geometry: every non-empty cube c1 with each non-empty cube
-// c2 >= c1 of its 27-neighbourhood (find_near_cubes, src/geometry.f90:275-326)
-// — the same tet pairs compute_near_zone_interactions_const visits.
+// Tiles from the geometry: every group g1 with each group g2 >= g1 whose box
+// lies in the 27-neighbourhood of g1's box (find_near_cubes,
+// src/geometry.f90:275-326) -- the tet pairs that
+// compute_near_zone_interactions_const visits.
 int build_tile_layout(scd_ctx *c) {
     std::vector<uint64_t> keys;
-    for (int z = 0; z < c->ncz; ++z)
-        for (int y = 0; y < c->ncy; ++y)
-            for (int x = 0; x < c->ncx; ++x) {
-                const int c1 = x + c->ncx * (y + c->ncy * z);
-                if (c->cube_off[c1 + 1] == c->cube_off[c1]) continue;
-                for (int dz = -1; dz <= 1; ++dz)
-                    for (int dy = -1; dy <= 1; ++dy)
-                        for (int dx = -1; dx <= 1; ++dx) {
-                            const int xx = x + dx, yy = y + dy, zz = z + dz;
-                            if (xx < 0 || yy < 0 || zz < 0 || xx >= c->ncx || yy >= c->ncy || zz >= c->ncz) continue;
-                            const int c2 = xx + c->ncx * (yy + c->ncy * zz);
-                            if (c2 < c1 || c->cube_off[c2 + 1] == c->cube_off[c2]) continue;
-                            keys.push_back((uint64_t)c1 * (uint64_t)c->ncubes + (uint64_t)c2);
-                        }
-            }
+    // groups of each box
+    std::vector<int> first(c->ncubes + 1, -1), last(c->ncubes, -1);
+    for (int g = 0; g < c->ngroups; ++g) {
+        if (first[c->grp_cube[g]] < 0) first[c->grp_cube[g]] = g;
+        last[c->grp_cube[g]] = g;
+    }
+    for (int g1 = 0; g1 < c->ngroups; ++g1) {
+        const int c1 = c->grp_cube[g1];
+        const int x = c1 % c->ncx, y = (c1 / c->ncx) % c->ncy, z = c1 / (c->ncx * c->ncy);
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    const int xx = x + dx, yy = y + dy, zz = z + dz;
+                    if (xx < 0 || yy < 0 || zz < 0 || xx >= c->ncx || yy >= c->ncy || zz >= c->ncz) continue;
+                    const int c2 = xx + c->ncx * (yy + c->ncy * zz);
+                    if (first[c2] < 0) continue;
+                    for (int g2 = std::max(first[c2], g1); g2 <= last[c2]; ++g2)
+                        keys.push_back((uint64_t)g1 * (uint64_t)c->ngroups + (uint64_t)g2);
+                }
+    }
     std::sort(keys.begin(), keys.end());
     std::vector<NearTile> tiles;
     const long long off = layout_tiles(c, keys, tiles);
@@ -206,21 +264,21 @@ int build_tile_layout(scd_ctx *c) {
 int set_order_from_cubes(scd_ctx *c, const std::vector<int> &cube_of_tet) { return set_order(c, cube_of_tet); }
 
 // Tile the reference's symmetric block list (tet_B >= tet_T) into dense
-// cube-pair tiles; see NearTile in ctx.h.  Blocks given twice are summed, as
+// group-pair tiles; see NearTile in ctx.h.  Blocks given twice are summed, as
 // the reference's SpMV would sum them.
 template <typename ST>
 static int build_tiles(scd_ctx *c, int64_t B, const ST *sp, const int32_t *ind) {
     const int T = c->T;
     std::unordered_map<uint64_t, int> tid;
-    tid.reserve((size_t)c->ncubes * 16);
+    tid.reserve((size_t)c->ngroups * 16);
     std::vector<uint64_t> keys;
     std::vector<int> btile((size_t)B);
     for (int64_t b = 0; b < B; ++b) {
         const int t1 = ind[2 * b] - 1, t2 = ind[2 * b + 1] - 1;
         if (t1 < 0 || t1 >= T || t2 < 0 || t2 >= T)
             return set_error(c, SCD_BAD_ARG, "sp_ind(:,%lld) = (%d,%d) outside 1..%d", (long long)b + 1, t1 + 1, t2 + 1, T);
-        const int ca = c->cube_of_slot[c->slot_of[t1]], cb = c->cube_of_slot[c->slot_of[t2]];
-        const uint64_t key = (uint64_t)std::min(ca, cb) * (uint64_t)c->ncubes + (uint64_t)std::max(ca, cb);
+        const int ga = c->grp_of_slot[c->slot_of[t1]], gb = c->grp_of_slot[c->slot_of[t2]];
+        const uint64_t key = (uint64_t)std::min(ga, gb) * (uint64_t)c->ngroups + (uint64_t)std::max(ga, gb);
         auto it = tid.find(key);
         int id;
         if (it == tid.end()) { id = (int)keys.size(); tid.emplace(key, id); keys.push_back(key); }
@@ -237,27 +295,32 @@ static int build_tiles(scd_ctx *c, int64_t B, const ST *sp, const int32_t *ind) 
     for (int i = 0; i < nt; ++i) skeys[i] = keys[order[i]];
     std::vector<NearTile> tiles;
     const long long off = layout_tiles(c, skeys, tiles);
-    std::vector<ST> data((size_t)off * 9);
+    std::vector<ST> data((size_t)off);
     std::memset(data.data(), 0, sizeof(ST) * data.size());
-    std::vector<char> seen((size_t)off, 0);
+    std::vector<char> seen((size_t)c->tile_blocks, 0);
+    std::vector<long long> block_base(nt);   // first block of each tile in `seen`
+    {
+        long long acc = 0;
+        for (int i = 0; i < nt; ++i) { block_base[i] = acc; acc += (long long)tiles[i].n1 * tiles[i].n2; }
+    }
     for (int64_t b = 0; b < B; ++b) {
-        const NearTile &tl = tiles[rank[btile[b]]];
+        const int ti = rank[btile[b]];
+        const NearTile &tl = tiles[ti];
         const int t1 = ind[2 * b] - 1, t2 = ind[2 * b + 1] - 1;
         const int s1 = c->slot_of[t1], s2 = c->slot_of[t2];
-        const int ca = c->cube_of_slot[s1];
         const ST *src = sp + 9 * b;
         // position of (row tet, column tet) in the tile and whether the block
         // must be transposed (M(B,T) = M(T,B)^T)
         auto place = [&](int srow, int scol, bool tr) {
-            const int i = srow - c->cube_off[tl.c1], j = scol - c->cube_off[tl.c2];
-            const size_t e = (size_t)tl.data_off + (size_t)i * tl.n2 + j;
-            if (seen[e]) add_block(&data[9 * e], src, tr);
-            else { put_block(&data[9 * e], src, tr); seen[e] = 1; }
+            const int i = srow - tl.s1, j = scol - tl.s2;
+            const size_t e = (size_t)block_base[ti] + (size_t)i * tl.n2 + j;
+            put_block(&data[(size_t)tl.data_off], tl.n1, i, j, src, tr, seen[e] != 0);
+            seen[e] = 1;
         };
-        if (tl.c1 == tl.c2) {
+        if (tl.g1 == tl.g2) {
             place(s1, s2, false);
             if (s1 != s2) place(s2, s1, true);
-        } else if (ca == tl.c1) {
+        } else if (c->grp_of_slot[s1] == tl.g1) {
             place(s1, s2, false);
         } else {
             place(s2, s1, true);
@@ -315,7 +378,7 @@ int scd_destroy(scd_ctx *c) {
     if (!c) return SCD_OK;
     cudaSetDevice(c->dev);
     if (c->st) cudaStreamSynchronize(c->st);
-    void *ptrs[] = {c->d_perm, c->d_cube_off, c->d_P, c->d_Fo, c->d_tdata, c->d_tiles, c->d_pslot_base,
+    void *ptrs[] = {c->d_perm, c->d_cube_off, c->d_grp_off, c->d_grp_cube, c->d_grp_tile, c->d_kerr, c->d_P, c->d_Fo, c->d_tdata, c->d_tiles, c->d_pslot_base,
                     c->d_pslot_cnt, c->d_tc, c->d_tvol, c->d_eps, c->d_bpart, c->d_W, c->d_R, c->d_nzpart, c->d_x,
                     c->d_y, c->d_io, c->d_V, c->d_H, c->d_cs, c->d_sn, c->d_g, c->d_rhs, c->d_w, c->d_red,
                     c->d_bar, c->d_err, c->d_state, c->d_tw[0], c->d_tw[1], c->d_tw[2], c->f_P, c->f_Fo,
@@ -398,9 +461,6 @@ int scd_set_nearzone(scd_ctx *c, int64_t B, const void *sp_mat, const int32_t *s
     if (!c->have_order) return set_error(c, SCD_NOT_READY, "set the projectors (or the mesh) before the near zone");
     if (B < 0 || (B > 0 && (!sp_mat || !sp_ind))) return set_error(c, SCD_BAD_ARG, "bad near-zone arrays");
     if (prec != SCD_STORE_C64 && prec != SCD_STORE_C128) return set_error(c, SCD_BAD_ARG, "storage_prec %d", prec);
-    if (c->max_per_cube > SCD_NEAR_MAXN)
-        return set_error(c, SCD_BAD_ARG, "%d tets in one projection box; the near-zone kernels support %d",
-                         c->max_per_cube, SCD_NEAR_MAXN);
     int rc;
     c->have_near = false;
     c->near_prec = prec;
@@ -432,6 +492,7 @@ int scd_matvec(scd_ctx *c, const scd_c128 *x, scd_c128 *Ax) {
     CK(cudaMemcpyAsync(Ax, c->d_io, bytes, cudaMemcpyDeviceToHost, c->st), "Ax");
     CK(cudaStreamSynchronize(c->st), "matvec");
     c->n_matvec += 1;
+    if ((rc = near_status(c))) return rc;
     return check_cuda(c, cudaGetLastError(), "matvec");
 }
 
@@ -453,6 +514,10 @@ int scd_gmres(scd_ctx *c, const scd_c128 *rhs, scd_c128 *x, double tol, int32_t 
     launch_permute_out(c, c->d_x, c->d_io, 1, c->n);
     CK(cudaMemcpyAsync(x, c->d_io, bytes, cudaMemcpyDeviceToHost, c->st), "x");
     CK(cudaStreamSynchronize(c->st), "gmres");
+    {
+        const int ns = near_status(c);
+        if (ns) return ns;
+    }
     {
         float ms = 0;
         cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]);
@@ -486,6 +551,10 @@ int scd_solve_columns(scd_ctx *c, int32_t ncol, const scd_c128 *mat, scd_c128 *T
     std::vector<int> it(ncol, 0);
     int worst = batch_solve(c, ncol, cols.data(), d_X, o->tol, o->m, o->cycles, ns, it.data(), nullptr, nullptr,
                             o->precision, o->inner_tol, o->max_outer);
+    if (worst == SCD_OK || worst == SCD_NOT_CONVERGED) {
+        const int ns_ = near_status(c);
+        if (ns_) worst = ns_;
+    }
     if (iters) for (int j = 0; j < ncol; ++j) iters[j] = it[j];
     if (worst == SCD_OK || worst == SCD_NOT_CONVERGED) {
         launch_T_assemble(c, d_mat, ncol, 0, ncol, d_X, d_T);
@@ -532,23 +601,38 @@ int scd_get_timing(scd_ctx *c, scd_timing *t, int32_t reset) {
     return SCD_OK;
 }
 
-int scd_profile_matvec(scd_ctx *c, int32_t reps, int32_t nrhs) {
+int scd_profile_matvec(scd_ctx *c, int32_t reps, int32_t nrhs, int32_t precision) {
     if (!c || reps < 1 || nrhs < 1) return SCD_BAD_ARG;
+    if (precision != SCD_PREC_FP64 && precision != SCD_PREC_MIXED)
+        return set_error(c, SCD_BAD_ARG, "precision %d", precision);
     cudaSetDevice(c->dev);
     int rc = ready(c);
     if (rc) return rc;
     if ((rc = ensure_work(c, nrhs))) return rc;
-    // a fixed non-trivial vector: the first VSWF-like pattern is not needed,
-    // any dense vector exercises the same memory traffic
+    const bool mixed = precision == SCD_PREC_MIXED;
+    cf *fx = nullptr, *fy = nullptr;
+    if (mixed) {
+        if ((rc = ensure_single(c)) || (rc = ensure_work_single(c, nrhs))) return rc;
+        if ((rc = dalloc(c, &fx, (size_t)nrhs * c->n, "profile x"))) return rc;
+        if ((rc = dalloc(c, &fy, (size_t)nrhs * c->n, "profile y"))) { cudaFree(fx); return rc; }
+    }
+    // a fixed dense vector: the memory traffic of a matvec does not depend on the values
     std::vector<cd> h((size_t)c->n);
-    for (long long i = 0; i < c->n; ++i) h[i] = cmk(std::sin(0.37 * (double)i), std::cos(0.11 * (double)i));
-    for (int r = 0; r < nrhs; ++r)
-        CK(cudaMemcpy(c->d_x + (size_t)r * c->n, h.data(), sizeof(cd) * c->n, cudaMemcpyHostToDevice), "profile x");
+    std::vector<cf> hf((size_t)c->n);
+    for (long long i = 0; i < c->n; ++i) {
+        h[i] = cmk(std::sin(0.37 * (double)i), std::cos(0.11 * (double)i));
+        hf[i] = make_float2((float)h[i].x, (float)h[i].y);
+    }
+    for (int r = 0; r < nrhs && !rc; ++r) {
+        if (mixed) rc = check_cuda(c, cudaMemcpy(fx + (size_t)r * c->n, hf.data(), sizeof(cf) * c->n, cudaMemcpyHostToDevice), "profile x");
+        else rc = check_cuda(c, cudaMemcpy(c->d_x + (size_t)r * c->n, h.data(), sizeof(cd) * c->n, cudaMemcpyHostToDevice), "profile x");
+    }
     double sn = 0, sf = 0, sg = 0, st = 0;
     c->timing = true;
-    for (int r = 0; r < reps + 1; ++r) {
-        run_matvec(c, c->d_x, c->d_y, nrhs, nullptr);
-        CK(cudaStreamSynchronize(c->st), "profile");
+    for (int r = 0; r < reps + 1 && !rc; ++r) {
+        if (mixed) run_matvec(c, fx, fy, nrhs, nullptr);
+        else run_matvec(c, c->d_x, c->d_y, nrhs, nullptr);
+        rc = check_cuda(c, cudaStreamSynchronize(c->st), "profile");
         float a = 0, b = 0, g = 0, t = 0;
         cudaEventElapsedTime(&a, c->ev[0], c->ev[1]);
         cudaEventElapsedTime(&b, c->ev[1], c->ev[2]);
@@ -558,10 +642,14 @@ int scd_profile_matvec(scd_ctx *c, int32_t reps, int32_t nrhs) {
         sn += a; sf += b; sg += g; st += t;
     }
     c->timing = false;
+    if (fx) cudaFree(fx);
+    if (fy) cudaFree(fy);
+    if (rc) return rc;
     c->t_near = sn / reps;
     c->t_fft = sf / reps;
     c->t_gather = sg / reps;
     c->t_matvec = st / reps;
+    if ((rc = near_status(c))) return rc;
     return check_cuda(c, cudaGetLastError(), "profile");
 }
 
@@ -575,7 +663,7 @@ int scd_column_latency(scd_ctx *c, int32_t ncol, double *ms) {
 
 int64_t scd_nearzone_bytes(scd_ctx *c) {
     if (!c || !c->have_near) return -1;
-    return (int64_t)c->tile_blocks * 9 * (c->near_prec == SCD_STORE_C64 ? 8 : 16);
+    return (int64_t)c->tile_store * (c->near_prec == SCD_STORE_C64 ? 8 : 16);
 }
 
 int scd_compute_T_matrix(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int32_t col0, int32_t ncol,
@@ -606,6 +694,10 @@ int scd_compute_T_matrix(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int3
     std::vector<int> it(ncol, 0);
     int worst = batch_solve(c, ncol, cols.data(), d_X, o->tol, o->m, o->cycles, ns, it.data(), nullptr, nullptr,
                             o->precision, o->inner_tol, o->max_outer);
+    if (worst == SCD_OK || worst == SCD_NOT_CONVERGED) {
+        const int ns_ = near_status(c);
+        if (ns_) worst = ns_;
+    }
     if (iters) for (int j = 0; j < ncol; ++j) iters[j] = it[j];
     if (worst == SCD_OK || worst == SCD_NOT_CONVERGED) {
         launch_T_assemble(c, c->d_mat, ntot, 0, ncol, d_X, d_T);

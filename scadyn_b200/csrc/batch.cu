@@ -33,6 +33,7 @@ enum { SLOT_FREE = 0, SLOT_START = 1, SLOT_ARNOLDI = 2, SLOT_DONE = 3, SLOT_RESI
 struct Slot {
     int mode, col, cycle, step, iters, conv, status, reorth, finish, zero_x;
     int outer, upd;    // mixed: outer steps taken; x += rho d pending
+    int mpos, rpos;    // column of this slot in the tick's compacted matvec input (inner, FP64 residual), -1: none
     double b_norm, beta, error;
     double rho;        // mixed: ||r|| of the residual the inner solve corrects
     double b64;        // mixed: ||rhs|| in FP64
@@ -61,6 +62,16 @@ __device__ __forceinline__ cd to_cd(cd a) { return a; }
 __device__ __forceinline__ cd to_cd(cf a) { return widen(a); }
 __device__ __forceinline__ void store_c(cd &d, cd v) { d = v; }
 __device__ __forceinline__ void store_c(cf &d, cd v) { d = make_float2((float)v.x, (float)v.y); }
+// v rounded to the storage precision C, back in FP64
+template <typename C> __device__ __forceinline__ cd rounded(cd v);
+template <> __device__ __forceinline__ cd rounded<cd>(cd v) { return v; }
+template <> __device__ __forceinline__ cd rounded<cf>(cd v) { return widen(make_float2((float)v.x, (float)v.y)); }
+
+// Streaming loops over a vector take this thread's elements q0, q0+stride,
+// ... TU at a time: the loads of TU elements are issued together (memory-
+// level parallelism), the arithmetic runs in the same element order as a
+// plain loop, so sums are unchanged.
+constexpr int TU = 4;
 
 template <typename C>
 __device__ __forceinline__ double *partial_slot(const TickArgs<C> &a, int parity, int s) {
@@ -88,11 +99,35 @@ __device__ void read_totals(const TickArgs<C> &a, int parity, int nv, double (*t
     __syncthreads();
 }
 
+constexpr int BW = BT / 32;   // warps per CTA
+
+// Per-slot reductions without a CTA barrier per slot: each warp folds its
+// NV values (xor tree) into wsh[s][warp]; flush_parts then adds the warps in
+// order -- the arithmetic of block_sum -- and stores the CTA partial of every
+// slot flagged in act[].
+template <int NV>
+__device__ __forceinline__ void warp_part(double (&v)[NV], double *wsh, int s) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) wsh[(s * BW + w) * 4 + q] = v[q];
+    }
+}
+
 template <typename C>
-__device__ __forceinline__ void put_partial(const TickArgs<C> &a, int parity, int s, const double *v, int nv) {
-    if (threadIdx.x == 0) {
-        double *p = partial_slot(a, parity, s);
-        for (int q = 0; q < nv; ++q) p[q] = v[q];
+__device__ __forceinline__ void flush_parts(const TickArgs<C> &a, int parity, const double *wsh, const int *act, int nv) {
+    __syncthreads();
+    for (int e = threadIdx.x; e < a.ns * 4; e += blockDim.x) {
+        const int s = e >> 2, q = e & 3;
+        if (q >= nv || !act[s]) continue;
+        double t = 0.0;
+        for (int i = 0; i < BW; ++i) t += wsh[(s * BW + i) * 4 + q];
+        partial_slot(a, parity, s)[q] = t;
     }
 }
 
@@ -100,9 +135,9 @@ __device__ __forceinline__ void put_partial(const TickArgs<C> &a, int parity, in
 // (MGS, normalisation, Givens) for every active slot; cycle ends update x.
 template <typename C>
 __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
-    __shared__ double bsh[64];
+    __shared__ double wsh[NSMAX * BW * 4];
     __shared__ double tot[NSMAX][4];
-    __shared__ int smode[NSMAX], sstep[NSMAX], szero[NSMAX];
+    __shared__ int smode[NSMAX], sstep[NSMAX], szero[NSMAX], swpos[NSMAX], sact[NSMAX];
     __shared__ double snormav[NSMAX], shn[NSMAX];
     __shared__ cd sh_h[NSMAX];
     __shared__ cd ysm[64];
@@ -114,6 +149,7 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
         smode[s] = a.slots[s].mode;
         sstep[s] = a.slots[s].step;
         szero[s] = a.slots[s].zero_x;
+        swpos[s] = max(a.slots[s].mpos, 0);   // A v of the slot sits in column mpos of w
     }
     __syncthreads();
     int parity = 0;
@@ -121,30 +157,55 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
     for (int s = 0; s < a.ns; ++s) {
         const int md = smode[s];
         double v[3] = {0, 0, 0};
-        const C *ws = a.w + (size_t)s * n;
+        const C *ws = a.w + (size_t)swpos[s] * n;
         C *V0 = a.V + (size_t)s * (a.m + 1) * n;
         if (md == SLOT_START) {
             const C *bs = a.rhs + (size_t)s * n;
             const bool zx = szero[s] != 0;
-            for (long long q = q0; q < n; q += stride) {
-                const cd b = to_cd(bs[q]);
-                const cd r = zx ? b : csub(b, to_cd(ws[q]));
-                store_c(V0[q], r);
-                v[0] += cabs2(r);
-                v[1] += cabs2(b);
+            for (long long q = q0; q < n; q += TU * stride) {
+                cd b[TU], w[TU];
+#pragma unroll
+                for (int u = 0; u < TU; ++u) {
+                    const long long qq = q + u * stride;
+                    b[u] = w[u] = cmk(0, 0);
+                    if (qq < n) {
+                        b[u] = to_cd(bs[qq]);
+                        if (!zx) w[u] = to_cd(ws[qq]);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < TU; ++u) {
+                    const long long qq = q + u * stride;
+                    if (qq >= n) break;
+                    const cd r = zx ? b[u] : csub(b[u], w[u]);
+                    store_c(V0[qq], r);
+                    v[0] += cabs2(r);
+                    v[1] += cabs2(b[u]);
+                }
             }
         } else if (md == SLOT_ARNOLDI) {
-            for (long long q = q0; q < n; q += stride) {
-                const cd w = to_cd(ws[q]), z = to_cd(V0[q]);
-                v[0] += cabs2(w);
-                cdot_acc(v[1], v[2], z, w);
+            for (long long q = q0; q < n; q += TU * stride) {
+                cd w[TU], z[TU];
+#pragma unroll
+                for (int u = 0; u < TU; ++u) {
+                    const long long qq = q + u * stride;
+                    w[u] = z[u] = cmk(0, 0);
+                    if (qq < n) { w[u] = to_cd(ws[qq]); z[u] = to_cd(V0[qq]); }
+                }
+#pragma unroll
+                for (int u = 0; u < TU; ++u) {
+                    if (q + u * stride >= n) break;
+                    v[0] += cabs2(w[u]);
+                    cdot_acc(v[1], v[2], z[u], w[u]);
+                }
             }
         } else {
             continue;
         }
-        block_sum<3>(v, bsh);
-        put_partial(a, parity, s, v, 3);
+        warp_part<3>(v, wsh, s);
     }
+    for (int s = threadIdx.x; s < a.ns; s += blockDim.x) sact[s] = smode[s] == SLOT_START || smode[s] == SLOT_ARNOLDI;
+    flush_parts(a, parity, wsh, sact, 3);
     grid_barrier(a.bar, gridDim.x, a.err);
     read_totals(a, parity, 3, tot);
     int kmax = 0;
@@ -161,9 +222,18 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
         if (smode[s] != SLOT_START) continue;
         const double beta = sqrt(tot[s][0]);
         C *V0 = a.V + (size_t)s * (a.m + 1) * n;
-        for (long long q = q0; q < n; q += stride) {
-            const cd r = to_cd(V0[q]);
-            store_c(V0[q], cmk(r.x / beta, r.y / beta));
+        for (long long q = q0; q < n; q += TU * stride) {
+            cd r[TU];
+#pragma unroll
+            for (int u = 0; u < TU; ++u) {
+                const long long qq = q + u * stride;
+                r[u] = qq < n ? to_cd(V0[qq]) : cmk(0, 0);
+            }
+#pragma unroll
+            for (int u = 0; u < TU; ++u) {
+                const long long qq = q + u * stride;
+                if (qq < n) store_c(V0[qq], cmk(r[u].x / beta, r[u].y / beta));
+            }
         }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             Slot &sl = a.slots[s];
@@ -187,27 +257,38 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
             if (k > i) continue;
             const cd h = sh_h[s];
             if (blockIdx.x == 0 && threadIdx.x == 0) a.H[(size_t)s * ldh * a.m + (size_t)ldh * (i - 1) + (k - 1)] = h;
-            C *ws = a.w + (size_t)s * n;
+            C *ws = a.w + (size_t)swpos[s] * n;
             const C *Vs = a.V + (size_t)s * (a.m + 1) * n;
             const C *vk = Vs + (size_t)(k - 1) * n;
             const C *vn = (k < i) ? Vs + (size_t)k * n : nullptr;
             double u[2] = {0, 0};
-            for (long long q = q0; q < n; q += stride) {
-                cd w = to_cd(ws[q]);
-                const cd p = to_cd(vk[q]);
-                csub_mul(w, h, p);
-                store_c(ws[q], w);
-                w = to_cd(ws[q]);
-                if (vn) {
-                    const cd z = to_cd(vn[q]);
-                    cdot_acc(u[0], u[1], z, w);
-                } else {
-                    u[0] += cabs2(w);
+            for (long long q = q0; q < n; q += TU * stride) {
+                cd w[TU], p[TU], z[TU];
+#pragma unroll
+                for (int e = 0; e < TU; ++e) {
+                    const long long qq = q + e * stride;
+                    w[e] = p[e] = z[e] = cmk(0, 0);
+                    if (qq < n) {
+                        w[e] = to_cd(ws[qq]);
+                        p[e] = to_cd(vk[qq]);
+                        if (vn) z[e] = to_cd(vn[qq]);
+                    }
+                }
+#pragma unroll
+                for (int e = 0; e < TU; ++e) {
+                    const long long qq = q + e * stride;
+                    if (qq >= n) break;
+                    csub_mul(w[e], h, p[e]);
+                    store_c(ws[qq], w[e]);
+                    const cd wr = rounded<C>(w[e]);
+                    if (vn) cdot_acc(u[0], u[1], z[e], wr);
+                    else u[0] += cabs2(wr);
                 }
             }
-            block_sum<2>(u, bsh);
-            put_partial(a, parity ^ 1, s, u, 2);
+            warp_part<2>(u, wsh, s);
         }
+        for (int s = threadIdx.x; s < a.ns; s += blockDim.x) sact[s] = smode[s] == SLOT_ARNOLDI && k <= sstep[s] + 1;
+        flush_parts(a, parity ^ 1, wsh, sact, 2);
         parity ^= 1;
         grid_barrier(a.bar, gridDim.x, a.err);
         read_totals(a, parity, 2, tot);
@@ -230,15 +311,27 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
         for (int s = 0; s < a.ns; ++s) {
             if (smode[s] != SLOT_ARNOLDI || !(snormav[s] + (double)0.001f * shn[s] == snormav[s]) || j > sstep[s] + 1) continue;
             const C *vj = a.V + (size_t)s * (a.m + 1) * n + (size_t)(j - 1) * n;
-            const C *ws = a.w + (size_t)s * n;
+            const C *ws = a.w + (size_t)swpos[s] * n;
             double u[2] = {0, 0};
-            for (long long q = q0; q < n; q += stride) {
-                const cd z = to_cd(vj[q]), w = to_cd(ws[q]);
-                cdot_acc(u[0], u[1], z, w);
+            for (long long q = q0; q < n; q += TU * stride) {
+                cd z[TU], w[TU];
+#pragma unroll
+                for (int e = 0; e < TU; ++e) {
+                    const long long qq = q + e * stride;
+                    z[e] = w[e] = cmk(0, 0);
+                    if (qq < n) { z[e] = to_cd(vj[qq]); w[e] = to_cd(ws[qq]); }
+                }
+#pragma unroll
+                for (int e = 0; e < TU; ++e) {
+                    if (q + e * stride >= n) break;
+                    cdot_acc(u[0], u[1], z[e], w[e]);
+                }
             }
-            block_sum<2>(u, bsh);
-            put_partial(a, parity ^ 1, s, u, 2);
+            warp_part<2>(u, wsh, s);
         }
+        for (int s = threadIdx.x; s < a.ns; s += blockDim.x)
+            sact[s] = smode[s] == SLOT_ARNOLDI && snormav[s] + (double)0.001f * shn[s] == snormav[s] && j <= sstep[s] + 1;
+        flush_parts(a, parity ^ 1, wsh, sact, 2);
         parity ^= 1;
         grid_barrier(a.bar, gridDim.x, a.err);
         read_totals(a, parity, 2, tot);
@@ -251,24 +344,48 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
                 Hc[j - 1] = cadd(Hc[j - 1], hr);
             }
             const C *vj = a.V + (size_t)s * (a.m + 1) * n + (size_t)(j - 1) * n;
-            C *ws = a.w + (size_t)s * n;
-            for (long long q = q0; q < n; q += stride) {
-                cd w = to_cd(ws[q]);
-                const cd p = to_cd(vj[q]);
-                csub_mul(w, hr, p);
-                store_c(ws[q], w);
+            C *ws = a.w + (size_t)swpos[s] * n;
+            for (long long q = q0; q < n; q += TU * stride) {
+                cd w[TU], p[TU];
+#pragma unroll
+                for (int e = 0; e < TU; ++e) {
+                    const long long qq = q + e * stride;
+                    w[e] = p[e] = cmk(0, 0);
+                    if (qq < n) { w[e] = to_cd(ws[qq]); p[e] = to_cd(vj[qq]); }
+                }
+#pragma unroll
+                for (int e = 0; e < TU; ++e) {
+                    const long long qq = q + e * stride;
+                    if (qq >= n) break;
+                    csub_mul(w[e], hr, p[e]);
+                    store_c(ws[qq], w[e]);
+                }
             }
         }
     }
     if (jmax > 0) {
         for (int s = 0; s < a.ns; ++s) {
             if (smode[s] != SLOT_ARNOLDI || !(snormav[s] + (double)0.001f * shn[s] == snormav[s])) continue;
-            const C *ws = a.w + (size_t)s * n;
+            const C *ws = a.w + (size_t)swpos[s] * n;
             double u[1] = {0};
-            for (long long q = q0; q < n; q += stride) u[0] += cabs2(to_cd(ws[q]));
-            block_sum<1>(u, bsh);
-            put_partial(a, parity ^ 1, s, u, 1);
+            for (long long q = q0; q < n; q += TU * stride) {
+                cd w[TU];
+#pragma unroll
+                for (int e = 0; e < TU; ++e) {
+                    const long long qq = q + e * stride;
+                    w[e] = qq < n ? to_cd(ws[qq]) : cmk(0, 0);
+                }
+#pragma unroll
+                for (int e = 0; e < TU; ++e) {
+                    if (q + e * stride >= n) break;
+                    u[0] += cabs2(w[e]);
+                }
+            }
+            warp_part<1>(u, wsh, s);
         }
+        for (int s = threadIdx.x; s < a.ns; s += blockDim.x)
+            sact[s] = smode[s] == SLOT_ARNOLDI && snormav[s] + (double)0.001f * shn[s] == snormav[s];
+        flush_parts(a, parity ^ 1, wsh, sact, 1);
         parity ^= 1;
         grid_barrier(a.bar, gridDim.x, a.err);
         read_totals(a, parity, 1, tot);
@@ -282,11 +399,20 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
         if (smode[s] != SLOT_ARNOLDI) continue;
         const int i = sstep[s] + 1;
         const double hn = shn[s];
-        const C *ws = a.w + (size_t)s * n;
+        const C *ws = a.w + (size_t)swpos[s] * n;
         C *vi = a.V + (size_t)s * (a.m + 1) * n + (size_t)i * n;
-        for (long long q = q0; q < n; q += stride) {
-            const cd w = to_cd(ws[q]);
-            store_c(vi[q], (hn != 0.0) ? cmk(w.x / hn, w.y / hn) : w);
+        for (long long q = q0; q < n; q += TU * stride) {
+            cd w[TU];
+#pragma unroll
+            for (int e = 0; e < TU; ++e) {
+                const long long qq = q + e * stride;
+                w[e] = qq < n ? to_cd(ws[qq]) : cmk(0, 0);
+            }
+#pragma unroll
+            for (int e = 0; e < TU; ++e) {
+                const long long qq = q + e * stride;
+                if (qq < n) store_c(vi[qq], (hn != 0.0) ? cmk(w[e].x / hn, w[e].y / hn) : w[e]);
+            }
         }
     }
     if (blockIdx.x == 0) {
@@ -370,17 +496,15 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
     }
 }
 
-// matvec input per slot: x at a cycle start, v_step during Arnoldi; idle
-// slots are skipped by every matvec kernel
+// matvec input per slot, compacted: x at a cycle start, v_step during
+// Arnoldi, into column mpos; slots without a matvec this tick have mpos < 0
 template <typename C>
-__global__ void k_stage(const Slot *slots, int ns, const C *V, const C *x, C *Xin, int *skip, long long n, int m) {
+__global__ void k_stage(const Slot *slots, int ns, const C *V, const C *x, C *Xin, long long n, int m) {
     const int s = blockIdx.y;
-    const int md = slots[s].mode;
-    const bool act = (md == SLOT_START && !slots[s].zero_x) || md == SLOT_ARNOLDI;
-    if (blockIdx.x == 0 && threadIdx.x == 0) skip[s] = act ? 0 : 1;
-    if (!act) return;
+    const int md = slots[s].mode, pos = slots[s].mpos;
+    if (pos < 0) return;
     const C *src = md == SLOT_START ? x + (size_t)s * n : V + ((size_t)s * (m + 1) + slots[s].step) * n;
-    C *dst = Xin + (size_t)s * n;
+    C *dst = Xin + (size_t)pos * n;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
         dst[q] = src[q];
 }
@@ -399,13 +523,12 @@ __global__ void k_outer_update(const Slot *slots, cd *x64, const cf *d32, long l
     }
 }
 
-__global__ void k_stage_resid(const Slot *slots, const cd *x64, cd *Xin, int *skip, long long n) {
+__global__ void k_stage_resid(const Slot *slots, const cd *x64, cd *Xin, long long n) {
     const int s = blockIdx.y;
-    const bool act = slots[s].mode == SLOT_RESID;
-    if (blockIdx.x == 0 && threadIdx.x == 0) skip[s] = act ? 0 : 1;
-    if (!act) return;
+    const int pos = slots[s].rpos;
+    if (slots[s].mode != SLOT_RESID || pos < 0) return;
     for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
-        Xin[(size_t)s * n + q] = x64[(size_t)s * n + q];
+        Xin[(size_t)pos * n + q] = x64[(size_t)s * n + q];
 }
 
 struct ResidArgs {
@@ -435,7 +558,7 @@ __global__ void __launch_bounds__(BT) k_resid(ResidArgs a) {
     for (int s = 0; s < a.ns; ++s) {
         if (smode[s] != SLOT_RESID) continue;
         double v[2] = {0, 0};
-        const cd *bs = a.b64 + (size_t)s * n, *ws = a.w64 + (size_t)s * n;
+        const cd *bs = a.b64 + (size_t)s * n, *ws = a.w64 + (size_t)max(a.slots[s].rpos, 0) * n;
         for (long long q = q0; q < n; q += stride) {
             const cd b = bs[q], r = csub(b, ws[q]);
             v[0] += cabs2(r);
@@ -472,7 +595,7 @@ __global__ void __launch_bounds__(BT) k_resid(ResidArgs a) {
         const double rel = bn > 0.0 ? rho / bn : 0.0;
         const bool stop = !(rel >= a.tol) || a.slots[s].outer >= a.max_outer;   // NaN stops too
         if (!stop) {
-            const cd *bs = a.b64 + (size_t)s * n, *ws = a.w64 + (size_t)s * n;
+            const cd *bs = a.b64 + (size_t)s * n, *ws = a.w64 + (size_t)max(a.slots[s].rpos, 0) * n;
             cf *rs = a.rhs32 + (size_t)s * n, *xs = a.x32 + (size_t)s * n;
             for (long long q = q0; q < n; q += stride) {
                 const cd r = csub(bs[q], ws[q]);
@@ -584,15 +707,17 @@ int batch_prepare(scd_ctx *c, int ns, int m, int mixed, BatchBuffers &b) {
 }
 
 template <typename C>
-static int launch_tick(scd_ctx *c, BatchBuffers &bb, int ns, int m, int cycles, double tol, int mixed) {
+static int launch_tick(scd_ctx *c, BatchBuffers &bb, int ns, int nact, int m, int cycles, double tol, int mixed) {
     TickArgs<C> a;
     a.slots = bb.slots; a.ns = ns; a.V = (C *)bb.V; a.H = bb.H; a.cs = bb.cs; a.sn = bb.sn; a.g = bb.g; a.y = bb.y;
     a.x = (C *)bb.x; a.rhs = (C *)bb.rhs; a.w = (C *)bb.W; a.red = bb.red; a.bar = c->d_bar; a.err = c->d_err;
     a.n = c->n; a.m = m; a.max_cycles = cycles; a.tol = tol; a.mixed = mixed;
     const long long n = c->n;
-    k_stage<C><<<dim3(std::min<long long>((n + 255) / 256, 1024), ns), 256, 0, c->st>>>(bb.slots, ns, (C *)bb.V, (C *)bb.x,
-                                                                                       (C *)bb.Xin, bb.skip, n, m);
-    run_matvec(c, (const C *)bb.Xin, (C *)bb.W, ns, bb.skip);
+    if (nact > 0) {
+        k_stage<C><<<dim3(std::min<long long>((n + 255) / 256, 1024), ns), 256, 0, c->st>>>(bb.slots, ns, (C *)bb.V,
+                                                                                           (C *)bb.x, (C *)bb.Xin, n, m);
+        run_matvec(c, (const C *)bb.Xin, (C *)bb.W, nact, nullptr);
+    }
     void *args[] = {&a};
     cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_tick<C>, dim3(bb.grid), dim3(BT), args, 0, c->st);
     c->launches += 2;
@@ -675,13 +800,21 @@ int batch_solve(scd_ctx *c, int ncol, const cd *const *rhs_cols, cd *X, double t
         }
         if (finished >= ncol) break;
         if (!inner && !resid) return set_error(c, SCD_CUDA_ERROR, "batch solver stalled");
+        // compacted matvec columns: only slots that need A x this tick
+        int nact = 0, nres = 0;
+        for (int s = 0; s < ns; ++s) {
+            hs[s].mpos = -1;
+            hs[s].rpos = -1;
+            if (hs[s].mode == SLOT_RESID) hs[s].rpos = nres++;
+            if ((hs[s].mode == SLOT_START && !hs[s].zero_x) || hs[s].mode == SLOT_ARNOLDI) hs[s].mpos = nact++;
+        }
         cudaMemcpyAsync(bb.slots, hs, sizeof(Slot) * ns, cudaMemcpyHostToDevice, c->st);
         if (mixed) {
             const dim3 g2(std::min<long long>((n + 255) / 256, 1024), ns);
             if (upd) k_outer_update<<<g2, 256, 0, c->st>>>(bb.slots, bb.x64, (const cf *)bb.x, n);
             if (resid) {
-                k_stage_resid<<<g2, 256, 0, c->st>>>(bb.slots, bb.x64, bb.Xin64, bb.skip64, n);
-                run_matvec(c, (const cd *)bb.Xin64, bb.W64, ns, bb.skip64);
+                k_stage_resid<<<g2, 256, 0, c->st>>>(bb.slots, bb.x64, bb.Xin64, n);
+                run_matvec(c, (const cd *)bb.Xin64, bb.W64, nres, nullptr);
                 ResidArgs ra;
                 ra.slots = bb.slots; ra.ns = ns; ra.b64 = bb.b64; ra.w64 = bb.W64; ra.rhs32 = (cf *)bb.rhs;
                 ra.x32 = (cf *)bb.x; ra.red = bb.red; ra.bar = c->d_bar; ra.err = c->d_err; ra.n = n; ra.tol = tol;
@@ -691,9 +824,9 @@ int batch_solve(scd_ctx *c, int ncol, const cd *const *rhs_cols, cd *X, double t
                 c->launches += 3 + (upd ? 1 : 0);
                 if ((rc = check_cuda(c, e, "residual launch"))) return rc;
             }
-            if ((rc = launch_tick<cf>(c, bb, ns, m, cycles, gm_tol, 1))) return rc;
+            if ((rc = launch_tick<cf>(c, bb, ns, nact, m, cycles, gm_tol, 1))) return rc;
         } else {
-            if ((rc = launch_tick<cd>(c, bb, ns, m, cycles, gm_tol, 0))) return rc;
+            if ((rc = launch_tick<cd>(c, bb, ns, nact, m, cycles, gm_tol, 0))) return rc;
         }
         cudaMemcpyAsync(hs, bb.slots, sizeof(Slot) * ns, cudaMemcpyDeviceToHost, c->st);
         if ((rc = check_cuda(c, cudaStreamSynchronize(c->st), "tick"))) return rc;

@@ -170,3 +170,114 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double *sh) {
     }
     __syncthreads();
 }
+
+// ---- asynchronous copies into shared memory ----
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// element copy global -> shared (LDGSTS); src_bytes = 0 fills zeros
+template <int BYTES>
+__device__ __forceinline__ void cp_async_el(void *dst, const void *src, bool valid) {
+    const int n = valid ? BYTES : 0;
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_addr(dst)), "l"(src), "r"(n) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(smem_addr(dst)), "l"(src), "n"(BYTES), "r"(n)
+                     : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// mbarrier + one-dimensional bulk copy (TMA engine, no tensor map): the
+// copy's completion is counted on the barrier in bytes.
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+// dst, src 16-byte aligned; bytes a multiple of 16
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for phase `parity` of *bar: after `limit` polls the thread
+// records a timeout in *err and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err, long long limit = (1LL << 22)) {
+    for (long long k = 0; k < limit; ++k) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (k > 16) __nanosleep(64);
+    }
+    atomicExch(err, 1);
+    return false;
+}
+// arrive on *bar once every cp.async issued so far by this thread has landed
+// (the barrier's expected count includes this arrival)
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t *bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// acc[a][u] += m[a] * x[u] for a 3 x U register tile.  Per accumulator the
+// operation sequence equals cfma (re: fma(m.x, x.x) then fma(-m.y, x.y);
+// im: fma(m.x, x.y) then fma(m.y, x.x)); the first halves of all products
+// are issued before the second halves so that the dependent pairs are far
+// apart in the instruction stream.
+template <typename C, int U>
+__device__ __forceinline__ void mac3(C (&acc)[3][U], const C (&m)[3], const C (&x)[U]) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if constexpr (sizeof(C) == 16) {
+                acc[a][u].x = SCD_FMA(m[a].x, x[u].x, acc[a][u].x);
+                acc[a][u].y = SCD_FMA(m[a].x, x[u].y, acc[a][u].y);
+            } else {
+                acc[a][u].x = SCD_FMAF(m[a].x, x[u].x, acc[a][u].x);
+                acc[a][u].y = SCD_FMAF(m[a].x, x[u].y, acc[a][u].y);
+            }
+        }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if constexpr (sizeof(C) == 16) {
+                acc[a][u].x = SCD_FMA(-m[a].y, x[u].y, acc[a][u].x);
+                acc[a][u].y = SCD_FMA(m[a].y, x[u].x, acc[a][u].y);
+            } else {
+                acc[a][u].x = SCD_FMAF(-m[a].y, x[u].y, acc[a][u].x);
+                acc[a][u].y = SCD_FMAF(m[a].y, x[u].x, acc[a][u].y);
+            }
+        }
+}
+
+// explicit shared-memory loads at 32-bit shared addresses (ld.shared)
+__device__ __forceinline__ cf lds_c(uint32_t addr, cf) {
+    cf v;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];\n" : "=f"(v.x), "=f"(v.y) : "r"(addr));
+    return v;
+}
+__device__ __forceinline__ cd lds_c(uint32_t addr, cd) {
+    cd v;
+    asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];\n" : "=d"(v.x), "=d"(v.y) : "r"(addr));
+    return v;
+}
+// two consecutive complex64 values (16-byte aligned address)
+__device__ __forceinline__ void lds_c2(uint32_t addr, cf &a, cf &b) {
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];\n" : "=f"(a.x), "=f"(a.y), "=f"(b.x), "=f"(b.y) : "r"(addr));
+}

@@ -13,21 +13,31 @@
 #include "../../include/scadyn_gpu.h"
 #include "common.cuh"
 
-// largest number of tets in one projection box that the near-zone kernels
-// handle (register-resident column accumulators)
-#define SCD_NEAR_MAXN 64
+// Near-zone groups: runs of consecutive slots of one projection box (cube)
+// holding at most SCD_GROUP_MAX tets; a box with more tets is split into
+// near-equal groups.  Tiles couple groups, so a tile's blocks, its two x
+// segments and its partial sums fit a CTA's shared memory together.
+#define SCD_GROUP_MAX 24
 
-// One dense tile of near-zone blocks coupling the tets of cube c1 (rows) to
-// the tets of cube c2 (columns), c1 <= c2.  Block (i, j) is the 3x3 matrix
-// that maps the unknowns of slot off(c2)+j onto the equations of slot
-// off(c1)+i; it is stored at data[(data_off + i*n2 + j)*9 + r + 3c].
-// Diagonal tiles (c1 == c2) hold the full symmetric n1 x n1 pattern.
+// One dense tile of near-zone blocks coupling the tets of group g1 (rows) to
+// the tets of group g2 (columns), g1 <= g2.  Block (i, j) is the 3x3 matrix
+// that maps the unknowns of slot s2+j onto the equations of slot s1+i; its
+// element e = r + 3c is stored at data[data_off + tile_at(n1, i, j, e)]:
+// planes over the row index i with the odd stride n1|1, so that lanes over i
+// and lanes over j both read shared memory without bank conflicts.  A tile
+// takes tile_elems(n1, n2) elements, an even count, so that tiles of
+// complex64 start on 16-byte boundaries.  Diagonal tiles (g1 == g2) hold the
+// full symmetric n1 x n1 pattern.
 struct NearTile {
-    int c1, c2, n1, n2;
-    long long data_off;   // in blocks
-    long long row_off;    // partial-sum slot of c1 (complex elements)
-    long long col_off;    // partial-sum slot of c2, -1 for diagonal tiles
+    int g1, g2;           // groups
+    int c1, c2;           // projection boxes of the two groups
+    int s1, s2;           // first slot of each group
+    int n1, n2;           // tets of each group
+    long long data_off;   // first element
+    long long col_off;    // partial slot of g2 that receives M^T x (complex elements), -1 on diagonal tiles
 };
+SCD_HD long long tile_elems(int n1, int n2) { return ((long long)9 * n2 * (n1 | 1) + 1) & ~1LL; }
+SCD_HD long long tile_at(int n1, int i, int j, int e) { return (long long)(9 * j + e) * (n1 | 1) + i; }
 
 struct GmresState {
     double b_norm;     // ||rhs||
@@ -63,6 +73,12 @@ struct scd_ctx {
     std::vector<int> cube_off;           // ncubes + 1
     int max_per_cube = 0;
     int *d_perm = nullptr, *d_cube_off = nullptr;
+    // near-zone groups (see SCD_GROUP_MAX), numbered in slot order
+    int ngroups = 0, max_per_group = 0;
+    std::vector<int> grp_off;            // ngroups + 1 slot offsets
+    std::vector<int> grp_cube;           // projection box of each group
+    std::vector<int> grp_of_slot;
+    int *d_grp_off = nullptr, *d_grp_cube = nullptr;
 
     // projectors: d_P[(g*27 + j)*T + slot], g = S, Sx, Sy, Sz
     bool have_proj = false;
@@ -80,10 +96,18 @@ struct scd_ctx {
     void *d_tdata = nullptr;
     NearTile *d_tiles = nullptr;
     int ntiles = 0;
-    long long tile_blocks = 0;
+    long long tile_blocks = 0;           // n1*n2 summed over the tiles
+    long long tile_store = 0;            // stored elements (tile_elems summed)
+    long long max_tile_store = 0;        // largest tile_elems
     long long B_ref = 0;                 // blocks in the reference layout
-    std::vector<long long> pslot_base;   // per cube, complex offset of its first slot
-    std::vector<int> pslot_cnt;          // per cube, number of slots
+    // partial-sum slots per group: slot 0 holds the group's row sums over
+    // all its tiles, slots 1.. the M^T x products of the tiles (g', g),
+    // g' < g, in tile order
+    std::vector<long long> pslot_base;   // per group, complex offset of its first slot
+    std::vector<int> pslot_cnt;          // per group, number of slots
+    std::vector<int> grp_tile;           // ngroups + 1: first tile whose g1 is the group
+    int *d_grp_tile = nullptr;
+    int *d_kerr = nullptr;               // near-zone kernel error word (bounded waits)
     long long *d_pslot_base = nullptr;
     int *d_pslot_cnt = nullptr;
     long long part_len = 0;
@@ -179,3 +203,4 @@ void launch_T_assemble(scd_ctx *c, const cd *d_mat, int ncol_total, int col0, in
 int set_error(scd_ctx *c, int code, const char *fmt, ...);
 int check_cuda(scd_ctx *c, cudaError_t e, const char *what);
 int ensure_work(scd_ctx *c, int nrhs);
+int near_status(scd_ctx *c);   // SCD_TIMEOUT if a near-zone pipeline wait ran out (and clears it)

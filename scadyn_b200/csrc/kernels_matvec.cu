@@ -348,139 +348,223 @@ k_fft_x_inv(const Cx *__restrict__ W, Cx *__restrict__ R, const Cx *__restrict__
 }
 
 // ------------------------------------------------------------ near zone
-// Row sums y(c1) += M x(c2) and, for off-diagonal tiles, column sums
-// y(c2) += M^T x(c1) (transpose, not conjugate: the operator is complex
+// Row sums y(g1) += M x(g2) and, for off-diagonal tiles, column sums
+// y(g2) += M^T x(g1) (transpose, not conjugate: the operator is complex
 // symmetric, src/sparse_mat.f90:113-116).  M(3i+a, 3j+b) is entry (a,b) of
-// block (i,j), stored at D[(i*n2 + j)*9 + a + 3b].  Results go to per-cube
-// partial slots that k_gather adds in a fixed order (deterministic).
-constexpr int NZ_MAXN = 64;            // tets per cube supported (two lanes' worth)
+// block (i,j), at tile_at(n1, i, j, a + 3b) (see NearTile).
+//
+// One CTA per group g: it walks the tiles (g, g2), g2 >= g, in tile order,
+// keeping the group's row sums in registers across them, so every group has
+// a single row slot; each off-diagonal tile's column sums go to that tile's
+// partial slot of g2.  k_gather adds the slots in a fixed order.
+//
+// Tiles stream through NZ_STAGES shared-memory stages filled by a producer
+// warp: the tile's blocks arrive by one bulk copy (TMA engine, completion
+// counted in bytes on the stage's "full" mbarrier) and the tile's x segment
+// by element copies (LDGSTS, transposed to x[3j+b][r], completion signalled
+// on the same barrier).  Consumer warps release a stage on its "empty"
+// barrier; there is no CTA-wide barrier in the tile loop, so row and column
+// warps run independently.  Warps [0, HT) hold row items (quad q, block row
+// i): a 3 x U register tile of row sums for right-hand sides Uq..Uq+U-1.
+// Warps [HT, 2HT) hold column items (q, block column j).  Lanes run over i
+// (resp. j), so with the odd plane stride both sides read the tile without
+// bank conflicts, and x is a broadcast.
+//
+// Every sum runs in one canonical order -- row sums: tiles in order, then
+// j = 0..n2-1, then b = 0..2; column sums: i = 0..n1-1, then a = 0..2 --
+// for any number of right-hand sides and any U, so a column's result does
+// not depend on the batch it is solved in.
+constexpr int NZ_QMAX = 4;             // quads of right-hand sides per pass
+constexpr int NZ_STAGES = 2;
+constexpr int NZ_MAX_THREADS = 2 * 32 * ((SCD_GROUP_MAX * NZ_QMAX + 31) / 32) + 32;
 
-// One warp per tile (4 tiles per CTA).  Tile rows stream through a
-// two-row shared-memory ring with cp.async (coalesced 8/16-byte copies): row
-// i+1 is in flight while row i is used.  Lane j takes block (i, j) from
-// shared memory and applies it to RG right-hand sides; each row sum is
-// reduced across the warp (xor tree), column j accumulates in lane j over the
-// rows in order.  The arithmetic of one right-hand side is the same for every
-// RG, so a column's result does not depend on the batch it is solved in.
-__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
-    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-    const unsigned sa = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+struct NearPass {
+    const NearTile *tiles;
+    const int *grp_tile, *grp_off;
+    const long long *pslot_base;
+    const void *data;
+    const void *x;
+    long long ld;
+    void *part;
+    long long part_len;
+    const int *skip;
+    int nrhs, nq, half;
+    long long stage_elems;   // ST elements per tile stage (even)
+    int xcap;                // C elements per x buffer
+    int *err;
+};
 
-template <typename ST>
-__device__ __forceinline__ void copy_row_async(ST *dst, const ST *src, int nel, int lane) {
-    for (int e = lane; e < nel; e += 32) {
-        if (sizeof(ST) == 8) cp_async8(dst + e, src + e);
-        else cp_async16(dst + e, src + e);
+// U consecutive values of C from shared address addr (16-byte aligned when
+// C is complex64 and U is even)
+template <typename C, int U>
+__device__ __forceinline__ void load_xu(uint32_t addr, C (&xu)[U]) {
+    if constexpr (sizeof(C) == 8 && U % 2 == 0) {
+#pragma unroll
+        for (int u = 0; u < U; u += 2) lds_c2(addr + 8 * u, xu[u], xu[u + 1]);
+    } else {
+#pragma unroll
+        for (int u = 0; u < U; ++u) xu[u] = lds_c(addr + (uint32_t)sizeof(C) * u, C{});
     }
-    cp_async_commit();
 }
 
-constexpr int NZ_WARPS = 4;
+template <typename ST, typename C, int U>
+__global__ void __launch_bounds__(NZ_MAX_THREADS) k_near_groups(NearPass a) {
+    extern __shared__ __align__(128) unsigned char nz_sh[];
+    uint64_t *full = reinterpret_cast<uint64_t *>(nz_sh);
+    uint64_t *empty = full + NZ_STAGES;
+    ST *const Ms0 = reinterpret_cast<ST *>(nz_sh + 128);                    // tile stages
+    C *const Xs0 = reinterpret_cast<C *>(Ms0 + NZ_STAGES * a.stage_elems);  // x(g2) stages
+    C *const X1 = Xs0 + NZ_STAGES * a.xcap;                                 // x(g)
+    const ST *data = static_cast<const ST *>(a.data);
+    const C *x = static_cast<const C *>(a.x);
+    C *part = static_cast<C *>(a.part);
 
-template <typename ST, typename C, int U, int RG>
-__global__ void __launch_bounds__(32 * NZ_WARPS)
-k_near_warp(const NearTile *__restrict__ tiles, int ntiles, const ST *__restrict__ data, const C *__restrict__ x,
-            long long ld, const int *__restrict__ cube_off, C *__restrict__ part, long long part_len,
-            const int *skip, int nrhs, int row_cap) {
-    extern __shared__ __align__(16) unsigned char nz_sh[];
+    const int g = blockIdx.x;
+    const int t0 = a.grp_tile[g], t1 = a.grp_tile[g + 1];
+    const int s1 = a.grp_off[g], n1 = a.grp_off[g + 1] - s1;
+    const int ld1 = n1 | 1;
+    const int RG = a.nq * U;
+    const int HT = a.half;
+    const int ncw = 2 * HT / 32;                 // consumer warps
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int t = blockIdx.x * NZ_WARPS + warp;
-    if (t >= ntiles) return;
-    ST *ring = (ST *)nz_sh + (size_t)warp * 2 * row_cap;       // two rows of this warp
-    const NearTile tl = tiles[t];
-    const int n1 = tl.n1, n2 = tl.n2;
-    const int s1 = cube_off[tl.c1], s2 = cube_off[tl.c2];
-    const ST *D = data + tl.data_off * 9;
-    const bool offd = tl.col_off >= 0;
-    const int nel = 9 * n2;
-    for (int r0 = 0; r0 < nrhs; r0 += RG) {
-        bool act[RG];
-        C y[RG][U][3], ca[RG][U][3];
-#pragma unroll
-        for (int rr = 0; rr < RG; ++rr) {
-            const int r = r0 + rr;
-            act[rr] = r < nrhs && !(skip && skip[r]);
-            const C *x2 = x + r * ld + 3LL * s2;
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int j = lane + 32 * u;
-                ca[rr][u][0] = ca[rr][u][1] = ca[rr][u][2] = czero<C>();
-                y[rr][u][0] = y[rr][u][1] = y[rr][u][2] = czero<C>();
-                if (act[rr] && j < n2) { y[rr][u][0] = x2[3 * j]; y[rr][u][1] = x2[3 * j + 1]; y[rr][u][2] = x2[3 * j + 2]; }
+
+    if (threadIdx.x == 0) {
+        for (int st = 0; st < NZ_STAGES; ++st) {
+            mbar_init(&full[st], 33);            // producer lane 0 (bytes) + 32 lanes' LDGSTS
+            mbar_init(&empty[st], ncw);
+        }
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    if (warp == ncw) {
+        // ------------------------------------------------------ producer
+        int ord = 0;
+        for (int r0 = 0; r0 < a.nrhs; r0 += RG) {
+            const int rg = min(RG, a.nrhs - r0);
+            for (int t = t0; t < t1; ++t, ++ord) {
+                const int st = ord % NZ_STAGES, use = ord / NZ_STAGES;
+                if (use > 0) mbar_wait(&empty[st], (uint32_t)((use - 1) & 1), a.err);
+                if (t == t0 && ord > 0) {
+                    // X1 is rewritten: every consumer must be done with the previous pass
+                    const int pst = (ord - 1) % NZ_STAGES, puse = (ord - 1) / NZ_STAGES;
+                    mbar_wait(&empty[pst], (uint32_t)(puse & 1), a.err);
+                }
+                const NearTile &tl = a.tiles[t];
+                if (lane == 0) {
+                    const uint32_t bytes = (uint32_t)(tile_elems(tl.n1, tl.n2) * (long long)sizeof(ST));
+                    mbar_expect_tx(&full[st], bytes);
+                    bulk_g2s(Ms0 + st * a.stage_elems, data + tl.data_off, bytes, &full[st]);
+                }
+                {
+                    const int w = 3 * tl.n2;
+                    const C *xs = x + 3LL * tl.s2;
+                    C *dst = Xs0 + st * a.xcap;
+                    for (int e = lane; e < w * RG; e += 32) {
+                        const int r = e / w, k = e - r * w;
+                        const bool v = r < rg;
+                        cp_async_el<sizeof(C)>(dst + k * RG + r, v ? xs + (long long)(r0 + r) * a.ld + k : xs, v);
+                    }
+                }
+                if (t == t0) {
+                    const int w = 3 * n1;
+                    const C *xs = x + 3LL * s1;
+                    for (int e = lane; e < w * RG; e += 32) {
+                        const int r = e / w, k = e - r * w;
+                        const bool v = r < rg;
+                        cp_async_el<sizeof(C)>(X1 + k * RG + r, v ? xs + (long long)(r0 + r) * a.ld + k : xs, v);
+                    }
+                }
+                cp_async_arrive_noinc(&full[st]);
             }
         }
-        __syncwarp();
-        copy_row_async(ring, D, nel, lane);
-        for (int i = 0; i < n1; ++i) {
-            ST *cur = ring + (size_t)(i & 1) * row_cap;
-            if (i + 1 < n1) {
-                copy_row_async(ring + (size_t)((i + 1) & 1) * row_cap, D + (size_t)(i + 1) * nel, nel, lane);
-                cp_async_wait<1>();
-            } else {
-                cp_async_wait<0>();
+        cp_async_wait_all();
+        return;
+    }
+
+    // ---------------------------------------------------------- consumers
+    const bool rowside = warp < HT / 32;
+    const int it = rowside ? threadIdx.x : threadIdx.x - HT;
+    const bool row_item = rowside && it < n1 * a.nq;
+    const int rq = row_item ? it / n1 : 0, ri = row_item ? it - rq * n1 : 0;
+    int ord = 0;
+    for (int r0 = 0; r0 < a.nrhs; r0 += RG) {
+        const int rg = min(RG, a.nrhs - r0);
+        C acc[3][U];
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+#pragma unroll
+            for (int u = 0; u < U; ++u) acc[q][u] = czero<C>();
+        for (int t = t0; t < t1; ++t, ++ord) {
+            const int st = ord % NZ_STAGES, use = ord / NZ_STAGES;
+            mbar_wait(&full[st], (uint32_t)(use & 1), a.err);
+            const NearTile &tl = a.tiles[t];
+            const int n2 = tl.n2;
+            const uint32_t M = smem_addr(Ms0 + st * a.stage_elems);
+            const uint32_t X2 = smem_addr(Xs0 + st * a.xcap);
+            constexpr uint32_t SB = sizeof(ST), CB = sizeof(C);
+            const uint32_t mrow = SB * ld1, xrow = CB * RG;   // bytes between planes / x rows
+            if (rowside) {
+                if (row_item) {
+                    uint32_t mp = M + SB * ri;            // plane (9j + 3b), lane i
+                    uint32_t xp = X2 + CB * U * rq;       // x row 3j + b
+                    for (int j = 0; j < n2; ++j) {
+#pragma unroll
+                        for (int b = 0; b < 3; ++b) {
+                            C xu[U];
+                            load_xu<C, U>(xp, xu);
+                            const C mm[3] = {as_c<C>(lds_c(mp, ST{})), as_c<C>(lds_c(mp + mrow, ST{})),
+                                             as_c<C>(lds_c(mp + 2 * mrow, ST{}))};
+                            mac3<C, U>(acc, mm, xu);
+                            mp += 3 * mrow;
+                            xp += xrow;
+                        }
+                    }
+                }
+            } else if (tl.col_off >= 0 && it < n2 * a.nq) {
+                const int q = it / n2, j = it - q * n2;
+                C cacc[3][U];
+#pragma unroll
+                for (int b = 0; b < 3; ++b)
+#pragma unroll
+                    for (int u = 0; u < U; ++u) cacc[b][u] = czero<C>();
+                const uint32_t mj = M + SB * 9 * j * ld1;
+                uint32_t xp = smem_addr(X1) + CB * U * q;   // x row 3i + a
+                for (int i = 0; i < n1; ++i) {
+#pragma unroll
+                    for (int aa = 0; aa < 3; ++aa) {
+                        C xu[U];
+                        load_xu<C, U>(xp, xu);
+                        const uint32_t mp = mj + aa * mrow + SB * i;
+                        const C mm[3] = {as_c<C>(lds_c(mp, ST{})), as_c<C>(lds_c(mp + 3 * mrow, ST{})),
+                                         as_c<C>(lds_c(mp + 6 * mrow, ST{}))};
+                        mac3<C, U>(cacc, mm, xu);
+                        xp += xrow;
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int r = U * q + u;
+                    if (r < rg && !(a.skip && a.skip[r0 + r])) {
+                        C *pc = part + (r0 + r) * a.part_len + tl.col_off + 3 * j;
+                        pc[0] = cacc[0][u];
+                        pc[1] = cacc[1][u];
+                        pc[2] = cacc[2][u];
+                    }
+                }
             }
             __syncwarp();
-            C m[U][9];
+            if (lane == 0) mbar_arrive(&empty[st]);
+        }
+        if (row_item) {
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                const int j = lane + 32 * u;
-#pragma unroll
-                for (int q = 0; q < 9; ++q) m[u][q] = (j < n2) ? as_c<C>(cur[9 * j + q]) : czero<C>();
-            }
-            __syncwarp();      // the ring slot may be refilled after this
-#pragma unroll
-            for (int rr = 0; rr < RG; ++rr) {
-                if (!act[rr]) continue;           // uniform across the warp
-                const C *x1 = x + (r0 + rr) * ld + 3LL * s1;
-                const C xa0 = x1[3 * i], xa1 = x1[3 * i + 1], xa2 = x1[3 * i + 2];
-                C t0 = czero<C>(), t1 = t0, t2 = t0;
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    cfma(t0, m[u][0], y[rr][u][0]); cfma(t1, m[u][1], y[rr][u][0]); cfma(t2, m[u][2], y[rr][u][0]);
-                    cfma(t0, m[u][3], y[rr][u][1]); cfma(t1, m[u][4], y[rr][u][1]); cfma(t2, m[u][5], y[rr][u][1]);
-                    cfma(t0, m[u][6], y[rr][u][2]); cfma(t1, m[u][7], y[rr][u][2]); cfma(t2, m[u][8], y[rr][u][2]);
-                    if (offd) {
-                        cfma(ca[rr][u][0], m[u][0], xa0); cfma(ca[rr][u][0], m[u][1], xa1); cfma(ca[rr][u][0], m[u][2], xa2);
-                        cfma(ca[rr][u][1], m[u][3], xa0); cfma(ca[rr][u][1], m[u][4], xa1); cfma(ca[rr][u][1], m[u][5], xa2);
-                        cfma(ca[rr][u][2], m[u][6], xa0); cfma(ca[rr][u][2], m[u][7], xa1); cfma(ca[rr][u][2], m[u][8], xa2);
-                    }
-                }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    t0.x += __shfl_xor_sync(0xffffffffu, t0.x, o);
-                    t0.y += __shfl_xor_sync(0xffffffffu, t0.y, o);
-                    t1.x += __shfl_xor_sync(0xffffffffu, t1.x, o);
-                    t1.y += __shfl_xor_sync(0xffffffffu, t1.y, o);
-                    t2.x += __shfl_xor_sync(0xffffffffu, t2.x, o);
-                    t2.y += __shfl_xor_sync(0xffffffffu, t2.y, o);
-                }
-                C *pr = part + (r0 + rr) * part_len + tl.row_off + 3 * i;
-                if (lane == 0) pr[0] = t0;
-                else if (lane == 1) pr[1] = t1;
-                else if (lane == 2) pr[2] = t2;
-            }
-        }
-        if (offd) {
-#pragma unroll
-            for (int rr = 0; rr < RG; ++rr) {
-                if (!act[rr]) continue;
-                C *pc = part + (r0 + rr) * part_len + tl.col_off;
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int j = lane + 32 * u;
-                    if (j < n2) {
-                        pc[3 * j] = ca[rr][u][0];
-                        pc[3 * j + 1] = ca[rr][u][1];
-                        pc[3 * j + 2] = ca[rr][u][2];
-                    }
+                const int r = U * rq + u;
+                if (r < rg && !(a.skip && a.skip[r0 + r])) {
+                    C *pr = part + (r0 + r) * a.part_len + a.pslot_base[g] + 3 * ri;
+                    pr[0] = acc[0][u];
+                    pr[1] = acc[1][u];
+                    pr[2] = acc[2][u];
                 }
             }
         }
@@ -489,29 +573,29 @@ k_near_warp(const NearTile *__restrict__ tiles, int ntiles, const ST *__restrict
 
 // ---------------------------------------------------------------- gather
 // Interpolation (sparse_eps_matmul, src/sparse.f90:47-77) and final
-// assembly (src/gmres_module.f90:148-170), one warp per cube, one lane per
-// tet: the 27 box-node values of the four result grids are staged in shared
-// memory for a group of right-hand sides, each lane forms its tet's six
-// 27-term sums from the projector rows P[(g*27 + j)*T + slot] (coalesced
-// across lanes), adds the cube's near-zone partial slots in slot order and
-// writes Ax = near + (Y2 - k^2 Y).
+// assembly (src/gmres_module.f90:148-170), one warp per near-zone group, one
+// lane per tet: the 27 box-node values of the four result grids are staged
+// in shared memory for a group of right-hand sides, each lane forms its
+// tet's six 27-term sums from the projector rows P[(g*27 + j)*T + slot]
+// (coalesced across lanes), adds the group's near-zone partial slots in slot
+// order and writes Ax = near + (Y2 - k^2 Y).
 template <typename C, int GA_RG>
 __global__ void __launch_bounds__(32 * WARPS_PER_CTA)
-k_gather(const C *__restrict__ Rg, const C *__restrict__ P, int T, const int *__restrict__ cube_off, GridDims G,
-         typename CReal<C>::type k2, const C *__restrict__ part, long long part_len,
-         const long long *__restrict__ pslot_base, const int *__restrict__ pslot_cnt, C *__restrict__ y, long long ld,
-         const int *skip, int nrhs) {
+k_gather(const C *__restrict__ Rg, const C *__restrict__ P, int T, const int *__restrict__ grp_off,
+         const int *__restrict__ grp_cube, int ngroups, GridDims G, typename CReal<C>::type k2,
+         const C *__restrict__ part, long long part_len, const long long *__restrict__ pslot_base,
+         const int *__restrict__ pslot_cnt, C *__restrict__ y, long long ld, const int *skip, int nrhs) {
     __shared__ C Rs[WARPS_PER_CTA][GA_RG][4][27];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int c = blockIdx.x * WARPS_PER_CTA + warp;
-    if (c >= G.ncubes) return;
-    const int s0 = cube_off[c], s1 = cube_off[c + 1];
-    if (s0 == s1) return;
+    const int gq = blockIdx.x * WARPS_PER_CTA + warp;
+    if (gq >= ngroups) return;
+    const int s0 = grp_off[gq], s1 = grp_off[gq + 1];
     const int nc = s1 - s0;
+    const int c = grp_cube[gq];
     const int bx = c % G.ncx, by = (c / G.ncx) % G.ncy, bz = c / (G.ncx * G.ncy);
     const long long NN = (long long)G.Nx * G.Ny * G.Nz;
-    const long long pbase = pslot_base[c];
-    const int nslot = pslot_cnt[c];
+    const long long pbase = pslot_base[gq];
+    const int nslot = pslot_cnt[gq];
     long long node = 0;
     if (lane < 27) {
         const int a = lane % 3, b = (lane / 3) % 3, cc = lane / 9;
@@ -689,54 +773,57 @@ void fft_chain_t(scd_ctx *c, const C *x, int nrhs, const int *done) {
 }
 
 template <typename ST, typename C, int U>
-void near_dispatch_u(scd_ctx *c, const ST *data, const C *x, int nrhs, const int *done) {
-    const int row_cap = 9 * c->max_per_cube;
-    const size_t sh = sizeof(ST) * 2 * (size_t)row_cap * NZ_WARPS;
-    const int grid = (c->ntiles + NZ_WARPS - 1) / NZ_WARPS;
-    C *part = Res<C>::part(c);
-    if (nrhs >= 4) {
-        cudaFuncSetAttribute(k_near_warp<ST, C, U, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-        k_near_warp<ST, C, U, 4><<<grid, 32 * NZ_WARPS, sh, c->st>>>(c->d_tiles, c->ntiles, data, x, c->n,
-                                                                    c->d_cube_off, part, c->part_len, done, nrhs, row_cap);
-    } else if (nrhs >= 2) {
-        cudaFuncSetAttribute(k_near_warp<ST, C, U, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-        k_near_warp<ST, C, U, 2><<<grid, 32 * NZ_WARPS, sh, c->st>>>(c->d_tiles, c->ntiles, data, x, c->n,
-                                                                    c->d_cube_off, part, c->part_len, done, nrhs, row_cap);
-    } else {
-        cudaFuncSetAttribute(k_near_warp<ST, C, U, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-        k_near_warp<ST, C, U, 1><<<grid, 32 * NZ_WARPS, sh, c->st>>>(c->d_tiles, c->ntiles, data, x, c->n,
-                                                                    c->d_cube_off, part, c->part_len, done, nrhs, row_cap);
-    }
+void near_launch(scd_ctx *c, const ST *data, const C *x, int nrhs, const int *done) {
+    NearPass a;
+    a.tiles = c->d_tiles; a.grp_tile = c->d_grp_tile; a.grp_off = c->d_grp_off; a.pslot_base = c->d_pslot_base;
+    a.data = data; a.x = x; a.ld = c->n; a.part = Res<C>::part(c); a.part_len = c->part_len;
+    a.skip = done; a.nrhs = nrhs;
+    a.stage_elems = c->max_tile_store;
+    a.err = c->d_kerr;
+    auto smem = [&](int nq) {
+        return 128 + NZ_STAGES * sizeof(ST) * (size_t)a.stage_elems +
+               (NZ_STAGES + 1) * sizeof(C) * (size_t)(3 * c->max_per_group * nq * U);
+    };
+    const int nq = U == 1 ? 1 : std::min(NZ_QMAX, (nrhs + U - 1) / U);
+    a.nq = nq;
+    a.half = 32 * ((c->max_per_group * a.nq + 31) / 32);
+    a.xcap = 3 * c->max_per_group * a.nq * U;
+    const size_t sh = smem(nq);
+    cudaFuncSetAttribute(k_near_groups<ST, C, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    k_near_groups<ST, C, U><<<c->ngroups, 2 * a.half + 32, sh, c->st>>>(a);
+}
+
+template <typename ST, typename C>
+void near_dispatch(scd_ctx *c, const ST *data, const C *x, int nrhs, const int *done) {
+    if (nrhs == 1) near_launch<ST, C, 1>(c, data, x, nrhs, done);
+    else near_launch<ST, C, 4>(c, data, x, nrhs, done);
 }
 
 template <typename C>
 void near_t(scd_ctx *c, const C *x, int nrhs, const int *done) {
-    if (c->ntiles == 0) return;
-    const bool u1 = c->max_per_cube <= 32;
-    if (c->near_prec == SCD_STORE_C64) {
-        if (u1) near_dispatch_u<cf, C, 1>(c, (const cf *)c->d_tdata, x, nrhs, done);
-        else near_dispatch_u<cf, C, 2>(c, (const cf *)c->d_tdata, x, nrhs, done);
-    } else {
-        if (u1) near_dispatch_u<cd, C, 1>(c, (const cd *)c->d_tdata, x, nrhs, done);
-        else near_dispatch_u<cd, C, 2>(c, (const cd *)c->d_tdata, x, nrhs, done);
-    }
+    if (c->ngroups == 0) return;
+    if (c->near_prec == SCD_STORE_C64) near_dispatch<cf, C>(c, (const cf *)c->d_tdata, x, nrhs, done);
+    else near_dispatch<cd, C>(c, (const cd *)c->d_tdata, x, nrhs, done);
     c->launches += 1;
 }
 
 template <typename C>
 void gather_t(scd_ctx *c, C *y, int nrhs, const int *done) {
     const GridDims G = dims_of(c);
-    dim3 grid((c->ncubes + WARPS_PER_CTA - 1) / WARPS_PER_CTA);
+    dim3 grid((c->ngroups + WARPS_PER_CTA - 1) / WARPS_PER_CTA);
+    if (c->ngroups == 0) return;
     typedef typename CReal<C>::type R;
     const R k2 = (R)(c->k * c->k);
     if (nrhs >= 4)
-        k_gather<C, 4><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(Res<C>::R(c), Res<C>::P(c), c->T, c->d_cube_off, G, k2,
-                                                               Res<C>::part(c), c->part_len, c->d_pslot_base,
-                                                               c->d_pslot_cnt, y, c->n, done, nrhs);
+        k_gather<C, 4><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(Res<C>::R(c), Res<C>::P(c), c->T, c->d_grp_off,
+                                                               c->d_grp_cube, c->ngroups, G, k2, Res<C>::part(c),
+                                                               c->part_len, c->d_pslot_base, c->d_pslot_cnt, y, c->n,
+                                                               done, nrhs);
     else
-        k_gather<C, 1><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(Res<C>::R(c), Res<C>::P(c), c->T, c->d_cube_off, G, k2,
-                                                               Res<C>::part(c), c->part_len, c->d_pslot_base,
-                                                               c->d_pslot_cnt, y, c->n, done, nrhs);
+        k_gather<C, 1><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(Res<C>::R(c), Res<C>::P(c), c->T, c->d_grp_off,
+                                                               c->d_grp_cube, c->ngroups, G, k2, Res<C>::part(c),
+                                                               c->part_len, c->d_pslot_base, c->d_pslot_cnt, y, c->n,
+                                                               done, nrhs);
     c->launches += 1;
 }
 

@@ -382,19 +382,15 @@ __device__ __forceinline__ void load_tet(const NearArgs &a, int slot, TetGeo &t)
     t.vol = a.vol[slot];
 }
 
-__device__ __forceinline__ void store_block(const NearArgs &a, long long e, const cd *blk, bool tr) {
-    if (a.c64) {
-        cf *d = (cf *)a.data + 9 * e;
-        for (int r = 0; r < 3; ++r)
-            for (int c = 0; c < 3; ++c) {
-                const cd v = tr ? blk[c + 3 * r] : blk[r + 3 * c];
-                d[r + 3 * c] = make_float2((float)v.x, (float)v.y);
-            }
-    } else {
-        cd *d = (cd *)a.data + 9 * e;
-        for (int r = 0; r < 3; ++r)
-            for (int c = 0; c < 3; ++c) d[r + 3 * c] = tr ? blk[c + 3 * r] : blk[r + 3 * c];
-    }
+// block (i, j) of tile tl, from column-major blk (transposed when tr)
+__device__ __forceinline__ void store_block(const NearArgs &a, const NearTile &tl, int i, int j, const cd *blk, bool tr) {
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            const cd v = tr ? blk[c + 3 * r] : blk[r + 3 * c];
+            const long long e = tl.data_off + tile_at(tl.n1, i, j, r + 3 * c);
+            if (a.c64) ((cf *)a.data)[e] = make_float2((float)v.x, (float)v.y);
+            else ((cd *)a.data)[e] = v;
+        }
 }
 
 constexpr int NEAR_THREADS = 128;
@@ -414,7 +410,7 @@ __global__ void __launch_bounds__(NEAR_THREADS) k_near_build(NearArgs a) {
     }
     __syncthreads();
     const long long TT = 27LL * a.T;
-    const int s1 = a.cube_off[tl.c1], s2 = a.cube_off[tl.c2];
+    const int s1 = tl.s1, s2 = tl.s2;
     // GP2[j][g][row i of c1-box] = sum_q G[i][q] P_g(q, tet j of c2)   (test in c1, basis in c2)
     for (int e = threadIdx.x; e < tl.n2 * 108; e += blockDim.x) {
         const int j = e / 108, g = (e / 27) % 4, i = e % 27;
@@ -424,7 +420,7 @@ __global__ void __launch_bounds__(NEAR_THREADS) k_near_build(NearArgs a) {
         GP2[e] = acc;
     }
     // GP1[i][g][row q of c2-box] = sum_p G[p][q] P_g(p, tet i of c1)   (test in c2, basis in c1)
-    if (tl.c1 != tl.c2) {
+    if (tl.g1 != tl.g2) {
         for (int e = threadIdx.x; e < tl.n1 * 108; e += blockDim.x) {
             const int i = e / 108, g = (e / 27) % 4, q = e % 27;
             const cd *p = a.P + (size_t)g * TT + (s1 + i);
@@ -434,7 +430,7 @@ __global__ void __launch_bounds__(NEAR_THREADS) k_near_build(NearArgs a) {
         }
     }
     __syncthreads();
-    const bool diag = tl.c1 == tl.c2;
+    const bool diag = tl.g1 == tl.g2;
     const int npairs = tl.n1 * tl.n2;
     for (int e = threadIdx.x; e < npairs; e += blockDim.x) {
         const int i = e / tl.n2, j = e % tl.n2;
@@ -449,8 +445,8 @@ __global__ void __launch_bounds__(NEAR_THREADS) k_near_build(NearArgs a) {
         cd blk[9];
         near_block(Tt, Bt, st == sbas, a.eps[st], a.k, a.P + st, a.P + TT + st, a.P + 2 * TT + st, a.P + 3 * TT + st,
                    a.T, gp, gp + 27, gp + 54, gp + 81, blk);
-        store_block(a, tl.data_off + (long long)i * tl.n2 + j, blk, !fwd);
-        if (diag && i != j) store_block(a, tl.data_off + (long long)j * tl.n2 + i, blk, true);
+        store_block(a, tl, i, j, blk, !fwd);
+        if (diag && i != j) store_block(a, tl, j, i, blk, true);
     }
 }
 
@@ -816,24 +812,22 @@ int setup_nearzone_device(scd_ctx *c, int prec) {
     if (rc) return rc;
     c->have_near = false;
     c->near_prec = prec;
-    if (c->max_per_cube > SCD_NEAR_MAXN)
-        return set_error(c, SCD_BAD_ARG, "%d tets in one projection box; the near-zone kernels support %d",
-                         c->max_per_cube, SCD_NEAR_MAXN);
     if ((rc = build_tile_layout(c))) return rc;
     const size_t esz = prec == SCD_STORE_C64 ? sizeof(cf) : sizeof(cd);
     if (c->d_tdata) { cudaFree(c->d_tdata); c->d_tdata = nullptr; }
-    if (cudaMalloc(&c->d_tdata, esz * 9 * (size_t)std::max<long long>(c->tile_blocks, 1)) != cudaSuccess)
+    if (cudaMalloc(&c->d_tdata, esz * (size_t)std::max<long long>(c->tile_store, 1)) != cudaSuccess)
         return set_error(c, SCD_OOM, "near-zone tiles (%lld blocks)", c->tile_blocks);
+    // padding between the planes of a tile is never written
+    if ((rc = check_cuda(c, cudaMemsetAsync(c->d_tdata, 0, esz * (size_t)std::max<long long>(c->tile_store, 1), c->st),
+                         "near-zone tiles")))
+        return rc;
     int *dperm = c->d_perm;
     NearArgs a;
     a.tiles = c->d_tiles; a.tc = c->d_tc; a.vol = c->d_tvol; a.eps = c->d_eps; a.P = c->d_P; a.perm = dperm;
     a.cube_off = c->d_cube_off; a.T = c->T; a.ncx = c->ncx; a.ncy = c->ncy; a.Nx = c->Nx; a.Ny = c->Ny;
     a.delta = c->d.delta; a.mx = c->d.min_coord[0]; a.my = c->d.min_coord[1]; a.mz = c->d.min_coord[2];
     a.k = c->k; a.data = c->d_tdata; a.c64 = prec == SCD_STORE_C64;
-    const size_t sh = sizeof(cd) * (27 * 27 + (size_t)2 * c->max_per_cube * 108);
-    if (sh > 227 * 1024)
-        return set_error(c, SCD_BAD_ARG, "%d tets in one projection box exceed the near-zone kernel's shared memory",
-                         c->max_per_cube);
+    const size_t sh = sizeof(cd) * (27 * 27 + (size_t)2 * c->max_per_group * 108);
     if (sh > 48 * 1024) cudaFuncSetAttribute(k_near_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
     k_near_build<<<c->ntiles, NEAR_THREADS, sh, c->st>>>(a);
     rc = check_cuda(c, cudaGetLastError(), "near-zone launch");
@@ -977,7 +971,7 @@ int64_t scd_nearzone_count(scd_ctx *c) {
     if (!c || !c->have_near) return -1;
     long long B = 0;
     for (const NearTile &tl : c->tiles_h) {
-        if (tl.c1 == tl.c2) B += (long long)tl.n1 * (tl.n1 + 1) / 2;
+        if (tl.g1 == tl.g2) B += (long long)tl.n1 * (tl.n1 + 1) / 2;
         else B += (long long)tl.n1 * tl.n2;
     }
     return B;
@@ -990,7 +984,7 @@ int scd_get_nearzone(scd_ctx *c, int64_t B, scd_c128 *sp, int32_t *ind) {
     if (!c->have_near) return set_error(c, SCD_NOT_READY, "near zone not set");
     if (B != scd_nearzone_count(c)) return set_error(c, SCD_BAD_ARG, "B = %lld, the near zone has %lld", (long long)B,
                                                    (long long)scd_nearzone_count(c));
-    const size_t nb = 9 * (size_t)c->tile_blocks;
+    const size_t nb = (size_t)c->tile_store;
     std::vector<cd> data(nb);
     if (c->near_prec == SCD_STORE_C64) {
         std::vector<cf> f(nb);
@@ -1001,26 +995,26 @@ int scd_get_nearzone(scd_ctx *c, int64_t B, scd_c128 *sp, int32_t *ind) {
         int rc = check_cuda(c, cudaMemcpy(data.data(), c->d_tdata, sizeof(cd) * nb, cudaMemcpyDeviceToHost), "get_nearzone");
         if (rc) return rc;
     }
-    struct E { int t, b; size_t e; bool tr; };
+    struct E { int t, b; size_t e; int ld; bool tr; };
     std::vector<E> list;
     list.reserve((size_t)B);
     for (const NearTile &tl : c->tiles_h) {
-        const int s1 = c->cube_off[tl.c1], s2 = c->cube_off[tl.c2];
         for (int i = 0; i < tl.n1; ++i)
             for (int j = 0; j < tl.n2; ++j) {
-                if (tl.c1 == tl.c2 && j < i) continue;
-                const int ta = c->perm[s1 + i], tb = c->perm[s2 + j];
-                const size_t e = (size_t)tl.data_off + (size_t)i * tl.n2 + j;
-                if (ta <= tb) list.push_back(E{ta, tb, e, false});
-                else list.push_back(E{tb, ta, e, true});
+                if (tl.g1 == tl.g2 && j < i) continue;
+                const int ta = c->perm[tl.s1 + i], tb = c->perm[tl.s2 + j];
+                const size_t e = (size_t)tl.data_off + (size_t)tile_at(tl.n1, i, j, 0);
+                if (ta <= tb) list.push_back(E{ta, tb, e, tl.n1 | 1, false});
+                else list.push_back(E{tb, ta, e, tl.n1 | 1, true});
             }
     }
     std::sort(list.begin(), list.end(), [](const E &x, const E &y) { return x.t != y.t ? x.t < y.t : x.b < y.b; });
     for (size_t q = 0; q < list.size(); ++q) {
-        const cd *src = &data[9 * list[q].e];
+        const cd *src = &data[list[q].e];
+        const size_t ld = (size_t)list[q].ld;
         for (int r = 0; r < 3; ++r)
             for (int cc = 0; cc < 3; ++cc) {
-                const cd v = list[q].tr ? src[cc + 3 * r] : src[r + 3 * cc];
+                const cd v = list[q].tr ? src[(cc + 3 * r) * ld] : src[(r + 3 * cc) * ld];
                 sp[9 * q + r + 3 * cc] = scd_c128{v.x, v.y};
             }
         ind[2 * q] = list[q].t + 1;
