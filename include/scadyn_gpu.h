@@ -67,13 +67,16 @@ typedef struct scd_grid_desc {
 #define SCD_STORE_C64   32   /* complex64, as the reference stores sp_mat */
 #define SCD_STORE_C128  64   /* complex128 */
 
+/* largest Krylov dimension the solvers accept */
+#define SCD_M_MAX       63
+
 /* solve precision */
 #define SCD_PREC_FP64   0    /* complex128 GMRES and matvec */
 #define SCD_PREC_MIXED  1    /* complex64 inner GMRES, complex128 outer refinement */
 
 typedef struct scd_solve_opts {
     double  tol;          /* GMRES relative residual (mesh%tol) */
-    int32_t m;            /* Krylov dimension (mesh%maxit) */
+    int32_t m;            /* Krylov dimension (mesh%maxit), 1..SCD_M_MAX */
     int32_t cycles;       /* restart cycles (mesh%restart) */
     int32_t block;        /* right-hand sides solved together; 0 = all */
     int32_t precision;    /* SCD_PREC_FP64 or SCD_PREC_MIXED */
@@ -136,8 +139,8 @@ SCD_API int scd_get_nearzone(scd_ctx *ctx, int64_t B, scd_c128 *sp_mat, int32_t 
 /* compute_Ax2 (src/gmres_module.f90:57-176): Ax = A x. */
 SCD_API int scd_matvec(scd_ctx *ctx, const scd_c128 *x, scd_c128 *Ax);
 
-/* gmres (src/gmres_module.f90:180-325): x0 = rhs, GMRES(m) with `cycles`
- * restarts, stop when |g(i+1)|/||rhs|| < tol.  Returns SCD_NOT_CONVERGED with
+/* gmres (src/gmres_module.f90:180-325): x0 = rhs, GMRES(m) (m <= SCD_M_MAX)
+ * with `cycles` restarts, stop when |g(i+1)|/||rhs|| < tol.  Returns SCD_NOT_CONVERGED with
  * the last iterate in x when the cycles run out. */
 SCD_API int scd_gmres(scd_ctx *ctx, const scd_c128 *rhs, scd_c128 *x, double tol, int32_t m,
               int32_t cycles, int32_t *iters, double *relres);

@@ -65,6 +65,7 @@ int ensure_work(scd_ctx *c, int nrhs) {
     if ((rc = dalloc(c, &c->d_y, r * c->n, "y"))) return rc;
     if ((rc = dalloc(c, &c->d_io, r * c->n, "io"))) return rc;
     if ((rc = dalloc(c, &c->d_rhs, r * c->n, "rhs"))) return rc;
+    if ((rc = dalloc(c, &c->d_xT, (size_t)xt_columns(nrhs) * c->n, "interleaved x"))) return rc;
     c->nrhs_cap = nrhs;
     return SCD_OK;
 }
@@ -380,11 +381,10 @@ int scd_destroy(scd_ctx *c) {
     if (c->st) cudaStreamSynchronize(c->st);
     void *ptrs[] = {c->d_perm, c->d_cube_off, c->d_grp_off, c->d_grp_cube, c->d_grp_tile, c->d_kerr, c->d_P, c->d_Fo, c->d_tdata, c->d_tiles, c->d_pslot_base,
                     c->d_pslot_cnt, c->d_tc, c->d_tvol, c->d_eps, c->d_bpart, c->d_W, c->d_R, c->d_nzpart, c->d_x,
-                    c->d_y, c->d_io, c->d_V, c->d_H, c->d_cs, c->d_sn, c->d_g, c->d_rhs, c->d_w, c->d_red,
-                    c->d_bar, c->d_err, c->d_state, c->d_tw[0], c->d_tw[1], c->d_tw[2], c->f_P, c->f_Fo,
-                    c->f_tw[0], c->f_tw[1], c->f_tw[2], c->f_bpart, c->f_W, c->f_R, c->f_nzpart};
+                    c->d_y, c->d_io, c->d_rhs,
+                    c->d_bar, c->d_err, c->d_tw[0], c->d_tw[1], c->d_tw[2], c->f_P, c->f_Fo,
+                    c->f_tw[0], c->f_tw[1], c->f_tw[2], c->f_bpart, c->f_W, c->f_R, c->f_nzpart, c->d_xT, c->f_xT};
     for (void *p : ptrs) if (p) cudaFree(p);
-    if (c->h_state) cudaFreeHost(c->h_state);
     batch_free(c);
     if (c->d_mat) cudaFree(c->d_mat);
     for (int i = 0; i < 8; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
@@ -498,7 +498,7 @@ int scd_matvec(scd_ctx *c, const scd_c128 *x, scd_c128 *Ax) {
 
 int scd_gmres(scd_ctx *c, const scd_c128 *rhs, scd_c128 *x, double tol, int32_t m, int32_t cycles, int32_t *iters,
               double *relres) {
-    if (!c || !rhs || !x || m < 1 || cycles < 1 || !(tol > 0)) return SCD_BAD_ARG;
+    if (!c || !rhs || !x || m < 1 || m > SCD_M_MAX || cycles < 1 || !(tol > 0)) return SCD_BAD_ARG;
     cudaSetDevice(c->dev);
     int rc = ready(c);
     if (rc) return rc;
@@ -508,7 +508,10 @@ int scd_gmres(scd_ctx *c, const scd_c128 *rhs, scd_c128 *x, double tol, int32_t 
     int it = 0;
     double rr = 0;
     cudaEventRecord(c->ev[4], c->st);
-    rc = gmres_solve(c, c->d_rhs, c->d_x, tol, m, cycles, &it, &rr);
+    // one slot of the batched solver: the same arithmetic as that column in
+    // any batch of scd_solve_columns
+    const cd *col = c->d_rhs;
+    rc = batch_solve(c, 1, &col, c->d_x, tol, m, cycles, 1, &it, nullptr, nullptr, &rr, SCD_PREC_FP64, 0.0, 0);
     if (rc != SCD_OK && rc != SCD_NOT_CONVERGED) return rc;
     cudaEventRecord(c->ev[5], c->st);
     launch_permute_out(c, c->d_x, c->d_io, 1, c->n);
@@ -550,7 +553,7 @@ int scd_solve_columns(scd_ctx *c, int32_t ncol, const scd_c128 *mat, scd_c128 *T
     const int ns = o->block > 0 ? o->block : ncol;
     std::vector<int> it(ncol, 0);
     int worst = batch_solve(c, ncol, cols.data(), d_X, o->tol, o->m, o->cycles, ns, it.data(), nullptr, nullptr,
-                            o->precision, o->inner_tol, o->max_outer);
+                            nullptr, o->precision, o->inner_tol, o->max_outer);
     if (worst == SCD_OK || worst == SCD_NOT_CONVERGED) {
         const int ns_ = near_status(c);
         if (ns_) worst = ns_;
@@ -693,7 +696,7 @@ int scd_compute_T_matrix(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int3
     const int ns = o->block > 0 ? o->block : ncol;
     std::vector<int> it(ncol, 0);
     int worst = batch_solve(c, ncol, cols.data(), d_X, o->tol, o->m, o->cycles, ns, it.data(), nullptr, nullptr,
-                            o->precision, o->inner_tol, o->max_outer);
+                            nullptr, o->precision, o->inner_tol, o->max_outer);
     if (worst == SCD_OK || worst == SCD_NOT_CONVERGED) {
         const int ns_ = near_status(c);
         if (ns_) worst = ns_;

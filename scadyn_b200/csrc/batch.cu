@@ -4,9 +4,9 @@
 // own restarted GMRES exactly as gmres (src/gmres_module.f90:180-325): x0 =
 // rhs, MGS with the conditional re-orthogonalisation, complex Givens, y =
 // H^-1 g, x += V y.  A slot's arithmetic does not depend on what the other
-// slots hold (per-slot reductions over a fixed CTA partition, summed in a
-// fixed order), so a column's result is bit-identical whether it is solved
-// alone or in a batch.  A slot whose column converged (or ran out of cycles)
+// slots hold (per-slot reductions over fixed chunks, summed in a fixed
+// order), so a column's result is bit-identical whether it is solved alone
+// (scd_gmres runs one slot) or in a batch.  A slot whose column converged (or ran out of cycles)
 // is refilled with the next column on the following tick (continuous
 // batching).
 #include <cuda_runtime.h>
@@ -23,6 +23,7 @@ namespace {
 
 constexpr int BT = 256;             // threads per CTA of the tick kernel
 constexpr int NSMAX = 64;           // slot limit (partial buffer sizing)
+constexpr int BW = BT / 32;         // warps per CTA
 
 enum { SLOT_FREE = 0, SLOT_START = 1, SLOT_ARNOLDI = 2, SLOT_DONE = 3, SLOT_RESID = 4, SLOT_INNER_DONE = 5 };
 
@@ -49,6 +50,9 @@ struct TickArgs {
     cd *cs, *sn, *g, *y;   // [slot][m+1]
     C *x, *rhs, *w; // [slot][n]
     double *red;    // [2][grid][NSMAX*4]
+    double *cpart;  // [NSMAX][NCH][4] chunk partials
+    double *ctot;   // [2][NSMAX][4] slot totals
+    int *ccnt;      // [NSMAX] chunks published in the current reduction
     GridBarrier *bar;
     int *err;
     long long n;
@@ -67,84 +71,106 @@ template <typename C> __device__ __forceinline__ cd rounded(cd v);
 template <> __device__ __forceinline__ cd rounded<cd>(cd v) { return v; }
 template <> __device__ __forceinline__ cd rounded<cf>(cd v) { return widen(make_float2((float)v.x, (float)v.y)); }
 
-// Streaming loops over a vector take this thread's elements q0, q0+stride,
-// ... TU at a time: the loads of TU elements are issued together (memory-
-// level parallelism), the arithmetic runs in the same element order as a
-// plain loop, so sums are unchanged.
+// Streaming loops take a lane's elements of a chunk TU at a time: the loads
+// of TU elements are issued together (memory-level parallelism), the
+// arithmetic runs in the same element order as a plain loop.
 constexpr int TU = 4;
 
-template <typename C>
-__device__ __forceinline__ double *partial_slot(const TickArgs<C> &a, int parity, int s) {
-    return a.red + ((size_t)parity * gridDim.x + blockIdx.x) * (NSMAX * 4) + s * 4;
-}
+// ---- reductions over fixed chunks
+// Every slot vector is cut into NCH fixed chunks; chunk c of slot s is
+// always handled by global warp (s*NCH + c) mod (warps in the grid), its
+// lanes take elements q = c*L + lane + 32t in order (TU at a time, loads
+// first), the lanes' sums meet in an xor tree, and the last warp to finish a
+// slot adds its NCH chunk partials (lane l: chunks l, l+32, ..., then an xor
+// tree) into the slot's total.  The arithmetic of a slot therefore depends
+// on n and the grid only -- never on which other slots are active -- and
+// each warp streams long contiguous runs (deep memory-level parallelism).
+constexpr int NCH = 512;
 
-// totals of the per-CTA partials of every slot: warp w reduces slots w,
-// w + nwarps, ...; lanes stride over CTAs; fixed order, deterministic
-template <typename C>
-__device__ void read_totals(const TickArgs<C> &a, int parity, int nv, double (*tot)[4]) {
-    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int s = wp; s < a.ns; s += nw) {
-        double acc[4] = {0, 0, 0, 0};
-        for (int b = lane; b < (int)gridDim.x; b += 32) {
-            const double *p = a.red + ((size_t)parity * gridDim.x + b) * (NSMAX * 4) + s * 4;
-            for (int q = 0; q < nv; ++q) acc[q] += __ldcg(p + q);
-        }
-        for (int q = 0; q < nv; ++q) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
-        }
-        if (lane == 0)
-            for (int q = 0; q < nv; ++q) tot[s][q] = acc[q];
+struct Chunks {
+    long long L;    // chunk length
+    int gw, nw;     // this warp, warps in the grid
+    int lane;
+    __device__ Chunks(long long n) {
+        L = (n + NCH - 1) / NCH;
+        gw = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+        nw = (int)(((long long)gridDim.x * blockDim.x) >> 5);
+        lane = threadIdx.x & 31;
     }
-    __syncthreads();
-}
+};
 
-constexpr int BW = BT / 32;   // warps per CTA
-
-// Per-slot reductions without a CTA barrier per slot: each warp folds its
-// NV values (xor tree) into wsh[s][warp]; flush_parts then adds the warps in
-// order -- the arithmetic of block_sum -- and stores the CTA partial of every
-// slot flagged in act[].
-template <int NV>
-__device__ __forceinline__ void warp_part(double (&v)[NV], double *wsh, int s) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+// the per-lane sums v of chunk c of slot s: fold, publish, and let the
+// slot's last warp form the total
+template <int NV, typename C>
+__device__ __forceinline__ void chunk_done(const TickArgs<C> &a, int s, int c, double (&v)[NV], int parity, int lane) {
 #pragma unroll
-    for (int q = 0; q < NV; ++q) {
+    for (int k = 0; k < NV; ++k) {
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
     }
+    int last = 0;
     if (lane == 0) {
+        double *p = a.cpart + ((size_t)s * NCH + c) * 4;
 #pragma unroll
-        for (int q = 0; q < NV; ++q) wsh[(s * BW + w) * 4 + q] = v[q];
+        for (int k = 0; k < NV; ++k) p[k] = v[k];
+        __threadfence();
+        last = atomicAdd(&a.ccnt[s], 1) == NCH - 1;
+    }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (last) {
+        __threadfence();
+        // all loads first (they are independent), then the sums in chunk order
+        double pv[NCH / 32][NV];
+#pragma unroll
+        for (int j = 0; j < NCH / 32; ++j) {
+            const double *p = a.cpart + ((size_t)s * NCH + lane + 32 * j) * 4;
+#pragma unroll
+            for (int k = 0; k < NV; ++k) pv[j][k] = __ldcg(p + k);
+        }
+        double t[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) t[k] = 0.0;
+#pragma unroll
+        for (int j = 0; j < NCH / 32; ++j)
+#pragma unroll
+            for (int k = 0; k < NV; ++k) t[k] += pv[j][k];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t[k] += __shfl_xor_sync(0xffffffffu, t[k], o);
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < NV; ++k) a.ctot[((size_t)parity * NSMAX + s) * 4 + k] = t[k];
+            a.ccnt[s] = 0;
+        }
     }
 }
 
+// after the grid barrier: the totals of the flagged slots into shared memory
 template <typename C>
-__device__ __forceinline__ void flush_parts(const TickArgs<C> &a, int parity, const double *wsh, const int *act, int nv) {
-    __syncthreads();
+__device__ __forceinline__ void load_totals(const TickArgs<C> &a, int parity, int nv, const int *act, double (*tot)[4]) {
     for (int e = threadIdx.x; e < a.ns * 4; e += blockDim.x) {
-        const int s = e >> 2, q = e & 3;
-        if (q >= nv || !act[s]) continue;
-        double t = 0.0;
-        for (int i = 0; i < BW; ++i) t += wsh[(s * BW + i) * 4 + q];
-        partial_slot(a, parity, s)[q] = t;
+        const int s = e >> 2, k = e & 3;
+        if (k < nv && act[s]) tot[s][k] = __ldcg(a.ctot + ((size_t)parity * NSMAX + s) * 4 + k);
     }
+    __syncthreads();
 }
 
 // One tick: cycle starts (r = rhs - A x, V0 = r/||r||) and Arnoldi steps
 // (MGS, normalisation, Givens) for every active slot; cycle ends update x.
 template <typename C>
 __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
-    __shared__ double wsh[NSMAX * BW * 4];
     __shared__ double tot[NSMAX][4];
-    __shared__ int smode[NSMAX], sstep[NSMAX], szero[NSMAX], swpos[NSMAX], sact[NSMAX];
+    __shared__ int smode[NSMAX], sstep[NSMAX], szero[NSMAX], swpos[NSMAX], sact[NSMAX], sro[NSMAX];
     __shared__ double snormav[NSMAX], shn[NSMAX];
     __shared__ cd sh_h[NSMAX];
-    __shared__ cd ysm[64];
+    __shared__ cd ysm[BW][SCD_M_MAX + 1];    // per warp: y of the slot being updated
     const long long n = a.n;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    const long long q0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const int ldh = a.m + 1;
+    const Chunks ch(n);
+    const int lane = ch.lane;
+    const int nitems = a.ns * NCH;
     for (int s = threadIdx.x; s < a.ns; s += blockDim.x) {
         smode[s] = a.slots[s].mode;
         sstep[s] = a.slots[s].step;
@@ -154,60 +180,60 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
     __syncthreads();
     int parity = 0;
     // ---- phase A: first reduction of every active slot
-    for (int s = 0; s < a.ns; ++s) {
+    for (int it = ch.gw; it < nitems; it += ch.nw) {
+        const int s = it / NCH, c = it - s * NCH;
         const int md = smode[s];
+        if (md != SLOT_START && md != SLOT_ARNOLDI) continue;
+        const long long qa = c * ch.L, qb = min(n, qa + ch.L);
         double v[3] = {0, 0, 0};
         const C *ws = a.w + (size_t)swpos[s] * n;
         C *V0 = a.V + (size_t)s * (a.m + 1) * n;
         if (md == SLOT_START) {
             const C *bs = a.rhs + (size_t)s * n;
             const bool zx = szero[s] != 0;
-            for (long long q = q0; q < n; q += TU * stride) {
+            for (long long q = qa + lane; q < qb; q += 32 * TU) {
                 cd b[TU], w[TU];
 #pragma unroll
                 for (int u = 0; u < TU; ++u) {
-                    const long long qq = q + u * stride;
+                    const long long qq = q + 32 * u;
                     b[u] = w[u] = cmk(0, 0);
-                    if (qq < n) {
+                    if (qq < qb) {
                         b[u] = to_cd(bs[qq]);
                         if (!zx) w[u] = to_cd(ws[qq]);
                     }
                 }
 #pragma unroll
                 for (int u = 0; u < TU; ++u) {
-                    const long long qq = q + u * stride;
-                    if (qq >= n) break;
+                    const long long qq = q + 32 * u;
+                    if (qq >= qb) break;
                     const cd r = zx ? b[u] : csub(b[u], w[u]);
                     store_c(V0[qq], r);
                     v[0] += cabs2(r);
                     v[1] += cabs2(b[u]);
                 }
             }
-        } else if (md == SLOT_ARNOLDI) {
-            for (long long q = q0; q < n; q += TU * stride) {
+        } else {
+            for (long long q = qa + lane; q < qb; q += 32 * TU) {
                 cd w[TU], z[TU];
 #pragma unroll
                 for (int u = 0; u < TU; ++u) {
-                    const long long qq = q + u * stride;
+                    const long long qq = q + 32 * u;
                     w[u] = z[u] = cmk(0, 0);
-                    if (qq < n) { w[u] = to_cd(ws[qq]); z[u] = to_cd(V0[qq]); }
+                    if (qq < qb) { w[u] = to_cd(ws[qq]); z[u] = to_cd(V0[qq]); }
                 }
 #pragma unroll
                 for (int u = 0; u < TU; ++u) {
-                    if (q + u * stride >= n) break;
+                    if (q + 32 * u >= qb) break;
                     v[0] += cabs2(w[u]);
                     cdot_acc(v[1], v[2], z[u], w[u]);
                 }
             }
-        } else {
-            continue;
         }
-        warp_part<3>(v, wsh, s);
+        chunk_done<3>(a, s, c, v, parity, lane);
     }
     for (int s = threadIdx.x; s < a.ns; s += blockDim.x) sact[s] = smode[s] == SLOT_START || smode[s] == SLOT_ARNOLDI;
-    flush_parts(a, parity, wsh, sact, 3);
     grid_barrier(a.bar, gridDim.x, a.err);
-    read_totals(a, parity, 3, tot);
+    load_totals(a, parity, 3, sact, tot);
     int kmax = 0;
     for (int s = 0; s < a.ns; ++s) {
         if (smode[s] == SLOT_ARNOLDI) kmax = max(kmax, sstep[s] + 1);
@@ -218,24 +244,30 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
     }
     __syncthreads();
     // cycle starts: normalise V0, set g, b_norm
-    for (int s = 0; s < a.ns; ++s) {
+    for (int it = ch.gw; it < nitems; it += ch.nw) {
+        const int s = it / NCH, c = it - s * NCH;
         if (smode[s] != SLOT_START) continue;
         const double beta = sqrt(tot[s][0]);
+        const long long qa = c * ch.L, qb = min(n, qa + ch.L);
         C *V0 = a.V + (size_t)s * (a.m + 1) * n;
-        for (long long q = q0; q < n; q += TU * stride) {
+        for (long long q = qa + lane; q < qb; q += 32 * TU) {
             cd r[TU];
 #pragma unroll
             for (int u = 0; u < TU; ++u) {
-                const long long qq = q + u * stride;
-                r[u] = qq < n ? to_cd(V0[qq]) : cmk(0, 0);
+                const long long qq = q + 32 * u;
+                r[u] = qq < qb ? to_cd(V0[qq]) : cmk(0, 0);
             }
 #pragma unroll
             for (int u = 0; u < TU; ++u) {
-                const long long qq = q + u * stride;
-                if (qq < n) store_c(V0[qq], cmk(r[u].x / beta, r[u].y / beta));
+                const long long qq = q + 32 * u;
+                if (qq < qb) store_c(V0[qq], cmk(r[u].x / beta, r[u].y / beta));
             }
         }
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
+    }
+    if (blockIdx.x == 0 && threadIdx.x < a.ns) {
+        const int s = threadIdx.x;
+        if (smode[s] == SLOT_START) {
+            const double beta = sqrt(tot[s][0]);
             Slot &sl = a.slots[s];
             cd *gs = a.g + (size_t)s * (a.m + 1);
             for (int i = 0; i <= a.m; ++i) gs[i] = cmk(0, 0);
@@ -251,24 +283,26 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
     }
     // ---- MGS for the Arnoldi slots: one barrier per term
     for (int k = 1; k <= kmax; ++k) {
-        for (int s = 0; s < a.ns; ++s) {
+        for (int it = ch.gw; it < nitems; it += ch.nw) {
+            const int s = it / NCH, c = it - s * NCH;
             if (smode[s] != SLOT_ARNOLDI) continue;
             const int i = sstep[s] + 1;
             if (k > i) continue;
             const cd h = sh_h[s];
-            if (blockIdx.x == 0 && threadIdx.x == 0) a.H[(size_t)s * ldh * a.m + (size_t)ldh * (i - 1) + (k - 1)] = h;
+            if (c == 0 && lane == 0) a.H[(size_t)s * ldh * a.m + (size_t)ldh * (i - 1) + (k - 1)] = h;
+            const long long qa = c * ch.L, qb = min(n, qa + ch.L);
             C *ws = a.w + (size_t)swpos[s] * n;
             const C *Vs = a.V + (size_t)s * (a.m + 1) * n;
             const C *vk = Vs + (size_t)(k - 1) * n;
             const C *vn = (k < i) ? Vs + (size_t)k * n : nullptr;
             double u[2] = {0, 0};
-            for (long long q = q0; q < n; q += TU * stride) {
+            for (long long q = qa + lane; q < qb; q += 32 * TU) {
                 cd w[TU], p[TU], z[TU];
 #pragma unroll
                 for (int e = 0; e < TU; ++e) {
-                    const long long qq = q + e * stride;
+                    const long long qq = q + 32 * e;
                     w[e] = p[e] = z[e] = cmk(0, 0);
-                    if (qq < n) {
+                    if (qq < qb) {
                         w[e] = to_cd(ws[qq]);
                         p[e] = to_cd(vk[qq]);
                         if (vn) z[e] = to_cd(vn[qq]);
@@ -276,8 +310,8 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
                 }
 #pragma unroll
                 for (int e = 0; e < TU; ++e) {
-                    const long long qq = q + e * stride;
-                    if (qq >= n) break;
+                    const long long qq = q + 32 * e;
+                    if (qq >= qb) break;
                     csub_mul(w[e], h, p[e]);
                     store_c(ws[qq], w[e]);
                     const cd wr = rounded<C>(w[e]);
@@ -285,133 +319,138 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
                     else u[0] += cabs2(wr);
                 }
             }
-            warp_part<2>(u, wsh, s);
+            chunk_done<2>(a, s, c, u, parity ^ 1, lane);
         }
         for (int s = threadIdx.x; s < a.ns; s += blockDim.x) sact[s] = smode[s] == SLOT_ARNOLDI && k <= sstep[s] + 1;
-        flush_parts(a, parity ^ 1, wsh, sact, 2);
         parity ^= 1;
         grid_barrier(a.bar, gridDim.x, a.err);
-        read_totals(a, parity, 2, tot);
-        if (threadIdx.x == 0) {
-            for (int s = 0; s < a.ns; ++s) {
-                if (smode[s] != SLOT_ARNOLDI) continue;
-                const int i = sstep[s] + 1;
-                if (k > i) continue;
+        load_totals(a, parity, 2, sact, tot);
+        if (threadIdx.x < a.ns) {
+            const int s = threadIdx.x;
+            if (sact[s]) {
                 sh_h[s] = cmk(tot[s][0], tot[s][1]);
-                if (k == i) shn[s] = sqrt(tot[s][0]);
+                if (k == sstep[s] + 1) shn[s] = sqrt(tot[s][0]);
             }
         }
         __syncthreads();
     }
     // ---- conditional re-orthogonalisation (src/gmres_module.f90:251-258)
+    for (int s = threadIdx.x; s < a.ns; s += blockDim.x)
+        sro[s] = smode[s] == SLOT_ARNOLDI && snormav[s] + (double)0.001f * shn[s] == snormav[s];
+    __syncthreads();
     int jmax = 0;
     for (int s = 0; s < a.ns; ++s)
-        if (smode[s] == SLOT_ARNOLDI && snormav[s] + (double)0.001f * shn[s] == snormav[s]) jmax = max(jmax, sstep[s] + 1);
+        if (sro[s]) jmax = max(jmax, sstep[s] + 1);
     for (int j = 1; j <= jmax; ++j) {
-        for (int s = 0; s < a.ns; ++s) {
-            if (smode[s] != SLOT_ARNOLDI || !(snormav[s] + (double)0.001f * shn[s] == snormav[s]) || j > sstep[s] + 1) continue;
+        for (int it = ch.gw; it < nitems; it += ch.nw) {
+            const int s = it / NCH, c = it - s * NCH;
+            if (!sro[s] || j > sstep[s] + 1) continue;
+            const long long qa = c * ch.L, qb = min(n, qa + ch.L);
             const C *vj = a.V + (size_t)s * (a.m + 1) * n + (size_t)(j - 1) * n;
             const C *ws = a.w + (size_t)swpos[s] * n;
             double u[2] = {0, 0};
-            for (long long q = q0; q < n; q += TU * stride) {
+            for (long long q = qa + lane; q < qb; q += 32 * TU) {
                 cd z[TU], w[TU];
 #pragma unroll
                 for (int e = 0; e < TU; ++e) {
-                    const long long qq = q + e * stride;
+                    const long long qq = q + 32 * e;
                     z[e] = w[e] = cmk(0, 0);
-                    if (qq < n) { z[e] = to_cd(vj[qq]); w[e] = to_cd(ws[qq]); }
+                    if (qq < qb) { z[e] = to_cd(vj[qq]); w[e] = to_cd(ws[qq]); }
                 }
 #pragma unroll
                 for (int e = 0; e < TU; ++e) {
-                    if (q + e * stride >= n) break;
+                    if (q + 32 * e >= qb) break;
                     cdot_acc(u[0], u[1], z[e], w[e]);
                 }
             }
-            warp_part<2>(u, wsh, s);
+            chunk_done<2>(a, s, c, u, parity ^ 1, lane);
         }
-        for (int s = threadIdx.x; s < a.ns; s += blockDim.x)
-            sact[s] = smode[s] == SLOT_ARNOLDI && snormav[s] + (double)0.001f * shn[s] == snormav[s] && j <= sstep[s] + 1;
-        flush_parts(a, parity ^ 1, wsh, sact, 2);
+        for (int s = threadIdx.x; s < a.ns; s += blockDim.x) sact[s] = sro[s] && j <= sstep[s] + 1;
         parity ^= 1;
         grid_barrier(a.bar, gridDim.x, a.err);
-        read_totals(a, parity, 2, tot);
-        for (int s = 0; s < a.ns; ++s) {
-            if (smode[s] != SLOT_ARNOLDI || !(snormav[s] + (double)0.001f * shn[s] == snormav[s]) || j > sstep[s] + 1) continue;
-            const int i = sstep[s] + 1;
-            const cd hr = cmk(tot[s][0], tot[s][1]);
-            if (blockIdx.x == 0 && threadIdx.x == 0) {
+        load_totals(a, parity, 2, sact, tot);
+        if (blockIdx.x == 0 && threadIdx.x < a.ns) {
+            const int s = threadIdx.x;
+            if (sact[s]) {
+                const int i = sstep[s] + 1;
                 cd *Hc = a.H + (size_t)s * ldh * a.m + (size_t)ldh * (i - 1);
-                Hc[j - 1] = cadd(Hc[j - 1], hr);
+                Hc[j - 1] = cadd(Hc[j - 1], cmk(tot[s][0], tot[s][1]));
             }
+        }
+        for (int it = ch.gw; it < nitems; it += ch.nw) {
+            const int s = it / NCH, c = it - s * NCH;
+            if (!sact[s]) continue;
+            const cd hr = cmk(tot[s][0], tot[s][1]);
+            const long long qa = c * ch.L, qb = min(n, qa + ch.L);
             const C *vj = a.V + (size_t)s * (a.m + 1) * n + (size_t)(j - 1) * n;
             C *ws = a.w + (size_t)swpos[s] * n;
-            for (long long q = q0; q < n; q += TU * stride) {
+            for (long long q = qa + lane; q < qb; q += 32 * TU) {
                 cd w[TU], p[TU];
 #pragma unroll
                 for (int e = 0; e < TU; ++e) {
-                    const long long qq = q + e * stride;
+                    const long long qq = q + 32 * e;
                     w[e] = p[e] = cmk(0, 0);
-                    if (qq < n) { w[e] = to_cd(ws[qq]); p[e] = to_cd(vj[qq]); }
+                    if (qq < qb) { w[e] = to_cd(ws[qq]); p[e] = to_cd(vj[qq]); }
                 }
 #pragma unroll
                 for (int e = 0; e < TU; ++e) {
-                    const long long qq = q + e * stride;
-                    if (qq >= n) break;
+                    const long long qq = q + 32 * e;
+                    if (qq >= qb) break;
                     csub_mul(w[e], hr, p[e]);
                     store_c(ws[qq], w[e]);
                 }
             }
         }
+        __syncthreads();   // sact / tot are rewritten by the next round
     }
     if (jmax > 0) {
-        for (int s = 0; s < a.ns; ++s) {
-            if (smode[s] != SLOT_ARNOLDI || !(snormav[s] + (double)0.001f * shn[s] == snormav[s])) continue;
+        for (int it = ch.gw; it < nitems; it += ch.nw) {
+            const int s = it / NCH, c = it - s * NCH;
+            if (!sro[s]) continue;
+            const long long qa = c * ch.L, qb = min(n, qa + ch.L);
             const C *ws = a.w + (size_t)swpos[s] * n;
             double u[1] = {0};
-            for (long long q = q0; q < n; q += TU * stride) {
+            for (long long q = qa + lane; q < qb; q += 32 * TU) {
                 cd w[TU];
 #pragma unroll
                 for (int e = 0; e < TU; ++e) {
-                    const long long qq = q + e * stride;
-                    w[e] = qq < n ? to_cd(ws[qq]) : cmk(0, 0);
+                    const long long qq = q + 32 * e;
+                    w[e] = qq < qb ? to_cd(ws[qq]) : cmk(0, 0);
                 }
 #pragma unroll
                 for (int e = 0; e < TU; ++e) {
-                    if (q + e * stride >= n) break;
+                    if (q + 32 * e >= qb) break;
                     u[0] += cabs2(w[e]);
                 }
             }
-            warp_part<1>(u, wsh, s);
+            chunk_done<1>(a, s, c, u, parity ^ 1, lane);
         }
-        for (int s = threadIdx.x; s < a.ns; s += blockDim.x)
-            sact[s] = smode[s] == SLOT_ARNOLDI && snormav[s] + (double)0.001f * shn[s] == snormav[s];
-        flush_parts(a, parity ^ 1, wsh, sact, 1);
         parity ^= 1;
         grid_barrier(a.bar, gridDim.x, a.err);
-        read_totals(a, parity, 1, tot);
-        if (threadIdx.x == 0)
-            for (int s = 0; s < a.ns; ++s)
-                if (smode[s] == SLOT_ARNOLDI && snormav[s] + (double)0.001f * shn[s] == snormav[s]) shn[s] = sqrt(tot[s][0]);
+        load_totals(a, parity, 1, sro, tot);
+        if (threadIdx.x < a.ns && sro[threadIdx.x]) shn[threadIdx.x] = sqrt(tot[threadIdx.x][0]);
         __syncthreads();
     }
     // ---- v_i = w / h(i+1,i) and the Givens update
-    for (int s = 0; s < a.ns; ++s) {
+    for (int it = ch.gw; it < nitems; it += ch.nw) {
+        const int s = it / NCH, c = it - s * NCH;
         if (smode[s] != SLOT_ARNOLDI) continue;
         const int i = sstep[s] + 1;
         const double hn = shn[s];
+        const long long qa = c * ch.L, qb = min(n, qa + ch.L);
         const C *ws = a.w + (size_t)swpos[s] * n;
         C *vi = a.V + (size_t)s * (a.m + 1) * n + (size_t)i * n;
-        for (long long q = q0; q < n; q += TU * stride) {
+        for (long long q = qa + lane; q < qb; q += 32 * TU) {
             cd w[TU];
 #pragma unroll
             for (int e = 0; e < TU; ++e) {
-                const long long qq = q + e * stride;
-                w[e] = qq < n ? to_cd(ws[qq]) : cmk(0, 0);
+                const long long qq = q + 32 * e;
+                w[e] = qq < qb ? to_cd(ws[qq]) : cmk(0, 0);
             }
 #pragma unroll
             for (int e = 0; e < TU; ++e) {
-                const long long qq = q + e * stride;
-                if (qq < n) store_c(vi[qq], (hn != 0.0) ? cmk(w[e].x / hn, w[e].y / hn) : w[e]);
+                const long long qq = q + 32 * e;
+                if (qq < qb) store_c(vi[qq], (hn != 0.0) ? cmk(w[e].x / hn, w[e].y / hn) : w[e]);
             }
         }
     }
@@ -465,22 +504,41 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
     }
     grid_barrier(a.bar, gridDim.x, a.err);
     // ---- cycle end: x += V(:,1:i) y; next cycle or done
-    for (int s = 0; s < a.ns; ++s) {
-        if (smode[s] != SLOT_ARNOLDI) continue;
-        const Slot *sl = a.slots + s;
-        if (!__ldcg(&sl->finish)) continue;      // uniform across the CTA (L2 read after the barrier)
-        const int kd = __ldcg(&sl->step);
-        const cd *ys = a.y + (size_t)s * (a.m + 1);
-        for (int c = threadIdx.x; c < kd; c += blockDim.x) ysm[c] = make_double2(__ldcg(&ys[c].x), __ldcg(&ys[c].y));
-        __syncthreads();
-        const C *Vs = a.V + (size_t)s * (a.m + 1) * n;
-        C *xs = a.x + (size_t)s * n;
-        for (long long q = q0; q < n; q += stride) {
-            cd acc = cmk(0, 0);
-            for (int c = 0; c < kd; ++c) cfma(acc, to_cd(Vs[(size_t)c * n + q]), ysm[c]);
-            store_c(xs[q], cadd(to_cd(xs[q]), acc));
+    {
+        cd *yw = ysm[threadIdx.x >> 5];
+        for (int it = ch.gw; it < nitems; it += ch.nw) {
+            const int s = it / NCH, c = it - s * NCH;
+            if (smode[s] != SLOT_ARNOLDI) continue;
+            const Slot *sl = a.slots + s;
+            if (!__ldcg(&sl->finish)) continue;      // uniform across the warp (L2 read after the barrier)
+            const int kd = __ldcg(&sl->step);
+            const cd *ys = a.y + (size_t)s * (a.m + 1);
+            for (int cc = lane; cc < kd; cc += 32) yw[cc] = make_double2(__ldcg(&ys[cc].x), __ldcg(&ys[cc].y));
+            __syncwarp();
+            const long long qa = c * ch.L, qb = min(n, qa + ch.L);
+            const C *Vs = a.V + (size_t)s * (a.m + 1) * n;
+            C *xs = a.x + (size_t)s * n;
+            for (long long q = qa + lane; q < qb; q += 32 * TU) {
+                cd acc[TU];
+#pragma unroll
+                for (int e = 0; e < TU; ++e) acc[e] = cmk(0, 0);
+                for (int cc = 0; cc < kd; ++cc) {
+                    const cd yc = yw[cc];
+                    const C *vc = Vs + (size_t)cc * n;
+#pragma unroll
+                    for (int e = 0; e < TU; ++e) {
+                        const long long qq = q + 32 * e;
+                        if (qq < qb) cfma(acc[e], to_cd(vc[qq]), yc);
+                    }
+                }
+#pragma unroll
+                for (int e = 0; e < TU; ++e) {
+                    const long long qq = q + 32 * e;
+                    if (qq < qb) store_c(xs[qq], cadd(to_cd(xs[qq]), acc[e]));
+                }
+            }
+            __syncwarp();
         }
-        __syncthreads();
     }
     if (blockIdx.x == 0) {
         // `finish` stays set: other CTAs may still be reading it; the next
@@ -639,14 +697,15 @@ struct BatchBuffers {
     cd *x64 = nullptr, *b64 = nullptr, *Xin64 = nullptr, *W64 = nullptr;   // mixed: FP64 outer vectors
     Slot *slots = nullptr;
     Slot *h_slots = nullptr;
-    int *skip = nullptr, *skip64 = nullptr;
     double *red = nullptr;
+    double *cpart = nullptr, *ctot = nullptr;
+    int *ccnt = nullptr;
     int grid = 0;
 };
 
 static void free_bb(BatchBuffers &b) {
     void *p[] = {b.V, b.H, b.cs, b.sn, b.g, b.y, b.x, b.rhs, b.Xin, b.W, b.x64, b.b64, b.Xin64, b.W64,
-                 b.slots, b.skip, b.skip64, b.red};
+                 b.slots, b.red, b.cpart, b.ctot, b.ccnt};
     for (void *q : p) if (q) cudaFree(q);
     if (b.h_slots) cudaFreeHost(b.h_slots);
     b = BatchBuffers();
@@ -684,10 +743,11 @@ int batch_prepare(scd_ctx *c, int ns, int m, int mixed, BatchBuffers &b) {
         if ((rc = al((void **)&b.b64, sizeof(cd) * (size_t)ns * n, "b64"))) return rc;
         if ((rc = al((void **)&b.Xin64, sizeof(cd) * (size_t)ns * n, "Xin64"))) return rc;
         if ((rc = al((void **)&b.W64, sizeof(cd) * (size_t)ns * n, "W64"))) return rc;
-        if ((rc = al((void **)&b.skip64, sizeof(int) * ns, "skip64"))) return rc;
     }
     if ((rc = al((void **)&b.slots, sizeof(Slot) * ns, "slots"))) return rc;
-    if ((rc = al((void **)&b.skip, sizeof(int) * ns, "skip"))) return rc;
+    if ((rc = al((void **)&b.cpart, sizeof(double) * (size_t)NSMAX * NCH * 4, "chunk partials"))) return rc;
+    if ((rc = al((void **)&b.ctot, sizeof(double) * 2 * NSMAX * 4, "slot totals"))) return rc;
+    if ((rc = al((void **)&b.ccnt, sizeof(int) * NSMAX, "chunk counters"))) return rc;
     if (cudaMallocHost((void **)&b.h_slots, sizeof(Slot) * ns) != cudaSuccess) return set_error(c, SCD_OOM, "pinned slots");
     int per_sm = 0, per_sm2 = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tick<cd>, BT, 0);
@@ -711,6 +771,7 @@ static int launch_tick(scd_ctx *c, BatchBuffers &bb, int ns, int nact, int m, in
     TickArgs<C> a;
     a.slots = bb.slots; a.ns = ns; a.V = (C *)bb.V; a.H = bb.H; a.cs = bb.cs; a.sn = bb.sn; a.g = bb.g; a.y = bb.y;
     a.x = (C *)bb.x; a.rhs = (C *)bb.rhs; a.w = (C *)bb.W; a.red = bb.red; a.bar = c->d_bar; a.err = c->d_err;
+    a.cpart = bb.cpart; a.ctot = bb.ctot; a.ccnt = bb.ccnt;
     a.n = c->n; a.m = m; a.max_cycles = cycles; a.tol = tol; a.mixed = mixed;
     const long long n = c->n;
     if (nact > 0) {
@@ -719,6 +780,7 @@ static int launch_tick(scd_ctx *c, BatchBuffers &bb, int ns, int nact, int m, in
         run_matvec(c, (const C *)bb.Xin, (C *)bb.W, nact, nullptr);
     }
     void *args[] = {&a};
+    cudaMemsetAsync(bb.ccnt, 0, sizeof(int) * NSMAX, c->st);
     cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_tick<C>, dim3(bb.grid), dim3(BT), args, 0, c->st);
     c->launches += 2;
     return check_cuda(c, e, "tick launch");
@@ -730,10 +792,12 @@ static int launch_tick(scd_ctx *c, BatchBuffers &bb, int ns, int nact, int m, in
 // algorithm); 1: FP64 iterative refinement to `tol` around complex64
 // GMRES(m) inner solves to `inner_tol`, at most `max_outer` outer steps.
 int batch_solve(scd_ctx *c, int ncol, const cd *const *rhs_cols, cd *X, double tol, int m, int cycles, int ns,
-                int *iters, int *conv_out, int *status_out, int precision, double inner_tol, int max_outer) {
+                int *iters, int *conv_out, int *status_out, double *relres_out, int precision, double inner_tol,
+                int max_outer) {
     if (!c->batch) c->batch = new BatchBuffers();
     BatchBuffers &bb = *(BatchBuffers *)c->batch;
     const int mixed = precision == SCD_PREC_MIXED ? 1 : 0;
+    if (m < 1 || m > SCD_M_MAX) return set_error(c, SCD_BAD_ARG, "m = %d outside 1..%d", m, SCD_M_MAX);
     if (ns > NSMAX) ns = NSMAX;
     if (ns > ncol) ns = ncol;
     int rc = batch_prepare(c, ns, m, mixed, bb);
@@ -770,6 +834,7 @@ int batch_solve(scd_ctx *c, int ncol, const cd *const *rhs_cols, cd *X, double t
                 if (iters) iters[col] = hs[s].iters;
                 if (conv_out) conv_out[col] = hs[s].conv;
                 if (status_out) status_out[col] = hs[s].status;
+                if (relres_out) relres_out[col] = mixed ? hs[s].relres : hs[s].error;
                 c->col_latency_ms[col] = now_ms() - t_in[col];
                 if (hs[s].status != SCD_OK) worst = hs[s].status;
                 else if (!hs[s].conv && worst == SCD_OK) worst = SCD_NOT_CONVERGED;

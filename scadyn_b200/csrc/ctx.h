@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -38,18 +39,6 @@ struct NearTile {
 };
 SCD_HD long long tile_elems(int n1, int n2) { return ((long long)9 * n2 * (n1 | 1) + 1) & ~1LL; }
 SCD_HD long long tile_at(int n1, int i, int j, int e) { return (long long)(9 * j + e) * (n1 | 1) + i; }
-
-struct GmresState {
-    double b_norm;     // ||rhs||
-    double beta;       // ||r0|| of the current cycle
-    double error;      // |g(i+1)|/b_norm after the last step
-    int    step;       // Arnoldi steps taken in the current cycle
-    int    done;       // 1 once error < tol (or a fault)
-    int    conv_step;  // step at which the tolerance was met (0 = not yet)
-    int    iters;      // Arnoldi steps over all cycles
-    int    status;     // SCD_OK / SCD_NAN / SCD_TIMEOUT
-    int    reorth;     // re-orthogonalisations taken
-};
 
 struct scd_ctx {
     int dev = 0;
@@ -130,19 +119,12 @@ struct scd_ctx {
     cd *d_R = nullptr;                   // nrhs * 4 * Nx*Ny*Nz
     cd *d_nzpart = nullptr;              // nrhs * part_len
     cd *d_x = nullptr, *d_y = nullptr, *d_io = nullptr;   // n each (nrhs_cap)
+    cd *d_xT = nullptr;                  // matvec input, right-hand sides interleaved per unknown
 
-    // GMRES
-    int gm_m = 0;
-    cd *d_V = nullptr;                   // (m+1) * n
-    cd *d_H = nullptr;                   // (m+1) * m
-    cd *d_cs = nullptr, *d_sn = nullptr, *d_g = nullptr;
-    cd *d_rhs = nullptr, *d_w = nullptr;
-    double *d_red = nullptr;             // 2 * grid * 8 partial sums
+    // GMRES (batch.cu): single right-hand side of scd_gmres, grid barrier
+    cd *d_rhs = nullptr;
     GridBarrier *d_bar = nullptr;
     int *d_err = nullptr;
-    GmresState *d_state = nullptr;
-    GmresState *h_state = nullptr;       // pinned
-    int coop_grid = 0;
 
     // timing
     cudaEvent_t ev[8] = {};
@@ -154,7 +136,7 @@ struct scd_ctx {
     // complex64 operator copies and work buffers (mixed-precision inner solves)
     bool f_ready = false;
     cf *f_P = nullptr, *f_Fo = nullptr, *f_tw[3] = {nullptr, nullptr, nullptr};
-    cf *f_bpart = nullptr, *f_W = nullptr, *f_R = nullptr, *f_nzpart = nullptr;
+    cf *f_bpart = nullptr, *f_W = nullptr, *f_R = nullptr, *f_nzpart = nullptr, *f_xT = nullptr;
     int f_cap = 0;
 
     void *batch = nullptr;               // batch-solver buffers (batch.cu)
@@ -181,15 +163,10 @@ void launch_fft_chain(scd_ctx *c, const cd *x, int nrhs, const int *done);
 void launch_gather(scd_ctx *c, const cd *x, cd *y, int nrhs, const int *done);
 int build_twiddles(scd_ctx *c, int P, cd **out);
 
-// ---- GMRES (kernels_gmres.cu) ----
-int gmres_prepare(scd_ctx *c, int m);
-int gmres_solve(scd_ctx *c, const cd *d_rhs_slot, cd *d_x_slot, double tol, int m, int cycles,
-                int *iters, double *relres);
-
 // ---- batched column solves (batch.cu) ----
 void batch_free(scd_ctx *c);
 int batch_solve(scd_ctx *c, int ncol, const cd *const *rhs_cols, cd *X, double tol, int m, int cycles, int ns,
-                int *iters, int *conv, int *status, int precision, double inner_tol, int max_outer);
+                int *iters, int *conv, int *status, double *relres, int precision, double inner_tol, int max_outer);
 
 // ---- setup (kernels_setup.cu) ----
 int setup_green(scd_ctx *c, const scd_c128 *Fg_host);
@@ -203,4 +180,7 @@ void launch_T_assemble(scd_ctx *c, const cd *d_mat, int ncol_total, int col0, in
 int set_error(scd_ctx *c, int code, const char *fmt, ...);
 int check_cuda(scd_ctx *c, cudaError_t e, const char *what);
 int ensure_work(scd_ctx *c, int nrhs);
-int near_status(scd_ctx *c);   // SCD_TIMEOUT if a near-zone pipeline wait ran out (and clears it)
+int near_status(scd_ctx *c);
+// columns of the interleaved matvec input for nrhs right-hand sides: passes
+// of 16, at least 2 (16-byte rows for complex64)
+inline int xt_columns(int nrhs) { return std::max(2, (nrhs + 15) / 16 * 16); }   // SCD_TIMEOUT if a near-zone pipeline wait ran out (and clears it)

@@ -359,12 +359,12 @@ k_fft_x_inv(const Cx *__restrict__ W, Cx *__restrict__ R, const Cx *__restrict__
 // partial slot of g2.  k_gather adds the slots in a fixed order.
 //
 // Tiles stream through NZ_STAGES shared-memory stages filled by a producer
-// warp: the tile's blocks arrive by one bulk copy (TMA engine, completion
-// counted in bytes on the stage's "full" mbarrier) and the tile's x segment
-// by element copies (LDGSTS, transposed to x[3j+b][r], completion signalled
-// on the same barrier).  Consumer warps release a stage on its "empty"
-// barrier; there is no CTA-wide barrier in the tile loop, so row and column
-// warps run independently.  Warps [0, HT) hold row items (quad q, block row
+// warp: the tile's blocks and its x segment arrive by bulk copies (TMA
+// engine, completion counted in bytes on the stage's "full" mbarrier).  The
+// x segments come from xT, the right-hand sides interleaved per unknown
+// (k_xpose), so a group's x is one contiguous run x[3j+b][r].  Consumer
+// warps release a stage on its "empty" barrier; there is no CTA-wide
+// barrier in the tile loop, so row and column warps run independently.  Warps [0, HT) hold row items (quad q, block row
 // i): a 3 x U register tile of row sums for right-hand sides Uq..Uq+U-1.
 // Warps [HT, 2HT) hold column items (q, block column j).  Lanes run over i
 // (resp. j), so with the odd plane stride both sides read the tile without
@@ -383,16 +383,30 @@ struct NearPass {
     const int *grp_tile, *grp_off;
     const long long *pslot_base;
     const void *data;
-    const void *x;
-    long long ld;
+    const void *xT;          // [pass][3T][RG]
+    long long n;             // 3T
     void *part;
     long long part_len;
     const int *skip;
-    int nrhs, nq, half;
+    int nrhs, nq, half, rg_stride;   // rg_stride: right-hand sides per xT row (nq*U, or 2 for a lone complex64 one)
     long long stage_elems;   // ST elements per tile stage (even)
     int xcap;                // C elements per x buffer
     int *err;
 };
+
+// x (nrhs columns of stride ld) -> xT[p][k][RG]: the RG right-hand sides of
+// pass p interleaved per unknown k, zero beyond nrhs
+template <typename C>
+__global__ void k_xpose(const C *__restrict__ x, long long ld, long long n, int nrhs, int PS, int RG, C *__restrict__ xT) {
+    const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int p = blockIdx.y;
+    if (k >= n) return;
+    C *dst = xT + ((long long)p * n + k) * RG;
+    for (int r = 0; r < RG; ++r) {
+        const int rr = p * PS + r;
+        dst[r] = (r < PS && rr < nrhs) ? x[(long long)rr * ld + k] : czero<C>();
+    }
+}
 
 // U consecutive values of C from shared address addr (16-byte aligned when
 // C is complex64 and U is even)
@@ -416,21 +430,22 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS) k_near_groups(NearPass a) {
     C *const Xs0 = reinterpret_cast<C *>(Ms0 + NZ_STAGES * a.stage_elems);  // x(g2) stages
     C *const X1 = Xs0 + NZ_STAGES * a.xcap;                                 // x(g)
     const ST *data = static_cast<const ST *>(a.data);
-    const C *x = static_cast<const C *>(a.x);
+    const C *xT = static_cast<const C *>(a.xT);
     C *part = static_cast<C *>(a.part);
 
     const int g = blockIdx.x;
     const int t0 = a.grp_tile[g], t1 = a.grp_tile[g + 1];
     const int s1 = a.grp_off[g], n1 = a.grp_off[g + 1] - s1;
     const int ld1 = n1 | 1;
-    const int RG = a.nq * U;
+    const int RG = a.rg_stride;     // xT row length
+    const int PS = a.nq * U;        // right-hand sides per pass
     const int HT = a.half;
     const int ncw = 2 * HT / 32;                 // consumer warps
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (threadIdx.x == 0) {
         for (int st = 0; st < NZ_STAGES; ++st) {
-            mbar_init(&full[st], 33);            // producer lane 0 (bytes) + 32 lanes' LDGSTS
+            mbar_init(&full[st], 1);             // the producer's arrive (with the stage's bytes)
             mbar_init(&empty[st], ncw);
         }
         mbar_fence_init();
@@ -439,46 +454,29 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS) k_near_groups(NearPass a) {
 
     if (warp == ncw) {
         // ------------------------------------------------------ producer
-        int ord = 0;
-        for (int r0 = 0; r0 < a.nrhs; r0 += RG) {
-            const int rg = min(RG, a.nrhs - r0);
-            for (int t = t0; t < t1; ++t, ++ord) {
-                const int st = ord % NZ_STAGES, use = ord / NZ_STAGES;
-                if (use > 0) mbar_wait(&empty[st], (uint32_t)((use - 1) & 1), a.err);
-                if (t == t0 && ord > 0) {
-                    // X1 is rewritten: every consumer must be done with the previous pass
-                    const int pst = (ord - 1) % NZ_STAGES, puse = (ord - 1) / NZ_STAGES;
-                    mbar_wait(&empty[pst], (uint32_t)(puse & 1), a.err);
-                }
-                const NearTile &tl = a.tiles[t];
-                if (lane == 0) {
-                    const uint32_t bytes = (uint32_t)(tile_elems(tl.n1, tl.n2) * (long long)sizeof(ST));
-                    mbar_expect_tx(&full[st], bytes);
-                    bulk_g2s(Ms0 + st * a.stage_elems, data + tl.data_off, bytes, &full[st]);
-                }
-                {
-                    const int w = 3 * tl.n2;
-                    const C *xs = x + 3LL * tl.s2;
-                    C *dst = Xs0 + st * a.xcap;
-                    for (int e = lane; e < w * RG; e += 32) {
-                        const int r = e / w, k = e - r * w;
-                        const bool v = r < rg;
-                        cp_async_el<sizeof(C)>(dst + k * RG + r, v ? xs + (long long)(r0 + r) * a.ld + k : xs, v);
+        if (lane == 0) {
+            int ord = 0;
+            for (int r0 = 0; r0 < a.nrhs; r0 += PS) {
+                const C *xp = xT + (long long)(r0 / PS) * a.n * RG;
+                for (int t = t0; t < t1; ++t, ++ord) {
+                    const int st = ord % NZ_STAGES, use = ord / NZ_STAGES;
+                    if (use > 0) mbar_wait(&empty[st], (uint32_t)((use - 1) & 1), a.err);
+                    if (t == t0 && ord > 0) {
+                        // X1 is rewritten: every consumer must be done with the previous pass
+                        const int pst = (ord - 1) % NZ_STAGES, puse = (ord - 1) / NZ_STAGES;
+                        mbar_wait(&empty[pst], (uint32_t)(puse & 1), a.err);
                     }
+                    const NearTile &tl = a.tiles[t];
+                    const uint32_t mb = (uint32_t)(tile_elems(tl.n1, tl.n2) * (long long)sizeof(ST));
+                    const uint32_t xb = (uint32_t)(3 * tl.n2 * RG * sizeof(C));
+                    const uint32_t x1b = t == t0 ? (uint32_t)(3 * n1 * RG * sizeof(C)) : 0u;
+                    mbar_expect_tx(&full[st], mb + xb + x1b);
+                    bulk_g2s(Ms0 + st * a.stage_elems, data + tl.data_off, mb, &full[st]);
+                    bulk_g2s(Xs0 + st * a.xcap, xp + 3LL * tl.s2 * RG, xb, &full[st]);
+                    if (x1b) bulk_g2s(X1, xp + 3LL * s1 * RG, x1b, &full[st]);
                 }
-                if (t == t0) {
-                    const int w = 3 * n1;
-                    const C *xs = x + 3LL * s1;
-                    for (int e = lane; e < w * RG; e += 32) {
-                        const int r = e / w, k = e - r * w;
-                        const bool v = r < rg;
-                        cp_async_el<sizeof(C)>(X1 + k * RG + r, v ? xs + (long long)(r0 + r) * a.ld + k : xs, v);
-                    }
-                }
-                cp_async_arrive_noinc(&full[st]);
             }
         }
-        cp_async_wait_all();
         return;
     }
 
@@ -488,8 +486,8 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS) k_near_groups(NearPass a) {
     const bool row_item = rowside && it < n1 * a.nq;
     const int rq = row_item ? it / n1 : 0, ri = row_item ? it - rq * n1 : 0;
     int ord = 0;
-    for (int r0 = 0; r0 < a.nrhs; r0 += RG) {
-        const int rg = min(RG, a.nrhs - r0);
+    for (int r0 = 0; r0 < a.nrhs; r0 += PS) {
+        const int rg = min(PS, a.nrhs - r0);
         C acc[3][U];
 #pragma unroll
         for (int q = 0; q < 3; ++q)
@@ -689,6 +687,7 @@ template <> struct Res<cd> {
     static cd *W(scd_ctx *c) { return c->d_W; }
     static cd *R(scd_ctx *c) { return c->d_R; }
     static cd *part(scd_ctx *c) { return c->d_nzpart; }
+    static cd *xT(scd_ctx *c) { return c->d_xT; }
 };
 template <> struct Res<cf> {
     static const cf *P(scd_ctx *c) { return c->f_P; }
@@ -698,6 +697,7 @@ template <> struct Res<cf> {
     static cf *W(scd_ctx *c) { return c->f_W; }
     static cf *R(scd_ctx *c) { return c->f_R; }
     static cf *part(scd_ctx *c) { return c->f_nzpart; }
+    static cf *xT(scd_ctx *c) { return c->f_xT; }
 };
 
 template <int P, typename C>
@@ -776,19 +776,24 @@ template <typename ST, typename C, int U>
 void near_launch(scd_ctx *c, const ST *data, const C *x, int nrhs, const int *done) {
     NearPass a;
     a.tiles = c->d_tiles; a.grp_tile = c->d_grp_tile; a.grp_off = c->d_grp_off; a.pslot_base = c->d_pslot_base;
-    a.data = data; a.x = x; a.ld = c->n; a.part = Res<C>::part(c); a.part_len = c->part_len;
+    a.data = data; a.xT = Res<C>::xT(c); a.n = c->n; a.part = Res<C>::part(c); a.part_len = c->part_len;
     a.skip = done; a.nrhs = nrhs;
     a.stage_elems = c->max_tile_store;
     a.err = c->d_kerr;
-    auto smem = [&](int nq) {
-        return 128 + NZ_STAGES * sizeof(ST) * (size_t)a.stage_elems +
-               (NZ_STAGES + 1) * sizeof(C) * (size_t)(3 * c->max_per_group * nq * U);
-    };
     const int nq = U == 1 ? 1 : std::min(NZ_QMAX, (nrhs + U - 1) / U);
     a.nq = nq;
     a.half = 32 * ((c->max_per_group * a.nq + 31) / 32);
-    a.xcap = 3 * c->max_per_group * a.nq * U;
-    const size_t sh = smem(nq);
+    // xT rows are whole 16-byte units (bulk-copy granularity)
+    a.rg_stride = nq * U;
+    while ((a.rg_stride * sizeof(C)) % 16) ++a.rg_stride;
+    a.xcap = 3 * c->max_per_group * a.rg_stride;
+    {
+        const int npass = (nrhs + nq * U - 1) / (nq * U);
+        dim3 g((unsigned)((c->n + 255) / 256), npass);
+        k_xpose<C><<<g, 256, 0, c->st>>>(x, c->n, c->n, nrhs, nq * U, a.rg_stride, Res<C>::xT(c));
+        c->launches += 1;
+    }
+    const size_t sh = 128 + NZ_STAGES * sizeof(ST) * (size_t)a.stage_elems + (NZ_STAGES + 1) * sizeof(C) * (size_t)a.xcap;
     cudaFuncSetAttribute(k_near_groups<ST, C, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
     k_near_groups<ST, C, U><<<c->ngroups, 2 * a.half + 32, sh, c->st>>>(a);
 }
@@ -889,7 +894,8 @@ int ensure_work_single(scd_ctx *c, int nrhs) {
     int rc;
     if ((rc = al(&c->f_bpart, r * c->ncubes * 4 * 27)) || (rc = al(&c->f_W, r * 4 * (size_t)c->Px * c->Py * c->Nz)) ||
         (rc = al(&c->f_R, r * 4 * (size_t)c->Nx * c->Ny * c->Nz)) ||
-        (rc = al(&c->f_nzpart, r * (size_t)std::max<long long>(c->part_len, 1))))
+        (rc = al(&c->f_nzpart, r * (size_t)std::max<long long>(c->part_len, 1))) ||
+        (rc = al(&c->f_xT, (size_t)xt_columns(nrhs) * c->n)))
         return rc;
     c->f_cap = nrhs;
     return SCD_OK;
