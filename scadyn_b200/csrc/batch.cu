@@ -3,12 +3,12 @@
 // Green octant, near-zone tiles) and every grid barrier.  Each slot runs its
 // own restarted GMRES exactly as gmres (src/gmres_module.f90:180-325): x0 =
 // rhs, MGS with the conditional re-orthogonalisation, complex Givens, y =
-// H^-1 g, x += V y.  A slot's arithmetic does not depend on what the other
-// slots hold (per-slot reductions over fixed chunks, summed in a fixed
-// order), so a column's result is bit-identical whether it is solved alone
-// (scd_gmres runs one slot) or in a batch.  A slot whose column converged (or ran out of cycles)
-// is refilled with the next column on the following tick (continuous
-// batching).
+// H^-1 g, x += V y.  A slot's arithmetic does not depend on what the other slots hold
+// (per-slot reductions over fixed chunks, summed in a fixed order), so a
+// column's result is bit-identical whether it is solved alone (scd_gmres
+// runs one slot) or in a batch.  A slot whose column converged (or ran out
+// of cycles) is refilled with the next column on the following tick
+// (continuous batching).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -91,8 +91,8 @@ struct Chunks {
     long long L;    // chunk length
     int gw, nw;     // this warp, warps in the grid
     int lane;
-    __device__ Chunks(long long n) {
-        L = (n + NCH - 1) / NCH;
+    __device__ Chunks(long long n, int nch) {
+        L = (n + nch - 1) / nch;
         gw = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
         nw = (int)(((long long)gridDim.x * blockDim.x) >> 5);
         lane = threadIdx.x & 31;
@@ -157,6 +157,121 @@ __device__ __forceinline__ void load_totals(const TickArgs<C> &a, int parity, in
     __syncthreads();
 }
 
+// Givens update of the new H column, residual estimate and, when a cycle
+// ends, y = H^-1 g (back substitution) for every Arnoldi slot: CTA 0, one
+// thread per slot.  H column i-1 is complete except H(i, i-1) = shn[s];
+// sreo[s] flags a re-orthogonalised step (counted).
+template <typename C>
+__device__ void givens_step(const TickArgs<C> &a, const int *smode, const int *sstep, const double *shn, const int *sreo) {
+    const int ldh = a.m + 1;
+    {
+        for (int s = threadIdx.x; s < a.ns; s += blockDim.x) {
+            if (smode[s] != SLOT_ARNOLDI) continue;
+            Slot &sl = a.slots[s];
+            const int i = sstep[s] + 1;
+            cd *Hc = a.H + (size_t)s * ldh * a.m + (size_t)ldh * (i - 1);
+            cd *cs = a.cs + (size_t)s * (a.m + 1), *sn = a.sn + (size_t)s * (a.m + 1), *g = a.g + (size_t)s * (a.m + 1);
+            Hc[i] = cmk(shn[s], 0.0);
+            for (int k = 1; k <= i - 1; ++k) {
+                const cd c = cs[k - 1], sv = sn[k - 1];
+                const cd tmp = csub(cmul(c, Hc[k - 1]), cmul(sv, Hc[k]));
+                Hc[k] = cadd(cmul(sv, Hc[k - 1]), cmul(cconj(c), Hc[k]));
+                Hc[k - 1] = tmp;
+            }
+            const double nu = sqrt(cabs2(Hc[i - 1]) + cabs2(Hc[i]));
+            if (nu != 0.0) {
+                const cd c = cconj(cmk(Hc[i - 1].x / nu, Hc[i - 1].y / nu));
+                const cd sv = cmk(-Hc[i].x / nu, -Hc[i].y / nu);
+                cs[i - 1] = c;
+                sn[i - 1] = sv;
+                Hc[i - 1] = csub(cmul(c, Hc[i - 1]), cmul(sv, Hc[i]));
+                Hc[i] = cmk(0, 0);
+                const cd t1 = g[i - 1], t2 = g[i];
+                g[i - 1] = csub(cmul(c, t1), cmul(sv, t2));
+                g[i] = cadd(cmul(sv, t1), cmul(cconj(c), t2));
+            }
+            const double error = sqrt(cabs2(g[i])) / sl.b_norm;
+            sl.error = error;
+            sl.step = i;
+            sl.iters += 1;
+            if (sreo[s]) sl.reorth += 1;
+            sl.finish = 0;
+            if (error < a.tol) { sl.conv = 1; sl.finish = 1; }
+            else if (i == a.m) sl.finish = 1;
+            if (!(error == error)) { sl.status = SCD_NAN; sl.finish = 0; sl.mode = SLOT_DONE; }
+            if (*a.err) { sl.status = SCD_TIMEOUT; sl.finish = 0; sl.mode = SLOT_DONE; }
+            if (sl.finish) {
+                // y = H(1:i,1:i)^-1 g(1:i), back substitution
+                cd *ys = a.y + (size_t)s * (a.m + 1);
+                const cd *Hs = a.H + (size_t)s * ldh * a.m;
+                for (int r = i - 1; r >= 0; --r) {
+                    cd acc = g[r];
+                    for (int cc = r + 1; cc < i; ++cc) acc = csub(acc, cmul(Hs[r + (size_t)ldh * cc], ys[cc]));
+                    ys[r] = cdiv(acc, Hs[r + (size_t)ldh * r]);
+                }
+            }
+        }
+    }
+}
+
+// Cycle ends (x += V(:,1:i) y, chunks handled like the streaming phases)
+// and the slots' next modes.  Call after the grid barrier that follows
+// givens_step.
+template <typename C>
+__device__ void cycle_end(const TickArgs<C> &a, const Chunks &ch, int nch, const int *smode, cd (*ysm)[SCD_M_MAX + 1]) {
+    const long long n = a.n;
+    const int lane = ch.lane;
+    const int nitems = a.ns * nch;
+    {
+        cd *yw = ysm[threadIdx.x >> 5];
+        for (int it = ch.gw; it < nitems; it += ch.nw) {
+            const int s = it / nch, c = it - s * nch;
+            if (smode[s] != SLOT_ARNOLDI) continue;
+            const Slot *sl = a.slots + s;
+            if (!__ldcg(&sl->finish)) continue;      // uniform across the warp (L2 read after the barrier)
+            const int kd = __ldcg(&sl->step);
+            const cd *ys = a.y + (size_t)s * (a.m + 1);
+            for (int cc = lane; cc < kd; cc += 32) yw[cc] = make_double2(__ldcg(&ys[cc].x), __ldcg(&ys[cc].y));
+            __syncwarp();
+            const long long qa = c * ch.L, qb = min(n, qa + ch.L);
+            const C *Vs = a.V + (size_t)s * (a.m + 1) * n;
+            C *xs = a.x + (size_t)s * n;
+            for (long long q = qa + lane; q < qb; q += 32 * TU) {
+                cd acc[TU];
+#pragma unroll
+                for (int e = 0; e < TU; ++e) acc[e] = cmk(0, 0);
+                for (int cc = 0; cc < kd; ++cc) {
+                    const cd yc = yw[cc];
+                    const C *vc = Vs + (size_t)cc * n;
+#pragma unroll
+                    for (int e = 0; e < TU; ++e) {
+                        const long long qq = q + 32 * e;
+                        if (qq < qb) cfma(acc[e], to_cd(vc[qq]), yc);
+                    }
+                }
+#pragma unroll
+                for (int e = 0; e < TU; ++e) {
+                    const long long qq = q + 32 * e;
+                    if (qq < qb) store_c(xs[qq], cadd(to_cd(xs[qq]), acc[e]));
+                }
+            }
+            __syncwarp();
+        }
+    }
+    if (blockIdx.x == 0) {
+        // `finish` stays set: other CTAs may still be reading it; the next
+        // Givens update of the slot overwrites it
+        for (int s = threadIdx.x; s < a.ns; s += blockDim.x) {
+            if (smode[s] != SLOT_ARNOLDI) continue;
+            Slot &sl = a.slots[s];
+            if (!sl.finish) continue;
+            if (sl.conv) sl.mode = a.mixed ? SLOT_INNER_DONE : SLOT_DONE;
+            else if (sl.cycle < a.max_cycles) { sl.mode = SLOT_START; sl.zero_x = 0; }
+            else sl.mode = a.mixed ? SLOT_INNER_DONE : SLOT_DONE;
+        }
+    }
+}
+
 // One tick: cycle starts (r = rhs - A x, V0 = r/||r||) and Arnoldi steps
 // (MGS, normalisation, Givens) for every active slot; cycle ends update x.
 template <typename C>
@@ -168,7 +283,7 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
     __shared__ cd ysm[BW][SCD_M_MAX + 1];    // per warp: y of the slot being updated
     const long long n = a.n;
     const int ldh = a.m + 1;
-    const Chunks ch(n);
+    const Chunks ch(n, NCH);
     const int lane = ch.lane;
     const int nitems = a.ns * NCH;
     for (int s = threadIdx.x; s < a.ns; s += blockDim.x) {
@@ -455,103 +570,12 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
         }
     }
     if (blockIdx.x == 0) {
-        for (int s = threadIdx.x; s < a.ns; s += blockDim.x) {
-            if (smode[s] != SLOT_ARNOLDI) continue;
-            Slot &sl = a.slots[s];
-            const int i = sstep[s] + 1;
-            cd *Hc = a.H + (size_t)s * ldh * a.m + (size_t)ldh * (i - 1);
-            cd *cs = a.cs + (size_t)s * (a.m + 1), *sn = a.sn + (size_t)s * (a.m + 1), *g = a.g + (size_t)s * (a.m + 1);
-            Hc[i] = cmk(shn[s], 0.0);
-            for (int k = 1; k <= i - 1; ++k) {
-                const cd c = cs[k - 1], sv = sn[k - 1];
-                const cd tmp = csub(cmul(c, Hc[k - 1]), cmul(sv, Hc[k]));
-                Hc[k] = cadd(cmul(sv, Hc[k - 1]), cmul(cconj(c), Hc[k]));
-                Hc[k - 1] = tmp;
-            }
-            const double nu = sqrt(cabs2(Hc[i - 1]) + cabs2(Hc[i]));
-            if (nu != 0.0) {
-                const cd c = cconj(cmk(Hc[i - 1].x / nu, Hc[i - 1].y / nu));
-                const cd sv = cmk(-Hc[i].x / nu, -Hc[i].y / nu);
-                cs[i - 1] = c;
-                sn[i - 1] = sv;
-                Hc[i - 1] = csub(cmul(c, Hc[i - 1]), cmul(sv, Hc[i]));
-                Hc[i] = cmk(0, 0);
-                const cd t1 = g[i - 1], t2 = g[i];
-                g[i - 1] = csub(cmul(c, t1), cmul(sv, t2));
-                g[i] = cadd(cmul(sv, t1), cmul(cconj(c), t2));
-            }
-            const double error = sqrt(cabs2(g[i])) / sl.b_norm;
-            sl.error = error;
-            sl.step = i;
-            sl.iters += 1;
-            if (snormav[s] + (double)0.001f * shn[s] == snormav[s]) sl.reorth += 1;
-            sl.finish = 0;
-            if (error < a.tol) { sl.conv = 1; sl.finish = 1; }
-            else if (i == a.m) sl.finish = 1;
-            if (!(error == error)) { sl.status = SCD_NAN; sl.finish = 0; sl.mode = SLOT_DONE; }
-            if (*a.err) { sl.status = SCD_TIMEOUT; sl.finish = 0; sl.mode = SLOT_DONE; }
-            if (sl.finish) {
-                // y = H(1:i,1:i)^-1 g(1:i), back substitution
-                cd *ys = a.y + (size_t)s * (a.m + 1);
-                const cd *Hs = a.H + (size_t)s * ldh * a.m;
-                for (int r = i - 1; r >= 0; --r) {
-                    cd acc = g[r];
-                    for (int cc = r + 1; cc < i; ++cc) acc = csub(acc, cmul(Hs[r + (size_t)ldh * cc], ys[cc]));
-                    ys[r] = cdiv(acc, Hs[r + (size_t)ldh * r]);
-                }
-            }
-        }
+        if (threadIdx.x < a.ns) sact[threadIdx.x] = snormav[threadIdx.x] + (double)0.001f * shn[threadIdx.x] == snormav[threadIdx.x];
+        __syncthreads();
+        givens_step(a, smode, sstep, shn, sact);
     }
     grid_barrier(a.bar, gridDim.x, a.err);
-    // ---- cycle end: x += V(:,1:i) y; next cycle or done
-    {
-        cd *yw = ysm[threadIdx.x >> 5];
-        for (int it = ch.gw; it < nitems; it += ch.nw) {
-            const int s = it / NCH, c = it - s * NCH;
-            if (smode[s] != SLOT_ARNOLDI) continue;
-            const Slot *sl = a.slots + s;
-            if (!__ldcg(&sl->finish)) continue;      // uniform across the warp (L2 read after the barrier)
-            const int kd = __ldcg(&sl->step);
-            const cd *ys = a.y + (size_t)s * (a.m + 1);
-            for (int cc = lane; cc < kd; cc += 32) yw[cc] = make_double2(__ldcg(&ys[cc].x), __ldcg(&ys[cc].y));
-            __syncwarp();
-            const long long qa = c * ch.L, qb = min(n, qa + ch.L);
-            const C *Vs = a.V + (size_t)s * (a.m + 1) * n;
-            C *xs = a.x + (size_t)s * n;
-            for (long long q = qa + lane; q < qb; q += 32 * TU) {
-                cd acc[TU];
-#pragma unroll
-                for (int e = 0; e < TU; ++e) acc[e] = cmk(0, 0);
-                for (int cc = 0; cc < kd; ++cc) {
-                    const cd yc = yw[cc];
-                    const C *vc = Vs + (size_t)cc * n;
-#pragma unroll
-                    for (int e = 0; e < TU; ++e) {
-                        const long long qq = q + 32 * e;
-                        if (qq < qb) cfma(acc[e], to_cd(vc[qq]), yc);
-                    }
-                }
-#pragma unroll
-                for (int e = 0; e < TU; ++e) {
-                    const long long qq = q + 32 * e;
-                    if (qq < qb) store_c(xs[qq], cadd(to_cd(xs[qq]), acc[e]));
-                }
-            }
-            __syncwarp();
-        }
-    }
-    if (blockIdx.x == 0) {
-        // `finish` stays set: other CTAs may still be reading it; the next
-        // Givens update of the slot overwrites it
-        for (int s = threadIdx.x; s < a.ns; s += blockDim.x) {
-            if (smode[s] != SLOT_ARNOLDI) continue;
-            Slot &sl = a.slots[s];
-            if (!sl.finish) continue;
-            if (sl.conv) sl.mode = a.mixed ? SLOT_INNER_DONE : SLOT_DONE;
-            else if (sl.cycle < a.max_cycles) { sl.mode = SLOT_START; sl.zero_x = 0; }
-            else sl.mode = a.mixed ? SLOT_INNER_DONE : SLOT_DONE;
-        }
-    }
+    cycle_end(a, ch, NCH, smode, ysm);
 }
 
 // matvec input per slot, compacted: x at a cycle start, v_step during
@@ -748,6 +772,7 @@ int batch_prepare(scd_ctx *c, int ns, int m, int mixed, BatchBuffers &b) {
     if ((rc = al((void **)&b.cpart, sizeof(double) * (size_t)NSMAX * NCH * 4, "chunk partials"))) return rc;
     if ((rc = al((void **)&b.ctot, sizeof(double) * 2 * NSMAX * 4, "slot totals"))) return rc;
     if ((rc = al((void **)&b.ccnt, sizeof(int) * NSMAX, "chunk counters"))) return rc;
+
     if (cudaMallocHost((void **)&b.h_slots, sizeof(Slot) * ns) != cudaSuccess) return set_error(c, SCD_OOM, "pinned slots");
     int per_sm = 0, per_sm2 = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_tick<cd>, BT, 0);
