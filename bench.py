@@ -4,17 +4,21 @@
 Workload (default): a seeded synthetic ellipsoid with semi-axes 1:0.8:0.6 at
 size parameter ka = 8 (~150k tetrahedra from a jittered cube-lattice mesh,
 per-tet eps with Re ~ U(2,3), Im ~ U(0.01,0.1)), zero-padded pFFT grid 128^3
-(64 nodes on the longest axis), Nmax = 14 (448 incident VSWF columns), GMRES
-Krylov dimension 50, 4 restart cycles, tol 1e-6.  `--config c1` runs the
-43k-tet sphere (ka = 2, Nmax = 6, grid 64^3).
+(64 nodes on the longest axis), Nmax = 14 (448 incident VSWF columns).
+`--config c1` runs the 43k-tet sphere (ka = 2, Nmax = 6, grid 64^3).
 
 A step solves `--block` consecutive T-matrix columns (cycling through the
-448).  `value` is columns/s over K timed steps with the operator and the
+448) in the mixed-precision form: complex64 inner GMRES(20) to 1e-4 and FP64
+iterative refinement on the true residual to 1e-6, `--slots` columns in
+flight.  `value` is columns/s over K timed steps with the operator and the
 incident columns resident in HBM (device time from CUDA events on the
 library's stream, max over ranks); `e2e` is the same through the C ABI call a
-host makes (scd_solve_columns with host buffers: the step's columns copied in,
-T columns copied out, inside the timed region).  `--impl reference` times the
-CPU oracle (the reference's algorithm restated in C) on the same operator.
+host makes (scd_solve_columns with host buffers: the step's columns copied
+in, T columns copied out, inside the timed region).  `forms` holds the plain
+FP64 GMRES(50) form one column at a time and batched, on the same columns,
+and `t_rel_err_vs_fp64` the Frobenius error of the mixed T against the FP64
+T.  `--impl reference` times the CPU oracle (the reference's algorithm
+restated in C) on the same operator.
 """
 from __future__ import annotations
 
@@ -36,11 +40,13 @@ CONFIGS = {
     "c1": dict(workload="C1: sphere ka=2, h=a/12 (~43k tets), eps=2.25+0.01i, Nmax=6 (96 columns), "
                         "padded pFFT grid 64^3, GMRES(50) tol 1e-6",
                body="sphere", n_major=12.0, axes=(1.0, 1.0, 1.0), ka=2.0, eps=2.25 + 0.01j,
-               Nmax=6, N=32, tol=1e-6, m=50, cycles=4, seed=1001, eps_seed=2001),
+               Nmax=6, N=32, tol=1e-6, m=50, cycles=4, seed=1001, eps_seed=2001,
+               inner_m=20, inner_tol=1e-4, max_outer=10),
     "c2": dict(workload="C2: ellipsoid 1:0.8:0.6, ka=8 (~150k tets), per-tet eps Re U(2,3) Im U(0.01,0.1), "
                         "Nmax=14 (448 columns), padded pFFT grid 128^3, GMRES(50) tol 1e-6",
                body="ellipsoid", n_major=23.2, axes=(1.0, 0.8, 0.6), ka=8.0, eps=None,
-               Nmax=14, N=64, tol=1e-6, m=50, cycles=12, seed=1002, eps_seed=2002),
+               Nmax=14, N=64, tol=1e-6, m=50, cycles=12, seed=1002, eps_seed=2002,
+               inner_m=20, inner_tol=1e-4, max_outer=10),
 }
 
 L2_BYTES = 126 * 1024 * 1024
@@ -273,10 +279,15 @@ def main():
         return
 
     # ---------------------------------------------------------------- ours
-    opts = dict(tol=cfg["tol"], m=cfg["m"], cycles=cfg["cycles"])
+    # headline form: mixed precision (complex64 inner GMRES(inner_m) to
+    # inner_tol, FP64 iterative refinement on the true residual to tol),
+    # `S` columns in flight as batched slots, continuous batching
+    fp64 = dict(tol=cfg["tol"], m=cfg["m"], cycles=cfg["cycles"])
+    mixed = dict(tol=cfg["tol"], m=cfg["inner_m"], cycles=60, precision=api.PREC_MIXED,
+                 inner_tol=cfg["inner_tol"], max_outer=cfg["max_outer"])
     S = min(args.slots, B)
     for st in range(args.warmup):
-        solver.compute_T_matrix(Nmax, col0=cols_for(st), ncol=B, block=S, **opts)
+        solver.compute_T_matrix(Nmax, col0=cols_for(st), ncol=B, block=S, **mixed)
 
     def barrier():
         if dist:
@@ -284,101 +295,119 @@ def main():
             dist.barrier()
             torch.cuda.synchronize()
 
-    lat, iters, cycles = [], [], []
+    def max_over_ranks(v):
+        if not dist:
+            return v
+        import torch
+        tt = torch.tensor([v], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
+    lat, iters, T_mixed0 = [], [], None
     barrier()
     solver.timing(reset=True)
     t_wall = time.time()
     with Clocks(local) as clk:
         for st in range(args.warmup, args.warmup + args.steps):
             c0 = cols_for(st)
-            _, it = solver.compute_T_matrix(Nmax, col0=c0, ncol=B, block=S, **opts)
+            Tm, it = solver.compute_T_matrix(Nmax, col0=c0, ncol=B, block=S, **mixed)
+            if T_mixed0 is None:
+                T_mixed0 = Tm
             lat += list(solver.column_latency(B))
             iters += [int(v) for v in it]
-            cycles += [max(1, -(-int(v) // cfg["m"])) for v in it]
     barrier()
     wall = time.time() - t_wall
     tm = solver.timing(reset=True)
-    dev_ms = tm["accum_ms"]
+    dev_ms = max_over_ranks(tm["accum_ms"])
     launches = int(tm["launches"])
     cols = args.steps * B
-    if dist:
-        import torch
-        tt = torch.tensor([dev_ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        dev_ms = float(tt.item())
     value = world * cols / (dev_ms / 1e3)
 
-    # the plain form: one column at a time (no batching), same columns
+    # the same columns in FP64 (the plain algorithm, batched): accuracy
+    # reference for the mixed T and the batched-FP64 comparison form
     forms = {}
+    c0 = cols_for(args.warmup)
+    solver.timing(reset=True)
+    T64, it64 = solver.compute_T_matrix(Nmax, col0=c0, ncol=B, block=S, **fp64)
+    ms64 = solver.timing(reset=True)["accum_ms"]
+    t_err = float(np.linalg.norm(T_mixed0 - T64) / np.linalg.norm(T64))
+    forms["batched_fp64_%d_slots" % S] = round(B / (ms64 / 1e3), 4)
+    fp64_iters, fp64_cycles = [int(v) for v in it64], [max(1, -(-int(v) // cfg["m"])) for v in it64]
+    # plain form: one column at a time, FP64 GMRES(m) -- the reference's algorithm on the GPU
     if args.plain_sample > 0:
         solver.timing(reset=True)
-        c0 = cols_for(args.warmup)
         for j in range(args.plain_sample):
-            solver.compute_T_matrix(Nmax, col0=c0 + j, ncol=1, block=1, **opts)
+            solver.compute_T_matrix(Nmax, col0=c0 + j, ncol=1, block=1, **fp64)
         pm = solver.timing(reset=True)["accum_ms"]
         forms["plain_fp64_one_column"] = round(args.plain_sample / (pm / 1e3), 4)
-    forms["batched_fp64_%d_slots" % S] = round(value / world, 4)
+    forms["mixed_batched_%d_slots" % S] = round(value / world, 4)
+    if "plain_fp64_one_column" in forms:
+        forms["mixed_batched_over_plain_fp64"] = round(forms["mixed_batched_%d_slots" % S] /
+                                                       forms["plain_fp64_one_column"], 3)
 
     # e2e: the same columns through scd_solve_columns with host buffers
+    # (incident columns host->device, T columns device->host, per step)
     mat_all = solver.vswf2constant(Nmax)
     e2e_ms = 0.0
     h2d = d2h = 0
     for st in range(args.warmup, args.warmup + args.steps):
-        c0 = cols_for(st)
-        blk = np.ascontiguousarray(mat_all[c0:c0 + B])
-        solver.timing(reset=True)
+        c0s = cols_for(st)
+        blk = np.ascontiguousarray(mat_all[c0s:c0s + B])
         t = time.time()
-        Tc, its, _, _ = solver.solve_columns(blk, block=S, **opts)
+        Tc, its, _, _ = solver.solve_columns(blk, block=S, **mixed)
         e2e_ms += (time.time() - t) * 1e3
         h2d = blk.nbytes
         d2h = Tc.nbytes + its.nbytes
-    e2e_val = cols / (e2e_ms / 1e3)
-    if dist:
-        import torch
-        tt = torch.tensor([e2e_ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_val = world * cols / (float(tt.item()) / 1e3)
+    e2e_val = world * cols / (max_over_ranks(e2e_ms) / 1e3)
 
-    # per-kernel times of the batched matvec (the timed region's shape)
-    profb = solver.profile_matvec(5, S)
-    batched = {"nrhs": S, "matvec_ms": profb["matvec_ms"], "nearzone_ms": profb["nearzone_ms"],
-               "fft_chain_ms": profb["fft_ms"], "gather_ms": profb["gather_ms"]}
-    # roofline of the dominant kernel of the memory-bound single-column form
-    # (near-zone tiles) from live CUDA events
+    # per-kernel times of the batched complex64 matvec (the timed region's shape)
+    profb = solver.profile_matvec(5, S, api.PREC_MIXED)
+    batched = {"nrhs": S, "precision": "complex64", "matvec_ms": profb["matvec_ms"],
+               "nearzone_ms": profb["nearzone_ms"], "fft_chain_ms": profb["fft_ms"],
+               "gather_ms": profb["gather_ms"]}
+    # roofline of the dominant HBM-bound kernel: the near-zone block SpMV of
+    # a single-column matvec (live CUDA events on the library's stream)
     prof = solver.profile_matvec(20, 1)
     Bref = solver.nearzone_count()
     alg_bytes = Bref * (9 * 8 + 8)                 # complex64 blocks + index pair, per matvec
     near_ms = prof["nearzone_ms"]
     achieved = alg_bytes / (near_ms / 1e3) / 1e9
     peak, kind = peaks()
-    traffic = profile_traffic(f"near_tiles_{args.config}.txt")
+    traffic = profile_traffic(f"near_groups_{args.config}.txt")
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": kind,
-            "kernel": "k_near_groups (near-zone block SpMV)", "alg_bytes_per_launch": alg_bytes,
-            "avg_launch_ms": near_ms, "matvec_ms": prof["matvec_ms"], "fft_chain_ms": prof["fft_ms"],
-            "gather_ms": prof["gather_ms"]}
+            "kernel": "k_near_groups (near-zone block SpMV, one right-hand side, FP64)",
+            "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": near_ms, "matvec_ms": prof["matvec_ms"],
+            "fft_chain_ms": prof["fft_ms"], "gather_ms": prof["gather_ms"]}
+    # whole pFFT matvec against HBM (algorithmic bytes per right-hand side,
+    # four merged convolutions, operator reads shared by the batch)
+    roof["matvec"] = matvec_roofline(solver, desc, mesh.n_tet, Bref, peak, prof["matvec_ms"], profb["matvec_ms"], S)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            cpu = cpu_baseline(solver, mesh, gs, k, cfg, iters, cycles)
+            cpu = cpu_baseline(solver, mesh, gs, k, cfg, fp64_iters, fp64_cycles)
         except Exception as e:   # the baseline is reported, never the headline
             cpu = {"value": None, "error": str(e)[:200]}
 
     if rank == 0:
         lat_s = sorted(lat)
         line = {
-            "metric": "T-matrix columns/s (FP64 GMRES(50), tol 1e-6, batched columns)",
+            "metric": "T-matrix columns/s (mixed complex64 GMRES + FP64 refinement to 1e-6, batched columns; "
+                      "T rel err vs FP64 <= 1e-5)",
             "value": round(value, 4), "unit": "columns/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(dev_ms / args.steps, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64 inner / f64 outer",
             "data": "synthetic (seeded jittered cube-lattice mesh)",
             "config": {"workload": cfg["workload"], "tets": mesh.n_tet,
                        "grid_nodes": [desc.Nx, desc.Ny, desc.Nz], "near_blocks": Bref,
                        "near_bytes": solver.nearzone_bytes(), "columns_per_step": B, "slots": S,
-                       "precision": "complex FP64 (near zone stored complex64 as the reference)",
+                       "precision": "complex64 inner GMRES(%d) to %g, FP64 outer refinement to %g (near zone "
+                                    "stored complex64 as the reference)" % (cfg["inner_m"], cfg["inner_tol"],
+                                                                            cfg["tol"]),
                        "l2": "inputs larger than L2 (near-zone tiles %.2f GB per matvec)" % (solver.nearzone_bytes() / 1e9),
                        "parallelism": f"replicas x{world}"},
+            "t_rel_err_vs_fp64": t_err,
             "p50_ms": round(float(np.percentile(lat_s, 50)), 3),
             "p99_ms": round(float(np.percentile(lat_s, 99)), 3),
             "iters_mean": float(np.mean(iters)),
@@ -397,6 +426,31 @@ def main():
     solver.close()
     if dist:
         dist.destroy_process_group()
+
+
+def matvec_roofline(solver, desc, T, Bref, peak, ms1, msb, nb):
+    """Algorithmic HBM bytes of one pFFT matvec per right-hand side (read x,
+    write Ax; four merged convolutions over the pruned grid, each spectrum
+    written and read twice; projectors, index-free box nodes, Green octant and
+    near-zone blocks read once per call and shared by the nb right-hand sides
+    of a batch) against the measured matvec time."""
+    n = 3 * T
+    Nx, Ny, Nz = desc.Nx, desc.Ny, desc.Nz
+    K = 4
+
+    def bytes_per_rhs(c, cs, cf, b):
+        own = 2 * n * c + K * 16 * Nx * Ny * Nz * c
+        shared = 4 * 27 * T * cs + K * (Nx + 1) * (Ny + 1) * (Nz + 1) * cf + Bref * (9 * 8 + 8)
+        return own + shared / b
+
+    b1 = bytes_per_rhs(16, 16, 16, 1)
+    bb = bytes_per_rhs(8, 8, 8, nb)
+    a1 = b1 / (ms1 / 1e3) / 1e9
+    ab = bb / (msb / nb / 1e3) / 1e9
+    return {"fp64_one_rhs": {"alg_bytes": int(b1), "ms": round(ms1, 4), "achieved": round(a1, 1),
+                             "frac": round(a1 / peak, 4)},
+            "complex64_batched": {"nrhs": nb, "alg_bytes_per_rhs": int(bb), "ms_per_rhs": round(msb / nb, 4),
+                                  "achieved": round(ab, 1), "frac": round(ab / peak, 4)}}
 
 
 if __name__ == "__main__":

@@ -358,12 +358,13 @@ k_fft_x_inv(const Cx *__restrict__ W, Cx *__restrict__ R, const Cx *__restrict__
 // a single row slot; each off-diagonal tile's column sums go to that tile's
 // partial slot of g2.  k_gather adds the slots in a fixed order.
 //
-// Tiles stream through NZ_STAGES shared-memory stages filled by a producer
-// warp: the tile's blocks and its x segment arrive by bulk copies (TMA
-// engine, completion counted in bytes on the stage's "full" mbarrier).  The
-// x segments come from xT, the right-hand sides interleaved per unknown
+// Tiles stream through a shared-memory ring filled by a producer thread: a
+// tile's blocks and its x segment arrive by bulk copies (TMA engine,
+// completion counted in bytes on the slot's "full" mbarrier) at the ring's
+// head, so as many tiles are in flight as their sizes allow (up to NZ_SLOTS).
+// The x segments come from xT, the right-hand sides interleaved per unknown
 // (k_xpose), so a group's x is one contiguous run x[3j+b][r].  Consumer
-// warps release a stage on its "empty" barrier; there is no CTA-wide
+// warps release a tile on its slot's "empty" barrier; there is no CTA-wide
 // barrier in the tile loop, so row and column warps run independently.  Warps [0, HT) hold row items (quad q, block row
 // i): a 3 x U register tile of row sums for right-hand sides Uq..Uq+U-1.
 // Warps [HT, 2HT) hold column items (q, block column j).  Lanes run over i
@@ -375,7 +376,10 @@ k_fft_x_inv(const Cx *__restrict__ W, Cx *__restrict__ R, const Cx *__restrict__
 // for any number of right-hand sides and any U, so a column's result does
 // not depend on the batch it is solved in.
 constexpr int NZ_QMAX = 4;             // quads of right-hand sides per pass
-constexpr int NZ_STAGES = 2;
+constexpr int NZ_SLOTS = 8;                 // tiles in flight at most (mbarrier pairs)
+constexpr int NZ_META = 256;                // bytes of barriers and ring offsets
+constexpr size_t NZ_SMEM_2CTA = 113 * 1024; // dynamic shared memory per CTA that lets two CTAs share an SM
+constexpr size_t NZ_SMEM_MAX = 227 * 1024;
 constexpr int NZ_MAX_THREADS = 2 * 32 * ((SCD_GROUP_MAX * NZ_QMAX + 31) / 32) + 32;
 
 struct NearPass {
@@ -389,8 +393,8 @@ struct NearPass {
     long long part_len;
     const int *skip;
     int nrhs, nq, half, rg_stride;   // rg_stride: right-hand sides per xT row (nq*U, or 2 for a lone complex64 one)
-    long long stage_elems;   // ST elements per tile stage (even)
-    int xcap;                // C elements per x buffer
+    uint32_t x1_bytes;       // x(g) buffer (multiple of 16)
+    uint32_t ring_bytes;     // tile ring (multiple of 16, at least one tile with its x segment)
     int *err;
 };
 
@@ -425,10 +429,10 @@ template <typename ST, typename C, int U>
 __global__ void __launch_bounds__(NZ_MAX_THREADS) k_near_groups(NearPass a) {
     extern __shared__ __align__(128) unsigned char nz_sh[];
     uint64_t *full = reinterpret_cast<uint64_t *>(nz_sh);
-    uint64_t *empty = full + NZ_STAGES;
-    ST *const Ms0 = reinterpret_cast<ST *>(nz_sh + 128);                    // tile stages
-    C *const Xs0 = reinterpret_cast<C *>(Ms0 + NZ_STAGES * a.stage_elems);  // x(g2) stages
-    C *const X1 = Xs0 + NZ_STAGES * a.xcap;                                 // x(g)
+    uint64_t *empty = full + NZ_SLOTS;
+    int *toff = reinterpret_cast<int *>(nz_sh + 16 * NZ_SLOTS);          // ring offset of each slot's tile
+    C *const X1 = reinterpret_cast<C *>(nz_sh + NZ_META);                 // x(g)
+    unsigned char *const ring = nz_sh + NZ_META + a.x1_bytes;
     const ST *data = static_cast<const ST *>(a.data);
     const C *xT = static_cast<const C *>(a.xT);
     C *part = static_cast<C *>(a.part);
@@ -444,9 +448,9 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS) k_near_groups(NearPass a) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (threadIdx.x == 0) {
-        for (int st = 0; st < NZ_STAGES; ++st) {
-            mbar_init(&full[st], 1);             // the producer's arrive (with the stage's bytes)
-            mbar_init(&empty[st], ncw);
+        for (int k = 0; k < NZ_SLOTS; ++k) {
+            mbar_init(&full[k], 1);              // the producer's arrive (with the tile's bytes)
+            mbar_init(&empty[k], ncw);
         }
         mbar_fence_init();
     }
@@ -454,26 +458,45 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS) k_near_groups(NearPass a) {
 
     if (warp == ncw) {
         // ------------------------------------------------------ producer
+        // ring accounting: `used` bytes are reserved by the `count` tiles in
+        // flight (a tile that wraps also reserves the unused end of the ring);
+        // tiles are released in order, oldest first
         if (lane == 0) {
-            int ord = 0;
+            const uint32_t R = a.ring_bytes;
+            uint32_t head = 0, used = 0;
+            uint32_t resv[NZ_SLOTS];
+            int oldest = 0, count = 0, ord = 0;
+            auto release_oldest = [&]() {
+                const int k = oldest % NZ_SLOTS;
+                mbar_wait(&empty[k], (uint32_t)((oldest / NZ_SLOTS) & 1), a.err);
+                used -= resv[k];
+                ++oldest;
+                --count;
+            };
             for (int r0 = 0; r0 < a.nrhs; r0 += PS) {
                 const C *xp = xT + (long long)(r0 / PS) * a.n * RG;
+                while (count > 0) release_oldest();   // X1 is rewritten: the previous pass must be done
                 for (int t = t0; t < t1; ++t, ++ord) {
-                    const int st = ord % NZ_STAGES, use = ord / NZ_STAGES;
-                    if (use > 0) mbar_wait(&empty[st], (uint32_t)((use - 1) & 1), a.err);
-                    if (t == t0 && ord > 0) {
-                        // X1 is rewritten: every consumer must be done with the previous pass
-                        const int pst = (ord - 1) % NZ_STAGES, puse = (ord - 1) / NZ_STAGES;
-                        mbar_wait(&empty[pst], (uint32_t)(puse & 1), a.err);
-                    }
                     const NearTile &tl = a.tiles[t];
                     const uint32_t mb = (uint32_t)(tile_elems(tl.n1, tl.n2) * (long long)sizeof(ST));
                     const uint32_t xb = (uint32_t)(3 * tl.n2 * RG * sizeof(C));
                     const uint32_t x1b = t == t0 ? (uint32_t)(3 * n1 * RG * sizeof(C)) : 0u;
-                    mbar_expect_tx(&full[st], mb + xb + x1b);
-                    bulk_g2s(Ms0 + st * a.stage_elems, data + tl.data_off, mb, &full[st]);
-                    bulk_g2s(Xs0 + st * a.xcap, xp + 3LL * tl.s2 * RG, xb, &full[st]);
-                    if (x1b) bulk_g2s(X1, xp + 3LL * s1 * RG, x1b, &full[st]);
+                    const uint32_t S = mb + xb;
+                    bool fit = head + S <= R;
+                    uint32_t res = fit ? S : (R - head) + S;
+                    while (count > 0 && (count == NZ_SLOTS || used + res > R)) release_oldest();
+                    if (count == 0) { head = 0; used = 0; fit = true; res = S; }
+                    const uint32_t st = fit ? head : 0u;
+                    const int k = ord % NZ_SLOTS;
+                    toff[k] = (int)st;
+                    mbar_expect_tx(&full[k], S + x1b);
+                    bulk_g2s(ring + st, data + tl.data_off, mb, &full[k]);
+                    bulk_g2s(ring + st + mb, xp + 3LL * tl.s2 * RG, xb, &full[k]);
+                    if (x1b) bulk_g2s(X1, xp + 3LL * s1 * RG, x1b, &full[k]);
+                    head = st + S;
+                    used += res;
+                    resv[k] = res;
+                    ++count;
                 }
             }
         }
@@ -494,12 +517,13 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS) k_near_groups(NearPass a) {
 #pragma unroll
             for (int u = 0; u < U; ++u) acc[q][u] = czero<C>();
         for (int t = t0; t < t1; ++t, ++ord) {
-            const int st = ord % NZ_STAGES, use = ord / NZ_STAGES;
-            mbar_wait(&full[st], (uint32_t)(use & 1), a.err);
+            const int kslot = ord % NZ_SLOTS;
+            mbar_wait(&full[kslot], (uint32_t)((ord / NZ_SLOTS) & 1), a.err);
             const NearTile &tl = a.tiles[t];
             const int n2 = tl.n2;
-            const uint32_t M = smem_addr(Ms0 + st * a.stage_elems);
-            const uint32_t X2 = smem_addr(Xs0 + st * a.xcap);
+            const int tof = toff[kslot];
+            const uint32_t M = smem_addr(ring + tof);
+            const uint32_t X2 = M + (uint32_t)(tile_elems(n1, n2) * (long long)sizeof(ST));
             constexpr uint32_t SB = sizeof(ST), CB = sizeof(C);
             const uint32_t mrow = SB * ld1, xrow = CB * RG;   // bytes between planes / x rows
             if (rowside) {
@@ -552,7 +576,7 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS) k_near_groups(NearPass a) {
                 }
             }
             __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[st]);
+            if (lane == 0) mbar_arrive(&empty[kslot]);
         }
         if (row_item) {
 #pragma unroll
@@ -778,7 +802,6 @@ void near_launch(scd_ctx *c, const ST *data, const C *x, int nrhs, const int *do
     a.tiles = c->d_tiles; a.grp_tile = c->d_grp_tile; a.grp_off = c->d_grp_off; a.pslot_base = c->d_pslot_base;
     a.data = data; a.xT = Res<C>::xT(c); a.n = c->n; a.part = Res<C>::part(c); a.part_len = c->part_len;
     a.skip = done; a.nrhs = nrhs;
-    a.stage_elems = c->max_tile_store;
     a.err = c->d_kerr;
     const int nq = U == 1 ? 1 : std::min(NZ_QMAX, (nrhs + U - 1) / U);
     a.nq = nq;
@@ -786,14 +809,19 @@ void near_launch(scd_ctx *c, const ST *data, const C *x, int nrhs, const int *do
     // xT rows are whole 16-byte units (bulk-copy granularity)
     a.rg_stride = nq * U;
     while ((a.rg_stride * sizeof(C)) % 16) ++a.rg_stride;
-    a.xcap = 3 * c->max_per_group * a.rg_stride;
+    a.x1_bytes = (uint32_t)(3 * c->max_per_group * a.rg_stride * sizeof(C));
+    // the ring fills what two CTAs per SM leave, and must hold the largest tile with its x
+    const size_t max_tile = (size_t)c->max_tile_store * sizeof(ST) + a.x1_bytes;
+    size_t ring = (NZ_SMEM_2CTA - NZ_META - a.x1_bytes) / 16 * 16;
+    if (ring < max_tile) ring = std::min((NZ_SMEM_MAX - NZ_META - a.x1_bytes) / 16 * 16, (max_tile + 15) / 16 * 16 * 2);
+    a.ring_bytes = (uint32_t)ring;
     {
         const int npass = (nrhs + nq * U - 1) / (nq * U);
         dim3 g((unsigned)((c->n + 255) / 256), npass);
         k_xpose<C><<<g, 256, 0, c->st>>>(x, c->n, c->n, nrhs, nq * U, a.rg_stride, Res<C>::xT(c));
         c->launches += 1;
     }
-    const size_t sh = 128 + NZ_STAGES * sizeof(ST) * (size_t)a.stage_elems + (NZ_STAGES + 1) * sizeof(C) * (size_t)a.xcap;
+    const size_t sh = NZ_META + a.x1_bytes + a.ring_bytes;
     cudaFuncSetAttribute(k_near_groups<ST, C, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
     k_near_groups<ST, C, U><<<c->ngroups, 2 * a.half + 32, sh, c->st>>>(a);
 }
