@@ -464,7 +464,7 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS) k_near_groups(NearPass a) {
         if (lane == 0) {
             const uint32_t R = a.ring_bytes;
             uint32_t head = 0, used = 0;
-            uint32_t resv[NZ_SLOTS];
+            uint32_t resv[NZ_SLOTS] = {};
             int oldest = 0, count = 0, ord = 0;
             auto release_oldest = [&]() {
                 const int k = oldest % NZ_SLOTS;

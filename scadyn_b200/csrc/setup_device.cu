@@ -506,7 +506,6 @@ __global__ void k_projectors(const double *tc, const double *vol, const int *cub
             for (int g = 0; g < 4; ++g) cfma(acc[g], w, Qs[warp][g][m]);
         }
         const double sv = sqrt(vb);
-        const long long TT = 27LL * T;
         for (int g = 0; g < 4; ++g) P[(size_t)(g * 27 + lane) * T + s] = cmk(acc[g].x / sv, acc[g].y / sv);
     }
 }
