@@ -220,7 +220,14 @@ def main():
     ap.add_argument("--slots", type=int, default=16, help="columns solved concurrently (batched GMRES slots)")
     ap.add_argument("--plain-sample", type=int, default=2, help="columns timed in the plain one-at-a-time form")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--serve", type=int, default=0,
+                    help="run a served request stream of this many requests instead (C4-shaped, scaled)")
+    ap.add_argument("--profile", default=None, choices=["near1", "near16", "mixed16"],
+                    help="only build the operator and run profile_matvec (for ncu captures)")
     args = ap.parse_args()
+    if args.serve:
+        print(json.dumps(serve_bench(args.serve)), flush=True)
+        return
     cfg = CONFIGS[args.config]
 
     rank = int(os.environ.get("RANK", "0"))
@@ -247,6 +254,15 @@ def main():
     B = args.block
     log(f"[rank {rank}] T={mesh.n_tet} grid={desc.Nx}x{desc.Ny}x{desc.Nz} near blocks={solver.nearzone_count()} "
         f"setup {setup_s:.1f}s")
+    if args.profile:
+        nrhs, prec = {"near1": (1, api.PREC_FP64), "near16": (16, api.PREC_FP64),
+                      "mixed16": (16, api.PREC_MIXED)}[args.profile]
+        for _ in range(3):
+            t = solver.profile_matvec(1, nrhs, prec)
+            log(f"profile {args.profile}: " + ", ".join(f"{k} {t[k]:.4f}" for k in ("nearzone_ms", "fft_ms",
+                                                                                   "gather_ms", "matvec_ms")))
+        solver.close()
+        return
 
     def cols_for(step):
         c0 = ((rank * (args.warmup + args.steps) + step) * B) % ncol_tot
@@ -383,6 +399,16 @@ def main():
     # four merged convolutions, operator reads shared by the batch)
     roof["matvec"] = matvec_roofline(solver, desc, mesh.n_tet, Bref, peak, prof["matvec_ms"], profb["matvec_ms"], S)
 
+    serving = None
+    if rank == 0 and world == 1:
+        try:
+            sv = serve_bench(8)
+            serving = {k: sv[k] for k in ("value", "unit", "p50_ms", "p99_ms", "completed", "columns",
+                                          "peak_running", "busy_s")}
+            serving["workload"] = sv["config"]["workload"]
+        except Exception as e:
+            serving = {"error": str(e)[:200]}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -413,6 +439,7 @@ def main():
             "iters_mean": float(np.mean(iters)),
             "forms": forms,
             "batched_matvec": batched,
+            "serving": serving,
             "e2e": {"value": round(e2e_val, 4), "unit": "columns/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "roofline": roof,
@@ -426,6 +453,63 @@ def main():
     solver.close()
     if dist:
         dist.destroy_process_group()
+
+
+def serve_bench(nreq):
+    """A served stream shaped like C4, scaled to minutes: Poisson arrivals
+    (seed 3000) of T-matrix requests over seeded meshes -- spheres, ellipsoids
+    with axis ratios U(0.5,1), core-mantle spheres (core eps 3.5+0.1i, mantle
+    1.8+0.01i) -- of 5k-60k tets, ka ~ U(1,6), Nmax = clip(round(ka)+2, 4, 8),
+    mixed precision, under a 150 GB HBM budget.  Reports the served
+    columns/s (columns of the completed requests over the time any request
+    was running) and the request latency p50/p99 (submit -> T ready)."""
+    from scadyn_b200 import geometry, meshgen
+    from scadyn_b200.server import Server
+    from scadyn_b200 import api
+    rng = np.random.default_rng(3000)
+    reqs = []
+    for r in range(nreq):
+        kind = rng.choice(["sphere", "ellipsoid", "core_mantle"])
+        nm = float(rng.uniform(6.0, 13.0))
+        if kind == "sphere":
+            eps = complex(rng.uniform(1.5, 3.0), rng.uniform(0.01, 0.1))
+            mesh = meshgen.sphere(nm, seed=4000 + r, eps=eps)
+        elif kind == "ellipsoid":
+            ax = (1.0, float(rng.uniform(0.5, 1.0)), float(rng.uniform(0.5, 1.0)))
+            eps = complex(rng.uniform(1.5, 3.0), rng.uniform(0.01, 0.1))
+            mesh = meshgen.ellipsoid(nm, ax, seed=4000 + r, eps=eps)
+        else:
+            mesh = meshgen.core_mantle(nm, seed=4000 + r)
+        ka = float(rng.uniform(1.0, 6.0))
+        nmax = int(np.clip(round(ka) + 2, 4, 8))
+        N = max(16, int(round(mesh.n_tet ** (1 / 3) / 2)) * 2)
+        gs = geometry.cell_size_for_grid(mesh.coord, mesh.etopol, N)
+        reqs.append((mesh, ka / mesh.a, gs, nmax, kind))
+    gaps = rng.exponential(0.5, size=len(reqs))
+    srv = Server(hbm_budget=150e9, max_running=4)
+    ids, t0 = [], time.time()
+    for (mesh, k, gs, nmax, kind), gap in zip(reqs, gaps):
+        time.sleep(float(gap))
+        ids.append(srv.submit(mesh, k, gs, nmax, tol=1e-6, m=20, cycles=60, block=16,
+                              precision=api.PREC_MIXED, inner_tol=1e-4, max_outer=10))
+    for i in ids:
+        srv.wait(i, 3600)
+    wall = time.time() - t0
+    st = srv.stats()
+    lat = [srv.poll(i)[2] for i in ids]
+    srv.close()
+    line = {"metric": "served T-matrix columns/s and request latency p50/p99 (mixed precision, batched)",
+            "value": round(st["columns"] / st["busy_s"], 4), "unit": "columns/s", "n_gpus": 1,
+            "higher_is_better": True, "dtype": "c64 inner / f64 outer", "data": "synthetic (seeded meshes)",
+            "config": {"workload": "C4-shaped served stream, scaled: %d requests, 5k-60k tets, ka U(1,6), "
+                                   "Nmax 4-8, Poisson arrivals mean gap 0.5 s, HBM budget 150 GB" % len(reqs),
+                       "tets": [int(m.n_tet) for m, *_ in reqs], "Nmax": [int(r[3]) for r in reqs],
+                       "bodies": [r[4] for r in reqs]},
+            "p50_ms": round(st["p50_ms"], 1), "p99_ms": round(st["p99_ms"], 1),
+            "request_latency_ms": [round(v, 1) for v in lat],
+            "completed": st["completed"], "columns": st["columns"], "peak_running": st["peak_running"],
+            "peak_bytes": st["peak_bytes"], "busy_s": round(st["busy_s"], 2), "wall_s": round(wall, 2)}
+    return line
 
 
 def matvec_roofline(solver, desc, T, Bref, peak, ms1, msb, nb):
