@@ -209,6 +209,14 @@ SCD_API int scd_column_latency(scd_ctx *ctx, int32_t ncol, double *ms);
  * the device tile storage. */
 SCD_API int64_t scd_nearzone_bytes(scd_ctx *ctx);
 
+/* Failure detection self-test (no counterpart in the reference): runs the
+ * library's bounded device waits -- the grid barrier of the cooperative
+ * solver kernels and the mbarrier wait of the near-zone pipeline -- against
+ * conditions that nothing satisfies, with short limits.  Returns SCD_TIMEOUT
+ * when both waits gave up and reported it (the behaviour a stuck launch gets),
+ * SCD_CUDA_ERROR otherwise.  The device stays usable. */
+SCD_API int scd_selftest_waits(int32_t device);
+
 #ifdef __cplusplus
 }
 #endif

@@ -26,6 +26,7 @@ LIB_PATH = os.path.join(_HERE, "libscadyn_gpu.so")
 SCD_OK, SCD_NOT_CONVERGED, SCD_NAN, SCD_OOM, SCD_BAD_ARG, SCD_TIMEOUT, SCD_CUDA_ERROR, SCD_NOT_READY, SCD_NO_DEVICE = range(9)
 STORE_C64, STORE_C128 = 32, 64
 PREC_FP64, PREC_MIXED = 0, 1
+SCD_M_MAX = 63
 
 _NAMES = {0: "SCD_OK", 1: "SCD_NOT_CONVERGED", 2: "SCD_NAN", 3: "SCD_OOM", 4: "SCD_BAD_ARG",
           5: "SCD_TIMEOUT", 6: "SCD_CUDA_ERROR", 7: "SCD_NOT_READY", 8: "SCD_NO_DEVICE"}
@@ -37,7 +38,7 @@ EXPORTS = [
     "scd_build_projectors", "scd_build_nearzone", "scd_get_projectors", "scd_nearzone_count",
     "scd_get_nearzone", "scd_matvec", "scd_gmres", "scd_solve_columns", "scd_vswf_rhs",
     "scd_get_timing", "scd_compute_T_matrix", "scd_profile_matvec", "scd_nearzone_bytes",
-    "scd_column_latency", "scd_T_assemble_noalloc",
+    "scd_column_latency", "scd_T_assemble_noalloc", "scd_selftest_waits",
 ]
 
 
@@ -102,6 +103,7 @@ def load_library(path: str = LIB_PATH):
         "scd_nearzone_bytes": ([vp], C.c_int64),
         "scd_column_latency": ([vp, i32, vp], C.c_int),
         "scd_T_assemble_noalloc": ([vp, i64, i32, vp, i32, vp, vp], C.c_int),
+        "scd_selftest_waits": ([i32], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
