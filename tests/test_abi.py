@@ -50,3 +50,33 @@ def test_no_device_is_reported_not_crashed():
     with pytest.raises(api.ScadynError) as e:
         api.Solver(8, 8, 8, 1.0, (0, 0, 0), 10)
     assert e.value.code == api.SCD_NO_DEVICE
+
+
+def test_c_consumer_compiles_links_and_runs(tmp_path):
+    """The headers are plain C: a C program includes both, links the library
+    and calls through it (without a GPU, scd_create reports SCD_NO_DEVICE)."""
+    import subprocess
+    import torch
+    src = tmp_path / "consumer.c"
+    src.write_text(r'''
+#include <stdio.h>
+#include "scadyn_gpu.h"
+#include "scadyn_server.h"
+int main(void) {
+    scd_grid_desc d = {8, 8, 8, 1.0, {0, 0, 0}, 10, 0, 2, 1, 0};
+    scd_ctx *c = 0;
+    int rc = scd_create(&c, &d);
+    printf("%d\n", rc);
+    if (c) scd_destroy(c);
+    return 0;
+}
+''')
+    lib = build.build()
+    exe = tmp_path / "consumer"
+    subprocess.check_call(["gcc", "-std=c99", "-Wall", "-Werror", str(src), "-I", os.path.join(ROOT, "include"),
+                           lib, "-Wl,-rpath," + os.path.dirname(lib), "-o", str(exe)])
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.strip()
+    if not torch.cuda.is_available():
+        assert int(out) == api.SCD_NO_DEVICE
+    else:
+        assert int(out) == api.SCD_OK
