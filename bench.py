@@ -8,7 +8,7 @@ per-tet eps with Re ~ U(2,3), Im ~ U(0.01,0.1)), zero-padded pFFT grid 128^3
 `--config c1` runs the 43k-tet sphere (ka = 2, Nmax = 6, grid 64^3).
 
 A step solves `--block` consecutive T-matrix columns (cycling through the
-448) in the mixed-precision form: complex64 inner GMRES(20) to 1e-4 and FP64
+448) in the mixed-precision form: complex64 inner GMRES(30) to 3e-4 and FP64
 iterative refinement on the true residual to 1e-6, `--slots` columns in
 flight.  `value` is columns/s over K timed steps with the operator and the
 incident columns resident in HBM (device time from CUDA events on the
@@ -41,12 +41,18 @@ CONFIGS = {
                         "padded pFFT grid 64^3, GMRES(50) tol 1e-6",
                body="sphere", n_major=12.0, axes=(1.0, 1.0, 1.0), ka=2.0, eps=2.25 + 0.01j,
                Nmax=6, N=32, tol=1e-6, m=50, cycles=4, seed=1001, eps_seed=2001,
-               inner_m=20, inner_tol=1e-4, max_outer=10),
+               inner_m=30, inner_tol=3e-4, max_outer=10),
     "c2": dict(workload="C2: ellipsoid 1:0.8:0.6, ka=8 (~150k tets), per-tet eps Re U(2,3) Im U(0.01,0.1), "
                         "Nmax=14 (448 columns), padded pFFT grid 128^3, GMRES(50) tol 1e-6",
                body="ellipsoid", n_major=23.2, axes=(1.0, 0.8, 0.6), ka=8.0, eps=None,
                Nmax=14, N=64, tol=1e-6, m=50, cycles=12, seed=1002, eps_seed=2002,
-               inner_m=20, inner_tol=1e-4, max_outer=10),
+               inner_m=30, inner_tol=3e-4, max_outer=10),
+    # C2-shaped case at a third of the size (for ncu captures: ~1 GB of near-zone tiles)
+    "c2s": dict(workload="C2-shaped ellipsoid 1:0.8:0.6 at n_major 16 (~49k tets), ka=8, per-tet eps Re U(2,3) "
+                         "Im U(0.01,0.1), Nmax=14, padded pFFT grid 88^3",
+                body="ellipsoid", n_major=16.0, axes=(1.0, 0.8, 0.6), ka=8.0, eps=None,
+                Nmax=14, N=44, tol=1e-6, m=50, cycles=12, seed=1002, eps_seed=2002,
+                inner_m=30, inner_tol=3e-4, max_outer=10),
 }
 
 L2_BYTES = 126 * 1024 * 1024

@@ -220,6 +220,7 @@ __device__ void givens_step(const TickArgs<C> &a, const int *smode, const int *s
 template <typename C>
 __device__ void cycle_end(const TickArgs<C> &a, const Chunks &ch, int nch, const int *smode, cd (*ysm)[SCD_M_MAX + 1]) {
     const long long n = a.n;
+    constexpr int TUC = sizeof(C) == 8 ? 2 * TU : TU;
     const int lane = ch.lane;
     const int nitems = a.ns * nch;
     {
@@ -236,21 +237,21 @@ __device__ void cycle_end(const TickArgs<C> &a, const Chunks &ch, int nch, const
             const long long qa = c * ch.L, qb = min(n, qa + ch.L);
             const C *Vs = a.V + (size_t)s * (a.m + 1) * n;
             C *xs = a.x + (size_t)s * n;
-            for (long long q = qa + lane; q < qb; q += 32 * TU) {
-                cd acc[TU];
+            for (long long q = qa + lane; q < qb; q += 32 * TUC) {
+                cd acc[TUC];
 #pragma unroll
-                for (int e = 0; e < TU; ++e) acc[e] = cmk(0, 0);
+                for (int e = 0; e < TUC; ++e) acc[e] = cmk(0, 0);
                 for (int cc = 0; cc < kd; ++cc) {
                     const cd yc = yw[cc];
                     const C *vc = Vs + (size_t)cc * n;
 #pragma unroll
-                    for (int e = 0; e < TU; ++e) {
+                    for (int e = 0; e < TUC; ++e) {
                         const long long qq = q + 32 * e;
                         if (qq < qb) cfma(acc[e], to_cd(vc[qq]), yc);
                     }
                 }
 #pragma unroll
-                for (int e = 0; e < TU; ++e) {
+                for (int e = 0; e < TUC; ++e) {
                     const long long qq = q + 32 * e;
                     if (qq < qb) store_c(xs[qq], cadd(to_cd(xs[qq]), acc[e]));
                 }
@@ -275,13 +276,14 @@ __device__ void cycle_end(const TickArgs<C> &a, const Chunks &ch, int nch, const
 // One tick: cycle starts (r = rhs - A x, V0 = r/||r||) and Arnoldi steps
 // (MGS, normalisation, Givens) for every active slot; cycle ends update x.
 template <typename C>
-__global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
+__global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
     __shared__ double tot[NSMAX][4];
     __shared__ int smode[NSMAX], sstep[NSMAX], szero[NSMAX], swpos[NSMAX], sact[NSMAX], sro[NSMAX];
     __shared__ double snormav[NSMAX], shn[NSMAX];
     __shared__ cd sh_h[NSMAX];
     __shared__ cd ysm[BW][SCD_M_MAX + 1];    // per warp: y of the slot being updated
     const long long n = a.n;
+    constexpr int TUC = sizeof(C) == 8 ? 2 * TU : TU;   // complex64: twice the elements in flight
     const int ldh = a.m + 1;
     const Chunks ch(n, NCH);
     const int lane = ch.lane;
@@ -306,10 +308,10 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
         if (md == SLOT_START) {
             const C *bs = a.rhs + (size_t)s * n;
             const bool zx = szero[s] != 0;
-            for (long long q = qa + lane; q < qb; q += 32 * TU) {
-                cd b[TU], w[TU];
+            for (long long q = qa + lane; q < qb; q += 32 * TUC) {
+                cd b[TUC], w[TUC];
 #pragma unroll
-                for (int u = 0; u < TU; ++u) {
+                for (int u = 0; u < TUC; ++u) {
                     const long long qq = q + 32 * u;
                     b[u] = w[u] = cmk(0, 0);
                     if (qq < qb) {
@@ -318,7 +320,7 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
                     }
                 }
 #pragma unroll
-                for (int u = 0; u < TU; ++u) {
+                for (int u = 0; u < TUC; ++u) {
                     const long long qq = q + 32 * u;
                     if (qq >= qb) break;
                     const cd r = zx ? b[u] : csub(b[u], w[u]);
@@ -328,16 +330,16 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
                 }
             }
         } else {
-            for (long long q = qa + lane; q < qb; q += 32 * TU) {
-                cd w[TU], z[TU];
+            for (long long q = qa + lane; q < qb; q += 32 * TUC) {
+                cd w[TUC], z[TUC];
 #pragma unroll
-                for (int u = 0; u < TU; ++u) {
+                for (int u = 0; u < TUC; ++u) {
                     const long long qq = q + 32 * u;
                     w[u] = z[u] = cmk(0, 0);
                     if (qq < qb) { w[u] = to_cd(ws[qq]); z[u] = to_cd(V0[qq]); }
                 }
 #pragma unroll
-                for (int u = 0; u < TU; ++u) {
+                for (int u = 0; u < TUC; ++u) {
                     if (q + 32 * u >= qb) break;
                     v[0] += cabs2(w[u]);
                     cdot_acc(v[1], v[2], z[u], w[u]);
@@ -365,15 +367,15 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
         const double beta = sqrt(tot[s][0]);
         const long long qa = c * ch.L, qb = min(n, qa + ch.L);
         C *V0 = a.V + (size_t)s * (a.m + 1) * n;
-        for (long long q = qa + lane; q < qb; q += 32 * TU) {
-            cd r[TU];
+        for (long long q = qa + lane; q < qb; q += 32 * TUC) {
+            cd r[TUC];
 #pragma unroll
-            for (int u = 0; u < TU; ++u) {
+            for (int u = 0; u < TUC; ++u) {
                 const long long qq = q + 32 * u;
                 r[u] = qq < qb ? to_cd(V0[qq]) : cmk(0, 0);
             }
 #pragma unroll
-            for (int u = 0; u < TU; ++u) {
+            for (int u = 0; u < TUC; ++u) {
                 const long long qq = q + 32 * u;
                 if (qq < qb) store_c(V0[qq], cmk(r[u].x / beta, r[u].y / beta));
             }
@@ -411,26 +413,27 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
             const C *vk = Vs + (size_t)(k - 1) * n;
             const C *vn = (k < i) ? Vs + (size_t)k * n : nullptr;
             double u[2] = {0, 0};
-            for (long long q = qa + lane; q < qb; q += 32 * TU) {
-                cd w[TU], p[TU], z[TU];
+            for (long long q = qa + lane; q < qb; q += 32 * TUC) {
+                C w[TUC], p[TUC], z[TUC];      // raw elements, widened at use
 #pragma unroll
-                for (int e = 0; e < TU; ++e) {
+                for (int e = 0; e < TUC; ++e) {
                     const long long qq = q + 32 * e;
-                    w[e] = p[e] = z[e] = cmk(0, 0);
+                    w[e] = p[e] = z[e] = C{};
                     if (qq < qb) {
-                        w[e] = to_cd(ws[qq]);
-                        p[e] = to_cd(vk[qq]);
-                        if (vn) z[e] = to_cd(vn[qq]);
+                        w[e] = ws[qq];
+                        p[e] = vk[qq];
+                        if (vn) z[e] = vn[qq];
                     }
                 }
 #pragma unroll
-                for (int e = 0; e < TU; ++e) {
+                for (int e = 0; e < TUC; ++e) {
                     const long long qq = q + 32 * e;
                     if (qq >= qb) break;
-                    csub_mul(w[e], h, p[e]);
-                    store_c(ws[qq], w[e]);
-                    const cd wr = rounded<C>(w[e]);
-                    if (vn) cdot_acc(u[0], u[1], z[e], wr);
+                    cd wv = to_cd(w[e]);
+                    csub_mul(wv, h, to_cd(p[e]));
+                    store_c(ws[qq], wv);
+                    const cd wr = rounded<C>(wv);
+                    if (vn) cdot_acc(u[0], u[1], to_cd(z[e]), wr);
                     else u[0] += cabs2(wr);
                 }
             }
@@ -464,16 +467,16 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
             const C *vj = a.V + (size_t)s * (a.m + 1) * n + (size_t)(j - 1) * n;
             const C *ws = a.w + (size_t)swpos[s] * n;
             double u[2] = {0, 0};
-            for (long long q = qa + lane; q < qb; q += 32 * TU) {
-                cd z[TU], w[TU];
+            for (long long q = qa + lane; q < qb; q += 32 * TUC) {
+                cd z[TUC], w[TUC];
 #pragma unroll
-                for (int e = 0; e < TU; ++e) {
+                for (int e = 0; e < TUC; ++e) {
                     const long long qq = q + 32 * e;
                     z[e] = w[e] = cmk(0, 0);
                     if (qq < qb) { z[e] = to_cd(vj[qq]); w[e] = to_cd(ws[qq]); }
                 }
 #pragma unroll
-                for (int e = 0; e < TU; ++e) {
+                for (int e = 0; e < TUC; ++e) {
                     if (q + 32 * e >= qb) break;
                     cdot_acc(u[0], u[1], z[e], w[e]);
                 }
@@ -499,16 +502,16 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
             const long long qa = c * ch.L, qb = min(n, qa + ch.L);
             const C *vj = a.V + (size_t)s * (a.m + 1) * n + (size_t)(j - 1) * n;
             C *ws = a.w + (size_t)swpos[s] * n;
-            for (long long q = qa + lane; q < qb; q += 32 * TU) {
-                cd w[TU], p[TU];
+            for (long long q = qa + lane; q < qb; q += 32 * TUC) {
+                cd w[TUC], p[TUC];
 #pragma unroll
-                for (int e = 0; e < TU; ++e) {
+                for (int e = 0; e < TUC; ++e) {
                     const long long qq = q + 32 * e;
                     w[e] = p[e] = cmk(0, 0);
                     if (qq < qb) { w[e] = to_cd(ws[qq]); p[e] = to_cd(vj[qq]); }
                 }
 #pragma unroll
-                for (int e = 0; e < TU; ++e) {
+                for (int e = 0; e < TUC; ++e) {
                     const long long qq = q + 32 * e;
                     if (qq >= qb) break;
                     csub_mul(w[e], hr, p[e]);
@@ -525,15 +528,15 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
             const long long qa = c * ch.L, qb = min(n, qa + ch.L);
             const C *ws = a.w + (size_t)swpos[s] * n;
             double u[1] = {0};
-            for (long long q = qa + lane; q < qb; q += 32 * TU) {
-                cd w[TU];
+            for (long long q = qa + lane; q < qb; q += 32 * TUC) {
+                cd w[TUC];
 #pragma unroll
-                for (int e = 0; e < TU; ++e) {
+                for (int e = 0; e < TUC; ++e) {
                     const long long qq = q + 32 * e;
                     w[e] = qq < qb ? to_cd(ws[qq]) : cmk(0, 0);
                 }
 #pragma unroll
-                for (int e = 0; e < TU; ++e) {
+                for (int e = 0; e < TUC; ++e) {
                     if (q + 32 * e >= qb) break;
                     u[0] += cabs2(w[e]);
                 }
@@ -555,15 +558,15 @@ __global__ void __launch_bounds__(BT) k_tick(TickArgs<C> a) {
         const long long qa = c * ch.L, qb = min(n, qa + ch.L);
         const C *ws = a.w + (size_t)swpos[s] * n;
         C *vi = a.V + (size_t)s * (a.m + 1) * n + (size_t)i * n;
-        for (long long q = qa + lane; q < qb; q += 32 * TU) {
-            cd w[TU];
+        for (long long q = qa + lane; q < qb; q += 32 * TUC) {
+            cd w[TUC];
 #pragma unroll
-            for (int e = 0; e < TU; ++e) {
+            for (int e = 0; e < TUC; ++e) {
                 const long long qq = q + 32 * e;
                 w[e] = qq < qb ? to_cd(ws[qq]) : cmk(0, 0);
             }
 #pragma unroll
-            for (int e = 0; e < TU; ++e) {
+            for (int e = 0; e < TUC; ++e) {
                 const long long qq = q + 32 * e;
                 if (qq < qb) store_c(vi[qq], (hn != 0.0) ? cmk(w[e].x / hn, w[e].y / hn) : w[e]);
             }
