@@ -13,6 +13,7 @@
 #include <cstdint>
 
 #include "ctx.h"
+#include "fft_reg.cuh"
 
 namespace {
 
@@ -108,9 +109,8 @@ __device__ __forceinline__ void radix4(C &v0, C &v1, C &v2, C &v3) {
     v3 = csub(a1, ia3);
 }
 
-// in-line padding: one spare slot per 16 complex values spreads the
-// strided Stockham writes over the shared-memory banks
-__device__ __forceinline__ int pidx(int i) { return i + (i >> 4); }
+// in-line padding pidx(i) = i + (i >> 4) (fft_reg.cuh): one spare slot per
+// 16 complex values spreads the strided Stockham writes over the banks
 
 template <bool INV, typename C>
 __device__ __forceinline__ C twid(const C *tw, int i) {
@@ -163,12 +163,25 @@ __device__ __forceinline__ void fft_line(C *s, const C *tw, int t) {
     }
 }
 
-template <int P> struct FftCfg {
-    static constexpr int TPL = P / 4;                        // threads per line
-    static constexpr int LPB = (256 / TPL) > 0 ? 256 / TPL : 1;   // lines per CTA
+// Line FFT of the passes: register-resident 8-thread transform for P = 64
+// and 128 (fft_reg.cuh), shared-memory radix-4 Stockham for other lengths.
+template <int P, typename Cx> struct FftCfg {
+    static constexpr bool REG = P == 64 || P == 128;
+    static constexpr int TPL = REG ? 8 : P / 4;              // threads per line
+    static constexpr int LPB = REG ? (sizeof(Cx) == 16 ? 16 : 32) : ((256 / TPL) > 0 ? 256 / TPL : 1);   // lines per CTA
     static constexpr int THREADS = TPL * LPB;
     static constexpr int LS = P + (P >> 4) + 1;              // padded line stride (bank spread)
 };
+
+template <int P, bool INV, typename Cx>
+__device__ __forceinline__ void fft_line_any(Cx *s, const Cx *tw, int t) {
+    if constexpr (FftCfg<P, Cx>::REG) {
+        fft_line_reg<P, INV, Cx>(s, tw, t);
+        __syncthreads();   // the passes' next loops read every line of the CTA
+    } else {
+        fft_line<P, INV, Cx>(s, tw, t);
+    }
+}
 
 struct GridDims {
     int Nx, Ny, Nz, Px, Py, Pz, Hx, Hy, Hz, ncx, ncy, ncz, ncubes;
@@ -204,10 +217,10 @@ __device__ __forceinline__ C node_value(const C *__restrict__ bp, const GridDims
 // X forward: lines (y < Ny, z < Nz) of grid (g, r); node assembly on load,
 // zero padding x >= Nx.  W[(rg)][(z*Py + y)*Px + x]
 template <int P, typename Cx>
-__global__ void __launch_bounds__(FftCfg<P>::THREADS)
+__global__ void __launch_bounds__(FftCfg<P, Cx>::THREADS)
 k_fft_x_fwd(const Cx *__restrict__ bpart, Cx *__restrict__ W, const Cx *__restrict__ twg, GridDims G, const int *done) {
     if (done && done[blockIdx.y >> 2]) return;
-    using Cf = FftCfg<P>;
+    using Cf = FftCfg<P, Cx>;
     __shared__ Cx sh[Cf::LPB * Cf::LS];
     __shared__ Cx tw[P];
     const int rg = blockIdx.y;                 // r*4 + g
@@ -227,7 +240,7 @@ k_fft_x_fwd(const Cx *__restrict__ bpart, Cx *__restrict__ W, const Cx *__restri
     }
     __syncthreads();
     const int l = threadIdx.x / Cf::TPL, t = threadIdx.x - l * Cf::TPL;
-    fft_line<P, false, Cx>(sh + l * Cf::LS, tw, t);
+    fft_line_any<P, false, Cx>(sh + l * Cf::LS, tw, t);
     Cx *Wr = W + (long long)rg * G.Px * G.Py * G.Nz;
     for (int e = threadIdx.x; e < Cf::LPB * P; e += blockDim.x) {
         const int ll = e / P, x = e - ll * P, line = line0 + ll;
@@ -241,10 +254,10 @@ k_fft_x_fwd(const Cx *__restrict__ bpart, Cx *__restrict__ W, const Cx *__restri
 // Y pass: lines (x < Px, z < Nz); forward reads y < Ny and writes y < Py,
 // inverse reads y < Py and writes y < Ny.  A CTA takes LPB consecutive x.
 template <int P, bool INV, typename Cx>
-__global__ void __launch_bounds__(FftCfg<P>::THREADS)
+__global__ void __launch_bounds__(FftCfg<P, Cx>::THREADS)
 k_fft_y(Cx *__restrict__ W, const Cx *__restrict__ twg, GridDims G, const int *done) {
     if (done && done[blockIdx.y >> 2]) return;
-    using Cf = FftCfg<P>;
+    using Cf = FftCfg<P, Cx>;
     __shared__ Cx sh[Cf::LPB * Cf::LS];
     __shared__ Cx tw[P];
     const int rg = blockIdx.y;
@@ -262,7 +275,7 @@ k_fft_y(Cx *__restrict__ W, const Cx *__restrict__ twg, GridDims G, const int *d
     }
     __syncthreads();
     const int l = threadIdx.x / Cf::TPL, t = threadIdx.x - l * Cf::TPL;
-    fft_line<P, INV, Cx>(sh + l * Cf::LS, tw, t);
+    fft_line_any<P, INV, Cx>(sh + l * Cf::LS, tw, t);
     for (int e = threadIdx.x; e < Cf::LPB * P; e += blockDim.x) {
         const int y = e / Cf::LPB, ll = e - y * Cf::LPB, x = x0 + ll;
         if (y < nout && x < G.Px) Wr[(long long)y * G.Px + x] = sh[ll * Cf::LS + pidx(y)];
@@ -272,10 +285,10 @@ k_fft_y(Cx *__restrict__ W, const Cx *__restrict__ twg, GridDims G, const int *d
 // Z pass: lines (x < Px, y < Py), forward FFT of z < Nz (zero padded), times
 // the Green octant Fo (folded by evenness), inverse FFT, keep z < Nz.
 template <int P, typename Cx>
-__global__ void __launch_bounds__(FftCfg<P>::THREADS)
+__global__ void __launch_bounds__(FftCfg<P, Cx>::THREADS)
 k_fft_z(Cx *__restrict__ W, const Cx *__restrict__ Fo, const Cx *__restrict__ twg, GridDims G, const int *done) {
     if (done && done[blockIdx.y >> 2]) return;
-    using Cf = FftCfg<P>;
+    using Cf = FftCfg<P, Cx>;
     __shared__ Cx sh[Cf::LPB * Cf::LS];
     __shared__ Cx tw[P];
     const int rg = blockIdx.y;
@@ -292,7 +305,7 @@ k_fft_z(Cx *__restrict__ W, const Cx *__restrict__ Fo, const Cx *__restrict__ tw
     }
     __syncthreads();
     const int l = threadIdx.x / Cf::TPL, t = threadIdx.x - l * Cf::TPL;
-    fft_line<P, false, Cx>(sh + l * Cf::LS, tw, t);
+    fft_line_any<P, false, Cx>(sh + l * Cf::LS, tw, t);
     const int fy = fold(y, G.Py);
     // consecutive threads take consecutive lines (x), so the octant reads of
     // one z plane are contiguous
@@ -304,7 +317,7 @@ k_fft_z(Cx *__restrict__ W, const Cx *__restrict__ Fo, const Cx *__restrict__ tw
         }
     }
     __syncthreads();
-    fft_line<P, true, Cx>(sh + l * Cf::LS, tw, t);
+    fft_line_any<P, true, Cx>(sh + l * Cf::LS, tw, t);
     for (int e = threadIdx.x; e < Cf::LPB * P; e += blockDim.x) {
         const int z = e / Cf::LPB, ll = e - z * Cf::LPB, x = x0 + ll;
         if (z < G.Nz && x < G.Px) Wr[(long long)z * plane + x] = sh[ll * Cf::LS + pidx(z)];
@@ -314,10 +327,10 @@ k_fft_z(Cx *__restrict__ W, const Cx *__restrict__ Fo, const Cx *__restrict__ tw
 // X inverse: lines (y < Ny, z < Nz), keep x < Nx, write the result grid
 // R[(rg)][(z*Ny + y)*Nx + x]
 template <int P, typename Cx>
-__global__ void __launch_bounds__(FftCfg<P>::THREADS)
+__global__ void __launch_bounds__(FftCfg<P, Cx>::THREADS)
 k_fft_x_inv(const Cx *__restrict__ W, Cx *__restrict__ R, const Cx *__restrict__ twg, GridDims G, const int *done) {
     if (done && done[blockIdx.y >> 2]) return;
-    using Cf = FftCfg<P>;
+    using Cf = FftCfg<P, Cx>;
     __shared__ Cx sh[Cf::LPB * Cf::LS];
     __shared__ Cx tw[P];
     const int rg = blockIdx.y;
@@ -336,7 +349,7 @@ k_fft_x_inv(const Cx *__restrict__ W, Cx *__restrict__ R, const Cx *__restrict__
     }
     __syncthreads();
     const int l = threadIdx.x / Cf::TPL, t = threadIdx.x - l * Cf::TPL;
-    fft_line<P, true, Cx>(sh + l * Cf::LS, tw, t);
+    fft_line_any<P, true, Cx>(sh + l * Cf::LS, tw, t);
     Cx *Rr = R + (long long)rg * G.Nx * G.Ny * G.Nz;
     for (int e = threadIdx.x; e < Cf::LPB * P; e += blockDim.x) {
         const int ll = e / P, x = e - ll * P, line = line0 + ll;
@@ -726,25 +739,25 @@ template <> struct Res<cf> {
 
 template <int P, typename C>
 void fft_x_fwd_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const C *tw) {
-    using Cf = FftCfg<P>;
+    using Cf = FftCfg<P, C>;
     dim3 grid((G.Ny * G.Nz + Cf::LPB - 1) / Cf::LPB, nrg);
     k_fft_x_fwd<P, C><<<grid, Cf::THREADS, 0, c->st>>>(Res<C>::bpart(c), Res<C>::W(c), tw, G, done);
 }
 template <int P, bool INV, typename C>
 void fft_y_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const C *tw) {
-    using Cf = FftCfg<P>;
+    using Cf = FftCfg<P, C>;
     dim3 grid(((G.Px + Cf::LPB - 1) / Cf::LPB) * G.Nz, nrg);
     k_fft_y<P, INV, C><<<grid, Cf::THREADS, 0, c->st>>>(Res<C>::W(c), tw, G, done);
 }
 template <int P, typename C>
 void fft_z_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const C *tw) {
-    using Cf = FftCfg<P>;
+    using Cf = FftCfg<P, C>;
     dim3 grid(((G.Px + Cf::LPB - 1) / Cf::LPB) * G.Py, nrg);
     k_fft_z<P, C><<<grid, Cf::THREADS, 0, c->st>>>(Res<C>::W(c), Res<C>::Fo(c), tw, G, done);
 }
 template <int P, typename C>
 void fft_x_inv_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const C *tw) {
-    using Cf = FftCfg<P>;
+    using Cf = FftCfg<P, C>;
     dim3 grid((G.Ny * G.Nz + Cf::LPB - 1) / Cf::LPB, nrg);
     k_fft_x_inv<P, C><<<grid, Cf::THREADS, 0, c->st>>>(Res<C>::W(c), Res<C>::R(c), tw, G, done);
 }
