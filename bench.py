@@ -47,6 +47,12 @@ CONFIGS = {
                body="ellipsoid", n_major=23.2, axes=(1.0, 0.8, 0.6), ka=8.0, eps=None,
                Nmax=14, N=64, tol=1e-6, m=50, cycles=12, seed=1002, eps_seed=2002,
                inner_m=30, inner_tol=3e-4, max_outer=10),
+    "c5": dict(workload="C5: core-mantle ellipsoid 1:0.7:0.5, core at 60% (eps 3.5+0.1i), mantle eps 1.8+0.01i, "
+                        "ka=20, ~1.2M tets, Nmax=25 (1350 columns), padded pFFT grid 256^3",
+               body="core_mantle", n_major=51.6, axes=(1.0, 0.7, 0.5), ka=20.0, eps=1.8 + 0.01j,
+               core_scale=0.6, core_eps=3.5 + 0.1j,
+               Nmax=25, N=128, tol=1e-6, m=50, cycles=12, seed=1005, eps_seed=2005,
+               inner_m=30, inner_tol=3e-4, max_outer=10),
     # C2-shaped case at a third of the size (for ncu captures: ~1 GB of near-zone tiles)
     "c2s": dict(workload="C2-shaped ellipsoid 1:0.8:0.6 at n_major 16 (~49k tets), ka=8, per-tet eps Re U(2,3) "
                          "Im U(0.01,0.1), Nmax=14, padded pFFT grid 88^3",
@@ -70,6 +76,9 @@ def make_mesh(cfg):
         rng_eps = np.random.default_rng(cfg["eps_seed"])
         mesh = meshgen.lattice_body(cfg["n_major"], cfg["axes"], eps=2.5, **kw)
         mesh.param = sampler(rng_eps, mesh.n_tet)
+    elif cfg.get("core_scale"):
+        mesh = meshgen.core_mantle(cfg["n_major"], cfg["axes"], core_scale=cfg["core_scale"],
+                                   core_eps=cfg["core_eps"], mantle_eps=cfg["eps"], **kw)
     else:
         mesh = meshgen.lattice_body(cfg["n_major"], cfg["axes"], eps=cfg["eps"], **kw)
     return mesh
@@ -228,11 +237,17 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serve", type=int, default=0,
                     help="run a served request stream of this many requests instead (C4-shaped, scaled)")
-    ap.add_argument("--profile", default=None, choices=["near1", "near16", "mixed16"],
+    ap.add_argument("--sweep", type=int, default=0,
+                    help="run a C3-shaped wavelength sweep with this many wavelengths instead")
+    ap.add_argument("--sweep-nmax", type=int, default=14, help="largest Nmax of the sweep (C3: 14)")
+    ap.add_argument("--profile", default=None, choices=["near1", "near16", "mixed16", "solve16"],
                     help="only build the operator and run profile_matvec (for ncu captures)")
     args = ap.parse_args()
     if args.serve:
         print(json.dumps(serve_bench(args.serve)), flush=True)
+        return
+    if args.sweep:
+        print(json.dumps(sweep_bench(args.sweep, args.sweep_nmax)), flush=True)
         return
     cfg = CONFIGS[args.config]
 
@@ -260,6 +275,19 @@ def main():
     B = args.block
     log(f"[rank {rank}] T={mesh.n_tet} grid={desc.Nx}x{desc.Ny}x{desc.Nz} near blocks={solver.nearzone_count()} "
         f"setup {setup_s:.1f}s")
+    if args.profile == "solve16":
+        # sixteen columns in the mixed batched form (large configs: a sample of the column loop)
+        solver.timing(reset=True)
+        _, it = solver.compute_T_matrix(Nmax, col0=0, ncol=16, block=16, tol=cfg["tol"], m=cfg["inner_m"],
+                                        cycles=60, precision=api.PREC_MIXED, inner_tol=cfg["inner_tol"],
+                                        max_outer=cfg["max_outer"])
+        ms = solver.timing(reset=True)["accum_ms"]
+        print(json.dumps({"config": args.config, "tets": mesh.n_tet, "grid_nodes": [desc.Nx, desc.Ny, desc.Nz],
+                          "near_bytes": solver.nearzone_bytes(), "setup_s": round(setup_s, 2),
+                          "columns": 16, "columns_per_s": round(16 / (ms / 1e3), 4),
+                          "iters_mean": float(np.mean(it))}), flush=True)
+        solver.close()
+        return
     if args.profile:
         nrhs, prec = {"near1": (1, api.PREC_FP64), "near16": (16, api.PREC_FP64),
                       "mixed16": (16, api.PREC_MIXED)}[args.profile]
@@ -516,6 +544,52 @@ def serve_bench(nreq):
             "completed": st["completed"], "columns": st["columns"], "peak_running": st["peak_running"],
             "peak_bytes": st["peak_bytes"], "busy_s": round(st["busy_s"], 2), "wall_s": round(wall, 2)}
     return line
+
+
+def sweep_bench(nw, nmax_cap):
+    """C3-shaped wavelength sweep: one ellipsoid mesh (1:0.8:0.6, ~60k tets,
+    eps 2.5+0.05i), nw wavelengths taken evenly from 32 values of ka
+    log-spaced in [1, 10], Nmax from the Wiscombe rule ka + 4 ka^(1/3) + 2
+    clipped to [4, nmax_cap], grid N = 16..64 nodes on the longest axis with
+    ka (padded 32^3-128^3), raised to the mesh resolution where that is finer.  Every wavelength is a request of the serving
+    layer (its own grid and operator), all submitted at once, mixed
+    precision; their solves overlap on the GPU."""
+    from scadyn_b200 import geometry, meshgen
+    from scadyn_b200.server import Server
+    from scadyn_b200 import api
+    mesh = meshgen.ellipsoid(17.1, (1.0, 0.8, 0.6), seed=1003, eps=2.5 + 0.05j)
+    kas = np.logspace(0, 1, 32)
+    pick = np.unique(np.round(np.linspace(0, 31, nw)).astype(int))
+    srv = Server(hbm_budget=150e9, max_running=4)
+    reqs = []
+    t0 = time.time()
+    for i in pick:
+        ka = float(kas[i])
+        nmax = int(np.clip(round(ka + 4 * ka ** (1 / 3) + 2), 4, nmax_cap))
+        # grid: the ka rule (16..64), but never coarser than the mesh resolution
+        # (about T^(1/3) nodes on the longest axis); coarser boxes would make
+        # the near zone dominate
+        N = int(np.clip(round((16 + 48 * (ka - 1) / 9) / 2) * 2, 16, 64))
+        N = max(N, int(round(0.9 * mesh.n_tet ** (1 / 3) / 2)) * 2)
+        gs = geometry.cell_size_for_grid(mesh.coord, mesh.etopol, N)
+        rid = srv.submit(mesh, ka / mesh.a, gs, nmax, tol=1e-6, m=30, cycles=60, block=16,
+                         precision=api.PREC_MIXED, inner_tol=3e-4, max_outer=10)
+        reqs.append((rid, ka, nmax, N))
+    for rid, *_ in reqs:
+        srv.wait(rid, 3600)
+    wall = time.time() - t0
+    st = srv.stats()
+    per = [{"ka": round(ka, 3), "Nmax": nmax, "N": N, "latency_ms": round(srv.poll(rid)[2], 1)}
+           for rid, ka, nmax, N in reqs]
+    srv.close()
+    return {"metric": "C3-shaped wavelength sweep: T-matrix columns/s over all wavelengths (mixed precision)",
+            "value": round(st["columns"] / st["busy_s"], 4), "unit": "columns/s", "n_gpus": 1,
+            "higher_is_better": True, "dtype": "c64 inner / f64 outer", "data": "synthetic (seeded mesh)",
+            "config": {"workload": "ellipsoid 1:0.8:0.6, %d tets, eps 2.5+0.05i, %d of 32 log-spaced ka in [1,10], "
+                                   "Nmax Wiscombe clipped to [4,%d], N 16-64" % (mesh.n_tet, len(pick), nmax_cap)},
+            "wavelengths": per, "columns": st["columns"], "busy_s": round(st["busy_s"], 2),
+            "wall_s": round(wall, 2), "p50_ms": round(st["p50_ms"], 1), "p99_ms": round(st["p99_ms"], 1),
+            "peak_running": st["peak_running"], "peak_bytes": st["peak_bytes"]}
 
 
 def matvec_roofline(solver, desc, T, Bref, peak, ms1, msb, nb):
