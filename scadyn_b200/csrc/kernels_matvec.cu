@@ -443,7 +443,11 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS) k_near_groups(NearPass a) {
     extern __shared__ __align__(128) unsigned char nz_sh[];
     uint64_t *full = reinterpret_cast<uint64_t *>(nz_sh);
     uint64_t *empty = full + NZ_SLOTS;
-    int *toff = reinterpret_cast<int *>(nz_sh + 16 * NZ_SLOTS);          // ring offset of each slot's tile
+    // per slot, written by the producer before the slot's arrive: ring offset,
+    // n2 and column partial slot of the tile (consumers read no tile table)
+    int *toff = reinterpret_cast<int *>(nz_sh + 16 * NZ_SLOTS);
+    int *tn2 = toff + NZ_SLOTS;
+    long long *tcol = reinterpret_cast<long long *>(nz_sh + 24 * NZ_SLOTS);
     C *const X1 = reinterpret_cast<C *>(nz_sh + NZ_META);                 // x(g)
     unsigned char *const ring = nz_sh + NZ_META + a.x1_bytes;
     const ST *data = static_cast<const ST *>(a.data);
@@ -502,6 +506,8 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS) k_near_groups(NearPass a) {
                     const uint32_t st = fit ? head : 0u;
                     const int k = ord % NZ_SLOTS;
                     toff[k] = (int)st;
+                    tn2[k] = tl.n2;
+                    tcol[k] = tl.col_off;
                     mbar_expect_tx(&full[k], S + x1b);
                     bulk_g2s(ring + st, data + tl.data_off, mb, &full[k]);
                     bulk_g2s(ring + st + mb, xp + 3LL * tl.s2 * RG, xb, &full[k]);
@@ -532,9 +538,9 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS) k_near_groups(NearPass a) {
         for (int t = t0; t < t1; ++t, ++ord) {
             const int kslot = ord % NZ_SLOTS;
             mbar_wait(&full[kslot], (uint32_t)((ord / NZ_SLOTS) & 1), a.err);
-            const NearTile &tl = a.tiles[t];
-            const int n2 = tl.n2;
+            const int n2 = tn2[kslot];
             const int tof = toff[kslot];
+            const long long tcoff = tcol[kslot];
             const uint32_t M = smem_addr(ring + tof);
             const uint32_t X2 = M + (uint32_t)(tile_elems(n1, n2) * (long long)sizeof(ST));
             constexpr uint32_t SB = sizeof(ST), CB = sizeof(C);
@@ -556,7 +562,7 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS) k_near_groups(NearPass a) {
                         }
                     }
                 }
-            } else if (tl.col_off >= 0 && it < n2 * a.nq) {
+            } else if (tcoff >= 0 && it < n2 * a.nq) {
                 const int q = it / n2, j = it - q * n2;
                 C cacc[3][U];
 #pragma unroll
@@ -581,7 +587,7 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS) k_near_groups(NearPass a) {
                 for (int u = 0; u < U; ++u) {
                     const int r = U * q + u;
                     if (r < rg && !(a.skip && a.skip[r0 + r])) {
-                        C *pc = part + (r0 + r) * a.part_len + tl.col_off + 3 * j;
+                        C *pc = part + (r0 + r) * a.part_len + tcoff + 3 * j;
                         pc[0] = cacc[0][u];
                         pc[1] = cacc[1][u];
                         pc[2] = cacc[2][u];
