@@ -231,8 +231,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
-    ap.add_argument("--block", type=int, default=32, help="columns per step")
-    ap.add_argument("--slots", type=int, default=16, help="columns solved concurrently (batched GMRES slots)")
+    ap.add_argument("--block", type=int, default=64, help="columns per step")
+    ap.add_argument("--slots", type=int, default=32, help="columns solved concurrently (batched GMRES slots)")
     ap.add_argument("--plain-sample", type=int, default=2, help="columns timed in the plain one-at-a-time form")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serve", type=int, default=0,
