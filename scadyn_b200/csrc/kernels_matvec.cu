@@ -392,6 +392,12 @@ constexpr int NZ_QMAX = 4;             // quads of right-hand sides per pass
 constexpr int NZ_SLOTS = 8;                 // tiles in flight at most (mbarrier pairs)
 constexpr int NZ_META = 256;                // bytes of barriers and ring offsets
 constexpr size_t NZ_SMEM_2CTA = 113 * 1024; // dynamic shared memory per CTA that lets two CTAs share an SM
+constexpr size_t NZ_SMEM_4CTA = 56 * 1024;  // ... four CTAs
+// With one right-hand side a tile's sums are short dependent chains, so the
+// kernel is latency-bound per tile: four CTAs per SM (registers and ring
+// bounded to fit) keep four tiles in progress.  With register tiles of four
+// right-hand sides the compiler is left free (two CTAs fit).
+template <int U> constexpr int NZ_MIN_CTAS = U == 1 ? 4 : 1;
 constexpr size_t NZ_SMEM_MAX = 227 * 1024;
 constexpr int NZ_MAX_THREADS = 2 * 32 * ((SCD_GROUP_MAX * NZ_QMAX + 31) / 32) + 32;
 
@@ -439,7 +445,7 @@ __device__ __forceinline__ void load_xu(uint32_t addr, C (&xu)[U]) {
 }
 
 template <typename ST, typename C, int U>
-__global__ void __launch_bounds__(NZ_MAX_THREADS) k_near_groups(NearPass a) {
+__global__ void __launch_bounds__(NZ_MAX_THREADS, NZ_MIN_CTAS<U>) k_near_groups(NearPass a) {
     extern __shared__ __align__(128) unsigned char nz_sh[];
     uint64_t *full = reinterpret_cast<uint64_t *>(nz_sh);
     uint64_t *empty = full + NZ_SLOTS;
@@ -831,7 +837,7 @@ void near_launch(scd_ctx *c, const ST *data, const C *x, int nrhs, const int *do
     a.x1_bytes = (uint32_t)(3 * c->max_per_group * a.rg_stride * sizeof(C));
     // the ring fills what two CTAs per SM leave, and must hold the largest tile with its x
     const size_t max_tile = (size_t)c->max_tile_store * sizeof(ST) + a.x1_bytes;
-    size_t ring = (NZ_SMEM_2CTA - NZ_META - a.x1_bytes) / 16 * 16;
+    size_t ring = ((U == 1 ? NZ_SMEM_4CTA : NZ_SMEM_2CTA) - NZ_META - a.x1_bytes) / 16 * 16;
     if (ring < max_tile) ring = std::min((NZ_SMEM_MAX - NZ_META - a.x1_bytes) / 16 * 16, (max_tile + 15) / 16 * 16 * 2);
     a.ring_bytes = (uint32_t)ring;
     {
