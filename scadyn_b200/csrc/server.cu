@@ -84,7 +84,8 @@ struct scd_server {
     clk::time_point busy_since;
     bool stop = false;
     std::thread dispatcher;
-    std::vector<std::thread> workers;
+    std::map<int64_t, std::thread> workers;   // running (or just finished) request threads
+    std::vector<int64_t> finished;            // workers done with the lock, to be joined
     std::string scratch_err;
 };
 
@@ -137,6 +138,7 @@ void run_request(scd_server *s, int64_t id) {
         }
         s->in_use -= r->est;
         s->running -= 1;
+        s->finished.push_back(id);   // after this the worker takes the lock no more
         if (s->running == 0) s->busy_s += std::chrono::duration<double>(clk::now() - s->busy_since).count();
     }
     s->cv.notify_all();
@@ -145,6 +147,15 @@ void run_request(scd_server *s, int64_t id) {
 void dispatch_loop(scd_server *s) {
     std::unique_lock<std::mutex> lk(s->m);
     while (true) {
+        // join the workers that finished (they no longer take the lock)
+        for (int64_t id : s->finished) {
+            auto w = s->workers.find(id);
+            if (w != s->workers.end()) {
+                if (w->second.joinable()) w->second.join();
+                s->workers.erase(w);
+            }
+        }
+        s->finished.clear();
         // admit, in arrival order, every queued request that fits now
         bool admitted = false;
         for (auto q = s->queue.begin(); q != s->queue.end();) {
@@ -157,7 +168,7 @@ void dispatch_loop(scd_server *s) {
             s->in_use += r.est;
             s->peak_running = std::max(s->peak_running, s->running);
             s->peak_bytes = std::max(s->peak_bytes, s->in_use);
-            s->workers.emplace_back(run_request, s, *q);
+            s->workers.emplace(*q, std::thread(run_request, s, *q));
             q = s->queue.erase(q);
             admitted = true;
         }
@@ -333,7 +344,7 @@ int scd_server_destroy(scd_server *s) {
     s->cv.notify_all();
     if (s->dispatcher.joinable()) s->dispatcher.join();
     for (auto &w : s->workers)
-        if (w.joinable()) w.join();
+        if (w.second.joinable()) w.second.join();
     delete s;
     return SCD_OK;
 }
