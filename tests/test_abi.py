@@ -80,3 +80,25 @@ int main(void) {
         assert int(out) == api.SCD_NO_DEVICE
     else:
         assert int(out) == api.SCD_OK
+
+
+def test_server_estimate_is_host_side_and_monotone():
+    """scd_server_estimate (the admission figure) needs no device: it grows
+    with the mesh, the VSWF order and FP64 storage of the near zone, and
+    counts both precision forms' buffers."""
+    from scadyn_b200 import meshgen
+    from scadyn_b200 import server as srv
+    lib = srv._lib()
+    import ctypes as C
+
+    def est(mesh, Nmax, storage=api.STORE_C64, precision=api.PREC_MIXED):
+        r, keep = srv.Server._request(None, mesh, 1.0 / mesh.a, 1.8, Nmax, storage=storage, precision=precision)
+        b = C.c_int64()
+        assert lib.scd_server_estimate(C.byref(r), C.byref(b)) == api.SCD_OK
+        return b.value
+
+    small, big = meshgen.sphere(4, seed=1), meshgen.sphere(7, seed=1)
+    assert est(big, 4) > est(small, 4) > 0
+    assert est(small, 8) > est(small, 4)
+    assert est(small, 4, storage=api.STORE_C128) > est(small, 4)
+    assert est(small, 4, precision=api.PREC_FP64) > 0
