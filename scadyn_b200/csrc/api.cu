@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <unordered_map>
 #include <vector>
@@ -101,6 +102,7 @@ static int set_order(scd_ctx *c, const std::vector<int> &cube_of_tet) {
             // a different binning invalidates anything stored in slot order
             c->have_proj = false;
             c->have_near = false;
+            c->nzm_ready = false;
         } else {
             return SCD_OK;
         }
@@ -351,6 +353,10 @@ int scd_create(scd_ctx **out, const scd_grid_desc *d) {
     scd_ctx *c = new scd_ctx();
     c->d = *d;
     c->dev = d->device;
+    {
+        const char *e = getenv("SCADYN_NEAR_MMA");
+        c->nzm_on = e && e[0] == '1';
+    }
     cudaSetDevice(c->dev);
     cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev);
     c->Nx = d->Nx; c->Ny = d->Ny; c->Nz = d->Nz;
@@ -383,7 +389,8 @@ int scd_destroy(scd_ctx *c) {
                     c->d_pslot_cnt, c->d_tc, c->d_tvol, c->d_eps, c->d_bpart, c->d_W, c->d_R, c->d_nzpart, c->d_x,
                     c->d_y, c->d_io, c->d_rhs,
                     c->d_bar, c->d_err, c->d_tw[0], c->d_tw[1], c->d_tw[2], c->f_P, c->f_Fo,
-                    c->f_tw[0], c->f_tw[1], c->f_tw[2], c->f_bpart, c->f_W, c->f_R, c->f_nzpart, c->d_xT, c->f_xT};
+                    c->f_tw[0], c->f_tw[1], c->f_tw[2], c->f_bpart, c->f_W, c->f_R, c->f_nzpart, c->d_xT, c->f_xT,
+                    c->d_t16, c->d_t16_off, c->d_xb, c->d_xb_off, c->d_xmax, c->d_xinv};
     for (void *p : ptrs) if (p) cudaFree(p);
     batch_free(c);
     if (c->d_mat) cudaFree(c->d_mat);
@@ -463,6 +470,7 @@ int scd_set_nearzone(scd_ctx *c, int64_t B, const void *sp_mat, const int32_t *s
     if (prec != SCD_STORE_C64 && prec != SCD_STORE_C128) return set_error(c, SCD_BAD_ARG, "storage_prec %d", prec);
     int rc;
     c->have_near = false;
+    c->nzm_ready = false;
     c->near_prec = prec;
     c->f_cap = 0;
     if (prec == SCD_STORE_C64) rc = build_tiles<cf>(c, B, (const cf *)sp_mat, sp_ind);

@@ -139,6 +139,18 @@ struct scd_ctx {
     cf *f_bpart = nullptr, *f_W = nullptr, *f_R = nullptr, *f_nzpart = nullptr, *f_xT = nullptr;
     int f_cap = 0;
 
+    // tensor-core near zone of the complex64 matvec (near_mma.cu), opt-in by
+    // SCADYN_NEAR_MMA=1 at context creation
+    bool nzm_on = false, nzm_ready = false;
+    unsigned char *d_t16 = nullptr;      // f16 hi/lo planes of every tile
+    long long *d_t16_off = nullptr;      // per tile byte offset
+    unsigned char *d_xb = nullptr;       // x blocks of one pass
+    long long *d_xb_off = nullptr;       // per group byte offset
+    unsigned int *d_xmax = nullptr;      // per right-hand side largest |x| (float bits), then the tiles'
+    float *d_xinv = nullptr;             // per right-hand side 1 / (sA sx)
+    float nzm_sA = 1.f;
+    uint32_t nzm_x1 = 0, nzm_ring = 0, nzm_slack = 0;
+
     void *batch = nullptr;               // batch-solver buffers (batch.cu)
     std::vector<double> col_latency_ms;  // admission -> completion, last batch solve
 
@@ -162,6 +174,9 @@ void launch_near(scd_ctx *c, const cd *x, int nrhs, const int *done);
 void launch_fft_chain(scd_ctx *c, const cd *x, int nrhs, const int *done);
 void launch_gather(scd_ctx *c, const cd *x, cd *y, int nrhs, const int *done);
 int build_twiddles(scd_ctx *c, int P, cd **out);
+// tensor-core near zone (near_mma.cu)
+int near_mma_prepare(scd_ctx *c);
+void near_mma_run(scd_ctx *c, const cf *x, int nrhs, const int *done);
 
 // ---- batched column solves (batch.cu) ----
 void batch_free(scd_ctx *c);

@@ -12,6 +12,8 @@
 #include <algorithm>
 #include <cstdint>
 
+#include <type_traits>
+
 #include "ctx.h"
 #include "fft_reg.cuh"
 
@@ -860,6 +862,12 @@ void near_dispatch(scd_ctx *c, const ST *data, const C *x, int nrhs, const int *
 template <typename C>
 void near_t(scd_ctx *c, const C *x, int nrhs, const int *done) {
     if (c->ngroups == 0) return;
+    if constexpr (std::is_same<C, cf>::value) {
+        if (c->nzm_on && c->nzm_ready) {
+            near_mma_run(c, x, nrhs, done);
+            return;
+        }
+    }
     if (c->near_prec == SCD_STORE_C64) near_dispatch<cf, C>(c, (const cf *)c->d_tdata, x, nrhs, done);
     else near_dispatch<cd, C>(c, (const cd *)c->d_tdata, x, nrhs, done);
     c->launches += 1;
@@ -909,6 +917,10 @@ int build_twiddles(scd_ctx *c, int P, cd **out) {
 // complex64 copies of the projectors, the Green octant and the twiddles for
 // the mixed-precision inner solves (rounded from the FP64 operator)
 int ensure_single(scd_ctx *c) {
+    if (c->nzm_on && !c->nzm_ready && c->have_near && c->ngroups > 0) {
+        const int rc = near_mma_prepare(c);
+        if (rc) return rc;
+    }
     if (c->f_ready) return SCD_OK;
     const long long np = 4LL * 27 * c->T, no = (long long)c->Hx * c->Hy * c->Hz;
     auto al = [&](cf **p, long long n) -> int {

@@ -810,6 +810,7 @@ int setup_nearzone_device(scd_ctx *c, int prec) {
     int rc = upload_quadrature(c);
     if (rc) return rc;
     c->have_near = false;
+    c->nzm_ready = false;
     c->near_prec = prec;
     if ((rc = build_tile_layout(c))) return rc;
     const size_t esz = prec == SCD_STORE_C64 ? sizeof(cf) : sizeof(cd);
