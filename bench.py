@@ -251,7 +251,11 @@ def main():
     ap.add_argument("--sweep-nmax", type=int, default=14, help="largest Nmax of the sweep (C3: 14)")
     ap.add_argument("--profile", default=None, choices=["near1", "near16", "mixed16", "solve16"],
                     help="only build the operator and run profile_matvec (for ncu captures)")
+    ap.add_argument("--near-mma", action="store_true",
+                    help="tensor-core near zone for the complex64 matvec (SCADYN_NEAR_MMA=1)")
     args = ap.parse_args()
+    if args.near_mma:
+        os.environ["SCADYN_NEAR_MMA"] = "1"
     if args.serve:
         print(json.dumps(serve_bench(args.serve)), flush=True)
         return
@@ -480,6 +484,7 @@ def main():
                                     "stored complex64 as the reference)" % (cfg["inner_m"], cfg["inner_tol"],
                                                                             cfg["tol"]),
                        "l2": "inputs larger than L2 (near-zone tiles %.2f GB per matvec)" % (solver.nearzone_bytes() / 1e9),
+                       "near_zone": "tensor cores (f16 hi/lo)" if args.near_mma else "CUDA cores",
                        "parallelism": f"replicas x{world}"},
             "t_rel_err_vs_fp64": t_err,
             "p50_ms": round(float(np.percentile(lat_s, 50)), 3),
