@@ -866,6 +866,30 @@ void orc_matmul_Acorr_const(int T, int64_t B, const fc *sp32, const zc *sp64, co
     free(priv);
 }
 
+/* matmul_Acorr, src/sparse_mat.f90:64-92 (linear basis): 12 unknowns per tet
+ * ordered (component, node) as x(12(t-1) + 4c + i); Ax[a] += V x[b] and, if
+ * a != b, Ax[b] += V^T x[a].  V(r, c) is stored column-major per block. */
+void orc_matmul_Acorr(int T, int64_t B, const fc *sp32, const zc *sp64, const int32_t *sp_ind,
+                      const zc *x, zc *Ax) {
+    size_t n = 12*(size_t)T;
+    for (size_t i = 0; i < n; ++i) Ax[i] = 0;
+    for (int64_t i1 = 0; i1 < B; ++i1) {
+        size_t a = 12*(size_t)(sp_ind[2*i1] - 1), b = 12*(size_t)(sp_ind[2*i1 + 1] - 1);
+        const size_t v0 = 144*(size_t)i1;
+        for (int r = 0; r < 12; ++r) {
+            zc s = 0;
+            for (int c = 0; c < 12; ++c) s += (sp32 ? (zc)sp32[v0 + r + 12*c] : sp64[v0 + r + 12*c])*x[b + c];
+            Ax[a + r] += s;
+        }
+        if (a != b)
+            for (int c = 0; c < 12; ++c) {
+                zc s = 0;
+                for (int r = 0; r < 12; ++r) s += (sp32 ? (zc)sp32[v0 + r + 12*c] : sp64[v0 + r + 12*c])*x[a + r];
+                Ax[b + c] += s;
+            }
+    }
+}
+
 /* one convolution: grid source -> pruned FFT -> x Fg -> pruned IFFT -> octant/(8N^3) */
 static void convolve(const orc_op *op, zc *grid_src /* N^3 */, zc *SS, zc *out /* N^3 */) {
     const orc_geom *g = op->g;
@@ -885,17 +909,25 @@ static void convolve(const orc_op *op, zc *grid_src /* N^3 */, zc *SS, zc *out /
         out[k + (size_t)Nx*(l + (size_t)Ny*m)] = SS[k + (size_t)Px*(l + (size_t)Py*m)]/sc;
 }
 
-/* compute_Ax2, src/gmres_module.f90:57-176 (constant basis).  merged = 1
- * folds convolutions 4-6 (:122-144) into one by linearity. */
+/* compute_Ax2, src/gmres_module.f90:57-176, constant (order 0) or linear
+ * (order 1) basis.  The linear basis has 4 projector columns per tet (one per
+ * node, S(27, 4T)) and 12 unknowns per tet, x(12(t-1) + 4c + i) for component
+ * c and node i (:88-95, :156-165).  merged = 1 folds convolutions 4-6
+ * (:122-144) into one by linearity. */
 int orc_compute_Ax2(const orc_op *op, const zc *x, zc *Ax) {
     const orc_geom *g = op->g;
-    const int T = op->T;
+    const int Nb = op->order == 1 ? 4 : 1;
+    const int T = Nb*op->T;   /* projector columns */
     const size_t mm = (size_t)g->Nx*g->Ny*g->Nz, tot = 8*mm;
     zc *X = (zc *)malloc(sizeof(zc)*3*(size_t)T);
     zc *src = (zc *)malloc(sizeof(zc)*mm), *res = (zc *)malloc(sizeof(zc)*mm), *SS = (zc *)malloc(sizeof(zc)*tot);
     zc *Y[3], *Y2[3], *tmp = (zc *)malloc(sizeof(zc)*(size_t)T);
     for (int d = 0; d < 3; ++d) { Y[d] = (zc *)malloc(sizeof(zc)*(size_t)T); Y2[d] = (zc *)calloc((size_t)T, sizeof(zc)); }
-    for (int t = 0; t < T; ++t) for (int d = 0; d < 3; ++d) X[(size_t)d*T + t] = x[3*(size_t)t + d];
+    if (Nb == 1)
+        for (int t = 0; t < T; ++t) for (int d = 0; d < 3; ++d) X[(size_t)d*T + t] = x[3*(size_t)t + d];
+    else
+        for (int t = 0; t < op->T; ++t) for (int i = 0; i < 4; ++i) for (int d = 0; d < 3; ++d)
+            X[(size_t)d*T + 4*(size_t)t + i] = x[12*(size_t)t + 4*d + i];
     const zc *P[3] = {op->Sx, op->Sy, op->Sz};
     for (int d = 0; d < 3; ++d) {
         orc_sparse_T_matmul(T, op->S, op->indS, X + (size_t)d*T, (int)mm, src);
@@ -921,10 +953,18 @@ int orc_compute_Ax2(const orc_op *op, const zc *x, zc *Ax) {
         for (int e = 0; e < 3; ++e) orc_sparse_eps_matmul(T, P[e], op->indS, res, Y2[e]);
         free(acc);
     }
-    orc_matmul_Acorr_const(T, op->B, op->sp32, op->sp64, op->sp_ind, x, Ax, op->nthreads);
     const double k2 = op->k*op->k;
-    for (int t = 0; t < T; ++t) for (int d = 0; d < 3; ++d)
-        Ax[3*(size_t)t + d] = Ax[3*(size_t)t + d] + (Y2[d][t] - k2*Y[d][t]);
+    if (Nb == 1) {
+        orc_matmul_Acorr_const(T, op->B, op->sp32, op->sp64, op->sp_ind, x, Ax, op->nthreads);
+        for (int t = 0; t < T; ++t) for (int d = 0; d < 3; ++d)
+            Ax[3*(size_t)t + d] = Ax[3*(size_t)t + d] + (Y2[d][t] - k2*Y[d][t]);
+    } else {
+        orc_matmul_Acorr(op->T, op->B, op->sp32, op->sp64, op->sp_ind, x, Ax);
+        for (int t = 0; t < op->T; ++t) for (int i = 0; i < 4; ++i) for (int d = 0; d < 3; ++d) {
+            const size_t b = 4*(size_t)t + i;
+            Ax[12*(size_t)t + 4*d + i] = Ax[12*(size_t)t + 4*d + i] + (Y2[d][b] - k2*Y[d][b]);
+        }
+    }
     free(X); free(src); free(res); free(SS); free(tmp);
     for (int d = 0; d < 3; ++d) { free(Y[d]); free(Y2[d]); }
     return 0;
@@ -958,7 +998,7 @@ static void tri_solve(int i, int ld, const zc *H, const zc *g, zc *y) {
  * the end of each cycle (:309) is not repeated: the next cycle recomputes it
  * (:224) and nothing reads the first one. */
 int orc_gmres(const orc_op *op, const zc *rhs, zc *xout, double tol, int m, int cycles, orc_gmres_info *info) {
-    const size_t n = 3*(size_t)op->T;
+    const size_t n = (op->order == 1 ? 12 : 3)*(size_t)op->T;
     zc *x = (zc *)malloc(sizeof(zc)*n), *r = (zc *)malloc(sizeof(zc)*n), *w = (zc *)malloc(sizeof(zc)*n);
     zc *V = (zc *)calloc(n*(size_t)(m + 1), sizeof(zc));
     zc *H = (zc *)calloc((size_t)(m + 1)*m, sizeof(zc));

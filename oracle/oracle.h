@@ -94,9 +94,13 @@ typedef struct {
     double k;
     int merged;                /* 0: six convolutions as the reference; 1: four */
     int nthreads;
+    int order;                 /* basis order: 0 constant (3 unknowns per tet), 1 linear (12: 4 nodes x 3) */
 } orc_op;
 
 int  orc_compute_Ax2(const orc_op *op, const zc *x, zc *Ax);
+/* matmul_Acorr (src/sparse_mat.f90:64-92): 12x12 blocks of the linear basis */
+void orc_matmul_Acorr(int T, int64_t B, const fc *sp32, const zc *sp64, const int32_t *sp_ind,
+                      const zc *x, zc *Ax);
 
 /* restarted GMRES (src/gmres_module.f90:180-325) */
 typedef struct {

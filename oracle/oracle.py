@@ -49,7 +49,7 @@ class _Op(C.Structure):
         ("S", C.c_void_p), ("Sx", C.c_void_p), ("Sy", C.c_void_p), ("Sz", C.c_void_p),
         ("indS", C.c_void_p), ("Fg", C.c_void_p),
         ("B", C.c_int64), ("sp32", C.c_void_p), ("sp64", C.c_void_p), ("sp_ind", C.c_void_p),
-        ("k", C.c_double), ("merged", C.c_int), ("nthreads", C.c_int),
+        ("k", C.c_double), ("merged", C.c_int), ("nthreads", C.c_int), ("order", C.c_int),
     ]
 
 
@@ -173,11 +173,12 @@ class Operator:
     sp_ind: np.ndarray
     merged: bool = False
     nthreads: int = 1
+    order: int = 0          # 1: linear basis, S (4T, 27), sp_mat (B, 12, 12), 12 unknowns per tet
 
     def _op(self):
         o = _Op()
         o.g = C.addressof(self.geom._g)
-        o.T = self.geom.T
+        o.T = self.S.shape[0] // (4 if self.order == 1 else 1)   # tets (projector columns / basis functions per tet)
         o.S, o.Sx, o.Sy, o.Sz = (a.ctypes.data for a in (self.S, self.Sx, self.Sy, self.Sz))
         o.indS = self.indS.ctypes.data
         o.Fg = self.Fg.ctypes.data
@@ -190,6 +191,7 @@ class Operator:
         o.k = self.geom.k
         o.merged = int(self.merged)
         o.nthreads = self.nthreads
+        o.order = int(self.order)
         return o
 
     def compute_Ax2(self, x: np.ndarray) -> np.ndarray:
@@ -211,6 +213,42 @@ class Operator:
         return x, {"iters": info.iters, "matvecs": info.matvecs, "cycles": info.cycles,
                    "converged": bool(info.converged), "relres": info.relres,
                    "history": hist[: info.history_len].copy()}
+
+
+def linear_from_constant(op, seed=0):
+    """A linear-basis (order 1) operator on the geometry of a constant-basis
+    one, for parity of the order-1 matvec: each tet's projector column is
+    split over its 4 nodes with seeded weights (one column per basis function,
+    same box nodes, as pfft_projection_lin stores them, src/projection.f90:
+    170-338), and each 3x3 near-zone block V becomes the 12x12 block
+    V(c, c') * m(i, j), m seeded and not symmetric (self blocks included)."""
+    rng = np.random.default_rng(seed)
+    T = op.geom.T
+    w = 0.25 + 0.05 * rng.standard_normal((T, 4, 4))          # per tet and node, one weight per projector kind
+
+    def split(P, kind):
+        return np.ascontiguousarray((P[:, None, :] * w[:, :, kind, None]).reshape(4 * T, 27))
+
+    S1, Sx1, Sy1, Sz1 = (split(P, q) for q, P in enumerate((op.S, op.Sx, op.Sy, op.Sz)))
+    indS1 = np.ascontiguousarray(np.repeat(op.indS, 4, axis=0))
+    B = op.sp_ind.shape[0]
+    m = (np.eye(4)[None] + 0.1 * (rng.standard_normal((B, 4, 4)) + 1j * rng.standard_normal((B, 4, 4)))) / 2
+    V = op.sp_mat.astype(np.complex128)       # memory (3,3,B): V[b, c', c] = V(c, c')
+    # 12x12 block, memory (12,12,B): A[b, 4c'+j, 4c+i] = V(c, c') m(i, j)
+    A = np.einsum("bdc,bij->bdjci", V, m).reshape(B, 12, 12)
+    sp12 = np.ascontiguousarray(A.astype(op.sp_mat.dtype))
+    return Operator(op.geom, S1, Sx1, Sy1, Sz1, indS1, op.Fg, sp12, op.sp_ind.copy(), merged=op.merged,
+                    nthreads=op.nthreads, order=1)
+
+
+def matmul_Acorr(T, sp_mat, sp_ind, x):
+    """matmul_Acorr (12x12 blocks, src/sparse_mat.f90:64-92)."""
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    Ax = np.zeros(12 * T, np.complex128)
+    sp32 = sp_mat if sp_mat.dtype == np.complex64 else None
+    sp64 = sp_mat if sp_mat.dtype == np.complex128 else None
+    lib().orc_matmul_Acorr(T, C.c_int64(sp_ind.shape[0]), _p(sp32), _p(sp64), _p(sp_ind), _p(x), _p(Ax))
+    return Ax
 
 
 def matmul_Acorr_const(T, sp_mat, sp_ind, x, nthreads=1):
