@@ -57,7 +57,12 @@ typedef struct scd_grid_desc {
     double  delta;           /* node spacing (mesh%delta) */
     double  min_coord[3];    /* grid origin (mesh%min_coord) */
     int32_t T;               /* tetrahedra (mesh%N_tet) */
-    int32_t order;           /* basis order (mesh%order); 0 only */
+    int32_t order;           /* basis order (mesh%order): 0 constant (3 unknowns per tet), 1 linear
+                                (12 per tet, x(12(t-1) + 4c + i)); with 1 only the host-built operator
+                                path is open (scd_set_projectors/scd_set_nearzone, scd_matvec,
+                                scd_gmres, scd_solve_columns), as the reference solves no linear-basis
+                                T-matrix (src/T_matrix.f90:250-259 pairs 3T-row right-hand sides with
+                                its 12T unknowns) */
     int32_t M_ex;            /* projection order (mesh%M_ex); 2 only */
     int32_t near_zone;       /* near-cube radius (mesh%near_zone); 1 only */
     int32_t device;          /* CUDA device ordinal */
@@ -98,14 +103,19 @@ SCD_API int scd_set_wavenumber(scd_ctx *ctx, double k);
  * delta, min_coord and k (requires scd_set_wavenumber first). */
 SCD_API int scd_set_green(scd_ctx *ctx, const scd_c128 *Fg);
 
-/* matrices%S/Sx/Sy/Sz/indS (src/projection.f90:155-164). M_box must be 27. */
+/* matrices%S/Sx/Sy/Sz/indS (src/projection.f90:155-164). M_box must be 27.
+ * T is the number of projector columns: the tets, or 4 per tet for the
+ * linear basis (pfft_projection_lin, src/projection.f90:170-338), whose four
+ * columns of a tet name its box. */
 SCD_API int scd_set_projectors(scd_ctx *ctx, int32_t M_box, int32_t T,
                        const scd_c128 *S, const scd_c128 *Sx, const scd_c128 *Sy,
                        const scd_c128 *Sz, const int32_t *indS);
 
 /* matrices%sp_mat / sp_ind (src/precorrection.f90:251-254).  sp_mat points to
  * scd_c64 when storage_prec == SCD_STORE_C64 and to scd_c128 otherwise; the
- * device copy is kept in the same precision. */
+ * device copy is kept in the same precision.  Blocks are 3x3 (sp_mat(3,3,B)),
+ * or 12x12 (sp_mat(12,12,B), matmul_Acorr, src/sparse_mat.f90:64-92) for the
+ * linear basis. */
 SCD_API int scd_set_nearzone(scd_ctx *ctx, int64_t B, const void *sp_mat, const int32_t *sp_ind,
                      int32_t storage_prec);
 

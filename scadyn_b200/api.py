@@ -156,16 +156,20 @@ class GridInfo:
 class Solver:
     """One device context (scd_ctx) for one mesh and grid."""
 
-    def __init__(self, Nx, Ny, Nz, delta, min_coord, T, device=0):
+    def __init__(self, Nx, Ny, Nz, delta, min_coord, T, device=0, order=0):
+        """order 1 (linear basis): 4 projector columns and 12 unknowns per tet;
+        only the host-built operator path (set_projectors, set_nearzone with
+        12x12 blocks, compute_Ax2, gmres, solve_columns) is open."""
         self.lib = load_library()
         d = GridDesc()
         d.Nx, d.Ny, d.Nz, d.delta = Nx, Ny, Nz, delta
         for i in range(3):
             d.min_coord[i] = float(min_coord[i])
-        d.T, d.order, d.M_ex, d.near_zone, d.device = T, 0, 2, 1, device
+        d.T, d.order, d.M_ex, d.near_zone, d.device = T, order, 2, 1, device
         self.desc = d
-        self.T = T
-        self.n = 3 * T
+        self.order = order
+        self.T = (4 if order == 1 else 1) * T      # projector columns (basis functions)
+        self.n = 3 * self.T
         h = C.c_void_p()
         rc = self.lib.scd_create(C.byref(h), C.byref(d))
         self.ctx = h

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "ctx.h"
+#include "linear_basis.h"
 
 // ------------------------------------------------------------------ errors
 int set_error(scd_ctx *c, int code, const char *fmt, ...) {
@@ -114,18 +115,20 @@ static int set_order(scd_ctx *c, const std::vector<int> &cube_of_tet) {
     c->max_per_cube = 0;
     for (int q = 0; q < c->ncubes; ++q) c->max_per_cube = std::max(c->max_per_cube, cnt[q + 1] - cnt[q]);
     // near-zone groups: each non-empty box split into ceil(n / SCD_GROUP_MAX)
-    // runs whose sizes differ by at most one
+    // runs whose sizes differ by at most one; with the linear basis the runs
+    // hold whole tets (the blocks inside a tet are one-sided)
     c->grp_off.assign(1, 0);
     c->grp_cube.clear();
     c->grp_of_slot.assign(T, 0);
     c->max_per_group = 0;
+    const int nb = c->nb;
     for (int q = 0; q < c->ncubes; ++q) {
-        const int n = cnt[q + 1] - cnt[q];
+        const int n = (cnt[q + 1] - cnt[q]) / nb;          // tets
         if (n == 0) continue;
-        const int ng = (n + SCD_GROUP_MAX - 1) / SCD_GROUP_MAX;
+        const int ng = (n + SCD_GROUP_MAX / nb - 1) / (SCD_GROUP_MAX / nb);
         int s = cnt[q];
         for (int g = 0; g < ng; ++g) {
-            const int m = n / ng + (g < n % ng ? 1 : 0);
+            const int m = nb * (n / ng + (g < n % ng ? 1 : 0));
             for (int k = 0; k < m; ++k) c->grp_of_slot[s + k] = (int)c->grp_cube.size();
             s += m;
             c->grp_off.push_back(s);
@@ -268,9 +271,10 @@ int set_order_from_cubes(scd_ctx *c, const std::vector<int> &cube_of_tet) { retu
 
 // Tile the reference's symmetric block list (tet_B >= tet_T) into dense
 // group-pair tiles; see NearTile in ctx.h.  Blocks given twice are summed, as
-// the reference's SpMV would sum them.
+// the reference's SpMV would sum them.  A block flagged one-sided (linear
+// basis, inside a tet) is applied as given only, without its mirror.
 template <typename ST>
-static int build_tiles(scd_ctx *c, int64_t B, const ST *sp, const int32_t *ind) {
+static int build_tiles(scd_ctx *c, int64_t B, const ST *sp, const int32_t *ind, const unsigned char *one_sided = nullptr) {
     const int T = c->T;
     std::unordered_map<uint64_t, int> tid;
     tid.reserve((size_t)c->ngroups * 16);
@@ -322,7 +326,9 @@ static int build_tiles(scd_ctx *c, int64_t B, const ST *sp, const int32_t *ind) 
         };
         if (tl.g1 == tl.g2) {
             place(s1, s2, false);
-            if (s1 != s2) place(s2, s1, true);
+            if (s1 != s2 && !(one_sided && one_sided[b])) place(s2, s1, true);
+        } else if (one_sided && one_sided[b]) {
+            return set_error(c, SCD_BAD_ARG, "one-sided block between groups");
         } else if (c->grp_of_slot[s1] == tl.g1) {
             place(s1, s2, false);
         } else {
@@ -345,7 +351,7 @@ const char *scd_last_error(const scd_ctx *ctx) { return ctx ? ctx->err.c_str() :
 int scd_create(scd_ctx **out, const scd_grid_desc *d) {
     if (!out || !d) return SCD_BAD_ARG;
     *out = nullptr;
-    if (d->order != 0 || d->M_ex != 2 || d->near_zone != 1) return SCD_BAD_ARG;
+    if ((d->order != 0 && d->order != 1) || d->M_ex != 2 || d->near_zone != 1) return SCD_BAD_ARG;
     if (d->Nx < 4 || d->Ny < 4 || d->Nz < 4 || d->T <= 0 || !(d->delta > 0)) return SCD_BAD_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return SCD_NO_DEVICE; }
@@ -369,8 +375,9 @@ int scd_create(scd_ctx **out, const scd_grid_desc *d) {
     c->Hx = c->Px / 2 + 1; c->Hy = c->Py / 2 + 1; c->Hz = c->Pz / 2 + 1;
     c->ncx = (d->Nx - 2) / 2; c->ncy = (d->Ny - 2) / 2; c->ncz = (d->Nz - 2) / 2;
     c->ncubes = c->ncx * c->ncy * c->ncz;
-    c->T = d->T;
-    c->n = 3LL * d->T;
+    c->nb = d->order == 1 ? 4 : 1;
+    c->T = c->nb * d->T;
+    c->n = 3LL * c->T;
     *out = c;
     int rc;
     if ((rc = check_cuda(c, cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking), "stream"))) return rc;
@@ -446,6 +453,11 @@ int scd_set_projectors(scd_ctx *c, int32_t M_box, int32_t T, const scd_c128 *S, 
         }
         cube[t] = x / 2 + c->ncx * (y / 2 + c->ncy * (z / 2));
     }
+    // linear basis: the four basis functions of a tet share its box
+    for (int t = 0; t + c->nb <= T; t += c->nb)
+        for (int i = 1; i < c->nb; ++i)
+            if (cube[t + i] != cube[t])
+                return set_error(c, SCD_BAD_ARG, "indS columns %d and %d (one tet) name different boxes", t + 1, t + i + 1);
     int rc = set_order(c, cube);
     if (rc) return rc;
     std::vector<cd> h((size_t)4 * 27 * T);
@@ -473,8 +485,30 @@ int scd_set_nearzone(scd_ctx *c, int64_t B, const void *sp_mat, const int32_t *s
     c->nzm_ready = false;
     c->near_prec = prec;
     c->f_cap = 0;
-    if (prec == SCD_STORE_C64) rc = build_tiles<cf>(c, B, (const cf *)sp_mat, sp_ind);
-    else rc = build_tiles<cd>(c, B, (const cd *)sp_mat, sp_ind);
+    if (c->nb == 4) {
+        // linear basis: 12x12 blocks between tets -> 3x3 blocks between pseudo-tets
+        const int ntet = c->T / 4;
+        for (int64_t b = 0; b < B; ++b)
+            if (sp_ind[2 * b] < 1 || sp_ind[2 * b] > ntet || sp_ind[2 * b + 1] < 1 || sp_ind[2 * b + 1] > ntet)
+                return set_error(c, SCD_BAD_ARG, "sp_ind(:,%lld) = (%d,%d) outside 1..%d", (long long)b + 1,
+                                 sp_ind[2 * b], sp_ind[2 * b + 1], ntet);
+        std::vector<int32_t> ind3((size_t)32 * B);
+        std::vector<unsigned char> one((size_t)16 * B);
+        if (prec == SCD_STORE_C64) {
+            std::vector<cf> sp3((size_t)144 * B);
+            expand_linear_blocks<cf>(B, (const cf *)sp_mat, sp_ind, sp3.data(), ind3.data(), one.data());
+            rc = build_tiles<cf>(c, 16 * B, sp3.data(), ind3.data(), one.data());
+        } else {
+            std::vector<cd> sp3((size_t)144 * B);
+            expand_linear_blocks<cd>(B, (const cd *)sp_mat, sp_ind, sp3.data(), ind3.data(), one.data());
+            rc = build_tiles<cd>(c, 16 * B, sp3.data(), ind3.data(), one.data());
+        }
+        if (rc == SCD_OK) c->B_ref = B;
+    } else if (prec == SCD_STORE_C64) {
+        rc = build_tiles<cf>(c, B, (const cf *)sp_mat, sp_ind);
+    } else {
+        rc = build_tiles<cd>(c, B, (const cd *)sp_mat, sp_ind);
+    }
     if (rc == SCD_OK) c->have_near = true;
     return rc;
 }
@@ -681,6 +715,9 @@ int scd_compute_T_matrix(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int3
                          scd_c128 *T, int32_t *iters) {
     if (!c || !o || !T || Nmax < 1) return SCD_BAD_ARG;
     cudaSetDevice(c->dev);
+    // the incident columns are constant-basis (vswf2constant); the reference
+    // has no linear-basis T-matrix solve (src/T_matrix.f90:250-259)
+    if (c->nb != 1) return set_error(c, SCD_BAD_ARG, "scd_compute_T_matrix: constant basis only");
     int rc = ready(c);
     if (rc) return rc;
     const int nm = (Nmax + 1) * (Nmax + 1) - 1, ntot = 2 * nm;

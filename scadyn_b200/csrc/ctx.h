@@ -49,7 +49,8 @@ struct scd_ctx {
     int Px = 0, Py = 0, Pz = 0;          // padded FFT lengths (powers of two >= 2N)
     int Hx = 0, Hy = 0, Hz = 0;          // P/2 + 1 (independent octant of Fg)
     int ncx = 0, ncy = 0, ncz = 0, ncubes = 0;
-    int T = 0;
+    int nb = 1;                          // basis functions per tet: 1 (constant), 4 (linear, as pseudo-tets)
+    int T = 0;                           // tets, or pseudo-tets (4 per tet) for the linear basis
     long long n = 0;                     // 3T unknowns
     double k = 0.0;
     bool have_k = false;

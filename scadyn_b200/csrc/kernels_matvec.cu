@@ -16,26 +16,29 @@
 
 #include "ctx.h"
 #include "fft_reg.cuh"
+#include "linear_basis.h"
 
 namespace {
 
 constexpr int WARPS_PER_CTA = 4;
 
+// slot order <-> the reference's unknown order (nb basis functions per tet:
+// 1, or 4 for the linear basis, see linear_basis.h)
 __global__ void k_permute_in(const cd *__restrict__ xo, cd *__restrict__ xs, const int *__restrict__ perm,
-                             int T, long long ld) {
+                             int T, long long ld, int nb) {
     const int r = blockIdx.y;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 3LL * T; i += (long long)gridDim.x * blockDim.x) {
         long long s = i / 3, d = i - 3 * s;
-        xs[r * ld + i] = xo[r * ld + 3LL * perm[s] + d];
+        xs[r * ld + i] = xo[r * ld + basis_unknown(nb, perm[s], (int)d)];
     }
 }
 
 __global__ void k_permute_out(const cd *__restrict__ xs, cd *__restrict__ xo, const int *__restrict__ perm,
-                              int T, long long ld) {
+                              int T, long long ld, int nb) {
     const int r = blockIdx.y;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 3LL * T; i += (long long)gridDim.x * blockDim.x) {
         long long s = i / 3, d = i - 3 * s;
-        xo[r * ld + 3LL * perm[s] + d] = xs[r * ld + i];
+        xo[r * ld + basis_unknown(nb, perm[s], (int)d)] = xs[r * ld + i];
     }
 }
 
@@ -968,12 +971,12 @@ int ensure_work_single(scd_ctx *c, int nrhs) {
 
 void launch_permute_in(scd_ctx *c, const cd *x_orig, cd *x_slot, int nrhs, long long ld) {
     dim3 grid((unsigned)std::min<long long>((3LL * c->T + 255) / 256, 4096), nrhs);
-    k_permute_in<<<grid, 256, 0, c->st>>>(x_orig, x_slot, c->d_perm, c->T, ld);
+    k_permute_in<<<grid, 256, 0, c->st>>>(x_orig, x_slot, c->d_perm, c->T, ld, c->nb);
 }
 
 void launch_permute_out(scd_ctx *c, const cd *x_slot, cd *x_orig, int nrhs, long long ld) {
     dim3 grid((unsigned)std::min<long long>((3LL * c->T + 255) / 256, 4096), nrhs);
-    k_permute_out<<<grid, 256, 0, c->st>>>(x_slot, x_orig, c->d_perm, c->T, ld);
+    k_permute_out<<<grid, 256, 0, c->st>>>(x_slot, x_orig, c->d_perm, c->T, ld, c->nb);
 }
 
 void launch_fft_chain(scd_ctx *c, const cd *x, int nrhs, const int *done) { fft_chain_t<cd>(c, x, nrhs, done); }

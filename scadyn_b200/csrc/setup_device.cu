@@ -883,6 +883,7 @@ int scd_grid_from_mesh(int32_t Nv, const double *coord, int32_t T, const int32_t
 
 int scd_set_mesh(scd_ctx *c, int32_t Nv, const double *coord, const int32_t *etopol, const scd_c128 *param) {
     if (!c) return SCD_BAD_ARG;
+    if (c->nb != 1) return set_error(c, SCD_BAD_ARG, "scd_set_mesh: constant basis only");
     cudaSetDevice(c->dev);
     if (!coord || !etopol || !param || Nv < 4) return set_error(c, SCD_BAD_ARG, "bad mesh arrays");
     c->Nv = Nv;
@@ -929,12 +930,14 @@ int scd_set_mesh(scd_ctx *c, int32_t Nv, const double *coord, const int32_t *eto
 
 int scd_build_projectors(scd_ctx *c) {
     if (!c) return SCD_BAD_ARG;
+    if (c->nb != 1) return set_error(c, SCD_BAD_ARG, "scd_build_projectors: constant basis only");
     cudaSetDevice(c->dev);
     return setup_projectors_device(c);
 }
 
 int scd_build_nearzone(scd_ctx *c, int32_t prec) {
     if (!c) return SCD_BAD_ARG;
+    if (c->nb != 1) return set_error(c, SCD_BAD_ARG, "scd_build_nearzone: constant basis only");
     cudaSetDevice(c->dev);
     return setup_nearzone_device(c, prec);
 }
@@ -980,6 +983,7 @@ int64_t scd_nearzone_count(scd_ctx *c) {
 // export in the reference layout, ordered by (tet_T, tet_B), widened to FP64
 int scd_get_nearzone(scd_ctx *c, int64_t B, scd_c128 *sp, int32_t *ind) {
     if (!c || !sp || !ind) return SCD_BAD_ARG;
+    if (c->nb != 1) return set_error(c, SCD_BAD_ARG, "scd_get_nearzone: constant basis only");
     cudaSetDevice(c->dev);
     if (!c->have_near) return set_error(c, SCD_NOT_READY, "near zone not set");
     if (B != scd_nearzone_count(c)) return set_error(c, SCD_BAD_ARG, "B = %lld, the near zone has %lld", (long long)B,
@@ -1025,6 +1029,7 @@ int scd_get_nearzone(scd_ctx *c, int64_t B, scd_c128 *sp, int32_t *ind) {
 
 int scd_vswf_rhs(scd_ctx *c, int32_t Nmax, scd_c128 *mat) {
     if (!c || !mat) return SCD_BAD_ARG;
+    if (c->nb != 1) return set_error(c, SCD_BAD_ARG, "scd_vswf_rhs: constant basis only");
     cudaSetDevice(c->dev);
     const int nm = (Nmax + 1) * (Nmax + 1) - 1;
     cd *d = nullptr;

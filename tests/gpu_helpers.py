@@ -4,9 +4,9 @@ from scadyn_b200 import api
 
 def solver_from_oracle(op, device=0, fg_from_host=False):
     """Load an oracle operator into a device Solver so that both sides see the
-    same operator data."""
+    same operator data (constant or linear basis, op.order)."""
     g = op.geom
-    s = api.Solver(g.Nx, g.Ny, g.Nz, g.delta, g.min_coord, g.T, device)
+    s = api.Solver(g.Nx, g.Ny, g.Nz, g.delta, g.min_coord, g.T, device, order=getattr(op, "order", 0))
     s.set_wavenumber(g.k)
     s.set_projectors(op.S, op.Sx, op.Sy, op.Sz, op.indS)
     s.build_G(op.Fg if fg_from_host else None)
