@@ -253,9 +253,13 @@ def main():
                     help="only build the operator and run profile_matvec (for ncu captures)")
     ap.add_argument("--near-mma", action="store_true",
                     help="tensor-core near zone for the complex64 matvec (SCADYN_NEAR_MMA=1)")
+    ap.add_argument("--cgs", action="store_true",
+                    help="classical Gram-Schmidt for the complex64 inner solves (SCADYN_CGS=1)")
     args = ap.parse_args()
     if args.near_mma:
         os.environ["SCADYN_NEAR_MMA"] = "1"
+    if args.cgs:
+        os.environ["SCADYN_CGS"] = "1"
     if args.serve:
         print(json.dumps(serve_bench(args.serve)), flush=True)
         return
@@ -485,6 +489,7 @@ def main():
                                                                             cfg["tol"]),
                        "l2": "inputs larger than L2 (near-zone tiles %.2f GB per matvec)" % (solver.nearzone_bytes() / 1e9),
                        "near_zone": "tensor cores (f16 hi/lo)" if args.near_mma else "CUDA cores",
+                       "inner_gram_schmidt": "classical, conditional re-orthogonalisation" if args.cgs else "modified",
                        "parallelism": f"replicas x{world}"},
             "t_rel_err_vs_fp64": t_err,
             "p50_ms": round(float(np.percentile(lat_s, 50)), 3),

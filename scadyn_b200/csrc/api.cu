@@ -362,6 +362,8 @@ int scd_create(scd_ctx **out, const scd_grid_desc *d) {
     {
         const char *e = getenv("SCADYN_NEAR_MMA");
         c->nzm_on = e && e[0] == '1';
+        e = getenv("SCADYN_CGS");
+        c->cgs_on = e && e[0] == '1';
     }
     cudaSetDevice(c->dev);
     cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev);

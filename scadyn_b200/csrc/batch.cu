@@ -59,6 +59,9 @@ struct TickArgs {
     int m, max_cycles;
     double tol;
     int mixed;      // inner solve of the mixed form: finish -> INNER_DONE
+    int cgs;        // classical Gram-Schmidt for the Arnoldi steps (complex64 inner solves, opt-in)
+    double *cpm;    // cgs: [slot][NCH][CGS_NV] chunk partials of the dots
+    double *ctm;    // cgs: [slot][CGS_NV] slot totals
 };
 
 // vector elements in FP64 for arithmetic, rounded back on store
@@ -86,6 +89,9 @@ constexpr int TU = 4;
 // on n and the grid only -- never on which other slots are active -- and
 // each warp streams long contiguous runs (deep memory-level parallelism).
 constexpr int NCH = 512;
+// values per slot of the classical Gram-Schmidt reduction: <v_k, w> for k <=
+// SCD_M_MAX (two doubles each) and ||w||^2
+constexpr int CGS_NV = 2 * SCD_M_MAX + 2;
 
 struct Chunks {
     long long L;    // chunk length
@@ -273,6 +279,65 @@ __device__ void cycle_end(const TickArgs<C> &a, const Chunks &ch, int nch, const
     }
 }
 
+// Classical Gram-Schmidt, first pass, chunk c of slot s: the dots <v_k, w>,
+// k = 1..i, and ||w||^2 in one sweep over the chunk (w is re-read from cache
+// for each k), published per chunk; the slot's last warp sums the NCH chunk
+// partials of every value in chunk order into ctm.
+template <typename C, int TUC>
+__device__ __forceinline__ void cgs_dots(const TickArgs<C> &a, int s, int c, int i, const C *Vs, const C *ws,
+                                         long long qa, long long qb, int lane) {
+    const long long n = a.n;
+    double *pp = a.cpm + ((size_t)s * NCH + c) * CGS_NV;
+    double nw = 0.0;
+    for (int k = 1; k <= i; ++k) {
+        const C *vk = Vs + (size_t)(k - 1) * n;
+        double d[2] = {0.0, 0.0};
+        for (long long q = qa + lane; q < qb; q += 32 * TUC) {
+            C w[TUC], z[TUC];
+#pragma unroll
+            for (int e = 0; e < TUC; ++e) {
+                const long long qq = q + 32 * e;
+                w[e] = z[e] = C{};
+                if (qq < qb) { w[e] = ws[qq]; z[e] = vk[qq]; }
+            }
+#pragma unroll
+            for (int e = 0; e < TUC; ++e) {
+                if (q + 32 * e >= qb) break;
+                const cd wv = to_cd(w[e]);
+                cdot_acc(d[0], d[1], to_cd(z[e]), wv);
+                if (k == 1) nw += cabs2(wv);
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) d[h] += __shfl_xor_sync(0xffffffffu, d[h], o);
+        if (lane == 0) { pp[2 * (k - 1)] = d[0]; pp[2 * (k - 1) + 1] = d[1]; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nw += __shfl_xor_sync(0xffffffffu, nw, o);
+    int last = 0;
+    if (lane == 0) {
+        pp[CGS_NV - 1] = nw;
+        __threadfence();
+        last = atomicAdd(&a.ccnt[s], 1) == NCH - 1;
+    }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (!last) return;
+    __threadfence();
+    double *tt = a.ctm + (size_t)s * CGS_NV;
+    for (int v = 0; v < CGS_NV; ++v) {
+        if (v >= 2 * i && v != CGS_NV - 1) continue;
+        double t = 0.0;
+#pragma unroll
+        for (int j = 0; j < NCH / 32; ++j) t += __ldcg(a.cpm + ((size_t)s * NCH + lane + 32 * j) * CGS_NV + v);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if (lane == 0) tt[v] = t;
+    }
+    if (lane == 0) a.ccnt[s] = 0;
+}
+
 // One tick: cycle starts (r = rhs - A x, V0 = r/||r||) and Arnoldi steps
 // (MGS, normalisation, Givens) for every active slot; cycle ends update x.
 template <typename C>
@@ -329,6 +394,9 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
                     v[1] += cabs2(b[u]);
                 }
             }
+        } else if (a.cgs) {
+            cgs_dots<C, TUC>(a, s, c, sstep[s] + 1, V0, ws, qa, qb, lane);
+            continue;
         } else {
             for (long long q = qa + lane; q < qb; q += 32 * TUC) {
                 cd w[TUC], z[TUC];
@@ -348,15 +416,20 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
         }
         chunk_done<3>(a, s, c, v, parity, lane);
     }
-    for (int s = threadIdx.x; s < a.ns; s += blockDim.x) sact[s] = smode[s] == SLOT_START || smode[s] == SLOT_ARNOLDI;
+    for (int s = threadIdx.x; s < a.ns; s += blockDim.x)
+        sact[s] = smode[s] == SLOT_START || (smode[s] == SLOT_ARNOLDI && !a.cgs);
     grid_barrier(a.bar, gridDim.x, a.err);
     load_totals(a, parity, 3, sact, tot);
     int kmax = 0;
     for (int s = 0; s < a.ns; ++s) {
-        if (smode[s] == SLOT_ARNOLDI) kmax = max(kmax, sstep[s] + 1);
+        if (smode[s] == SLOT_ARNOLDI && !a.cgs) kmax = max(kmax, sstep[s] + 1);
         if (threadIdx.x == 0) {
-            snormav[s] = sqrt(tot[s][0]);
-            sh_h[s] = cmk(tot[s][1], tot[s][2]);
+            if (smode[s] == SLOT_ARNOLDI && a.cgs) {
+                snormav[s] = sqrt(__ldcg(a.ctm + (size_t)s * CGS_NV + CGS_NV - 1));
+            } else {
+                snormav[s] = sqrt(tot[s][0]);
+                sh_h[s] = cmk(tot[s][1], tot[s][2]);
+            }
         }
     }
     __syncthreads();
@@ -450,6 +523,60 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
                 if (k == sstep[s] + 1) shn[s] = sqrt(tot[s][0]);
             }
         }
+        __syncthreads();
+    }
+    // ---- classical Gram-Schmidt update: w -= sum_k h_k v_k (k ascending,
+    // FP64 per element, one rounding to the storage precision), ||w||^2
+    if (a.cgs) {
+        cd *hs = ysm[threadIdx.x >> 5];
+        for (int it = ch.gw; it < nitems; it += ch.nw) {
+            const int s = it / NCH, c = it - s * NCH;
+            if (smode[s] != SLOT_ARNOLDI) continue;
+            const int i = sstep[s] + 1;
+            const double *tt = a.ctm + (size_t)s * CGS_NV;
+            for (int k = lane; k < i; k += 32) hs[k] = cmk(__ldcg(tt + 2 * k), __ldcg(tt + 2 * k + 1));
+            __syncwarp();
+            if (c == 0 && lane == 0)
+                for (int k = 0; k < i; ++k) a.H[(size_t)s * ldh * a.m + (size_t)ldh * (i - 1) + k] = hs[k];
+            const long long qa = c * ch.L, qb = min(n, qa + ch.L);
+            C *ws = a.w + (size_t)swpos[s] * n;
+            const C *Vs = a.V + (size_t)s * (a.m + 1) * n;
+            double u[1] = {0.0};
+            for (long long q = qa + lane; q < qb; q += 32 * TUC) {
+                cd acc[TUC];
+#pragma unroll
+                for (int e = 0; e < TUC; ++e) {
+                    const long long qq = q + 32 * e;
+                    acc[e] = qq < qb ? to_cd(ws[qq]) : cmk(0, 0);
+                }
+                for (int k = 0; k < i; ++k) {
+                    const cd hk = hs[k];
+                    const C *vk = Vs + (size_t)k * n;
+                    C p[TUC];
+#pragma unroll
+                    for (int e = 0; e < TUC; ++e) {
+                        const long long qq = q + 32 * e;
+                        p[e] = qq < qb ? vk[qq] : C{};
+                    }
+#pragma unroll
+                    for (int e = 0; e < TUC; ++e) csub_mul(acc[e], hk, to_cd(p[e]));
+                }
+#pragma unroll
+                for (int e = 0; e < TUC; ++e) {
+                    const long long qq = q + 32 * e;
+                    if (qq >= qb) break;
+                    store_c(ws[qq], acc[e]);
+                    u[0] += cabs2(rounded<C>(acc[e]));
+                }
+            }
+            __syncwarp();
+            chunk_done<1>(a, s, c, u, parity ^ 1, lane);
+        }
+        for (int s = threadIdx.x; s < a.ns; s += blockDim.x) sact[s] = smode[s] == SLOT_ARNOLDI;
+        parity ^= 1;
+        grid_barrier(a.bar, gridDim.x, a.err);
+        load_totals(a, parity, 1, sact, tot);
+        if (threadIdx.x < a.ns && sact[threadIdx.x]) shn[threadIdx.x] = sqrt(tot[threadIdx.x][0]);
         __syncthreads();
     }
     // ---- conditional re-orthogonalisation (src/gmres_module.f90:251-258)
@@ -726,13 +853,14 @@ struct BatchBuffers {
     Slot *h_slots = nullptr;
     double *red = nullptr;
     double *cpart = nullptr, *ctot = nullptr;
+    double *cpm = nullptr, *ctm = nullptr;   // classical Gram-Schmidt reductions (opt-in)
     int *ccnt = nullptr;
     int grid = 0;
 };
 
 static void free_bb(BatchBuffers &b) {
     void *p[] = {b.V, b.H, b.cs, b.sn, b.g, b.y, b.x, b.rhs, b.Xin, b.W, b.x64, b.b64, b.Xin64, b.W64,
-                 b.slots, b.red, b.cpart, b.ctot, b.ccnt};
+                 b.slots, b.red, b.cpart, b.ctot, b.ccnt, b.cpm, b.ctm};
     for (void *q : p) if (q) cudaFree(q);
     if (b.h_slots) cudaFreeHost(b.h_slots);
     b = BatchBuffers();
@@ -746,7 +874,8 @@ void batch_free(scd_ctx *c) {
 }
 
 int batch_prepare(scd_ctx *c, int ns, int m, int mixed, BatchBuffers &b) {
-    if (b.ns >= ns && b.m >= m && b.n == c->n && b.mixed == mixed && b.V) return SCD_OK;
+    if (b.ns >= ns && b.m >= m && b.n == c->n && b.mixed == mixed && b.V && (!(mixed && c->cgs_on) || b.cpm))
+        return SCD_OK;
     free_bb(b);
     const long long n = c->n;
     const size_t es = mixed ? sizeof(cf) : sizeof(cd);
@@ -775,6 +904,10 @@ int batch_prepare(scd_ctx *c, int ns, int m, int mixed, BatchBuffers &b) {
     if ((rc = al((void **)&b.cpart, sizeof(double) * (size_t)NSMAX * NCH * 4, "chunk partials"))) return rc;
     if ((rc = al((void **)&b.ctot, sizeof(double) * 2 * NSMAX * 4, "slot totals"))) return rc;
     if ((rc = al((void **)&b.ccnt, sizeof(int) * NSMAX, "chunk counters"))) return rc;
+    if (mixed && c->cgs_on) {
+        if ((rc = al((void **)&b.cpm, sizeof(double) * (size_t)ns * NCH * CGS_NV, "Gram-Schmidt partials"))) return rc;
+        if ((rc = al((void **)&b.ctm, sizeof(double) * (size_t)ns * CGS_NV, "Gram-Schmidt totals"))) return rc;
+    }
 
     if (cudaMallocHost((void **)&b.h_slots, sizeof(Slot) * ns) != cudaSuccess) return set_error(c, SCD_OOM, "pinned slots");
     int per_sm = 0, per_sm2 = 0;
@@ -801,6 +934,8 @@ static int launch_tick(scd_ctx *c, BatchBuffers &bb, int ns, int nact, int m, in
     a.x = (C *)bb.x; a.rhs = (C *)bb.rhs; a.w = (C *)bb.W; a.red = bb.red; a.bar = c->d_bar; a.err = c->d_err;
     a.cpart = bb.cpart; a.ctot = bb.ctot; a.ccnt = bb.ccnt;
     a.n = c->n; a.m = m; a.max_cycles = cycles; a.tol = tol; a.mixed = mixed;
+    a.cgs = (mixed && c->cgs_on && bb.cpm) ? 1 : 0;
+    a.cpm = bb.cpm; a.ctm = bb.ctm;
     const long long n = c->n;
     if (nact > 0) {
         k_stage<C><<<dim3(std::min<long long>((n + 255) / 256, 1024), ns), 256, 0, c->st>>>(bb.slots, ns, (C *)bb.V,

@@ -140,6 +140,9 @@ struct scd_ctx {
     cf *f_bpart = nullptr, *f_W = nullptr, *f_R = nullptr, *f_nzpart = nullptr, *f_xT = nullptr;
     int f_cap = 0;
 
+    // classical Gram-Schmidt for the complex64 inner solves (batch.cu), opt-in
+    // by SCADYN_CGS=1 at context creation
+    bool cgs_on = false;
     // tensor-core near zone of the complex64 matvec (near_mma.cu), opt-in by
     // SCADYN_NEAR_MMA=1 at context creation
     bool nzm_on = false, nzm_ready = false;
