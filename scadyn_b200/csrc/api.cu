@@ -45,6 +45,17 @@ static int next_pow2(int v) {
     return p;
 }
 
+// FFT length of an axis with N nodes: the smallest power of two >= 2N, or
+// (opt-in) the smallest length >= 2N among the powers of two and the 5-smooth
+// lengths with register transforms (80, 96, 192)
+static int fft_len(int v, bool smooth) {
+    const int p2 = next_pow2(v);
+    if (!smooth) return p2;
+    for (int p : {80, 96, 192})
+        if (p >= v && p < p2) return p;
+    return p2;
+}
+
 template <typename Tp>
 static int dalloc(scd_ctx *c, Tp **p, size_t count, const char *what) {
     if (*p) { cudaFree(*p); *p = nullptr; }
@@ -368,7 +379,11 @@ int scd_create(scd_ctx **out, const scd_grid_desc *d) {
     cudaSetDevice(c->dev);
     cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev);
     c->Nx = d->Nx; c->Ny = d->Ny; c->Nz = d->Nz;
-    c->Px = next_pow2(2 * d->Nx); c->Py = next_pow2(2 * d->Ny); c->Pz = next_pow2(2 * d->Nz);
+    {
+        const char *e = getenv("SCADYN_FFT_SMOOTH");
+        const bool smooth = e && e[0] == '1';
+        c->Px = fft_len(2 * d->Nx, smooth); c->Py = fft_len(2 * d->Ny, smooth); c->Pz = fft_len(2 * d->Nz, smooth);
+    }
     if (c->Px > 512 || c->Py > 512 || c->Pz > 512) {
         set_error(c, SCD_BAD_ARG, "grid %dx%dx%d needs an FFT longer than 512", d->Nx, d->Ny, d->Nz);
         *out = c;

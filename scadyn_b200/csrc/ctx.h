@@ -46,7 +46,7 @@ struct scd_ctx {
     cudaStream_t st = nullptr;
     scd_grid_desc d{};
     int Nx = 0, Ny = 0, Nz = 0;          // grid nodes
-    int Px = 0, Py = 0, Pz = 0;          // padded FFT lengths (powers of two >= 2N)
+    int Px = 0, Py = 0, Pz = 0;          // padded FFT lengths >= 2N (powers of two; 80, 96, 192 opt-in)
     int Hx = 0, Hy = 0, Hz = 0;          // P/2 + 1 (independent octant of Fg)
     int ncx = 0, ncy = 0, ncz = 0, ncubes = 0;
     int nb = 1;                          // basis functions per tet: 1 (constant), 4 (linear, as pseudo-tets)

@@ -15,6 +15,7 @@
 #include <type_traits>
 
 #include "ctx.h"
+#include "fft_mixed.cuh"
 #include "fft_reg.cuh"
 #include "linear_basis.h"
 
@@ -169,13 +170,22 @@ __device__ __forceinline__ void fft_line(C *s, const C *tw, int t) {
 }
 
 // Line FFT of the passes: register-resident 8-thread transform for P = 64
-// and 128 (fft_reg.cuh), shared-memory radix-4 Stockham for other lengths.
+// and 128 (fft_reg.cuh), register-resident mixed-radix transform with 4 or 8
+// threads for the 5-smooth lengths below (fft_mixed.cuh), shared-memory
+// radix-4 Stockham for other powers of two.
+// (N1 = P / threads <= 24 keeps the FP64 transforms within the register file)
+template <int P> constexpr bool fft_mixed_len() { return P == 80 || P == 96 || P == 192; }
+// lines per CTA halved until the line buffers fit 44 KB of static shared memory
+constexpr int fft_fit_lpb(int lpb, int ls, int es) { return (lpb > 1 && lpb * ls * es > 44 * 1024) ? fft_fit_lpb(lpb / 2, ls, es) : lpb; }
 template <int P, typename Cx> struct FftCfg {
     static constexpr bool REG = P == 64 || P == 128;
-    static constexpr int TPL = REG ? 8 : P / 4;              // threads per line
-    static constexpr int LPB = REG ? (sizeof(Cx) == 16 ? 16 : 32) : ((256 / TPL) > 0 ? 256 / TPL : 1);   // lines per CTA
-    static constexpr int THREADS = TPL * LPB;
+    static constexpr bool MIX = !REG && fft_mixed_len<P>();
     static constexpr int LS = P + (P >> 4) + 1;              // padded line stride (bank spread)
+    static constexpr int TPL = REG ? 8 : MIX ? (P % 64 == 0 ? 8 : 4) : P / 4;   // threads per line
+    static constexpr int LPB = REG ? (sizeof(Cx) == 16 ? 16 : 32)
+                               : MIX ? fft_fit_lpb(256 / TPL / (sizeof(Cx) == 16 ? 2 : 1), LS, (int)sizeof(Cx))
+                                     : ((256 / TPL) > 0 ? 256 / TPL : 1);   // lines per CTA
+    static constexpr int THREADS = TPL * LPB;
 };
 
 template <int P, bool INV, typename Cx>
@@ -183,6 +193,9 @@ __device__ __forceinline__ void fft_line_any(Cx *s, const Cx *tw, int t) {
     if constexpr (FftCfg<P, Cx>::REG) {
         fft_line_reg<P, INV, Cx>(s, tw, t);
         __syncthreads();   // the passes' next loops read every line of the CTA
+    } else if constexpr (FftCfg<P, Cx>::MIX) {
+        fft_line_mixed<P, FftCfg<P, Cx>::TPL, INV, Cx>(s, tw, t);
+        __syncthreads();
     } else {
         fft_line<P, INV, Cx>(s, tw, t);
     }
@@ -786,6 +799,9 @@ void fft_x_inv_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const 
         case 32: CALL(32); break;                    \
         case 64: CALL(64); break;                    \
         case 128: CALL(128); break;                  \
+        case 80: CALL(80); break;                    \
+        case 96: CALL(96); break;                    \
+        case 192: CALL(192); break;                  \
         case 256: CALL(256); break;                  \
         case 512: CALL(512); break;                  \
         default: break;                              \
