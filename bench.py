@@ -255,11 +255,15 @@ def main():
                     help="tensor-core near zone for the complex64 matvec (SCADYN_NEAR_MMA=1)")
     ap.add_argument("--cgs", action="store_true",
                     help="classical Gram-Schmidt for the complex64 inner solves (SCADYN_CGS=1)")
+    ap.add_argument("--fft-smooth", action="store_true",
+                    help="5-smooth padded FFT lengths (80, 96, 192) where shorter than a power of two (SCADYN_FFT_SMOOTH=1)")
     args = ap.parse_args()
     if args.near_mma:
         os.environ["SCADYN_NEAR_MMA"] = "1"
     if args.cgs:
         os.environ["SCADYN_CGS"] = "1"
+    if args.fft_smooth:
+        os.environ["SCADYN_FFT_SMOOTH"] = "1"
     if args.serve:
         print(json.dumps(serve_bench(args.serve)), flush=True)
         return
@@ -490,6 +494,7 @@ def main():
                        "l2": "inputs larger than L2 (near-zone tiles %.2f GB per matvec)" % (solver.nearzone_bytes() / 1e9),
                        "near_zone": "tensor cores (f16 hi/lo)" if args.near_mma else "CUDA cores",
                        "inner_gram_schmidt": "classical, conditional re-orthogonalisation" if args.cgs else "modified",
+                       "fft_lengths": [fft_len(2 * v, args.fft_smooth) for v in (desc.Nx, desc.Ny, desc.Nz)],
                        "parallelism": f"replicas x{world}"},
             "t_rel_err_vs_fp64": t_err,
             "p50_ms": round(float(np.percentile(lat_s, 50)), 3),
@@ -614,6 +619,19 @@ def sweep_bench(nw, nmax_cap):
             "wavelengths": per, "columns": st["columns"], "busy_s": round(st["busy_s"], 2),
             "wall_s": round(wall, 2), "p50_ms": round(st["p50_ms"], 1), "p99_ms": round(st["p99_ms"], 1),
             "peak_running": st["peak_running"], "peak_bytes": st["peak_bytes"]}
+
+
+def fft_len(v, smooth):
+    """Padded FFT length the library picks for 2N = v (power of two, or the
+    shorter of 80, 96, 192 with 5-smooth lengths enabled)."""
+    p2 = 8
+    while p2 < v:
+        p2 *= 2
+    if smooth:
+        for p in (80, 96, 192):
+            if v <= p < p2:
+                return p
+    return p2
 
 
 def matvec_roofline(solver, desc, T, Bref, peak, ms1, msb, nb):
