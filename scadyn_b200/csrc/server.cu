@@ -6,6 +6,7 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -62,6 +63,14 @@ int64_t estimate(const scd_request *r, const scd_grid_desc &d) {
     b += ns * n * (4.0 * es + 6.0 * 16.0 + (mixed ? 4.0 * 16.0 : 0.0));           // solver and work vectors
     b += n * ncol * 16.0;                                                         // incident columns
     b += 12.0 * T * 8.0 + T * 16.0;                                               // mesh on the device
+    {
+        // opt-in tensor-core near zone (mixed form, complex64 storage): f16
+        // hi/lo planes of every tile (8 B per complex plus padding) and a
+        // pass of x blocks
+        const char *e = getenv("SCADYN_NEAR_MMA");
+        if (e && e[0] == '1' && mixed && r->storage_prec != SCD_STORE_C128)
+            b += T * 250.0 * 9.0 * 8.0 * 1.3 + n * 128.0 * 1.3;   // x block: 32 rows x 2 B x hi/lo per unknown
+    }
     return (int64_t)(b * 1.1) + (64LL << 20);
 }
 
