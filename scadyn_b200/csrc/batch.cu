@@ -942,6 +942,7 @@ static int launch_tick(scd_ctx *c, BatchBuffers &bb, int ns, int nact, int m, in
                                                                                            (C *)bb.x, (C *)bb.Xin, n, m);
         run_matvec(c, (const C *)bb.Xin, (C *)bb.W, nact, nullptr);
     }
+    NvtxRange r("arnoldi tick");
     void *args[] = {&a};
     cudaMemsetAsync(bb.ccnt, 0, sizeof(int) * NSMAX, c->st);
     cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_tick<C>, dim3(bb.grid), dim3(BT), args, 0, c->st);
@@ -957,6 +958,7 @@ static int launch_tick(scd_ctx *c, BatchBuffers &bb, int ns, int nact, int m, in
 int batch_solve(scd_ctx *c, int ncol, const cd *const *rhs_cols, cd *X, double tol, int m, int cycles, int ns,
                 int *iters, int *conv_out, int *status_out, double *relres_out, int precision, double inner_tol,
                 int max_outer) {
+    NvtxRange range(precision == SCD_PREC_MIXED ? "batch solve (mixed)" : "batch solve (fp64)");
     if (!c->batch) c->batch = new BatchBuffers();
     BatchBuffers &bb = *(BatchBuffers *)c->batch;
     const int mixed = precision == SCD_PREC_MIXED ? 1 : 0;

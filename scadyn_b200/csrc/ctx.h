@@ -11,8 +11,19 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/scadyn_gpu.h"
 #include "common.cuh"
+
+// NVTX range for the lifetime of a scope (host side; a no-op unless a
+// profiler is attached)
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // Near-zone groups: runs of consecutive slots of one projection box (cube)
 // holding at most SCD_GROUP_MAX tets; a box with more tets is split into

@@ -915,11 +915,20 @@ void gather_t(scd_ctx *c, C *y, int nrhs, const int *done) {
 template <typename C>
 void run_matvec_t(scd_ctx *c, const C *x, C *y, int nrhs, const int *done) {
     if (c->timing) cudaEventRecord(c->ev[0], c->st);
-    near_t<C>(c, x, nrhs, done);
+    {
+        NvtxRange r("near zone");
+        near_t<C>(c, x, nrhs, done);
+    }
     if (c->timing) cudaEventRecord(c->ev[1], c->st);
-    fft_chain_t<C>(c, x, nrhs, done);
+    {
+        NvtxRange r("fft convolutions");
+        fft_chain_t<C>(c, x, nrhs, done);
+    }
     if (c->timing) cudaEventRecord(c->ev[2], c->st);
-    gather_t<C>(c, y, nrhs, done);
+    {
+        NvtxRange r("gather");
+        gather_t<C>(c, y, nrhs, done);
+    }
     if (c->timing) cudaEventRecord(c->ev[3], c->st);
 }
 

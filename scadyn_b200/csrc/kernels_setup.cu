@@ -102,6 +102,7 @@ __global__ void k_tgemm_reduce(const cd *part, int nsplit, int ncol, int ncb, cd
 }  // namespace
 
 int setup_green(scd_ctx *c, const scd_c128 *Fg) {
+    NvtxRange range("Green octant");
     const long long oct = (long long)c->Hx * c->Hy * c->Hz;
     cd *tmp = nullptr;
     if (c->d_Fo) { cudaFree(c->d_Fo); c->d_Fo = nullptr; }

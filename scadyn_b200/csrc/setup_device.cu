@@ -745,6 +745,7 @@ void tet_vertices(const scd_ctx *c, int t, double out[12]) {
 int set_order_from_cubes(scd_ctx *c, const std::vector<int> &cube_of_tet);
 
 int setup_projectors_device(scd_ctx *c) {
+    NvtxRange range("projectors build");
     if (!c->have_mesh) return set_error(c, SCD_NOT_READY, "scd_build_projectors needs scd_set_mesh");
     if (!c->have_k) return set_error(c, SCD_NOT_READY, "scd_build_projectors needs scd_set_wavenumber");
     int rc = upload_quadrature(c);
@@ -803,6 +804,7 @@ int setup_projectors_device(scd_ctx *c) {
 int build_tile_layout(scd_ctx *c);
 
 int setup_nearzone_device(scd_ctx *c, int prec) {
+    NvtxRange range("near-zone build");
     if (!c->have_mesh) return set_error(c, SCD_NOT_READY, "scd_build_nearzone needs scd_set_mesh");
     if (!c->have_proj) return set_error(c, SCD_NOT_READY, "scd_build_nearzone needs the projectors");
     if (!c->have_k) return set_error(c, SCD_NOT_READY, "scd_build_nearzone needs scd_set_wavenumber");
@@ -837,6 +839,7 @@ int setup_nearzone_device(scd_ctx *c, int prec) {
 }
 
 int setup_vswf(scd_ctx *c, int Nmax, cd *d_mat) {
+    NvtxRange range("VSWF columns");
     if (!c->have_mesh) return set_error(c, SCD_NOT_READY, "VSWF right-hand sides need scd_set_mesh");
     if (!c->have_k) return set_error(c, SCD_NOT_READY, "VSWF right-hand sides need scd_set_wavenumber");
     if (Nmax < 1 || Nmax > VSWF_NMAX - 2) return set_error(c, SCD_BAD_ARG, "Nmax %d outside 1..%d", Nmax, VSWF_NMAX - 2);
