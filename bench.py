@@ -251,15 +251,15 @@ def main():
     ap.add_argument("--sweep-nmax", type=int, default=14, help="largest Nmax of the sweep (C3: 14)")
     ap.add_argument("--profile", default=None, choices=["near1", "near16", "mixed16", "solve16"],
                     help="only build the operator and run profile_matvec (for ncu captures)")
-    ap.add_argument("--near-mma", action="store_true",
-                    help="tensor-core near zone for the complex64 matvec (SCADYN_NEAR_MMA=1)")
+    ap.add_argument("--near-mma", nargs="?", const="1", default=None, choices=["1", "2"],
+                    help="tensor-core near zone for the complex64 matvec (SCADYN_NEAR_MMA=1; 2: merged schedule)")
     ap.add_argument("--cgs", action="store_true",
                     help="classical Gram-Schmidt for the complex64 inner solves (SCADYN_CGS=1)")
     ap.add_argument("--fft-smooth", action="store_true",
                     help="5-smooth padded FFT lengths (80, 96, 192) where shorter than a power of two (SCADYN_FFT_SMOOTH=1)")
     args = ap.parse_args()
     if args.near_mma:
-        os.environ["SCADYN_NEAR_MMA"] = "1"
+        os.environ["SCADYN_NEAR_MMA"] = args.near_mma
     if args.cgs:
         os.environ["SCADYN_CGS"] = "1"
     if args.fft_smooth:
@@ -492,7 +492,8 @@ def main():
                                     "stored complex64 as the reference)" % (cfg["inner_m"], cfg["inner_tol"],
                                                                             cfg["tol"]),
                        "l2": "inputs larger than L2 (near-zone tiles %.2f GB per matvec)" % (solver.nearzone_bytes() / 1e9),
-                       "near_zone": "tensor cores (f16 hi/lo)" if args.near_mma else "CUDA cores",
+                       "near_zone": ("tensor cores (f16 hi/lo, %s schedule)" % ("merged" if args.near_mma == "2" else "split"))
+                                    if args.near_mma else "CUDA cores",
                        "inner_gram_schmidt": "classical, conditional re-orthogonalisation" if args.cgs else "modified",
                        "fft_lengths": [fft_len(2 * v, args.fft_smooth) for v in (desc.Nx, desc.Ny, desc.Nz)],
                        "parallelism": f"replicas x{world}"},

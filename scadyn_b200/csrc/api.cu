@@ -372,7 +372,8 @@ int scd_create(scd_ctx **out, const scd_grid_desc *d) {
     c->dev = d->device;
     {
         const char *e = getenv("SCADYN_NEAR_MMA");
-        c->nzm_on = e && e[0] == '1';
+        c->nzm_on = e && (e[0] == '1' || e[0] == '2');
+        c->nzm_sched = (e && e[0] == '2') ? 1 : 0;
         e = getenv("SCADYN_CGS");
         c->cgs_on = e && e[0] == '1';
     }

@@ -157,6 +157,7 @@ struct scd_ctx {
     // tensor-core near zone of the complex64 matvec (near_mma.cu), opt-in by
     // SCADYN_NEAR_MMA=1 at context creation
     bool nzm_on = false, nzm_ready = false;
+    int nzm_sched = 0;                   // instruction schedule (near_mma.cuh): 0 split, 1 merged (SCADYN_NEAR_MMA=2)
     unsigned char *d_t16 = nullptr;      // f16 hi/lo planes of every tile
     long long *d_t16_off = nullptr;      // per tile byte offset
     unsigned char *d_xb = nullptr;       // x blocks of one pass

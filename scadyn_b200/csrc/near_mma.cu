@@ -20,7 +20,6 @@ namespace {
 
 constexpr int NZM_SLOTS = 8;
 constexpr int NZM_THREADS = 192;          // warp 0 producer, warp 1 MMA issuer, warps 2-5 epilogue
-constexpr uint32_t NZM_TMEM_COLS = 128;   // row product + two transposed buffers of NZM_N columns
 constexpr uint32_t NZM_META = 256;
 constexpr size_t NZM_SMEM = 113 * 1024;   // two CTAs per SM
 
@@ -72,23 +71,73 @@ __device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
 }
 
 // issue every instruction of one product (use 0: row, 1: transposed)
+template <int S>
 __device__ __forceinline__ void issue_product(int use, int n1, int n2, uint32_t tile, uint32_t xblk, uint32_t dcol,
                                               bool overwrite) {
     const int ks = nzm_ksteps(use, n1, n2);
-    for (int kk = 0; kk < ks; ++kk)
+    if constexpr (S == 0) {
+        for (int kk = 0; kk < ks; ++kk)
 #pragma unroll
-        for (int s = 0; s < NZM_SPLITS; ++s)
+            for (int s = 0; s < NZM_SPLITS; ++s)
 #pragma unroll
-            for (int q = 0; q < NZM_OPS; ++q) {
-                const NzmOp o = nzm_op(use, n1, n2, kk, s, q);
-                const uint64_t da = nzm_sdesc(tile + o.a_off, o.a_lbo, o.a_sbo);
-                const uint64_t db = nzm_sdesc(xblk + o.b_off, o.b_lbo, o.b_sbo);
-                tc_mma(dcol + (uint32_t)o.d_col, da, db, nzm_idesc(o), (overwrite && o.first) ? 0u : 1u);
-            }
+                for (int q = 0; q < NZM_OPS; ++q) {
+                    const NzmOp o = nzm_op(use, n1, n2, kk, s, q);
+                    const uint64_t da = nzm_sdesc(tile + o.a_off, o.a_lbo, o.a_sbo);
+                    const uint64_t db = nzm_sdesc(xblk + o.b_off, o.b_lbo, o.b_sbo);
+                    tc_mma(dcol + (uint32_t)o.d_col, da, db, nzm_idesc(o), (overwrite && o.first) ? 0u : 1u);
+                }
+    } else {
+        // descriptors of K step 0, then constant start-address steps (the
+        // 14-bit address field cannot carry: shared addresses stay below 2^18)
+        constexpr int NOP = NzmSched<S>::PARTS * NZM_OPS;
+        uint64_t da[NOP], db[NOP];
+        uint32_t id[NOP], dc[NOP];
+#pragma unroll
+        for (int j = 0; j < NOP; ++j) {
+            const NzmOp o = nzm_op_s<S>(use, n1, n2, 0, j / NZM_OPS, j % NZM_OPS);
+            da[j] = nzm_sdesc(tile + o.a_off, o.a_lbo, o.a_sbo);
+            db[j] = nzm_sdesc(xblk + o.b_off, o.b_lbo, o.b_sbo);
+            id[j] = nzm_idesc(o);
+            dc[j] = dcol + (uint32_t)o.d_col;
+        }
+        const uint64_t sa = nzm_a_step(use, n2) >> 4, sb = NZM_B_STEP >> 4;
+        for (int kk = 0; kk < ks; ++kk)
+#pragma unroll
+            for (int j = 0; j < NOP; ++j)
+                tc_mma(dc[j], da[j] + (uint64_t)kk * sa, db[j] + (uint64_t)kk * sb, id[j],
+                       (overwrite && kk == 0 && j == 0) ? 0u : 1u);
+    }
+}
+
+// a lane's accumulator row of a product (all lanes of the warp take part)
+template <int S>
+__device__ __forceinline__ void load_rows(uint32_t taddr, float (&v)[32], float (&w)[32]) {
+    tc_ld32(taddr, v);
+    if constexpr (S == 1) tc_ld32(taddr + 32, w);
+}
+
+// that row as the complex y_r of the pass's right-hand sides, scaled by
+// xinv, written to part[(r0 + r) * part_len + base + row]
+template <int S>
+__device__ __forceinline__ void store_rows(const NzmArgs &a, const float (&v)[32], const float (&w)[32], int row_ok,
+                                           int row, long long base) {
+    if (!row_ok) return;
+#pragma unroll
+    for (int r = 0; r < NZM_R; ++r) {
+        if (r >= a.rg || (a.skip && a.skip[a.r0 + r])) continue;
+        const float sc = a.xinv[r];
+        float re, im;
+        if constexpr (S == 0) { re = v[r]; im = v[NZM_R + r]; }
+        else { re = v[r] + v[NZM_R + r]; im = w[r] + w[NZM_R + r]; }
+        a.part[(long long)(a.r0 + r) * a.part_len + base + row] = make_float2(re * sc, im * sc);
+    }
 }
 
 // one CTA per near-zone group, one pass of up to NZM_R right-hand sides
+template <int S>
 __global__ void __launch_bounds__(NZM_THREADS, 2) k_near_mma(NzmArgs a) {
+    constexpr uint32_t NZM_TMEM_COLS = NzmSched<S>::TMEM;   // row product + two transposed buffers
+    constexpr uint32_t DC = NzmSched<S>::DCOLS;
     extern __shared__ unsigned char nzm_raw[];
     // 128-byte aligned base: core matrices and bulk copies start on 16-byte
     // boundaries, slots on 128-byte boundaries
@@ -154,9 +203,9 @@ __global__ void __launch_bounds__(NZM_THREADS, 2) k_near_mma(NzmArgs a) {
                 const uint32_t mb = nzm_tile_bytes(tl.n1, tl.n2);
                 const uint32_t xb = nzm_xblock_bytes(tl.n2);
                 const uint32_t x1b = t == t0 ? nzm_xblock_bytes(n1) : 0u;
-                const uint32_t S = mb + xb;
-                bool fit = head + S <= R;
-                uint32_t res = fit ? S : (R - head) + S;
+                const uint32_t SZ = mb + xb;
+                bool fit = head + SZ <= R;
+                uint32_t res = fit ? SZ : (R - head) + SZ;
                 while (ok && count > 0 && (count == NZM_SLOTS || used + res > R)) {
                     const int k = oldest % NZM_SLOTS;
                     ok = mbar_wait(&empty[k], (uint32_t)((oldest / NZM_SLOTS) & 1), a.err);
@@ -165,15 +214,15 @@ __global__ void __launch_bounds__(NZM_THREADS, 2) k_near_mma(NzmArgs a) {
                     --count;
                 }
                 if (!ok) break;
-                if (count == 0) { head = 0; used = 0; fit = true; res = S; }
+                if (count == 0) { head = 0; used = 0; fit = true; res = SZ; }
                 const uint32_t st = fit ? head : 0u;
                 const int k = ord % NZM_SLOTS;
                 toff[k] = st;
-                mbar_expect_tx(&full[k], S + x1b);
+                mbar_expect_tx(&full[k], SZ + x1b);
                 bulk_g2s(ring + st, a.t16 + a.t16_off[t], mb, &full[k]);
                 bulk_g2s(ring + st + mb, a.xb + a.xb_off[tl.g2], xb, &full[k]);
                 if (x1b) bulk_g2s(X1, a.xb + a.xb_off[g], x1b, &full[k]);
-                head = st + S;
+                head = st + SZ;
                 used += res;
                 resv[k] = res;
                 ++count;
@@ -195,12 +244,12 @@ __global__ void __launch_bounds__(NZM_THREADS, 2) k_near_mma(NzmArgs a) {
                 tc_fence_after();
                 const uint32_t tile = smem_addr(ring + toff[k]);
                 const uint32_t xblk = tile + nzm_tile_bytes(n1, tl.n2);
-                issue_product(0, n1, tl.n2, tile, xblk, tbase, t == t0);
+                issue_product<S>(0, n1, tl.n2, tile, xblk, tbase, t == t0);
                 if (tl.col_off >= 0) {
                     const int b = tcount & 1;
                     if (!(ok = mbar_wait(&tempty[b], (uint32_t)(((tcount >> 1) & 1) ^ 1), a.err))) break;
                     tc_fence_after();
-                    issue_product(1, n1, tl.n2, tile, smem_addr(X1), tbase + (uint32_t)NZM_N * (1 + b), true);
+                    issue_product<S>(1, n1, tl.n2, tile, smem_addr(X1), tbase + DC * (1 + b), true);
                     tc_commit(&tfull[b]);
                     ++tcount;
                 }
@@ -223,35 +272,21 @@ __global__ void __launch_bounds__(NZM_THREADS, 2) k_near_mma(NzmArgs a) {
             const int b = tcount & 1;
             if (!(ok = mbar_wait(&tfull[b], (uint32_t)((tcount >> 1) & 1), a.err))) break;
             tc_fence_after();
-            float v[32];
-            tc_ld32(tbase + ((uint32_t)(32 * quarter) << 16) + (uint32_t)NZM_N * (1 + b), v);
+            float v[32], w[32];
+            load_rows<S>(tbase + ((uint32_t)(32 * quarter) << 16) + DC * (1 + b), v, w);
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty[b]);
             const int row = nzm_row_of_lane(nzm_M(1, n1, tl.n2), 32 * quarter + lane);
-            if (row >= 0 && row < 3 * tl.n2) {
-#pragma unroll
-                for (int r = 0; r < NZM_R; ++r) {
-                    if (r >= a.rg || (a.skip && a.skip[a.r0 + r])) continue;
-                    const float s = a.xinv[r];
-                    a.part[(long long)(a.r0 + r) * a.part_len + tl.col_off + row] = make_float2(v[r] * s, v[NZM_R + r] * s);
-                }
-            }
+            store_rows<S>(a, v, w, row >= 0 && row < 3 * tl.n2, row, tl.col_off);
             ++tcount;
         }
         if (ok && mbar_wait(rowfull, 0u, a.err)) {
             tc_fence_after();
-            float v[32];
-            tc_ld32(tbase + ((uint32_t)(32 * quarter) << 16), v);
+            float v[32], w[32];
+            load_rows<S>(tbase + ((uint32_t)(32 * quarter) << 16), v, w);
             const int row = nzm_row_of_lane(nzm_M(0, n1, 1), 32 * quarter + lane);
-            if (row >= 0 && row < 3 * n1) {
-#pragma unroll
-                for (int r = 0; r < NZM_R; ++r) {
-                    if (r >= a.rg || (a.skip && a.skip[a.r0 + r])) continue;
-                    const float s = a.xinv[r];
-                    a.part[(long long)(a.r0 + r) * a.part_len + a.pslot_base[g] + row] = make_float2(v[r] * s, v[NZM_R + r] * s);
-                }
-            }
+            store_rows<S>(a, v, w, row >= 0 && row < 3 * n1, row, a.pslot_base[g]);
         }
     }
     tc_fence_before();
@@ -278,6 +313,7 @@ __global__ void k_xabsmax(const cf *__restrict__ x, long long n, int r0, int rg,
 // x blocks of one pass for every group: f16 hi/lo of sx * x (zero for
 // unknowns beyond the group, absent or skipped right-hand sides); block 0
 // also records 1 / (sA sx) per right-hand side
+template <int S>
 __global__ void k_xblocks(const cf *__restrict__ x, long long n, int r0, int rg, const int *__restrict__ skip,
                           const unsigned int *__restrict__ xmax, float sA, const int *__restrict__ grp_off,
                           const long long *__restrict__ xb_off, unsigned char *__restrict__ xb, float *__restrict__ xinv) {
@@ -287,16 +323,9 @@ __global__ void k_xblocks(const cf *__restrict__ x, long long n, int r0, int rg,
     const int g = blockIdx.x;
     const int s0 = grp_off[g], ng = grp_off[g + 1] - s0;
     const int K = nzm_xk(ng);
-    uint16_t *hi = reinterpret_cast<uint16_t *>(xb + xb_off[g]);
-    uint16_t *lo = hi + NZM_N * K;
-    const int total = NZM_N * K;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-        const float v = nzm_xblock_value(x, n, r0, rg, skip, sx, s0, ng, e);
-        uint16_t h, l;
-        nzm_split(v, h, l);
-        hi[e] = h;
-        lo[e] = l;
-    }
+    uint16_t *blk = reinterpret_cast<uint16_t *>(xb + xb_off[g]);
+    const int total = 4 * NZM_R * K;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) blk[e] = nzm_xblock_bits<S>(x, n, r0, rg, skip, sx, s0, ng, e);
     if (g == 0 && threadIdx.x < NZM_R) {
         const int r = threadIdx.x;
         xinv[r] = r < rg ? 1.f / (sA * sx[r]) : 0.f;
@@ -340,7 +369,7 @@ int near_mma_prepare(scd_ctx *c) {
     for (int t = 0; t < c->ntiles; ++t) {
         const NearTile &tl = c->tiles_h[t];
         toff[t + 1] = toff[t] + nzm_tile_bytes(tl.n1, tl.n2);
-        slack = std::max(slack, nzm_overrun(tl.n1, tl.n2));
+        slack = std::max(slack, std::max(nzm_overrun<0>(tl.n1, tl.n2), nzm_overrun<1>(tl.n1, tl.n2)));
     }
     std::vector<long long> xoff(c->ngroups + 1, 0);
     for (int g = 0; g < c->ngroups; ++g) xoff[g + 1] = xoff[g] + nzm_xblock_bytes(c->grp_off[g + 1] - c->grp_off[g]);
@@ -399,21 +428,27 @@ int near_mma_prepare(scd_ctx *c) {
 }
 
 // near-zone partial slots of nrhs complex64 right-hand sides (columns of stride n)
-void near_mma_run(scd_ctx *c, const cf *x, int nrhs, const int *done) {
+template <int S>
+static void near_mma_run_s(scd_ctx *c, const cf *x, int nrhs, const int *done) {
     const size_t sh = 128 + NZM_META + c->nzm_x1 + c->nzm_ring + c->nzm_slack;
-    cudaFuncSetAttribute(k_near_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    cudaFuncSetAttribute(k_near_mma<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
     for (int r0 = 0; r0 < nrhs; r0 += NZM_R) {
         const int rg = std::min(NZM_R, nrhs - r0);
         cudaMemsetAsync(c->d_xmax, 0, sizeof(unsigned int) * NZM_R, c->st);
         k_xabsmax<<<dim3((unsigned)c->nsm, (unsigned)rg), 256, 0, c->st>>>(x, c->n, r0, rg, c->d_xmax);
-        k_xblocks<<<c->ngroups, 256, 0, c->st>>>(x, c->n, r0, rg, done, c->d_xmax, c->nzm_sA, c->d_grp_off, c->d_xb_off,
-                                                c->d_xb, c->d_xinv);
+        k_xblocks<S><<<c->ngroups, 256, 0, c->st>>>(x, c->n, r0, rg, done, c->d_xmax, c->nzm_sA, c->d_grp_off,
+                                                   c->d_xb_off, c->d_xb, c->d_xinv);
         NzmArgs a;
         a.tiles = c->d_tiles; a.grp_tile = c->d_grp_tile; a.grp_off = c->d_grp_off; a.pslot_base = c->d_pslot_base;
         a.t16 = c->d_t16; a.t16_off = c->d_t16_off; a.xb = c->d_xb; a.xb_off = c->d_xb_off;
         a.part = c->f_nzpart; a.part_len = c->part_len; a.skip = done; a.r0 = r0; a.rg = rg; a.xinv = c->d_xinv;
         a.x1_bytes = c->nzm_x1; a.ring_bytes = c->nzm_ring; a.slack_bytes = c->nzm_slack; a.err = c->d_kerr;
-        k_near_mma<<<c->ngroups, NZM_THREADS, sh, c->st>>>(a);
+        k_near_mma<S><<<c->ngroups, NZM_THREADS, sh, c->st>>>(a);
         c->launches += 3;
     }
+}
+
+void near_mma_run(scd_ctx *c, const cf *x, int nrhs, const int *done) {
+    if (c->nzm_sched == 1) near_mma_run_s<1>(c, x, nrhs, done);
+    else near_mma_run_s<0>(c, x, nrhs, done);
 }

@@ -29,9 +29,22 @@
 #include "common.cuh"
 
 constexpr int NZM_R = 16;              // right-hand sides per pass
-constexpr int NZM_N = 2 * NZM_R;       // x-block rows: Re x of the pass, then Im x
-constexpr int NZM_SPLITS = 3;          // (hi A, hi x), (hi A, lo x), (lo A, hi x)
-constexpr int NZM_OPS = 3;             // per split: Re A X, -Im A Im x, Im A Re x
+constexpr int NZM_N = 2 * NZM_R;       // schedule 0: x-block rows per half (Re x, then Im x)
+constexpr int NZM_SPLITS = 3;          // schedule 0: (hi A, hi x), (hi A, lo x), (lo A, hi x)
+constexpr int NZM_OPS = 3;             // per A part: Re A X, -Im A Im x, Im A Re x
+
+// Two instruction schedules over the same tile planes:
+//  0 ("split"): the x block is a hi half then a lo half, each of NZM_N rows
+//    (Re x_r, then Im x_r); per K step 3 splits x 3 ops; accumulator
+//    columns [Re y_r | Im y_r].
+//  1 ("merged"): the x block is one block of 4R rows (Re x hi, Re x lo,
+//    Im x hi, Im x lo); per K step 2 A parts (hi, lo) x 3 ops, each over both
+//    x halves at once (6 instead of 9 instructions; lo A lo x is included);
+//    accumulator columns [Re y (x hi) | Re y (x lo) | Im y (x hi) | Im y (x lo)],
+//    summed pairwise by the epilogue.  Descriptors advance by constant steps.
+template <int S> struct NzmSched;
+template <> struct NzmSched<0> { static constexpr int PARTS = NZM_SPLITS, DCOLS = 2 * NZM_R, TMEM = 128; };
+template <> struct NzmSched<1> { static constexpr int PARTS = 2, DCOLS = 4 * NZM_R, TMEM = 256; };
 
 SCD_HD int nzm_ceil8(int v) { return (v + 7) & ~7; }
 SCD_HD int nzm_ceil16(int v) { return (v + 15) & ~15; }
@@ -110,6 +123,31 @@ SCD_HD float nzm_xblock_value(const float2 *x, long long n, int r0, int rg, cons
     return (im ? xv.y : xv.x) * sx[r];
 }
 
+// f16 bits at position e (halves, 0 <= e < 4 R K16) of a group's x block in
+// schedule S's layout
+template <int S>
+SCD_HD uint16_t nzm_xblock_bits(const float2 *x, long long n, int r0, int rg, const int *skip, const float *sx, int s0,
+                                int ng, int e) {
+    const int K = nzm_xk(ng);
+    uint16_t hi, lo;
+    if constexpr (S == 0) {
+        const int half = e / (NZM_N * K);
+        nzm_split(nzm_xblock_value(x, n, r0, rg, skip, sx, s0, ng, e - half * NZM_N * K), hi, lo);
+        return half ? lo : hi;
+    } else {
+        int row, k;
+        nzm_cpos(e, K, row, k);
+        const int part = row / NZM_R, r = row % NZM_R, im = part >> 1, want_lo = part & 1;
+        float v = 0.f;
+        if (r < rg && k < 3 * ng && !(skip && skip[r0 + r])) {
+            const float2 xv = x[(long long)(r0 + r) * n + 3LL * s0 + k];
+            v = (im ? xv.y : xv.x) * sx[r];
+        }
+        nzm_split(v, hi, lo);
+        return want_lo ? lo : hi;
+    }
+}
+
 // ---- products: use 0 = row product D (3n1 rows) += A x(g2), K over 3n2,
 //      tile read K-major; use 1 = transposed product D (3n2 rows) = A^T x(g1),
 //      K over 3n1, tile read MN-major.  Accumulator columns: [Re y_r | Im y_r].
@@ -123,7 +161,38 @@ struct NzmOp {
     int first;                      // first instruction of the product: overwrite instead of accumulate
 };
 
-// instruction (kk, s, q) of a product: K step kk (16 wide), split s, op q
+// instruction (kk, s, q) of a product in schedule 1: K step kk, A part s
+// (0 hi, 1 lo), op q
+//   q 0: D[:, 0:4R)  += Re A * X[0:4R)     (Re and Im of x, hi and lo halves)
+//   q 1: D[:, 0:2R)  += -Im A * X[2R:4R)   (Re y gets -Im A Im x)
+//   q 2: D[:, 2R:4R) += Im A * X[0:2R)     (Im y gets Im A Re x)
+SCD_HD NzmOp nzm_op_merged(int use, int n1, int n2, int kk, int s, int q) {
+    const uint32_t C1 = (uint32_t)nzm_cols8(n2);
+    const uint32_t plane = nzm_plane_bytes(n1, n2);
+    const int im = q != 0;
+    NzmOp o;
+    const uint32_t pbase = plane * (uint32_t)(2 * s + im);
+    if (use == 0) {
+        o.a_off = pbase + 256u * kk; o.a_lbo = 128u; o.a_sbo = 16u * C1; o.a_major = 0;
+    } else {
+        o.a_off = pbase + 32u * C1 * kk; o.a_lbo = 16u * C1; o.a_sbo = 128u; o.a_major = 1;
+    }
+    const uint32_t xsbo = 16u * (uint32_t)nzm_xk(use ? n1 : n2);
+    const uint32_t xbase = 256u * kk;
+    o.b_lbo = 128u; o.b_sbo = xsbo;
+    if (q == 0) { o.b_off = xbase; o.N = 4 * NZM_R; o.d_col = 0; o.a_neg = 0; }
+    else if (q == 1) { o.b_off = xbase + (2 * NZM_R / 8) * xsbo; o.N = 2 * NZM_R; o.d_col = 0; o.a_neg = 1; }
+    else { o.b_off = xbase; o.N = 2 * NZM_R; o.d_col = 2 * NZM_R; o.a_neg = 0; }
+    o.M = nzm_M(use, n1, n2);
+    o.first = kk == 0 && s == 0 && q == 0;
+    return o;
+}
+
+// bytes an operand start advances per K step (the same for every instruction of a product)
+SCD_HD uint32_t nzm_a_step(int use, int n2) { return use ? 32u * (uint32_t)nzm_cols8(n2) : 256u; }
+constexpr uint32_t NZM_B_STEP = 256u;
+
+// instruction (kk, s, q) of a product in schedule 0: K step kk (16 wide), split s, op q
 //   q 0: D[:, 0:2R) += Re A * X[0:2R)      (Re y gets Re A Re x, Im y gets Re A Im x)
 //   q 1: D[:, 0:R)  += -Im A * X[R:2R)     (Re y gets -Im A Im x)
 //   q 2: D[:, R:2R) += Im A * X[0:R)       (Im y gets Im A Re x)
@@ -150,6 +219,12 @@ SCD_HD NzmOp nzm_op(int use, int n1, int n2, int kk, int s, int q) {
     return o;
 }
 
+template <int S>
+SCD_HD NzmOp nzm_op_s(int use, int n1, int n2, int kk, int s, int q) {
+    if constexpr (S == 0) return nzm_op(use, n1, n2, kk, s, q);
+    else return nzm_op_merged(use, n1, n2, kk, s, q);
+}
+
 // last byte (exclusive) an instruction reads, relative to its operand start
 SCD_HD uint32_t nzm_a_end(const NzmOp &o) { return o.a_off + (uint32_t)(o.M / 8 - 1) * o.a_sbo + o.a_lbo + 128u; }
 SCD_HD uint32_t nzm_b_end(const NzmOp &o) { return o.b_off + (uint32_t)(o.N / 8 - 1) * o.b_sbo + o.b_lbo + 128u; }
@@ -157,13 +232,14 @@ SCD_HD uint32_t nzm_b_end(const NzmOp &o) { return o.b_off + (uint32_t)(o.N / 8 
 // bytes past a tile's end that its products may read (rows beyond 3n1 / 3n2
 // up to M and the 8 columns of a half-filled K step): the ring keeps that
 // much zeroed slack after its end
+template <int S = 0>
 SCD_HD uint32_t nzm_overrun(int n1, int n2) {
     uint32_t end = 0;
     for (int use = 0; use < 2; ++use) {
         const int ks = nzm_ksteps(use, n1, n2);
-        for (int s = 0; s < NZM_SPLITS; ++s)
+        for (int s = 0; s < NzmSched<S>::PARTS; ++s)
             for (int q = 0; q < NZM_OPS; ++q) {
-                const uint32_t e = nzm_a_end(nzm_op(use, n1, n2, ks - 1, s, q));
+                const uint32_t e = nzm_a_end(nzm_op_s<S>(use, n1, n2, ks - 1, s, q));
                 end = e > end ? e : end;
             }
     }

@@ -68,7 +68,7 @@ int64_t estimate(const scd_request *r, const scd_grid_desc &d) {
         // hi/lo planes of every tile (8 B per complex plus padding) and a
         // pass of x blocks
         const char *e = getenv("SCADYN_NEAR_MMA");
-        if (e && e[0] == '1' && mixed && r->storage_prec != SCD_STORE_C128)
+        if (e && (e[0] == '1' || e[0] == '2') && mixed && r->storage_prec != SCD_STORE_C128)
             b += T * 250.0 * 9.0 * 8.0 * 1.3 + n * 128.0 * 1.3;   // x block: 32 rows x 2 B x hi/lo per unknown
     }
     return (int64_t)(b * 1.1) + (64LL << 20);

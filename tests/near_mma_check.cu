@@ -68,6 +68,7 @@ static void emulate(float (*tm)[128], uint32_t dcol, const Image &A, uint32_t a_
 static unsigned rs = 12345u;
 static double urand() { rs = rs * 1664525u + 1013904223u; return (rs >> 8) / 16777216.0 - 0.5; }
 
+template <int S>
 static int check_tile(int n1, int n2, int rg, bool with_skip) {
     const int R = NZM_R;
     // complex64 tile in the k_near_groups layout
@@ -104,13 +105,13 @@ static int check_tile(int n1, int n2, int rg, bool with_skip) {
     const uint32_t tb = nzm_tile_bytes(n1, n2), P = tb / 8;
     auto xblock = [&](int s0, int ng) {
         std::vector<unsigned char> b(nzm_xblock_bytes(ng));
-        uint16_t *hi = (uint16_t *)b.data(), *lo = hi + NZM_N * nzm_xk(ng);
-        for (int e = 0; e < NZM_N * nzm_xk(ng); ++e)
-            nzm_split(nzm_xblock_value(x.data(), n, 0, rg, skip.data(), sx, s0, ng, e), hi[e], lo[e]);
+        uint16_t *h = (uint16_t *)b.data();
+        for (int e = 0; e < 4 * NZM_R * nzm_xk(ng); ++e)
+            h[e] = nzm_xblock_bits<S>(x.data(), n, 0, rg, skip.data(), sx, s0, ng, e);
         return b;
     };
     const std::vector<unsigned char> x1 = xblock(0, n1), x2 = xblock(n1, n2);
-    const uint32_t slack = (nzm_overrun(n1, n2) + 127u) & ~127u;
+    const uint32_t slack = (nzm_overrun<S>(n1, n2) + 127u) & ~127u;
     Image slot, X1;
     slot.b.assign(tb + x2.size() + slack, 0);
     for (long long e = 0; e < P; ++e) {
@@ -124,25 +125,32 @@ static int check_tile(int n1, int n2, int rg, bool with_skip) {
     // B operands stay inside their x block
     for (int use = 0; use < 2; ++use)
         for (int kk = 0; kk < nzm_ksteps(use, n1, n2); ++kk)
-            for (int s = 0; s < NZM_SPLITS; ++s)
+            for (int s = 0; s < NzmSched<S>::PARTS; ++s)
                 for (int q = 0; q < NZM_OPS; ++q) {
-                    const NzmOp o = nzm_op(use, n1, n2, kk, s, q);
+                    const NzmOp o = nzm_op_s<S>(use, n1, n2, kk, s, q);
                     const uint32_t bx = (uint32_t)(use ? x1.size() : x2.size());
                     if (nzm_a_end(o) > tb + slack || nzm_b_end(o) > bx) {
                         printf("(%d,%d) use %d kk %d s %d q %d: A end %u > %u or B end %u > %u\n", n1, n2, use, kk, s, q,
                                nzm_a_end(o), tb + slack, nzm_b_end(o), bx);
                         return 0;
                     }
+                    // the kernel advances K step 0's descriptors by constant steps
+                    const NzmOp o0 = nzm_op_s<S>(use, n1, n2, 0, s, q);
+                    if (o.a_off != o0.a_off + kk * nzm_a_step(use, n2) || o.b_off != o0.b_off + kk * NZM_B_STEP) {
+                        printf("(%d,%d) use %d kk %d: operand offsets do not advance by the constant steps\n", n1, n2, use, kk);
+                        return 0;
+                    }
                 }
     static float tm[128][128];
     for (auto &row : tm) for (float &v : row) v = NAN;
-    // row product into columns 0.., transposed product into columns NZM_N..
+    // row product into columns 0.., transposed product into columns DCOLS..
+    constexpr int DC = NzmSched<S>::DCOLS;
     for (int use = 0; use < 2; ++use) {
-        const uint32_t dcol = use ? NZM_N : 0;
+        const uint32_t dcol = use ? DC : 0;
         for (int kk = 0; kk < nzm_ksteps(use, n1, n2); ++kk)
-            for (int s = 0; s < NZM_SPLITS; ++s)
+            for (int s = 0; s < NzmSched<S>::PARTS; ++s)
                 for (int q = 0; q < NZM_OPS; ++q) {
-                    const NzmOp o = nzm_op(use, n1, n2, kk, s, q);
+                    const NzmOp o = nzm_op_s<S>(use, n1, n2, kk, s, q);
                     if (use == 0) emulate(tm, dcol + o.d_col, slot, o.a_off, slot, tb + o.b_off, o, !o.first);
                     else emulate(tm, dcol + o.d_col, slot, o.a_off, X1, o.b_off, o, !o.first);
                 }
@@ -150,7 +158,7 @@ static int check_tile(int n1, int n2, int rg, bool with_skip) {
     // epilogue and reference
     double err = 0, ref = 0;
     for (int use = 0; use < 2; ++use) {
-        const int M = nzm_M(use, n1, n2), rows = use ? 3 * n2 : 3 * n1, dcol = use ? NZM_N : 0;
+        const int M = nzm_M(use, n1, n2), rows = use ? 3 * n2 : 3 * n1, dcol = use ? DC : 0;
         std::vector<int> seen(rows, 0);
         for (int lane = 0; lane < 128; ++lane) {
             const int row = nzm_row_of_lane(M, lane);
@@ -158,7 +166,9 @@ static int check_tile(int n1, int n2, int rg, bool with_skip) {
             ++seen[row];
             for (int r = 0; r < rg; ++r) {
                 if (skip[r]) continue;
-                const zc got(tm[lane][dcol + r] * xinv[r], tm[lane][dcol + R + r] * xinv[r]);
+                const float *d = &tm[lane][dcol];
+                const zc got = S == 0 ? zc(d[r] * xinv[r], d[R + r] * xinv[r])
+                                      : zc((d[r] + d[R + r]) * xinv[r], (d[2 * R + r] + d[3 * R + r]) * xinv[r]);
                 zc want = 0;
                 if (use == 0)
                     for (int c = 0; c < 3 * n2; ++c) {
@@ -179,8 +189,8 @@ static int check_tile(int n1, int n2, int rg, bool with_skip) {
     }
     const double rel = err / ref;
     const bool ok = rel < 2e-6;
-    printf("tile %2d x %2d  rg %2d%s  M %3d/%3d  rel err %.2e  slack %u  %s\n", n1, n2, rg, with_skip ? " skip" : "     ",
-           nzm_M(0, n1, n2), nzm_M(1, n1, n2), rel, slack, ok ? "ok" : "FAIL");
+    printf("schedule %d  tile %2d x %2d  rg %2d%s  M %3d/%3d  rel err %.2e  slack %u  %s\n", S, n1, n2, rg,
+           with_skip ? " skip" : "     ", nzm_M(0, n1, n2), nzm_M(1, n1, n2), rel, slack, ok ? "ok" : "FAIL");
     return ok;
 }
 
@@ -189,12 +199,14 @@ int main() {
     int bad = 0, n = 0;
     for (auto &sh : shapes)
         for (int v = 0; v < 2; ++v) {
-            ++n;
-            bad += !check_tile(sh[0], sh[1], v ? 16 : 7, v == 1);
+            n += 2;
+            bad += !check_tile<0>(sh[0], sh[1], v ? 16 : 7, v == 1);
+            bad += !check_tile<1>(sh[0], sh[1], v ? 16 : 7, v == 1);
         }
     uint32_t slack = 0;
     for (int a = 1; a <= SCD_GROUP_MAX; ++a)
-        for (int b = 1; b <= SCD_GROUP_MAX; ++b) slack = std::max(slack, nzm_overrun(a, b));
+        for (int b = 1; b <= SCD_GROUP_MAX; ++b)
+            slack = std::max(slack, std::max(nzm_overrun<0>(a, b), nzm_overrun<1>(a, b)));
     printf("largest overrun over all shapes: %u bytes\n", slack);
     printf("%d of %d tiles ok\n", n - bad, n);
     return bad ? 1 : 0;

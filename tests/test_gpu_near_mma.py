@@ -1,5 +1,6 @@
-"""The tensor-core near zone (opt-in with SCADYN_NEAR_MMA=1 at context
-creation) against the CUDA-core kernel on the same operator: mixed-precision
+"""The tensor-core near zone (opt-in with SCADYN_NEAR_MMA=1, or =2 for the
+merged instruction schedule, at context creation) against the CUDA-core
+kernel on the same operator: mixed-precision
 T-matrices agree to 1e-6 and both meet the FP64 residual, iteration counts
 stay within 20%, results are batch-invariant, and the pipeline never times
 out.  Two grid cell sizes give groups below and above 64 rows (M = 64 and
@@ -24,7 +25,7 @@ def rel(a, b):
 
 def _solver(op, mma):
     old = os.environ.get("SCADYN_NEAR_MMA")
-    os.environ["SCADYN_NEAR_MMA"] = "1" if mma else "0"
+    os.environ["SCADYN_NEAR_MMA"] = mma if mma else "0"
     try:
         return solver_from_oracle(op)
     finally:
@@ -34,11 +35,13 @@ def _solver(op, mma):
             os.environ["SCADYN_NEAR_MMA"] = old
 
 
-@pytest.fixture(scope="module", params=[1.8, 3.2])
+@pytest.fixture(scope="module", params=[(1.8, "1"), (3.2, "1"), (1.8, "2"), (3.2, "2")],
+                ids=["1.8", "3.2", "1.8-merged", "3.2-merged"])
 def ops(request, small_sphere):
+    grid_size, sched = request.param
     k = 1.0 / small_sphere.a
-    op = O.setup(small_sphere, k, grid_size=request.param, nthreads=0)
-    a, b = _solver(op, False), _solver(op, True)
+    op = O.setup(small_sphere, k, grid_size=grid_size, nthreads=0)
+    a, b = _solver(op, None), _solver(op, sched)
     yield op, a, b
     a.close()
     b.close()
