@@ -9,6 +9,7 @@ import dataclasses
 
 import numpy as np
 import pytest
+import scipy.sparse
 
 from oracle import oracle as O
 
@@ -28,25 +29,30 @@ def pseudo_x(x1, T):
     return np.ascontiguousarray(x1.reshape(T, 3, 4).transpose(0, 2, 1).reshape(-1))
 
 
-def dense_near(op1, T):
-    """Dense 12T x 12T near-zone matrix from the 12x12 block list."""
-    A = np.zeros((12 * T, 12 * T), np.complex128)
-    for b, (t1, t2) in enumerate(op1.sp_ind):
-        V = op1.sp_mat[b].T.astype(np.complex128)          # V[r, c] = V(r, c)
-        a, c = 12 * (t1 - 1), 12 * (t2 - 1)
-        A[a:a + 12, c:c + 12] += V
-        if a != c:
-            A[c:c + 12, a:a + 12] += V.T
-    return A
+def sparse_from(n, rows, cols, vals):
+    return scipy.sparse.coo_matrix((vals.ravel(), (rows.ravel(), cols.ravel())), shape=(n, n)).tocsr()
 
 
-def test_matmul_Acorr_matches_dense_blocks(ops):
+def near_matrix(op1, T):
+    """Sparse 12T x 12T near-zone matrix from the 12x12 block list."""
+    V = op1.sp_mat.astype(np.complex128).transpose(0, 2, 1)      # V[b, r, c] = V(r, c)
+    a = 12 * (op1.sp_ind[:, 0] - 1)[:, None, None] + np.arange(12)[None, :, None]
+    c = 12 * (op1.sp_ind[:, 1] - 1)[:, None, None] + np.arange(12)[None, None, :]
+    a, c = np.broadcast_to(a, V.shape), np.broadcast_to(c, V.shape)
+    off = op1.sp_ind[:, 0] != op1.sp_ind[:, 1]
+    rows = np.concatenate([a.ravel(), c[off].ravel()])
+    cols = np.concatenate([c.ravel(), a[off].ravel()])
+    vals = np.concatenate([V.ravel(), V[off].ravel()])
+    return sparse_from(12 * T, rows, cols, vals)
+
+
+def test_matmul_Acorr_matches_block_assembly(ops):
     _, op1 = ops
     T = op1.geom.T
     rng = np.random.default_rng(7)
     x = crand(rng, 12 * T)
     got = O.matmul_Acorr(T, op1.sp_mat, op1.sp_ind, x)
-    want = dense_near(op1, T) @ x
+    want = near_matrix(op1, T) @ x
     assert np.linalg.norm(got - want) / np.linalg.norm(want) < 1e-13
 
 
@@ -69,19 +75,22 @@ def test_pseudo_tet_near_blocks_one_sided_inside_a_tet(ops):
     different tets, rebuild the near-zone matrix in pseudo-tet order."""
     _, op1 = ops
     T = op1.geom.T
-    P = np.zeros((12 * T, 12 * T), np.complex128)
-    for b, (t1, t2) in enumerate(op1.sp_ind):
-        V = op1.sp_mat[b].T.astype(np.complex128)
-        for i in range(4):
-            for j in range(4):
-                blk = V[i::4, j::4]                         # (c, c') of nodes i, j
-                p, q = 4 * (t1 - 1) + i, 4 * (t2 - 1) + j
-                P[3 * p:3 * p + 3, 3 * q:3 * q + 3] += blk
-                if t1 != t2:
-                    P[3 * q:3 * q + 3, 3 * p:3 * p + 3] += blk.T
-    A = dense_near(op1, T)
+    V = op1.sp_mat.astype(np.complex128).transpose(0, 2, 1)      # V[b, 4c + i, 4c' + j]
+    blk = V.reshape(-1, 3, 4, 3, 4).transpose(0, 2, 4, 1, 3)     # [b, i, j, c, c']
+    t1, t2 = (op1.sp_ind[:, 0] - 1), (op1.sp_ind[:, 1] - 1)
+    ar4, ar3 = np.arange(4), np.arange(3)
+    p = 4 * t1[:, None, None, None, None] + ar4[None, :, None, None, None]
+    q = 4 * t2[:, None, None, None, None] + ar4[None, None, :, None, None]
+    rows = np.broadcast_to(3 * p + ar3[None, None, None, :, None], blk.shape)
+    cols = np.broadcast_to(3 * q + ar3[None, None, None, None, :], blk.shape)
+    off = t1 != t2                                                # mirrored between different tets only
+    P = sparse_from(12 * T, np.concatenate([rows.ravel(), cols[off].ravel()]),
+                    np.concatenate([cols.ravel(), rows[off].ravel()]),
+                    np.concatenate([blk.ravel(), blk[off].ravel()]))
+    A = near_matrix(op1, T)
     perm = pseudo_x(np.arange(12 * T), T)                   # pseudo index -> original index
-    assert np.array_equal(P, A[np.ix_(perm, perm)])
+    D = P - A[perm][:, perm]
+    assert D.count_nonzero() == 0 or abs(D).max() == 0
 
 
 def test_linear_gmres_converges(ops):
