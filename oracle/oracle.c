@@ -4,11 +4,12 @@
  * T-matrix solve (pFFT JVIE matvec inside restarted GMRES, plus the
  * per-wavelength setup that produces its operator data).  Each function cites
  * the reference file:line it restates.  Only tests/, __graft_entry__.smoke()
- * and bench.py's CPU-baseline leg load this library, as the checker.
+ * and bench.py's CPU-baseline leg load this library, to check results.
  *
  * Parity: UNPINNED by reference golden vectors (the reference ships none and
  * cannot be compiled here).  Cross-checked against an independent numpy/scipy
- * restatement and the Mie series (see tests/).
+ * restatement, the Mie series, T-matrix reciprocity and the energy balance
+ * (see tests/).
  *
  * Floating-point notes that follow the reference's source literally:
  *  - single-precision literals promoted to double: `(x)**(1.0/3.0)` uses the

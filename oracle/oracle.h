@@ -2,7 +2,7 @@
  *
  * A plain-C restatement of the reference's Fortran algorithm (jherrane/scadyn,
  * src/ Fortran files), used only by tests/, __graft_entry__.smoke() and bench.py's CPU
- * baseline leg as the checker.  Nothing in the product links or calls it.
+ * baseline leg, to check results.  Nothing in the product links or calls it.
  *
  * Parity status: UNPINNED by the reference's own tests — the reference ships
  * no tests, golden vectors or fixtures, and cannot be compiled here (no

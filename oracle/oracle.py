@@ -1,7 +1,7 @@
 """ctypes binding of the CPU oracle (``oracle/liborc.so``) — TEST INFRASTRUCTURE.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
-leg import this module, as the checker.  The oracle restates the reference's
+leg import this module, to check results.  The oracle restates the reference's
 Fortran algorithm (jherrane/scadyn ``src/``); parity against the reference is
 UNPINNED (no golden vectors exist upstream).
 
