@@ -717,14 +717,157 @@ static void plan_line(fft_plan *p, zc *A, size_t base, size_t stride) {
     for (int i = 0; i < p->L; ++i) A[base + i*stride] = p->line[i];
 }
 
-/* pass over lines (i1 < n1, i2 < n2) with base = i1*s1 + i2*s2 */
+/* Batched mixed-radix Stockham transforms for 5-smooth lengths: FB lines at
+ * a time, held as separate real and imaginary arrays [L][FB] so that the
+ * butterflies run over the batch with plain double arithmetic (the C
+ * `_Complex` multiply of -O2 goes through a library call).  Stage with radix
+ * R and sub-transform size Ns: element j < L/R takes x[j + q L/R] (q < R),
+ * multiplies by exp(sign 2 pi i k q / (Ns R)), k = j mod Ns, forms the R-point
+ * DFT and stores it at (j / Ns) Ns R + k + s Ns -- natural order out, no bit
+ * reversal.  Other lengths keep the line routines above. */
+#define FB 16
+typedef struct {
+    int L, nst, ok;
+    int R[40];
+    double *twr[40], *twi[40];        /* per stage: [k*R + q], k < Ns */
+    double *ar, *ai, *br, *bi;        /* [L][FB] */
+    fft_plan slow;
+} bfft_plan;
+
+static void bplan_init(bfft_plan *p, int L, int sign) {
+    memset(p, 0, sizeof *p);
+    p->L = L;
+    int n = L;
+    const int rs[4] = {4, 2, 3, 5};
+    for (int i = 0; i < 4; ++i) while (n % rs[i] == 0 && p->nst < 40) { p->R[p->nst++] = rs[i]; n /= rs[i]; }
+    p->ok = n == 1;
+    if (!p->ok) { plan_init(&p->slow, L, sign); return; }
+    int Ns = 1;
+    for (int st = 0; st < p->nst; ++st) {
+        const int R = p->R[st];
+        p->twr[st] = (double *)malloc(sizeof(double)*(size_t)Ns*R);
+        p->twi[st] = (double *)malloc(sizeof(double)*(size_t)Ns*R);
+        for (int k = 0; k < Ns; ++k)
+            for (int q = 0; q < R; ++q) {
+                const double a = sign*2.0*PI*(double)(k*q)/(double)(Ns*R);
+                p->twr[st][k*R + q] = cos(a);
+                p->twi[st][k*R + q] = sin(a);
+            }
+        Ns *= R;
+    }
+    p->ar = (double *)malloc(sizeof(double)*(size_t)L*FB); p->ai = (double *)malloc(sizeof(double)*(size_t)L*FB);
+    p->br = (double *)malloc(sizeof(double)*(size_t)L*FB); p->bi = (double *)malloc(sizeof(double)*(size_t)L*FB);
+}
+
+static void bplan_free(bfft_plan *p) {
+    if (!p->ok) { plan_free(&p->slow); return; }
+    for (int st = 0; st < p->nst; ++st) { free(p->twr[st]); free(p->twi[st]); }
+    free(p->ar); free(p->ai); free(p->br); free(p->bi);
+}
+
+/* one Stockham stage over the batch: x -> y */
+static void bstage(const bfft_plan *p, int st, int Ns, int sign, const double *xr, const double *xi, double *yr, double *yi) {
+    const int L = p->L, R = p->R[st], NR = L/R;
+    const double *twr = p->twr[st], *twi = p->twi[st];
+    double cr[5], ci[5];                                   /* roots exp(sign 2 pi i t / R) */
+    for (int t = 0; t < R; ++t) { const double a = sign*2.0*PI*(double)t/(double)R; cr[t] = cos(a); ci[t] = sin(a); }
+    for (int j = 0; j < NR; ++j) {
+        const int k = j % Ns, idx = (j/Ns)*Ns*R + k;
+        double vr[5][FB], vi[5][FB];
+        for (int q = 0; q < R; ++q) {
+            const double *sr = xr + (size_t)(j + q*NR)*FB, *si = xi + (size_t)(j + q*NR)*FB;
+            const double wr = twr[k*R + q], wi = twi[k*R + q];
+            for (int b = 0; b < FB; ++b) { vr[q][b] = sr[b]*wr - si[b]*wi; vi[q][b] = sr[b]*wi + si[b]*wr; }
+        }
+        double *o[5][2];
+        for (int t = 0; t < R; ++t) { o[t][0] = yr + (size_t)(idx + t*Ns)*FB; o[t][1] = yi + (size_t)(idx + t*Ns)*FB; }
+        if (R == 2) {
+            for (int b = 0; b < FB; ++b) {
+                o[0][0][b] = vr[0][b] + vr[1][b]; o[0][1][b] = vi[0][b] + vi[1][b];
+                o[1][0][b] = vr[0][b] - vr[1][b]; o[1][1][b] = vi[0][b] - vi[1][b];
+            }
+        } else if (R == 4) {
+            /* X1 = (v0 - v2) + w (v1 - v3), X3 = (v0 - v2) - w (v1 - v3), w = sign * i */
+            for (int b = 0; b < FB; ++b) {
+                const double a0r = vr[0][b] + vr[2][b], a0i = vi[0][b] + vi[2][b];
+                const double a1r = vr[0][b] - vr[2][b], a1i = vi[0][b] - vi[2][b];
+                const double a2r = vr[1][b] + vr[3][b], a2i = vi[1][b] + vi[3][b];
+                const double a3r = vr[1][b] - vr[3][b], a3i = vi[1][b] - vi[3][b];
+                const double w3r = -sign*a3i, w3i = sign*a3r;   /* w * a3 */
+                o[0][0][b] = a0r + a2r; o[0][1][b] = a0i + a2i;
+                o[2][0][b] = a0r - a2r; o[2][1][b] = a0i - a2i;
+                o[1][0][b] = a1r + w3r; o[1][1][b] = a1i + w3i;
+                o[3][0][b] = a1r - w3r; o[3][1][b] = a1i - w3i;
+            }
+        } else {
+            for (int t = 0; t < R; ++t)
+                for (int b = 0; b < FB; ++b) {
+                    double sr = vr[0][b], si = vi[0][b];
+                    for (int q = 1; q < R; ++q) {
+                        const int e = (q*t) % R;
+                        sr += vr[q][b]*cr[e] - vi[q][b]*ci[e];
+                        si += vr[q][b]*ci[e] + vi[q][b]*cr[e];
+                    }
+                    o[t][0][b] = sr; o[t][1][b] = si;
+                }
+        }
+    }
+}
+
+/* transform lines base_b + i*stride (b < nb <= FB, i < L) in place */
+static void bplan_lines(bfft_plan *p, int sign, zc *A, const size_t *base, int nb, size_t stride) {
+    const int L = p->L;
+    if (!p->ok) { for (int b = 0; b < nb; ++b) plan_line(&p->slow, A, base[b], stride); return; }
+    for (int i = 0; i < L; ++i)
+        for (int b = 0; b < FB; ++b) {
+            const zc v = b < nb ? A[base[b] + i*stride] : 0;
+            p->ar[(size_t)i*FB + b] = creal(v);
+            p->ai[(size_t)i*FB + b] = cimag(v);
+        }
+    double *xr = p->ar, *xi = p->ai, *yr = p->br, *yi = p->bi;
+    int Ns = 1;
+    for (int st = 0; st < p->nst; ++st) {
+        bstage(p, st, Ns, sign, xr, xi, yr, yi);
+        double *t = xr; xr = yr; yr = t;
+        t = xi; xi = yi; yi = t;
+        Ns *= p->R[st];
+    }
+    for (int i = 0; i < L; ++i)
+        for (int b = 0; b < nb; ++b) A[base[b] + i*stride] = CMPLX(xr[(size_t)i*FB + b], xi[(size_t)i*FB + b]);
+}
+
+static int smooth5(int L) {
+    for (int r = 2; r <= 5; ++r) while (L % r == 0) L /= r;
+    return L == 1;
+}
+
+/* pass over lines (i1 < n1, i2 < n2) with base = i1*s1 + i2*s2: FB
+ * consecutive i2 per batch for 5-smooth lengths, one line per work item
+ * otherwise (finer load balance for the slower generic routine) */
 static void pass_lines(int L, int sign, zc *A, int n1, size_t s1, int n2, size_t s2, size_t stride) {
+    if (!smooth5(L)) {
+#pragma omp parallel
+        {
+            fft_plan p; plan_init(&p, L, sign);
+#pragma omp for collapse(2) schedule(static)
+            for (int i1 = 0; i1 < n1; ++i1) for (int i2 = 0; i2 < n2; ++i2) plan_line(&p, A, i1*s1 + i2*s2, stride);
+            plan_free(&p);
+        }
+        return;
+    }
+    const int nc = (n2 + FB - 1)/FB;
 #pragma omp parallel
     {
-        fft_plan p; plan_init(&p, L, sign);
+        bfft_plan p; bplan_init(&p, L, sign);
+        size_t base[FB];
 #pragma omp for collapse(2) schedule(static)
-        for (int i1 = 0; i1 < n1; ++i1) for (int i2 = 0; i2 < n2; ++i2) plan_line(&p, A, i1*s1 + i2*s2, stride);
-        plan_free(&p);
+        for (int i1 = 0; i1 < n1; ++i1)
+            for (int c = 0; c < nc; ++c) {
+                const int i2a = c*FB, nb = n2 - i2a < FB ? n2 - i2a : FB;
+                for (int b = 0; b < nb; ++b) base[b] = i1*s1 + (size_t)(i2a + b)*s2;
+                bplan_lines(&p, sign, A, base, nb, stride);
+            }
+        bplan_free(&p);
     }
 }
 
