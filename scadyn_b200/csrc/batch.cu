@@ -534,6 +534,7 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
             if (smode[s] != SLOT_ARNOLDI) continue;
             const int i = sstep[s] + 1;
             const double *tt = a.ctm + (size_t)s * CGS_NV;
+            __syncwarp();   // every lane is done with the previous item's coefficients
             for (int k = lane; k < i; k += 32) hs[k] = cmk(__ldcg(tt + 2 * k), __ldcg(tt + 2 * k + 1));
             __syncwarp();
             if (c == 0 && lane == 0)
