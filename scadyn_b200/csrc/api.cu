@@ -132,14 +132,15 @@ static int set_order(scd_ctx *c, const std::vector<int> &cube_of_tet) {
     c->grp_cube.clear();
     c->grp_of_slot.assign(T, 0);
     c->max_per_group = 0;
-    const int nb = c->nb;
+    std::vector<int> sizes;
     for (int q = 0; q < c->ncubes; ++q) {
-        const int n = (cnt[q + 1] - cnt[q]) / nb;          // tets
-        if (n == 0) continue;
-        const int ng = (n + SCD_GROUP_MAX / nb - 1) / (SCD_GROUP_MAX / nb);
+        const int n = cnt[q + 1] - cnt[q];
+        if ((int)sizes.size() < n + 1) sizes.resize(n + 1);   // at most n runs
+        const int ng = split_box(n, c->nb, SCD_GROUP_MAX, sizes.data());
+        if (ng == 0) continue;
         int s = cnt[q];
         for (int g = 0; g < ng; ++g) {
-            const int m = nb * (n / ng + (g < n % ng ? 1 : 0));
+            const int m = sizes[g];
             for (int k = 0; k < m; ++k) c->grp_of_slot[s + k] = (int)c->grp_cube.size();
             s += m;
             c->grp_off.push_back(s);

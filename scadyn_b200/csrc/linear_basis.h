@@ -44,3 +44,15 @@ inline void expand_linear_blocks(int64_t B, const ST *sp12, const int32_t *ind, 
             }
     }
 }
+
+// Near-zone groups of one projection box holding n basis functions (nb per
+// tet, n a multiple of nb): ceil(tets / (gmax / nb)) runs of whole tets whose
+// tet counts differ by at most one.  Writes the run sizes (in basis
+// functions) to sizes and returns their number.
+inline int split_box(int n, int nb, int gmax, int *sizes) {
+    const int tets = n / nb, per = gmax / nb;
+    if (tets == 0) return 0;
+    const int ng = (tets + per - 1) / per;
+    for (int g = 0; g < ng; ++g) sizes[g] = nb * (tets / ng + (g < tets % ng ? 1 : 0));
+    return ng;
+}
