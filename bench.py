@@ -249,8 +249,9 @@ def main():
     ap.add_argument("--sweep", type=int, default=0,
                     help="run a C3-shaped wavelength sweep with this many wavelengths instead")
     ap.add_argument("--sweep-nmax", type=int, default=14, help="largest Nmax of the sweep (C3: 14)")
-    ap.add_argument("--profile", default=None, choices=["near1", "near16", "mixed16", "solve16"],
-                    help="only build the operator and run profile_matvec (for ncu captures)")
+    ap.add_argument("--profile", default=None, choices=["near1", "near16", "mixed16", "solve16", "near-compare"],
+                    help="only build the operator and run profile_matvec (for ncu captures); near-compare times "
+                         "the complex64 x16 matvec with the CUDA-core near zone and both tensor-core schedules")
     ap.add_argument("--near-mma", nargs="?", const="1", default=None, choices=["1", "2"],
                     help="tensor-core near zone for the complex64 matvec (SCADYN_NEAR_MMA=1; 2: merged schedule)")
     ap.add_argument("--cgs", action="store_true",
@@ -308,6 +309,21 @@ def main():
                           "columns": 16, "columns_per_s": round(16 / (ms / 1e3), 4),
                           "iters_mean": float(np.mean(it))}), flush=True)
         solver.close()
+        return
+    if args.profile == "near-compare":
+        # one operator build per context (the switch is read at creation); the
+        # same mesh, 16 complex64 right-hand sides, median of 5 profiled loops
+        solver.close()
+        out = {"config": args.config, "tets": mesh.n_tet, "nrhs": 16, "ms": {}}
+        for mode, label in (("0", "cuda_cores"), ("1", "tensor_split"), ("2", "tensor_merged")):
+            os.environ["SCADYN_NEAR_MMA"] = mode
+            sv, _, _, _, _ = build_solver(cfg, mesh, local)
+            runs = [sv.profile_matvec(10, 16, api.PREC_MIXED) for _ in range(5)]
+            out["ms"][label] = {key: round(float(np.median([r[key] for r in runs])), 4)
+                                for key in ("nearzone_ms", "fft_ms", "gather_ms", "matvec_ms")}
+            sv.close()
+        os.environ.pop("SCADYN_NEAR_MMA", None)
+        print(json.dumps(out), flush=True)
         return
     if args.profile:
         nrhs, prec = {"near1": (1, api.PREC_FP64), "near16": (16, api.PREC_FP64),
