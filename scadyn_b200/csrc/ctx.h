@@ -155,7 +155,7 @@ struct scd_ctx {
     // by SCADYN_CGS=1 at context creation
     bool cgs_on = false;
     // tensor-core near zone of the complex64 matvec (near_mma.cu), opt-in by
-    // SCADYN_NEAR_MMA=1 at context creation
+    // SCADYN_NEAR_MMA=1 (or =2) at context creation
     bool nzm_on = false, nzm_ready = false;
     int nzm_sched = 0;                   // instruction schedule (near_mma.cuh): 0 split, 1 merged (SCADYN_NEAR_MMA=2)
     unsigned char *d_t16 = nullptr;      // f16 hi/lo planes of every tile

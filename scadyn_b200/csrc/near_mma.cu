@@ -7,8 +7,9 @@
 // to partial slot 0, and each tile (g, g2), g2 != g, writes A^T x(g) to its
 // partial slot of g2; k_gather adds the slots in a fixed order.
 //
-// Opt-in (environment SCADYN_NEAR_MMA=1 when the context is created) for
-// complex64 near-zone storage; the CUDA-core kernel stays the default.
+// Opt-in (environment SCADYN_NEAR_MMA=1 for the split instruction schedule,
+// =2 for the merged one, when the context is created) for complex64
+// near-zone storage; the CUDA-core kernel stays the default.
 #include <cuda_fp16.h>
 
 #include <cmath>
