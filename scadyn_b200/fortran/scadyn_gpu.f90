@@ -37,10 +37,46 @@ module scadyn_gpu
       integer(c_int32_t) :: max_outer = 10
    end type
 
+   ! device timing block (scd_get_timing), milliseconds
+   type, bind(C), public :: scd_timing
+      real(c_double)     :: matvec_ms, nearzone_ms, fft_ms, gather_ms, arnoldi_ms
+      real(c_double)     :: last_call_ms, accum_ms
+      integer(c_int64_t) :: launches, matvecs, arnoldi_steps
+   end type
+
+   ! request server (include/scadyn_server.h)
+   integer(c_int), parameter, public :: SCD_REQ_QUEUED = 0, SCD_REQ_RUNNING = 1, SCD_REQ_DONE = 2, &
+                                        SCD_REQ_FAILED = 3, SCD_REQ_CANCELLED = 4
+
+   ! coord, etopol, param: c_loc of the mesh arrays (copied by scd_server_submit)
+   type, bind(C), public :: scd_request
+      integer(c_int32_t)   :: Nv, T
+      type(c_ptr)          :: coord, etopol, param
+      real(c_double)       :: k, grid_size
+      integer(c_int32_t)   :: Nmax, storage_prec
+      type(scd_solve_opts) :: opts
+   end type
+
+   type, bind(C), public :: scd_server_stats
+      integer(c_int64_t) :: submitted, completed, failed, cancelled
+      integer(c_int64_t) :: columns
+      integer(c_int32_t) :: queued, running
+      integer(c_int32_t) :: peak_running
+      integer(c_int64_t) :: bytes_in_use
+      integer(c_int64_t) :: peak_bytes
+      real(c_double)     :: p50_ms, p99_ms
+      real(c_double)     :: busy_s
+   end type
+
    public :: scd_create, scd_destroy, scd_set_wavenumber, scd_set_green, scd_set_projectors, &
              scd_set_nearzone, scd_grid_from_mesh, scd_set_mesh, scd_build_projectors, &
-             scd_build_nearzone, scd_matvec, scd_gmres, scd_solve_columns, scd_compute_T_matrix, &
-             scd_last_error_f
+             scd_build_nearzone, scd_get_projectors, scd_nearzone_count, scd_get_nearzone, &
+             scd_matvec, scd_gmres, scd_solve_columns, scd_vswf_rhs, scd_compute_T_matrix, &
+             scd_get_timing, scd_profile_matvec, scd_T_assemble_noalloc, scd_column_latency, &
+             scd_nearzone_bytes, scd_selftest_waits, scd_last_error_f
+   public :: scd_server_create, scd_server_submit, scd_server_estimate, scd_server_poll, &
+             scd_server_wait, scd_server_result, scd_server_cancel, scd_server_stats_get, &
+             scd_server_destroy, scd_server_error_f
 
    interface
       integer(c_int) function scd_create(ctx, desc) bind(C, name="scd_create")
@@ -149,6 +185,129 @@ module scadyn_gpu
          complex(c_double_complex), intent(out) :: T(*)
          integer(c_int32_t), intent(out) :: iters(*)
       end function
+      ! the device operator back in the reference's layouts: S(27,T) .. indS(27,T)
+      integer(c_int) function scd_get_projectors(ctx, S, Sx, Sy, Sz, indS) bind(C, name="scd_get_projectors")
+         import :: c_ptr, c_int, c_int32_t, c_double_complex
+         type(c_ptr), value :: ctx
+         complex(c_double_complex), intent(out) :: S(*), Sx(*), Sy(*), Sz(*)
+         integer(c_int32_t), intent(out) :: indS(*)
+      end function
+      integer(c_int64_t) function scd_nearzone_count(ctx) bind(C, name="scd_nearzone_count")
+         import :: c_ptr, c_int64_t
+         type(c_ptr), value :: ctx
+      end function
+      ! sp_mat(3,3,B) in FP64, sp_ind(2,B)
+      integer(c_int) function scd_get_nearzone(ctx, B, sp_mat, sp_ind) bind(C, name="scd_get_nearzone")
+         import :: c_ptr, c_int, c_int32_t, c_int64_t, c_double_complex
+         type(c_ptr), value :: ctx
+         integer(c_int64_t), value :: B
+         complex(c_double_complex), intent(out) :: sp_mat(*)
+         integer(c_int32_t), intent(out) :: sp_ind(*)
+      end function
+      ! vswf2constant on the device: mat(3T, 2nm)
+      integer(c_int) function scd_vswf_rhs(ctx, Nmax, mat) bind(C, name="scd_vswf_rhs")
+         import :: c_ptr, c_int, c_int32_t, c_double_complex
+         type(c_ptr), value :: ctx
+         integer(c_int32_t), value :: Nmax
+         complex(c_double_complex), intent(out) :: mat(*)
+      end function
+      ! reset /= 0 clears the accumulated figures after reading them
+      integer(c_int) function scd_get_timing(ctx, t, reset) bind(C, name="scd_get_timing")
+         import :: c_ptr, c_int, c_int32_t, scd_timing
+         type(c_ptr), value :: ctx
+         type(scd_timing), intent(out) :: t
+         integer(c_int32_t), value :: reset
+      end function
+      integer(c_int) function scd_profile_matvec(ctx, reps, nrhs, precision) bind(C, name="scd_profile_matvec")
+         import :: c_ptr, c_int, c_int32_t
+         type(c_ptr), value :: ctx
+         integer(c_int32_t), value :: reps, nrhs, precision
+      end function
+      ! mat, X, T: DEVICE addresses (e.g. c_loc of CUDA Fortran device arrays); stream: a cudaStream_t
+      integer(c_int) function scd_T_assemble_noalloc(mat, n, ncol, X, ncb, T, stream) &
+            bind(C, name="scd_T_assemble_noalloc")
+         import :: c_ptr, c_int, c_int32_t, c_int64_t
+         type(c_ptr), value :: mat
+         integer(c_int64_t), value :: n
+         integer(c_int32_t), value :: ncol
+         type(c_ptr), value :: X
+         integer(c_int32_t), value :: ncb
+         type(c_ptr), value :: T, stream
+      end function
+      integer(c_int) function scd_column_latency(ctx, ncol, ms) bind(C, name="scd_column_latency")
+         import :: c_ptr, c_int, c_int32_t, c_double
+         type(c_ptr), value :: ctx
+         integer(c_int32_t), value :: ncol
+         real(c_double), intent(out) :: ms(*)
+      end function
+      integer(c_int64_t) function scd_nearzone_bytes(ctx) bind(C, name="scd_nearzone_bytes")
+         import :: c_ptr, c_int64_t
+         type(c_ptr), value :: ctx
+      end function
+      integer(c_int) function scd_selftest_waits(device) bind(C, name="scd_selftest_waits")
+         import :: c_int, c_int32_t
+         integer(c_int32_t), value :: device
+      end function
+      ! request server
+      integer(c_int) function scd_server_create(srv, device, hbm_budget, max_running) &
+            bind(C, name="scd_server_create")
+         import :: c_ptr, c_int, c_int32_t, c_int64_t
+         type(c_ptr), intent(out) :: srv
+         integer(c_int32_t), value :: device
+         integer(c_int64_t), value :: hbm_budget
+         integer(c_int32_t), value :: max_running
+      end function
+      integer(c_int) function scd_server_submit(srv, req, id) bind(C, name="scd_server_submit")
+         import :: c_ptr, c_int, c_int64_t, scd_request
+         type(c_ptr), value :: srv
+         type(scd_request), intent(in) :: req
+         integer(c_int64_t), intent(out) :: id
+      end function
+      integer(c_int) function scd_server_estimate(req, bytes) bind(C, name="scd_server_estimate")
+         import :: c_int, c_int64_t, scd_request
+         type(scd_request), intent(in) :: req
+         integer(c_int64_t), intent(out) :: bytes
+      end function
+      integer(c_int) function scd_server_poll(srv, id, state, status, latency_ms) bind(C, name="scd_server_poll")
+         import :: c_ptr, c_int, c_int32_t, c_int64_t, c_double
+         type(c_ptr), value :: srv
+         integer(c_int64_t), value :: id
+         integer(c_int32_t), intent(out) :: state, status
+         real(c_double), intent(out) :: latency_ms
+      end function
+      integer(c_int) function scd_server_wait(srv, id, timeout_s) bind(C, name="scd_server_wait")
+         import :: c_ptr, c_int, c_int64_t, c_double
+         type(c_ptr), value :: srv
+         integer(c_int64_t), value :: id
+         real(c_double), value :: timeout_s
+      end function
+      ! T(ncol, ncol); iters: c_loc of an (ncol) array, or c_null_ptr
+      integer(c_int) function scd_server_result(srv, id, T, iters) bind(C, name="scd_server_result")
+         import :: c_ptr, c_int, c_int64_t, c_double_complex
+         type(c_ptr), value :: srv
+         integer(c_int64_t), value :: id
+         complex(c_double_complex), intent(out) :: T(*)
+         type(c_ptr), value :: iters
+      end function
+      integer(c_int) function scd_server_cancel(srv, id) bind(C, name="scd_server_cancel")
+         import :: c_ptr, c_int, c_int64_t
+         type(c_ptr), value :: srv
+         integer(c_int64_t), value :: id
+      end function
+      integer(c_int) function scd_server_stats_get(srv, st) bind(C, name="scd_server_stats_get")
+         import :: c_ptr, c_int, scd_server_stats
+         type(c_ptr), value :: srv
+         type(scd_server_stats), intent(out) :: st
+      end function
+      type(c_ptr) function scd_server_error(srv, id) bind(C, name="scd_server_error")
+         import :: c_ptr, c_int64_t
+         type(c_ptr), value :: srv
+         integer(c_int64_t), value :: id
+      end function
+      integer(c_int) function scd_server_destroy(srv) bind(C, name="scd_server_destroy")
+         import :: c_ptr, c_int
+         type(c_ptr), value :: srv
+      end function
       integer(c_size_t) function c_strlen(s) bind(C, name="strlen")
          import :: c_ptr, c_size_t
          type(c_ptr), value :: s
@@ -161,13 +320,27 @@ contains
    function scd_last_error_f(ctx) result(msg)
       type(c_ptr), intent(in) :: ctx
       character(len=:), allocatable :: msg
+      msg = c_string(scd_last_error(ctx))
+   end function
+
+   ! scd_server_error as a Fortran string
+   function scd_server_error_f(srv, id) result(msg)
+      type(c_ptr), intent(in) :: srv
+      integer(c_int64_t), intent(in) :: id
+      character(len=:), allocatable :: msg
+      msg = c_string(scd_server_error(srv, id))
+   end function
+
+   ! a NUL-terminated C string (owned by the library) copied into a Fortran string
+   function c_string(s) result(msg)
+      type(c_ptr), intent(in) :: s
+      character(len=:), allocatable :: msg
       character(kind=c_char), pointer :: p(:)
-      type(c_ptr) :: s
       integer :: i, n
-      s = scd_last_error(ctx)
       n = int(c_strlen(s))
-      call c_f_pointer(s, p, [n])
       allocate (character(len=n) :: msg)
+      if (n == 0) return
+      call c_f_pointer(s, p, [n])
       do i = 1, n
          msg(i:i) = p(i)
       end do
