@@ -647,6 +647,486 @@ int orc_nearzone_const(const orc_geom *g, const zc *S, const zc *Sx, const zc *S
     return err;
 }
 
+/* ---------------------------------------------- linear basis (order 1) set-up */
+/* gradshape, src/common.f90:454-492: gradients of the four barycentric shape
+ * functions, dN[n][d] = dN_n/dx_d (the rot output is not needed here) */
+static void gradshape(const double tc[4][3], double dN[4][3]) {
+    double J[3][3];   /* J[row d][col e] = tc[e+1][d] - tc[0][d] */
+    for (int d = 0; d < 3; ++d) for (int e = 0; e < 3; ++e) J[d][e] = tc[e + 1][d] - tc[0][d];
+    const double detJ = J[0][0]*(J[1][1]*J[2][2] - J[1][2]*J[2][1]) - J[0][1]*(J[1][0]*J[2][2] - J[1][2]*J[2][0])
+                      + J[0][2]*(J[1][0]*J[2][1] - J[1][1]*J[2][0]);
+    double J0[3][3];
+    J0[0][0] = J[1][1]*J[2][2] - J[1][2]*J[2][1];
+    J0[1][0] = -(J[0][1]*J[2][2] - J[0][2]*J[2][1]);
+    J0[2][0] = (J[0][1]*J[1][2] - J[0][2]*J[1][1]);
+    J0[0][1] = -(J[1][0]*J[2][2] - J[1][2]*J[2][0]);
+    J0[1][1] = (J[0][0]*J[2][2] - J[0][2]*J[2][0]);
+    J0[2][1] = -(J[0][0]*J[1][2] - J[0][2]*J[1][0]);
+    J0[0][2] = J[1][0]*J[2][1] - J[1][1]*J[2][0];
+    J0[1][2] = -(J[0][0]*J[2][1] - J[0][1]*J[2][0]);
+    J0[2][2] = (J[0][0]*J[1][1] - J[0][1]*J[1][0]);
+    for (int d = 0; d < 3; ++d) {
+        dN[1][d] = J0[d][0]/detJ;
+        dN[2][d] = J0[d][1]/detJ;
+        dN[3][d] = J0[d][2]/detJ;
+        dN[0][d] = -dN[1][d] - dN[2][d] - dN[3][d];
+    }
+}
+
+/* analytical_integration_N, src/singularity_subtraction_N.f90:15-136: for the
+ * three shape functions of a triangle (vertex l <-> the edge opposite it) the
+ * integrals of N_l R^(2 nm - 3) over the triangle, out[nm-1][l], nm = 1..Np */
+#define NPMAX 2
+static void analytical_integration_N(const double tri[3][3], const double n[3], const double r[3], int Np,
+                                     double out[NPMAX][3]) {
+    static const int ind[7] = {3, 1, 2, 3, 1, 2, 3};
+    double Kl[NPMAX + 1] = {0}, Il[3] = {0}, tl[3] = {0}, hhl[3] = {0}, mvek[3][3] = {{0}};
+    double Inl[NPMAX + 1][3];
+    double rmp1[3]; sub3(r, tri[0], rmp1);
+    const double w0 = dot3(rmp1, n);
+    int nn = 0;
+    for (int m = 0; m <= Np; ++m) {
+        const int nexp = 2*m - 1;
+        for (int l = 1; l <= 3; ++l) {
+            const int l2 = ind[l + 2] - 1, l1 = ind[l + 1] - 1, l0 = ind[l] - 1, lm1 = ind[l - 1] - 1;
+            double slv[3], sl[3], ml[3], pl1mr[3], pl2mpl1[3], rmplm1[3], pl1mpl0[3];
+            sub3(tri[l2], tri[l1], slv);
+            const double normslv = sqrt(dot3(slv, slv));
+            for (int d = 0; d < 3; ++d) sl[d] = slv[d]/normslv;
+            cross3(sl, n, ml);
+            sub3(tri[l1], r, pl1mr);
+            const double tl0 = dot3(pl1mr, ml);
+            sub3(tri[l2], tri[l1], pl2mpl1);
+            const double ll = sqrt(dot3(pl2mpl1, pl2mpl1));
+            const double sml = dot3(pl1mr, sl), spl = sml + ll;
+            sub3(r, tri[lm1], rmplm1);
+            const double Rpl = sqrt(dot3(rmplm1, rmplm1)), Rml = sqrt(dot3(pl1mr, pl1mr));
+            const double R0l = sqrt(tl0*tl0 + w0*w0);
+            sub3(tri[l1], tri[l0], pl1mpl0);
+            const double hl = dot3(pl1mpl0, ml);
+            if (nexp == -1) {
+                for (int d = 0; d < 3; ++d) mvek[l - 1][d] = ml[d];
+                tl[l - 1] = tl0;
+                hhl[l - 1] = hl;
+                double Km3;
+                if (fabs(w0) > 1.0e-10) {
+                    const double Bl = atan((tl0*spl)/(R0l*R0l + fabs(w0)*Rpl)) - atan((tl0*sml)/(R0l*R0l + fabs(w0)*Rml));
+                    Km3 = 1.0/fabs(w0)*Bl;
+                } else {
+                    Km3 = 0.0;
+                    Il[l - 1] = 0.0;
+                }
+                if (fabs(Rml + sml) > 0.0) Il[l - 1] = log((Rpl + spl)/(Rml + sml));
+                else Il[l - 1] = 0.0;
+                Kl[nn] = Kl[nn] + 1.0/((double)nexp + 2.0)*((double)nexp*w0*w0*Km3 + tl0*Il[l - 1]);
+            } else {
+                Il[l - 1] = 1.0/((double)nexp + 1.0)*(spl*pow(Rpl, (double)nexp) - sml*pow(Rml, (double)nexp)
+                                                     + (double)nexp*R0l*R0l*Il[l - 1]);
+            }
+        }
+        if (nexp != -1)
+            Kl[nn] = 1.0/((double)nexp + 2.0)*((double)nexp*w0*w0*Kl[nn - 1] + (tl[0]*Il[0] + tl[1]*Il[1] + tl[2]*Il[2]));
+        for (int l = 0; l < 3; ++l) Inl[nn][l] = Il[l];
+        nn++;
+    }
+    double v1[NPMAX + 1][3];
+    for (int i1 = 0; i1 <= Np; ++i1)
+        for (int d = 0; d < 3; ++d) v1[i1][d] = Inl[i1][0]*mvek[0][d] + Inl[i1][1]*mvek[1][d] + Inl[i1][2]*mvek[2][d];
+    for (int nm = 1; nm <= Np; ++nm)
+        for (int l = 0; l < 3; ++l) {
+            const double dl = dot3(mvek[l], v1[nm]);
+            out[nm - 1][l] = 1.0/hhl[l]*(tl[l]*Kl[nm - 1] - 1.0/(2.0*(double)nm - 1.0)*dl);
+        }
+}
+
+/* singularity_subtraction_int_V_GN, src/singularity_subtraction_N.f90:140-238:
+ * I_j(rf) = int_B G(rf, r') N_j(r') dV' (j = 1..4), 1/R subtracted and
+ * integrated analytically (Np = 1); shape[i][j] at the 24 points Pb */
+static void int_V_GN(const double rf[3], double k, const double (*Pb)[3], const double *wb, const double B[4][3],
+                     const double (*shape)[4], zc out[4]) {
+    zc intR[4] = {0, 0, 0, 0};
+    double sw = 0; for (int i = 0; i < 24; ++i) sw += wb[i];
+    const double cut = 1.0e-10*pow(sw, F13);
+    for (int i = 0; i < 24; ++i) {
+        const double RR = norm2pt(Pb[i], rf);
+        zc II;
+        if (RR < cut) II = CMPLX(0.0, k/(4.0*PI));
+        else {
+            const double f = 1.0/(4*PI)*pow(k, 0.0)*1.0*pow(RR, -1.0);
+            II = Gr(rf, Pb[i], k) - f;
+        }
+        for (int j = 0; j < 4; ++j) intR[j] = intR[j] + II*shape[i][j]*wb[i];
+    }
+    double intR5[4] = {0}, intR6[4] = {0}, dN[4][3];
+    gradshape(B, dN);
+    for (int f1 = 0; f1 < 4; ++f1) {
+        double tri[3][3], tn[3], i2[NPMAX][3], rr2[3];
+        tetra_face(B, f1, tri);
+        tri_n_vector(tri, tn);
+        analytical_integration_N(tri, tn, rf, 2, i2);
+        sub3(tri[0], rf, rr2);
+        const double a1 = dot3(tn, rr2);
+        for (int l = 0; l < 3; ++l) intR6[FACE[f1][l]] += i2[0][l]*a1*0.5;
+        const double s2 = i2[1][0] + i2[1][1] + i2[1][2];
+        for (int j = 0; j < 4; ++j) intR5[j] += dot3(tn, dN[j])*s2*0.5*1.0;
+    }
+    for (int j = 0; j < 4; ++j) out[j] = intR[j] + 1.0/(4*PI)*1.0*1.0*(-intR5[j] + intR6[j]);
+}
+
+/* singularity_subtraction_int_S_GN, src/singularity_subtraction_N.f90:242-294:
+ * int_tri G(rf, r') N_l(r') dS' for the triangle's three shape functions */
+static void int_S_GN(const double rf[3], const double tri[3][3], const double tn[3], double k,
+                     const double (*Pb)[3], const double *wb, zc out[3]) {
+    zc intR[3] = {0, 0, 0};
+    double sw = 0; for (int i = 0; i < 7; ++i) sw += wb[i];
+    const double cut = 1.0e-10*pow(sw, 0.5);
+    for (int i = 0; i < 7; ++i) {
+        const double R = norm2pt(Pb[i], rf);
+        zc II;
+        if (R < cut) II = CMPLX(0.0, k/(4*PI));
+        else II = Gr(rf, Pb[i], k) - 1.0/(4*PI)*pow(k, 0.0)*1.0*pow(R, -1.0);
+        const double s[3] = {1.0 - QR5P[i][0] - QR5P[i][1], QR5P[i][0], QR5P[i][1]};
+        for (int l = 0; l < 3; ++l) intR[l] = intR[l] + II*wb[i]*s[l];
+    }
+    double i2[NPMAX][3];
+    analytical_integration_N(tri, tn, rf, 1, i2);
+    for (int l = 0; l < 3; ++l) out[l] = intR[l] + 1.0/(4*PI)*1.0*1.0*i2[0][l];
+}
+
+/* tet shape functions at the 24 order-5 points: shape[i][j] */
+static void tet5_shape(double shape[24][4]) {
+    for (int i = 0; i < 24; ++i) {
+        shape[i][0] = 1 - QT5P[i][0] - QT5P[i][1] - QT5P[i][2];
+        shape[i][1] = QT5P[i][0]; shape[i][2] = QT5P[i][1]; shape[i][3] = QT5P[i][2];
+    }
+}
+
+/* single-point forms of the above for tests: B (4,3) vertices, tri (3,3) */
+void orc_int_V_GN(const double rf[3], double k, const double B[12], zc out[4]) {
+    quad_init();
+    double Bc[4][3], Pb[24][3], wb[24], shape[24][4];
+    memcpy(Bc, B, sizeof Bc);
+    linmap_tet(Bc, 24, (const double (*)[3])QT5P, QT5W, Pb, wb);
+    tet5_shape(shape);
+    int_V_GN(rf, k, (const double (*)[3])Pb, wb, (const double (*)[3])Bc, (const double (*)[4])shape, out);
+}
+void orc_int_S_GN(const double rf[3], const double tri[9], double k, zc out[3]) {
+    quad_init();
+    double t[3][3], n[3], Pb[7][3], wb[7];
+    memcpy(t, tri, sizeof t);
+    tri_n_vector(t, n);
+    linmap_tri(t, 7, (const double (*)[2])QR5P, QR5W, Pb, wb);
+    int_S_GN(rf, (const double (*)[3])t, n, k, (const double (*)[3])Pb, wb, out);
+}
+void orc_gradshape(const double tc[12], double dN[12]) {
+    double t[4][3], d[4][3];
+    memcpy(t, tc, sizeof t);
+    gradshape(t, d);
+    memcpy(dN, d, sizeof d);
+}
+
+/* pfft_projection_lin, src/projection.f90:170-338: four projector columns per
+ * tet (node n of tet t in column 4(t-1)+n), order-5 tet and triangle rules.
+ * Outputs (27, 4T). */
+int orc_pfft_projection_lin(const orc_geom *g, zc *S, zc *Sx, zc *Sy, zc *Sz, int32_t *indS) {
+    quad_init();
+    double P0[98][3], Ps[98][3], shape[24][4];
+    sample_points_cube(P0);
+    tet5_shape(shape);
+    for (int m = 0; m < 98; ++m) for (int d = 0; d < 3; ++d) Ps[m][d] = 2.0*g->box_delta*P0[m][d];
+    const double k = g->k;
+    double tc[4][3], cp[3], node1[3], cpc[3];
+    tet_coord(g->coord, g->etopol, 0, tc);
+    for (int d = 0; d < 3; ++d) cp[d] = (tc[0][d] + tc[1][d] + tc[2][d] + tc[3][d])/4;
+    int cube = orc_point_in_cube(g, cp);
+    if (cube == 0) return -2;
+    const int32_t *bn = g->etopol_box + 27*(cube - 1);
+    orc_node_coord(g, bn[0], node1);
+    for (int d = 0; d < 3; ++d) cpc[d] = node1[d] + g->box_delta/2.0;
+    zc *W = (zc *)malloc(sizeof(zc)*98*27), *WW = (zc *)malloc(sizeof(zc)*27*98);
+    for (int m = 0; m < 98; ++m) {
+        double r[3] = {Ps[m][0] + cpc[0], Ps[m][1] + cpc[1], Ps[m][2] + cpc[2]};
+        for (int u = 0; u < 27; ++u) { double pn[3]; orc_node_coord(g, bn[u], pn); W[98*u + m] = Gr(r, pn, k); }
+    }
+    orc_pinv(98, 27, W, WW);
+    int err = 0;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 16)
+#endif
+    for (int t = 0; t < g->T; ++t) {
+        double Bc[4][3], c3[3], n1c[3], cc[3], Pb[24][3], wb[24], dN[4][3];
+        tet_coord(g->coord, g->etopol, t, Bc);
+        const double volB = tetra_volume(Bc);
+        linmap_tet(Bc, 24, (const double (*)[3])QT5P, QT5W, Pb, wb);
+        gradshape(Bc, dN);
+        for (int d = 0; d < 3; ++d) c3[d] = (Bc[0][d] + Bc[1][d] + Bc[2][d] + Bc[3][d])/4;
+        const int cb = orc_point_in_cube(g, c3);
+        if (cb == 0) { err = -2; continue; }
+        const int32_t *bt = g->etopol_box + 27*(cb - 1);
+        orc_node_coord(g, bt[0], n1c);
+        for (int d = 0; d < 3; ++d) cc[d] = n1c[d] + g->box_delta/2.0;
+        zc Q[98][4], Q2[3][98][4];
+        double ftri[4][3][3], fn[4][3], Pt[4][7][3], wt[4][7];
+        for (int f = 0; f < 4; ++f) {
+            tetra_face(Bc, f, ftri[f]);
+            linmap_tri(ftri[f], 7, (const double (*)[2])QR5P, QR5W, Pt[f], wt[f]);
+            tri_n_vector(ftri[f], fn[f]);
+        }
+        for (int m = 0; m < 98; ++m) {
+            const double r[3] = {Ps[m][0] + cc[0], Ps[m][1] + cc[1], Ps[m][2] + cc[2]};
+            for (int n = 0; n < 4; ++n) { Q[m][n] = 0; Q2[0][m][n] = Q2[1][m][n] = Q2[2][m][n] = 0; }
+            for (int i = 0; i < 24; ++i) {
+                const zc gg = Gr(r, Pb[i], k);
+                for (int n = 0; n < 4; ++n) Q[m][n] = Q[m][n] + shape[i][n]*gg*wb[i];
+            }
+            for (int f = 0; f < 4; ++f) {
+                zc q2[3] = {0, 0, 0};
+                for (int i = 0; i < 7; ++i) {
+                    const double s[3] = {1.0 - QR5P[i][0] - QR5P[i][1], QR5P[i][0], QR5P[i][1]};
+                    const zc gg = Gr(r, Pt[f][i], k);
+                    for (int l = 0; l < 3; ++l) q2[l] = q2[l] + s[l]*wt[f][i]*gg;
+                }
+                for (int l = 0; l < 3; ++l)
+                    for (int d = 0; d < 3; ++d) Q2[d][m][FACE[f][l]] += fn[f][d]*q2[l];
+            }
+        }
+        const double sv = sqrt(volB);
+        for (int n = 0; n < 4; ++n) {
+            const size_t col = 27*(size_t)(4*t + n);
+            for (int u = 0; u < 27; ++u) {
+                zc s0 = 0, sd[3] = {0, 0, 0}, qd[3] = {0, 0, 0};
+                for (int m = 0; m < 98; ++m) {
+                    const zc w = WW[27*m + u];
+                    const zc qdn = Q[m][0] + Q[m][1] + Q[m][2] + Q[m][3];
+                    s0 += w*Q[m][n];
+                    for (int d = 0; d < 3; ++d) { sd[d] += w*Q2[d][m][n]; qd[d] += w*(qdn*dN[n][d]); }
+                }
+                S[col + u] = s0/sv;
+                Sx[col + u] = (sd[0] - qd[0])/sv;
+                Sy[col + u] = (sd[1] - qd[1])/sv;
+                Sz[col + u] = (sd[2] - qd[2])/sv;
+                indS[col + u] = bt[u];
+            }
+        }
+    }
+    free(W); free(WW);
+    return err;
+}
+
+/* One 12x12 block of compute_near_zone_interactions_lin
+ * (src/precorrection.f90:268-371) for test tet tT <= basis tet tB (1-based),
+ * V(4c + n, 4c' + n') column-major in blk[r + 12 q]; G is compute_pG of their
+ * boxes (G(i1, i2) at G[i1 + 27 i2]).  Pieces: integrate_NN (:375-405),
+ * integrate_V_V_GNN (:409-445), integrate_dV_V_GNN (:449-524),
+ * integrate_dV_dV_GNN (:528-617), integrate_V_dV_GNN (:621-685), aloks
+ * (:689-717), precorrect_lin (:86-127). */
+static void near_block_lin(const orc_geom *g, const zc *S, const zc *Sx, const zc *Sy, const zc *Sz, const zc *G,
+                           int tT, int tB, zc blk[144]) {
+    const double k = g->k;
+    double Tc[4][3], Bc[4][3], dNT[4][3], dNB[4][3], shape[24][4];
+    tet_coord(g->coord, g->etopol, tT - 1, Tc);
+    tet_coord(g->coord, g->etopol, tB - 1, Bc);
+    const double volT = tetra_volume(Tc), volB = tetra_volume(Bc);
+    gradshape(Tc, dNT);
+    gradshape(Bc, dNB);
+    tet5_shape(shape);
+    /* precorrect_lin: corr(n_T, n_B) and corr2(4r + n_T, 4c + n_B) */
+    zc corr[144], corr2[144];
+    for (int q = 0; q < 144; ++q) corr[q] = corr2[q] = 0;
+    const zc *PS[4] = {S, Sx, Sy, Sz};
+    for (int i1 = 0; i1 < 4; ++i1) {
+        zc gv[4][27];
+        for (int s = 0; s < 4; ++s) {
+            const zc *pb = PS[s] + 27*(size_t)(4*(tB - 1) + i1);
+            for (int a = 0; a < 27; ++a) {
+                zc acc = 0;
+                for (int b = 0; b < 27; ++b) acc += G[a + 27*b]*pb[b];
+                gv[s][a] = acc;
+            }
+        }
+        for (int i2 = 0; i2 < 4; ++i2) {
+            const size_t colT = 27*(size_t)(4*(tT - 1) + i2);
+            zc a0 = 0;
+            for (int a = 0; a < 27; ++a) a0 += gv[0][a]*S[colT + a];
+            for (int c = 0; c < 3; ++c) corr[(4*c + i2) + 12*(4*c + i1)] = a0;
+            for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) {
+                    zc s = 0;
+                    for (int a = 0; a < 27; ++a) s += gv[1 + c][a]*PS[1 + r][colT + a];
+                    corr2[(4*r + i2) + 12*(4*c + i1)] = s;
+                }
+        }
+    }
+    const double sv = sqrt(volT*volB);
+    for (int q = 0; q < 144; ++q) { corr[q] = corr[q]*sv; corr2[q] = corr2[q]*sv; }
+    double Pt[24][3], wt[24], Pb[24][3], wb[24];
+    linmap_tet(Tc, 24, (const double (*)[3])QT5P, QT5W, Pt, wt);
+    linmap_tet(Bc, 24, (const double (*)[3])QT5P, QT5W, Pb, wb);
+    /* integrate_NN */
+    zc alok[144];
+    for (int q = 0; q < 144; ++q) alok[q] = 0;
+    if (tT == tB) {
+        double intN[4][4] = {{0}};
+        for (int i = 0; i < 24; ++i)
+            for (int b = 0; b < 4; ++b)
+                for (int a = 0; a < 4; ++a) intN[a][b] += shape[i][b]*shape[i][a]*wt[i];
+        for (int c = 0; c < 3; ++c)
+            for (int a = 0; a < 4; ++a) for (int b = 0; b < 4; ++b) alok[(4*c + a) + 12*(4*c + b)] = intN[a][b];
+    }
+    /* integrate_V_V_GNN: GNN(a, b) */
+    zc GNN[4][4] = {{0}};
+    for (int i = 0; i < 24; ++i) {
+        zc Iv[4];
+        int_V_GN(Pt[i], k, (const double (*)[3])Pb, wb, (const double (*)[3])Bc, (const double (*)[4])shape, Iv);
+        for (int a = 0; a < 4; ++a)
+            for (int b = 0; b < 4; ++b) GNN[a][b] = GNN[a][b] + Iv[b]*shape[i][a]*wt[i];
+    }
+    /* faces of both tets with their order-5 points */
+    double Ttri[4][3][3], Tn[4][3], Ptt[4][7][3], wtt[4][7];
+    double Btri[4][3][3], Bn[4][3], Pbt[4][7][3], wbt[4][7];
+    for (int f = 0; f < 4; ++f) {
+        tetra_face(Tc, f, Ttri[f]); tri_n_vector(Ttri[f], Tn[f]);
+        linmap_tri(Ttri[f], 7, (const double (*)[2])QR5P, QR5W, Ptt[f], wtt[f]);
+        tetra_face(Bc, f, Btri[f]); tri_n_vector(Btri[f], Bn[f]);
+        linmap_tri(Btri[f], 7, (const double (*)[2])QR5P, QR5W, Pbt[f], wbt[f]);
+    }
+    /* integrate_dV_V_GNN: alok4(row, 4c + b) = II4(row) dN_B[b][c] */
+    zc II4[12];
+    for (int q = 0; q < 12; ++q) II4[q] = 0;
+    for (int ft = 0; ft < 4; ++ft) {
+        zc intN[4] = {0, 0, 0, 0};
+        for (int i = 0; i < 7; ++i) {
+            zc Iv[4];
+            int_V_GN(Ptt[ft][i], k, (const double (*)[3])Pb, wb, (const double (*)[3])Bc, (const double (*)[4])shape, Iv);
+            const zc Is = Iv[0] + Iv[1] + Iv[2] + Iv[3];
+            const double s[3] = {1.0 - QR5P[i][0] - QR5P[i][1], QR5P[i][0], QR5P[i][1]};
+            for (int l = 0; l < 3; ++l) intN[FACE[ft][l]] = intN[FACE[ft][l]] + Is*s[l]*wtt[ft][i];
+        }
+        for (int r = 0; r < 3; ++r)
+            for (int a = 0; a < 4; ++a) II4[4*r + a] = II4[4*r + a] + intN[a]*Tn[ft][r];
+    }
+    /* J_c(b; rf) = sum over the faces of B of n_c int_face G N_b dS' */
+#define JSUM(rf, J)                                                                                   \
+    do {                                                                                              \
+        for (int q_ = 0; q_ < 12; ++q_) (J)[q_] = 0;                                                  \
+        for (int fb_ = 0; fb_ < 4; ++fb_) {                                                           \
+            zc in_[3];                                                                                \
+            int_S_GN((rf), (const double (*)[3])Btri[fb_], Bn[fb_], k, (const double (*)[3])Pbt[fb_], \
+                     wbt[fb_], in_);                                                                  \
+            for (int l_ = 0; l_ < 3; ++l_)                                                            \
+                for (int c_ = 0; c_ < 3; ++c_)                                                        \
+                    (J)[4*c_ + FACE[fb_][l_]] = (J)[4*c_ + FACE[fb_][l_]] + in_[l_]*Bn[fb_][c_];      \
+        }                                                                                             \
+    } while (0)
+    /* integrate_dV_dV_GNN */
+    zc alok2[144];
+    for (int q = 0; q < 144; ++q) alok2[q] = 0;
+    for (int ft = 0; ft < 4; ++ft) {
+        zc II[3][4][4];   /* II[c][a][b] */
+        memset(II, 0, sizeof II);
+        for (int i = 0; i < 7; ++i) {
+            zc J[12];
+            JSUM(Ptt[ft][i], J);
+            const double s[3] = {1.0 - QR5P[i][0] - QR5P[i][1], QR5P[i][0], QR5P[i][1]};
+            for (int l = 0; l < 3; ++l)
+                for (int c = 0; c < 3; ++c)
+                    for (int b = 0; b < 4; ++b)
+                        II[c][FACE[ft][l]][b] = II[c][FACE[ft][l]][b] + J[4*c + b]*s[l]*wtt[ft][i];
+        }
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 3; ++c)
+                for (int a = 0; a < 4; ++a)
+                    for (int b = 0; b < 4; ++b)
+                        alok2[(4*r + a) + 12*(4*c + b)] = alok2[(4*r + a) + 12*(4*c + b)] + II[c][a][b]*Tn[ft][r];
+    }
+    /* integrate_V_dV_GNN: alok5(4r + a, col) = dN_T[a][r] II5(col) */
+    zc II5[12];
+    for (int q = 0; q < 12; ++q) II5[q] = 0;
+    for (int i = 0; i < 24; ++i) {
+        zc J[12];
+        JSUM(Pt[i], J);
+        for (int q = 0; q < 12; ++q) II5[q] = II5[q] + J[q]*wt[i];
+    }
+#undef JSUM
+    /* aloks and the block */
+    zc sG = 0;
+    for (int b = 0; b < 4; ++b) for (int a = 0; a < 4; ++a) sG += GNN[a][b];
+    const zc ep = g->param[tT - 1];
+    const double k2 = k*k, inv = 1.0/sqrt(volB*volT);
+    for (int c = 0; c < 3; ++c)
+        for (int b = 0; b < 4; ++b)
+            for (int r = 0; r < 3; ++r)
+                for (int a = 0; a < 4; ++a) {
+                    const int row = 4*r + a, col = 4*c + b, q = row + 12*col;
+                    const zc alok1 = r == c ? GNN[a][b] : 0;
+                    const zc alok3 = (dNT[a][r]*dNB[b][c])*sG;
+                    const zc alok4 = II4[row]*dNB[b][c];
+                    const zc alok5 = dNT[a][r]*II5[col];
+                    blk[q] = inv*(alok[q]/(ep - 1.0) + (-k2*(alok1 - corr[q]) + (alok2[q] + alok3 - alok4 - alok5) - corr2[q]));
+                }
+}
+
+/* compute_near_zone_interactions_lin, src/precorrection.f90:268-371: 12x12
+ * blocks sp(12,12,B) for the same tet pairs, in the same order, as the
+ * constant-basis assembly. */
+int orc_nearzone_lin(const orc_geom *g, const zc *S, const zc *Sx, const zc *Sy, const zc *Sz,
+                     int64_t B, fc *sp32, zc *sp64, int32_t *sp_ind, int nthreads) {
+    quad_init();
+    const int NC = g->N_cubes;
+    int64_t *off = (int64_t *)malloc(sizeof(int64_t)*(size_t)(NC + 1));
+    off[0] = 0;
+    {
+        int32_t near[125];
+        for (int c = 1; c <= NC; ++c) {
+            int nn = orc_find_near_cubes(g, c, near);
+            off[c] = off[c - 1] + count_cube(g, c, near, nn);
+        }
+    }
+    if (off[NC] != B) { free(off); return -3; }
+    const double k = g->k;
+    int err = 0;
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+#endif
+    for (int tcube = 1; tcube <= NC; ++tcube) {
+        const int32_t *tests = g->tetras + (size_t)g->N_tet_cube*(tcube - 1);
+        if (tests[0] == 0) continue;
+        int32_t near[125];
+        int nn = orc_find_near_cubes(g, tcube, near);
+        int64_t blok = off[tcube - 1];
+        zc G[27*27];
+        for (int i1 = 0; i1 < nn; ++i1) {
+            const int bcube = near[i1];
+            const int32_t *bases = g->tetras + (size_t)g->N_tet_cube*(bcube - 1);
+            const int32_t *tb = g->etopol_box + 27*(tcube - 1), *bb = g->etopol_box + 27*(bcube - 1);
+            for (int a = 0; a < 27; ++a) {
+                double r[3]; orc_node_coord(g, tb[a], r);
+                for (int b = 0; b < 27; ++b) {
+                    if (tb[a] != bb[b]) { double rp[3]; orc_node_coord(g, bb[b], rp); G[a + 27*b] = Gr(r, rp, k); }
+                    else G[a + 27*b] = 0;
+                }
+            }
+            for (int t1 = 0; t1 < g->N_tet_cube && tests[t1]; ++t1)
+                for (int b1 = 0; b1 < g->N_tet_cube && bases[b1]; ++b1) {
+                    const int tT = tests[t1], tB = bases[b1];
+                    if (tB < tT) continue;
+                    zc blk[144];
+                    near_block_lin(g, S, Sx, Sy, Sz, G, tT, tB, blk);
+                    for (int q = 0; q < 144; ++q) {
+                        if (sp32) sp32[144*blok + q] = (fc)blk[q];
+                        if (sp64) sp64[144*blok + q] = blk[q];
+                    }
+                    sp_ind[2*blok] = tT; sp_ind[2*blok + 1] = tB;
+                    blok++;
+                }
+        }
+        if (blok != off[tcube]) err = -4;
+    }
+    free(off);
+    return err;
+}
+
 /* -------------------------------------------------------------------- FFT */
 /* Recursive mixed-radix DFT with FFTW's sign convention (forward exp(-i),
  * unnormalised).  Any length; small prime factors. */

@@ -67,6 +67,20 @@ int64_t orc_nearzone_count(const orc_geom *g);
 int  orc_nearzone_const(const orc_geom *g, const zc *S, const zc *Sx, const zc *Sy, const zc *Sz,
                         int64_t B, fc *sp_mat32, zc *sp_mat64, int32_t *sp_ind, int nthreads);
 
+/* linear basis set-up (mesh%order = 1): projectors (27, 4T) with column
+ * 4(t-1)+n for node n of tet t (src/projection.f90:170-338), and 12x12 near-zone
+ * blocks sp(12,12,B) over the same tet pairs as the constant basis
+ * (src/precorrection.f90:268-725, src/singularity_subtraction_N.f90) */
+int  orc_pfft_projection_lin(const orc_geom *g, zc *S, zc *Sx, zc *Sy, zc *Sz, int32_t *indS);
+int  orc_nearzone_lin(const orc_geom *g, const zc *S, const zc *Sx, const zc *Sy, const zc *Sz,
+                      int64_t B, fc *sp_mat32, zc *sp_mat64, int32_t *sp_ind, int nthreads);
+
+/* test forms: singularity_subtraction_int_V_GN / _int_S_GN at one point with
+ * the order-5 rules, B (4,3) and tri (3,3) vertex coordinates; gradshape */
+void orc_int_V_GN(const double rf[3], double k, const double B[12], zc out[4]);
+void orc_int_S_GN(const double rf[3], const double tri[9], double k, zc out[3]);
+void orc_gradshape(const double tc[12], double dN[12]);
+
 /* Green's function grid (src/build_G.f90) */
 int  orc_build_G(const orc_geom *g, zc *Fg);
 

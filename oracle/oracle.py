@@ -153,6 +153,28 @@ class Geometry:
             raise RuntimeError(f"nearzone failed ({rc})")
         return (sp64 if fp64 else sp32), ind
 
+    def projectors_lin(self):
+        """pfft_projection_lin -> S, Sx, Sy, Sz (4T,27) c128 and indS (4T,27) int32; row 4t+n is node n of tet t."""
+        T4 = 4 * self.T
+        S, Sx, Sy, Sz = (np.zeros((T4, 27), np.complex128) for _ in range(4))
+        indS = np.zeros((T4, 27), np.int32)
+        rc = lib().orc_pfft_projection_lin(C.byref(self._g), _p(S), _p(Sx), _p(Sy), _p(Sz), _p(indS))
+        if rc != 0:
+            raise RuntimeError(f"linear projection failed ({rc})")
+        return S, Sx, Sy, Sz, indS
+
+    def nearzone_lin(self, S, Sx, Sy, Sz, fp64: bool = False, nthreads: int = 0):
+        """compute_near_zone_interactions_lin -> (sp_mat (B,12,12) [memory (12,12,B)], sp_ind (B,2))."""
+        B = lib().orc_nearzone_count(C.byref(self._g))
+        sp32 = None if fp64 else np.zeros((B, 12, 12), np.complex64)
+        sp64 = np.zeros((B, 12, 12), np.complex128) if fp64 else None
+        ind = np.zeros((B, 2), np.int32)
+        rc = lib().orc_nearzone_lin(C.byref(self._g), _p(S), _p(Sx), _p(Sy), _p(Sz), C.c_int64(B),
+                                    _p(sp32), _p(sp64), _p(ind), nthreads)
+        if rc != 0:
+            raise RuntimeError(f"linear near zone failed ({rc})")
+        return (sp64 if fp64 else sp32), ind
+
     def build_G(self):
         """build_G -> Fg (2Nz, 2Ny, 2Nx) c128 (memory of Fortran Fg(2Nx,2Ny,2Nz))."""
         Fg = np.zeros((2 * self.Nz, 2 * self.Ny, 2 * self.Nx), np.complex128)
@@ -357,3 +379,36 @@ def setup(mesh, k, grid_size=1.8, fp64_near=False, nthreads=0):
     Fg = g.build_G()
     sp, ind = g.nearzone(S, Sx, Sy, Sz, fp64=fp64_near, nthreads=nthreads)
     return Operator(g, S, Sx, Sy, Sz, indS, Fg, sp, ind)
+
+
+def setup_lin(mesh, k, grid_size=1.8, fp64_near=False, nthreads=0):
+    """Per-wavelength setup with the linear basis (mesh%order = 1): geometry,
+    pfft_projection_lin, Green grid, compute_near_zone_interactions_lin."""
+    g = Geometry(mesh.coord, mesh.etopol, mesh.param, k=k, grid_size=grid_size)
+    S, Sx, Sy, Sz, indS = g.projectors_lin()
+    Fg = g.build_G()
+    sp, ind = g.nearzone_lin(S, Sx, Sy, Sz, fp64=fp64_near, nthreads=nthreads)
+    return Operator(g, S, Sx, Sy, Sz, indS, Fg, sp, ind, order=1)
+
+
+def int_V_GN(rf, k, B):
+    """singularity_subtraction_int_V_GN at one point: int_B G(rf, r') N_j(r') dV', j = 1..4; B (4,3)."""
+    out = np.zeros(4, np.complex128)
+    lib().orc_int_V_GN(_p(np.ascontiguousarray(rf, np.float64)), C.c_double(k),
+                       _p(np.ascontiguousarray(B, np.float64)), _p(out))
+    return out
+
+
+def int_S_GN(rf, k, tri):
+    """singularity_subtraction_int_S_GN at one point: int_tri G(rf, r') N_l(r') dS', l = 1..3; tri (3,3)."""
+    out = np.zeros(3, np.complex128)
+    lib().orc_int_S_GN(_p(np.ascontiguousarray(rf, np.float64)), C.c_double(k),
+                       _p(np.ascontiguousarray(tri, np.float64)), _p(out))
+    return out
+
+
+def gradshape(tc):
+    """gradshape: dN (4,3), row n = gradient of the shape function of vertex n."""
+    out = np.zeros((4, 3), np.float64)
+    lib().orc_gradshape(_p(np.ascontiguousarray(tc, np.float64)), _p(out))
+    return out
