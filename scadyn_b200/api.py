@@ -157,9 +157,12 @@ class Solver:
     """One device context (scd_ctx) for one mesh and grid."""
 
     def __init__(self, Nx, Ny, Nz, delta, min_coord, T, device=0, order=0):
-        """order 1 (linear basis): 4 projector columns and 12 unknowns per tet;
-        only the host-built operator path (set_projectors, set_nearzone with
-        12x12 blocks, compute_Ax2, gmres, solve_columns) is open."""
+        """order 1 (linear basis): 4 projector columns and 12 unknowns per tet.
+        The operator comes from the host (set_projectors, set_nearzone with
+        12x12 blocks) or from the mesh on the device (set_mesh,
+        pfft_projection_lin, compute_near_zone_interactions_lin); compute_Ax2,
+        gmres and solve_columns run on it.  The VSWF right-hand sides and the
+        T-matrix entry points are constant-basis only, as in the reference."""
         self.lib = load_library()
         d = GridDesc()
         d.Nx, d.Ny, d.Nz, d.delta = Nx, Ny, Nz, delta
@@ -182,7 +185,7 @@ class Solver:
 
     @classmethod
     def from_desc(cls, d: GridDesc, device=0):
-        return cls(d.Nx, d.Ny, d.Nz, d.delta, list(d.min_coord), d.T, device)
+        return cls(d.Nx, d.Ny, d.Nz, d.delta, list(d.min_coord), d.T, device, order=d.order)
 
     def _chk(self, rc, what, ok=(SCD_OK,)):
         if rc not in ok:
@@ -246,14 +249,24 @@ class Solver:
         self._chk(self.lib.scd_get_projectors(self.ctx, _p(S), _p(Sx), _p(Sy), _p(Sz), _p(indS)), "get_projectors")
         return S, Sx, Sy, Sz, indS
 
+    def pfft_projection_lin(self):
+        """Linear-basis projectors on the device (src/projection.f90:170-338): (4T, 27) columns."""
+        return self.pfft_projection_const()
+
     def compute_near_zone_interactions_const(self, storage=STORE_C64):
         self._chk(self.lib.scd_build_nearzone(self.ctx, storage), "build_nearzone")
 
+    def compute_near_zone_interactions_lin(self, storage=STORE_C64):
+        """Linear-basis 12x12 near-zone blocks on the device (src/precorrection.f90:268-725)."""
+        self.compute_near_zone_interactions_const(storage)
+
     def get_nearzone(self):
+        """(sp_mat, sp_ind) ordered by (tet_T, tet_B): (B, 3, 3) blocks, or (B, 12, 12) with the linear basis."""
         B = self.lib.scd_nearzone_count(self.ctx)
         if B < 0:
             raise ScadynError(SCD_NOT_READY, "near zone not set")
-        sp = np.zeros((B, 3, 3), np.complex128)
+        nbk = 12 if self.order == 1 else 3
+        sp = np.zeros((B, nbk, nbk), np.complex128)
         ind = np.zeros((B, 2), np.int32)
         self._chk(self.lib.scd_get_nearzone(self.ctx, B, _p(sp), _p(ind)), "get_nearzone")
         return sp, ind

@@ -20,57 +20,16 @@
 #include <vector>
 
 #include "ctx.h"
+#include "geom.cuh"
+#include "lin_setup.cuh"
 
 namespace {
-
-constexpr double PI = 3.141592653589793;            // src/common.f90:20
-constexpr double F13_D = (double)(1.0f / 3.0f);     // Fortran default-real 1.0/3.0
 
 // ------------------------------------------------------------- quadrature
 __constant__ double cQT5[24][4];   // (xi, eta, zeta, w)
 __constant__ double cQR5[7][3];    // (xi, eta, w)
 __constant__ double cPs[98][3];    // cube sample points (unscaled)
 
-struct HostQuad {
-    double t5[24][4];
-    double r5[7][3];
-    double ps[98][3];
-    HostQuad() {
-        const double A[3][2] = {{3.561913862225449e-01, 2.146028712591517e-01},
-                                {8.779781243961660e-01, 4.067395853461134e-02},
-                                {3.298632957317306e-02, 3.223378901422757e-01}};
-        const double W4[3] = {6.653791709694644e-03, 1.679535175886776e-03, 9.226196923942397e-03};
-        int p = 0;
-        for (int o = 0; o < 3; ++o) {
-            const double a = A[o][0], b = A[o][1];
-            const double pts[4][3] = {{a, b, b}, {b, b, b}, {b, b, a}, {b, a, b}};
-            for (int i = 0; i < 4; ++i, ++p) {
-                t5[p][0] = pts[i][0]; t5[p][1] = pts[i][1]; t5[p][2] = pts[i][2]; t5[p][3] = W4[o];
-            }
-        }
-        const double c = 6.366100187501753e-02, d = 2.696723314583159e-01, e = 6.030056647916491e-01;
-        const double p12[12][3] = {{d, c, c}, {c, d, c}, {c, c, d}, {e, c, c}, {c, e, c}, {c, c, e},
-                                   {c, d, e}, {d, e, c}, {e, c, d}, {c, e, d}, {d, c, e}, {e, d, c}};
-        for (int i = 0; i < 12; ++i, ++p) {
-            t5[p][0] = p12[i][0]; t5[p][1] = p12[i][1]; t5[p][2] = p12[i][2]; t5[p][3] = 8.035714285714281e-03;
-        }
-        const double t0 = 3.333333333333330e-01, a1 = 5.971587178977000e-02, b1 = 4.701420641051150e-01;
-        const double a2 = 7.974269853530870e-01, b2 = 1.012865073234560e-01;
-        const double w1 = 6.619707639425300e-02, w2 = 6.296959027241350e-02;
-        const double tri[7][3] = {{t0, t0, 1.125000000000000e-01}, {a1, b1, w1}, {b1, b1, w1}, {b1, a1, w1},
-                                  {a2, b2, w2}, {b2, b2, w2}, {b2, a2, w2}};
-        std::memcpy(r5, tri, sizeof tri);
-        const double v[5] = {-1.0, -0.5, 0.0, 0.5, 1.0};
-        int n = 0;
-        auto put = [&](double x, double y, double z) { ps[n][0] = x; ps[n][1] = y; ps[n][2] = z; ++n; };
-        for (int iy = 4; iy >= 0; --iy) for (int ix = 0; ix < 5; ++ix) put(v[ix], v[iy], -1.0);
-        for (int iy = 0; iy < 5; ++iy) for (int ix = 0; ix < 5; ++ix) put(v[ix], v[iy], 1.0);
-        for (int iz = 1; iz <= 3; ++iz) for (int ix = 0; ix < 5; ++ix) put(v[ix], -1.0, v[iz]);
-        for (int iz = 3; iz >= 1; --iz) for (int ix = 0; ix < 5; ++ix) put(v[ix], 1.0, v[iz]);
-        for (int iz = 1; iz <= 3; ++iz) for (int iy = 3; iy >= 1; --iy) put(-1.0, v[iy], v[iz]);
-        for (int iz = 1; iz <= 3; ++iz) for (int iy = 1; iy <= 3; ++iy) put(1.0, v[iy], v[iz]);
-    }
-};
 const HostQuad &hq() {
     static HostQuad q;
     return q;
@@ -88,37 +47,10 @@ int upload_quadrature(scd_ctx *c) {
 }
 
 // -------------------------------------------------------- geometry helpers
-struct V3 { double x, y, z; };
-SCD_HD V3 vsub(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
-SCD_HD double vdot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-SCD_HD V3 vcross(V3 a, V3 b) { return V3{a.y * b.z - a.z * b.y, -a.x * b.z + a.z * b.x, a.x * b.y - a.y * b.x}; }
-SCD_HD double vdist(V3 r, V3 p) {
-    const double a = r.x - p.x, b = r.y - p.y, c = r.z - p.z;
-    return sqrt(a * a + b * b + c * c);
-}
-SCD_HD double tet_vol(const V3 *t) {
-    const V3 cr = vcross(vsub(t[1], t[0]), vsub(t[2], t[0]));
-    const double dt = vdot(vsub(t[3], t[0]), cr);
-    return sqrt(dt * dt) / 6.0;
-}
 // faces opposite vertex 1..4 (src/common.f90:296-322)
 __constant__ int cFACE[4][3] = {{1, 2, 3}, {0, 3, 2}, {0, 1, 3}, {0, 2, 1}};
 __device__ __forceinline__ void face_of(const V3 *t, int f, V3 *tri) {
     tri[0] = t[cFACE[f][0]]; tri[1] = t[cFACE[f][1]]; tri[2] = t[cFACE[f][2]];
-}
-SCD_HD V3 tri_normal(const V3 *tri) {
-    const V3 c = vcross(vsub(tri[1], tri[0]), vsub(tri[2], tri[0]));
-    const double l = sqrt(c.x * c.x + c.y * c.y + c.z * c.z);
-    return V3{c.x / l, c.y / l, c.z / l};
-}
-// linmap_tri weight factor: twice the triangle area (src/common.f90:1381-1408)
-SCD_HD double tri_ww1(const V3 *tri, V3 &a, V3 &b) {
-    a = vsub(tri[1], tri[0]);
-    b = vsub(tri[2], tri[0]);
-    const double aa = a.x * a.x + a.y * a.y + a.z * a.z;
-    const double ww0 = aa * b.x, ww1 = aa * b.y, ww2 = aa * b.z;
-    const double ab = a.x * b.x + a.y * b.y + a.z * b.z;
-    return sqrt((ww0 * b.x + ww1 * b.y + ww2 * b.z) - ab * ab);
 }
 __device__ __forceinline__ cd green(V3 rf, V3 rp, double k) {
     const double R = vdist(rf, rp);
@@ -395,12 +327,9 @@ __device__ __forceinline__ void store_block(const NearArgs &a, const NearTile &t
 
 constexpr int NEAR_THREADS = 128;
 
-__global__ void __launch_bounds__(NEAR_THREADS) k_near_build(NearArgs a) {
-    extern __shared__ cd shm[];
-    const NearTile tl = a.tiles[blockIdx.x];
-    cd *G = shm;                                    // 27 x 27: G[i*27 + j] = Gr(node_c1(i), node_c2(j))
-    cd *GP1 = G + 27 * 27;                          // per tet of c1: G^T P (4 x 27)
-    cd *GP2 = GP1 + (size_t)tl.n1 * 108;            // per tet of c2: G P (4 x 27)
+// box-node Green matrix of a tile's two boxes and G (resp. G^T) times the
+// projectors of every basis function of the tile, in shared memory
+__device__ void tile_green(const NearArgs &a, const NearTile &tl, cd *G, cd *GP1, cd *GP2) {
     for (int e = threadIdx.x; e < 27 * 27; e += blockDim.x) {
         const int i = e / 27, j = e % 27;
         cd v = cmk(0, 0);
@@ -430,6 +359,17 @@ __global__ void __launch_bounds__(NEAR_THREADS) k_near_build(NearArgs a) {
         }
     }
     __syncthreads();
+}
+
+__global__ void __launch_bounds__(NEAR_THREADS) k_near_build(NearArgs a) {
+    extern __shared__ cd shm[];
+    const NearTile tl = a.tiles[blockIdx.x];
+    cd *G = shm;                                    // 27 x 27: G[i*27 + j] = Gr(node_c1(i), node_c2(j))
+    cd *GP1 = G + 27 * 27;                          // per tet of c1: G^T P (4 x 27)
+    cd *GP2 = GP1 + (size_t)tl.n1 * 108;            // per tet of c2: G P (4 x 27)
+    tile_green(a, tl, G, GP1, GP2);
+    const long long TT = 27LL * a.T;
+    const int s1 = tl.s1, s2 = tl.s2;
     const bool diag = tl.g1 == tl.g2;
     const int npairs = tl.n1 * tl.n2;
     for (int e = threadIdx.x; e < npairs; e += blockDim.x) {
@@ -447,6 +387,138 @@ __global__ void __launch_bounds__(NEAR_THREADS) k_near_build(NearArgs a) {
                    a.T, gp, gp + 27, gp + 54, gp + 81, blk);
         store_block(a, tl, i, j, blk, !fwd);
         if (diag && i != j) store_block(a, tl, j, i, blk, true);
+    }
+}
+
+// ------------------------------------------------------- linear basis
+// quadrature accessor for the shared set-up arithmetic (lin_setup.cuh)
+struct DevQ {
+    SCD_HD static double t5(int i, int c) {
+#ifdef __CUDA_ARCH__
+        return cQT5[i][c];
+#else
+        return hq().t5[i][c];
+#endif
+    }
+    SCD_HD static double r5(int i, int c) {
+#ifdef __CUDA_ARCH__
+        return cQR5[i][c];
+#else
+        return hq().r5[i][c];
+#endif
+    }
+};
+
+__device__ __forceinline__ void store_elem(const NearArgs &a, const NearTile &tl, int i, int j, int el, cd v) {
+    const long long e = tl.data_off + tile_at(tl.n1, i, j, el);
+    if (a.c64) ((cf *)a.data)[e] = make_float2((float)v.x, (float)v.y);
+    else ((cd *)a.data)[e] = v;
+}
+
+constexpr int LIN_WARPS = 4;
+constexpr int LIN_WARP_CD = LIN_POINTS * LIN_SCR + LIN_SMALL + 432;   // scratch, small sums, test projectors
+
+// compute_near_zone_interactions_lin (src/precorrection.f90:268-371) on a
+// tile of pseudo-tets (4 consecutive slots per tet, whole tets per group):
+// one warp per tet pair computes the 12x12 block and writes its 16 3x3
+// pseudo-tet blocks, mirrored between different tets, one-sided inside a tet.
+__global__ void __launch_bounds__(32 * LIN_WARPS) k_near_build_lin(NearArgs a) {
+    extern __shared__ cd shm[];
+    const NearTile tl = a.tiles[blockIdx.x];
+    cd *G = shm;
+    cd *GP1 = G + 27 * 27;
+    cd *GP2 = GP1 + (size_t)tl.n1 * 108;
+    tile_green(a, tl, G, GP1, GP2);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    cd *scr = GP2 + (size_t)tl.n2 * 108 + (size_t)warp * LIN_WARP_CD;
+    cd *sm = scr + LIN_POINTS * LIN_SCR;
+    cd *st = sm + LIN_SMALL;
+    const bool diag = tl.g1 == tl.g2;
+    const int nt1 = tl.n1 / 4, nt2 = tl.n2 / 4;
+    for (int e = warp; e < nt1 * nt2; e += LIN_WARPS) {
+        const int p = e / nt2, q = e % nt2;
+        if (diag && q < p) continue;
+        const int sa = tl.s1 + 4 * p, sb = tl.s2 + 4 * q;
+        const bool fwd = a.perm[sa] <= a.perm[sb];      // test = lower original tet
+        const int s_t = fwd ? sa : sb, s_b = fwd ? sb : sa;
+        const cd *gp = diag ? GP2 + (size_t)4 * (fwd ? q : p) * 108 : fwd ? GP2 + (size_t)4 * q * 108 : GP1 + (size_t)4 * p * 108;
+        LinPair pr;
+        lin_pair_init(pr, a.tc + 12LL * s_t, a.tc + 12LL * s_b, a.vol[s_t], a.vol[s_b], a.k, a.eps[s_t], s_t == s_b);
+        for (int i = lane; i < 432; i += 32) {
+            const int an = i / 108, g = (i / 27) % 4, u = i % 27;
+            st[i] = a.P[(size_t)(g * 27 + u) * a.T + s_t + an];
+        }
+        for (int it = lane; it < LIN_ITEMS; it += 32) lin_point<DevQ>(pr, it, scr);
+        __syncwarp();
+        for (int i = lane; i < LIN_SMALL; i += 32) lin_small<DevQ>(pr, i, scr, sm);
+        __syncwarp();
+        // local (row-group) indices of the test and basis tets
+        const int lt = fwd ? p : q, lb = fwd ? q : p;
+        for (int i = lane; i < 144; i += 32) {
+            const cd v = lin_entry<DevQ>(pr, i, scr, sm, st, gp);
+            const int row = i % 12, col = i / 12;
+            const int r = row / 4, an = row % 4, c = col / 4, bn = col % 4;
+            if (diag) {
+                store_elem(a, tl, 4 * lt + an, 4 * lb + bn, r + 3 * c, v);
+                if (lt != lb) store_elem(a, tl, 4 * lb + bn, 4 * lt + an, c + 3 * r, v);
+            } else if (fwd) {
+                store_elem(a, tl, 4 * p + an, 4 * q + bn, r + 3 * c, v);
+            } else {
+                store_elem(a, tl, 4 * p + bn, 4 * q + an, c + 3 * r, v);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// pfft_projection_lin (src/projection.f90:170-338) for one tet per warp: the
+// node integrals against the 98 samples, then S = WW Q / sqrt(vol) and
+// Sd = (WW Q2_d - WW (QdN dN_d)) / sqrt(vol) for its four pseudo-tet slots
+__global__ void __launch_bounds__(32) k_projectors_lin(const double *tc, const double *vol, const int *cube_of_slot,
+                                                       const int *slot0, int ntet, int T, const cd *WW, int ncx, int ncy,
+                                                       double delta, double mx, double my, double mz, double box_delta,
+                                                       double k, cd *P) {
+    __shared__ cd Qs[17][98];   // Q[n] (4), Q2[d][n] (12), QdN
+    const int q = blockIdx.x, lane = threadIdx.x;
+    if (q >= ntet) return;
+    const int s0 = slot0[q];
+    const double *p = tc + 12LL * s0;
+    V3 v[4];
+    for (int i = 0; i < 4; ++i) v[i] = V3{p[3 * i], p[3 * i + 1], p[3 * i + 2]};
+    const double vb = vol[s0];
+    const int cube = cube_of_slot[s0];
+    const int bx = cube % ncx, by = (cube / ncx) % ncy, bz = cube / (ncx * ncy);
+    const V3 cpc = V3{mx + delta * (double)(2 * bx) + box_delta / 2.0, my + delta * (double)(2 * by) + box_delta / 2.0,
+                      mz + delta * (double)(2 * bz) + box_delta / 2.0};
+    const double sc = 2.0 * box_delta;
+    for (int m = lane; m < 98; m += 32) {
+        const V3 r = V3{sc * cPs[m][0] + cpc.x, sc * cPs[m][1] + cpc.y, sc * cPs[m][2] + cpc.z};
+        cd qq[4], q2[3][4];
+        lin_proj_sample<DevQ>(v, vb, r, k, qq, q2);
+        for (int n = 0; n < 4; ++n) {
+            Qs[n][m] = qq[n];
+            for (int d = 0; d < 3; ++d) Qs[4 + 4 * d + n][m] = q2[d][n];
+        }
+        Qs[16][m] = cadd(cadd(cadd(qq[0], qq[1]), qq[2]), qq[3]);
+    }
+    __syncwarp();
+    if (lane < 27) {
+        V3 dN[4];
+        gradshape_hd(v, dN);
+        cd acc[17];
+        for (int j = 0; j < 17; ++j) acc[j] = cmk(0, 0);
+        for (int m = 0; m < 98; ++m) {
+            const cd w = WW[lane * 98 + m];
+            for (int j = 0; j < 17; ++j) cfma(acc[j], w, Qs[j][m]);
+        }
+        const double sv = sqrt(vb);
+        for (int n = 0; n < 4; ++n) {
+            P[(size_t)lane * T + s0 + n] = cmk(acc[n].x / sv, acc[n].y / sv);
+            for (int d = 0; d < 3; ++d) {
+                const cd x = csub(acc[4 + 4 * d + n], cscale(acc[16], comp(dN[n], d)));
+                P[(size_t)((1 + d) * 27 + lane) * T + s0 + n] = cmk(x.x / sv, x.y / sv);
+            }
+        }
     }
 }
 
@@ -788,12 +860,27 @@ int setup_projectors_device(scd_ctx *c) {
     int *dcube = nullptr;
     cudaMalloc(&dcube, sizeof(int) * c->T);
     cudaMemcpy(dcube, c->cube_of_slot.data(), sizeof(int) * c->T, cudaMemcpyHostToDevice);
-    k_projectors<<<(c->T + 3) / 4, 128, 0, c->st>>>(c->d_tc, c->d_tvol, dcube, c->T, dWW, c->ncx, c->ncy, c->d.delta,
-                                                    c->d.min_coord[0], c->d.min_coord[1], c->d.min_coord[2], bd, c->k,
-                                                    c->d_P);
-    rc = check_cuda(c, cudaStreamSynchronize(c->st), "projectors");
+    int *dslot0 = nullptr;
+    if (c->nb == 4) {
+        // linear basis: one warp per tet over its four consecutive pseudo-tet slots
+        const int ntet = c->T / 4;
+        std::vector<int> slot0(ntet);
+        for (int q = 0; q < ntet; ++q) slot0[q] = c->slot_of[4 * q];
+        cudaMalloc(&dslot0, sizeof(int) * ntet);
+        cudaMemcpy(dslot0, slot0.data(), sizeof(int) * ntet, cudaMemcpyHostToDevice);
+        k_projectors_lin<<<ntet, 32, 0, c->st>>>(c->d_tc, c->d_tvol, dcube, dslot0, ntet, c->T, dWW, c->ncx, c->ncy,
+                                                  c->d.delta, c->d.min_coord[0], c->d.min_coord[1], c->d.min_coord[2],
+                                                  bd, c->k, c->d_P);
+    } else {
+        k_projectors<<<(c->T + 3) / 4, 128, 0, c->st>>>(c->d_tc, c->d_tvol, dcube, c->T, dWW, c->ncx, c->ncy, c->d.delta,
+                                                        c->d.min_coord[0], c->d.min_coord[1], c->d.min_coord[2], bd, c->k,
+                                                        c->d_P);
+    }
+    rc = check_cuda(c, cudaGetLastError(), "projectors launch");
+    if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->st), "projectors");
     cudaFree(dWW);
     cudaFree(dcube);
+    cudaFree(dslot0);
     if (!rc) c->have_proj = true;
     c->f_ready = false;
     return rc;
@@ -829,9 +916,16 @@ int setup_nearzone_device(scd_ctx *c, int prec) {
     a.cube_off = c->d_cube_off; a.T = c->T; a.ncx = c->ncx; a.ncy = c->ncy; a.Nx = c->Nx; a.Ny = c->Ny;
     a.delta = c->d.delta; a.mx = c->d.min_coord[0]; a.my = c->d.min_coord[1]; a.mz = c->d.min_coord[2];
     a.k = c->k; a.data = c->d_tdata; a.c64 = prec == SCD_STORE_C64;
-    const size_t sh = sizeof(cd) * (27 * 27 + (size_t)2 * c->max_per_group * 108);
-    if (sh > 48 * 1024) cudaFuncSetAttribute(k_near_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-    k_near_build<<<c->ntiles, NEAR_THREADS, sh, c->st>>>(a);
+    if (c->nb == 4) {
+        // linear basis: 12x12 blocks per tet pair, written as pseudo-tet blocks
+        const size_t sh = sizeof(cd) * (27 * 27 + (size_t)2 * c->max_per_group * 108 + (size_t)LIN_WARPS * LIN_WARP_CD);
+        cudaFuncSetAttribute(k_near_build_lin, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+        k_near_build_lin<<<c->ntiles, 32 * LIN_WARPS, sh, c->st>>>(a);
+    } else {
+        const size_t sh = sizeof(cd) * (27 * 27 + (size_t)2 * c->max_per_group * 108);
+        if (sh > 48 * 1024) cudaFuncSetAttribute(k_near_build, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+        k_near_build<<<c->ntiles, NEAR_THREADS, sh, c->st>>>(a);
+    }
     rc = check_cuda(c, cudaGetLastError(), "near-zone launch");
     if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->st), "near-zone build");
     if (!rc) { c->have_near = true; c->nrhs_cap = 0; c->f_cap = 0; }
@@ -845,6 +939,45 @@ int setup_vswf(scd_ctx *c, int Nmax, cd *d_mat) {
     if (Nmax < 1 || Nmax > VSWF_NMAX - 2) return set_error(c, SCD_BAD_ARG, "Nmax %d outside 1..%d", Nmax, VSWF_NMAX - 2);
     k_vswf<<<(c->T + 127) / 128, 128, 0, c->st>>>(c->d_tc, c->d_tvol, c->T, c->k, Nmax, d_mat, c->n);
     return check_cuda(c, cudaGetLastError(), "vswf");
+}
+
+// 12x12 blocks V(4c + n, 4c' + n') of the linear basis, ordered by (tet_T,
+// tet_B), from the pseudo-tet tiles: pseudo-block (n, n') of the tet pair is
+// stored at (row slot, column slot) of its tile, or transposed at the mirrored
+// position when the test tet's group is the tile's column group
+static int export_linear_blocks(scd_ctx *c, int64_t B, const std::vector<cd> &data, scd_c128 *sp, int32_t *ind) {
+    struct E { int t, b; const NearTile *tl; int pt, pb; bool swap; };
+    std::vector<E> list;
+    list.reserve((size_t)B);
+    for (const NearTile &tl : c->tiles_h) {
+        const int nt1 = tl.n1 / 4, nt2 = tl.n2 / 4;
+        for (int p = 0; p < nt1; ++p)
+            for (int q = 0; q < nt2; ++q) {
+                if (tl.g1 == tl.g2 && q < p) continue;
+                const int ta = c->perm[tl.s1 + 4 * p] / 4, tb = c->perm[tl.s2 + 4 * q] / 4;
+                if (ta <= tb) list.push_back(E{ta, tb, &tl, p, q, false});
+                else list.push_back(E{tb, ta, &tl, p, q, true});
+            }
+    }
+    if ((int64_t)list.size() != B) return set_error(c, SCD_BAD_ARG, "B = %lld, the near zone has %zu tet pairs", (long long)B, list.size());
+    std::sort(list.begin(), list.end(), [](const E &x, const E &y) { return x.t != y.t ? x.t < y.t : x.b < y.b; });
+    for (size_t k = 0; k < list.size(); ++k) {
+        const E &e = list[k];
+        const NearTile &tl = *e.tl;
+        for (int col = 0; col < 12; ++col)
+            for (int row = 0; row < 12; ++row) {
+                const int r = row / 4, an = row % 4, cc = col / 4, bn = col % 4;
+                // test node an of tet t, basis node bn of tet b
+                size_t pos;
+                if (!e.swap) pos = (size_t)tl.data_off + (size_t)tile_at(tl.n1, 4 * e.pt + an, 4 * e.pb + bn, r + 3 * cc);
+                else pos = (size_t)tl.data_off + (size_t)tile_at(tl.n1, 4 * e.pt + bn, 4 * e.pb + an, cc + 3 * r);
+                const cd v = data[pos];
+                sp[144 * k + row + 12 * col] = scd_c128{v.x, v.y};
+            }
+        ind[2 * k] = e.t + 1;
+        ind[2 * k + 1] = e.b + 1;
+    }
+    return SCD_OK;
 }
 
 extern "C" {
@@ -886,16 +1019,18 @@ int scd_grid_from_mesh(int32_t Nv, const double *coord, int32_t T, const int32_t
 
 int scd_set_mesh(scd_ctx *c, int32_t Nv, const double *coord, const int32_t *etopol, const scd_c128 *param) {
     if (!c) return SCD_BAD_ARG;
-    if (c->nb != 1) return set_error(c, SCD_BAD_ARG, "scd_set_mesh: constant basis only");
     cudaSetDevice(c->dev);
     if (!coord || !etopol || !param || Nv < 4) return set_error(c, SCD_BAD_ARG, "bad mesh arrays");
+    // with the linear basis every tet holds nb = 4 basis functions (pseudo-tets
+    // 4t..4t+3, consecutive slots of the tet's box) that share its geometry
+    const int ntet = c->T / c->nb;
     c->Nv = Nv;
     c->coord.assign(coord, coord + 3LL * Nv);
-    c->etopol.assign(etopol, etopol + 4LL * c->T);
-    c->param.resize(c->T);
-    for (int t = 0; t < c->T; ++t) c->param[t] = cmk(param[t].re, param[t].im);
+    c->etopol.assign(etopol, etopol + 4LL * ntet);
+    c->param.resize(ntet);
+    for (int t = 0; t < ntet; ++t) c->param[t] = cmk(param[t].re, param[t].im);
     std::vector<int> cube(c->T);
-    for (int t = 0; t < c->T; ++t) {
+    for (int t = 0; t < ntet; ++t) {
         for (int v = 0; v < 4; ++v) {
             const int id = etopol[4LL * t + v];
             if (id < 1 || id > Nv) return set_error(c, SCD_BAD_ARG, "etopol(%d,%d) = %d outside 1..%d", v + 1, t + 1, id, Nv);
@@ -903,15 +1038,16 @@ int scd_set_mesh(scd_ctx *c, int32_t Nv, const double *coord, const int32_t *eto
         double tv[12], cp[3];
         tet_vertices(c, t, tv);
         for (int d = 0; d < 3; ++d) cp[d] = (tv[d] + tv[3 + d] + tv[6 + d] + tv[9 + d]) / 4;
-        cube[t] = host_point_cube(c, cp);
-        if (cube[t] < 0) return set_error(c, SCD_BAD_ARG, "tet %d lies outside the projection boxes", t + 1);
+        const int cb = host_point_cube(c, cp);
+        if (cb < 0) return set_error(c, SCD_BAD_ARG, "tet %d lies outside the projection boxes", t + 1);
+        for (int i = 0; i < c->nb; ++i) cube[c->nb * t + i] = cb;
     }
     int rc = set_order_from_cubes(c, cube);
     if (rc) return rc;
     std::vector<double> tc(12LL * c->T), vol(c->T);
     std::vector<cd> eps(c->T);
     for (int s = 0; s < c->T; ++s) {
-        const int t = c->perm[s];
+        const int t = c->perm[s] / c->nb;
         tet_vertices(c, t, &tc[12LL * s]);
         const double *p = &tc[12LL * s];
         const V3 tv[4] = {V3{p[0], p[1], p[2]}, V3{p[3], p[4], p[5]}, V3{p[6], p[7], p[8]}, V3{p[9], p[10], p[11]}};
@@ -933,14 +1069,12 @@ int scd_set_mesh(scd_ctx *c, int32_t Nv, const double *coord, const int32_t *eto
 
 int scd_build_projectors(scd_ctx *c) {
     if (!c) return SCD_BAD_ARG;
-    if (c->nb != 1) return set_error(c, SCD_BAD_ARG, "scd_build_projectors: constant basis only");
     cudaSetDevice(c->dev);
     return setup_projectors_device(c);
 }
 
 int scd_build_nearzone(scd_ctx *c, int32_t prec) {
     if (!c) return SCD_BAD_ARG;
-    if (c->nb != 1) return set_error(c, SCD_BAD_ARG, "scd_build_nearzone: constant basis only");
     cudaSetDevice(c->dev);
     return setup_nearzone_device(c, prec);
 }
@@ -975,10 +1109,12 @@ int scd_get_projectors(scd_ctx *c, scd_c128 *S, scd_c128 *Sx, scd_c128 *Sy, scd_
 
 int64_t scd_nearzone_count(scd_ctx *c) {
     if (!c || !c->have_near) return -1;
+    // blocks between basis functions (nb = 1) or between tets (nb = 4: 12x12)
     long long B = 0;
     for (const NearTile &tl : c->tiles_h) {
-        if (tl.g1 == tl.g2) B += (long long)tl.n1 * (tl.n1 + 1) / 2;
-        else B += (long long)tl.n1 * tl.n2;
+        const long long n1 = tl.n1 / c->nb, n2 = tl.n2 / c->nb;
+        if (tl.g1 == tl.g2) B += n1 * (n1 + 1) / 2;
+        else B += n1 * n2;
     }
     return B;
 }
@@ -986,7 +1122,6 @@ int64_t scd_nearzone_count(scd_ctx *c) {
 // export in the reference layout, ordered by (tet_T, tet_B), widened to FP64
 int scd_get_nearzone(scd_ctx *c, int64_t B, scd_c128 *sp, int32_t *ind) {
     if (!c || !sp || !ind) return SCD_BAD_ARG;
-    if (c->nb != 1) return set_error(c, SCD_BAD_ARG, "scd_get_nearzone: constant basis only");
     cudaSetDevice(c->dev);
     if (!c->have_near) return set_error(c, SCD_NOT_READY, "near zone not set");
     if (B != scd_nearzone_count(c)) return set_error(c, SCD_BAD_ARG, "B = %lld, the near zone has %lld", (long long)B,
@@ -1002,6 +1137,7 @@ int scd_get_nearzone(scd_ctx *c, int64_t B, scd_c128 *sp, int32_t *ind) {
         int rc = check_cuda(c, cudaMemcpy(data.data(), c->d_tdata, sizeof(cd) * nb, cudaMemcpyDeviceToHost), "get_nearzone");
         if (rc) return rc;
     }
+    if (c->nb == 4) return export_linear_blocks(c, B, data, sp, ind);
     struct E { int t, b; size_t e; int ld; bool tr; };
     std::vector<E> list;
     list.reserve((size_t)B);

@@ -1,0 +1,86 @@
+"""Linear-basis (mesh%order = 1) operator construction on the device --
+pfft_projection_lin (src/projection.f90:170-338) and
+compute_near_zone_interactions_lin (src/precorrection.f90:268-725) -- against
+the CPU oracle, and the order-1 matvec on the device-built operator.  An
+816-tet sphere at ka = 1.  Collected only with SCADYN_TEST_LINEAR=1 until the
+linear basis has run on a GPU."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from scadyn_b200 import api
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(os.environ.get("SCADYN_TEST_LINEAR") != "1",
+                                 reason="linear basis not yet run on a GPU; set SCADYN_TEST_LINEAR=1")]
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.fixture(scope="module")
+def mesh():
+    from scadyn_b200 import meshgen
+    return meshgen.sphere(3, seed=1, eps=2.25 + 0.01j)
+
+
+@pytest.fixture(scope="module")
+def oracle_lin(mesh):
+    k = 1.0 / mesh.a
+    return O.setup_lin(mesh, k, grid_size=1.8, fp64_near=True)
+
+
+def _device(mesh, k, storage):
+    d = api.grid_from_mesh(mesh.coord, mesh.etopol, grid_size=1.8)
+    d.order = 1
+    s = api.Solver.from_desc(d)
+    s.set_wavenumber(k)
+    s.set_mesh(mesh.coord, mesh.etopol, mesh.param)
+    s.build_G()
+    proj = s.pfft_projection_lin()
+    s.compute_near_zone_interactions_lin(storage)
+    return s, proj
+
+
+@pytest.fixture(scope="module")
+def dev128(mesh, oracle_lin):
+    s, proj = _device(mesh, oracle_lin.geom.k, api.STORE_C128)
+    yield s, proj
+    s.close()
+
+
+def test_projectors_lin_match_oracle(dev128, oracle_lin):
+    _, (S, Sx, Sy, Sz, indS) = dev128
+    assert S.shape == oracle_lin.S.shape
+    for got, want in zip((S, Sx, Sy, Sz), (oracle_lin.S, oracle_lin.Sx, oracle_lin.Sy, oracle_lin.Sz)):
+        assert rel(got, want) < 1e-8
+    assert (indS == oracle_lin.indS).all()
+
+
+def test_nearzone_lin_c128_matches_oracle(dev128, oracle_lin):
+    s, _ = dev128
+    sp, ind = s.get_nearzone()
+    assert sp.shape == oracle_lin.sp_mat.shape
+    order = np.lexsort((oracle_lin.sp_ind[:, 1], oracle_lin.sp_ind[:, 0]))
+    assert (ind == oracle_lin.sp_ind[order]).all()
+    assert rel(sp, oracle_lin.sp_mat[order]) < 1e-9
+
+
+def test_nearzone_lin_c64_matches_oracle(mesh, oracle_lin):
+    s, _ = _device(mesh, oracle_lin.geom.k, api.STORE_C64)
+    try:
+        sp, ind = s.get_nearzone()
+        order = np.lexsort((oracle_lin.sp_ind[:, 1], oracle_lin.sp_ind[:, 0]))
+        assert rel(sp, oracle_lin.sp_mat[order].astype(np.complex64).astype(np.complex128)) < 1e-6
+    finally:
+        s.close()
+
+
+def test_matvec_on_device_built_operator(dev128, oracle_lin):
+    s, _ = dev128
+    rng = np.random.default_rng(21)
+    x = rng.standard_normal(s.n) + 1j * rng.standard_normal(s.n)
+    assert rel(s.compute_Ax2(x), oracle_lin.compute_Ax2(x)) < 1e-9
