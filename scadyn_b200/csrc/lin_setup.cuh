@@ -428,3 +428,28 @@ SCD_HD void lin_proj_sample(const V3 *t, double vol, V3 r, double k, cd *q, cd (
         }
     }
 }
+
+// Tile positions of block entry e = row + 12 col (row = 4 r + an, col = 4 c + bn)
+// of the pair (test tet, basis tet), for a tile whose row group holds tet p and
+// column group tet q (local tet indices).  A tile stores row pseudo-tet i x
+// column pseudo-tet j as 3x3 blocks, element (r', c') at r' + 3 c'; an
+// off-diagonal tile is also applied transposed, a diagonal tile holds both
+// halves, and the 16 blocks inside one tet are stored once.  fwd: the test
+// tet is tet p.  Writes (i, j, element) triples to pos and returns their number.
+SCD_HD int lin_tile_positions(bool diag, bool fwd, int p, int q, int e, int *pos) {
+    const int row = e % 12, col = e / 12;
+    const int r = row / 4, an = row % 4, c = col / 4, bn = col % 4;
+    if (diag) {
+        const int lt = fwd ? p : q, lb = fwd ? q : p;
+        pos[0] = 4 * lt + an; pos[1] = 4 * lb + bn; pos[2] = r + 3 * c;
+        if (lt == lb) return 1;
+        pos[3] = 4 * lb + bn; pos[4] = 4 * lt + an; pos[5] = c + 3 * r;
+        return 2;
+    }
+    if (fwd) {
+        pos[0] = 4 * p + an; pos[1] = 4 * q + bn; pos[2] = r + 3 * c;
+    } else {
+        pos[0] = 4 * p + bn; pos[1] = 4 * q + an; pos[2] = c + 3 * r;
+    }
+    return 1;
+}

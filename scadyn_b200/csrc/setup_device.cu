@@ -452,20 +452,11 @@ __global__ void __launch_bounds__(32 * LIN_WARPS) k_near_build_lin(NearArgs a) {
         __syncwarp();
         for (int i = lane; i < LIN_SMALL; i += 32) lin_small<DevQ>(pr, i, scr, sm);
         __syncwarp();
-        // local (row-group) indices of the test and basis tets
-        const int lt = fwd ? p : q, lb = fwd ? q : p;
         for (int i = lane; i < 144; i += 32) {
             const cd v = lin_entry<DevQ>(pr, i, scr, sm, st, gp);
-            const int row = i % 12, col = i / 12;
-            const int r = row / 4, an = row % 4, c = col / 4, bn = col % 4;
-            if (diag) {
-                store_elem(a, tl, 4 * lt + an, 4 * lb + bn, r + 3 * c, v);
-                if (lt != lb) store_elem(a, tl, 4 * lb + bn, 4 * lt + an, c + 3 * r, v);
-            } else if (fwd) {
-                store_elem(a, tl, 4 * p + an, 4 * q + bn, r + 3 * c, v);
-            } else {
-                store_elem(a, tl, 4 * p + bn, 4 * q + an, c + 3 * r, v);
-            }
+            int pos[6];
+            const int np = lin_tile_positions(diag, fwd, p, q, i, pos);
+            for (int w = 0; w < np; ++w) store_elem(a, tl, pos[3 * w], pos[3 * w + 1], pos[3 * w + 2], v);
         }
         __syncwarp();
     }
@@ -966,12 +957,10 @@ static int export_linear_blocks(scd_ctx *c, int64_t B, const std::vector<cd> &da
         const NearTile &tl = *e.tl;
         for (int col = 0; col < 12; ++col)
             for (int row = 0; row < 12; ++row) {
-                const int r = row / 4, an = row % 4, cc = col / 4, bn = col % 4;
-                // test node an of tet t, basis node bn of tet b
-                size_t pos;
-                if (!e.swap) pos = (size_t)tl.data_off + (size_t)tile_at(tl.n1, 4 * e.pt + an, 4 * e.pb + bn, r + 3 * cc);
-                else pos = (size_t)tl.data_off + (size_t)tile_at(tl.n1, 4 * e.pt + bn, 4 * e.pb + an, cc + 3 * r);
-                const cd v = data[pos];
+                // the first position the kernel wrote the entry to
+                int pp[6];
+                lin_tile_positions(tl.g1 == tl.g2, !e.swap, e.pt, e.pb, row + 12 * col, pp);
+                const cd v = data[(size_t)tl.data_off + (size_t)tile_at(tl.n1, pp[0], pp[1], pp[2])];
                 sp[144 * k + row + 12 * col] = scd_c128{v.x, v.y};
             }
         ind[2 * k] = e.t + 1;

@@ -5,6 +5,7 @@ the phase functions of scadyn_b200/csrc/lin_setup.cuh; tests/lin_setup_check.cu
 runs the same functions on the host, item by item, and this test compares them
 with the oracle's compute_near_zone_interactions_lin blocks (self, same-box and
 neighbouring-box pairs) and with pfft_projection_lin's node integrals.
+tests/lin_tile_check.cu checks where the kernel writes the blocks in a tile.
 """
 import os
 import subprocess
@@ -103,3 +104,16 @@ def test_projector_sample_arithmetic(exe, setup):
     got = np.frombuffer(r.stdout, np.complex128).reshape(len(want), 16)
     want = np.array(want)
     assert np.abs(got - want).max() / np.abs(want).max() < 1e-12
+
+
+def test_tile_positions_apply_as_matmul_Acorr(tmp_path):
+    """lin_tile_positions puts every entry where the near-zone kernels' tile
+    application reproduces matmul_Acorr, for diagonal and off-diagonal tiles
+    with the test tet in either group; its first position reads the entry back."""
+    out = tmp_path / "lin_tile_check"
+    nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+    subprocess.check_call([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "-O2",
+                           "-I", CSRC, os.path.join(HERE, "lin_tile_check.cu"), "-o", str(out)])
+    r = subprocess.run([str(out)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "6 of 6 tiles ok" in r.stdout
