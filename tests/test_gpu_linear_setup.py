@@ -84,3 +84,20 @@ def test_matvec_on_device_built_operator(dev128, oracle_lin):
     rng = np.random.default_rng(21)
     x = rng.standard_normal(s.n) + 1j * rng.standard_normal(s.n)
     assert rel(s.compute_Ax2(x), oracle_lin.compute_Ax2(x)) < 1e-9
+
+
+@pytest.mark.parametrize("precision,block", [(api.PREC_FP64, 1), (api.PREC_FP64, 4), (api.PREC_MIXED, 4)])
+def test_solve_columns_on_device_built_operator(dev128, oracle_lin, precision, block):
+    """The batched column solver (FP64 one at a time, FP64 batched, mixed batched) on
+    the device-built linear operator: matH X against the oracle's GMRES solutions."""
+    s, _ = dev128
+    rng = np.random.default_rng(22)
+    ncol = 4
+    mat = rng.standard_normal((ncol, s.n)) + 1j * rng.standard_normal((ncol, s.n))
+    Tc, iters, X, rc = s.solve_columns(mat, tol=1e-8, m=50, cycles=8, block=block, precision=precision,
+                                       inner_tol=1e-4, want_x=True)
+    assert rc == api.SCD_OK
+    Xr = np.array([oracle_lin.gmres(mat[c], tol=1e-8, m=50, cycles=8)[0] for c in range(ncol)])
+    assert rel(X, Xr) < 1e-6
+    Tr = np.conj(mat) @ Xr.T                 # Tr[r, c] = mat_r^H x_c
+    assert rel(Tc.T, Tr) < 1e-6
