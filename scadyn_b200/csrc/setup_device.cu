@@ -848,16 +848,19 @@ int setup_projectors_device(scd_ctx *c) {
         cudaFree(dWW);
         return set_error(c, SCD_OOM, "projectors");
     }
-    int *dcube = nullptr;
-    cudaMalloc(&dcube, sizeof(int) * c->T);
+    int *dcube = nullptr, *dslot0 = nullptr;
+    const int ntet = c->T / c->nb;
+    if (cudaMalloc(&dcube, sizeof(int) * c->T) != cudaSuccess ||
+        (c->nb == 4 && cudaMalloc(&dslot0, sizeof(int) * ntet) != cudaSuccess)) {
+        cudaFree(dWW);
+        cudaFree(dcube);
+        return set_error(c, SCD_OOM, "projector tables");
+    }
     cudaMemcpy(dcube, c->cube_of_slot.data(), sizeof(int) * c->T, cudaMemcpyHostToDevice);
-    int *dslot0 = nullptr;
     if (c->nb == 4) {
         // linear basis: one warp per tet over its four consecutive pseudo-tet slots
-        const int ntet = c->T / 4;
         std::vector<int> slot0(ntet);
         for (int q = 0; q < ntet; ++q) slot0[q] = c->slot_of[4 * q];
-        cudaMalloc(&dslot0, sizeof(int) * ntet);
         cudaMemcpy(dslot0, slot0.data(), sizeof(int) * ntet, cudaMemcpyHostToDevice);
         k_projectors_lin<<<ntet, 32, 0, c->st>>>(c->d_tc, c->d_tvol, dcube, dslot0, ntet, c->T, dWW, c->ncx, c->ncy,
                                                   c->d.delta, c->d.min_coord[0], c->d.min_coord[1], c->d.min_coord[2],
@@ -910,7 +913,9 @@ int setup_nearzone_device(scd_ctx *c, int prec) {
     if (c->nb == 4) {
         // linear basis: 12x12 blocks per tet pair, written as pseudo-tet blocks
         const size_t sh = sizeof(cd) * (27 * 27 + (size_t)2 * c->max_per_group * 108 + (size_t)LIN_WARPS * LIN_WARP_CD);
-        cudaFuncSetAttribute(k_near_build_lin, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+        if ((rc = check_cuda(c, cudaFuncSetAttribute(k_near_build_lin, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh),
+                             "near-zone shared memory")))
+            return rc;
         k_near_build_lin<<<c->ntiles, 32 * LIN_WARPS, sh, c->st>>>(a);
     } else {
         const size_t sh = sizeof(cd) * (27 * 27 + (size_t)2 * c->max_per_group * 108);
