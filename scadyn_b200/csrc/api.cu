@@ -14,6 +14,7 @@
 
 #include "ctx.h"
 #include "linear_basis.h"
+#include "layout_check.h"
 
 // ------------------------------------------------------------------ errors
 int set_error(scd_ctx *c, int code, const char *fmt, ...) {
@@ -228,6 +229,10 @@ static int upload_layout(scd_ctx *c, std::vector<NearTile> &tiles, long long off
     (void)off;
     const int nt = (int)tiles.size();
     const int ng = c->ngroups;
+    const LayoutView lv{c->T, c->nb, c->ncubes, ng, &c->perm, &c->slot_of, &c->cube_of_slot, &c->cube_off,
+                        &c->grp_off, &c->grp_cube, &c->grp_tile, &tiles, &c->pslot_base, &c->pslot_cnt, c->tile_store};
+    const std::string why = check_layout(lv);
+    if (!why.empty()) return set_error(c, SCD_BAD_ARG, "near-zone layout check: %s", why.c_str());
     int rc;
     if ((rc = dalloc(c, &c->d_tiles, nt, "tile table"))) return rc;
     if ((rc = dalloc(c, &c->d_pslot_base, ng + 1, "slot bases"))) return rc;
