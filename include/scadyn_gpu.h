@@ -58,11 +58,13 @@ typedef struct scd_grid_desc {
     double  min_coord[3];    /* grid origin (mesh%min_coord) */
     int32_t T;               /* tetrahedra (mesh%N_tet) */
     int32_t order;           /* basis order (mesh%order): 0 constant (3 unknowns per tet), 1 linear
-                                (12 per tet, x(12(t-1) + 4c + i)); with 1 only the host-built operator
-                                path is open (scd_set_projectors/scd_set_nearzone, scd_matvec,
-                                scd_gmres, scd_solve_columns), as the reference solves no linear-basis
-                                T-matrix (src/T_matrix.f90:250-259 pairs 3T-row right-hand sides with
-                                its 12T unknowns) */
+                                (12 per tet, x(12(t-1) + 4c + i)); with 1 the operator comes from the
+                                host (scd_set_projectors/scd_set_nearzone) or from the mesh
+                                (scd_set_mesh, scd_build_projectors, scd_build_nearzone) for
+                                scd_matvec, scd_gmres and scd_solve_columns; scd_vswf_rhs and the
+                                T-matrix entry points refuse it, as the reference solves no
+                                linear-basis T-matrix (src/T_matrix.f90:250-259 pairs 3T-row
+                                right-hand sides with its 12T unknowns) */
     int32_t M_ex;            /* projection order (mesh%M_ex); 2 only */
     int32_t near_zone;       /* near-cube radius (mesh%near_zone); 1 only */
     int32_t device;          /* CUDA device ordinal */
@@ -130,15 +132,19 @@ SCD_API int scd_grid_from_mesh(int32_t Nv, const double *coord, int32_t T, const
 SCD_API int scd_set_mesh(scd_ctx *ctx, int32_t Nv, const double *coord, const int32_t *etopol,
                  const scd_c128 *param);
 
-/* pfft_projection_const (src/projection.f90:17-166) on the device. */
+/* pfft_projection_const (src/projection.f90:17-166) on the device; with
+ * order 1 pfft_projection_lin (src/projection.f90:170-338), 4T columns. */
 SCD_API int scd_build_projectors(scd_ctx *ctx);
 
 /* compute_near_zone_interactions_const (src/precorrection.f90:131-264) on the
- * device, FP64 arithmetic, stored in storage_prec. */
+ * device, FP64 arithmetic, stored in storage_prec; with order 1
+ * compute_near_zone_interactions_lin (src/precorrection.f90:268-725). */
 SCD_API int scd_build_nearzone(scd_ctx *ctx, int32_t storage_prec);
 
 /* Copy the device operator back in the reference's layouts (for a Fortran
- * host that keeps its own copy, and for checking). */
+ * host that keeps its own copy, and for checking).  The near zone comes
+ * back ordered by (tet_T, tet_B): B = scd_nearzone_count blocks, 3x3
+ * (sp_mat(3,3,B)), or 12x12 (sp_mat(12,12,B)) with order 1. */
 SCD_API int scd_get_projectors(scd_ctx *ctx, scd_c128 *S, scd_c128 *Sx, scd_c128 *Sy, scd_c128 *Sz,
                        int32_t *indS);
 SCD_API int64_t scd_nearzone_count(scd_ctx *ctx);
