@@ -36,9 +36,8 @@ int main() {
     }
     printf("production layout: ok (%d groups; the upload then stopped: %s)\n", c->ngroups, c->err.c_str());
 
-    // a valid two-group layout by hand: groups 0 and 1 in boxes 0 and 1 of the
-    // production binning's first two non-empty boxes are not needed -- the
-    // checker sees only the tables, so a small self-contained layout serves
+    // a valid two-group layout by hand (check_layout sees only the tables):
+    // group 0 = 2 tets in box 0, group 1 = 3 tets in box 1, tiles (0,0), (0,1), (1,1)
     const int nb = c->nb, n0 = 2 * nb, n1 = 3 * nb, T = n0 + n1;
     std::vector<int> perm(T), slot_of(T), cos(T), co{0, n0, T}, go{0, n0, T}, gc{0, 1}, gt{0, 2, 3}, pc{2, 1};
     for (int s = 0; s < T; ++s) { perm[s] = s; slot_of[s] = s; cos[s] = s < n0 ? 0 : 1; }
