@@ -86,6 +86,10 @@ int ensure_work(scd_ctx *c, int nrhs) {
 
 // error word of the near-zone kernel: a bounded wait that ran out
 int near_status(scd_ctx *c) {
+    if (c->near_cfg_err) {
+        c->near_cfg_err = 0;
+        return set_error(c, SCD_BAD_ARG, "near-zone kernel not launched: a tile with its x segment exceeds the shared-memory ring");
+    }
     if (!c->d_kerr) return SCD_OK;
     int h = 0;
     CK(cudaMemcpy(&h, c->d_kerr, sizeof(int), cudaMemcpyDeviceToHost), "near-zone status");

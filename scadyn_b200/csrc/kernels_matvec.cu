@@ -860,6 +860,12 @@ void near_launch(scd_ctx *c, const ST *data, const C *x, int nrhs, const int *do
     const size_t max_tile = (size_t)c->max_tile_store * sizeof(ST) + a.x1_bytes;
     size_t ring = ((U == 1 ? NZ_SMEM_4CTA : NZ_SMEM_2CTA) - NZ_META - a.x1_bytes) / 16 * 16;
     if (ring < max_tile) ring = std::min((NZ_SMEM_MAX - NZ_META - a.x1_bytes) / 16 * 16, (max_tile + 15) / 16 * 16 * 2);
+    if (ring < max_tile) {
+        // cannot happen with groups of at most SCD_GROUP_MAX slots; reported
+        // by near_status instead of overrunning the ring
+        c->near_cfg_err = 1;
+        return;
+    }
     a.ring_bytes = (uint32_t)ring;
     {
         const int npass = (nrhs + nq * U - 1) / (nq * U);
