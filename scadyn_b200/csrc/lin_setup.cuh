@@ -26,6 +26,7 @@
 #pragma once
 #include "geom.cuh"
 
+// Gr (src/common.f90:271-279): exp(ikR) / (4 pi R)
 SCD_HD cd green_hd(V3 rf, V3 rp, double k) {
     const double R = vdist(rf, rp);
     const double d = 4.0 * PI * R;

@@ -52,13 +52,8 @@ __constant__ int cFACE[4][3] = {{1, 2, 3}, {0, 3, 2}, {0, 1, 3}, {0, 2, 1}};
 __device__ __forceinline__ void face_of(const V3 *t, int f, V3 *tri) {
     tri[0] = t[cFACE[f][0]]; tri[1] = t[cFACE[f][1]]; tri[2] = t[cFACE[f][2]];
 }
-__device__ __forceinline__ cd green(V3 rf, V3 rp, double k) {
-    const double R = vdist(rf, rp);
-    const double d = 4.0 * PI * R;
-    double s, c;
-    sincos(k * R, &s, &c);
-    return cmk(c / d, s / d);
-}
+// Gr (src/common.f90:271-279): exp(ikR) / (4 pi R)
+__device__ __forceinline__ cd green(V3 rf, V3 rp, double k) { return green_hd(rf, rp, k); }
 
 // analytical_integration, src/singularity_subtraction.f90:15-108: the
 // integrals of 1/R and R over a triangle (Np = 2)
