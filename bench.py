@@ -84,11 +84,13 @@ def make_mesh(cfg):
     return mesh
 
 
-def build_solver(cfg, mesh, device):
+def build_solver(cfg, mesh, device, order=0):
+    """The operator from the mesh on the device; order 1 = linear basis (4 basis functions per tet)."""
     from scadyn_b200 import api, geometry
     gs = geometry.cell_size_for_grid(mesh.coord, mesh.etopol, cfg["N"])
     d = api.grid_from_mesh(mesh.coord, mesh.etopol, grid_size=gs)
     d.device = device
+    d.order = order
     s = api.Solver.from_desc(d, device=device)
     k = cfg["ka"] / mesh.a
     t0 = time.time()
@@ -249,9 +251,11 @@ def main():
     ap.add_argument("--sweep", type=int, default=0,
                     help="run a C3-shaped wavelength sweep with this many wavelengths instead")
     ap.add_argument("--sweep-nmax", type=int, default=14, help="largest Nmax of the sweep (C3: 14)")
-    ap.add_argument("--profile", default=None, choices=["near1", "near16", "mixed16", "solve16", "near-compare"],
+    ap.add_argument("--profile", default=None,
+                    choices=["near1", "near16", "mixed16", "solve16", "near-compare", "linear"],
                     help="only build the operator and run profile_matvec (for ncu captures); near-compare times "
-                         "the complex64 x16 matvec with the CUDA-core near zone and both tensor-core schedules")
+                         "the complex64 x16 matvec with the CUDA-core near zone and both tensor-core schedules; "
+                         "linear times the linear-basis set-up and matvec against the constant basis")
     ap.add_argument("--near-mma", nargs="?", const="1", default=None, choices=["1", "2"],
                     help="tensor-core near zone for the complex64 matvec (SCADYN_NEAR_MMA=1; 2: merged schedule)")
     ap.add_argument("--cgs", action="store_true",
@@ -309,6 +313,24 @@ def main():
                           "columns": 16, "columns_per_s": round(16 / (ms / 1e3), 4),
                           "iters_mean": float(np.mean(it))}), flush=True)
         solver.close()
+        return
+    if args.profile == "linear":
+        # linear basis (mesh%order = 1) on the same mesh and grid: set-up from
+        # the mesh, then median FP64 and complex64 matvec times, beside the
+        # constant basis already built
+        out = {"config": args.config, "tets": mesh.n_tet, "setup_s": {"constant": round(setup_s, 2)}, "ms": {}}
+        runs = [solver.profile_matvec(10, 1, api.PREC_FP64) for _ in range(5)]
+        out["ms"]["constant_fp64_1rhs"] = round(float(np.median([r["matvec_ms"] for r in runs])), 4)
+        solver.close()
+        sv, _, _, _, lin_setup_s = build_solver(cfg, mesh, local, order=1)
+        out["setup_s"]["linear"] = round(lin_setup_s, 2)
+        out["near_blocks_12x12"] = sv.nearzone_count()
+        for label, nrhs, prec in (("linear_fp64_1rhs", 1, api.PREC_FP64), ("linear_c64_16rhs", 16, api.PREC_MIXED)):
+            runs = [sv.profile_matvec(10, nrhs, prec) for _ in range(5)]
+            out["ms"][label] = {key: round(float(np.median([r[key] for r in runs])), 4)
+                                for key in ("nearzone_ms", "fft_ms", "gather_ms", "matvec_ms")}
+        sv.close()
+        print(json.dumps(out), flush=True)
         return
     if args.profile == "near-compare":
         # one operator build per context (the switch is read at creation); the
