@@ -121,8 +121,8 @@ def _c128(a):
     return np.ascontiguousarray(a, dtype=np.complex128)
 
 
-def grid_from_mesh(coord, etopol, grid_size=1.8, M_ex=2) -> GridDesc:
-    """build_grid (src/geometry.f90:60-125) -> GridDesc."""
+def grid_from_mesh(coord, etopol, grid_size=1.8, M_ex=2, order=0) -> GridDesc:
+    """build_grid (src/geometry.f90:60-125) -> GridDesc; order 1 selects the linear basis."""
     lib = load_library()
     coord = np.ascontiguousarray(coord, np.float64)
     etopol = np.ascontiguousarray(etopol, np.int32)
@@ -130,6 +130,7 @@ def grid_from_mesh(coord, etopol, grid_size=1.8, M_ex=2) -> GridDesc:
     rc = lib.scd_grid_from_mesh(coord.shape[0], _p(coord), etopol.shape[0], _p(etopol), grid_size, M_ex, C.byref(d))
     if rc:
         raise ScadynError(rc, "scd_grid_from_mesh")
+    d.order = order
     return d
 
 
