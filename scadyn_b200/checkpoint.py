@@ -9,9 +9,9 @@ midway is lost.  Here the columns are solved in blocks through
 compute_T_matrix's column range, and after every block the solved columns and
 a manifest (problem key, block list, per-column iterations) are written
 atomically to one .npz file, so an interrupted solve resumes at block
-granularity.  A JSON line of per-block metrics (columns/s, iterations, and the
-solver's per-phase device milliseconds when it keeps them) can be appended to a
-log.
+granularity.  A JSON line of per-block metrics (columns/s, iterations, the
+solver's per-phase device milliseconds when it keeps them, and once the near
+zone's achieved bandwidth and HBM-roofline fraction) can be appended to a log.
 """
 from __future__ import annotations
 
@@ -32,12 +32,29 @@ def _save(path, T, done, iters, key):
     os.replace(tmp, path)
 
 
-def solve_T_with_checkpoints(solver, Nmax, path, block=64, tag="", log=None, **opts):
+def near_zone_roofline(solver, hbm_gbs=None, reps=5):
+    """Achieved near-zone bandwidth of `solver` (profile_matvec at one FP64
+    right-hand side; the kernel reads every stored tile once per matvec) and,
+    given the HBM peak in GB/s, its roofline fraction."""
+    t = solver.profile_matvec(reps, 1, 0)
+    gbs = solver.nearzone_bytes() / (t["nearzone_ms"] * 1e-3) / 1e9
+    out = {"near_zone_ms": round(t["nearzone_ms"], 4), "gb_per_s": round(gbs, 1)}
+    if hbm_gbs:
+        out["frac_of_hbm"] = round(gbs / hbm_gbs, 4)
+    return out
+
+
+def solve_T_with_checkpoints(solver, Nmax, path, block=64, tag="", log=None, hbm_gbs=None, **opts):
     """T (2nm, 2nm) of `solver` (anything with compute_T_matrix(Nmax, col0,
     ncol, **opts) -> (T_cols, iters)), resuming from `path` when it holds a
     checkpoint of the same problem (same Nmax, options and tag).  Returns
-    (T, iters, blocks solved in this call)."""
+    (T, iters, blocks solved in this call).  With a log and a solver that
+    profiles (profile_matvec, nearzone_bytes), the first record also carries
+    the near zone's achieved bandwidth, as a fraction of hbm_gbs when given."""
     ncol = 2 * ((Nmax + 1) ** 2 - 1)
+    roof = None
+    if log and hasattr(solver, "profile_matvec") and hasattr(solver, "nearzone_bytes"):
+        roof = near_zone_roofline(solver, hbm_gbs)
     key = _key(Nmax, opts, tag)
     T = np.zeros((ncol, ncol), np.complex128)
     done = np.zeros(ncol, bool)
@@ -68,6 +85,9 @@ def solve_T_with_checkpoints(solver, Nmax, path, block=64, tag="", log=None, **o
                    "of": ncol}
             if timed:
                 rec["device"] = {k: v for k, v in solver.timing().items()}
+            if roof is not None:
+                rec["near_zone_roofline"] = roof
+                roof = None
             with open(log, "a") as f:
                 f.write(json.dumps(rec) + "\n")
     return T, iters, solved

@@ -67,3 +67,20 @@ def test_log_carries_device_phases(tmp_path):
     lines = [json.loads(x) for x in open(log)]
     assert len(lines) == 2 and s.resets == 2
     assert lines[0]["device"] == {"matvec_ms": 1.5, "matvecs": 7} and lines[0]["iters_max"] == 3
+
+
+class _Profiled(_Timed):
+    def profile_matvec(self, reps, nrhs, precision):
+        assert (nrhs, precision) == (1, 0)
+        return {"nearzone_ms": 0.5, "matvec_ms": 1.0}
+
+    def nearzone_bytes(self):
+        return 3_000_000_000
+
+
+def test_log_carries_near_zone_roofline_once(tmp_path):
+    log = str(tmp_path / "T.jsonl")
+    solve_T_with_checkpoints(_Profiled(), 2, str(tmp_path / "T.npz"), block=8, log=log, hbm_gbs=6000.0)
+    lines = [json.loads(x) for x in open(log)]
+    assert lines[0]["near_zone_roofline"] == {"near_zone_ms": 0.5, "gb_per_s": 6000.0, "frac_of_hbm": 1.0}
+    assert "near_zone_roofline" not in lines[1]
