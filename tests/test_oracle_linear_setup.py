@@ -363,3 +363,17 @@ def test_linear_operator_solves(lin_setup):
     assert info["converged"], info["relres"]
     r = op.compute_Ax2(x) - rhs
     assert np.linalg.norm(r) / np.linalg.norm(rhs) < 1e-5
+
+
+def test_self_blocks_nearly_symmetric(lin_setup):
+    """The operator is complex-symmetric; a self block V(T, T) applied one-sided must be
+    symmetric up to its quadrature (the singular double integrals are not evaluated
+    symmetrically, as for the constant basis).  A sign or transposition slip between
+    integrate_dV_V_GNN and integrate_V_dV_GNN, or in the (component, node) order of
+    integrate_dV_dV_GNN, would make it O(1) asymmetric."""
+    m, k, g, P, sp, ind = lin_setup
+    V = np.transpose(sp, (0, 2, 1))                  # V[b, row, col]
+    own = ind[:, 0] == ind[:, 1]
+    asym = np.array([np.linalg.norm(v - v.T) / np.linalg.norm(v) for v in V[own]])
+    assert own.sum() == m.n_tet
+    assert asym.max() < 5e-3, asym.max()
