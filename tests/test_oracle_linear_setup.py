@@ -377,3 +377,40 @@ def test_self_blocks_nearly_symmetric(lin_setup):
     asym = np.array([np.linalg.norm(v - v.T) / np.linalg.norm(v) for v in V[own]])
     assert own.sum() == m.n_tet
     assert asym.max() < 5e-3, asym.max()
+
+
+def test_linear_T_matrix_matches_mie_series(small_sphere):
+    """Physics pin of the whole linear-basis operator (projectors, 12x12 near zone,
+    order-1 compute_Ax2): a T-matrix solved in the linear basis agrees with the Mie
+    coefficients at discretisation level, as the constant basis does.  The reference
+    defines no linear-basis T-matrix, so the right-hand sides here are the VSWFs
+    projected on the basis functions N_n / sqrt(vol) (24-point rule), the counterpart
+    of vswf2constant's centroid values times sqrt(vol)."""
+    m = small_sphere
+    k, Nmax = 1.0 / m.a, 2
+    nm = (Nmax + 1) ** 2 - 1
+    op = O.setup_lin(m, k, grid_size=1.8, nthreads=0)
+    op.nthreads = 0
+    T = m.n_tet
+    mat = np.zeros((2 * nm, 12 * T), complex)
+    for t in range(T):
+        tc = m.coord[m.etopol[t] - 1]
+        vol = vol6(tc) / 6
+        Pq, w = SHP_T @ tc, QW * 6 * vol
+        for i in range(24):
+            MM, NN = O.calc_MN(Nmax, k, Pq[i])
+            f = SHP_T[i] * w[i] / np.sqrt(vol)             # per node
+            for c in range(3):
+                mat[:nm, 12 * t + 4 * c:12 * t + 4 * c + 4] += np.outer(MM[:, c], f)
+                mat[nm:, 12 * t + 4 * c:12 * t + 4 * c + 4] += np.outer(NN[:, c], f)
+    X = np.zeros_like(mat)
+    for c in range(2 * nm):
+        X[c], info = op.gmres(mat[c], tol=1e-6, m=50, cycles=6)
+        assert info["converged"]
+    Tl = (np.conj(mat) @ X.T) * (1j * k ** 3)
+    a_n, b_n = O.mie_T(Nmax, k * m.a, np.sqrt(2.25 + 0.01j))
+    for j in range(nm):
+        n = int(np.floor(np.sqrt(j + 1)))
+        assert abs(Tl[j, j] - a_n[n - 1]) < 0.08 * abs(a_n[n - 1])
+        assert abs(Tl[nm + j, nm + j] - b_n[n - 1]) < 0.08 * abs(b_n[n - 1])
+    assert np.abs(Tl[:nm, :nm] - np.diag(np.diag(Tl[:nm, :nm]))).max() < 0.05 * abs(a_n[0])
