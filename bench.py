@@ -260,6 +260,8 @@ def main():
                     help="tensor-core near zone for the complex64 matvec (SCADYN_NEAR_MMA=1; 2: merged schedule)")
     ap.add_argument("--cgs", action="store_true",
                     help="classical Gram-Schmidt for the complex64 inner solves (SCADYN_CGS=1)")
+    ap.add_argument("--near-split", action="store_true",
+                    help="near-zone row and column sums split in two partial sums (SCADYN_NEAR_SPLIT=2)")
     ap.add_argument("--fft-smooth", action="store_true",
                     help="5-smooth padded FFT lengths (80, 96, 192) where shorter than a power of two (SCADYN_FFT_SMOOTH=1)")
     args = ap.parse_args()
@@ -269,6 +271,8 @@ def main():
         os.environ["SCADYN_CGS"] = "1"
     if args.fft_smooth:
         os.environ["SCADYN_FFT_SMOOTH"] = "1"
+    if args.near_split:
+        os.environ["SCADYN_NEAR_SPLIT"] = "2"
     if args.serve:
         print(json.dumps(serve_bench(args.serve)), flush=True)
         return
@@ -533,6 +537,7 @@ def main():
                        "near_zone": ("tensor cores (f16 hi/lo, %s schedule)" % ("merged" if args.near_mma == "2" else "split"))
                                     if args.near_mma else "CUDA cores",
                        "inner_gram_schmidt": "classical, conditional re-orthogonalisation" if args.cgs else "modified",
+                       "near_zone_sums": "two partial sums per row/column" if args.near_split else "one",
                        "fft_lengths": [fft_len(2 * v, args.fft_smooth) for v in (desc.Nx, desc.Ny, desc.Nz)],
                        "parallelism": f"replicas x{world}"},
             "t_rel_err_vs_fp64": t_err,

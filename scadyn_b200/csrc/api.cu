@@ -386,6 +386,8 @@ int scd_create(scd_ctx **out, const scd_grid_desc *d) {
         c->nzm_sched = (e && e[0] == '2') ? 1 : 0;
         e = getenv("SCADYN_CGS");
         c->cgs_on = e && e[0] == '1';
+        e = getenv("SCADYN_NEAR_SPLIT");
+        c->near_split = (e && e[0] == '2') ? 2 : 1;
     }
     cudaSetDevice(c->dev);
     cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev);

@@ -101,6 +101,7 @@ struct scd_ctx {
     long long tile_store = 0;            // stored elements (tile_elems summed)
     long long max_tile_store = 0;        // largest tile_elems
     long long B_ref = 0;                 // blocks in the reference layout
+    int near_split = 1;                  // partial sums per near-zone row/column sum (SCADYN_NEAR_SPLIT=2)
     int near_cfg_err = 0;                // a near-zone launch was skipped: a tile outgrew the shared-memory ring
     // partial-sum slots per group: slot 0 holds the group's row sums over
     // all its tiles, slots 1.. the M^T x products of the tiles (g', g),

@@ -462,8 +462,40 @@ __device__ __forceinline__ void load_xu(uint32_t addr, C (&xu)[U]) {
     }
 }
 
-template <typename ST, typename C, int U>
+// partial sums p = 0..NS-1 -> p0 + p1 (NS = 2): NP partials in the lane, or
+// one per lane over L adjacent lanes (lane 0 of each pair gets the total;
+// every lane of the warp must call it)
+template <typename C> __device__ __forceinline__ C shfl_down_c(C v, int d, int width) {
+    v.x = __shfl_down_sync(0xffffffffu, v.x, d, width);
+    v.y = __shfl_down_sync(0xffffffffu, v.y, d, width);
+    return v;
+}
+template <typename C, int U, int NP, int L>
+__device__ __forceinline__ void combine_split(const C (&p)[NP][3][U], C (&tot)[3][U]) {
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if constexpr (NP == 2) {
+                tot[q][u] = cadd(p[0][q][u], p[1][q][u]);
+            } else if constexpr (L == 2) {
+                tot[q][u] = cadd(p[0][q][u], shfl_down_c(p[0][q][u], 1, 2));
+            } else {
+                tot[q][u] = p[0][q][u];
+            }
+        }
+}
+
+// NS (1 or 2) splits every row and column sum into NS partial sums over the
+// j (row) or i (column) residues mod NS, added in order at the end: with one
+// right-hand side (U = 1) NS lanes share a row or column, one partial each;
+// with U = 4 one lane keeps all NS partials.  Either way the sums are formed
+// in the same order, so a column stays bit-identical alone and in a batch.
+template <typename ST, typename C, int U, int NS>
 __global__ void __launch_bounds__(NZ_MAX_THREADS, NZ_MIN_CTAS<U>) k_near_groups(NearPass a) {
+    static_assert(NS == 1 || NS == 2, "split");
+    constexpr int L = U == 1 ? NS : 1;     // lanes per row or column
+    constexpr int NP = NS / L;             // partial sums per lane
     extern __shared__ __align__(128) unsigned char nz_sh[];
     uint64_t *full = reinterpret_cast<uint64_t *>(nz_sh);
     uint64_t *empty = full + NZ_SLOTS;
@@ -549,16 +581,20 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS, NZ_MIN_CTAS<U>) k_near_groups(
     // ---------------------------------------------------------- consumers
     const bool rowside = warp < HT / 32;
     const int it = rowside ? threadIdx.x : threadIdx.x - HT;
-    const bool row_item = rowside && it < n1 * a.nq;
-    const int rq = row_item ? it / n1 : 0, ri = row_item ? it - rq * n1 : 0;
+    const bool row_item = rowside && it < n1 * a.nq * L;
+    const int rq = row_item ? it / (n1 * L) : 0;
+    const int ri = row_item ? (it - rq * n1 * L) / L : 0, hl = row_item ? (it - rq * n1 * L) % L : 0;
     int ord = 0;
     for (int r0 = 0; r0 < a.nrhs; r0 += PS) {
         const int rg = min(PS, a.nrhs - r0);
-        C acc[3][U];
+        C accs[NP][3][U];
 #pragma unroll
-        for (int q = 0; q < 3; ++q)
+        for (int p = 0; p < NP; ++p)
 #pragma unroll
-            for (int u = 0; u < U; ++u) acc[q][u] = czero<C>();
+            for (int q = 0; q < 3; ++q)
+#pragma unroll
+                for (int u = 0; u < U; ++u) accs[p][q][u] = czero<C>();
+        C (&acc)[3][U] = accs[0];
         for (int t = t0; t < t1; ++t, ++ord) {
             const int kslot = ord % NZ_SLOTS;
             mbar_wait(&full[kslot], (uint32_t)((ord / NZ_SLOTS) & 1), a.err);
@@ -573,20 +609,36 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS, NZ_MIN_CTAS<U>) k_near_groups(
                 if (row_item) {
                     uint32_t mp = M + SB * ri;            // plane (9j + 3b), lane i
                     uint32_t xp = X2 + CB * U * rq;       // x row 3j + b
-                    for (int j = 0; j < n2; ++j) {
+                    // one j: the three b-planes into partial pp
+                    auto row_j = [&](C (&pp)[3][U]) {
 #pragma unroll
                         for (int b = 0; b < 3; ++b) {
                             C xu[U];
                             load_xu<C, U>(xp, xu);
                             const C mm[3] = {as_c<C>(lds_c(mp, ST{})), as_c<C>(lds_c(mp + mrow, ST{})),
                                              as_c<C>(lds_c(mp + 2 * mrow, ST{}))};
-                            mac3<C, U>(acc, mm, xu);
+                            mac3<C, U>(pp, mm, xu);
                             mp += 3 * mrow;
                             xp += xrow;
                         }
+                    };
+                    if constexpr (NP == 1) {
+                        // lane hl takes j = hl, hl + L, ...
+                        mp += hl * 9 * mrow;
+                        xp += hl * 3 * xrow;
+                        for (int j = hl; j < n2; j += L) {
+                            row_j(acc);
+                            mp += (L - 1) * 9 * mrow;
+                            xp += (L - 1) * 3 * xrow;
+                        }
+                    } else {
+                        for (int j = 0; j < n2; j += 2) {
+                            row_j(accs[0]);
+                            if (j + 1 < n2) row_j(accs[1]);
+                        }
                     }
                 }
-            } else if (tcoff >= 0 && it < n2 * a.nq) {
+            } else if (NS == 1 && tcoff >= 0 && it < n2 * a.nq) {
                 const int q = it / n2, j = it - q * n2;
                 C cacc[3][U];
 #pragma unroll
@@ -617,11 +669,74 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS, NZ_MIN_CTAS<U>) k_near_groups(
                         pc[2] = cacc[2][u];
                     }
                 }
+            } else if (NS > 1 && tcoff >= 0) {
+                // split column sums: partial p over i = p, p + NS, ...; the
+                // lanes of a column are adjacent (all lanes join the shuffle)
+                const bool col_item = it < n2 * a.nq * L;
+                const int q = col_item ? it / (n2 * L) : 0;
+                const int j = col_item ? (it - q * n2 * L) / L : 0, cl = col_item ? (it - q * n2 * L) % L : 0;
+                C cps[NP][3][U];
+#pragma unroll
+                for (int p = 0; p < NP; ++p)
+#pragma unroll
+                    for (int b = 0; b < 3; ++b)
+#pragma unroll
+                        for (int u = 0; u < U; ++u) cps[p][b][u] = czero<C>();
+                if (col_item) {
+                    const uint32_t mj = M + SB * 9 * j * ld1;
+                    const uint32_t x0 = smem_addr(X1) + CB * U * q;   // x row 3i + a
+                    auto col_i = [&](int i, C (&pp)[3][U]) {
+                        uint32_t xp = x0 + 3 * i * xrow;
+#pragma unroll
+                        for (int aa = 0; aa < 3; ++aa) {
+                            C xu[U];
+                            load_xu<C, U>(xp, xu);
+                            const uint32_t mp = mj + aa * mrow + SB * i;
+                            const C mm[3] = {as_c<C>(lds_c(mp, ST{})), as_c<C>(lds_c(mp + 3 * mrow, ST{})),
+                                             as_c<C>(lds_c(mp + 6 * mrow, ST{}))};
+                            mac3<C, U>(pp, mm, xu);
+                            xp += xrow;
+                        }
+                    };
+                    if constexpr (NP == 1) {
+                        for (int i = cl; i < n1; i += L) col_i(i, cps[0]);
+                    } else {
+                        for (int i = 0; i < n1; i += 2) {
+                            col_i(i, cps[0]);
+                            if (i + 1 < n1) col_i(i + 1, cps[1]);
+                        }
+                    }
+                }
+                C ctot[3][U];
+                combine_split<C, U, NP, L>(cps, ctot);
+                if (col_item && cl == 0) {
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int r = U * q + u;
+                        if (r < rg && !(a.skip && a.skip[r0 + r])) {
+                            C *pc = part + (r0 + r) * a.part_len + tcoff + 3 * j;
+                            pc[0] = ctot[0][u];
+                            pc[1] = ctot[1][u];
+                            pc[2] = ctot[2][u];
+                        }
+                    }
+                }
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[kslot]);
         }
-        if (row_item) {
+        if constexpr (NS > 1) {
+            if (rowside) {
+                // all row-side lanes take part in the combination (shuffles)
+                C tot[3][U];
+                combine_split<C, U, NP, L>(accs, tot);
+#pragma unroll
+                for (int q = 0; q < 3; ++q)
+#pragma unroll
+                    for (int u = 0; u < U; ++u) acc[q][u] = tot[q][u];
+            }
+        }
+        if (row_item && hl == 0) {
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int r = U * rq + u;
@@ -842,7 +957,7 @@ void fft_chain_t(scd_ctx *c, const C *x, int nrhs, const int *done) {
     c->launches += 6;
 }
 
-template <typename ST, typename C, int U>
+template <typename ST, typename C, int U, int NS>
 void near_launch(scd_ctx *c, const ST *data, const C *x, int nrhs, const int *done) {
     NearPass a;
     a.tiles = c->d_tiles; a.grp_tile = c->d_grp_tile; a.grp_off = c->d_grp_off; a.pslot_base = c->d_pslot_base;
@@ -851,7 +966,7 @@ void near_launch(scd_ctx *c, const ST *data, const C *x, int nrhs, const int *do
     a.err = c->d_kerr;
     const int nq = U == 1 ? 1 : std::min(NZ_QMAX, (nrhs + U - 1) / U);
     a.nq = nq;
-    a.half = 32 * ((c->max_per_group * a.nq + 31) / 32);
+    a.half = 32 * ((c->max_per_group * a.nq * (U == 1 ? NS : 1) + 31) / 32);   // lanes per side
     // xT rows are whole 16-byte units (bulk-copy granularity)
     a.rg_stride = nq * U;
     while ((a.rg_stride * sizeof(C)) % 16) ++a.rg_stride;
@@ -874,14 +989,20 @@ void near_launch(scd_ctx *c, const ST *data, const C *x, int nrhs, const int *do
         c->launches += 1;
     }
     const size_t sh = NZ_META + a.x1_bytes + a.ring_bytes;
-    cudaFuncSetAttribute(k_near_groups<ST, C, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-    k_near_groups<ST, C, U><<<c->ngroups, 2 * a.half + 32, sh, c->st>>>(a);
+    cudaFuncSetAttribute(k_near_groups<ST, C, U, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    k_near_groups<ST, C, U, NS><<<c->ngroups, 2 * a.half + 32, sh, c->st>>>(a);
 }
 
 template <typename ST, typename C>
 void near_dispatch(scd_ctx *c, const ST *data, const C *x, int nrhs, const int *done) {
-    if (nrhs == 1) near_launch<ST, C, 1>(c, data, x, nrhs, done);
-    else near_launch<ST, C, 4>(c, data, x, nrhs, done);
+    // SCADYN_NEAR_SPLIT=2: two partial sums per row and column (two lanes each at one right-hand side)
+    if (c->near_split == 2) {
+        if (nrhs == 1) near_launch<ST, C, 1, 2>(c, data, x, nrhs, done);
+        else near_launch<ST, C, 4, 2>(c, data, x, nrhs, done);
+    } else {
+        if (nrhs == 1) near_launch<ST, C, 1, 1>(c, data, x, nrhs, done);
+        else near_launch<ST, C, 4, 1>(c, data, x, nrhs, done);
+    }
 }
 
 template <typename C>
