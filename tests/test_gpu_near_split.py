@@ -1,8 +1,8 @@
-"""The near-zone kernel with split row and column sums (opt-in with
+"""The FP64 near-zone kernel with split row and column sums (opt-in with
 SCADYN_NEAR_SPLIT=2 at context creation: two lanes per sum at one right-hand
 side, two partial sums per lane at four): the FP64 matvec against the oracle,
-the complex64 matvec against the default kernel, and bit-identical columns
-alone and in batches (FP64 and mixed forms).  Collected only with
+solutions against the default kernel, and bit-identical columns alone and in
+batches (the mixed form's complex64 kernels are left unsplit).  Collected only with
 SCADYN_TEST_NEAR_SPLIT=1 until the variant has run on a GPU."""
 import os
 
