@@ -13,12 +13,15 @@ iterative refinement on the true residual to 1e-6, `--slots` columns in
 flight.  `value` is columns/s over K timed steps with the operator and the
 incident columns resident in HBM (device time from CUDA events on the
 library's stream, max over ranks); `e2e` is the same through the C ABI call a
-host makes (scd_solve_columns with host buffers: the step's columns copied
-in, T columns copied out, inside the timed region).  `forms` holds the plain
-FP64 GMRES(50) form one column at a time and batched, on the same columns,
-and `t_rel_err_vs_fp64` the Frobenius error of the mixed T against the FP64
-T.  `--impl reference` times the CPU oracle (the reference's algorithm
-restated in C) on the same operator.
+host makes (scd_solve_columns with host buffers: the whole incident matrix
+copied in from page-locked memory and the step's T columns copied out, every
+step, inside the timed region).  `forms` holds the plain FP64 GMRES(50) form
+one column at a time and batched, on the same columns, and
+`t_rel_err_vs_fp64` the Frobenius error of the mixed T against the FP64 T.
+`--impl reference` runs the reference's algorithm on the host cores through
+the CPU oracle (its C restatement), end to end: the oracle sets up its own
+operator and solves `--ref-columns` columns with its FP64 GMRES; the metric
+string, unit and direction are the same as this arm's.
 """
 from __future__ import annotations
 
@@ -63,6 +66,13 @@ CONFIGS = {
 
 L2_BYTES = 126 * 1024 * 1024
 
+# the headline metric, the same string in both arms
+METRIC = "T-matrix columns/sec & p50/p99 solve latency at \u22641e-5 rel err, mixed vs plain FP64"
+# kernel choices of scd_grid_desc / scd_solve_opts (0 = the library's default)
+NEAR_KERNELS = {"default": 0, "cuda": 1, "split": 2, "merged": 3}
+GRAM_SCHMIDT = {"default": 0, "modified": 1, "classical": 2}
+FFT_LENGTHS = {"default": 0, "pow2": 1, "smooth": 2}
+
 
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
@@ -84,13 +94,16 @@ def make_mesh(cfg):
     return mesh
 
 
-def build_solver(cfg, mesh, device, order=0):
-    """The operator from the mesh on the device; order 1 = linear basis (4 basis functions per tet)."""
+def build_solver(cfg, mesh, device, order=0, choices=None):
+    """The operator from the mesh on the device; order 1 = linear basis (4
+    basis functions per tet); choices = kernel choices of scd_grid_desc."""
     from scadyn_b200 import api, geometry
     gs = geometry.cell_size_for_grid(mesh.coord, mesh.etopol, cfg["N"])
     d = api.grid_from_mesh(mesh.coord, mesh.etopol, grid_size=gs)
     d.device = device
     d.order = order
+    for key, v in (choices or {}).items():
+        setattr(d, key, v)
     s = api.Solver.from_desc(d, device=device)
     k = cfg["ka"] / mesh.a
     t0 = time.time()
@@ -188,12 +201,41 @@ def cpu_oracle_op(solver, mesh, grid_size, k):
     return op, time.time() - t0
 
 
-def cpu_baseline(solver, mesh, grid_size, k, cfg, iters, cycles_run, budget_s=25.0, op=None):
-    """Time the CPU oracle on the same operator data: compute_Ax2 calls (six
-    convolutions, complex64 near zone, all host threads) and a 4-step GMRES
-    cycle for the orthogonalisation cost; columns/s = 1 / (mean over the
-    timed columns of (iters + cycles) * t_matvec + t_mgs_unit * sum of MGS
-    terms)."""
+def mgs_unit_s(n, nvec=8, reps=3):
+    """Seconds per modified Gram-Schmidt term (one <v_k, w> and one w -= h v_k
+    over n unknowns, all host threads) of the oracle's GMRES, timed directly
+    on nvec random Krylov vectors."""
+    from oracle import oracle as O
+    rng = np.random.default_rng(11)
+    V = rng.standard_normal((nvec, n)) + 1j * rng.standard_normal((nvec, n))
+    w = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    O.mgs_terms(V, w.copy())                       # warm
+    best = 1e30
+    for _ in range(reps):
+        ww = w.copy()
+        t = time.time()
+        O.mgs_terms(V, ww)
+        best = min(best, (time.time() - t) / nvec)
+    return best
+
+
+def mgs_terms_of(it, m):
+    """MGS terms of a restarted GMRES(m) column that took `it` Arnoldi steps."""
+    terms, left = 0, it
+    while left > 0:
+        s = min(left, m)
+        terms += s * (s + 1) // 2
+        left -= s
+    return terms
+
+
+def cpu_baseline(solver, mesh, grid_size, k, cfg, iters, cycles_run, op=None):
+    """A bounded CPU sample beside the GPU line (about half a minute): the
+    oracle's compute_Ax2 (six convolutions, complex64 near zone widened, all
+    host threads) on the device-built operator copied back, and its MGS term
+    cost timed alone; columns/s extrapolated with the GPU FP64 form's
+    per-column iteration counts of the same columns.  `bench.py --impl
+    reference` is the measured end-to-end CPU run."""
     prep = 0.0
     if op is None:
         op, prep = cpu_oracle_op(solver, mesh, grid_size, k)
@@ -203,36 +245,81 @@ def cpu_baseline(solver, mesh, grid_size, k, cfg, iters, cycles_run, budget_s=25
     x = rng.standard_normal(3 * g.T) + 1j * rng.standard_normal(3 * g.T)
     op.compute_Ax2(x)                      # warm
     t = time.time()
-    nmv = 0
-    while True:
+    for _ in range(3):
         op.compute_Ax2(x)
-        nmv += 1
-        if nmv >= 2 or time.time() - t > budget_s / 2:
-            break
-    t_mv = (time.time() - t) / nmv
-    mat_col = solver.vswf2constant(1)[0]
-    t = time.time()
-    _, info = op.gmres(mat_col, tol=1e-30, m=4, cycles=1)
-    t_cyc = time.time() - t
-    mgs_terms_4 = sum(range(1, 5))
-    t_unit = max(t_cyc - (info["matvecs"]) * t_mv, 0.0) / mgs_terms_4
-
-    def col_time(it, cy):
-        terms = 0
-        left = it
-        while left > 0:
-            s = min(left, cfg["m"])
-            terms += s * (s + 1) // 2
-            left -= s
-        return (it + cy) * t_mv + t_unit * terms
-
-    per_col = [col_time(i, c) for i, c in zip(iters, cycles_run)]
+    t_mv = (time.time() - t) / 3
+    t_unit = mgs_unit_s(3 * g.T)
+    per_col = [(it + cy) * t_mv + t_unit * mgs_terms_of(it, cfg["m"]) for it, cy in zip(iters, cycles_run)]
     value = 1.0 / float(np.mean(per_col))
-    sample = (f"oracle compute_Ax2 x{nmv} ({t_mv:.2f} s each, six convolutions, complex64 near zone) and a "
-              f"4-step GMRES cycle ({t_cyc:.2f} s) on the same operator; columns/s extrapolated with the "
-              f"measured per-column iteration counts (mean {np.mean(iters):.1f}); operator copy-back {prep:.1f} s")
+    sample = (f"extrapolated: oracle compute_Ax2 x3 ({t_mv:.3f} s each) and MGS terms timed alone "
+              f"({t_unit * 1e3:.2f} ms each) on the device-built operator copied back; per column "
+              f"(iters + cycles) matvecs + MGS terms with the GPU FP64 iteration counts of the same columns "
+              f"(mean {np.mean(iters):.1f}); operator copy-back {prep:.1f} s")
     return {"value": value, "unit": "columns/s", "cores": ncores, "kind": "port", "sample": sample,
             "t_matvec_s": t_mv, "t_mgs_unit_s": t_unit}
+
+
+def reference_arm(args, cfg):
+    """The reference's algorithm on the host cores, end to end, through the
+    oracle (its C restatement of the Fortran): the operator set up by the
+    oracle itself (pfft_projection_const, build_G,
+    compute_near_zone_interactions_const), then `--ref-columns` T-matrix
+    columns spread over all 2nm solved one at a time with its restarted FP64
+    GMRES(m) (src/T_matrix.f90:254-268, src/gmres_module.f90:180-325) and
+    assembled as mat^H x.  Columns/s = columns / measured solve time."""
+    from oracle import oracle as O
+    from scadyn_b200 import geometry
+    mesh = make_mesh(cfg)
+    gs = geometry.cell_size_for_grid(mesh.coord, mesh.etopol, cfg["N"])
+    k = cfg["ka"] / mesh.a
+    t0 = time.time()
+    op = O.setup(mesh, k, grid_size=gs, nthreads=0)
+    op.nthreads = 0
+    setup_s = time.time() - t0
+    mat = O.vswf2constant(mesh.coord, mesh.etopol, k, cfg["Nmax"])
+    ncol_tot = mat.shape[0]
+    log(f"[reference] T={mesh.n_tet} grid={op.geom.Nx}x{op.geom.Ny}x{op.geom.Nz} "
+        f"near blocks={op.sp_ind.shape[0]} oracle set-up {setup_s:.0f}s")
+    rng = np.random.default_rng(7)
+    x = rng.standard_normal(3 * mesh.n_tet) + 1j * rng.standard_normal(3 * mesh.n_tet)
+    for _ in range(args.warmup):
+        op.compute_Ax2(x)
+    nref = max(1, args.ref_columns)
+    cols = [int(c) for c in np.unique(np.linspace(0, ncol_tot - 1, nref + 2).round().astype(int)[1:-1])]
+    secs, iters, T_err = [], [], []
+    for c in cols:
+        t = time.time()
+        xs, info = op.gmres(mat[c], tol=cfg["tol"], m=cfg["m"], cycles=cfg["cycles"])
+        Tc = mat.conj() @ xs                       # T_mat(:, c) = mat^H x (src/T_matrix.f90:260)
+        secs.append(time.time() - t)
+        iters.append(int(info["iters"]))
+        log(f"[reference] column {c}: {info['iters']} iterations, relres {info['relres']:.2e}, {secs[-1]:.1f}s")
+    value = len(cols) / float(sum(secs))
+    ncores = os.cpu_count()
+    sample = (f"{len(cols)} columns {cols} of {ncol_tot} solved end to end (FP64 GMRES({cfg['m']}), tol {cfg['tol']:g}, "
+              f"mean {np.mean(iters):.1f} iterations) on the oracle's own operator, all {ncores} host threads; "
+              f"operator set-up {setup_s:.0f} s not timed")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "columns/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128 (near zone stored complex64, as the reference)",
+            "data": "synthetic (seeded jittered cube-lattice mesh)",
+            "config": {"workload": cfg["workload"], "tets": mesh.n_tet,
+                       "grid_nodes": [op.geom.Nx, op.geom.Ny, op.geom.Nz], "near_blocks": int(op.sp_ind.shape[0]),
+                       "form": "plain FP64 GMRES(%d), one column at a time (the reference's only form)" % cfg["m"]},
+            "p50_ms": round(float(np.percentile(secs, 50)) * 1e3, 1),
+            "p99_ms": round(float(np.percentile(secs, 99)) * 1e3, 1),
+            "columns": cols, "iters": iters, "column_s": [round(v, 2) for v in secs], "setup_s": round(setup_s, 1),
+            "cpu_baseline": {"value": value, "unit": "columns/s", "cores": ncores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "columns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def pinned_like(a):
+    """A page-locked host copy of a numpy array (torch pin_memory), so that
+    host->device copies run at full bus speed as a host application's would."""
+    import torch
+    t = torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+    return t, t.numpy()
 
 
 def main():
@@ -244,35 +331,32 @@ def main():
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--block", type=int, default=64, help="columns per step")
     ap.add_argument("--slots", type=int, default=32, help="columns solved concurrently (batched GMRES slots)")
-    ap.add_argument("--plain-sample", type=int, default=2, help="columns timed in the plain one-at-a-time form")
+    ap.add_argument("--plain-sample", type=int, default=8, help="columns timed in the plain one-at-a-time form")
+    ap.add_argument("--ref-columns", type=int, default=2, help="columns the CPU reference arm solves end to end")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serve", action="store_true", help="skip the served-stream summary")
     ap.add_argument("--serve", type=int, default=0,
                     help="run a served request stream of this many requests instead (C4-shaped, scaled)")
     ap.add_argument("--sweep", type=int, default=0,
                     help="run a C3-shaped wavelength sweep with this many wavelengths instead")
     ap.add_argument("--sweep-nmax", type=int, default=14, help="largest Nmax of the sweep (C3: 14)")
     ap.add_argument("--profile", default=None,
-                    choices=["near1", "near16", "mixed16", "solve16", "near-compare", "linear"],
+                    choices=["near1", "near16", "mixed16", "mixed32", "solve16", "near-compare", "linear"],
                     help="only build the operator and run profile_matvec (for ncu captures); near-compare times "
                          "the complex64 x16 matvec with the CUDA-core near zone and both tensor-core schedules; "
                          "linear times the linear-basis set-up and matvec against the constant basis")
-    ap.add_argument("--near-mma", nargs="?", const="1", default=None, choices=["1", "2"],
-                    help="tensor-core near zone for the complex64 matvec (SCADYN_NEAR_MMA=1; 2: merged schedule)")
-    ap.add_argument("--cgs", action="store_true",
-                    help="classical Gram-Schmidt for the complex64 inner solves (SCADYN_CGS=1)")
+    ap.add_argument("--near-kernel", default="default", choices=sorted(NEAR_KERNELS),
+                    help="near zone of the complex64 matvec (scd_grid_desc.near_kernel)")
+    ap.add_argument("--gram-schmidt", default="default", choices=sorted(GRAM_SCHMIDT),
+                    help="orthogonalisation of the complex64 inner solves (scd_solve_opts.gram_schmidt)")
+    ap.add_argument("--fft-lengths", default="default", choices=sorted(FFT_LENGTHS),
+                    help="padded FFT lengths (scd_grid_desc.fft_lengths)")
     ap.add_argument("--near-split", action="store_true",
-                    help="near-zone row and column sums split in two partial sums (SCADYN_NEAR_SPLIT=2)")
-    ap.add_argument("--fft-smooth", action="store_true",
-                    help="5-smooth padded FFT lengths (80, 96, 192) where shorter than a power of two (SCADYN_FFT_SMOOTH=1)")
+                    help="FP64 near-zone row and column sums split in two partial sums (scd_grid_desc.near_split)")
     args = ap.parse_args()
-    if args.near_mma:
-        os.environ["SCADYN_NEAR_MMA"] = args.near_mma
-    if args.cgs:
-        os.environ["SCADYN_CGS"] = "1"
-    if args.fft_smooth:
-        os.environ["SCADYN_FFT_SMOOTH"] = "1"
-    if args.near_split:
-        os.environ["SCADYN_NEAR_SPLIT"] = "2"
+    choices = dict(near_kernel=NEAR_KERNELS[args.near_kernel], fft_lengths=FFT_LENGTHS[args.fft_lengths],
+                   near_split=2 if args.near_split else 0)
+    gs_choice = GRAM_SCHMIDT[args.gram_schmidt]
     if args.serve:
         print(json.dumps(serve_bench(args.serve)), flush=True)
         return
@@ -284,6 +368,11 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        # the CPU arm: rank 0 alone, no GPU work and no collective
+        if rank == 0:
+            reference_arm(args, cfg)
+        return
     dist = None
     if world > 1:
         import datetime
@@ -292,25 +381,20 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
-    if args.impl == "reference" and rank != 0:
-        if dist:
-            dist.destroy_process_group()
-        return
-
     from scadyn_b200 import api
     mesh = make_mesh(cfg)
-    solver, desc, gs, k, setup_s = build_solver(cfg, mesh, local)
+    solver, desc, gs, k, setup_s = build_solver(cfg, mesh, local, choices=choices)
     Nmax = cfg["Nmax"]
     ncol_tot = 2 * ((Nmax + 1) ** 2 - 1)
     B = args.block
     log(f"[rank {rank}] T={mesh.n_tet} grid={desc.Nx}x{desc.Ny}x{desc.Nz} near blocks={solver.nearzone_count()} "
         f"setup {setup_s:.1f}s")
+    mixed = dict(tol=cfg["tol"], m=cfg["inner_m"], cycles=60, precision=api.PREC_MIXED,
+                 inner_tol=cfg["inner_tol"], max_outer=cfg["max_outer"], gram_schmidt=gs_choice)
     if args.profile == "solve16":
         # sixteen columns in the mixed batched form (large configs: a sample of the column loop)
         solver.timing(reset=True)
-        _, it = solver.compute_T_matrix(Nmax, col0=0, ncol=16, block=16, tol=cfg["tol"], m=cfg["inner_m"],
-                                        cycles=60, precision=api.PREC_MIXED, inner_tol=cfg["inner_tol"],
-                                        max_outer=cfg["max_outer"])
+        _, it = solver.compute_T_matrix(Nmax, col0=0, ncol=16, block=16, **mixed)
         ms = solver.timing(reset=True)["accum_ms"]
         print(json.dumps({"config": args.config, "tets": mesh.n_tet, "grid_nodes": [desc.Nx, desc.Ny, desc.Nz],
                           "near_bytes": solver.nearzone_bytes(), "setup_s": round(setup_s, 2),
@@ -326,7 +410,7 @@ def main():
         runs = [solver.profile_matvec(10, 1, api.PREC_FP64) for _ in range(5)]
         out["ms"]["constant_fp64_1rhs"] = round(float(np.median([r["matvec_ms"] for r in runs])), 4)
         solver.close()
-        sv, _, _, _, lin_setup_s = build_solver(cfg, mesh, local, order=1)
+        sv, _, _, _, lin_setup_s = build_solver(cfg, mesh, local, order=1, choices=choices)
         out["setup_s"]["linear"] = round(lin_setup_s, 2)
         out["near_blocks_12x12"] = sv.nearzone_count()
         for label, nrhs, prec in (("linear_fp64_1rhs", 1, api.PREC_FP64), ("linear_c64_16rhs", 16, api.PREC_MIXED)):
@@ -337,27 +421,28 @@ def main():
         print(json.dumps(out), flush=True)
         return
     if args.profile == "near-compare":
-        # one operator build per context (the switch is read at creation); the
-        # same mesh, 16 complex64 right-hand sides, median of 5 profiled loops
+        # one operator build per context (the kernel is fixed at creation); the
+        # same mesh, 16 and 32 complex64 right-hand sides, median of 5 profiled loops
         solver.close()
-        out = {"config": args.config, "tets": mesh.n_tet, "nrhs": 16, "ms": {}}
-        for mode, label in (("0", "cuda_cores"), ("1", "tensor_split"), ("2", "tensor_merged")):
-            os.environ["SCADYN_NEAR_MMA"] = mode
-            sv, _, _, _, _ = build_solver(cfg, mesh, local)
-            runs = [sv.profile_matvec(10, 16, api.PREC_MIXED) for _ in range(5)]
-            out["ms"][label] = {key: round(float(np.median([r[key] for r in runs])), 4)
-                                for key in ("nearzone_ms", "fft_ms", "gather_ms", "matvec_ms")}
+        out = {"config": args.config, "tets": mesh.n_tet, "ms": {}}
+        for label in ("cuda", "split", "merged"):
+            sv, _, _, _, _ = build_solver(cfg, mesh, local, choices=dict(choices, near_kernel=NEAR_KERNELS[label]))
+            for nrhs in (16, 32):
+                runs = [sv.profile_matvec(10, nrhs, api.PREC_MIXED) for _ in range(5)]
+                out["ms"][f"{label}_{nrhs}"] = {key: round(float(np.median([r[key] for r in runs])), 4)
+                                                for key in ("nearzone_ms", "near_kernel_ms", "fft_ms", "gather_ms",
+                                                            "matvec_ms")}
             sv.close()
-        os.environ.pop("SCADYN_NEAR_MMA", None)
         print(json.dumps(out), flush=True)
         return
     if args.profile:
         nrhs, prec = {"near1": (1, api.PREC_FP64), "near16": (16, api.PREC_FP64),
-                      "mixed16": (16, api.PREC_MIXED)}[args.profile]
+                      "mixed16": (16, api.PREC_MIXED), "mixed32": (32, api.PREC_MIXED)}[args.profile]
         for _ in range(3):
             t = solver.profile_matvec(1, nrhs, prec)
-            log(f"profile {args.profile}: " + ", ".join(f"{k} {t[k]:.4f}" for k in ("nearzone_ms", "fft_ms",
-                                                                                   "gather_ms", "matvec_ms")))
+            log(f"profile {args.profile}: " + ", ".join(f"{k} {t[k]:.4f}" for k in ("nearzone_ms", "near_kernel_ms",
+                                                                                   "fft_ms", "gather_ms",
+                                                                                   "matvec_ms")))
         solver.close()
         return
 
@@ -365,44 +450,11 @@ def main():
         c0 = ((rank * (args.warmup + args.steps) + step) * B) % ncol_tot
         return min(c0, ncol_tot - B)
 
-    if args.impl == "reference":
-        # reference arm: the CPU oracle on the same operator, one bounded
-        # sample per step (W untimed, K timed); the per-column iteration
-        # counts of the timed columns come from the FP64 GMRES on the device
-        # (the reference's algorithm: the same counts one column at a time
-        # or batched)
-        iters, cycles = [], []
-        for st in range(args.warmup, args.warmup + args.steps):
-            _, it = solver.compute_T_matrix(Nmax, col0=cols_for(st), ncol=B, tol=cfg["tol"], m=cfg["m"],
-                                            cycles=cfg["cycles"], block=min(args.slots, B))
-            iters += list(it)
-            cycles += [max(1, -(-int(i) // cfg["m"])) for i in it]
-        op, _ = cpu_oracle_op(solver, mesh, gs, k)
-        for st in range(args.warmup):
-            cpu_baseline(solver, mesh, gs, k, cfg, iters, cycles, budget_s=2.0, op=op)
-        vals = []
-        for st in range(args.steps):
-            cb = cpu_baseline(solver, mesh, gs, k, cfg, iters, cycles, budget_s=4.0, op=op)
-            vals.append(cb["value"])
-        value = float(np.median(vals))
-        line = {"impl": "reference", "metric": "T-matrix columns/s", "value": value, "unit": "columns/s",
-                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic (seeded mesh)", "config": {"workload": cfg["workload"], "tets": mesh.n_tet},
-                "cpu_baseline": {"value": value, "unit": "columns/s", "cores": cb["cores"], "kind": "port",
-                                 "sample": cb["sample"]},
-                "e2e": {"value": value, "unit": "columns/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
-        solver.close()
-        return
-
     # ---------------------------------------------------------------- ours
     # headline form: mixed precision (complex64 inner GMRES(inner_m) to
     # inner_tol, FP64 iterative refinement on the true residual to tol),
     # `S` columns in flight as batched slots, continuous batching
     fp64 = dict(tol=cfg["tol"], m=cfg["m"], cycles=cfg["cycles"])
-    mixed = dict(tol=cfg["tol"], m=cfg["inner_m"], cycles=60, precision=api.PREC_MIXED,
-                 inner_tol=cfg["inner_tol"], max_outer=cfg["max_outer"])
     S = min(args.slots, B)
     for st in range(args.warmup):
         solver.compute_T_matrix(Nmax, col0=cols_for(st), ncol=B, block=S, **mixed)
@@ -454,55 +506,75 @@ def main():
     # plain form: one column at a time, FP64 GMRES(m) -- the reference's algorithm on the GPU
     if args.plain_sample > 0:
         solver.timing(reset=True)
-        for j in range(args.plain_sample):
-            solver.compute_T_matrix(Nmax, col0=c0 + j, ncol=1, block=1, **fp64)
+        pick = np.unique(np.linspace(0, B - 1, args.plain_sample).round().astype(int))
+        for j in pick:
+            solver.compute_T_matrix(Nmax, col0=c0 + int(j), ncol=1, block=1, **fp64)
         pm = solver.timing(reset=True)["accum_ms"]
-        forms["plain_fp64_one_column"] = round(args.plain_sample / (pm / 1e3), 4)
+        forms["plain_fp64_one_column"] = round(len(pick) / (pm / 1e3), 4)
+        forms["plain_fp64_columns_timed"] = int(len(pick))
     forms["mixed_batched_%d_slots" % S] = round(value / world, 4)
     if "plain_fp64_one_column" in forms:
         forms["mixed_batched_over_plain_fp64"] = round(forms["mixed_batched_%d_slots" % S] /
                                                        forms["plain_fp64_one_column"], 3)
 
-    # e2e: the same columns through scd_solve_columns with host buffers
-    # (incident columns host->device, T columns device->host, per step)
+    # e2e: the same columns through the C ABI a host calls, scd_solve_columns
+    # with host buffers: every step copies the whole incident matrix mat
+    # (3T, 2nm) in from page-locked memory (T_mat = mat^H x needs all of it)
+    # and the step's T columns (2nm, B) out
     mat_all = solver.vswf2constant(Nmax)
+    _keep, mat_pinned = pinned_like(mat_all)
     e2e_ms = 0.0
     h2d = d2h = 0
+    T_e2e0 = None
     for st in range(args.warmup, args.warmup + args.steps):
         c0s = cols_for(st)
-        blk = np.ascontiguousarray(mat_all[c0s:c0s + B])
         t = time.time()
-        Tc, its, _, _ = solver.solve_columns(blk, block=S, **mixed)
+        Tc, its, _, _ = solver.solve_columns(mat_pinned, col0=c0s, ncol=B, block=S, **mixed)
         e2e_ms += (time.time() - t) * 1e3
-        h2d = blk.nbytes
+        if T_e2e0 is None:
+            T_e2e0 = Tc
+        h2d = mat_pinned.nbytes
         d2h = Tc.nbytes + its.nbytes
     e2e_val = world * cols / (max_over_ranks(e2e_ms) / 1e3)
+    # the e2e T columns are the unscaled T_mat = mat^H x; times i k^3 they are
+    # the timed region's first T block
+    k3 = k ** 3
+    e2e_vs_device = float(np.linalg.norm(1j * k3 * T_e2e0.T - T_mixed0) / np.linalg.norm(T_mixed0))
 
     # per-kernel times of the batched complex64 matvec (the timed region's shape)
     profb = solver.profile_matvec(5, S, api.PREC_MIXED)
     batched = {"nrhs": S, "precision": "complex64", "matvec_ms": profb["matvec_ms"],
                "nearzone_ms": profb["nearzone_ms"], "fft_chain_ms": profb["fft_ms"],
                "gather_ms": profb["gather_ms"]}
-    # roofline of the dominant HBM-bound kernel: the near-zone block SpMV of
-    # a single-column matvec (live CUDA events on the library's stream)
-    prof = solver.profile_matvec(20, 1)
-    Bref = solver.nearzone_count()
-    alg_bytes = Bref * (9 * 8 + 8)                 # complex64 blocks + index pair, per matvec
-    near_ms = prof["nearzone_ms"]
-    achieved = alg_bytes / (near_ms / 1e3) / 1e9
     peak, kind = peaks()
-    traffic = profile_traffic(f"near_groups_{args.config}.txt")
+    Bref = solver.nearzone_count()
+    alg_bytes = Bref * (9 * 8 + 8)                 # complex64 blocks + index pair, per pass over the tiles
+    # roofline of the headline's dominant kernel: the complex64 near-zone
+    # kernel at 16 right-hand sides per pass (one launch of the batched inner
+    # matvec), live CUDA events on the library's stream
+    prof16 = solver.profile_matvec(20, 16, api.PREC_MIXED)
+    near_ms = prof16["near_kernel_ms"]
+    achieved = alg_bytes / (near_ms / 1e3) / 1e9
+    traffic = profile_traffic(f"near_mma_{args.config}.txt")
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": kind,
-            "kernel": "k_near_groups (near-zone block SpMV, one right-hand side, FP64)",
-            "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": near_ms, "matvec_ms": prof["matvec_ms"],
-            "fft_chain_ms": prof["fft_ms"], "gather_ms": prof["gather_ms"]}
+            "kernel": ("k_near_mma (tensor-core near-zone tile products, 16 complex64 right-hand sides per launch)"
+                       if choices["near_kernel"] != NEAR_KERNELS["cuda"] else
+                       "k_near_groups (near-zone block SpMV, 16 complex64 right-hand sides per launch)"),
+            "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": near_ms,
+            "flops_per_launch": Bref * 144 * 16 * 2}
+    # secondary: the FP64 one-right-hand-side near zone of the plain form
+    prof1 = solver.profile_matvec(20, 1)
+    roof["fp64_one_rhs"] = {"kernel": "k_near_groups (FP64, one right-hand side)", "avg_launch_ms": prof1["near_kernel_ms"],
+                            "achieved": round(alg_bytes / (prof1["near_kernel_ms"] / 1e3) / 1e9, 1),
+                            "frac": round(alg_bytes / (prof1["near_kernel_ms"] / 1e3) / 1e9 / peak, 4),
+                            "traffic": profile_traffic(f"near_groups_{args.config}.txt")}
     # whole pFFT matvec against HBM (algorithmic bytes per right-hand side,
     # four merged convolutions, operator reads shared by the batch)
-    roof["matvec"] = matvec_roofline(solver, desc, mesh.n_tet, Bref, peak, prof["matvec_ms"], profb["matvec_ms"], S)
+    roof["matvec"] = matvec_roofline(solver, desc, mesh.n_tet, Bref, peak, prof1["matvec_ms"], profb["matvec_ms"], S)
 
     serving = None
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_serve:
         try:
             sv = serve_bench(8)
             serving = {k: sv[k] for k in ("value", "unit", "p50_ms", "p99_ms", "completed", "columns",
@@ -521,8 +593,7 @@ def main():
     if rank == 0:
         lat_s = sorted(lat)
         line = {
-            "metric": "T-matrix columns/s (mixed complex64 GMRES + FP64 refinement to 1e-6, batched columns; "
-                      "T rel err vs FP64 <= 1e-5)",
+            "metric": METRIC,
             "value": round(value, 4), "unit": "columns/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(dev_ms / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c64 inner / f64 outer",
@@ -530,15 +601,14 @@ def main():
             "config": {"workload": cfg["workload"], "tets": mesh.n_tet,
                        "grid_nodes": [desc.Nx, desc.Ny, desc.Nz], "near_blocks": Bref,
                        "near_bytes": solver.nearzone_bytes(), "columns_per_step": B, "slots": S,
+                       "form": "mixed precision, batched columns",
                        "precision": "complex64 inner GMRES(%d) to %g, FP64 outer refinement to %g (near zone "
                                     "stored complex64 as the reference)" % (cfg["inner_m"], cfg["inner_tol"],
                                                                             cfg["tol"]),
                        "l2": "inputs larger than L2 (near-zone tiles %.2f GB per matvec)" % (solver.nearzone_bytes() / 1e9),
-                       "near_zone": ("tensor cores (f16 hi/lo, %s schedule)" % ("merged" if args.near_mma == "2" else "split"))
-                                    if args.near_mma else "CUDA cores",
-                       "inner_gram_schmidt": "classical, conditional re-orthogonalisation" if args.cgs else "modified",
-                       "near_zone_sums": "two partial sums per row/column" if args.near_split else "one",
-                       "fft_lengths": [fft_len(2 * v, args.fft_smooth) for v in (desc.Nx, desc.Ny, desc.Nz)],
+                       "near_kernel": args.near_kernel, "gram_schmidt": args.gram_schmidt,
+                       "near_split": bool(args.near_split),
+                       "fft_lengths": [fft_len(2 * v, FFT_LENGTHS[args.fft_lengths] != 1) for v in (desc.Nx, desc.Ny, desc.Nz)],
                        "parallelism": f"replicas x{world}"},
             "t_rel_err_vs_fp64": t_err,
             "p50_ms": round(float(np.percentile(lat_s, 50)), 3),
@@ -548,7 +618,7 @@ def main():
             "batched_matvec": batched,
             "serving": serving,
             "e2e": {"value": round(e2e_val, 4), "unit": "columns/s", "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h)},
+                    "d2h_bytes_per_step": int(d2h), "T_rel_diff_vs_device_region": e2e_vs_device},
             "roofline": roof,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),

@@ -15,8 +15,8 @@
  *   sp_mat           (3, 3, B)     near-zone blocks, tet_B >= tet_T
  *   sp_ind           (2, B)        1-based (tet_T, tet_B)
  *   Fg               (2Nx,2Ny,2Nz) FFT of the zero-padded Green's function
- *   mat              (3T, ncol)    incident VSWF columns
- *   Tcols            (ncol, ncol)  matᴴ·X, unscaled T_mat columns
+ *   mat              (3T, nmat)    incident VSWF columns, nmat = 2nm
+ *   Tcols            (nmat, ncol)  matᴴ·X, unscaled T_mat columns
  * Host arrays are borrowed for the duration of a call; device copies belong
  * to the context until scd_destroy.  A context is not thread-safe.
  */
@@ -68,7 +68,26 @@ typedef struct scd_grid_desc {
     int32_t M_ex;            /* projection order (mesh%M_ex); 2 only */
     int32_t near_zone;       /* near-cube radius (mesh%near_zone); 1 only */
     int32_t device;          /* CUDA device ordinal */
+    /* kernel choices fixed at scd_create (0 = the library's default; no
+     * counterpart in the reference, whose FFTW plans are made at run time,
+     * src/possu.f90:82-89) */
+    int32_t fft_lengths;     /* SCD_FFT_*: padded FFT length per axis */
+    int32_t near_kernel;     /* SCD_NEAR_*: near-zone kernel of the complex64 matvec */
+    int32_t near_split;      /* partial sums per near-zone row/column sum of the FP64 matvec: 0 or 1 one, 2 two */
 } scd_grid_desc;
+
+/* scd_grid_desc.fft_lengths.  Every choice is an exact linear convolution:
+ * the input occupies N <= P/2 samples of each axis. */
+#define SCD_FFT_DEFAULT         0   /* SCD_FFT_SMOOTH */
+#define SCD_FFT_POW2            1   /* smallest power of two >= 2N */
+#define SCD_FFT_SMOOTH          2   /* smallest of the powers of two and 80, 96, 192 that is >= 2N */
+
+/* scd_grid_desc.near_kernel: the near-zone SpMV of the complex64 matvec of the
+ * mixed-precision inner solves (the FP64 matvec always runs on the CUDA cores) */
+#define SCD_NEAR_DEFAULT        0   /* SCD_NEAR_TENSOR_MERGED when the blocks are stored complex64, else CUDA cores */
+#define SCD_NEAR_CUDA_CORES     1   /* complex64 FMAs on the CUDA cores */
+#define SCD_NEAR_TENSOR_SPLIT   2   /* tcgen05 MMAs on f16 hi/lo tile planes, 9 MMAs per K step */
+#define SCD_NEAR_TENSOR_MERGED  3   /* the same with x hi/lo merged into one operand, 6 MMAs per K step */
 
 /* near-zone storage precision */
 #define SCD_STORE_C64   32   /* complex64, as the reference stores sp_mat */
@@ -89,7 +108,15 @@ typedef struct scd_solve_opts {
     int32_t precision;    /* SCD_PREC_FP64 or SCD_PREC_MIXED */
     double  inner_tol;    /* mixed: inner complex64 GMRES tolerance */
     int32_t max_outer;    /* mixed: outer refinement steps */
+    int32_t gram_schmidt; /* mixed: SCD_GS_* orthogonalisation of the complex64 inner solves */
 } scd_solve_opts;
+
+/* scd_solve_opts.gram_schmidt.  FP64 solves always use the reference's
+ * modified Gram-Schmidt with its conditional re-orthogonalisation
+ * (src/gmres_module.f90:241-258), so that iteration counts match it. */
+#define SCD_GS_DEFAULT          0   /* SCD_GS_CLASSICAL */
+#define SCD_GS_MODIFIED         1   /* one grid-wide pass per Krylov vector */
+#define SCD_GS_CLASSICAL        2   /* all dots in one pass, then the reference's re-orthogonalisation test */
 
 /* --- context ----------------------------------------------------------- */
 
@@ -161,12 +188,21 @@ SCD_API int scd_matvec(scd_ctx *ctx, const scd_c128 *x, scd_c128 *Ax);
 SCD_API int scd_gmres(scd_ctx *ctx, const scd_c128 *rhs, scd_c128 *x, double tol, int32_t m,
               int32_t cycles, int32_t *iters, double *relres);
 
-/* The column loop of compute_T_matrix (src/T_matrix.f90:254-268): solve
- * A X = mat column by column (in blocks of opts->block right-hand sides) and
- * return Tcols = matᴴ·X.  iters (ncol) receives per-column Arnoldi steps;
- * X (3T, ncol) receives the solutions when non-NULL. */
-SCD_API int scd_solve_columns(scd_ctx *ctx, int32_t ncol, const scd_c128 *mat, scd_c128 *Tcols,
-                      const scd_solve_opts *opts, int32_t *iters, scd_c128 *X);
+/* The incident matrix mat (3T, nmat) of vswf2constant (src/T_matrix.f90:252),
+ * copied to the device once per wavelength and kept there for
+ * scd_solve_columns(mat = NULL) until it is replaced, the context is
+ * destroyed, or scd_compute_T_matrix builds its own columns. */
+SCD_API int scd_set_rhs_matrix(scd_ctx *ctx, int32_t nmat, const scd_c128 *mat);
+
+/* The column loop of compute_T_matrix (src/T_matrix.f90:254-268) over columns
+ * col0+1 .. col0+ncol of mat (3T, nmat): each column is solved (in blocks of
+ * opts->block right-hand sides), and Tcols (nmat, ncol) receives
+ * T_mat(:, col0+j) = matᴴ·x_j with the whole of mat (src/T_matrix.f90:260),
+ * unscaled.  mat is the host array, copied in by this call, or NULL for the
+ * matrix of scd_set_rhs_matrix (nmat must match).  iters (ncol) receives
+ * per-column Arnoldi steps; X (3T, ncol) receives the solutions when non-NULL. */
+SCD_API int scd_solve_columns(scd_ctx *ctx, int32_t nmat, const scd_c128 *mat, int32_t col0, int32_t ncol,
+                              scd_c128 *Tcols, const scd_solve_opts *opts, int32_t *iters, scd_c128 *X);
 
 /* vswf2constant (src/T_matrix.f90:280-305) on the device: mat (3T, 2nm) for
  * the mesh set by scd_set_mesh and the current wavenumber. */
@@ -193,6 +229,8 @@ typedef struct scd_timing {
     int64_t launches;      /* kernels launched since the last reset */
     int64_t matvecs;       /* operator applications since the last reset */
     int64_t arnoldi_steps; /* Arnoldi steps since the last reset */
+    double near_kernel_ms; /* average duration of the main near-zone kernel launch (the last pass of a
+                              matvec: k_near_mma or k_near_groups), scd_profile_matvec */
 } scd_timing;
 SCD_API int scd_get_timing(scd_ctx *ctx, scd_timing *t, int32_t reset);
 
@@ -206,13 +244,18 @@ SCD_API int scd_profile_matvec(scd_ctx *ctx, int32_t reps, int32_t nrhs, int32_t
  * are DEVICE pointers owned by the caller; the kernels run on `stream`
  * (a cudaStream_t, NULL = the legacy default stream) and the call returns
  * after launching them.  No counterpart in the reference: it is for callers
- * that cannot let a library call cudaMalloc (device memory owned by the
- * host's own allocator; column loops recorded into CUDA graphs).  Scratch
- * is a fixed 4 MiB per-device array, so ncol*ncb must not exceed 262144
+ * that cannot let a library call cudaMalloc, such as a Fortran host whose
+ * device memory all comes from its own allocator (CUDA Fortran device
+ * arrays, OpenACC data regions) and must stay under its accounting.  Scratch
+ * is a fixed 4 MiB per-device array, held by every GPU that loads the
+ * library until the process exits, so ncol*ncb must not exceed 262144
  * (SCD_BAD_ARG otherwise).  The first call on a device looks up that array's
- * device address; make it before any stream capture.  All calls share the
- * array: calls that overlap on the GPU race and must be ordered by the
- * caller (one stream, or events). */
+ * device address and keeps it; make it before any stream capture.  The kept
+ * address is not valid after cudaDeviceReset, so do not call this after a
+ * reset in the same process.  An error left pending by an earlier call of
+ * the caller's is returned as SCD_CUDA_ERROR before anything launches, and
+ * left pending.  All calls share the array: calls that overlap on the GPU
+ * race and must be ordered by the caller (one stream, or events). */
 SCD_API int scd_T_assemble_noalloc(const scd_c128 *mat, int64_t n, int32_t ncol, const scd_c128 *X, int32_t ncb,
                                    scd_c128 *T, void *stream);
 

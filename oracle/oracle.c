@@ -1707,6 +1707,16 @@ int orc_gmres(const orc_op *op, const zc *rhs, zc *xout, double tol, int m, int 
     return (error < tol) ? 0 : 1;
 }
 
+/* The orthogonalisation of one Arnoldi step of orc_gmres against i Krylov
+ * vectors (src/gmres_module.f90:241-244): h_k = <v_k, w>, w -= h_k v_k for
+ * k = 1..i, with the same zdot/zaxpy; timed alone by the CPU baseline. */
+void orc_mgs_terms(size_t n, int i, const zc *V, zc *w, zc *h) {
+    for (int k = 0; k < i; ++k) {
+        h[k] = zdot(n, V + n*(size_t)k, w);
+        zaxpy(n, h[k], V + n*(size_t)k, w);
+    }
+}
+
 /* ------------------------------------------------- special functions */
 /* envj / msta1 / msta2, src/sfunctions.f90:81-145 (Zhang & Jin) */
 static double envj(int n, double x) {

@@ -23,6 +23,7 @@
 #define SCADYN_ORACLE_H
 #include <stdint.h>
 #include <complex.h>
+#include <stddef.h>
 
 typedef double _Complex zc;
 typedef float _Complex  fc;
@@ -128,6 +129,7 @@ typedef struct {
 } orc_gmres_info;
 int  orc_gmres(const orc_op *op, const zc *rhs, zc *x, double tol, int m, int cycles,
                orc_gmres_info *info);
+void orc_mgs_terms(size_t n, int i, const zc *V, zc *w, zc *h);   /* one Arnoldi step's MGS over i vectors */
 
 /* incident VSWFs and T assembly (src/T_matrix.f90:240-305, src/mie.f90:408-496) */
 int  orc_calc_MN(int Nmax, zc k, const double Po[3], zc *MM, zc *NN);   /* (3,nm) each */

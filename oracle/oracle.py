@@ -237,6 +237,17 @@ class Operator:
                    "history": hist[: info.history_len].copy()}
 
 
+def mgs_terms(V: np.ndarray, w: np.ndarray) -> np.ndarray:
+    """One Arnoldi step's modified Gram-Schmidt of w (in place) against the
+    rows of V (i, n), as orc_gmres does it; returns the coefficients h."""
+    V = np.ascontiguousarray(V, np.complex128)
+    h = np.zeros(V.shape[0], np.complex128)
+    f = lib().orc_mgs_terms
+    f.argtypes = [C.c_size_t, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    f(V.shape[1], V.shape[0], _p(V), _p(w), _p(h))
+    return h
+
+
 def linear_from_constant(op, seed=0):
     """A linear-basis (order 1) operator on the geometry of a constant-basis
     one, for parity of the order-1 matvec: each tet's projector column is

@@ -27,6 +27,9 @@ SCD_OK, SCD_NOT_CONVERGED, SCD_NAN, SCD_OOM, SCD_BAD_ARG, SCD_TIMEOUT, SCD_CUDA_
 STORE_C64, STORE_C128 = 32, 64
 PREC_FP64, PREC_MIXED = 0, 1
 SCD_M_MAX = 63
+FFT_DEFAULT, FFT_POW2, FFT_SMOOTH = 0, 1, 2
+NEAR_DEFAULT, NEAR_CUDA_CORES, NEAR_TENSOR_SPLIT, NEAR_TENSOR_MERGED = 0, 1, 2, 3
+GS_DEFAULT, GS_MODIFIED, GS_CLASSICAL = 0, 1, 2
 
 _NAMES = {0: "SCD_OK", 1: "SCD_NOT_CONVERGED", 2: "SCD_NAN", 3: "SCD_OOM", 4: "SCD_BAD_ARG",
           5: "SCD_TIMEOUT", 6: "SCD_CUDA_ERROR", 7: "SCD_NOT_READY", 8: "SCD_NO_DEVICE"}
@@ -36,7 +39,7 @@ EXPORTS = [
     "scd_create", "scd_destroy", "scd_last_error", "scd_set_wavenumber", "scd_set_green",
     "scd_set_projectors", "scd_set_nearzone", "scd_grid_from_mesh", "scd_set_mesh",
     "scd_build_projectors", "scd_build_nearzone", "scd_get_projectors", "scd_nearzone_count",
-    "scd_get_nearzone", "scd_matvec", "scd_gmres", "scd_solve_columns", "scd_vswf_rhs",
+    "scd_get_nearzone", "scd_matvec", "scd_gmres", "scd_set_rhs_matrix", "scd_solve_columns", "scd_vswf_rhs",
     "scd_get_timing", "scd_compute_T_matrix", "scd_profile_matvec", "scd_nearzone_bytes",
     "scd_column_latency", "scd_T_assemble_noalloc", "scd_selftest_waits",
 ]
@@ -51,19 +54,21 @@ class ScadynError(RuntimeError):
 class GridDesc(C.Structure):
     _fields_ = [("Nx", C.c_int32), ("Ny", C.c_int32), ("Nz", C.c_int32), ("delta", C.c_double),
                 ("min_coord", C.c_double * 3), ("T", C.c_int32), ("order", C.c_int32),
-                ("M_ex", C.c_int32), ("near_zone", C.c_int32), ("device", C.c_int32)]
+                ("M_ex", C.c_int32), ("near_zone", C.c_int32), ("device", C.c_int32),
+                ("fft_lengths", C.c_int32), ("near_kernel", C.c_int32), ("near_split", C.c_int32)]
 
 
 class SolveOpts(C.Structure):
     _fields_ = [("tol", C.c_double), ("m", C.c_int32), ("cycles", C.c_int32), ("block", C.c_int32),
-                ("precision", C.c_int32), ("inner_tol", C.c_double), ("max_outer", C.c_int32)]
+                ("precision", C.c_int32), ("inner_tol", C.c_double), ("max_outer", C.c_int32),
+                ("gram_schmidt", C.c_int32)]
 
 
 class Timing(C.Structure):
     _fields_ = [("matvec_ms", C.c_double), ("nearzone_ms", C.c_double), ("fft_ms", C.c_double),
                 ("gather_ms", C.c_double), ("arnoldi_ms", C.c_double), ("last_call_ms", C.c_double),
                 ("accum_ms", C.c_double), ("launches", C.c_int64), ("matvecs", C.c_int64),
-                ("arnoldi_steps", C.c_int64)]
+                ("arnoldi_steps", C.c_int64), ("near_kernel_ms", C.c_double)]
 
 
 _lib = None
@@ -95,7 +100,8 @@ def load_library(path: str = LIB_PATH):
         "scd_get_nearzone": ([vp, i64, vp, vp], C.c_int),
         "scd_matvec": ([vp, vp, vp], C.c_int),
         "scd_gmres": ([vp, vp, vp, dbl, i32, i32, C.POINTER(i32), C.POINTER(dbl)], C.c_int),
-        "scd_solve_columns": ([vp, i32, vp, vp, C.POINTER(SolveOpts), vp, vp], C.c_int),
+        "scd_set_rhs_matrix": ([vp, i32, vp], C.c_int),
+        "scd_solve_columns": ([vp, i32, vp, i32, i32, vp, C.POINTER(SolveOpts), vp, vp], C.c_int),
         "scd_vswf_rhs": ([vp, i32, vp], C.c_int),
         "scd_get_timing": ([vp, C.POINTER(Timing), i32], C.c_int),
         "scd_compute_T_matrix": ([vp, i32, C.POINTER(SolveOpts), i32, i32, vp, vp], C.c_int),
@@ -157,19 +163,23 @@ class GridInfo:
 class Solver:
     """One device context (scd_ctx) for one mesh and grid."""
 
-    def __init__(self, Nx, Ny, Nz, delta, min_coord, T, device=0, order=0):
+    def __init__(self, Nx, Ny, Nz, delta, min_coord, T, device=0, order=0, fft_lengths=FFT_DEFAULT,
+                 near_kernel=NEAR_DEFAULT, near_split=0):
         """order 1 (linear basis): 4 projector columns and 12 unknowns per tet.
         The operator comes from the host (set_projectors, set_nearzone with
         12x12 blocks) or from the mesh on the device (set_mesh,
         pfft_projection_lin, compute_near_zone_interactions_lin); compute_Ax2,
         gmres and solve_columns run on it.  The VSWF right-hand sides and the
-        T-matrix entry points are constant-basis only, as in the reference."""
+        T-matrix entry points are constant-basis only, as in the reference.
+        fft_lengths, near_kernel and near_split are the kernel choices of
+        scd_grid_desc (0 = the library's default)."""
         self.lib = load_library()
         d = GridDesc()
         d.Nx, d.Ny, d.Nz, d.delta = Nx, Ny, Nz, delta
         for i in range(3):
             d.min_coord[i] = float(min_coord[i])
         d.T, d.order, d.M_ex, d.near_zone, d.device = T, order, 2, 1, device
+        d.fft_lengths, d.near_kernel, d.near_split = fft_lengths, near_kernel, near_split
         self.desc = d
         self.order = order
         self.T = (4 if order == 1 else 1) * T      # projector columns (basis functions)
@@ -186,7 +196,8 @@ class Solver:
 
     @classmethod
     def from_desc(cls, d: GridDesc, device=0):
-        return cls(d.Nx, d.Ny, d.Nz, d.delta, list(d.min_coord), d.T, device, order=d.order)
+        return cls(d.Nx, d.Ny, d.Nz, d.delta, list(d.min_coord), d.T, device, order=d.order,
+                   fft_lengths=d.fft_lengths, near_kernel=d.near_kernel, near_split=d.near_split)
 
     def _chk(self, rc, what, ok=(SCD_OK,)):
         if rc not in ok:
@@ -294,22 +305,39 @@ class Solver:
         self._chk(self.lib.scd_vswf_rhs(self.ctx, Nmax, _p(mat)), "vswf_rhs")
         return mat
 
-    def solve_columns(self, mat, tol=1e-5, m=50, cycles=4, block=1, precision=PREC_FP64,
-                      inner_tol=1e-3, max_outer=10, want_x=False):
-        """The column loop of compute_T_matrix: returns (T_mat (ncol, ncol)
-        memory of Fortran T_mat(ncol,ncol) i.e. out[c, r] = T(r, c), iters, X)."""
+    def set_rhs_matrix(self, mat):
+        """The incident matrix (vswf2constant, src/T_matrix.f90:252), mat
+        (nmat, n) memory of Fortran mat(n, nmat), kept on the device for
+        solve_columns(None, ...)."""
         mat = _c128(mat)
-        ncol = mat.shape[0]
-        Tc = np.zeros((ncol, ncol), np.complex128)
+        self._nmat = mat.shape[0]
+        self._chk(self.lib.scd_set_rhs_matrix(self.ctx, mat.shape[0], _p(mat)), "set_rhs_matrix")
+
+    def solve_columns(self, mat, col0=0, ncol=None, tol=1e-5, m=50, cycles=4, block=1, precision=PREC_FP64,
+                      inner_tol=1e-3, max_outer=10, gram_schmidt=GS_DEFAULT, want_x=False, nmat=None):
+        """The column loop of compute_T_matrix over columns col0 .. col0+ncol-1
+        of mat (nmat, n) (memory of Fortran mat(n, nmat)), or of the matrix of
+        set_rhs_matrix when mat is None.  Returns (Tc, iters, X, rc): Tc
+        (ncol, nmat) is the memory of Fortran T_mat(nmat, ncol), i.e.
+        Tc[j, r] = T_mat(r, col0+j) = (mat^H x_j)[r] unscaled; X (ncol, n)."""
+        if mat is not None:
+            mat = _c128(mat)
+            nmat = mat.shape[0]
+        elif nmat is None:
+            nmat = self._nmat
+        if ncol is None:
+            ncol = nmat - col0
+        Tc = np.zeros((ncol, nmat), np.complex128)
         iters = np.zeros(ncol, np.int32)
-        X = np.zeros_like(mat) if want_x else None
-        o = SolveOpts(tol, m, cycles, block, precision, inner_tol, max_outer)
-        rc = self._chk(self.lib.scd_solve_columns(self.ctx, ncol, _p(mat), _p(Tc), C.byref(o), _p(iters), _p(X)),
+        X = np.zeros((ncol, self.n), np.complex128) if want_x else None
+        o = SolveOpts(tol, m, cycles, block, precision, inner_tol, max_outer, gram_schmidt)
+        rc = self._chk(self.lib.scd_solve_columns(self.ctx, nmat, _p(mat), col0, ncol, _p(Tc), C.byref(o),
+                                                  _p(iters), _p(X)),
                        "solve_columns", ok=(SCD_OK, SCD_NOT_CONVERGED))
         return Tc, iters, X, rc
 
     def compute_T_matrix(self, Nmax, col0=0, ncol=None, tol=1e-5, m=50, cycles=4, block=1,
-                         precision=PREC_FP64, inner_tol=1e-3, max_outer=10):
+                         precision=PREC_FP64, inner_tol=1e-3, max_outer=10, gram_schmidt=GS_DEFAULT):
         """compute_T_matrix (src/T_matrix.f90:240-277) on device-resident data:
         returns (T (2nm, ncol) with T[:, j] the scaled T column col0+j, iters).
         With all columns, T = [[Taa, Tab], [Tba, Tbb]]."""
@@ -318,7 +346,7 @@ class Solver:
             ncol = 2 * nm - col0
         Tf = np.zeros((ncol, 2 * nm), np.complex128)       # memory of Fortran T(2nm, ncol)
         iters = np.zeros(ncol, np.int32)
-        o = SolveOpts(tol, m, cycles, block, precision, inner_tol, max_outer)
+        o = SolveOpts(tol, m, cycles, block, precision, inner_tol, max_outer, gram_schmidt)
         self._chk(self.lib.scd_compute_T_matrix(self.ctx, Nmax, C.byref(o), col0, ncol, _p(Tf), _p(iters)),
                   "compute_T_matrix", ok=(SCD_OK, SCD_NOT_CONVERGED))
         return Tf.T, iters

@@ -120,6 +120,8 @@ static int set_order(scd_ctx *c, const std::vector<int> &cube_of_tet) {
             c->have_proj = false;
             c->have_near = false;
             c->nzm_ready = false;
+            c->mat_cols = 0;
+            c->mat_Nmax = -1;
         } else {
             return SCD_OK;
         }
@@ -377,24 +379,22 @@ int scd_create(scd_ctx **out, const scd_grid_desc *d) {
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return SCD_NO_DEVICE; }
     if (d->device < 0 || d->device >= ndev) return SCD_BAD_ARG;
+    if (d->fft_lengths < SCD_FFT_DEFAULT || d->fft_lengths > SCD_FFT_SMOOTH) return SCD_BAD_ARG;
+    if (d->near_kernel < SCD_NEAR_DEFAULT || d->near_kernel > SCD_NEAR_TENSOR_MERGED) return SCD_BAD_ARG;
+    if (d->near_split < 0 || d->near_split > 2) return SCD_BAD_ARG;
     scd_ctx *c = new scd_ctx();
     c->d = *d;
     c->dev = d->device;
-    {
-        const char *e = getenv("SCADYN_NEAR_MMA");
-        c->nzm_on = e && (e[0] == '1' || e[0] == '2');
-        c->nzm_sched = (e && e[0] == '2') ? 1 : 0;
-        e = getenv("SCADYN_CGS");
-        c->cgs_on = e && e[0] == '1';
-        e = getenv("SCADYN_NEAR_SPLIT");
-        c->near_split = (e && e[0] == '2') ? 2 : 1;
-    }
+    // kernel choices: the tensor-core near zone applies to complex64 storage
+    // only (checked when the near zone is set); 0 selects the defaults
+    c->nzm_on = d->near_kernel != SCD_NEAR_CUDA_CORES;
+    c->nzm_sched = d->near_kernel == SCD_NEAR_TENSOR_SPLIT ? 0 : 1;
+    c->near_split = d->near_split == 2 ? 2 : 1;
     cudaSetDevice(c->dev);
     cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev);
     c->Nx = d->Nx; c->Ny = d->Ny; c->Nz = d->Nz;
     {
-        const char *e = getenv("SCADYN_FFT_SMOOTH");
-        const bool smooth = e && e[0] == '1';
+        const bool smooth = d->fft_lengths != SCD_FFT_POW2;
         c->Px = fft_len(2 * d->Nx, smooth); c->Py = fft_len(2 * d->Ny, smooth); c->Pz = fft_len(2 * d->Nz, smooth);
     }
     if (c->Px > 512 || c->Py > 512 || c->Pz > 512) {
@@ -604,24 +604,73 @@ int scd_gmres(scd_ctx *c, const scd_c128 *rhs, scd_c128 *x, double tol, int32_t 
     return rc;
 }
 
-int scd_solve_columns(scd_ctx *c, int32_t ncol, const scd_c128 *mat, scd_c128 *Tcols, const scd_solve_opts *o,
-                      int32_t *iters, scd_c128 *X) {
-    if (!c || ncol <= 0 || !mat || !Tcols || !o) return SCD_BAD_ARG;
+// the incident matrix mat (3T, nmat) on the device, slot-ordered, in c->d_mat
+// (mat_Nmax = 0 marks a host-supplied matrix; scd_compute_T_matrix builds its
+// own columns over it)
+static int upload_rhs_matrix(scd_ctx *c, int nmat, const scd_c128 *mat) {
+    const long long n = c->n;
+    int rc;
+    if (!c->d_mat || c->mat_cols != nmat || c->mat_Nmax != 0) {
+        cudaFree(c->d_mat);
+        c->d_mat = nullptr;
+        c->mat_cols = 0;
+        if ((rc = dalloc(c, &c->d_mat, (size_t)n * nmat, "incident matrix"))) return rc;
+    }
+    c->mat_Nmax = 0;
+    c->mat_k = 0.0;
+    for (int col = 0; col < nmat; ++col) {
+        CK(cudaMemcpyAsync(c->d_io, mat + (size_t)n * col, sizeof(cd) * n, cudaMemcpyHostToDevice, c->st), "mat");
+        launch_permute_in(c, c->d_io, c->d_mat + (size_t)n * col, 1, n);
+    }
+    c->mat_cols = nmat;
+    return SCD_OK;
+}
+
+static int check_opts(scd_ctx *c, const scd_solve_opts *o) {
+    if (o->m < 1 || o->m > SCD_M_MAX || o->cycles < 1 || !(o->tol > 0) || o->block < 0)
+        return set_error(c, SCD_BAD_ARG, "solve options: m %d (1..%d), cycles %d, tol %g, block %d", o->m, SCD_M_MAX,
+                         o->cycles, o->tol, o->block);
+    if (o->precision != SCD_PREC_FP64 && o->precision != SCD_PREC_MIXED)
+        return set_error(c, SCD_BAD_ARG, "precision %d", o->precision);
+    if (o->gram_schmidt < SCD_GS_DEFAULT || o->gram_schmidt > SCD_GS_CLASSICAL)
+        return set_error(c, SCD_BAD_ARG, "gram_schmidt %d", o->gram_schmidt);
+    if (o->precision == SCD_PREC_MIXED && (!(o->inner_tol > 0) || o->max_outer < 1))
+        return set_error(c, SCD_BAD_ARG, "mixed form: inner_tol %g, max_outer %d", o->inner_tol, o->max_outer);
+    c->cgs_on = o->gram_schmidt != SCD_GS_MODIFIED;
+    return SCD_OK;
+}
+
+int scd_set_rhs_matrix(scd_ctx *c, int32_t nmat, const scd_c128 *mat) {
+    if (!c || nmat <= 0 || !mat) return SCD_BAD_ARG;
     cudaSetDevice(c->dev);
+    if (!c->have_order) return set_error(c, SCD_NOT_READY, "scd_set_rhs_matrix needs the projectors or the mesh first");
+    int rc = ensure_work(c, 1);
+    if (rc) return rc;
+    if ((rc = upload_rhs_matrix(c, nmat, mat))) return rc;
+    return check_cuda(c, cudaStreamSynchronize(c->st), "incident matrix");
+}
+
+int scd_solve_columns(scd_ctx *c, int32_t nmat, const scd_c128 *mat, int32_t col0, int32_t ncol, scd_c128 *Tcols,
+                      const scd_solve_opts *o, int32_t *iters, scd_c128 *X) {
+    if (!c || nmat <= 0 || ncol <= 0 || !Tcols || !o) return SCD_BAD_ARG;
+    cudaSetDevice(c->dev);
+    if (col0 < 0 || col0 + ncol > nmat)
+        return set_error(c, SCD_BAD_ARG, "columns %d..%d outside 1..%d", col0 + 1, col0 + ncol, nmat);
     int rc = ready(c);
     if (rc) return rc;
+    if ((rc = check_opts(c, o))) return rc;
     const long long n = c->n;
-    cd *d_mat = nullptr, *d_X = nullptr, *d_T = nullptr;
-    if ((rc = dalloc(c, &d_mat, (size_t)n * ncol, "mat"))) return rc;
-    if ((rc = dalloc(c, &d_X, (size_t)n * ncol, "X"))) { cudaFree(d_mat); return rc; }
-    if ((rc = dalloc(c, &d_T, (size_t)ncol * ncol, "T"))) { cudaFree(d_mat); cudaFree(d_X); return rc; }
     cudaEventRecord(c->ev[4], c->st);
-    for (int col = 0; col < ncol; ++col) {
-        CK(cudaMemcpyAsync(c->d_io, mat + (size_t)n * col, sizeof(cd) * n, cudaMemcpyHostToDevice, c->st), "mat");
-        launch_permute_in(c, c->d_io, d_mat + (size_t)n * col, 1, n);
+    if (mat) {
+        if ((rc = upload_rhs_matrix(c, nmat, mat))) return rc;
+    } else if (!c->d_mat || c->mat_Nmax != 0 || c->mat_cols != nmat) {
+        return set_error(c, SCD_NOT_READY, "mat is NULL and no incident matrix of %d columns was set", nmat);
     }
+    cd *d_X = nullptr, *d_T = nullptr;
+    if ((rc = dalloc(c, &d_X, (size_t)n * ncol, "X"))) return rc;
+    if ((rc = dalloc(c, &d_T, (size_t)nmat * ncol, "T"))) { cudaFree(d_X); return rc; }
     std::vector<const cd *> cols(ncol);
-    for (int j = 0; j < ncol; ++j) cols[j] = d_mat + (size_t)n * j;
+    for (int j = 0; j < ncol; ++j) cols[j] = c->d_mat + (size_t)n * (col0 + j);
     const int ns = o->block > 0 ? o->block : ncol;
     std::vector<int> it(ncol, 0);
     int worst = batch_solve(c, ncol, cols.data(), d_X, o->tol, o->m, o->cycles, ns, it.data(), nullptr, nullptr,
@@ -632,8 +681,9 @@ int scd_solve_columns(scd_ctx *c, int32_t ncol, const scd_c128 *mat, scd_c128 *T
     }
     if (iters) for (int j = 0; j < ncol; ++j) iters[j] = it[j];
     if (worst == SCD_OK || worst == SCD_NOT_CONVERGED) {
-        launch_T_assemble(c, d_mat, ncol, 0, ncol, d_X, d_T);
-        rc = check_cuda(c, cudaMemcpyAsync(Tcols, d_T, sizeof(cd) * ncol * ncol, cudaMemcpyDeviceToHost, c->st), "T");
+        // T_mat(:, col0+j) = mat^H x_j over all nmat rows (src/T_matrix.f90:260)
+        launch_T_assemble(c, c->d_mat, nmat, 0, ncol, d_X, d_T);
+        rc = check_cuda(c, cudaMemcpyAsync(Tcols, d_T, sizeof(cd) * (size_t)nmat * ncol, cudaMemcpyDeviceToHost, c->st), "T");
         if (!rc && X) {
             for (int col = 0; col < ncol && !rc; ++col) {
                 launch_permute_out(c, d_X + (size_t)n * col, c->d_io, 1, n);
@@ -651,7 +701,7 @@ int scd_solve_columns(scd_ctx *c, int32_t ncol, const scd_c128 *mat, scd_c128 *T
         }
     }
     cudaStreamSynchronize(c->st);
-    cudaFree(d_mat); cudaFree(d_X); cudaFree(d_T);
+    cudaFree(d_X); cudaFree(d_T);
     return worst;
 }
 
@@ -667,6 +717,7 @@ int scd_get_timing(scd_ctx *c, scd_timing *t, int32_t reset) {
     t->launches = c->launches;
     t->matvecs = c->n_matvec;
     t->arnoldi_steps = c->n_arn;
+    t->near_kernel_ms = c->t_near_k;
     if (reset) {
         c->accum_ms = 0;
         c->launches = 0;
@@ -702,7 +753,7 @@ int scd_profile_matvec(scd_ctx *c, int32_t reps, int32_t nrhs, int32_t precision
         if (mixed) rc = check_cuda(c, cudaMemcpy(fx + (size_t)r * c->n, hf.data(), sizeof(cf) * c->n, cudaMemcpyHostToDevice), "profile x");
         else rc = check_cuda(c, cudaMemcpy(c->d_x + (size_t)r * c->n, h.data(), sizeof(cd) * c->n, cudaMemcpyHostToDevice), "profile x");
     }
-    double sn = 0, sf = 0, sg = 0, st = 0;
+    double sn = 0, sf = 0, sg = 0, st = 0, sk = 0;
     c->timing = true;
     for (int r = 0; r < reps + 1 && !rc; ++r) {
         if (mixed) run_matvec(c, fx, fy, nrhs, nullptr);
@@ -713,8 +764,10 @@ int scd_profile_matvec(scd_ctx *c, int32_t reps, int32_t nrhs, int32_t precision
         cudaEventElapsedTime(&b, c->ev[1], c->ev[2]);
         cudaEventElapsedTime(&g, c->ev[2], c->ev[3]);
         cudaEventElapsedTime(&t, c->ev[0], c->ev[3]);
+        float k = 0;
+        cudaEventElapsedTime(&k, c->ev[6], c->ev[7]);
         if (r == 0) continue;   // warm-up
-        sn += a; sf += b; sg += g; st += t;
+        sn += a; sf += b; sg += g; st += t; sk += k;
     }
     c->timing = false;
     if (fx) cudaFree(fx);
@@ -724,6 +777,7 @@ int scd_profile_matvec(scd_ctx *c, int32_t reps, int32_t nrhs, int32_t precision
     c->t_fft = sf / reps;
     c->t_gather = sg / reps;
     c->t_matvec = st / reps;
+    c->t_near_k = sk / reps;
     if ((rc = near_status(c))) return rc;
     return check_cuda(c, cudaGetLastError(), "profile");
 }
@@ -750,6 +804,7 @@ int scd_compute_T_matrix(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int3
     if (c->nb != 1) return set_error(c, SCD_BAD_ARG, "scd_compute_T_matrix: constant basis only");
     int rc = ready(c);
     if (rc) return rc;
+    if ((rc = check_opts(c, o))) return rc;
     const int nm = (Nmax + 1) * (Nmax + 1) - 1, ntot = 2 * nm;
     if (col0 < 0 || ncol < 1 || col0 + ncol > ntot)
         return set_error(c, SCD_BAD_ARG, "columns %d..%d outside 1..%d", col0 + 1, col0 + ncol, ntot);
@@ -757,10 +812,13 @@ int scd_compute_T_matrix(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int3
     if (!c->d_mat || c->mat_Nmax != Nmax || c->mat_k != c->k) {
         cudaFree(c->d_mat);
         c->d_mat = nullptr;
+        c->mat_cols = 0;
+        c->mat_Nmax = -1;
         if ((rc = dalloc(c, &c->d_mat, (size_t)n * ntot, "resident VSWF columns"))) return rc;
         if ((rc = setup_vswf(c, Nmax, c->d_mat))) return rc;
         c->mat_Nmax = Nmax;
         c->mat_k = c->k;
+        c->mat_cols = ntot;
     }
     cd *d_X = nullptr, *d_T = nullptr;
     if ((rc = dalloc(c, &d_X, (size_t)n * ncol, "X"))) return rc;

@@ -101,7 +101,7 @@ struct scd_ctx {
     long long tile_store = 0;            // stored elements (tile_elems summed)
     long long max_tile_store = 0;        // largest tile_elems
     long long B_ref = 0;                 // blocks in the reference layout
-    int near_split = 1;                  // partial sums per near-zone row/column sum (SCADYN_NEAR_SPLIT=2)
+    int near_split = 1;                  // partial sums per near-zone row/column sum (scd_grid_desc.near_split)
     int near_cfg_err = 0;                // a near-zone launch was skipped: a tile outgrew the shared-memory ring
     // partial-sum slots per group: slot 0 holds the group's row sums over
     // all its tiles, slots 1.. the M^T x products of the tiles (g', g),
@@ -142,7 +142,7 @@ struct scd_ctx {
 
     // timing
     cudaEvent_t ev[8] = {};
-    double t_matvec = 0, t_near = 0, t_fft = 0, t_gather = 0, t_arn = 0;
+    double t_matvec = 0, t_near = 0, t_fft = 0, t_gather = 0, t_arn = 0, t_near_k = 0;
     double last_call_ms = 0, accum_ms = 0;
     long long n_matvec = 0, n_arn = 0, launches = 0;
     bool timing = false;
@@ -153,13 +153,13 @@ struct scd_ctx {
     cf *f_bpart = nullptr, *f_W = nullptr, *f_R = nullptr, *f_nzpart = nullptr, *f_xT = nullptr;
     int f_cap = 0;
 
-    // classical Gram-Schmidt for the complex64 inner solves (batch.cu), opt-in
-    // by SCADYN_CGS=1 at context creation
+    // classical Gram-Schmidt for the complex64 inner solves of the current
+    // solve (batch.cu; scd_solve_opts.gram_schmidt)
     bool cgs_on = false;
-    // tensor-core near zone of the complex64 matvec (near_mma.cu), opt-in by
-    // SCADYN_NEAR_MMA=1 (or =2) at context creation
+    // tensor-core near zone of the complex64 matvec (near_mma.cu;
+    // scd_grid_desc.near_kernel, fixed at context creation)
     bool nzm_on = false, nzm_ready = false;
-    int nzm_sched = 0;                   // instruction schedule (near_mma.cuh): 0 split, 1 merged (SCADYN_NEAR_MMA=2)
+    int nzm_sched = 1;                   // instruction schedule (near_mma.cuh): 0 split, 1 merged
     unsigned char *d_t16 = nullptr;      // f16 hi/lo planes of every tile
     long long *d_t16_off = nullptr;      // per tile byte offset
     unsigned char *d_xb = nullptr;       // x blocks of one pass
@@ -172,9 +172,12 @@ struct scd_ctx {
     void *batch = nullptr;               // batch-solver buffers (batch.cu)
     std::vector<double> col_latency_ms;  // admission -> completion, last batch solve
 
-    // resident right-hand sides (vswf2constant for mat_Nmax, mat_k)
+    // resident incident matrix (3T, mat_cols), slot order: vswf2constant
+    // built on the device for (mat_Nmax, mat_k), or the host's matrix
+    // (mat_Nmax = 0, scd_set_rhs_matrix / scd_solve_columns); -1 = stale
     cd *d_mat = nullptr;
-    int mat_Nmax = 0;
+    int mat_cols = 0;
+    int mat_Nmax = -1;
     double mat_k = 0.0;
 
     std::string err;

@@ -44,11 +44,12 @@ __global__ void k_permute_out(const cd *__restrict__ xs, cd *__restrict__ xo, co
 }
 
 // ---------------------------------------------------------------- scatter
-// Anterpolation (sparse_T_matmul, src/sparse.f90:13-43), one warp per cube:
-// lane j < 27 accumulates the four box-node sums of node j over the cube's
-// tets, for a group of right-hand sides at a time (projector values are read
-// once per group).  Projectors are stored P[(g*27 + j)*T + slot].
-// bpart[((r*ncubes + c)*4 + g)*27 + j].
+// Anterpolation (sparse_T_matmul, src/sparse.f90:13-43), one warp per
+// (cube, group of SC_RG right-hand sides): lane j < 27 accumulates the four
+// box-node sums of node j over the cube's tets (projector values are read
+// once per group; the groups of right-hand sides are the grid's y index, so
+// every cube has nrhs/SC_RG warps in flight).  Projectors are stored
+// P[(g*27 + j)*T + slot].  bpart[((r*ncubes + c)*4 + g)*27 + j].
 template <typename C, int SC_RG>
 __global__ void __launch_bounds__(32 * WARPS_PER_CTA)
 k_scatter(const C *__restrict__ x, long long ld, const C *__restrict__ P, int T,
@@ -59,7 +60,8 @@ k_scatter(const C *__restrict__ x, long long ld, const C *__restrict__ P, int T,
     const int s0 = cube_off[c], s1 = cube_off[c + 1];
     const C *P0 = P + (size_t)lane * T, *PX = P + (size_t)(27 + lane) * T;
     const C *PY = P + (size_t)(54 + lane) * T, *PZ = P + (size_t)(81 + lane) * T;
-    for (int r0 = 0; r0 < nrhs; r0 += SC_RG) {
+    {
+        const int r0 = blockIdx.y * SC_RG;
         C acc[SC_RG][4];
 #pragma unroll
         for (int q = 0; q < SC_RG; ++q) acc[q][0] = acc[q][1] = acc[q][2] = acc[q][3] = czero<C>();
@@ -753,12 +755,14 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS, NZ_MIN_CTAS<U>) k_near_groups(
 
 // ---------------------------------------------------------------- gather
 // Interpolation (sparse_eps_matmul, src/sparse.f90:47-77) and final
-// assembly (src/gmres_module.f90:148-170), one warp per near-zone group, one
-// lane per tet: the 27 box-node values of the four result grids are staged
-// in shared memory for a group of right-hand sides, each lane forms its
-// tet's six 27-term sums from the projector rows P[(g*27 + j)*T + slot]
-// (coalesced across lanes), adds the group's near-zone partial slots in slot
-// order and writes Ax = near + (Y2 - k^2 Y).
+// assembly (src/gmres_module.f90:148-170), one warp per (near-zone group,
+// group of GA_RG right-hand sides), one lane per tet: the 27 box-node values
+// of the four result grids are staged in shared memory for the warp's
+// right-hand sides, each lane forms its tet's six 27-term sums from the
+// projector rows P[(g*27 + j)*T + slot] (coalesced across lanes), adds the
+// group's near-zone partial slots in slot order and writes
+// Ax = near + (Y2 - k^2 Y).  The groups of right-hand sides are the grid's y
+// index, so a near-zone group has nrhs/GA_RG warps in flight.
 template <typename C, int GA_RG>
 __global__ void __launch_bounds__(32 * WARPS_PER_CTA)
 k_gather(const C *__restrict__ Rg, const C *__restrict__ P, int T, const int *__restrict__ grp_off,
@@ -781,7 +785,8 @@ k_gather(const C *__restrict__ Rg, const C *__restrict__ P, int T, const int *__
         const int a = lane % 3, b = (lane / 3) % 3, cc = lane / 9;
         node = ((long long)(2 * bz + cc) * G.Ny + (2 * by + b)) * G.Nx + (2 * bx + a);
     }
-    for (int r0 = 0; r0 < nrhs; r0 += GA_RG) {
+    {
+        const int r0 = blockIdx.y * GA_RG;
         __syncwarp();
         if (lane < 27) {
 #pragma unroll
@@ -926,17 +931,17 @@ template <typename C>
 void fft_chain_t(scd_ctx *c, const C *x, int nrhs, const int *done) {
     const GridDims G = dims_of(c);
     {
-        dim3 grid((c->ncubes + WARPS_PER_CTA - 1) / WARPS_PER_CTA);
+        const unsigned gx = (unsigned)((c->ncubes + WARPS_PER_CTA - 1) / WARPS_PER_CTA);
         const C *P = Res<C>::P(c);
         if (nrhs >= 8)
-            k_scatter<C, 8><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(x, c->n, P, c->T, c->d_cube_off, c->ncubes,
-                                                                    Res<C>::bpart(c), done, nrhs);
+            k_scatter<C, 8><<<dim3(gx, (nrhs + 7) / 8), 32 * WARPS_PER_CTA, 0, c->st>>>(
+                x, c->n, P, c->T, c->d_cube_off, c->ncubes, Res<C>::bpart(c), done, nrhs);
         else if (nrhs >= 4)
-            k_scatter<C, 4><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(x, c->n, P, c->T, c->d_cube_off, c->ncubes,
-                                                                    Res<C>::bpart(c), done, nrhs);
+            k_scatter<C, 4><<<dim3(gx, (nrhs + 3) / 4), 32 * WARPS_PER_CTA, 0, c->st>>>(
+                x, c->n, P, c->T, c->d_cube_off, c->ncubes, Res<C>::bpart(c), done, nrhs);
         else
-            k_scatter<C, 1><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(x, c->n, P, c->T, c->d_cube_off, c->ncubes,
-                                                                    Res<C>::bpart(c), done, nrhs);
+            k_scatter<C, 1><<<dim3(gx, nrhs), 32 * WARPS_PER_CTA, 0, c->st>>>(
+                x, c->n, P, c->T, c->d_cube_off, c->ncubes, Res<C>::bpart(c), done, nrhs);
     }
     const int nrg = 4 * nrhs;
 #define XF(PP) fft_x_fwd_t<PP, C>(c, G, nrg, done, Res<C>::tw(c, 0))
@@ -990,12 +995,14 @@ void near_launch(scd_ctx *c, const ST *data, const C *x, int nrhs, const int *do
     }
     const size_t sh = NZ_META + a.x1_bytes + a.ring_bytes;
     cudaFuncSetAttribute(k_near_groups<ST, C, U, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+    if (c->timing) cudaEventRecord(c->ev[6], c->st);
     k_near_groups<ST, C, U, NS><<<c->ngroups, 2 * a.half + 32, sh, c->st>>>(a);
+    if (c->timing) cudaEventRecord(c->ev[7], c->st);
 }
 
 template <typename ST, typename C>
 void near_dispatch(scd_ctx *c, const ST *data, const C *x, int nrhs, const int *done) {
-    // SCADYN_NEAR_SPLIT=2: two partial sums per row and column (two lanes each
+    // near_split 2: two partial sums per row and column (two lanes each
     // at one right-hand side) for the FP64 matvec; the complex64 matvec of the
     // mixed form keeps one sum per lane (its U = 4 kernel would lose occupancy
     // to the second set of accumulators)
@@ -1025,17 +1032,17 @@ void near_t(scd_ctx *c, const C *x, int nrhs, const int *done) {
 template <typename C>
 void gather_t(scd_ctx *c, C *y, int nrhs, const int *done) {
     const GridDims G = dims_of(c);
-    dim3 grid((c->ngroups + WARPS_PER_CTA - 1) / WARPS_PER_CTA);
+    const unsigned gx = (unsigned)((c->ngroups + WARPS_PER_CTA - 1) / WARPS_PER_CTA);
     if (c->ngroups == 0) return;
     typedef typename CReal<C>::type R;
     const R k2 = (R)(c->k * c->k);
     if (nrhs >= 4)
-        k_gather<C, 4><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(Res<C>::R(c), Res<C>::P(c), c->T, c->d_grp_off,
+        k_gather<C, 4><<<dim3(gx, (nrhs + 3) / 4), 32 * WARPS_PER_CTA, 0, c->st>>>(Res<C>::R(c), Res<C>::P(c), c->T, c->d_grp_off,
                                                                c->d_grp_cube, c->ngroups, G, k2, Res<C>::part(c),
                                                                c->part_len, c->d_pslot_base, c->d_pslot_cnt, y, c->n,
                                                                done, nrhs);
     else
-        k_gather<C, 1><<<grid, 32 * WARPS_PER_CTA, 0, c->st>>>(Res<C>::R(c), Res<C>::P(c), c->T, c->d_grp_off,
+        k_gather<C, 1><<<dim3(gx, nrhs), 32 * WARPS_PER_CTA, 0, c->st>>>(Res<C>::R(c), Res<C>::P(c), c->T, c->d_grp_off,
                                                                c->d_grp_cube, c->ngroups, G, k2, Res<C>::part(c),
                                                                c->part_len, c->d_pslot_base, c->d_pslot_cnt, y, c->n,
                                                                done, nrhs);
@@ -1075,7 +1082,11 @@ int build_twiddles(scd_ctx *c, int P, cd **out) {
 // complex64 copies of the projectors, the Green octant and the twiddles for
 // the mixed-precision inner solves (rounded from the FP64 operator)
 int ensure_single(scd_ctx *c) {
-    if (c->nzm_on && !c->nzm_ready && c->have_near && c->ngroups > 0) {
+    // the tensor-core near zone reads complex64 tiles; by default a context
+    // with complex128 storage keeps the CUDA-core kernel, an explicit request
+    // is an error (near_mma_prepare)
+    if (c->nzm_on && !c->nzm_ready && c->have_near && c->ngroups > 0 &&
+        (c->near_prec == SCD_STORE_C64 || c->d.near_kernel != SCD_NEAR_DEFAULT)) {
         const int rc = near_mma_prepare(c);
         if (rc) return rc;
     }

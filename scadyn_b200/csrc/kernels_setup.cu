@@ -152,10 +152,10 @@ void launch_T_assemble(scd_ctx *c, const cd *d_mat, int ncol, int col0, int ncb,
 // scd_T_assemble_noalloc: the same split-K assembly T = mat^H X for callers
 // that must not allocate device memory -- e.g. a Fortran host whose device
 // arrays all come from its own allocator (CUDA Fortran `device` arrays,
-// OpenACC data regions) and which may record the column loop into a CUDA
-// graph, where a cudaMalloc inside the library would break the capture or
-// synchronise the device.  The split-K partial sums live in this fixed
-// file-scope array instead of a cudaMallocAsync buffer.
+// OpenACC data regions), where a cudaMalloc inside the library would hold
+// memory outside that allocator's accounting and synchronise the device.
+// The split-K partial sums live in this fixed file-scope array instead of a
+// cudaMallocAsync buffer.
 #define SCD_NOALLOC_SCRATCH (1 << 18)   // complex doubles: 4 MiB per device
 static __device__ __align__(256) cd g_noalloc_scratch[SCD_NOALLOC_SCRATCH];
 
@@ -178,6 +178,9 @@ extern "C" SCD_API int scd_T_assemble_noalloc(const scd_c128 *mat, int64_t n, in
         }
         g_noalloc_ptr[dev] = p;
     }
+    // an error left pending by an earlier call of the caller's is not this
+    // call's: report it without launching and leave it for the caller to read
+    if (cudaPeekAtLastError() != cudaSuccess) return SCD_CUDA_ERROR;
     cd *part = g_noalloc_ptr[dev];
     cudaStream_t st = (cudaStream_t)stream;
     // as many K splits as the scratch holds (at most 64); every partial entry
@@ -188,6 +191,14 @@ extern "C" SCD_API int scd_T_assemble_noalloc(const scd_c128 *mat, int64_t n, in
     nsplit = (int)((n + kchunk - 1) / kchunk);
     dim3 grid(nsplit, (ncol + TB - 1) / TB, (ncb + TB - 1) / TB);
     k_tgemm_partial<<<grid, dim3(TB, TB), 0, st>>>((const cd *)mat, n, ncol, (const cd *)X, ncb, kchunk, part);
+    if (cudaPeekAtLastError() != cudaSuccess) {
+        cudaGetLastError();   // this launch's own error
+        return SCD_CUDA_ERROR;
+    }
     k_tgemm_reduce<<<(ncol * ncb + 255) / 256, 256, 0, st>>>(part, nsplit, ncol, ncb, (cd *)T, 0);
-    return cudaGetLastError() == cudaSuccess ? SCD_OK : SCD_CUDA_ERROR;
+    if (cudaPeekAtLastError() != cudaSuccess) {
+        cudaGetLastError();
+        return SCD_CUDA_ERROR;
+    }
+    return SCD_OK;
 }

@@ -7,9 +7,10 @@
 // to partial slot 0, and each tile (g, g2), g2 != g, writes A^T x(g) to its
 // partial slot of g2; k_gather adds the slots in a fixed order.
 //
-// Opt-in (environment SCADYN_NEAR_MMA=1 for the split instruction schedule,
-// =2 for the merged one, when the context is created) for complex64
-// near-zone storage; the CUDA-core kernel stays the default.
+// The default near zone of the complex64 matvec when the blocks are stored
+// complex64 (scd_grid_desc.near_kernel: SCD_NEAR_TENSOR_MERGED, or
+// SCD_NEAR_TENSOR_SPLIT for the split instruction schedule; SCD_NEAR_CUDA_CORES
+// selects k_near_groups instead).
 #include <cuda_fp16.h>
 
 #include <cmath>
@@ -444,7 +445,9 @@ static void near_mma_run_s(scd_ctx *c, const cf *x, int nrhs, const int *done) {
         a.t16 = c->d_t16; a.t16_off = c->d_t16_off; a.xb = c->d_xb; a.xb_off = c->d_xb_off;
         a.part = c->f_nzpart; a.part_len = c->part_len; a.skip = done; a.r0 = r0; a.rg = rg; a.xinv = c->d_xinv;
         a.x1_bytes = c->nzm_x1; a.ring_bytes = c->nzm_ring; a.slack_bytes = c->nzm_slack; a.err = c->d_kerr;
+        if (c->timing) cudaEventRecord(c->ev[6], c->st);
         k_near_mma<S><<<c->ngroups, NZM_THREADS, sh, c->st>>>(a);
+        if (c->timing) cudaEventRecord(c->ev[7], c->st);
         c->launches += 3;
     }
 }

@@ -63,14 +63,11 @@ int64_t estimate(const scd_request *r, const scd_grid_desc &d) {
     b += ns * n * (4.0 * es + 6.0 * 16.0 + (mixed ? 4.0 * 16.0 : 0.0));           // solver and work vectors
     b += n * ncol * 16.0;                                                         // incident columns
     b += 12.0 * T * 8.0 + T * 16.0;                                               // mesh on the device
-    {
-        // opt-in tensor-core near zone (mixed form, complex64 storage): f16
-        // hi/lo planes of every tile (8 B per complex plus padding) and a
-        // pass of x blocks
-        const char *e = getenv("SCADYN_NEAR_MMA");
-        if (e && (e[0] == '1' || e[0] == '2') && mixed && r->storage_prec != SCD_STORE_C128)
-            b += T * 250.0 * 9.0 * 8.0 * 1.3 + n * 128.0 * 1.3;   // x block: 32 rows x 2 B x hi/lo per unknown
-    }
+    // tensor-core near zone (the default of the mixed form with complex64
+    // storage): f16 hi/lo planes of every tile (8 B per complex plus
+    // padding) and a pass of x blocks
+    if (d.near_kernel != SCD_NEAR_CUDA_CORES && mixed && r->storage_prec != SCD_STORE_C128)
+        b += T * 250.0 * 9.0 * 8.0 * 1.3 + n * 128.0 * 1.3;   // x block: 32 rows x 2 B x hi/lo per unknown
     return (int64_t)(b * 1.1) + (64LL << 20);
 }
 

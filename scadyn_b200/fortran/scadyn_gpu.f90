@@ -15,6 +15,11 @@ module scadyn_gpu
    integer(c_int), parameter, public :: SCD_STORE_C64 = 32, SCD_STORE_C128 = 64
    integer(c_int), parameter, public :: SCD_PREC_FP64 = 0, SCD_PREC_MIXED = 1
    integer(c_int), parameter, public :: SCD_M_MAX = 63
+   ! kernel choices (0 = the library's default)
+   integer(c_int), parameter, public :: SCD_FFT_DEFAULT = 0, SCD_FFT_POW2 = 1, SCD_FFT_SMOOTH = 2
+   integer(c_int), parameter, public :: SCD_NEAR_DEFAULT = 0, SCD_NEAR_CUDA_CORES = 1, &
+                                        SCD_NEAR_TENSOR_SPLIT = 2, SCD_NEAR_TENSOR_MERGED = 3
+   integer(c_int), parameter, public :: SCD_GS_DEFAULT = 0, SCD_GS_MODIFIED = 1, SCD_GS_CLASSICAL = 2
 
    type, bind(C), public :: scd_grid_desc
       integer(c_int32_t) :: Nx, Ny, Nz
@@ -25,6 +30,9 @@ module scadyn_gpu
       integer(c_int32_t) :: M_ex = 2
       integer(c_int32_t) :: near_zone = 1
       integer(c_int32_t) :: device = 0
+      integer(c_int32_t) :: fft_lengths = 0
+      integer(c_int32_t) :: near_kernel = 0
+      integer(c_int32_t) :: near_split = 0
    end type
 
    type, bind(C), public :: scd_solve_opts
@@ -35,6 +43,7 @@ module scadyn_gpu
       integer(c_int32_t) :: precision = 0
       real(c_double)     :: inner_tol = 1d-4
       integer(c_int32_t) :: max_outer = 10
+      integer(c_int32_t) :: gram_schmidt = 0
    end type
 
    ! device timing block (scd_get_timing), milliseconds
@@ -42,6 +51,7 @@ module scadyn_gpu
       real(c_double)     :: matvec_ms, nearzone_ms, fft_ms, gather_ms, arnoldi_ms
       real(c_double)     :: last_call_ms, accum_ms
       integer(c_int64_t) :: launches, matvecs, arnoldi_steps
+      real(c_double)     :: near_kernel_ms
    end type
 
    ! request server (include/scadyn_server.h)
@@ -71,7 +81,7 @@ module scadyn_gpu
    public :: scd_create, scd_destroy, scd_set_wavenumber, scd_set_green, scd_set_projectors, &
              scd_set_nearzone, scd_grid_from_mesh, scd_set_mesh, scd_build_projectors, &
              scd_build_nearzone, scd_get_projectors, scd_nearzone_count, scd_get_nearzone, &
-             scd_matvec, scd_gmres, scd_solve_columns, scd_vswf_rhs, scd_compute_T_matrix, &
+             scd_matvec, scd_gmres, scd_set_rhs_matrix, scd_solve_columns, scd_vswf_rhs, scd_compute_T_matrix, &
              scd_get_timing, scd_profile_matvec, scd_T_assemble_noalloc, scd_column_latency, &
              scd_nearzone_bytes, scd_selftest_waits, scd_last_error_f
    public :: scd_server_create, scd_server_submit, scd_server_estimate, scd_server_poll, &
@@ -163,13 +173,23 @@ module scadyn_gpu
          integer(c_int32_t), intent(out) :: iters
          real(c_double), intent(out) :: relres
       end function
-      ! the column loop body of compute_T_matrix: Tcols(:, j) = mat(:, :)^H x_j
-      integer(c_int) function scd_solve_columns(ctx, ncol, mat, Tcols, opts, iters, X) &
+      ! the incident matrix mat(3T, nmat) of vswf2constant, kept on the device
+      integer(c_int) function scd_set_rhs_matrix(ctx, nmat, mat) bind(C, name="scd_set_rhs_matrix")
+         import :: c_ptr, c_int, c_int32_t, c_double_complex
+         type(c_ptr), value :: ctx
+         integer(c_int32_t), value :: nmat
+         complex(c_double_complex), intent(in) :: mat(*)
+      end function
+      ! the column loop body of compute_T_matrix for columns col0+1..col0+ncol:
+      ! Tcols(:, j) = mat(:, :)^H x_j (T_matrix.f90:260); mat = c_loc(mat) or
+      ! c_null_ptr for the matrix of scd_set_rhs_matrix
+      integer(c_int) function scd_solve_columns(ctx, nmat, mat, col0, ncol, Tcols, opts, iters, X) &
             bind(C, name="scd_solve_columns")
          import :: c_ptr, c_int, c_int32_t, c_double_complex, scd_solve_opts
          type(c_ptr), value :: ctx
-         integer(c_int32_t), value :: ncol
-         complex(c_double_complex), intent(in) :: mat(*)
+         integer(c_int32_t), value :: nmat
+         type(c_ptr), value :: mat
+         integer(c_int32_t), value :: col0, ncol
          complex(c_double_complex), intent(out) :: Tcols(*)
          type(scd_solve_opts), intent(in) :: opts
          integer(c_int32_t), intent(out) :: iters(*)

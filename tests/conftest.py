@@ -28,5 +28,15 @@ def small_op(small_sphere):
 
 
 @pytest.fixture(scope="session")
+def dev_small(small_op):
+    """The oracle's operator of the 1680-tet sphere loaded into a device
+    context with the default kernel choices (GPU tests only)."""
+    from tests.gpu_helpers import solver_from_oracle
+    s = solver_from_oracle(small_op)
+    yield s
+    s.close()
+
+
+@pytest.fixture(scope="session")
 def rng():
     return np.random.default_rng(1234)

@@ -100,5 +100,7 @@ def test_server_estimate_is_host_side_and_monotone():
     small, big = meshgen.sphere(4, seed=1), meshgen.sphere(7, seed=1)
     assert est(big, 4) > est(small, 4) > 0
     assert est(small, 8) > est(small, 4)
-    assert est(small, 4, storage=api.STORE_C128) > est(small, 4)
-    assert est(small, 4, precision=api.PREC_FP64) > 0
+    fp64 = api.PREC_FP64
+    assert est(small, 4, storage=api.STORE_C128, precision=fp64) > est(small, 4, precision=fp64) > 0
+    # the mixed form with complex64 storage adds the tensor-core tile planes
+    assert est(small, 4) > est(small, 4, precision=fp64)

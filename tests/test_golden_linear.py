@@ -1,7 +1,7 @@
 """Committed linear-basis fixtures (tests/golden/sphere336_linear.npz, made by
 tests/golden/make_golden_linear.py from the CPU oracle): the oracle must keep
 reproducing them (CPU), and the device-built linear operator must match them
-(GPU, collected with SCADYN_TEST_LINEAR=1) -- projectors, 12x12 near-zone
+(GPU) -- projectors, 12x12 near-zone
 blocks and one order-1 matvec of a 336-tet sphere at ka = 1."""
 import os
 
@@ -40,8 +40,6 @@ def test_oracle_reproduces_linear_fixture(lin_op):
 
 
 @pytest.mark.gpu
-@pytest.mark.skipif(os.environ.get("SCADYN_TEST_LINEAR") != "1",
-                    reason="linear basis not yet run on a GPU; set SCADYN_TEST_LINEAR=1")
 def test_device_linear_operator_matches_fixture():
     from scadyn_b200 import api
     d = api.grid_from_mesh(G["coord"], G["etopol"], grid_size=float(G["grid_size"]))

@@ -1,52 +1,26 @@
-"""Classical Gram-Schmidt for the complex64 inner solves (opt-in with
-SCADYN_CGS=1 at context creation) against the default MGS: mixed-precision
-T-matrices agree to 1e-6, both meet the FP64 residual, iteration counts stay
-within 20%, and results are batch-invariant.  Collected only with
-SCADYN_TEST_CGS=1 until the variant has run on a GPU."""
-import os
-
+"""Classical Gram-Schmidt for the complex64 inner solves
+(scd_solve_opts.gram_schmidt = SCD_GS_CLASSICAL, the default) against modified
+Gram-Schmidt (SCD_GS_MODIFIED) on the same context: mixed-precision T-matrices
+agree to 1e-6, both meet the FP64 residual, iteration counts stay within 20%,
+and results are batch-invariant.  The FP64 form always uses MGS."""
 import numpy as np
 import pytest
 
 from oracle import oracle as O
-from tests.gpu_helpers import solver_from_oracle
+from scadyn_b200 import api
 
-pytestmark = [pytest.mark.gpu,
-              pytest.mark.skipif(os.environ.get("SCADYN_TEST_CGS") != "1",
-                                 reason="classical Gram-Schmidt is opt-in; set SCADYN_TEST_CGS=1")]
+pytestmark = pytest.mark.gpu
 
 
 def rel(a, b):
     return np.linalg.norm(a - b) / np.linalg.norm(b)
 
 
-def _solver(op, cgs):
-    old = os.environ.get("SCADYN_CGS")
-    os.environ["SCADYN_CGS"] = "1" if cgs else "0"
-    try:
-        return solver_from_oracle(op)
-    finally:
-        if old is None:
-            os.environ.pop("SCADYN_CGS", None)
-        else:
-            os.environ["SCADYN_CGS"] = old
-
-
-@pytest.fixture(scope="module")
-def pair(small_op):
-    a, b = _solver(small_op, False), _solver(small_op, True)
-    yield a, b
-    a.close()
-    b.close()
-
-
-def test_cgs_T_matches_mgs(pair, small_op, small_sphere):
-    from scadyn_b200 import api
-    a, b = pair
+def test_cgs_T_matches_mgs(dev_small, small_op, small_sphere):
     mat = O.vswf2constant(small_sphere.coord, small_sphere.etopol, small_op.geom.k, 2)
     kw = dict(tol=1e-9, block=16, precision=api.PREC_MIXED, inner_tol=1e-4, max_outer=10, want_x=True)
-    Ta, ita, Xa, rca = a.solve_columns(mat, **kw)
-    Tb, itb, Xb, rcb = b.solve_columns(mat, **kw)
+    Ta, ita, Xa, rca = dev_small.solve_columns(mat, gram_schmidt=api.GS_MODIFIED, **kw)
+    Tb, itb, Xb, rcb = dev_small.solve_columns(mat, gram_schmidt=api.GS_CLASSICAL, **kw)
     assert rca == api.SCD_OK and rcb == api.SCD_OK
     assert rel(Tb, Ta) < 1e-6
     for c in (0, 5, mat.shape[0] - 1):
@@ -55,21 +29,19 @@ def test_cgs_T_matches_mgs(pair, small_op, small_sphere):
     assert itb.sum() <= 1.2 * ita.sum() + 16
 
 
-def test_cgs_batch_invariant(pair, small_op, small_sphere):
-    from scadyn_b200 import api
-    _, b = pair
+@pytest.mark.parametrize("gs", [api.GS_CLASSICAL, api.GS_MODIFIED])
+def test_gram_schmidt_batch_invariant(dev_small, small_op, small_sphere, gs):
     mat = O.vswf2constant(small_sphere.coord, small_sphere.etopol, small_op.geom.k, 1)
-    kw = dict(tol=1e-8, precision=api.PREC_MIXED, inner_tol=1e-3, want_x=True)
-    x1 = b.solve_columns(mat, block=1, **kw)
-    x2 = b.solve_columns(mat, block=6, **kw)
+    kw = dict(tol=1e-8, precision=api.PREC_MIXED, inner_tol=1e-3, want_x=True, gram_schmidt=gs)
+    x1 = dev_small.solve_columns(mat, block=1, **kw)
+    x2 = dev_small.solve_columns(mat, block=6, **kw)
     assert np.array_equal(x1[1], x2[1])
     assert np.array_equal(x1[2], x2[2])
 
 
-def test_fp64_form_unaffected(pair, small_op, small_sphere):
-    """The FP64 form keeps MGS: identical results with and without the flag."""
-    a, b = pair
+def test_fp64_form_unaffected(dev_small, small_op, small_sphere):
+    """The FP64 form keeps MGS: identical results whatever gram_schmidt says."""
     mat = O.vswf2constant(small_sphere.coord, small_sphere.etopol, small_op.geom.k, 1)
-    ra = a.solve_columns(mat, tol=1e-8, block=4, want_x=True)
-    rb = b.solve_columns(mat, tol=1e-8, block=4, want_x=True)
+    ra = dev_small.solve_columns(mat, tol=1e-8, block=4, want_x=True, gram_schmidt=api.GS_MODIFIED)
+    rb = dev_small.solve_columns(mat, tol=1e-8, block=4, want_x=True, gram_schmidt=api.GS_CLASSICAL)
     assert np.array_equal(ra[1], rb[1]) and np.array_equal(ra[2], rb[2])

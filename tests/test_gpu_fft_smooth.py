@@ -1,20 +1,17 @@
-"""5-smooth padded FFT lengths (opt-in with SCADYN_FFT_SMOOTH=1 at context
-creation): on grids of 40 and 44 nodes per axis the device picks P = 80 (the
-reference's 2N) and P = 96 instead of 128, and the FP64 matvec still matches
-the oracle (which uses 2N) to 1e-11, as does GMRES (same iteration count).
-Collected only with SCADYN_TEST_FFT_SMOOTH=1 until the lengths have run on a
-GPU."""
-import os
-
+"""5-smooth padded FFT lengths (scd_grid_desc.fft_lengths = SCD_FFT_SMOOTH,
+the default): on grids of 40 and 44 nodes per axis the device picks P = 80
+(the reference's 2N) and P = 96 instead of 128, and the FP64 matvec still
+matches the oracle (which uses 2N) to 1e-11, as does GMRES (same iteration
+count).  SCD_FFT_POW2 on the same operator gives the same results to
+rounding."""
 import numpy as np
 import pytest
 
 from oracle import oracle as O
+from scadyn_b200 import api
 from tests.gpu_helpers import solver_from_oracle
 
-pytestmark = [pytest.mark.gpu,
-              pytest.mark.skipif(os.environ.get("SCADYN_TEST_FFT_SMOOTH") != "1",
-                                 reason="5-smooth FFT lengths are opt-in; set SCADYN_TEST_FFT_SMOOTH=1")]
+pytestmark = pytest.mark.gpu
 
 
 def rel(a, b):
@@ -24,15 +21,7 @@ def rel(a, b):
 @pytest.fixture(scope="module", params=[0.8, 0.7])
 def op_dev(request, small_sphere):
     op = O.setup(small_sphere, 1.0 / small_sphere.a, grid_size=request.param, nthreads=0)
-    old = os.environ.get("SCADYN_FFT_SMOOTH")
-    os.environ["SCADYN_FFT_SMOOTH"] = "1"
-    try:
-        s = solver_from_oracle(op)
-    finally:
-        if old is None:
-            os.environ.pop("SCADYN_FFT_SMOOTH", None)
-        else:
-            os.environ["SCADYN_FFT_SMOOTH"] = old
+    s = solver_from_oracle(op)
     yield op, s
     s.close()
 
@@ -51,3 +40,14 @@ def test_smooth_length_gmres_matches_oracle(op_dev, small_sphere):
     xr, ir = op.gmres(b, tol=1e-8, m=50, cycles=4)
     assert info["iters"] == ir["iters"]
     assert rel(x, xr) < 1e-9
+
+
+def test_pow2_lengths_match_smooth(op_dev):
+    op, s = op_dev
+    p = solver_from_oracle(op, fft_lengths=api.FFT_POW2)
+    try:
+        rng = np.random.default_rng(22)
+        x = rng.standard_normal(3 * op.geom.T) + 1j * rng.standard_normal(3 * op.geom.T)
+        assert rel(p.compute_Ax2(x), s.compute_Ax2(x)) < 1e-12
+    finally:
+        p.close()

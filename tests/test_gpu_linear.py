@@ -3,10 +3,8 @@ against the oracle's compute_Ax2 with order 1 (src/gmres_module.f90:57-176,
 matmul_Acorr src/sparse_mat.f90:64-92) on the same operator data, complex64
 and complex128 near-zone storage, and GMRES against the oracle's (same
 iteration count).  The operator is the seeded linear-basis operator the
-oracle derives from the 1680-tet sphere.  Collected only with
-SCADYN_TEST_LINEAR=1 until the linear basis has run on a GPU."""
+oracle derives from the 1680-tet sphere."""
 import dataclasses
-import os
 
 import numpy as np
 import pytest
@@ -14,9 +12,7 @@ import pytest
 from oracle import oracle as O
 from tests.gpu_helpers import solver_from_oracle
 
-pytestmark = [pytest.mark.gpu,
-              pytest.mark.skipif(os.environ.get("SCADYN_TEST_LINEAR") != "1",
-                                 reason="linear basis not yet run on a GPU; set SCADYN_TEST_LINEAR=1")]
+pytestmark = pytest.mark.gpu
 
 
 def crand(rng, n):

@@ -2,19 +2,14 @@
 pfft_projection_lin (src/projection.f90:170-338) and
 compute_near_zone_interactions_lin (src/precorrection.f90:268-725) -- against
 the CPU oracle, and the order-1 matvec on the device-built operator.  An
-816-tet sphere at ka = 1.  Collected only with SCADYN_TEST_LINEAR=1 until the
-linear basis has run on a GPU."""
-import os
-
+816-tet sphere at ka = 1."""
 import numpy as np
 import pytest
 
 from oracle import oracle as O
 from scadyn_b200 import api
 
-pytestmark = [pytest.mark.gpu,
-              pytest.mark.skipif(os.environ.get("SCADYN_TEST_LINEAR") != "1",
-                                 reason="linear basis not yet run on a GPU; set SCADYN_TEST_LINEAR=1")]
+pytestmark = pytest.mark.gpu
 
 
 def rel(a, b):

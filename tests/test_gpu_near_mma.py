@@ -1,54 +1,40 @@
-"""The tensor-core near zone (opt-in with SCADYN_NEAR_MMA=1, or =2 for the
-merged instruction schedule, at context creation) against the CUDA-core
-kernel on the same operator: mixed-precision
-T-matrices agree to 1e-6 and both meet the FP64 residual, iteration counts
-stay within 20%, results are batch-invariant, and the pipeline never times
-out.  Two grid cell sizes give groups below and above 64 rows (M = 64 and
-M = 128 accumulators).  Collected only with SCADYN_TEST_NEAR_MMA=1 until the
-kernel is enabled by default."""
-import os
-
+"""The tensor-core near zone of the complex64 matvec (scd_grid_desc.near_kernel:
+SCD_NEAR_TENSOR_SPLIT, or SCD_NEAR_TENSOR_MERGED, the default with complex64
+storage) against the CUDA-core kernel (SCD_NEAR_CUDA_CORES) on the same
+operator: mixed-precision T-matrices agree to 1e-6 and both meet the FP64
+residual, iteration counts stay within 20%, results are batch-invariant, and
+the pipeline never times out.  Two grid cell sizes give groups below and
+above 64 rows (M = 64 and M = 128 accumulators)."""
 import numpy as np
 import pytest
 
 from oracle import oracle as O
+from scadyn_b200 import api
 from tests.gpu_helpers import solver_from_oracle
 
-pytestmark = [pytest.mark.gpu,
-              pytest.mark.skipif(os.environ.get("SCADYN_TEST_NEAR_MMA") != "1",
-                                 reason="tensor-core near zone is opt-in; set SCADYN_TEST_NEAR_MMA=1")]
+pytestmark = pytest.mark.gpu
 
 
 def rel(a, b):
     return np.linalg.norm(a - b) / np.linalg.norm(b)
 
 
-def _solver(op, mma):
-    old = os.environ.get("SCADYN_NEAR_MMA")
-    os.environ["SCADYN_NEAR_MMA"] = mma if mma else "0"
-    try:
-        return solver_from_oracle(op)
-    finally:
-        if old is None:
-            os.environ.pop("SCADYN_NEAR_MMA", None)
-        else:
-            os.environ["SCADYN_NEAR_MMA"] = old
-
-
-@pytest.fixture(scope="module", params=[(1.8, "1"), (3.2, "1"), (1.8, "2"), (3.2, "2")],
-                ids=["1.8", "3.2", "1.8-merged", "3.2-merged"])
+@pytest.fixture(scope="module",
+                params=[(1.8, api.NEAR_TENSOR_SPLIT), (3.2, api.NEAR_TENSOR_SPLIT),
+                        (1.8, api.NEAR_DEFAULT), (3.2, api.NEAR_TENSOR_MERGED)],
+                ids=["1.8", "3.2", "1.8-default", "3.2-merged"])
 def ops(request, small_sphere):
-    grid_size, sched = request.param
+    grid_size, kernel = request.param
     k = 1.0 / small_sphere.a
     op = O.setup(small_sphere, k, grid_size=grid_size, nthreads=0)
-    a, b = _solver(op, None), _solver(op, sched)
+    a = solver_from_oracle(op, near_kernel=api.NEAR_CUDA_CORES)
+    b = solver_from_oracle(op, near_kernel=kernel)
     yield op, a, b
     a.close()
     b.close()
 
 
 def test_tensor_near_zone_T_matches_cuda_core(ops, small_sphere):
-    from scadyn_b200 import api
     op, a, b = ops
     mat = O.vswf2constant(small_sphere.coord, small_sphere.etopol, op.geom.k, 2)
     kw = dict(tol=1e-9, block=16, precision=api.PREC_MIXED, inner_tol=1e-4, max_outer=10, want_x=True)
@@ -63,7 +49,6 @@ def test_tensor_near_zone_T_matches_cuda_core(ops, small_sphere):
 
 
 def test_tensor_near_zone_batch_invariant(ops, small_sphere):
-    from scadyn_b200 import api
     op, _, b = ops
     mat = O.vswf2constant(small_sphere.coord, small_sphere.etopol, op.geom.k, 1)
     kw = dict(tol=1e-8, precision=api.PREC_MIXED, inner_tol=1e-3, want_x=True)
@@ -74,7 +59,27 @@ def test_tensor_near_zone_batch_invariant(ops, small_sphere):
 
 
 def test_tensor_near_zone_profile_runs(ops):
-    from scadyn_b200 import api
     _, _, b = ops
     t = b.profile_matvec(reps=3, nrhs=16, precision=api.PREC_MIXED)
     assert t["matvecs"] >= 3 and t["nearzone_ms"] > 0
+
+
+def test_complex128_storage_keeps_cuda_cores(small_sphere):
+    """With complex128 near-zone storage the default falls back to the CUDA-core
+    kernel, and an explicit tensor-core request is refused."""
+    k = 1.0 / small_sphere.a
+    op = O.setup(small_sphere, k, grid_size=1.8, fp64_near=True, nthreads=0)
+    s = solver_from_oracle(op)
+    try:
+        mat = O.vswf2constant(small_sphere.coord, small_sphere.etopol, k, 1)
+        _, _, _, rc = s.solve_columns(mat, tol=1e-8, block=6, precision=api.PREC_MIXED, inner_tol=1e-3)
+        assert rc == api.SCD_OK
+    finally:
+        s.close()
+    s = solver_from_oracle(op, near_kernel=api.NEAR_TENSOR_MERGED)
+    try:
+        with pytest.raises(api.ScadynError) as e:
+            s.solve_columns(mat, tol=1e-8, block=6, precision=api.PREC_MIXED, inner_tol=1e-3)
+        assert e.value.code == api.SCD_BAD_ARG
+    finally:
+        s.close()

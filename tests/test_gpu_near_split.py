@@ -1,20 +1,15 @@
-"""The FP64 near-zone kernel with split row and column sums (opt-in with
-SCADYN_NEAR_SPLIT=2 at context creation: two lanes per sum at one right-hand
-side, two partial sums per lane at four): the FP64 matvec against the oracle,
-solutions against the default kernel, and bit-identical columns alone and in
-batches (the mixed form's complex64 kernels are left unsplit).  Collected only with
-SCADYN_TEST_NEAR_SPLIT=1 until the variant has run on a GPU."""
-import os
-
+"""The FP64 near-zone kernel with split row and column sums
+(scd_grid_desc.near_split = 2: two lanes per sum at one right-hand side, two
+partial sums per lane at four): the FP64 matvec against the oracle, solutions
+against the default kernel, and bit-identical columns alone and in batches
+(the mixed form's complex64 kernels are left unsplit)."""
 import numpy as np
 import pytest
 
 from oracle import oracle as O
 from tests.gpu_helpers import solver_from_oracle
 
-pytestmark = [pytest.mark.gpu,
-              pytest.mark.skipif(os.environ.get("SCADYN_TEST_NEAR_SPLIT") != "1",
-                                 reason="split near-zone sums are opt-in; set SCADYN_TEST_NEAR_SPLIT=1")]
+pytestmark = pytest.mark.gpu
 
 
 def rel(a, b):
@@ -22,15 +17,7 @@ def rel(a, b):
 
 
 def _solver(op, split):
-    old = os.environ.get("SCADYN_NEAR_SPLIT")
-    os.environ["SCADYN_NEAR_SPLIT"] = "2" if split else "1"
-    try:
-        return solver_from_oracle(op)
-    finally:
-        if old is None:
-            os.environ.pop("SCADYN_NEAR_SPLIT", None)
-        else:
-            os.environ["SCADYN_NEAR_SPLIT"] = old
+    return solver_from_oracle(op, near_split=2 if split else 1)
 
 
 @pytest.fixture(scope="module")

@@ -112,3 +112,28 @@ def test_full_device_T_matrix_matches_oracle(dev_setup, small_sphere, small_op):
     # a column range returns the same columns
     Tpart, _ = s.compute_T_matrix(1, col0=2, ncol=3, tol=1e-10)
     assert rel(Tpart, Td[:, 2:5]) < 1e-12
+
+
+@pytest.mark.parametrize("precision", [api.PREC_FP64, api.PREC_MIXED])
+def test_solve_columns_in_blocks_reproduce_T_matrix(dev_setup, small_op, precision):
+    """The column loop run by the host in two blocks (scd_solve_columns over
+    columns 0..4 and 5..nmat-1 of the whole mat, T_matrix.f90:254-268) returns
+    T_mat(:, col) = mat^H x over all nmat rows (T_matrix.f90:260); times i k^3
+    (T_matrix.f90:271-275) the blocks are scd_compute_T_matrix's full T.  The
+    resident matrix of scd_set_rhs_matrix serves a call with mat = NULL the
+    same way.  Columns are batch-invariant, so the two agree to rounding of
+    the scaling only."""
+    s, _ = dev_setup
+    k = small_op.geom.k
+    Nmax = 2
+    mat = s.vswf2constant(Nmax)                  # (nmat, n)
+    nmat = mat.shape[0]
+    kw = dict(tol=1e-10, m=50, cycles=8, block=4, precision=precision, inner_tol=1e-4, max_outer=10)
+    Tfull, _ = s.compute_T_matrix(Nmax, **kw)     # (nmat, nmat), scaled
+    Ta, ita, _, rca = s.solve_columns(mat, col0=0, ncol=5, **kw)
+    s.set_rhs_matrix(mat)
+    Tb, itb, _, rcb = s.solve_columns(None, col0=5, ncol=nmat - 5, nmat=nmat, **kw)
+    assert rca == api.SCD_OK and rcb == api.SCD_OK
+    assert Ta.shape == (5, nmat) and Tb.shape == (nmat - 5, nmat)
+    Tblocks = np.concatenate([Ta, Tb]).T          # (nmat rows, nmat columns), unscaled
+    assert rel(1j * k ** 3 * Tblocks, Tfull) < 1e-13

@@ -1,11 +1,11 @@
 """scd_T_assemble_noalloc: T = mat^H X on caller-owned device buffers with no
 allocation inside the library.
 
-It serves hosts that cannot let a library call cudaMalloc: device memory that
-belongs to the host's own allocator, or column loops recorded into CUDA
-graphs.  Its output must match the T columns that scd_solve_columns
-assembles for the same solutions, on two calls in a row.  This file is named
-to be collected last."""
+It serves hosts that cannot let a library call cudaMalloc, such as a Fortran
+host whose device memory all comes from its own allocator (CUDA Fortran
+device arrays, OpenACC data regions).  Its output must match the T columns
+that scd_solve_columns assembles for the same solutions, on two calls in a
+row.  This file is named to be collected last."""
 import ctypes
 
 import numpy as np
