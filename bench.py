@@ -72,6 +72,7 @@ METRIC = "T-matrix columns/sec & p50/p99 solve latency at \u22641e-5 rel err, mi
 NEAR_KERNELS = {"default": 0, "cuda": 1, "split": 2, "merged": 3}
 GRAM_SCHMIDT = {"default": 0, "modified": 1, "classical": 2}
 FFT_LENGTHS = {"default": 0, "pow2": 1, "smooth": 2}
+FFT_PASSES = {"default": 0, "fused": 1, "three": 2}
 
 
 def log(*a):
@@ -335,6 +336,9 @@ def main():
     ap.add_argument("--ref-columns", type=int, default=2, help="columns the CPU reference arm solves end to end")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true", help="skip the served-stream summary")
+    ap.add_argument("--no-tune", action="store_true", help="keep the library's default matvec kernels")
+    ap.add_argument("--tune-slots", action="store_true",
+                    help="also choose slots and the inner Krylov dimension from a sample of columns")
     ap.add_argument("--serve", type=int, default=0,
                     help="run a served request stream of this many requests instead (C4-shaped, scaled)")
     ap.add_argument("--sweep", type=int, default=0,
@@ -351,11 +355,13 @@ def main():
                     help="orthogonalisation of the complex64 inner solves (scd_solve_opts.gram_schmidt)")
     ap.add_argument("--fft-lengths", default="default", choices=sorted(FFT_LENGTHS),
                     help="padded FFT lengths (scd_grid_desc.fft_lengths)")
+    ap.add_argument("--fft-passes", default="default", choices=sorted(FFT_PASSES),
+                    help="fused y-z FFT pass or three separate passes (scd_grid_desc.fft_passes)")
     ap.add_argument("--near-split", action="store_true",
                     help="FP64 near-zone row and column sums split in two partial sums (scd_grid_desc.near_split)")
     args = ap.parse_args()
     choices = dict(near_kernel=NEAR_KERNELS[args.near_kernel], fft_lengths=FFT_LENGTHS[args.fft_lengths],
-                   near_split=2 if args.near_split else 0)
+                   near_split=2 if args.near_split else 0, fft_passes=FFT_PASSES[args.fft_passes])
     gs_choice = GRAM_SCHMIDT[args.gram_schmidt]
     if args.serve:
         print(json.dumps(serve_bench(args.serve)), flush=True)
@@ -456,6 +462,25 @@ def main():
     # `S` columns in flight as batched slots, continuous batching
     fp64 = dict(tol=cfg["tol"], m=cfg["m"], cycles=cfg["cycles"])
     S = min(args.slots, B)
+    # autotuner: the matvec kernels for the timed region's shape (S complex64
+    # right-hand sides), and on request the slots and inner Krylov dimension
+    # from a short sample of columns (untimed, before the warm-up)
+    tuning = None
+    if not args.no_tune:
+        from scadyn_b200 import autotune
+        t_tune = time.time()
+        mv, cached = autotune.tune_matvec(solver, S, api.PREC_MIXED)
+        tuning = {"matvec": {k: (round(v, 4) if isinstance(v, float) else v) for k, v in mv.items()},
+                  "cached": cached}
+        if args.tune_slots:
+            choice, rates, _ = autotune.tune_slots(solver, Nmax, sample_cols=B, slots=(16, 32, 64),
+                                                   inner_m=(20, 30), col0=cols_for(0),
+                                                   tol=cfg["tol"], cycles=60, inner_tol=cfg["inner_tol"],
+                                                   max_outer=cfg["max_outer"])
+            S = min(choice["slots"], B)
+            mixed["m"] = choice["inner_m"]
+            tuning["slots"] = {"choice": choice, "columns_per_s": rates}
+        tuning["seconds"] = round(time.time() - t_tune, 2)
     for st in range(args.warmup):
         solver.compute_T_matrix(Nmax, col0=cols_for(st), ncol=B, block=S, **mixed)
 
@@ -559,7 +584,8 @@ def main():
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": kind,
             "kernel": ("k_near_mma (tensor-core near-zone tile products, 16 complex64 right-hand sides per launch)"
-                       if choices["near_kernel"] != NEAR_KERNELS["cuda"] else
+                       if (tuning["matvec"]["near_kernel"] if tuning else choices["near_kernel"]) != NEAR_KERNELS["cuda"]
+                       else
                        "k_near_groups (near-zone block SpMV, 16 complex64 right-hand sides per launch)"),
             "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": near_ms,
             "flops_per_launch": Bref * 144 * 16 * 2}
@@ -607,6 +633,7 @@ def main():
                                                                             cfg["tol"]),
                        "l2": "inputs larger than L2 (near-zone tiles %.2f GB per matvec)" % (solver.nearzone_bytes() / 1e9),
                        "near_kernel": args.near_kernel, "gram_schmidt": args.gram_schmidt,
+                       "fft_passes": args.fft_passes,
                        "near_split": bool(args.near_split),
                        "fft_lengths": [fft_len(2 * v, FFT_LENGTHS[args.fft_lengths] != 1) for v in (desc.Nx, desc.Ny, desc.Nz)],
                        "parallelism": f"replicas x{world}"},
@@ -624,6 +651,7 @@ def main():
             "clocks": clk.summary(),
             "gpu_launches": launches,
             "setup_s": round(setup_s, 2),
+            "tuning": tuning,
             "wall_s": round(wall, 2),
         }
         print(json.dumps(line), flush=True)

@@ -74,7 +74,14 @@ typedef struct scd_grid_desc {
     int32_t fft_lengths;     /* SCD_FFT_*: padded FFT length per axis */
     int32_t near_kernel;     /* SCD_NEAR_*: near-zone kernel of the complex64 matvec */
     int32_t near_split;      /* partial sums per near-zone row/column sum of the FP64 matvec: 0 or 1 one, 2 two */
+    int32_t fft_passes;      /* SCD_FFT_PASSES_*: how the y and z transforms run */
 } scd_grid_desc;
+
+/* scd_grid_desc.fft_passes */
+#define SCD_FFT_PASSES_DEFAULT  0   /* SCD_FFT_PASSES_FUSED_YZ where the lengths and shared memory allow */
+#define SCD_FFT_PASSES_FUSED_YZ 1   /* one kernel per (x column, grid) transforms y, z, x Fg, z^-1, y^-1 in
+                                       shared memory (y and z lengths 64, 80, 96, 128 or 192) */
+#define SCD_FFT_PASSES_THREE    2   /* separate y forward, z (forward, x Fg, inverse), y inverse passes */
 
 /* scd_grid_desc.fft_lengths.  Every choice is an exact linear convolution:
  * the input occupies N <= P/2 samples of each axis. */
@@ -239,6 +246,33 @@ SCD_API int scd_get_timing(scd_ctx *ctx, scd_timing *t, int32_t reset);
  * solves use (SCD_PREC_MIXED), and record per-kernel averages per call in
  * the timing block (matvec_ms, nearzone_ms, fft_ms, gather_ms). */
 SCD_API int scd_profile_matvec(scd_ctx *ctx, int32_t reps, int32_t nrhs, int32_t precision);
+
+/* Matvec kernel settings of a context that can change between calls; the
+ * autotuner's result (scd_tune_matvec) and what scd_apply_tuning sets. */
+typedef struct scd_tuning {
+    int32_t nrhs;             /* right-hand sides per matvec the setting was timed at */
+    int32_t precision;        /* SCD_PREC_FP64 or SCD_PREC_MIXED (the complex64 matvec) */
+    int32_t near_kernel;      /* SCD_NEAR_CUDA_CORES / _TENSOR_SPLIT / _TENSOR_MERGED (complex64 matvec) */
+    int32_t fft_passes;       /* SCD_FFT_PASSES_FUSED_YZ or SCD_FFT_PASSES_THREE */
+    int32_t scatter_span;     /* right-hand sides per warp of the anterpolation, 0 = all of a call's */
+    int32_t gather_span;      /* right-hand sides per warp of the interpolation, 0 = all */
+    double matvec_ms;         /* the chosen setting's matvec time */
+    double default_ms;        /* the library defaults' matvec time */
+} scd_tuning;
+
+/* Autotuner (no counterpart in the reference, whose analogue is FFTW's
+ * planning, src/possu.f90:82-89): times `reps` device-resident matvecs of
+ * `nrhs` right-hand sides for the candidate settings of each knob in turn
+ * (near-zone kernel, fused or three-pass y-z FFT, anterpolation and
+ * interpolation spans), keeps the fastest, applies it to the context and
+ * returns it.  Results do not depend on the choice beyond rounding (the
+ * near-zone kernels round differently; every choice keeps a column
+ * bit-identical alone and in any batch). */
+SCD_API int scd_tune_matvec(scd_ctx *ctx, int32_t nrhs, int32_t precision, int32_t reps, scd_tuning *out);
+
+/* Apply a stored tuning (e.g. a cached scd_tune_matvec result for the same
+ * grid, tets and right-hand sides) without timing anything. */
+SCD_API int scd_apply_tuning(scd_ctx *ctx, const scd_tuning *tuning);
 
 /* T = mat^H X without allocating: mat (n, ncol), X (n, ncb) and T (ncol, ncb)
  * are DEVICE pointers owned by the caller; the kernels run on `stream`

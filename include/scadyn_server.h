@@ -2,16 +2,21 @@
  *
  * Requests (a tetrahedral mesh with per-tet permittivity, a wavenumber, a
  * VSWF order and solve options) arrive at any time through
- * scd_server_submit.  A dispatcher thread admits queued requests in arrival
- * order whenever their estimated device memory fits the HBM budget and an
- * execution slot is free (a request that fits may pass one that does not).
- * Each admitted request runs on its own worker thread with its own context
- * and CUDA stream: the operator is built on the device (Green octant,
- * projectors, near zone) and all its columns are solved with the batched
- * solver (continuous batching over the request's columns), so the kernels of
- * concurrent requests overlap on the GPU.  A request's arithmetic depends on
- * its own data only: its T-matrix is bit-identical whether it runs alone or
- * in a mix.
+ * scd_server_submit.  Requests with the same operator key (mesh,
+ * permittivities, wavenumber, cell size, near-zone storage and solve
+ * options) share one resident pool: a device context with the operator
+ * built once (Green octant, projectors, near zone) and the batched solver's
+ * slots, on its own worker thread and CUDA stream.  A request joining a
+ * pool that is solving has its incident columns queued at once; they take
+ * slots as running columns finish, beside the columns of the other requests
+ * (continuous batching across requests).  Pools stay resident when idle, so
+ * a later request of the same key skips the operator build; idle pools are
+ * evicted, least recently used first, when a new pool needs the memory.  A
+ * dispatcher admits queued requests in arrival order whenever the estimated
+ * memory fits the HBM budget (a request that fits may pass one that does
+ * not).  Pools solve concurrently, so their kernels overlap on the GPU.  A
+ * column's arithmetic does not depend on its batch: a request's T-matrix is
+ * bit-identical alone, in a mix, or sharing a pool.
  *
  * This layer has no counterpart in the reference (a batch program that
  * solves one geometry per run); it serves the per-request entry points of
@@ -56,10 +61,14 @@ typedef struct scd_server_stats {
     int64_t peak_bytes;
     double p50_ms, p99_ms;      /* submit -> done latency over the completed requests */
     double busy_s;              /* wall time with at least one request running */
+    int64_t pools_built;        /* operator pools built (one per distinct operator key) */
+    int64_t pool_reuses;        /* requests that joined a resident pool instead of building one */
+    int32_t pools_resident;     /* pools on the device now, solving or idle */
 } scd_server_stats;
 
-/* Start a server on `device` with an HBM budget (bytes) for the running
- * requests and at most max_running requests at once. */
+/* Start a server on `device` with an HBM budget (bytes) for the resident
+ * pools and the running requests; max_running bounds the pools solving at
+ * once (0: only the budget bounds them). */
 SCD_API int scd_server_create(scd_server **srv, int32_t device, int64_t hbm_budget, int32_t max_running);
 
 /* Queue a request; its arrays are copied.  *id identifies it.  A request
@@ -79,7 +88,7 @@ SCD_API int scd_server_wait(scd_server *srv, int64_t id, double timeout_s);
 
 /* T (ncol x ncol, column-major, ncol = 2((Nmax+1)^2 - 1)) and per-column
  * iteration counts (may be NULL) of a finished request; the request's
- * result is released afterwards. */
+ * result is released afterwards, and a second call returns SCD_NOT_READY. */
 SCD_API int scd_server_result(scd_server *srv, int64_t id, scd_c128 *T, int32_t *iters);
 
 /* Drop a queued request (a running one finishes). */

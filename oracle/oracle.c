@@ -801,6 +801,30 @@ static void tet5_shape(double shape[24][4]) {
     }
 }
 
+/* single-point forms of the constant-basis integrals for tests: B (4,3)
+ * vertices, tri (3,3); out[0] = int 1/R dS, out[1] = int R dS */
+void orc_analytical_integration(const double tri[9], const double r[3], double out[2]) {
+    double t[3][3], n[3];
+    memcpy(t, tri, sizeof t);
+    tri_n_vector(t, n);
+    analytical_integration(t, n, r, out);
+}
+zc orc_int_V_G(const double rf[3], double k, const double B[12]) {
+    quad_init();
+    double Bc[4][3], Pb[24][3], wb[24];
+    memcpy(Bc, B, sizeof Bc);
+    linmap_tet(Bc, 24, (const double (*)[3])QT5P, QT5W, Pb, wb);
+    return int_V_G(rf, k, 24, (const double (*)[3])Pb, wb, (const double (*)[3])Bc);
+}
+zc orc_int_S_G(const double rf[3], double k, const double tri[9]) {
+    quad_init();
+    double t[3][3], n[3], Pb[7][3], wb[7];
+    memcpy(t, tri, sizeof t);
+    tri_n_vector(t, n);
+    linmap_tri(t, 7, (const double (*)[2])QR5P, QR5W, Pb, wb);
+    return int_S_G(rf, (const double (*)[3])t, n, k, 7, (const double (*)[3])Pb, wb);
+}
+
 /* single-point forms of the above for tests: B (4,3) vertices, tri (3,3) */
 void orc_int_V_GN(const double rf[3], double k, const double B[12], zc out[4]) {
     quad_init();

@@ -79,6 +79,9 @@ int  orc_nearzone_lin(const orc_geom *g, const zc *S, const zc *Sx, const zc *Sy
 /* test forms: singularity_subtraction_int_V_GN / _int_S_GN at one point with
  * the order-5 rules, B (4,3) and tri (3,3) vertex coordinates; gradshape */
 void orc_int_V_GN(const double rf[3], double k, const double B[12], zc out[4]);
+void orc_analytical_integration(const double tri[9], const double r[3], double out[2]);  /* int 1/R, int R */
+zc   orc_int_V_G(const double rf[3], double k, const double B[12]);
+zc   orc_int_S_G(const double rf[3], double k, const double tri[9]);
 void orc_int_S_GN(const double rf[3], const double tri[9], double k, zc out[3]);
 void orc_gradshape(const double tc[12], double dN[12]);
 

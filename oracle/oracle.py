@@ -402,6 +402,35 @@ def setup_lin(mesh, k, grid_size=1.8, fp64_near=False, nthreads=0):
     return Operator(g, S, Sx, Sy, Sz, indS, Fg, sp, ind, order=1)
 
 
+def analytical_integration(tri, r):
+    """analytical_integration (src/singularity_subtraction.f90:15-108) at one
+    point: [int_tri 1/R dS, int_tri R dS]; tri (3,3)."""
+    out = np.zeros(2, np.float64)
+    lib().orc_analytical_integration(_p(np.ascontiguousarray(tri, np.float64)),
+                                     _p(np.ascontiguousarray(r, np.float64)), _p(out))
+    return out
+
+
+def int_V_G(rf, k, B):
+    """singularity_subtraction_int_V_G (src/singularity_subtraction.f90:112-189)
+    at one point: int_B G(rf, r') dV'; B (4,3)."""
+    f = lib().orc_int_V_G
+    f.argtypes = [C.c_void_p, C.c_double, C.c_void_p]
+    f.restype = _Z
+    z = f(_p(np.ascontiguousarray(rf, np.float64)), float(k), _p(np.ascontiguousarray(B, np.float64)))
+    return complex(z.re, z.im)
+
+
+def int_S_G(rf, k, tri):
+    """singularity_subtraction_int_S_G (src/singularity_subtraction.f90:193-243)
+    at one point: int_tri G(rf, r') dS'; tri (3,3)."""
+    f = lib().orc_int_S_G
+    f.argtypes = [C.c_void_p, C.c_double, C.c_void_p]
+    f.restype = _Z
+    z = f(_p(np.ascontiguousarray(rf, np.float64)), float(k), _p(np.ascontiguousarray(tri, np.float64)))
+    return complex(z.re, z.im)
+
+
 def int_V_GN(rf, k, B):
     """singularity_subtraction_int_V_GN at one point: int_B G(rf, r') N_j(r') dV', j = 1..4; B (4,3)."""
     out = np.zeros(4, np.complex128)

@@ -15,6 +15,7 @@ that computes needs the CUDA library and a device and raises otherwise.
 from __future__ import annotations
 
 import ctypes as C
+import hashlib
 import os
 from dataclasses import dataclass
 
@@ -30,6 +31,7 @@ SCD_M_MAX = 63
 FFT_DEFAULT, FFT_POW2, FFT_SMOOTH = 0, 1, 2
 NEAR_DEFAULT, NEAR_CUDA_CORES, NEAR_TENSOR_SPLIT, NEAR_TENSOR_MERGED = 0, 1, 2, 3
 GS_DEFAULT, GS_MODIFIED, GS_CLASSICAL = 0, 1, 2
+FFT_PASSES_DEFAULT, FFT_PASSES_FUSED_YZ, FFT_PASSES_THREE = 0, 1, 2
 
 _NAMES = {0: "SCD_OK", 1: "SCD_NOT_CONVERGED", 2: "SCD_NAN", 3: "SCD_OOM", 4: "SCD_BAD_ARG",
           5: "SCD_TIMEOUT", 6: "SCD_CUDA_ERROR", 7: "SCD_NOT_READY", 8: "SCD_NO_DEVICE"}
@@ -41,7 +43,7 @@ EXPORTS = [
     "scd_build_projectors", "scd_build_nearzone", "scd_get_projectors", "scd_nearzone_count",
     "scd_get_nearzone", "scd_matvec", "scd_gmres", "scd_set_rhs_matrix", "scd_solve_columns", "scd_vswf_rhs",
     "scd_get_timing", "scd_compute_T_matrix", "scd_profile_matvec", "scd_nearzone_bytes",
-    "scd_column_latency", "scd_T_assemble_noalloc", "scd_selftest_waits",
+    "scd_column_latency", "scd_T_assemble_noalloc", "scd_selftest_waits", "scd_tune_matvec", "scd_apply_tuning",
 ]
 
 
@@ -55,7 +57,8 @@ class GridDesc(C.Structure):
     _fields_ = [("Nx", C.c_int32), ("Ny", C.c_int32), ("Nz", C.c_int32), ("delta", C.c_double),
                 ("min_coord", C.c_double * 3), ("T", C.c_int32), ("order", C.c_int32),
                 ("M_ex", C.c_int32), ("near_zone", C.c_int32), ("device", C.c_int32),
-                ("fft_lengths", C.c_int32), ("near_kernel", C.c_int32), ("near_split", C.c_int32)]
+                ("fft_lengths", C.c_int32), ("near_kernel", C.c_int32), ("near_split", C.c_int32),
+                ("fft_passes", C.c_int32)]
 
 
 class SolveOpts(C.Structure):
@@ -69,6 +72,12 @@ class Timing(C.Structure):
                 ("gather_ms", C.c_double), ("arnoldi_ms", C.c_double), ("last_call_ms", C.c_double),
                 ("accum_ms", C.c_double), ("launches", C.c_int64), ("matvecs", C.c_int64),
                 ("arnoldi_steps", C.c_int64), ("near_kernel_ms", C.c_double)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("nrhs", C.c_int32), ("precision", C.c_int32), ("near_kernel", C.c_int32), ("fft_passes", C.c_int32),
+                ("scatter_span", C.c_int32), ("gather_span", C.c_int32), ("matvec_ms", C.c_double),
+                ("default_ms", C.c_double)]
 
 
 _lib = None
@@ -106,6 +115,8 @@ def load_library(path: str = LIB_PATH):
         "scd_get_timing": ([vp, C.POINTER(Timing), i32], C.c_int),
         "scd_compute_T_matrix": ([vp, i32, C.POINTER(SolveOpts), i32, i32, vp, vp], C.c_int),
         "scd_profile_matvec": ([vp, i32, i32, i32], C.c_int),
+        "scd_tune_matvec": ([vp, i32, i32, i32, C.POINTER(Tuning)], C.c_int),
+        "scd_apply_tuning": ([vp, C.POINTER(Tuning)], C.c_int),
         "scd_nearzone_bytes": ([vp], C.c_int64),
         "scd_column_latency": ([vp, i32, vp], C.c_int),
         "scd_T_assemble_noalloc": ([vp, i64, i32, vp, i32, vp, vp], C.c_int),
@@ -164,7 +175,7 @@ class Solver:
     """One device context (scd_ctx) for one mesh and grid."""
 
     def __init__(self, Nx, Ny, Nz, delta, min_coord, T, device=0, order=0, fft_lengths=FFT_DEFAULT,
-                 near_kernel=NEAR_DEFAULT, near_split=0):
+                 near_kernel=NEAR_DEFAULT, near_split=0, fft_passes=FFT_PASSES_DEFAULT):
         """order 1 (linear basis): 4 projector columns and 12 unknowns per tet.
         The operator comes from the host (set_projectors, set_nearzone with
         12x12 blocks) or from the mesh on the device (set_mesh,
@@ -180,6 +191,7 @@ class Solver:
             d.min_coord[i] = float(min_coord[i])
         d.T, d.order, d.M_ex, d.near_zone, d.device = T, order, 2, 1, device
         d.fft_lengths, d.near_kernel, d.near_split = fft_lengths, near_kernel, near_split
+        d.fft_passes = fft_passes
         self.desc = d
         self.order = order
         self.T = (4 if order == 1 else 1) * T      # projector columns (basis functions)
@@ -197,7 +209,8 @@ class Solver:
     @classmethod
     def from_desc(cls, d: GridDesc, device=0):
         return cls(d.Nx, d.Ny, d.Nz, d.delta, list(d.min_coord), d.T, device, order=d.order,
-                   fft_lengths=d.fft_lengths, near_kernel=d.near_kernel, near_split=d.near_split)
+                   fft_lengths=d.fft_lengths, near_kernel=d.near_kernel, near_split=d.near_split,
+                   fft_passes=d.fft_passes)
 
     def _chk(self, rc, what, ok=(SCD_OK,)):
         if rc not in ok:
@@ -218,6 +231,19 @@ class Solver:
     # --- operator pieces
     def set_wavenumber(self, k):
         self._chk(self.lib.scd_set_wavenumber(self.ctx, float(k)), "set_wavenumber")
+        self._k = float(k)
+
+    def problem_key(self):
+        """Identity of the problem this context solves, for checkpoints:
+        unknowns, grid, wavenumber and a digest of the mesh (set_mesh) or of
+        the host projectors (set_projectors) it was set up from; None before
+        either is known."""
+        src = getattr(self, "_mesh_digest", None) or getattr(self, "_proj_digest", None)
+        if src is None or not hasattr(self, "_k"):
+            return None
+        d = self.desc
+        return {"n": int(self.n), "grid": [int(d.Nx), int(d.Ny), int(d.Nz)], "delta": float(d.delta),
+                "k": self._k, "source": src}
 
     def build_G(self, Fg=None):
         """matrices%Fg; None builds it on the device (src/build_G.f90)."""
@@ -232,6 +258,10 @@ class Solver:
         indS = np.ascontiguousarray(indS, np.int32)
         self._chk(self.lib.scd_set_projectors(self.ctx, 27, self.T, _p(S), _p(Sx), _p(Sy), _p(Sz), _p(indS)),
                   "set_projectors")
+        h = hashlib.sha256()
+        for a in (S, Sx, Sy, Sz, indS):
+            h.update(a.tobytes())
+        self._proj_digest = "projectors:" + h.hexdigest()
 
     def set_nearzone(self, sp_mat, sp_ind):
         sp_ind = np.ascontiguousarray(sp_ind, np.int32)
@@ -249,6 +279,10 @@ class Solver:
         self._param = _c128(param)
         self._chk(self.lib.scd_set_mesh(self.ctx, self._coord.shape[0], _p(self._coord), _p(self._etopol),
                                         _p(self._param)), "set_mesh")
+        h = hashlib.sha256()
+        for a in (self._coord, self._etopol, self._param):
+            h.update(a.tobytes())
+        self._mesh_digest = "mesh:" + h.hexdigest()
 
     def pfft_projection_const(self):
         """Projectors on the device; returns (S, Sx, Sy, Sz, indS) in the reference layout."""
@@ -354,6 +388,18 @@ class Solver:
     def profile_matvec(self, reps=10, nrhs=1, precision=PREC_FP64):
         self._chk(self.lib.scd_profile_matvec(self.ctx, reps, nrhs, precision), "profile_matvec")
         return self.timing()
+
+    def tune_matvec(self, nrhs, precision=PREC_MIXED, reps=10):
+        """scd_tune_matvec: time the matvec kernel choices, keep the fastest
+        (applied to this context) and return it as a dict."""
+        t = Tuning()
+        self._chk(self.lib.scd_tune_matvec(self.ctx, nrhs, precision, reps, C.byref(t)), "tune_matvec")
+        return {f: getattr(t, f) for f, _ in Tuning._fields_}
+
+    def apply_tuning(self, tuning):
+        """scd_apply_tuning with a dict of tune_matvec's fields."""
+        t = Tuning(**{f: tuning[f] for f, _ in Tuning._fields_ if f in tuning})
+        self._chk(self.lib.scd_apply_tuning(self.ctx, C.byref(t)), "apply_tuning")
 
     def column_latency(self, ncol):
         ms = np.zeros(ncol, np.float64)

@@ -10,7 +10,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libscadyn_gpu.so")
 SOURCES = ["api.cu", "kernels_matvec.cu", "kernels_setup.cu", "setup_device.cu", "batch.cu", "server.cu", "selftest.cu", "near_mma.cu"]
-HEADERS = ["common.cuh", "ctx.h", "fft_reg.cuh", "near_mma.cuh", "linear_basis.h", "fft_mixed.cuh", "geom.cuh", "lin_setup.cuh", "layout_check.h"]
+HEADERS = ["common.cuh", "ctx.h", "fft_reg.cuh", "near_mma.cuh", "linear_basis.h", "fft_mixed.cuh", "fft_yz.cuh",
+           "geom.cuh", "lin_setup.cuh", "layout_check.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden",
          "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]

@@ -22,8 +22,9 @@ import time
 import numpy as np
 
 
-def _key(Nmax, opts, tag):
-    return json.dumps({"Nmax": int(Nmax), "opts": {k: opts[k] for k in sorted(opts)}, "tag": tag}, sort_keys=True)
+def _key(Nmax, opts, tag, problem):
+    return json.dumps({"Nmax": int(Nmax), "opts": {k: opts[k] for k in sorted(opts)}, "tag": tag,
+                       "problem": problem}, sort_keys=True)
 
 
 def _save(path, T, done, iters, key):
@@ -44,18 +45,28 @@ def near_zone_roofline(solver, hbm_gbs=None, reps=5):
     return out
 
 
-def solve_T_with_checkpoints(solver, Nmax, path, block=64, tag="", log=None, hbm_gbs=None, **opts):
+def solve_T_with_checkpoints(solver, Nmax, path, block=64, tag="", log=None, hbm_gbs=None, problem=None, **opts):
     """T (2nm, 2nm) of `solver` (anything with compute_T_matrix(Nmax, col0,
     ncol, **opts) -> (T_cols, iters)), resuming from `path` when it holds a
-    checkpoint of the same problem (same Nmax, options and tag).  Returns
-    (T, iters, blocks solved in this call).  With a log and a solver that
-    profiles (profile_matvec, nearzone_bytes), the first record also carries
-    the near zone's achieved bandwidth, as a fraction of hbm_gbs when given."""
+    checkpoint of the same problem: the same Nmax, options, tag and problem
+    identity -- `problem`, or else the solver's problem_key() (unknowns, grid,
+    wavenumber and a digest of the mesh or operator it was set up from).  A
+    solve whose identity is unknown needs a non-empty tag, so that a
+    checkpoint of another mesh or wavelength is never mixed into it.
+    Returns (T, iters, blocks solved in this call).  With a log and a solver
+    that profiles (profile_matvec, nearzone_bytes), the first record also
+    carries the near zone's achieved bandwidth, as a fraction of hbm_gbs when
+    given."""
     ncol = 2 * ((Nmax + 1) ** 2 - 1)
+    if problem is None and hasattr(solver, "problem_key"):
+        problem = solver.problem_key()
+    if problem is None and not tag:
+        raise ValueError("a checkpoint needs the problem's identity: pass problem=..., a non-empty tag, "
+                         "or a solver with problem_key()")
     roof = None
     if log and hasattr(solver, "profile_matvec") and hasattr(solver, "nearzone_bytes"):
         roof = near_zone_roofline(solver, hbm_gbs)
-    key = _key(Nmax, opts, tag)
+    key = _key(Nmax, opts, tag, problem)
     T = np.zeros((ncol, ncol), np.complex128)
     done = np.zeros(ncol, bool)
     iters = np.zeros(ncol, np.int32)

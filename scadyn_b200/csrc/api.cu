@@ -382,6 +382,7 @@ int scd_create(scd_ctx **out, const scd_grid_desc *d) {
     if (d->fft_lengths < SCD_FFT_DEFAULT || d->fft_lengths > SCD_FFT_SMOOTH) return SCD_BAD_ARG;
     if (d->near_kernel < SCD_NEAR_DEFAULT || d->near_kernel > SCD_NEAR_TENSOR_MERGED) return SCD_BAD_ARG;
     if (d->near_split < 0 || d->near_split > 2) return SCD_BAD_ARG;
+    if (d->fft_passes < SCD_FFT_PASSES_DEFAULT || d->fft_passes > SCD_FFT_PASSES_THREE) return SCD_BAD_ARG;
     scd_ctx *c = new scd_ctx();
     c->d = *d;
     c->dev = d->device;
@@ -390,6 +391,7 @@ int scd_create(scd_ctx **out, const scd_grid_desc *d) {
     c->nzm_on = d->near_kernel != SCD_NEAR_CUDA_CORES;
     c->nzm_sched = d->near_kernel == SCD_NEAR_TENSOR_SPLIT ? 0 : 1;
     c->near_split = d->near_split == 2 ? 2 : 1;
+    c->yz_on = d->fft_passes != SCD_FFT_PASSES_THREE;
     cudaSetDevice(c->dev);
     cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev);
     c->Nx = d->Nx; c->Ny = d->Ny; c->Nz = d->Nz;
@@ -427,7 +429,7 @@ int scd_destroy(scd_ctx *c) {
                     c->d_y, c->d_io, c->d_rhs,
                     c->d_bar, c->d_err, c->d_tw[0], c->d_tw[1], c->d_tw[2], c->f_P, c->f_Fo,
                     c->f_tw[0], c->f_tw[1], c->f_tw[2], c->f_bpart, c->f_W, c->f_R, c->f_nzpart, c->d_xT, c->f_xT,
-                    c->d_t16, c->d_t16_off, c->d_xb, c->d_xb_off, c->d_xmax, c->d_xinv};
+                    c->d_t16, c->d_t16_off, c->d_xb, c->d_xb_off, c->d_xmax, c->d_xinv, c->d_Fyz, c->f_Fyz};
     for (void *p : ptrs) if (p) cudaFree(p);
     batch_free(c);
     if (c->d_mat) cudaFree(c->d_mat);
@@ -457,6 +459,7 @@ int scd_set_green(scd_ctx *c, const scd_c128 *Fg) {
     int rc = setup_green(c, Fg);
     if (rc == SCD_OK) c->have_green = true;
     c->f_ready = false;
+    c->fyz_ready = c->fyz_ready_f = false;
     return rc;
 }
 
@@ -780,6 +783,84 @@ int scd_profile_matvec(scd_ctx *c, int32_t reps, int32_t nrhs, int32_t precision
     c->t_near_k = sk / reps;
     if ((rc = near_status(c))) return rc;
     return check_cuda(c, cudaGetLastError(), "profile");
+}
+
+// ---------------------------------------------------------------- autotuner
+static void put_tuning(scd_ctx *c, const scd_tuning &t) {
+    if (t.near_kernel == SCD_NEAR_CUDA_CORES) {
+        c->nzm_on = false;
+    } else if (t.near_kernel == SCD_NEAR_TENSOR_SPLIT || t.near_kernel == SCD_NEAR_TENSOR_MERGED) {
+        c->nzm_on = true;
+        c->nzm_sched = t.near_kernel == SCD_NEAR_TENSOR_SPLIT ? 0 : 1;
+    }
+    c->yz_on = t.fft_passes != SCD_FFT_PASSES_THREE;
+    c->scatter_span = std::max(0, t.scatter_span);
+    c->gather_span = std::max(0, t.gather_span);
+}
+
+static scd_tuning get_tuning(const scd_ctx *c, int nrhs, int precision) {
+    scd_tuning t{};
+    t.nrhs = nrhs;
+    t.precision = precision;
+    t.near_kernel = !c->nzm_on ? SCD_NEAR_CUDA_CORES : c->nzm_sched == 0 ? SCD_NEAR_TENSOR_SPLIT : SCD_NEAR_TENSOR_MERGED;
+    t.fft_passes = c->yz_on ? SCD_FFT_PASSES_FUSED_YZ : SCD_FFT_PASSES_THREE;
+    t.scatter_span = c->scatter_span;
+    t.gather_span = c->gather_span;
+    return t;
+}
+
+int scd_apply_tuning(scd_ctx *c, const scd_tuning *t) {
+    if (!c || !t) return SCD_BAD_ARG;
+    if ((t->near_kernel < SCD_NEAR_DEFAULT || t->near_kernel > SCD_NEAR_TENSOR_MERGED) ||
+        (t->fft_passes < SCD_FFT_PASSES_DEFAULT || t->fft_passes > SCD_FFT_PASSES_THREE) || t->scatter_span < 0 ||
+        t->gather_span < 0)
+        return set_error(c, SCD_BAD_ARG, "tuning out of range");
+    if (t->near_kernel >= SCD_NEAR_TENSOR_SPLIT && c->have_near && c->near_prec != SCD_STORE_C64)
+        return set_error(c, SCD_BAD_ARG, "the tensor-core near zone needs complex64 storage");
+    put_tuning(c, *t);
+    return SCD_OK;
+}
+
+int scd_tune_matvec(scd_ctx *c, int32_t nrhs, int32_t precision, int32_t reps, scd_tuning *out) {
+    if (!c || !out || nrhs < 1 || reps < 1) return SCD_BAD_ARG;
+    if (precision != SCD_PREC_FP64 && precision != SCD_PREC_MIXED)
+        return set_error(c, SCD_BAD_ARG, "precision %d", precision);
+    int rc = ready(c);
+    if (rc) return rc;
+    auto time_of = [&](const scd_tuning &t, double *ms) {
+        put_tuning(c, t);
+        const int r = scd_profile_matvec(c, reps, nrhs, precision);
+        *ms = c->t_matvec;
+        return r;
+    };
+    scd_tuning best = get_tuning(c, nrhs, precision);
+    double best_ms = 0;
+    if ((rc = time_of(best, &best_ms))) return rc;
+    const double default_ms = best_ms;
+    // one knob at a time, the others at their best so far
+    auto knob = [&](int32_t scd_tuning::*field, std::initializer_list<int32_t> values) -> int {
+        for (int32_t v : values) {
+            if (best.*field == v) continue;
+            scd_tuning t = best;
+            t.*field = v;
+            double ms = 0;
+            const int r = time_of(t, &ms);
+            if (r) return r;
+            if (ms < best_ms) { best = t; best_ms = ms; }
+        }
+        return SCD_OK;
+    };
+    if (precision == SCD_PREC_MIXED && c->near_prec == SCD_STORE_C64 && c->nb == 1 &&
+        (rc = knob(&scd_tuning::near_kernel, {SCD_NEAR_CUDA_CORES, SCD_NEAR_TENSOR_SPLIT, SCD_NEAR_TENSOR_MERGED})))
+        return rc;
+    if ((rc = knob(&scd_tuning::fft_passes, {SCD_FFT_PASSES_FUSED_YZ, SCD_FFT_PASSES_THREE}))) return rc;
+    if (nrhs > 8 && (rc = knob(&scd_tuning::scatter_span, {0, 8, 16}))) return rc;
+    if (nrhs > 4 && (rc = knob(&scd_tuning::gather_span, {0, 4, 8, 16}))) return rc;
+    put_tuning(c, best);
+    best.matvec_ms = best_ms;
+    best.default_ms = default_ms;
+    *out = best;
+    return SCD_OK;
 }
 
 int scd_column_latency(scd_ctx *c, int32_t ncol, double *ms) {

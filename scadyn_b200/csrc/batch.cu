@@ -956,16 +956,15 @@ static int launch_tick(scd_ctx *c, BatchBuffers &bb, int ns, int nact, int m, in
 // precision 0: restarted GMRES(m) in complex128 to `tol` (the reference's
 // algorithm); 1: FP64 iterative refinement to `tol` around complex64
 // GMRES(m) inner solves to `inner_tol`, at most `max_outer` outer steps.
-int batch_solve(scd_ctx *c, int ncol, const cd *const *rhs_cols, cd *X, double tol, int m, int cycles, int ns,
-                int *iters, int *conv_out, int *status_out, double *relres_out, int precision, double inner_tol,
-                int max_outer) {
+int batch_run(scd_ctx *c, ColumnSource &src, double tol, int m, int cycles, int ns, int precision, double inner_tol,
+              int max_outer) {
     NvtxRange range(precision == SCD_PREC_MIXED ? "batch solve (mixed)" : "batch solve (fp64)");
     if (!c->batch) c->batch = new BatchBuffers();
     BatchBuffers &bb = *(BatchBuffers *)c->batch;
     const int mixed = precision == SCD_PREC_MIXED ? 1 : 0;
     if (m < 1 || m > SCD_M_MAX) return set_error(c, SCD_BAD_ARG, "m = %d outside 1..%d", m, SCD_M_MAX);
     if (ns > NSMAX) ns = NSMAX;
-    if (ns > ncol) ns = ncol;
+    if (ns < 1) ns = 1;
     int rc = batch_prepare(c, ns, m, mixed, bb);
     if (rc) return rc;
     if (mixed) {
@@ -983,53 +982,49 @@ int batch_solve(scd_ctx *c, int ncol, const cd *const *rhs_cols, cd *X, double t
     Slot *hs = bb.h_slots;
     std::memset(hs, 0, sizeof(Slot) * ns);
     for (int s = 0; s < ns; ++s) { hs[s].mode = SLOT_FREE; hs[s].col = -1; }
-    int next = 0, finished = 0, worst = SCD_OK;
-    using clk = std::chrono::steady_clock;
-    const auto t0 = clk::now();
-    auto now_ms = [&]() { return std::chrono::duration<double, std::milli>(clk::now() - t0).count(); };
-    std::vector<double> t_in(ncol, 0.0);
-    c->col_latency_ms.assign(ncol, 0.0);
+    std::vector<cd *> xout(ns, nullptr);        // where each slot's solution goes
     const double gm_tol = mixed ? inner_tol : tol;
-    while (finished < ncol) {
+    while (true) {
         bool inner = false, resid = false, upd = false;
+        int busy = 0;
         for (int s = 0; s < ns; ++s) {
             if (hs[s].mode == SLOT_DONE) {
-                const int col = hs[s].col;
                 const cd *xs = mixed ? bb.x64 + (size_t)s * n : (const cd *)bb.x + (size_t)s * n;
-                cudaMemcpyAsync(X + (size_t)col * n, xs, sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
-                if (iters) iters[col] = hs[s].iters;
-                if (conv_out) conv_out[col] = hs[s].conv;
-                if (status_out) status_out[col] = hs[s].status;
-                if (relres_out) relres_out[col] = mixed ? hs[s].relres : hs[s].error;
-                c->col_latency_ms[col] = now_ms() - t_in[col];
-                if (hs[s].status != SCD_OK) worst = hs[s].status;
-                else if (!hs[s].conv && worst == SCD_OK) worst = SCD_NOT_CONVERGED;
+                cudaMemcpyAsync(xout[s], xs, sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
                 c->n_arn += hs[s].iters;
                 c->n_matvec += hs[s].iters + hs[s].cycle;
-                ++finished;
+                src.finished(hs[s].col, hs[s].iters, hs[s].conv, hs[s].status, mixed ? hs[s].relres : hs[s].error);
                 std::memset(&hs[s], 0, sizeof(Slot));
                 hs[s].mode = SLOT_FREE;
                 hs[s].col = -1;
+                xout[s] = nullptr;
             }
-            if (hs[s].mode == SLOT_FREE && next < ncol) {
+            const cd *rhs = nullptr;
+            int tag = -1;
+            if (hs[s].mode == SLOT_FREE && src.next(&rhs, &xout[s], &tag)) {
                 std::memset(&hs[s], 0, sizeof(Slot));
                 if (mixed) {
-                    cudaMemcpyAsync(bb.b64 + (size_t)s * n, rhs_cols[next], sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
-                    cudaMemcpyAsync(bb.x64 + (size_t)s * n, rhs_cols[next], sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
+                    cudaMemcpyAsync(bb.b64 + (size_t)s * n, rhs, sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
+                    cudaMemcpyAsync(bb.x64 + (size_t)s * n, rhs, sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
                     hs[s].mode = SLOT_RESID;
                 } else {
-                    cudaMemcpyAsync((cd *)bb.rhs + (size_t)s * n, rhs_cols[next], sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
-                    cudaMemcpyAsync((cd *)bb.x + (size_t)s * n, rhs_cols[next], sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
+                    cudaMemcpyAsync((cd *)bb.rhs + (size_t)s * n, rhs, sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
+                    cudaMemcpyAsync((cd *)bb.x + (size_t)s * n, rhs, sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st);
                     hs[s].mode = SLOT_START;
                 }
-                t_in[next] = now_ms();
-                hs[s].col = next++;
+                hs[s].col = tag;
             }
             if (hs[s].mode == SLOT_INNER_DONE) { hs[s].mode = SLOT_RESID; hs[s].upd = 1; upd = true; }
             if (hs[s].mode == SLOT_RESID) resid = true;
             if (hs[s].mode == SLOT_START || hs[s].mode == SLOT_ARNOLDI) inner = true;
+            if (hs[s].mode != SLOT_FREE) ++busy;
         }
-        if (finished >= ncol) break;
+        if (busy == 0) {
+            // every slot idle: the source may still bring columns (a served pool)
+            if ((rc = check_cuda(c, cudaStreamSynchronize(c->st), "batch idle"))) return rc;
+            if (!src.wait_more()) break;
+            continue;
+        }
         if (!inner && !resid) return set_error(c, SCD_CUDA_ERROR, "batch solver stalled");
         // compacted matvec columns: only slots that need A x this tick
         int nact = 0, nres = 0;
@@ -1064,7 +1059,60 @@ int batch_solve(scd_ctx *c, int ncol, const cd *const *rhs_cols, cd *X, double t
         for (int s = 0; s < ns; ++s)
             if (hs[s].status == SCD_TIMEOUT) return set_error(c, SCD_TIMEOUT, "grid barrier wait expired in the batch solver");
     }
-    rc = check_cuda(c, cudaStreamSynchronize(c->st), "batch end");
+    return check_cuda(c, cudaStreamSynchronize(c->st), "batch end");
+}
+
+namespace {
+// the columns of one call, in order
+struct ArraySource final : ColumnSource {
+    scd_ctx *c;
+    int ncol, next_col = 0;
+    const cd *const *rhs;
+    cd *X;
+    int *iters, *conv, *status;
+    double *relres;
+    int worst = SCD_OK;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    std::vector<double> t_in;
+    double now_ms() const {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    bool next(const cd **r, cd **xout, int *tag) override {
+        if (next_col >= ncol) return false;
+        *r = rhs[next_col];
+        *xout = X + (size_t)next_col * c->n;
+        *tag = next_col;
+        t_in[next_col] = now_ms();
+        ++next_col;
+        return true;
+    }
+    void finished(int col, int it, int cv, int st, double rr) override {
+        if (iters) iters[col] = it;
+        if (conv) conv[col] = cv;
+        if (status) status[col] = st;
+        if (relres) relres[col] = rr;
+        c->col_latency_ms[col] = now_ms() - t_in[col];
+        if (st != SCD_OK) worst = st;
+        else if (!cv && worst == SCD_OK) worst = SCD_NOT_CONVERGED;
+    }
+};
+}  // namespace
+
+int batch_solve(scd_ctx *c, int ncol, const cd *const *rhs_cols, cd *X, double tol, int m, int cycles, int ns,
+                int *iters, int *conv_out, int *status_out, double *relres_out, int precision, double inner_tol,
+                int max_outer) {
+    ArraySource src;
+    src.c = c;
+    src.ncol = ncol;
+    src.rhs = rhs_cols;
+    src.X = X;
+    src.iters = iters;
+    src.conv = conv_out;
+    src.status = status_out;
+    src.relres = relres_out;
+    src.t_in.assign(ncol, 0.0);
+    c->col_latency_ms.assign(ncol, 0.0);
+    const int rc = batch_run(c, src, tol, m, cycles, std::min(ns, ncol), precision, inner_tol, max_outer);
     if (rc) return rc;
-    return worst;
+    return src.worst;
 }

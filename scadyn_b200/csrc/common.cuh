@@ -223,6 +223,19 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *e
     atomicExch(err, 1);
     return false;
 }
+// The same wait, also ended (false, nothing recorded) as soon as another
+// thread of the CTA raises *stop: once one wait of a pipeline has given up,
+// the others stop waiting for copies that will not be issued.
+__device__ __forceinline__ bool mbar_wait_or(uint64_t *bar, uint32_t parity, int *err, const volatile int *stop,
+                                             long long limit = (1LL << 22)) {
+    for (long long k = 0; k < limit; ++k) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (*stop) return false;
+        if (k > 16) __nanosleep(64);
+    }
+    atomicExch(err, 1);
+    return false;
+}
 // arrive on *bar once every cp.async issued so far by this thread has landed
 // (the barrier's expected count includes this arrival)
 __device__ __forceinline__ void cp_async_arrive_noinc(uint64_t *bar) {

@@ -90,6 +90,16 @@ struct scd_ctx {
     // Green octant (Hx*Hy*Hz), pre-scaled by 1/(Px*Py*Pz)
     bool have_green = false;
     cd *d_Fo = nullptr;
+    // the octant transposed for the fused y-z FFT pass (fft_yz.cuh), FP64 and
+    // complex64, rebuilt after every new Green spectrum
+    bool yz_on = true;                   // take the fused y-z pass where its lengths allow
+    // right-hand sides per warp of the anterpolation and interpolation
+    // kernels (0 = all of a call's; smaller spans give more warps in flight,
+    // larger ones reuse the projector rows from L1)
+    int scatter_span = 0, gather_span = 0;
+    bool fyz_ready = false, fyz_ready_f = false;
+    cd *d_Fyz = nullptr;
+    cf *f_Fyz = nullptr;
 
     // near zone
     bool have_near = false;
@@ -200,6 +210,23 @@ int near_mma_prepare(scd_ctx *c);
 void near_mma_run(scd_ctx *c, const cf *x, int nrhs, const int *done);
 
 // ---- batched column solves (batch.cu) ----
+// Where the batched solver's columns come from: the array of one call, or
+// the queue of a served operator pool that arriving requests keep filling.
+// All calls come from the thread that runs the solver.
+struct ColumnSource {
+    virtual ~ColumnSource() = default;
+    // the next column to admit into a free slot: its right-hand side (device,
+    // slot order), where its solution goes, and a tag; false if none is ready
+    virtual bool next(const cd **rhs, cd **xout, int *tag) = 0;
+    // the column `tag` left its slot; its solution copy is queued on the
+    // context's stream
+    virtual void finished(int tag, int iters, int conv, int status, double relres) = 0;
+    // every slot is idle and the stream drained: block until columns may be
+    // ready (true) or no more will come (false, the solver returns)
+    virtual bool wait_more() { return false; }
+};
+int batch_run(scd_ctx *c, ColumnSource &src, double tol, int m, int cycles, int ns, int precision, double inner_tol,
+              int max_outer);
 void batch_free(scd_ctx *c);
 int batch_solve(scd_ctx *c, int ncol, const cd *const *rhs_cols, cd *X, double tol, int m, int cycles, int ns,
                 int *iters, int *conv, int *status, double *relres, int precision, double inner_tol, int max_outer);

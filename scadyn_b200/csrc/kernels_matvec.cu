@@ -17,6 +17,7 @@
 #include "ctx.h"
 #include "fft_mixed.cuh"
 #include "fft_reg.cuh"
+#include "fft_yz.cuh"
 #include "linear_basis.h"
 
 namespace {
@@ -45,23 +46,24 @@ __global__ void k_permute_out(const cd *__restrict__ xs, cd *__restrict__ xo, co
 
 // ---------------------------------------------------------------- scatter
 // Anterpolation (sparse_T_matmul, src/sparse.f90:13-43), one warp per
-// (cube, group of SC_RG right-hand sides): lane j < 27 accumulates the four
-// box-node sums of node j over the cube's tets (projector values are read
-// once per group; the groups of right-hand sides are the grid's y index, so
-// every cube has nrhs/SC_RG warps in flight).  Projectors are stored
-// P[(g*27 + j)*T + slot].  bpart[((r*ncubes + c)*4 + g)*27 + j].
+// (cube, span of rspan right-hand sides): lane j < 27 accumulates the four
+// box-node sums of node j over the cube's tets, SC_RG right-hand sides at a
+// time (projector values are read once per group of SC_RG and stay in L1 for
+// the next group of the span).  The spans are the grid's y index; rspan is a
+// multiple of SC_RG.  Projectors are stored P[(g*27 + j)*T + slot].
+// bpart[((r*ncubes + c)*4 + g)*27 + j].
 template <typename C, int SC_RG>
 __global__ void __launch_bounds__(32 * WARPS_PER_CTA)
 k_scatter(const C *__restrict__ x, long long ld, const C *__restrict__ P, int T,
-          const int *__restrict__ cube_off, int ncubes, C *__restrict__ bpart, const int *skip, int nrhs) {
+          const int *__restrict__ cube_off, int ncubes, C *__restrict__ bpart, const int *skip, int nrhs, int rspan) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int c = blockIdx.x * WARPS_PER_CTA + warp;
     if (c >= ncubes || lane >= 27) return;
     const int s0 = cube_off[c], s1 = cube_off[c + 1];
     const C *P0 = P + (size_t)lane * T, *PX = P + (size_t)(27 + lane) * T;
     const C *PY = P + (size_t)(54 + lane) * T, *PZ = P + (size_t)(81 + lane) * T;
-    {
-        const int r0 = blockIdx.y * SC_RG;
+    const int rend = min(nrhs, (int)(blockIdx.y + 1) * rspan);
+    for (int r0 = blockIdx.y * rspan; r0 < rend; r0 += SC_RG) {
         C acc[SC_RG][4];
 #pragma unroll
         for (int q = 0; q < SC_RG; ++q) acc[q][0] = acc[q][1] = acc[q][2] = acc[q][3] = czero<C>();
@@ -235,8 +237,11 @@ __device__ __forceinline__ C node_value(const C *__restrict__ bp, const GridDims
 }
 
 // X forward: lines (y < Ny, z < Nz) of grid (g, r); node assembly on load,
-// zero padding x >= Nx.  W[(rg)][(z*Py + y)*Px + x]
-template <int P, typename Cx>
+// zero padding x >= Nx.  W[(rg)][(z*Py + y)*Px + x] for the three-pass
+// y/z chain, or (TL) the fused y-z pass's layout Wt[rg][x][z][y] (fft_yz.cuh):
+// a CTA's lines are consecutive (z, y), so for every x its outputs are one
+// contiguous run.
+template <int P, typename Cx, bool TL>
 __global__ void __launch_bounds__(FftCfg<P, Cx>::THREADS)
 k_fft_x_fwd(const Cx *__restrict__ bpart, Cx *__restrict__ W, const Cx *__restrict__ twg, GridDims G, const int *done) {
     if (done && done[blockIdx.y >> 2]) return;
@@ -261,12 +266,20 @@ k_fft_x_fwd(const Cx *__restrict__ bpart, Cx *__restrict__ W, const Cx *__restri
     __syncthreads();
     const int l = threadIdx.x / Cf::TPL, t = threadIdx.x - l * Cf::TPL;
     fft_line_any<P, false, Cx>(sh + l * Cf::LS, tw, t);
-    Cx *Wr = W + (long long)rg * G.Px * G.Py * G.Nz;
-    for (int e = threadIdx.x; e < Cf::LPB * P; e += blockDim.x) {
-        const int ll = e / P, x = e - ll * P, line = line0 + ll;
-        if (line < nlines) {
-            const int y = line % G.Ny, z = line / G.Ny;
-            Wr[((long long)z * G.Py + y) * G.Px + x] = sh[ll * Cf::LS + pidx(x)];
+    if constexpr (TL) {
+        Cx *Wr = W + (long long)rg * P * nlines;
+        for (int e = threadIdx.x; e < Cf::LPB * P; e += blockDim.x) {
+            const int x = e / Cf::LPB, ll = e - x * Cf::LPB, line = line0 + ll;
+            if (line < nlines) Wr[(long long)x * nlines + line] = sh[ll * Cf::LS + pidx(x)];
+        }
+    } else {
+        Cx *Wr = W + (long long)rg * G.Px * G.Py * G.Nz;
+        for (int e = threadIdx.x; e < Cf::LPB * P; e += blockDim.x) {
+            const int ll = e / P, x = e - ll * P, line = line0 + ll;
+            if (line < nlines) {
+                const int y = line % G.Ny, z = line / G.Ny;
+                Wr[((long long)z * G.Py + y) * G.Px + x] = sh[ll * Cf::LS + pidx(x)];
+            }
         }
     }
 }
@@ -345,8 +358,9 @@ k_fft_z(Cx *__restrict__ W, const Cx *__restrict__ Fo, const Cx *__restrict__ tw
 }
 
 // X inverse: lines (y < Ny, z < Nz), keep x < Nx, write the result grid
-// R[(rg)][(z*Ny + y)*Nx + x]
-template <int P, typename Cx>
+// R[(rg)][(z*Ny + y)*Nx + x]; the input in the three-pass layout or (TL) the
+// fused y-z pass's Wt[rg][x][z][y]
+template <int P, typename Cx, bool TL>
 __global__ void __launch_bounds__(FftCfg<P, Cx>::THREADS)
 k_fft_x_inv(const Cx *__restrict__ W, Cx *__restrict__ R, const Cx *__restrict__ twg, GridDims G, const int *done) {
     if (done && done[blockIdx.y >> 2]) return;
@@ -357,15 +371,23 @@ k_fft_x_inv(const Cx *__restrict__ W, Cx *__restrict__ R, const Cx *__restrict__
     for (int i = threadIdx.x; i < P; i += blockDim.x) tw[i] = twg[i];
     const int nlines = G.Ny * G.Nz;
     const int line0 = blockIdx.x * Cf::LPB;
-    const Cx *Wr = W + (long long)rg * G.Px * G.Py * G.Nz;
-    for (int e = threadIdx.x; e < Cf::LPB * P; e += blockDim.x) {
-        const int l = e / P, x = e - l * P, line = line0 + l;
-        Cx v = czero<Cx>();
-        if (line < nlines) {
-            const int y = line % G.Ny, z = line / G.Ny;
-            v = Wr[((long long)z * G.Py + y) * G.Px + x];
+    if constexpr (TL) {
+        const Cx *Wr = W + (long long)rg * P * nlines;
+        for (int e = threadIdx.x; e < Cf::LPB * P; e += blockDim.x) {
+            const int x = e / Cf::LPB, l = e - x * Cf::LPB, line = line0 + l;
+            sh[l * Cf::LS + pidx(x)] = line < nlines ? Wr[(long long)x * nlines + line] : czero<Cx>();
         }
-        sh[l * Cf::LS + pidx(x)] = v;
+    } else {
+        const Cx *Wr = W + (long long)rg * G.Px * G.Py * G.Nz;
+        for (int e = threadIdx.x; e < Cf::LPB * P; e += blockDim.x) {
+            const int l = e / P, x = e - l * P, line = line0 + l;
+            Cx v = czero<Cx>();
+            if (line < nlines) {
+                const int y = line % G.Ny, z = line / G.Ny;
+                v = Wr[((long long)z * G.Py + y) * G.Px + x];
+            }
+            sh[l * Cf::LS + pidx(x)] = v;
+        }
     }
     __syncthreads();
     const int l = threadIdx.x / Cf::TPL, t = threadIdx.x - l * Cf::TPL;
@@ -410,7 +432,7 @@ k_fft_x_inv(const Cx *__restrict__ W, Cx *__restrict__ R, const Cx *__restrict__
 // not depend on the batch it is solved in.
 constexpr int NZ_QMAX = 4;             // quads of right-hand sides per pass
 constexpr int NZ_SLOTS = 8;                 // tiles in flight at most (mbarrier pairs)
-constexpr int NZ_META = 256;                // bytes of barriers and ring offsets
+constexpr int NZ_META = 272;                // bytes of barriers, ring offsets and the stop flag
 constexpr size_t NZ_SMEM_2CTA = 113 * 1024; // dynamic shared memory per CTA that lets two CTAs share an SM
 constexpr size_t NZ_SMEM_4CTA = 56 * 1024;  // ... four CTAs
 // With one right-hand side a tile's sums are short dependent chains, so the
@@ -506,6 +528,10 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS, NZ_MIN_CTAS<U>) k_near_groups(
     int *toff = reinterpret_cast<int *>(nz_sh + 16 * NZ_SLOTS);
     int *tn2 = toff + NZ_SLOTS;
     long long *tcol = reinterpret_cast<long long *>(nz_sh + 24 * NZ_SLOTS);
+    // raised by the first wait that gives up: the producer issues no more
+    // copies, the consumers skip the remaining tiles (still arriving on their
+    // barriers), and the kernel returns with a.err set
+    volatile int *stop = reinterpret_cast<volatile int *>(nz_sh + 32 * NZ_SLOTS);
     C *const X1 = reinterpret_cast<C *>(nz_sh + NZ_META);                 // x(g)
     unsigned char *const ring = nz_sh + NZ_META + a.x1_bytes;
     const ST *data = static_cast<const ST *>(a.data);
@@ -527,6 +553,7 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS, NZ_MIN_CTAS<U>) k_near_groups(
             mbar_init(&full[k], 1);              // the producer's arrive (with the tile's bytes)
             mbar_init(&empty[k], ncw);
         }
+        *stop = 0;
         mbar_fence_init();
     }
     __syncthreads();
@@ -541,17 +568,20 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS, NZ_MIN_CTAS<U>) k_near_groups(
             uint32_t head = 0, used = 0;
             uint32_t resv[NZ_SLOTS] = {};
             int oldest = 0, count = 0, ord = 0;
+            int last[NZ_SLOTS];                  // latest tile issued into each slot
+            for (int k = 0; k < NZ_SLOTS; ++k) last[k] = -1;
+            bool halt = false;
             auto release_oldest = [&]() {
                 const int k = oldest % NZ_SLOTS;
-                mbar_wait(&empty[k], (uint32_t)((oldest / NZ_SLOTS) & 1), a.err);
+                if (!mbar_wait_or(&empty[k], (uint32_t)((oldest / NZ_SLOTS) & 1), a.err, stop)) halt = true;
                 used -= resv[k];
                 ++oldest;
                 --count;
             };
-            for (int r0 = 0; r0 < a.nrhs; r0 += PS) {
+            for (int r0 = 0; r0 < a.nrhs && !halt; r0 += PS) {
                 const C *xp = xT + (long long)(r0 / PS) * a.n * RG;
-                while (count > 0) release_oldest();   // X1 is rewritten: the previous pass must be done
-                for (int t = t0; t < t1; ++t, ++ord) {
+                while (count > 0 && !halt) release_oldest();   // X1 is rewritten: the previous pass must be done
+                for (int t = t0; t < t1 && !halt; ++t, ++ord) {
                     const NearTile &tl = a.tiles[t];
                     const uint32_t mb = (uint32_t)(tile_elems(tl.n1, tl.n2) * (long long)sizeof(ST));
                     const uint32_t xb = (uint32_t)(3 * tl.n2 * RG * sizeof(C));
@@ -559,7 +589,8 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS, NZ_MIN_CTAS<U>) k_near_groups(
                     const uint32_t S = mb + xb;
                     bool fit = head + S <= R;
                     uint32_t res = fit ? S : (R - head) + S;
-                    while (count > 0 && (count == NZ_SLOTS || used + res > R)) release_oldest();
+                    while (count > 0 && !halt && (count == NZ_SLOTS || used + res > R)) release_oldest();
+                    if (halt || *stop) { halt = true; break; }
                     if (count == 0) { head = 0; used = 0; fit = true; res = S; }
                     const uint32_t st = fit ? head : 0u;
                     const int k = ord % NZ_SLOTS;
@@ -573,8 +604,16 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS, NZ_MIN_CTAS<U>) k_near_groups(
                     head = st + S;
                     used += res;
                     resv[k] = res;
+                    last[k] = ord;
                     ++count;
                 }
+            }
+            if (halt) {
+                // a wait gave up: tell the consumers, then let every copy
+                // still landing in the ring finish before the CTA exits
+                *stop = 1;
+                for (int k = 0; k < NZ_SLOTS; ++k)
+                    if (last[k] >= 0) mbar_wait(&full[k], (uint32_t)((last[k] / NZ_SLOTS) & 1), a.err);
             }
         }
         return;
@@ -599,7 +638,14 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS, NZ_MIN_CTAS<U>) k_near_groups(
         C (&acc)[3][U] = accs[0];
         for (int t = t0; t < t1; ++t, ++ord) {
             const int kslot = ord % NZ_SLOTS;
-            mbar_wait(&full[kslot], (uint32_t)((ord / NZ_SLOTS) & 1), a.err);
+            bool ok = !*stop && mbar_wait_or(&full[kslot], (uint32_t)((ord / NZ_SLOTS) & 1), a.err, stop);
+            ok = __all_sync(0xffffffffu, ok);   // the warp skips or computes as one (shuffles below)
+            if (!ok) {
+                *stop = 1;
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&empty[kslot]);
+                continue;
+            }
             const int n2 = tn2[kslot];
             const int tof = toff[kslot];
             const long long tcoff = tcol[kslot];
@@ -756,19 +802,20 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS, NZ_MIN_CTAS<U>) k_near_groups(
 // ---------------------------------------------------------------- gather
 // Interpolation (sparse_eps_matmul, src/sparse.f90:47-77) and final
 // assembly (src/gmres_module.f90:148-170), one warp per (near-zone group,
-// group of GA_RG right-hand sides), one lane per tet: the 27 box-node values
-// of the four result grids are staged in shared memory for the warp's
-// right-hand sides, each lane forms its tet's six 27-term sums from the
-// projector rows P[(g*27 + j)*T + slot] (coalesced across lanes), adds the
-// group's near-zone partial slots in slot order and writes
-// Ax = near + (Y2 - k^2 Y).  The groups of right-hand sides are the grid's y
-// index, so a near-zone group has nrhs/GA_RG warps in flight.
+// span of rspan right-hand sides), one lane per tet, GA_RG right-hand sides
+// at a time: the 27 box-node values of the four result grids are staged in
+// shared memory, each lane forms its tet's six 27-term sums from the
+// projector rows P[(g*27 + j)*T + slot] (coalesced across lanes; they stay
+// in L1 for the next group of the span), adds the group's near-zone partial
+// slots in slot order and writes Ax = near + (Y2 - k^2 Y).  The spans are the
+// grid's y index; rspan is a multiple of GA_RG.
 template <typename C, int GA_RG>
 __global__ void __launch_bounds__(32 * WARPS_PER_CTA)
 k_gather(const C *__restrict__ Rg, const C *__restrict__ P, int T, const int *__restrict__ grp_off,
          const int *__restrict__ grp_cube, int ngroups, GridDims G, typename CReal<C>::type k2,
          const C *__restrict__ part, long long part_len, const long long *__restrict__ pslot_base,
-         const int *__restrict__ pslot_cnt, C *__restrict__ y, long long ld, const int *skip, int nrhs) {
+         const int *__restrict__ pslot_cnt, C *__restrict__ y, long long ld, const int *skip, int nrhs,
+         int rspan) {
     __shared__ C Rs[WARPS_PER_CTA][GA_RG][4][27];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int gq = blockIdx.x * WARPS_PER_CTA + warp;
@@ -785,8 +832,8 @@ k_gather(const C *__restrict__ Rg, const C *__restrict__ P, int T, const int *__
         const int a = lane % 3, b = (lane / 3) % 3, cc = lane / 9;
         node = ((long long)(2 * bz + cc) * G.Ny + (2 * by + b)) * G.Nx + (2 * bx + a);
     }
-    {
-        const int r0 = blockIdx.y * GA_RG;
+    const int rend = min(nrhs, (int)(blockIdx.y + 1) * rspan);
+    for (int r0 = blockIdx.y * rspan; r0 < rend; r0 += GA_RG) {
         __syncwarp();
         if (lane < 27) {
 #pragma unroll
@@ -869,6 +916,7 @@ template <typename C> struct Res;
 template <> struct Res<cd> {
     static const cd *P(scd_ctx *c) { return c->d_P; }
     static const cd *Fo(scd_ctx *c) { return c->d_Fo; }
+    static const cd *Fyz(scd_ctx *c) { return c->d_Fyz; }
     static const cd *tw(scd_ctx *c, int a) { return c->d_tw[a]; }
     static cd *bpart(scd_ctx *c) { return c->d_bpart; }
     static cd *W(scd_ctx *c) { return c->d_W; }
@@ -879,6 +927,7 @@ template <> struct Res<cd> {
 template <> struct Res<cf> {
     static const cf *P(scd_ctx *c) { return c->f_P; }
     static const cf *Fo(scd_ctx *c) { return c->f_Fo; }
+    static const cf *Fyz(scd_ctx *c) { return c->f_Fyz; }
     static const cf *tw(scd_ctx *c, int a) { return c->f_tw[a]; }
     static cf *bpart(scd_ctx *c) { return c->f_bpart; }
     static cf *W(scd_ctx *c) { return c->f_W; }
@@ -888,10 +937,11 @@ template <> struct Res<cf> {
 };
 
 template <int P, typename C>
-void fft_x_fwd_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const C *tw) {
+void fft_x_fwd_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const C *tw, bool tl) {
     using Cf = FftCfg<P, C>;
     dim3 grid((G.Ny * G.Nz + Cf::LPB - 1) / Cf::LPB, nrg);
-    k_fft_x_fwd<P, C><<<grid, Cf::THREADS, 0, c->st>>>(Res<C>::bpart(c), Res<C>::W(c), tw, G, done);
+    if (tl) k_fft_x_fwd<P, C, true><<<grid, Cf::THREADS, 0, c->st>>>(Res<C>::bpart(c), Res<C>::W(c), tw, G, done);
+    else k_fft_x_fwd<P, C, false><<<grid, Cf::THREADS, 0, c->st>>>(Res<C>::bpart(c), Res<C>::W(c), tw, G, done);
 }
 template <int P, bool INV, typename C>
 void fft_y_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const C *tw) {
@@ -906,10 +956,88 @@ void fft_z_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const C *t
     k_fft_z<P, C><<<grid, Cf::THREADS, 0, c->st>>>(Res<C>::W(c), Res<C>::Fo(c), tw, G, done);
 }
 template <int P, typename C>
-void fft_x_inv_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const C *tw) {
+void fft_x_inv_t(scd_ctx *c, const GridDims &G, int nrg, const int *done, const C *tw, bool tl) {
     using Cf = FftCfg<P, C>;
     dim3 grid((G.Ny * G.Nz + Cf::LPB - 1) / Cf::LPB, nrg);
-    k_fft_x_inv<P, C><<<grid, Cf::THREADS, 0, c->st>>>(Res<C>::W(c), Res<C>::R(c), tw, G, done);
+    if (tl) k_fft_x_inv<P, C, true><<<grid, Cf::THREADS, 0, c->st>>>(Res<C>::W(c), Res<C>::R(c), tw, G, done);
+    else k_fft_x_inv<P, C, false><<<grid, Cf::THREADS, 0, c->st>>>(Res<C>::W(c), Res<C>::R(c), tw, G, done);
+}
+
+// the fused y-z pass (fft_yz.cuh) for one (PY, PZ) pair
+template <int PY, int PZ, typename C>
+void fft_yz_t(scd_ctx *c, const GridDims &G, int nrg, const int *done) {
+    if constexpr (YzLine<PY>::OK && YzLine<PZ>::OK) {
+        YzDims D;
+        D.Nx = G.Nx; D.Ny = G.Ny; D.Nz = G.Nz; D.NzR = yz_round8(G.Nz);
+        D.Px = G.Px; D.Hx = G.Hx; D.Hy = G.Hy; D.Hz = G.Hz;
+        const size_t sh = sizeof(C) * (size_t)yz_smem_elems<PY, PZ>(D.NzR);
+        cudaFuncSetAttribute(k_fft_yz<PY, PZ, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+        k_fft_yz<PY, PZ, C><<<dim3(G.Px, nrg), YZ_THREADS, sh, c->st>>>(Res<C>::W(c), Res<C>::Fyz(c), Res<C>::tw(c, 1),
+                                                                       Res<C>::tw(c, 2), D, done);
+    }
+}
+
+template <int PY, typename C>
+void fft_yz_pz(scd_ctx *c, const GridDims &G, int nrg, const int *done) {
+    switch (G.Pz) {
+        case 64: fft_yz_t<PY, 64, C>(c, G, nrg, done); break;
+        case 80: fft_yz_t<PY, 80, C>(c, G, nrg, done); break;
+        case 96: fft_yz_t<PY, 96, C>(c, G, nrg, done); break;
+        case 128: fft_yz_t<PY, 128, C>(c, G, nrg, done); break;
+        case 192: fft_yz_t<PY, 192, C>(c, G, nrg, done); break;
+        default: break;
+    }
+}
+
+template <typename C>
+void fft_yz(scd_ctx *c, const GridDims &G, int nrg, const int *done) {
+    switch (G.Py) {
+        case 64: fft_yz_pz<64, C>(c, G, nrg, done); break;
+        case 80: fft_yz_pz<80, C>(c, G, nrg, done); break;
+        case 96: fft_yz_pz<96, C>(c, G, nrg, done); break;
+        case 128: fft_yz_pz<128, C>(c, G, nrg, done); break;
+        case 192: fft_yz_pz<192, C>(c, G, nrg, done); break;
+        default: break;
+    }
+}
+
+constexpr bool yz_len_ok(int P) { return P == 64 || P == 80 || P == 96 || P == 128 || P == 192; }
+
+// shared-memory bytes of the fused y-z pass for the context's lengths
+template <typename C>
+size_t yz_smem_bytes(const scd_ctx *c) {
+    const int NzR = yz_round8(c->Nz);
+    auto lines = [](int P) { return (P == 64 || P == 128 || P % 64 == 0) ? YZ_THREADS / 8 : YZ_THREADS / 4; };
+    auto ls = [](int P) { return P + (P >> 4) + 1; };
+    return sizeof(C) * (size_t)(c->Py + c->Pz + (long long)NzR * ls(c->Py) + (long long)lines(c->Pz) * ls(c->Pz));
+}
+
+// whether the complex64 (or FP64) chain takes the fused y-z pass: both lengths
+// have warp-synchronous line transforms and the CTA fits shared memory
+template <typename C>
+bool use_yz(const scd_ctx *c) {
+    if (!c->yz_on || !yz_len_ok(c->Py) || !yz_len_ok(c->Pz)) return false;
+    return yz_smem_bytes<C>(c) <= (size_t)(227 * 1024);
+}
+
+// the transposed Green octant of the fused pass, built from Fo once per
+// Green spectrum; false (three-pass chain) if it cannot be allocated
+template <typename C>
+bool ensure_fyz(scd_ctx *c) {
+    constexpr bool single = std::is_same<C, cf>::value;
+    bool &ready = single ? c->fyz_ready_f : c->fyz_ready;
+    if (ready) return true;
+    C *&buf = *reinterpret_cast<C **>(single ? (void *)&c->f_Fyz : (void *)&c->d_Fyz);
+    const long long no = (long long)c->Hx * c->Hy * c->Hz;
+    if (!buf && cudaMalloc((void **)&buf, sizeof(C) * (size_t)no) != cudaSuccess) {
+        cudaGetLastError();
+        buf = nullptr;
+        return false;
+    }
+    k_green_yz<C><<<(unsigned)std::min<long long>((no + 255) / 256, 4096), 256, 0, c->st>>>(Res<C>::Fo(c), buf, c->Hx,
+                                                                                          c->Hy, c->Hz);
+    ready = true;
+    return true;
 }
 
 #define SCD_DISPATCH_P(PV, CALL)                     \
@@ -933,33 +1061,44 @@ void fft_chain_t(scd_ctx *c, const C *x, int nrhs, const int *done) {
     {
         const unsigned gx = (unsigned)((c->ncubes + WARPS_PER_CTA - 1) / WARPS_PER_CTA);
         const C *P = Res<C>::P(c);
-        if (nrhs >= 8)
-            k_scatter<C, 8><<<dim3(gx, (nrhs + 7) / 8), 32 * WARPS_PER_CTA, 0, c->st>>>(
-                x, c->n, P, c->T, c->d_cube_off, c->ncubes, Res<C>::bpart(c), done, nrhs);
-        else if (nrhs >= 4)
-            k_scatter<C, 4><<<dim3(gx, (nrhs + 3) / 4), 32 * WARPS_PER_CTA, 0, c->st>>>(
-                x, c->n, P, c->T, c->d_cube_off, c->ncubes, Res<C>::bpart(c), done, nrhs);
-        else
-            k_scatter<C, 1><<<dim3(gx, nrhs), 32 * WARPS_PER_CTA, 0, c->st>>>(
-                x, c->n, P, c->T, c->d_cube_off, c->ncubes, Res<C>::bpart(c), done, nrhs);
+        // spans of right-hand sides per warp (c->scatter_span, 0 = all of them)
+        auto span = [&](int rg) { int sp = c->scatter_span > 0 ? c->scatter_span : nrhs; return (sp + rg - 1) / rg * rg; };
+        if (nrhs >= 8) {
+            const int sp = span(8);
+            k_scatter<C, 8><<<dim3(gx, (nrhs + sp - 1) / sp), 32 * WARPS_PER_CTA, 0, c->st>>>(
+                x, c->n, P, c->T, c->d_cube_off, c->ncubes, Res<C>::bpart(c), done, nrhs, sp);
+        } else if (nrhs >= 4) {
+            const int sp = span(4);
+            k_scatter<C, 4><<<dim3(gx, (nrhs + sp - 1) / sp), 32 * WARPS_PER_CTA, 0, c->st>>>(
+                x, c->n, P, c->T, c->d_cube_off, c->ncubes, Res<C>::bpart(c), done, nrhs, sp);
+        } else {
+            const int sp = span(1);
+            k_scatter<C, 1><<<dim3(gx, (nrhs + sp - 1) / sp), 32 * WARPS_PER_CTA, 0, c->st>>>(
+                x, c->n, P, c->T, c->d_cube_off, c->ncubes, Res<C>::bpart(c), done, nrhs, sp);
+        }
     }
     const int nrg = 4 * nrhs;
-#define XF(PP) fft_x_fwd_t<PP, C>(c, G, nrg, done, Res<C>::tw(c, 0))
+    const bool tl = use_yz<C>(c) && ensure_fyz<C>(c);
+#define XF(PP) fft_x_fwd_t<PP, C>(c, G, nrg, done, Res<C>::tw(c, 0), tl)
 #define YF(PP) fft_y_t<PP, false, C>(c, G, nrg, done, Res<C>::tw(c, 1))
 #define ZC(PP) fft_z_t<PP, C>(c, G, nrg, done, Res<C>::tw(c, 2))
 #define YI(PP) fft_y_t<PP, true, C>(c, G, nrg, done, Res<C>::tw(c, 1))
-#define XI(PP) fft_x_inv_t<PP, C>(c, G, nrg, done, Res<C>::tw(c, 0))
+#define XI(PP) fft_x_inv_t<PP, C>(c, G, nrg, done, Res<C>::tw(c, 0), tl)
     SCD_DISPATCH_P(c->Px, XF)
-    SCD_DISPATCH_P(c->Py, YF)
-    SCD_DISPATCH_P(c->Pz, ZC)
-    SCD_DISPATCH_P(c->Py, YI)
+    if (tl) {
+        fft_yz<C>(c, G, nrg, done);
+    } else {
+        SCD_DISPATCH_P(c->Py, YF)
+        SCD_DISPATCH_P(c->Pz, ZC)
+        SCD_DISPATCH_P(c->Py, YI)
+    }
     SCD_DISPATCH_P(c->Px, XI)
 #undef XF
 #undef YF
 #undef ZC
 #undef YI
 #undef XI
-    c->launches += 6;
+    c->launches += tl ? 4 : 6;
 }
 
 template <typename ST, typename C, int U, int NS>
@@ -1036,16 +1175,19 @@ void gather_t(scd_ctx *c, C *y, int nrhs, const int *done) {
     if (c->ngroups == 0) return;
     typedef typename CReal<C>::type R;
     const R k2 = (R)(c->k * c->k);
-    if (nrhs >= 4)
-        k_gather<C, 4><<<dim3(gx, (nrhs + 3) / 4), 32 * WARPS_PER_CTA, 0, c->st>>>(Res<C>::R(c), Res<C>::P(c), c->T, c->d_grp_off,
-                                                               c->d_grp_cube, c->ngroups, G, k2, Res<C>::part(c),
-                                                               c->part_len, c->d_pslot_base, c->d_pslot_cnt, y, c->n,
-                                                               done, nrhs);
-    else
-        k_gather<C, 1><<<dim3(gx, nrhs), 32 * WARPS_PER_CTA, 0, c->st>>>(Res<C>::R(c), Res<C>::P(c), c->T, c->d_grp_off,
-                                                               c->d_grp_cube, c->ngroups, G, k2, Res<C>::part(c),
-                                                               c->part_len, c->d_pslot_base, c->d_pslot_cnt, y, c->n,
-                                                               done, nrhs);
+    // spans of right-hand sides per warp (c->gather_span, 0 = all of them)
+    auto span = [&](int rg) { int sp = c->gather_span > 0 ? c->gather_span : nrhs; return (sp + rg - 1) / rg * rg; };
+    if (nrhs >= 4) {
+        const int sp = span(4);
+        k_gather<C, 4><<<dim3(gx, (nrhs + sp - 1) / sp), 32 * WARPS_PER_CTA, 0, c->st>>>(
+            Res<C>::R(c), Res<C>::P(c), c->T, c->d_grp_off, c->d_grp_cube, c->ngroups, G, k2, Res<C>::part(c),
+            c->part_len, c->d_pslot_base, c->d_pslot_cnt, y, c->n, done, nrhs, sp);
+    } else {
+        const int sp = span(1);
+        k_gather<C, 1><<<dim3(gx, (nrhs + sp - 1) / sp), 32 * WARPS_PER_CTA, 0, c->st>>>(
+            Res<C>::R(c), Res<C>::P(c), c->T, c->d_grp_off, c->d_grp_cube, c->ngroups, G, k2, Res<C>::part(c),
+            c->part_len, c->d_pslot_base, c->d_pslot_cnt, y, c->n, done, nrhs, sp);
+    }
     c->launches += 1;
 }
 

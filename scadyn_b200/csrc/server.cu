@@ -1,5 +1,24 @@
-// Request loop (include/scadyn_server.h): HBM-budget admission, one worker
-// thread, context and CUDA stream per running request.
+// Request loop (include/scadyn_server.h) over resident operator pools.
+//
+// A pool is one device context (scd_ctx: grid, Green octant, projectors,
+// near-zone tiles, batched-solver workspace) for one operator key -- the
+// mesh and its permittivities, the wavenumber, the cell size, the near-zone
+// storage and the solve options -- with its own worker thread and CUDA
+// stream.  Its worker builds the operator once and then runs the batched
+// solver on a queue of columns that every request of that key feeds: a
+// request that arrives while the pool is solving has its incident columns
+// built on the device and queued at once, and they take slots as the
+// running columns finish (continuous batching across requests).  When its
+// requests are done the pool stays resident, so a later request of the same
+// key starts solving without a rebuild; idle pools are evicted, least
+// recently used first, when a new pool needs their memory.
+//
+// Admission is by the HBM budget: a new pool needs its estimated operator
+// and workspace bytes, every request its incident columns and solutions
+// (2 x 3T x 2nm complex128); max_running (0 = no limit but the budget)
+// bounds the pools solving at once.  Kernels of different pools overlap on
+// the GPU.  A column's arithmetic does not depend on its batch, so a
+// request's T is bit-identical alone, in a mix, and in a shared pool.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -10,16 +29,43 @@
 #include <cstring>
 #include <deque>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
 
 #include "../../include/scadyn_server.h"
+#include "ctx.h"
 
 namespace {
 
 using clk = std::chrono::steady_clock;
+
+int ncols_of(int Nmax) { return 2 * ((Nmax + 1) * (Nmax + 1) - 1); }
+
+// FNV-1a over the mesh arrays: the pool key's fingerprint of a geometry
+uint64_t fnv(uint64_t h, const void *p, size_t bytes) {
+    const unsigned char *b = static_cast<const unsigned char *>(p);
+    for (size_t i = 0; i < bytes; ++i) {
+        h ^= b[i];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+struct PoolKey {
+    uint64_t mesh = 0;
+    int32_t Nv = 0, T = 0, storage_prec = 0;
+    double k = 0, grid_size = 0;
+    scd_solve_opts opts{};
+    bool operator==(const PoolKey &o) const {
+        return mesh == o.mesh && Nv == o.Nv && T == o.T && storage_prec == o.storage_prec && k == o.k &&
+               grid_size == o.grid_size && std::memcmp(&opts, &o.opts, sizeof opts) == 0;
+    }
+};
+
+struct Pool;
 
 struct Req {
     int64_t id = 0;
@@ -30,24 +76,43 @@ struct Req {
     double k = 0, grid_size = 0;
     int32_t Nmax = 0, storage_prec = SCD_STORE_C64;
     scd_solve_opts opts{};
-    int64_t est = 0;
+    PoolKey key;
+    int64_t est_req = 0;          // the request's own device bytes
+    int64_t est_pool = 0;         // a new pool's bytes for it
     int32_t state = SCD_REQ_QUEUED, status = SCD_OK;
+    bool consumed = false;        // the result has been read
     std::string err;
     clk::time_point t_submit, t_done;
     std::vector<scd_c128> Tm;
     std::vector<int32_t> iters;
+    // while solving (owned by the pool's worker)
+    std::shared_ptr<Pool> pool;
+    cd *d_mat = nullptr, *d_X = nullptr;
+    int cols_done = 0;
+    int worst = SCD_OK;
 };
 
-int ncols_of(int Nmax) { return 2 * ((Nmax + 1) * (Nmax + 1) - 1); }
+struct Pool {
+    PoolKey key;
+    int64_t est = 0;                       // operator and workspace bytes
+    scd_ctx *ctx = nullptr;
+    std::thread worker;
+    std::deque<int64_t> joining;           // admitted requests the worker has not set up yet
+    std::deque<std::pair<int64_t, int>> cols;   // queued columns (request, column)
+    int active = 0;                        // admitted requests not finished
+    bool stop = false, dead = false;
+    clk::time_point last_used;
+};
 
-// Device bytes of one request: near-zone tiles (about 250 blocks per tet in
-// the 27-box neighbourhood), projectors, Green octant, FFT grids and
+// Device bytes of a request's pool: near-zone tiles (about 250 blocks per
+// tet in the 27-box neighbourhood), projectors, Green octant, FFT grids and
 // partial sums for the slots, Krylov bases and vectors of the batched
-// solver, resident incident columns; plus a fixed 10% and 64 MiB margin.
-int64_t estimate(const scd_request *r, const scd_grid_desc &d) {
+// solver, the mesh; plus a fixed 10% and 64 MiB margin.  And the request's
+// own incident columns and solutions.
+void estimate(const scd_request *r, const scd_grid_desc &d, int64_t *pool_bytes, int64_t *req_bytes) {
     const double T = r->T, n = 3.0 * T;
     const int ncol = ncols_of(r->Nmax);
-    const int ns = std::max(1, std::min(r->opts.block > 0 ? r->opts.block : ncol, std::min(ncol, 64)));
+    const int ns = std::max(1, std::min(r->opts.block > 0 ? r->opts.block : 64, 64));
     const bool mixed = r->opts.precision == SCD_PREC_MIXED;
     auto p2 = [](int v) { int p = 8; while (p < 2 * v) p <<= 1; return (double)p; };
     const double Px = p2(d.Nx), Py = p2(d.Ny);
@@ -55,20 +120,21 @@ int64_t estimate(const scd_request *r, const scd_grid_desc &d) {
     double b = 0;
     b += T * 250.0 * 9.0 * (r->storage_prec == SCD_STORE_C128 ? 16.0 : 8.0);   // near zone
     b += 4.0 * 27.0 * T * (16.0 + 8.0);                                           // projectors
-    b += (Px / 2 + 1) * (Py / 2 + 1) * (p2(d.Nz) / 2 + 1) * 24.0;                 // Green octant
+    b += (Px / 2 + 1) * (Py / 2 + 1) * (p2(d.Nz) / 2 + 1) * 48.0;                 // Green octant (and its transpose)
     b += ns * 4.0 * Px * Py * d.Nz * (16.0 + (mixed ? 8.0 : 0.0));               // FFT work grids
     b += ns * 4.0 * (double)d.Nx * d.Ny * d.Nz * (16.0 + (mixed ? 8.0 : 0.0));   // result grids
     b += ns * n * 15.0 * (16.0 + (mixed ? 8.0 : 0.0));                            // near-zone partial sums
     b += ns * (r->opts.m + 1.0) * n * es;                                         // Krylov bases
     b += ns * n * (4.0 * es + 6.0 * 16.0 + (mixed ? 4.0 * 16.0 : 0.0));           // solver and work vectors
-    b += n * ncol * 16.0;                                                         // incident columns
     b += 12.0 * T * 8.0 + T * 16.0;                                               // mesh on the device
     // tensor-core near zone (the default of the mixed form with complex64
     // storage): f16 hi/lo planes of every tile (8 B per complex plus
     // padding) and a pass of x blocks
     if (d.near_kernel != SCD_NEAR_CUDA_CORES && mixed && r->storage_prec != SCD_STORE_C128)
-        b += T * 250.0 * 9.0 * 8.0 * 1.3 + n * 128.0 * 1.3;   // x block: 32 rows x 2 B x hi/lo per unknown
-    return (int64_t)(b * 1.1) + (64LL << 20);
+        b += T * 250.0 * 9.0 * 8.0 * 1.3 + n * 128.0 * 1.3;
+    *pool_bytes = (int64_t)(b * 1.1) + (64LL << 20);
+    // incident columns, solutions, T and the T assembly's partial sums
+    *req_bytes = (int64_t)(2.0 * n * ncol * 16.0 + 70.0 * (double)ncol * ncol * 16.0);
 }
 
 }  // namespace
@@ -76,109 +142,305 @@ int64_t estimate(const scd_request *r, const scd_grid_desc &d) {
 struct scd_server {
     int dev = 0;
     int64_t budget = 0;
-    int max_running = 1;
+    int max_running = 0;                   // pools solving at once (0 = the budget decides)
     std::mutex m;
     std::condition_variable cv;
     std::deque<int64_t> queue;
     std::map<int64_t, Req> reqs;
+    std::vector<std::shared_ptr<Pool>> pools;
     int64_t next_id = 1;
     int64_t in_use = 0, peak_bytes = 0;
     int running = 0, peak_running = 0;
     int64_t submitted = 0, completed = 0, failed = 0, cancelled = 0, columns = 0;
+    int64_t pools_built = 0, pool_reuses = 0;
     std::vector<double> lat_ms;
     double busy_s = 0;
     clk::time_point busy_since;
     bool stop = false;
     std::thread dispatcher;
-    std::map<int64_t, std::thread> workers;   // running (or just finished) request threads
-    std::vector<int64_t> finished;            // workers done with the lock, to be joined
+    std::vector<std::shared_ptr<Pool>> retired;   // pools whose worker returned, to be joined
     std::string scratch_err;
 };
 
 namespace {
 
-void run_request(scd_server *s, int64_t id) {
-    Req *r;
-    {
-        std::lock_guard<std::mutex> g(s->m);
-        r = &s->reqs[id];   // map nodes are stable; the worker owns the request while running
+// a request left the running set (under the lock)
+void finish_request(scd_server *s, Req &r, int rc, const std::string &err) {
+    r.status = rc;
+    r.err = err;
+    r.t_done = clk::now();
+    if (rc == SCD_OK || rc == SCD_NOT_CONVERGED) {
+        r.state = SCD_REQ_DONE;
+        s->completed += 1;
+        s->columns += ncols_of(r.Nmax);
+        s->lat_ms.push_back(std::chrono::duration<double, std::milli>(r.t_done - r.t_submit).count());
+    } else {
+        r.state = SCD_REQ_FAILED;
+        s->failed += 1;
     }
+    s->in_use -= r.est_req;
+    s->running -= 1;
+    if (s->running == 0) s->busy_s += std::chrono::duration<double>(clk::now() - s->busy_since).count();
+    if (r.pool) {
+        r.pool->active -= 1;
+        r.pool->last_used = clk::now();
+        r.pool.reset();
+    }
+}
+
+// The pool's column queue as the batched solver's source.  Runs on the
+// pool's worker thread, which owns the context.
+struct PoolSource final : ColumnSource {
+    scd_server *s;
+    std::shared_ptr<Pool> P;
+    std::map<int, std::pair<int64_t, int>> inflight;   // tag -> (request, column)
+    int next_tag = 0;
+
+    // set up newly admitted requests: incident columns on the device, room for
+    // their solutions, their columns queued
+    void take_joining() {
+        while (true) {
+            int64_t id;
+            Req *r;
+            {
+                std::lock_guard<std::mutex> g(s->m);
+                if (P->joining.empty()) return;
+                id = P->joining.front();
+                P->joining.pop_front();
+                r = &s->reqs[id];
+            }
+            scd_ctx *c = P->ctx;
+            const int ncol = ncols_of(r->Nmax);
+            const size_t bytes = sizeof(cd) * (size_t)c->n * ncol;
+            int rc = SCD_OK;
+            if (cudaMalloc(&r->d_mat, bytes) != cudaSuccess || cudaMalloc(&r->d_X, bytes) != cudaSuccess) {
+                cudaGetLastError();
+                rc = set_error(c, SCD_OOM, "request columns (%zu bytes)", 2 * bytes);
+            }
+            if (!rc) rc = setup_vswf(c, r->Nmax, r->d_mat);
+            if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->st), "request columns");
+            std::lock_guard<std::mutex> g(s->m);
+            if (rc) {
+                cudaFree(r->d_mat); cudaFree(r->d_X);
+                r->d_mat = r->d_X = nullptr;
+                finish_request(s, *r, rc, c->err);
+                s->cv.notify_all();
+                continue;
+            }
+            r->iters.assign(ncol, 0);
+            r->cols_done = 0;
+            r->worst = SCD_OK;
+            for (int j = 0; j < ncol; ++j) P->cols.emplace_back(id, j);
+        }
+    }
+
+    bool next(const cd **rhs, cd **xout, int *tag) override {
+        take_joining();
+        std::lock_guard<std::mutex> g(s->m);
+        if (P->cols.empty()) return false;
+        const auto job = P->cols.front();
+        P->cols.pop_front();
+        Req &r = s->reqs[job.first];
+        const long long n = P->ctx->n;
+        *rhs = r.d_mat + (size_t)job.second * n;
+        *xout = r.d_X + (size_t)job.second * n;
+        *tag = next_tag;
+        inflight[next_tag++] = job;
+        return true;
+    }
+
+    void finished(int tag, int it, int cv, int st, double) override {
+        const auto job = inflight[tag];
+        inflight.erase(tag);
+        Req *r;
+        {
+            std::lock_guard<std::mutex> g(s->m);
+            r = &s->reqs[job.first];
+        }
+        r->iters[job.second] = it;
+        if (st != SCD_OK) r->worst = st;
+        else if (!cv && r->worst == SCD_OK) r->worst = SCD_NOT_CONVERGED;
+        if (++r->cols_done < ncols_of(r->Nmax)) return;
+        // the request's last column: T = i k^3 mat^H X (src/T_matrix.f90:260,
+        // 271-275) on the stream, after the solution copies
+        scd_ctx *c = P->ctx;
+        const int ncol = ncols_of(r->Nmax);
+        int rc = r->worst == SCD_NOT_CONVERGED ? SCD_OK : r->worst;
+        std::vector<cd> h((size_t)ncol * ncol);
+        cd *d_T = nullptr;
+        if (!rc) {
+            if (cudaMalloc(&d_T, sizeof(cd) * h.size()) != cudaSuccess) {
+                cudaGetLastError();
+                rc = set_error(c, SCD_OOM, "T");
+            }
+        }
+        if (!rc) {
+            launch_T_assemble(c, r->d_mat, ncol, 0, ncol, r->d_X, d_T);
+            rc = check_cuda(c, cudaMemcpyAsync(h.data(), d_T, sizeof(cd) * h.size(), cudaMemcpyDeviceToHost, c->st), "T");
+            if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->st), "T");
+        }
+        cudaFree(d_T);
+        cudaFree(r->d_mat);
+        cudaFree(r->d_X);
+        r->d_mat = r->d_X = nullptr;
+        std::vector<scd_c128> Tm;
+        if (!rc) {
+            const double k3 = std::pow(c->k, 3.0);
+            Tm.resize(h.size());
+            for (size_t i = 0; i < h.size(); ++i) Tm[i] = scd_c128{-k3 * h[i].y, k3 * h[i].x};
+            if (r->worst == SCD_NOT_CONVERGED) rc = SCD_NOT_CONVERGED;
+        }
+        std::lock_guard<std::mutex> g(s->m);
+        r->Tm.swap(Tm);
+        finish_request(s, *r, rc, rc && rc != SCD_NOT_CONVERGED ? c->err : std::string());
+        s->cv.notify_all();
+    }
+
+    bool wait_more() override {
+        std::unique_lock<std::mutex> lk(s->m);
+        while (P->joining.empty() && P->cols.empty() && !P->stop) s->cv.wait(lk);
+        return !(P->stop && P->joining.empty() && P->cols.empty());
+    }
+};
+
+// a pool's worker: build the operator, then solve whatever its requests queue
+void pool_worker(scd_server *s, std::shared_ptr<Pool> P, Req seed) {
     cudaSetDevice(s->dev);
-    int rc = SCD_OK;
-    std::string err;
-    scd_ctx *ctx = nullptr;
     scd_grid_desc d{};
-    const int ncol = ncols_of(r->Nmax);
-    std::vector<scd_c128> Tm((size_t)ncol * ncol);
-    std::vector<int32_t> it(ncol, 0);
-    rc = scd_grid_from_mesh(r->Nv, r->coord.data(), r->T, r->etopol.data(), r->grid_size, 2, &d);
+    scd_ctx *ctx = nullptr;
+    int rc = scd_grid_from_mesh(seed.Nv, seed.coord.data(), seed.T, seed.etopol.data(), seed.grid_size, 2, &d);
     if (!rc) {
         d.device = s->dev;
         rc = scd_create(&ctx, &d);
     }
-    if (!rc) rc = scd_set_wavenumber(ctx, r->k);
-    if (!rc) rc = scd_set_mesh(ctx, r->Nv, r->coord.data(), r->etopol.data(), r->param.data());
+    if (!rc) rc = scd_set_wavenumber(ctx, seed.k);
+    if (!rc) rc = scd_set_mesh(ctx, seed.Nv, seed.coord.data(), seed.etopol.data(), seed.param.data());
     if (!rc) rc = scd_set_green(ctx, nullptr);
     if (!rc) rc = scd_build_projectors(ctx);
-    if (!rc) rc = scd_build_nearzone(ctx, r->storage_prec);
-    if (!rc || rc == SCD_NOT_CONVERGED) {
-        if (!rc) rc = scd_compute_T_matrix(ctx, r->Nmax, &r->opts, 0, ncol, Tm.data(), it.data());
+    if (!rc) rc = scd_build_nearzone(ctx, seed.storage_prec);
+    std::string err = rc ? (ctx ? scd_last_error(ctx) : "context creation failed") : "";
+    if (!rc) {
+        P->ctx = ctx;
+        ctx->cgs_on = seed.opts.gram_schmidt != SCD_GS_MODIFIED;
+        PoolSource src;
+        src.s = s;
+        src.P = P;
+        const scd_solve_opts &o = seed.opts;
+        const int ns = o.block > 0 ? o.block : 64;
+        rc = batch_run(ctx, src, o.tol, o.m, o.cycles, ns, o.precision, o.inner_tol, o.max_outer);
+        if (rc) err = scd_last_error(ctx);
+        // a solver error fails whatever is still in flight or queued
+        std::lock_guard<std::mutex> g(s->m);
+        for (auto &kv : src.inflight) P->cols.emplace_front(kv.second);
     }
-    if (rc && rc != SCD_NOT_CONVERGED) err = ctx ? scd_last_error(ctx) : "context creation failed";
+    std::vector<int64_t> orphans;
+    {
+        std::lock_guard<std::mutex> g(s->m);
+        P->dead = true;
+        for (int64_t id : P->joining) orphans.push_back(id);
+        for (auto &job : P->cols)
+            if (std::find(orphans.begin(), orphans.end(), job.first) == orphans.end()) orphans.push_back(job.first);
+        P->joining.clear();
+        P->cols.clear();
+        for (int64_t id : orphans) {
+            Req &r = s->reqs[id];
+            if (r.state != SCD_REQ_RUNNING) continue;
+            cudaFree(r.d_mat); cudaFree(r.d_X);
+            r.d_mat = r.d_X = nullptr;
+            finish_request(s, r, rc ? rc : SCD_CUDA_ERROR, err.empty() ? "pool stopped" : err);
+        }
+    }
     if (ctx) scd_destroy(ctx);
     {
         std::lock_guard<std::mutex> g(s->m);
-        r->status = rc;
-        r->err = err;
-        r->t_done = clk::now();
-        if (rc == SCD_OK || rc == SCD_NOT_CONVERGED) {
-            r->state = SCD_REQ_DONE;
-            r->Tm.swap(Tm);
-            r->iters.swap(it);
-            s->completed += 1;
-            s->columns += ncol;
-            s->lat_ms.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
-        } else {
-            r->state = SCD_REQ_FAILED;
-            s->failed += 1;
-        }
-        s->in_use -= r->est;
-        s->running -= 1;
-        s->finished.push_back(id);   // after this the worker takes the lock no more
-        if (s->running == 0) s->busy_s += std::chrono::duration<double>(clk::now() - s->busy_since).count();
+        P->ctx = nullptr;
+        s->in_use -= P->est;
+        s->pools.erase(std::remove(s->pools.begin(), s->pools.end(), P), s->pools.end());
+        s->retired.push_back(P);
     }
     s->cv.notify_all();
+}
+
+int solving_pools(const scd_server *s) {
+    int k = 0;
+    for (auto &p : s->pools)
+        if (!p->dead && !p->stop && p->active > 0) ++k;
+    return k;
 }
 
 void dispatch_loop(scd_server *s) {
     std::unique_lock<std::mutex> lk(s->m);
     while (true) {
-        // join the workers that finished (they no longer take the lock)
-        for (int64_t id : s->finished) {
-            auto w = s->workers.find(id);
-            if (w != s->workers.end()) {
-                if (w->second.joinable()) w->second.join();
-                s->workers.erase(w);
-            }
+        // join the workers of retired pools
+        for (auto &p : s->retired) {
+            std::thread t = std::move(p->worker);
+            lk.unlock();
+            if (t.joinable()) t.join();
+            lk.lock();
         }
-        s->finished.clear();
-        // admit, in arrival order, every queued request that fits now
+        s->retired.clear();
+        // admit, in arrival order, every queued request that fits now: into
+        // the resident pool of its key, or into a new pool (evicting idle
+        // pools, least recently used first, when their memory is needed)
         bool admitted = false;
         for (auto q = s->queue.begin(); q != s->queue.end();) {
-            if (s->running >= s->max_running) break;
             Req &r = s->reqs[*q];
-            if (s->in_use + r.est > s->budget) { ++q; continue; }
+            std::shared_ptr<Pool> pool;
+            for (auto &p : s->pools)
+                if (!p->dead && !p->stop && p->key == r.key) pool = p;
+            int64_t need = r.est_req + (pool ? 0 : r.est_pool);
+            if (!pool && s->max_running > 0 && solving_pools(s) >= s->max_running) { ++q; continue; }
+            if (s->in_use + need > s->budget) {
+                // free idle pools of other keys, oldest first
+                std::vector<std::shared_ptr<Pool>> idle;
+                for (auto &p : s->pools)
+                    if (!p->dead && !p->stop && p->active == 0 && p != pool) idle.push_back(p);
+                std::sort(idle.begin(), idle.end(), [](auto &a, auto &b) { return a->last_used < b->last_used; });
+                int64_t freeable = 0;
+                for (auto &p : idle) freeable += p->est;
+                if (s->in_use - freeable + need <= s->budget) {
+                    int64_t over = s->in_use + need - s->budget;
+                    for (auto &p : idle) {
+                        if (over <= 0) break;
+                        p->stop = true;   // its worker returns and releases p->est
+                        over -= p->est;
+                    }
+                    s->cv.notify_all();
+                }
+                ++q;   // admitted once the memory is back
+                continue;
+            }
+            if (!pool) {
+                pool = std::make_shared<Pool>();
+                pool->key = r.key;
+                pool->est = r.est_pool;
+                pool->last_used = clk::now();
+                s->in_use += pool->est;
+                s->pools.push_back(pool);
+                s->pools_built += 1;
+                pool->worker = std::thread(pool_worker, s, pool, r);
+            } else {
+                s->pool_reuses += 1;
+            }
             r.state = SCD_REQ_RUNNING;
+            r.pool = pool;
+            pool->active += 1;
+            pool->joining.push_back(*q);
             if (s->running == 0) s->busy_since = clk::now();
             s->running += 1;
-            s->in_use += r.est;
+            s->in_use += r.est_req;
             s->peak_running = std::max(s->peak_running, s->running);
             s->peak_bytes = std::max(s->peak_bytes, s->in_use);
-            s->workers.emplace(*q, std::thread(run_request, s, *q));
             q = s->queue.erase(q);
             admitted = true;
         }
-        if (s->stop && s->queue.empty()) break;
+        if (admitted) s->cv.notify_all();
+        if (s->stop && s->queue.empty() && s->running == 0) {
+            // shut the resident pools down
+            for (auto &p : s->pools) p->stop = true;
+            s->cv.notify_all();
+            if (s->pools.empty() && s->retired.empty()) break;
+        }
         if (!admitted) s->cv.wait(lk);
     }
 }
@@ -192,12 +454,21 @@ double pct(std::vector<double> v, double p) {
     return i + 1 < v.size() ? v[i] * (1 - f) + v[i + 1] * f : v[i];
 }
 
+int request_estimate(const scd_request *req, int64_t *pool_bytes, int64_t *req_bytes) {
+    if (!req || req->T <= 0 || req->Nv < 4 || !req->coord || !req->etopol || req->Nmax < 1) return SCD_BAD_ARG;
+    scd_grid_desc d{};
+    const int rc = scd_grid_from_mesh(req->Nv, req->coord, req->T, req->etopol, req->grid_size, 2, &d);
+    if (rc) return rc;
+    estimate(req, d, pool_bytes, req_bytes);
+    return SCD_OK;
+}
+
 }  // namespace
 
 extern "C" {
 
 int scd_server_create(scd_server **out, int32_t device, int64_t hbm_budget, int32_t max_running) {
-    if (!out || hbm_budget <= 0 || max_running < 1) return SCD_BAD_ARG;
+    if (!out || hbm_budget <= 0 || max_running < 0) return SCD_BAD_ARG;
     *out = nullptr;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return SCD_NO_DEVICE; }
@@ -212,21 +483,25 @@ int scd_server_create(scd_server **out, int32_t device, int64_t hbm_budget, int3
 }
 
 int scd_server_estimate(const scd_request *req, int64_t *bytes) {
-    if (!req || !bytes || req->T <= 0 || req->Nv < 4 || !req->coord || !req->etopol || req->Nmax < 1) return SCD_BAD_ARG;
-    scd_grid_desc d{};
-    const int rc = scd_grid_from_mesh(req->Nv, req->coord, req->T, req->etopol, req->grid_size, 2, &d);
+    if (!bytes) return SCD_BAD_ARG;
+    int64_t pb = 0, rb = 0;
+    const int rc = request_estimate(req, &pb, &rb);
     if (rc) return rc;
-    *bytes = estimate(req, d);
+    *bytes = pb + rb;
     return SCD_OK;
 }
 
 int scd_server_submit(scd_server *s, const scd_request *req, int64_t *id) {
     if (!s || !req || !id || !req->param) return SCD_BAD_ARG;
-    if (!(req->k > 0) || req->opts.m < 1 || req->opts.m > SCD_M_MAX) return SCD_BAD_ARG;
-    int64_t est = 0;
-    int rc = scd_server_estimate(req, &est);
+    if (!(req->k > 0) || req->opts.m < 1 || req->opts.m > SCD_M_MAX || req->opts.cycles < 1 || !(req->opts.tol > 0))
+        return SCD_BAD_ARG;
+    if (req->opts.precision != SCD_PREC_FP64 && req->opts.precision != SCD_PREC_MIXED) return SCD_BAD_ARG;
+    if (req->opts.gram_schmidt < SCD_GS_DEFAULT || req->opts.gram_schmidt > SCD_GS_CLASSICAL) return SCD_BAD_ARG;
+    if (req->opts.block < 0) return SCD_BAD_ARG;
+    int64_t pb = 0, rb = 0;
+    int rc = request_estimate(req, &pb, &rb);
     if (rc) return rc;
-    if (est > s->budget) return SCD_OOM;
+    if (pb + rb > s->budget) return SCD_OOM;
     Req r;
     r.Nv = req->Nv;
     r.T = req->T;
@@ -238,7 +513,19 @@ int scd_server_submit(scd_server *s, const scd_request *req, int64_t *id) {
     r.Nmax = req->Nmax;
     r.storage_prec = req->storage_prec;
     r.opts = req->opts;
-    r.est = est;
+    r.est_pool = pb;
+    r.est_req = rb;
+    uint64_t h = 1469598103934665603ull;
+    h = fnv(h, r.coord.data(), sizeof(double) * r.coord.size());
+    h = fnv(h, r.etopol.data(), sizeof(int32_t) * r.etopol.size());
+    h = fnv(h, r.param.data(), sizeof(scd_c128) * r.param.size());
+    r.key.mesh = h;
+    r.key.Nv = r.Nv;
+    r.key.T = r.T;
+    r.key.storage_prec = r.storage_prec;
+    r.key.k = r.k;
+    r.key.grid_size = r.grid_size;
+    r.key.opts = r.opts;
     r.t_submit = clk::now();
     {
         std::lock_guard<std::mutex> g(s->m);
@@ -288,10 +575,12 @@ int scd_server_result(scd_server *s, int64_t id, scd_c128 *T, int32_t *iters) {
     Req &r = it->second;
     if (r.state == SCD_REQ_FAILED) return r.status;
     if (r.state != SCD_REQ_DONE) return SCD_NOT_READY;
+    if (r.consumed) return SCD_NOT_READY;   // read once: the result was released by the first read
     std::memcpy(T, r.Tm.data(), sizeof(scd_c128) * r.Tm.size());
     if (iters) std::memcpy(iters, r.iters.data(), sizeof(int32_t) * r.iters.size());
     const int rc = r.status;
     std::vector<scd_c128>().swap(r.Tm);
+    r.consumed = true;
     return rc;
 }
 
@@ -324,6 +613,12 @@ int scd_server_stats_get(scd_server *s, scd_server_stats *st) {
     st->p50_ms = pct(s->lat_ms, 50);
     st->p99_ms = pct(s->lat_ms, 99);
     st->busy_s = s->busy_s + (s->running ? std::chrono::duration<double>(clk::now() - s->busy_since).count() : 0.0);
+    st->pools_built = s->pools_built;
+    st->pool_reuses = s->pool_reuses;
+    int res = 0;
+    for (auto &p : s->pools)
+        if (!p->dead) ++res;
+    st->pools_resident = res;
     return SCD_OK;
 }
 
@@ -349,8 +644,6 @@ int scd_server_destroy(scd_server *s) {
     }
     s->cv.notify_all();
     if (s->dispatcher.joinable()) s->dispatcher.join();
-    for (auto &w : s->workers)
-        if (w.second.joinable()) w.second.join();
     delete s;
     return SCD_OK;
 }

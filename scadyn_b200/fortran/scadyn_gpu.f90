@@ -20,6 +20,8 @@ module scadyn_gpu
    integer(c_int), parameter, public :: SCD_NEAR_DEFAULT = 0, SCD_NEAR_CUDA_CORES = 1, &
                                         SCD_NEAR_TENSOR_SPLIT = 2, SCD_NEAR_TENSOR_MERGED = 3
    integer(c_int), parameter, public :: SCD_GS_DEFAULT = 0, SCD_GS_MODIFIED = 1, SCD_GS_CLASSICAL = 2
+   integer(c_int), parameter, public :: SCD_FFT_PASSES_DEFAULT = 0, SCD_FFT_PASSES_FUSED_YZ = 1, &
+                                        SCD_FFT_PASSES_THREE = 2
 
    type, bind(C), public :: scd_grid_desc
       integer(c_int32_t) :: Nx, Ny, Nz
@@ -33,6 +35,7 @@ module scadyn_gpu
       integer(c_int32_t) :: fft_lengths = 0
       integer(c_int32_t) :: near_kernel = 0
       integer(c_int32_t) :: near_split = 0
+      integer(c_int32_t) :: fft_passes = 0
    end type
 
    type, bind(C), public :: scd_solve_opts
@@ -52,6 +55,12 @@ module scadyn_gpu
       real(c_double)     :: last_call_ms, accum_ms
       integer(c_int64_t) :: launches, matvecs, arnoldi_steps
       real(c_double)     :: near_kernel_ms
+   end type
+
+   ! matvec kernel settings (scd_tune_matvec, scd_apply_tuning)
+   type, bind(C), public :: scd_tuning
+      integer(c_int32_t) :: nrhs, precision, near_kernel, fft_passes, scatter_span, gather_span
+      real(c_double)     :: matvec_ms, default_ms
    end type
 
    ! request server (include/scadyn_server.h)
@@ -76,13 +85,16 @@ module scadyn_gpu
       integer(c_int64_t) :: peak_bytes
       real(c_double)     :: p50_ms, p99_ms
       real(c_double)     :: busy_s
+      integer(c_int64_t) :: pools_built, pool_reuses
+      integer(c_int32_t) :: pools_resident
    end type
 
    public :: scd_create, scd_destroy, scd_set_wavenumber, scd_set_green, scd_set_projectors, &
              scd_set_nearzone, scd_grid_from_mesh, scd_set_mesh, scd_build_projectors, &
              scd_build_nearzone, scd_get_projectors, scd_nearzone_count, scd_get_nearzone, &
              scd_matvec, scd_gmres, scd_set_rhs_matrix, scd_solve_columns, scd_vswf_rhs, scd_compute_T_matrix, &
-             scd_get_timing, scd_profile_matvec, scd_T_assemble_noalloc, scd_column_latency, &
+             scd_get_timing, scd_profile_matvec, scd_tune_matvec, scd_apply_tuning, &
+             scd_T_assemble_noalloc, scd_column_latency, &
              scd_nearzone_bytes, scd_selftest_waits, scd_last_error_f
    public :: scd_server_create, scd_server_submit, scd_server_estimate, scd_server_poll, &
              scd_server_wait, scd_server_result, scd_server_cancel, scd_server_stats_get, &
@@ -237,6 +249,18 @@ module scadyn_gpu
          type(c_ptr), value :: ctx
          type(scd_timing), intent(out) :: t
          integer(c_int32_t), value :: reset
+      end function
+      ! autotuner: time the matvec kernel choices, keep and return the fastest
+      integer(c_int) function scd_tune_matvec(ctx, nrhs, precision, reps, tuning) bind(C, name="scd_tune_matvec")
+         import :: c_ptr, c_int, c_int32_t, scd_tuning
+         type(c_ptr), value :: ctx
+         integer(c_int32_t), value :: nrhs, precision, reps
+         type(scd_tuning), intent(out) :: tuning
+      end function
+      integer(c_int) function scd_apply_tuning(ctx, tuning) bind(C, name="scd_apply_tuning")
+         import :: c_ptr, c_int, scd_tuning
+         type(c_ptr), value :: ctx
+         type(scd_tuning), intent(in) :: tuning
       end function
       integer(c_int) function scd_profile_matvec(ctx, reps, nrhs, precision) bind(C, name="scd_profile_matvec")
          import :: c_ptr, c_int, c_int32_t

@@ -1,10 +1,12 @@
 """Python binding of the request loop (include/scadyn_server.h).
 
 A :class:`Server` owns one GPU; requests (a mesh with per-tet permittivity, a
-wavenumber, a VSWF order and solve options) are submitted at any time, admitted
-by an HBM budget, built and solved concurrently on their own CUDA streams, and
-return their full T-matrix.  A request's result does not depend on what else
-runs beside it.
+wavenumber, a VSWF order and solve options) are submitted at any time and
+admitted by an HBM budget.  Requests with the same operator key share a
+resident pool (the operator is built once, their columns are solved in the
+same batched slots); pools solve concurrently on their own CUDA streams and
+stay resident when idle.  Every request returns its full T-matrix, and a
+request's result does not depend on what else runs beside it.
 """
 from __future__ import annotations
 
@@ -32,7 +34,8 @@ class Stats(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
                 ("cancelled", C.c_int64), ("columns", C.c_int64), ("queued", C.c_int32), ("running", C.c_int32),
                 ("peak_running", C.c_int32), ("bytes_in_use", C.c_int64), ("peak_bytes", C.c_int64),
-                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("busy_s", C.c_double)]
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("busy_s", C.c_double),
+                ("pools_built", C.c_int64), ("pool_reuses", C.c_int64), ("pools_resident", C.c_int32)]
 
 
 _bound = False
@@ -68,7 +71,9 @@ def ncols(Nmax):
 
 
 class Server:
-    def __init__(self, device=0, hbm_budget=150e9, max_running=4):
+    def __init__(self, device=0, hbm_budget=150e9, max_running=0):
+        """max_running bounds the pools solving at once; 0 leaves it to the
+        HBM budget."""
         self.lib = _lib()
         self.srv = C.c_void_p()
         rc = self.lib.scd_server_create(C.byref(self.srv), device, int(hbm_budget), max_running)
@@ -78,13 +83,14 @@ class Server:
         self._nmax = {}
 
     def _request(self, mesh, k, grid_size, Nmax, tol=1e-6, m=50, cycles=12, block=16,
-                 precision=api.PREC_FP64, inner_tol=1e-4, max_outer=10, storage=api.STORE_C64):
+                 precision=api.PREC_FP64, inner_tol=1e-4, max_outer=10, storage=api.STORE_C64,
+                 gram_schmidt=api.GS_DEFAULT):
         coord = np.ascontiguousarray(mesh.coord, np.float64)
         etopol = np.ascontiguousarray(mesh.etopol, np.int32)
         param = np.ascontiguousarray(mesh.param, np.complex128)
         r = Request(coord.shape[0], etopol.shape[0], coord.ctypes.data, etopol.ctypes.data, param.ctypes.data,
                     float(k), float(grid_size), int(Nmax), int(storage),
-                    SolveOpts(tol, m, cycles, block, precision, inner_tol, max_outer))
+                    SolveOpts(tol, m, cycles, block, precision, inner_tol, max_outer, gram_schmidt))
         return r, (coord, etopol, param)
 
     def estimate(self, mesh, k, grid_size, Nmax, **opts):

@@ -11,9 +11,13 @@ from scadyn_b200.checkpoint import solve_T_with_checkpoints
 
 
 class _Stub:
-    def __init__(self, fail_after=None):
+    def __init__(self, fail_after=None, problem="mesh-a"):
         self.calls = []
         self.fail_after = fail_after
+        self.problem = problem
+
+    def problem_key(self):
+        return {"source": self.problem, "k": 1.0}
 
     def compute_T_matrix(self, Nmax, col0=0, ncol=None, **kw):
         if self.fail_after is not None and len(self.calls) >= self.fail_after:
@@ -48,6 +52,20 @@ def test_other_problem_is_not_resumed(tmp_path):
     s2 = _Stub()
     _, _, solved = solve_T_with_checkpoints(s2, 3, path, block=8, tol=1e-8)   # same: nothing left
     assert solved == 0 and not s2.calls
+    s3 = _Stub(problem="mesh-b")                                        # same Nmax and options, other mesh
+    solve_T_with_checkpoints(s3, 3, path, block=8, tol=1e-8)
+    assert s3.calls[0] == (0, 8)
+
+
+def test_unknown_problem_needs_a_tag(tmp_path):
+    class _Anonymous(_Stub):
+        problem_key = None
+    s = _Anonymous()
+    s.problem_key = lambda: None
+    with pytest.raises(ValueError):
+        solve_T_with_checkpoints(s, 2, str(tmp_path / "T.npz"), block=8)
+    T, _, solved = solve_T_with_checkpoints(s, 2, str(tmp_path / "T.npz"), block=8, tag="sphere ka=1")
+    assert solved == 2
 
 
 class _Timed(_Stub):

@@ -97,3 +97,37 @@ def test_oversize_request_refused():
         srv.submit(mesh, k, gs, nmax, **o)
     srv.close()
     assert e.value.code == api.SCD_OOM
+
+
+def test_same_key_requests_share_a_resident_pool():
+    """Requests with one operator key share a pool: the second joins while the
+    first is solving (its columns batch with the first's), a third after both
+    finished finds the pool resident (no rebuild); each T is bit-identical to
+    the same request served alone, and a result is read once."""
+    from scadyn_b200 import api
+    from scadyn_b200.server import Server
+    mesh, k, gs, _, o = _requests()[0]
+    alone = Server()
+    ia = alone.submit(mesh, k, gs, 2, **o)
+    alone.wait(ia, 600)
+    T2_alone = alone.result(ia)[0]
+    alone.close()
+
+    srv = Server()
+    i3 = srv.submit(mesh, k, gs, 3, **o)
+    i2 = srv.submit(mesh, k, gs, 2, **o)
+    srv.wait(i3, 600)
+    srv.wait(i2, 600)
+    st = srv.stats()
+    assert st["pools_built"] == 1 and st["pool_reuses"] == 1 and st["pools_resident"] == 1
+    T2 = srv.result(i2)[0]
+    assert np.array_equal(T2, T2_alone)
+    with pytest.raises(api.ScadynError) as e:       # released by the first read
+        srv.result(i2)
+    assert e.value.code == api.SCD_NOT_READY
+    i2b = srv.submit(mesh, k, gs, 2, **o)
+    srv.wait(i2b, 600)
+    st = srv.stats()
+    assert st["pools_built"] == 1 and st["pool_reuses"] == 2
+    assert np.array_equal(srv.result(i2b)[0], T2_alone)
+    srv.close()
