@@ -341,6 +341,8 @@ def main():
                     help="also choose slots and the inner Krylov dimension from a sample of columns")
     ap.add_argument("--serve", type=int, default=0,
                     help="run a served request stream of this many requests instead (C4-shaped, scaled)")
+    ap.add_argument("--serve-scale", default="small", choices=["small", "c4"],
+                    help="request sizes of the served stream: small (5k-60k tets) or c4 (5k-300k tets, Nmax 4-16)")
     ap.add_argument("--sweep", type=int, default=0,
                     help="run a C3-shaped wavelength sweep with this many wavelengths instead")
     ap.add_argument("--sweep-nmax", type=int, default=14, help="largest Nmax of the sweep (C3: 14)")
@@ -364,7 +366,8 @@ def main():
                    near_split=2 if args.near_split else 0, fft_passes=FFT_PASSES[args.fft_passes])
     gs_choice = GRAM_SCHMIDT[args.gram_schmidt]
     if args.serve:
-        print(json.dumps(serve_bench(args.serve)), flush=True)
+        print(json.dumps(serve_bench(args.serve, args.serve_scale, check_err=args.serve_scale != "small")),
+              flush=True)
         return
     if args.sweep:
         print(json.dumps(sweep_bench(args.sweep, args.sweep_nmax)), flush=True)
@@ -660,22 +663,17 @@ def main():
         dist.destroy_process_group()
 
 
-def serve_bench(nreq):
-    """A served stream shaped like C4, scaled to minutes: Poisson arrivals
-    (seed 3000) of T-matrix requests over seeded meshes -- spheres, ellipsoids
-    with axis ratios U(0.5,1), core-mantle spheres (core eps 3.5+0.1i, mantle
-    1.8+0.01i) -- of 5k-60k tets, ka ~ U(1,6), Nmax = clip(round(ka)+2, 4, 8),
-    mixed precision, under a 150 GB HBM budget.  Reports the served
-    columns/s (columns of the completed requests over the time any request
-    was running) and the request latency p50/p99 (submit -> T ready)."""
+def _serve_stream(nreq, scale, seed=3000):
+    """The requests of a served stream: (mesh, k, cell size, Nmax, body) with
+    repeats -- nreq requests drawn from nreq // 2 distinct problems, so that
+    some arrive while an earlier request of the same operator is resident."""
     from scadyn_b200 import geometry, meshgen
-    from scadyn_b200.server import Server
-    from scadyn_b200 import api
-    rng = np.random.default_rng(3000)
-    reqs = []
-    for r in range(nreq):
+    rng = np.random.default_rng(seed)
+    nm_range, ka_range, nmax_cap = ((6.0, 13.0), (1.0, 6.0), 8) if scale == "small" else ((6.0, 22.5), (1.0, 12.0), 16)
+    problems = []
+    for r in range(max(1, nreq // 2)):
         kind = rng.choice(["sphere", "ellipsoid", "core_mantle"])
-        nm = float(rng.uniform(6.0, 13.0))
+        nm = float(rng.uniform(*nm_range))
         if kind == "sphere":
             eps = complex(rng.uniform(1.5, 3.0), rng.uniform(0.01, 0.1))
             mesh = meshgen.sphere(nm, seed=4000 + r, eps=eps)
@@ -685,54 +683,110 @@ def serve_bench(nreq):
             mesh = meshgen.ellipsoid(nm, ax, seed=4000 + r, eps=eps)
         else:
             mesh = meshgen.core_mantle(nm, seed=4000 + r)
-        ka = float(rng.uniform(1.0, 6.0))
-        nmax = int(np.clip(round(ka) + 2, 4, 8))
-        N = max(16, int(round(mesh.n_tet ** (1 / 3) / 2)) * 2)
+        ka = float(rng.uniform(*ka_range))
+        nmax = int(np.clip(round(ka + 4 * ka ** (1 / 3) + 2) if scale != "small" else round(ka) + 2, 4, nmax_cap))
+        N = int(min(128, max(16, int(round(mesh.n_tet ** (1 / 3) / 2)) * 2)))
         gs = geometry.cell_size_for_grid(mesh.coord, mesh.etopol, N)
-        reqs.append((mesh, ka / mesh.a, gs, nmax, kind))
-    gaps = rng.exponential(0.5, size=len(reqs))
-    srv = Server(hbm_budget=150e9, max_running=4)
-    ids, t0 = [], time.time()
-    for (mesh, k, gs, nmax, kind), gap in zip(reqs, gaps):
-        time.sleep(float(gap))
-        ids.append(srv.submit(mesh, k, gs, nmax, tol=1e-6, m=20, cycles=60, block=16,
-                              precision=api.PREC_MIXED, inner_tol=1e-4, max_outer=10))
-    for i in ids:
-        srv.wait(i, 3600)
-    wall = time.time() - t0
-    st = srv.stats()
-    lat = [srv.poll(i)[2] for i in ids]
-    srv.close()
-    line = {"metric": "served T-matrix columns/s and request latency p50/p99 (mixed precision, batched)",
-            "value": round(st["columns"] / st["busy_s"], 4), "unit": "columns/s", "n_gpus": 1,
+        problems.append((mesh, ka / mesh.a, gs, nmax, str(kind)))
+    order = list(range(len(problems))) + list(rng.integers(0, len(problems), size=nreq - len(problems)))
+    rng.shuffle(order[len(problems) // 2:])
+    return [problems[i] for i in order[:nreq]], [int(i) for i in order[:nreq]], problems
+
+
+def serve_bench(nreq, scale="small", check_err=False):
+    """A served stream shaped like C4: Poisson arrivals (seed 3000) of T-matrix
+    requests over seeded meshes -- spheres, ellipsoids with axis ratios
+    U(0.5,1), core-mantle spheres (core eps 3.5+0.1i, mantle 1.8+0.01i) --
+    mixed precision, under a 150 GB HBM budget.  scale "small": 5k-60k tets,
+    ka U(1,6), Nmax 4-8 (minutes, the bench line's summary); "c4": 5k-300k
+    tets, ka U(1,12), Nmax from the Wiscombe rule in 4-16.  Requests repeat
+    problems (nreq // 2 distinct operators).  The stream runs twice on fresh
+    servers: with resident pools shared by requests of one operator, and
+    with every request isolated in its own pool (a per-request key), the
+    one-context-per-request baseline.  Reports served columns/s (columns of
+    completed requests over the time any request was running), request
+    latency p50/p99 (submit -> T ready) of both, and with check_err the T
+    error of four columns of every distinct problem against a separate FP64
+    solve."""
+    from scadyn_b200.server import Server
+    from scadyn_b200 import api
+    reqs, which, problems = _serve_stream(nreq, scale)
+    gap_mean = 0.5 if scale == "small" else 4.0
+    gaps = np.random.default_rng(3001).exponential(gap_mean, size=len(reqs))
+    opts = dict(m=30, cycles=60, block=32, precision=api.PREC_MIXED, inner_tol=3e-4, max_outer=10)
+
+    def run(isolated):
+        srv = Server(hbm_budget=150e9)
+        ids, t0 = [], time.time()
+        for q, ((mesh, k, gs, nmax, kind), gap) in enumerate(zip(reqs, gaps)):
+            time.sleep(float(gap))
+            tol = 1e-6 * (1 + 1e-12 * q) if isolated else 1e-6      # a per-request key: no sharing
+            ids.append(srv.submit(mesh, k, gs, nmax, tol=tol, **opts))
+        for i in ids:
+            srv.wait(i, 7200)
+        wall = time.time() - t0
+        st = srv.stats()
+        lat = [srv.poll(i)[2] for i in ids]
+        Ts = [srv.result(i)[0] for i in ids]
+        srv.close()
+        return {"value": round(st["columns"] / st["busy_s"], 4), "p50_ms": round(st["p50_ms"], 1),
+                "p99_ms": round(st["p99_ms"], 1), "request_latency_ms": [round(v, 1) for v in lat],
+                "completed": st["completed"], "columns": st["columns"], "peak_running": st["peak_running"],
+                "peak_bytes": st["peak_bytes"], "pools_built": st["pools_built"], "pool_reuses": st["pool_reuses"],
+                "busy_s": round(st["busy_s"], 2), "wall_s": round(wall, 2)}, Ts
+
+    shared, Ts = run(False)
+    isolated, _ = run(True)
+    errs = None
+    if check_err:
+        errs = []
+        for p_idx, (mesh, k, gs, nmax, kind) in enumerate(problems):
+            q = which.index(p_idx)
+            d = api.grid_from_mesh(mesh.coord, mesh.etopol, grid_size=gs)
+            s = api.Solver.from_desc(d)
+            s.set_wavenumber(k)
+            s.set_mesh(mesh.coord, mesh.etopol, mesh.param)
+            s.build_G()
+            s.pfft_projection_const()
+            s.compute_near_zone_interactions_const(api.STORE_C64)
+            T64, _ = s.compute_T_matrix(nmax, col0=0, ncol=4, tol=1e-8, m=50, cycles=60, block=4)
+            s.close()
+            errs.append(float(np.linalg.norm(Ts[q][:, :4] - T64) / np.linalg.norm(T64)))
+    line = {"metric": "served T-matrix columns/s and request latency p50/p99 (mixed precision, resident pools)",
+            "value": shared["value"], "unit": "columns/s", "n_gpus": 1,
             "higher_is_better": True, "dtype": "c64 inner / f64 outer", "data": "synthetic (seeded meshes)",
-            "config": {"workload": "C4-shaped served stream, scaled: %d requests, 5k-60k tets, ka U(1,6), "
-                                   "Nmax 4-8, Poisson arrivals mean gap 0.5 s, HBM budget 150 GB" % len(reqs),
+            "config": {"workload": "C4-shaped served stream (%s): %d requests over %d operators, %s, Poisson arrivals "
+                                   "mean gap %.1f s, HBM budget 150 GB"
+                                   % (scale, len(reqs), len(problems),
+                                      "5k-60k tets, ka U(1,6), Nmax 4-8" if scale == "small" else
+                                      "5k-300k tets, ka U(1,12), Nmax 4-16", gap_mean),
                        "tets": [int(m.n_tet) for m, *_ in reqs], "Nmax": [int(r[3]) for r in reqs],
-                       "bodies": [r[4] for r in reqs]},
-            "p50_ms": round(st["p50_ms"], 1), "p99_ms": round(st["p99_ms"], 1),
-            "request_latency_ms": [round(v, 1) for v in lat],
-            "completed": st["completed"], "columns": st["columns"], "peak_running": st["peak_running"],
-            "peak_bytes": st["peak_bytes"], "busy_s": round(st["busy_s"], 2), "wall_s": round(wall, 2)}
+                       "bodies": [r[4] for r in reqs], "problem_of_request": which},
+            "p50_ms": shared["p50_ms"], "p99_ms": shared["p99_ms"], "shared": shared,
+            "one_pool_per_request": isolated}
+    for key in ("completed", "columns", "peak_running", "busy_s"):
+        line[key] = shared[key]
+    if errs is not None:
+        line["t_rel_err_vs_fp64"] = {"max": max(errs), "per_problem": errs, "columns": "4 per problem"}
     return line
 
 
 def sweep_bench(nw, nmax_cap):
-    """C3-shaped wavelength sweep: one ellipsoid mesh (1:0.8:0.6, ~60k tets,
-    eps 2.5+0.05i), nw wavelengths taken evenly from 32 values of ka
-    log-spaced in [1, 10], Nmax from the Wiscombe rule ka + 4 ka^(1/3) + 2
-    clipped to [4, nmax_cap], grid N = 16..64 nodes on the longest axis with
-    ka (padded 32^3-128^3), raised to the mesh resolution where that is finer.  Every wavelength is a request of the serving
-    layer (its own grid and operator), all submitted at once, mixed
-    precision; their solves overlap on the GPU."""
-    from scadyn_b200 import geometry, meshgen
-    from scadyn_b200.server import Server
-    from scadyn_b200 import api
+    """C3-shaped wavelength sweep in one batched solve: one ellipsoid mesh
+    (1:0.8:0.6, ~60k tets, eps 2.5+0.05i), nw wavelengths taken evenly from
+    32 values of ka log-spaced in [1, 10], Nmax from the Wiscombe rule
+    ka + 4 ka^(1/3) + 2 clipped to [4, nmax_cap], grid N = 16..64 nodes on the
+    longest axis with ka (padded 32^3-128^3), raised to the mesh resolution
+    where that is finer.  Every wavelength gets its own context (grid,
+    operator); all columns of all wavelengths are slots of one batched solver
+    (scd_solve_sweep), mixed precision.  Reports columns/s over the whole
+    sweep (device time), set-up separately, and the T error of a sample of
+    columns per wavelength against the FP64 form."""
+    from scadyn_b200 import api, geometry, meshgen
     mesh = meshgen.ellipsoid(17.1, (1.0, 0.8, 0.6), seed=1003, eps=2.5 + 0.05j)
     kas = np.logspace(0, 1, 32)
     pick = np.unique(np.round(np.linspace(0, 31, nw)).astype(int))
-    srv = Server(hbm_budget=150e9, max_running=4)
-    reqs = []
+    ctxs, waves = [], []
     t0 = time.time()
     for i in pick:
         ka = float(kas[i])
@@ -743,24 +797,45 @@ def sweep_bench(nw, nmax_cap):
         N = int(np.clip(round((16 + 48 * (ka - 1) / 9) / 2) * 2, 16, 64))
         N = max(N, int(round(0.9 * mesh.n_tet ** (1 / 3) / 2)) * 2)
         gs = geometry.cell_size_for_grid(mesh.coord, mesh.etopol, N)
-        rid = srv.submit(mesh, ka / mesh.a, gs, nmax, tol=1e-6, m=30, cycles=60, block=16,
-                         precision=api.PREC_MIXED, inner_tol=3e-4, max_outer=10)
-        reqs.append((rid, ka, nmax, N))
-    for rid, *_ in reqs:
-        srv.wait(rid, 3600)
-    wall = time.time() - t0
-    st = srv.stats()
-    per = [{"ka": round(ka, 3), "Nmax": nmax, "N": N, "latency_ms": round(srv.poll(rid)[2], 1)}
-           for rid, ka, nmax, N in reqs]
-    srv.close()
-    return {"metric": "C3-shaped wavelength sweep: T-matrix columns/s over all wavelengths (mixed precision)",
-            "value": round(st["columns"] / st["busy_s"], 4), "unit": "columns/s", "n_gpus": 1,
+        d = api.grid_from_mesh(mesh.coord, mesh.etopol, grid_size=gs)
+        s = api.Solver.from_desc(d)
+        s.set_wavenumber(ka / mesh.a)
+        s.set_mesh(mesh.coord, mesh.etopol, mesh.param)
+        s.build_G()
+        s.pfft_projection_const()
+        s.compute_near_zone_interactions_const(api.STORE_C64)
+        ctxs.append(s)
+        waves.append({"ka": round(ka, 3), "Nmax": nmax, "grid_nodes": [d.Nx, d.Ny, d.Nz],
+                      "columns": 2 * ((nmax + 1) ** 2 - 1)})
+    setup_s = time.time() - t0
+    opts = dict(tol=1e-6, m=30, cycles=60, block=64, precision=api.PREC_MIXED, inner_tol=3e-4, max_outer=10)
+    lead = ctxs[0]
+    lead.timing(reset=True)
+    t = time.time()
+    Ts, its, st, rc = api.solve_sweep(ctxs, [w["Nmax"] for w in waves], **opts)
+    wall = time.time() - t
+    ms = lead.timing(reset=True)["accum_ms"]
+    cols = sum(w["columns"] for w in waves)
+    # accuracy: four columns of every fourth wavelength in FP64 GMRES(50)
+    errs = []
+    for wi in range(0, len(ctxs), 4):
+        c, w = ctxs[wi], waves[wi]
+        T64, _ = c.compute_T_matrix(w["Nmax"], col0=0, ncol=4, tol=1e-8, m=50, cycles=40, block=4)
+        errs.append(float(np.linalg.norm(Ts[wi][:, :4] - T64) / np.linalg.norm(T64)))
+    for w, it in zip(waves, its):
+        w["iters_mean"] = round(float(np.mean(it)), 1)
+    for c in ctxs:
+        c.close()
+    return {"metric": "C3-shaped wavelength sweep: T-matrix columns/s over all wavelengths in one batched solve "
+                      "(mixed precision)",
+            "value": round(cols / (ms / 1e3), 4), "unit": "columns/s", "n_gpus": 1,
             "higher_is_better": True, "dtype": "c64 inner / f64 outer", "data": "synthetic (seeded mesh)",
             "config": {"workload": "ellipsoid 1:0.8:0.6, %d tets, eps 2.5+0.05i, %d of 32 log-spaced ka in [1,10], "
-                                   "Nmax Wiscombe clipped to [4,%d], N 16-64" % (mesh.n_tet, len(pick), nmax_cap)},
-            "wavelengths": per, "columns": st["columns"], "busy_s": round(st["busy_s"], 2),
-            "wall_s": round(wall, 2), "p50_ms": round(st["p50_ms"], 1), "p99_ms": round(st["p99_ms"], 1),
-            "peak_running": st["peak_running"], "peak_bytes": st["peak_bytes"]}
+                                   "Nmax Wiscombe clipped to [4,%d], N 16-64, one scd_solve_sweep, 64 slots"
+                                   % (mesh.n_tet, len(pick), nmax_cap)},
+            "wavelengths": waves, "columns": cols, "solve_ms": round(ms, 1), "wall_s": round(wall, 2),
+            "setup_s": round(setup_s, 2), "status": [int(v) for v in st],
+            "t_rel_err_vs_fp64_sample": {"max": max(errs), "columns": "4 per wavelength, every 4th wavelength"}}
 
 
 def fft_len(v, smooth):

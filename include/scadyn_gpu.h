@@ -224,6 +224,21 @@ SCD_API int scd_vswf_rhs(scd_ctx *ctx, int32_t Nmax, scd_c128 *mat);
 SCD_API int scd_compute_T_matrix(scd_ctx *ctx, int32_t Nmax, const scd_solve_opts *opts, int32_t col0,
                                  int32_t ncol, scd_c128 *T, int32_t *iters);
 
+/* The wavelength loop of calc_T (src/T_matrix.f90:36-79) in one solve: ctxs[w]
+ * holds wavelength w's operator (scd_set_wavenumber, scd_set_mesh with the
+ * one mesh, Green spectrum, projectors and near zone, each with its own grid),
+ * and all 2nm_w columns of every wavelength (nm_w from Nmax[w]) are solved
+ * as slots of one batched solver on ctxs[0]'s stream: columns of different
+ * wavelengths share each tick, each multiplied by its own operator (the
+ * operators' matvecs run on their contexts' streams, joined back per tick).
+ * T[w] (2nm_w, 2nm_w) receives [Taa Tab; Tba Tbb] of wavelength w
+ * (src/T_matrix.f90:271-275), iters[w] (may be NULL, or hold NULLs) the
+ * per-column Arnoldi steps, status[w] (may be NULL) each wavelength's status.
+ * The contexts must share the device and the mesh (the same unknowns); a
+ * column gives the same bits here as in scd_compute_T_matrix on its context. */
+SCD_API int scd_solve_sweep(scd_ctx *const *ctxs, int32_t nw, const int32_t *Nmax, const scd_solve_opts *opts,
+                            scd_c128 *const *T, int32_t *const *iters, int32_t *status);
+
 /* Device timing, milliseconds, from CUDA events on the context's stream. */
 typedef struct scd_timing {
     double matvec_ms;      /* average matvec (scd_profile_matvec) */

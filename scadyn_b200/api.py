@@ -44,6 +44,7 @@ EXPORTS = [
     "scd_get_nearzone", "scd_matvec", "scd_gmres", "scd_set_rhs_matrix", "scd_solve_columns", "scd_vswf_rhs",
     "scd_get_timing", "scd_compute_T_matrix", "scd_profile_matvec", "scd_nearzone_bytes",
     "scd_column_latency", "scd_T_assemble_noalloc", "scd_selftest_waits", "scd_tune_matvec", "scd_apply_tuning",
+    "scd_solve_sweep",
 ]
 
 
@@ -117,6 +118,7 @@ def load_library(path: str = LIB_PATH):
         "scd_profile_matvec": ([vp, i32, i32, i32], C.c_int),
         "scd_tune_matvec": ([vp, i32, i32, i32, C.POINTER(Tuning)], C.c_int),
         "scd_apply_tuning": ([vp, C.POINTER(Tuning)], C.c_int),
+        "scd_solve_sweep": ([vp, i32, vp, C.POINTER(SolveOpts), vp, vp, vp], C.c_int),
         "scd_nearzone_bytes": ([vp], C.c_int64),
         "scd_column_latency": ([vp, i32, vp], C.c_int),
         "scd_T_assemble_noalloc": ([vp, i64, i32, vp, i32, vp, vp], C.c_int),
@@ -159,6 +161,30 @@ def T_assemble_noalloc(mat_ptr, n, ncol, X_ptr, ncb, T_ptr, stream=0):
                                     C.c_void_p(stream))
     if rc:
         raise ScadynError(rc, "scd_T_assemble_noalloc")
+
+
+def solve_sweep(solvers, Nmax, tol=1e-6, m=30, cycles=60, block=32, precision=PREC_MIXED, inner_tol=3e-4,
+                max_outer=10, gram_schmidt=GS_DEFAULT):
+    """scd_solve_sweep: the T-matrices of every wavelength of a sweep in one
+    batched solve (calc_T's wavelength loop, src/T_matrix.f90:36-79).
+    solvers[w] holds wavelength w's operator on the same mesh; Nmax[w] its
+    VSWF order.  Returns ([T_w (2nm_w, 2nm_w)], [iters_w], [status_w], rc)."""
+    lib = load_library()
+    nw = len(solvers)
+    ctxs = (C.c_void_p * nw)(*[s.ctx.value for s in solvers])
+    nm = np.ascontiguousarray(Nmax, np.int32)
+    ncol = [2 * ((int(v) + 1) ** 2 - 1) for v in nm]
+    Ts = [np.zeros((c, c), np.complex128) for c in ncol]       # memory of Fortran T(2nm, 2nm)
+    its = [np.zeros(c, np.int32) for c in ncol]
+    Tp = (C.c_void_p * nw)(*[t.ctypes.data for t in Ts])
+    Ip = (C.c_void_p * nw)(*[i.ctypes.data for i in its])
+    st = np.zeros(nw, np.int32)
+    o = SolveOpts(tol, m, cycles, block, precision, inner_tol, max_outer, gram_schmidt)
+    rc = lib.scd_solve_sweep(C.cast(ctxs, C.c_void_p), nw, _p(nm), C.byref(o), C.cast(Tp, C.c_void_p),
+                             C.cast(Ip, C.c_void_p), _p(st))
+    if rc not in (SCD_OK, SCD_NOT_CONVERGED):
+        raise ScadynError(rc, "scd_solve_sweep: " + lib.scd_last_error(solvers[0].ctx).decode())
+    return [t.T.copy() for t in Ts], its, st, rc
 
 
 @dataclass

@@ -434,6 +434,8 @@ int scd_destroy(scd_ctx *c) {
     batch_free(c);
     if (c->d_mat) cudaFree(c->d_mat);
     for (int i = 0; i < 8; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
     return SCD_OK;
@@ -876,6 +878,24 @@ int64_t scd_nearzone_bytes(scd_ctx *c) {
     return (int64_t)c->tile_store * (c->near_prec == SCD_STORE_C64 ? 8 : 16);
 }
 
+// the device-built incident columns vswf2constant (src/T_matrix.f90:280-305)
+// for Nmax at the current wavenumber, kept in c->d_mat
+static int ensure_vswf(scd_ctx *c, int Nmax) {
+    if (c->d_mat && c->mat_Nmax == Nmax && c->mat_k == c->k) return SCD_OK;
+    const int ntot = 2 * ((Nmax + 1) * (Nmax + 1) - 1);
+    cudaFree(c->d_mat);
+    c->d_mat = nullptr;
+    c->mat_cols = 0;
+    c->mat_Nmax = -1;
+    int rc;
+    if ((rc = dalloc(c, &c->d_mat, (size_t)c->n * ntot, "resident VSWF columns"))) return rc;
+    if ((rc = setup_vswf(c, Nmax, c->d_mat))) return rc;
+    c->mat_Nmax = Nmax;
+    c->mat_k = c->k;
+    c->mat_cols = ntot;
+    return SCD_OK;
+}
+
 int scd_compute_T_matrix(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int32_t col0, int32_t ncol,
                          scd_c128 *T, int32_t *iters) {
     if (!c || !o || !T || Nmax < 1) return SCD_BAD_ARG;
@@ -890,17 +910,7 @@ int scd_compute_T_matrix(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int3
     if (col0 < 0 || ncol < 1 || col0 + ncol > ntot)
         return set_error(c, SCD_BAD_ARG, "columns %d..%d outside 1..%d", col0 + 1, col0 + ncol, ntot);
     const long long n = c->n;
-    if (!c->d_mat || c->mat_Nmax != Nmax || c->mat_k != c->k) {
-        cudaFree(c->d_mat);
-        c->d_mat = nullptr;
-        c->mat_cols = 0;
-        c->mat_Nmax = -1;
-        if ((rc = dalloc(c, &c->d_mat, (size_t)n * ntot, "resident VSWF columns"))) return rc;
-        if ((rc = setup_vswf(c, Nmax, c->d_mat))) return rc;
-        c->mat_Nmax = Nmax;
-        c->mat_k = c->k;
-        c->mat_cols = ntot;
-    }
+    if ((rc = ensure_vswf(c, Nmax))) return rc;
     cd *d_X = nullptr, *d_T = nullptr;
     if ((rc = dalloc(c, &d_X, (size_t)n * ncol, "X"))) return rc;
     if ((rc = dalloc(c, &d_T, (size_t)ntot * ncol, "T"))) { cudaFree(d_X); return rc; }
@@ -938,6 +948,112 @@ int scd_compute_T_matrix(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int3
     cudaFree(d_X);
     cudaFree(d_T);
     return worst;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ wavelength sweep
+namespace {
+// every column of every wavelength, wavelength after wavelength; column j of
+// wavelength w is solved with operator w
+struct SweepSource final : ColumnSource {
+    std::vector<scd_ctx *> ops;
+    std::vector<int> ncol;
+    std::vector<cd *> X;
+    std::vector<int32_t *> iters;
+    std::vector<std::pair<int, int>> jobs;   // tag -> (wavelength, column)
+    size_t next_job = 0;
+    std::vector<int> worst;
+    bool next(const cd **rhs, cd **xout, int *tag) override {
+        if (next_job >= jobs.size()) return false;
+        const auto [w, j] = jobs[next_job];
+        const long long n = ops[w]->n;
+        *rhs = ops[w]->d_mat + (size_t)j * n;
+        *xout = X[w] + (size_t)j * n;
+        *tag = (int)next_job++;
+        return true;
+    }
+    void finished(int tag, int it, int cv, int st, double) override {
+        const auto [w, j] = jobs[tag];
+        if (iters[w]) iters[w][j] = it;
+        if (st != SCD_OK) worst[w] = st;
+        else if (!cv && worst[w] == SCD_OK) worst[w] = SCD_NOT_CONVERGED;
+    }
+    int op_of(int tag) override { return jobs[tag].first; }
+};
+}  // namespace
+
+extern "C" {
+
+int scd_solve_sweep(scd_ctx *const *ctxs, int32_t nw, const int32_t *Nmax, const scd_solve_opts *o, scd_c128 *const *T,
+                    int32_t *const *iters, int32_t *status) {
+    if (!ctxs || nw < 1 || !Nmax || !o || !T) return SCD_BAD_ARG;
+    scd_ctx *c = ctxs[0];
+    if (!c) return SCD_BAD_ARG;
+    cudaSetDevice(c->dev);
+    int rc = SCD_OK;
+    for (int w = 0; w < nw; ++w) {
+        scd_ctx *cw = ctxs[w];
+        if (!cw || Nmax[w] < 1 || !T[w]) return set_error(c, SCD_BAD_ARG, "wavelength %d: null context, Nmax or T", w);
+        if (cw->dev != c->dev || cw->n != c->n)
+            return set_error(c, SCD_BAD_ARG, "wavelength %d: the sweep's contexts share one device and one mesh", w);
+        if (cw->nb != 1) return set_error(c, SCD_BAD_ARG, "scd_solve_sweep: constant basis only");
+        for (int v = 0; v < w; ++v)
+            if (ctxs[v] == cw) return set_error(c, SCD_BAD_ARG, "wavelength %d repeats the context of %d", w, v);
+        if ((rc = ready(cw)) || (rc = check_opts(cw, o)) || (rc = ensure_vswf(cw, Nmax[w])))
+            return set_error(c, rc, "wavelength %d: %s", w, cw->err.c_str());
+    }
+    if ((rc = check_opts(c, o))) return rc;
+    SweepSource src;
+    src.ops.assign(ctxs, ctxs + nw);
+    src.worst.assign(nw, SCD_OK);
+    auto release = [&]() { for (cd *p : src.X) cudaFree(p); };
+    for (int w = 0; w < nw; ++w) {
+        const int ncol = 2 * ((Nmax[w] + 1) * (Nmax[w] + 1) - 1);
+        src.ncol.push_back(ncol);
+        src.iters.push_back(iters ? iters[w] : nullptr);
+        cd *X = nullptr;
+        if ((rc = dalloc(c, &X, (size_t)c->n * ncol, "sweep solutions"))) { release(); return rc; }
+        src.X.push_back(X);
+        for (int j = 0; j < ncol; ++j) src.jobs.emplace_back(w, j);
+    }
+    cudaEventRecord(c->ev[4], c->st);
+    const int ns = o->block > 0 ? o->block : 64;
+    rc = batch_run(c, src, o->tol, o->m, o->cycles, ns, o->precision, o->inner_tol, o->max_outer, &src.ops);
+    if (rc) { release(); return rc; }
+    cudaEventRecord(c->ev[5], c->st);   // the solve's end: every column of every wavelength
+    int worst = SCD_OK;
+    for (int w = 0; w < nw && !rc; ++w) {
+        scd_ctx *cw = ctxs[w];
+        const int ns_ = near_status(cw);
+        if (ns_) { rc = set_error(c, ns_, "wavelength %d: %s", w, cw->err.c_str()); break; }
+        // T_mat = mat^H X times i k^3 (src/T_matrix.f90:260, 271-275), on the
+        // wavelength's stream after the solver's stream
+        const int ncol = src.ncol[w];
+        cd *d_T = nullptr;
+        if ((rc = dalloc(c, &d_T, (size_t)ncol * ncol, "sweep T"))) break;
+        cudaStreamWaitEvent(cw->st, c->ev[5], 0);
+        launch_T_assemble(cw, cw->d_mat, ncol, 0, ncol, src.X[w], d_T);
+        std::vector<cd> h((size_t)ncol * ncol);
+        rc = check_cuda(c, cudaMemcpyAsync(h.data(), d_T, sizeof(cd) * h.size(), cudaMemcpyDeviceToHost, cw->st), "T");
+        if (!rc) rc = check_cuda(c, cudaStreamSynchronize(cw->st), "sweep T");
+        cudaFree(d_T);
+        if (rc) break;
+        const double k3 = std::pow(cw->k, 3.0);
+        for (size_t i = 0; i < h.size(); ++i) T[w][i] = scd_c128{-k3 * h[i].y, k3 * h[i].x};
+        if (status) status[w] = src.worst[w];
+        if (src.worst[w] != SCD_OK && src.worst[w] != SCD_NOT_CONVERGED) worst = src.worst[w];
+        else if (src.worst[w] == SCD_NOT_CONVERGED && worst == SCD_OK) worst = SCD_NOT_CONVERGED;
+    }
+    cudaEventSynchronize(c->ev[5]);
+    if (!rc) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c->ev[4], c->ev[5]);
+        c->last_call_ms = ms;
+        c->accum_ms += ms;
+    }
+    release();
+    return rc ? rc : worst;
 }
 
 }  // extern "C"

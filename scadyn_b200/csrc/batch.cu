@@ -928,8 +928,39 @@ int batch_prepare(scd_ctx *c, int ns, int m, int mixed, BatchBuffers &b) {
     return SCD_OK;
 }
 
+// The matvecs of one tick: columns [off_w, off_w + cnt[w]) of in/out (stride
+// n) with operator ops[w].  The other contexts' matvecs run on their own
+// streams, forked from and joined back to c's stream, so the operators of a
+// sweep work concurrently.
 template <typename C>
-static int launch_tick(scd_ctx *c, BatchBuffers &bb, int ns, int nact, int m, int cycles, double tol, int mixed) {
+static void multi_matvec(scd_ctx *c, const std::vector<scd_ctx *> &ops, const C *in, C *out, const std::vector<int> &cnt) {
+    const long long n = c->n;
+    if (ops.size() == 1) {
+        if (cnt[0] > 0) run_matvec(ops[0], in, out, cnt[0], nullptr);
+        return;
+    }
+    if (!c->ev_fork) cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+    cudaEventRecord(c->ev_fork, c->st);
+    long long off = 0;
+    for (size_t w = 0; w < ops.size(); ++w) {
+        if (cnt[w] == 0) continue;
+        scd_ctx *o = ops[w];
+        if (o == c) {
+            run_matvec(o, in + off * n, out + off * n, cnt[w], nullptr);
+        } else {
+            if (!o->ev_join) cudaEventCreateWithFlags(&o->ev_join, cudaEventDisableTiming);
+            cudaStreamWaitEvent(o->st, c->ev_fork, 0);
+            run_matvec(o, in + off * n, out + off * n, cnt[w], nullptr);
+            cudaEventRecord(o->ev_join, o->st);
+            cudaStreamWaitEvent(c->st, o->ev_join, 0);
+        }
+        off += cnt[w];
+    }
+}
+
+template <typename C>
+static int launch_tick(scd_ctx *c, BatchBuffers &bb, int ns, int nact, int m, int cycles, double tol, int mixed,
+                       const std::vector<scd_ctx *> &ops, const std::vector<int> &cnt) {
     TickArgs<C> a;
     a.slots = bb.slots; a.ns = ns; a.V = (C *)bb.V; a.H = bb.H; a.cs = bb.cs; a.sn = bb.sn; a.g = bb.g; a.y = bb.y;
     a.x = (C *)bb.x; a.rhs = (C *)bb.rhs; a.w = (C *)bb.W; a.red = bb.red; a.bar = c->d_bar; a.err = c->d_err;
@@ -941,7 +972,7 @@ static int launch_tick(scd_ctx *c, BatchBuffers &bb, int ns, int nact, int m, in
     if (nact > 0) {
         k_stage<C><<<dim3(std::min<long long>((n + 255) / 256, 1024), ns), 256, 0, c->st>>>(bb.slots, ns, (C *)bb.V,
                                                                                            (C *)bb.x, (C *)bb.Xin, n, m);
-        run_matvec(c, (const C *)bb.Xin, (C *)bb.W, nact, nullptr);
+        multi_matvec<C>(c, ops, (const C *)bb.Xin, (C *)bb.W, cnt);
     }
     NvtxRange r("arnoldi tick");
     void *args[] = {&a};
@@ -957,7 +988,7 @@ static int launch_tick(scd_ctx *c, BatchBuffers &bb, int ns, int nact, int m, in
 // algorithm); 1: FP64 iterative refinement to `tol` around complex64
 // GMRES(m) inner solves to `inner_tol`, at most `max_outer` outer steps.
 int batch_run(scd_ctx *c, ColumnSource &src, double tol, int m, int cycles, int ns, int precision, double inner_tol,
-              int max_outer) {
+              int max_outer, const std::vector<scd_ctx *> *ops_in) {
     NvtxRange range(precision == SCD_PREC_MIXED ? "batch solve (mixed)" : "batch solve (fp64)");
     if (!c->batch) c->batch = new BatchBuffers();
     BatchBuffers &bb = *(BatchBuffers *)c->batch;
@@ -965,13 +996,23 @@ int batch_run(scd_ctx *c, ColumnSource &src, double tol, int m, int cycles, int 
     if (m < 1 || m > SCD_M_MAX) return set_error(c, SCD_BAD_ARG, "m = %d outside 1..%d", m, SCD_M_MAX);
     if (ns > NSMAX) ns = NSMAX;
     if (ns < 1) ns = 1;
+    const std::vector<scd_ctx *> ops = ops_in && !ops_in->empty() ? *ops_in : std::vector<scd_ctx *>{c};
+    const int nops = (int)ops.size();
+    for (scd_ctx *o : ops)
+        if (o->n != c->n || o->dev != c->dev)
+            return set_error(c, SCD_BAD_ARG, "operators of one batch need the same device and unknowns");
     int rc = batch_prepare(c, ns, m, mixed, bb);
     if (rc) return rc;
-    if (mixed) {
-        if ((rc = ensure_single(c)) || (rc = ensure_work_single(c, ns)) || (rc = ensure_work(c, ns))) return rc;
-    } else if ((rc = ensure_work(c, ns))) {
-        return rc;
+    for (scd_ctx *o : ops) {
+        if (mixed) {
+            if ((rc = ensure_single(o)) || (rc = ensure_work_single(o, ns)) || (rc = ensure_work(o, ns)))
+                return o == c ? rc : set_error(c, rc, "operator of the batch: %s", o->err.c_str());
+        } else if ((rc = ensure_work(o, ns))) {
+            return o == c ? rc : set_error(c, rc, "operator of the batch: %s", o->err.c_str());
+        }
     }
+    if (mixed && (rc = ensure_work(c, ns))) return rc;
+    std::vector<int> sop(ns, 0), cnt_m(nops, 0), cnt_r(nops, 0);   // slot operators, columns per operator
     if (!c->d_bar) {
         if (cudaMalloc(&c->d_bar, sizeof(GridBarrier)) != cudaSuccess || cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess)
             return set_error(c, SCD_OOM, "barrier");
@@ -1013,6 +1054,8 @@ int batch_run(scd_ctx *c, ColumnSource &src, double tol, int m, int cycles, int 
                     hs[s].mode = SLOT_START;
                 }
                 hs[s].col = tag;
+                sop[s] = nops > 1 ? src.op_of(tag) : 0;
+                if (sop[s] < 0 || sop[s] >= nops) return set_error(c, SCD_BAD_ARG, "column %d: operator %d", tag, sop[s]);
             }
             if (hs[s].mode == SLOT_INNER_DONE) { hs[s].mode = SLOT_RESID; hs[s].upd = 1; upd = true; }
             if (hs[s].mode == SLOT_RESID) resid = true;
@@ -1026,13 +1069,20 @@ int batch_run(scd_ctx *c, ColumnSource &src, double tol, int m, int cycles, int 
             continue;
         }
         if (!inner && !resid) return set_error(c, SCD_CUDA_ERROR, "batch solver stalled");
-        // compacted matvec columns: only slots that need A x this tick
+        // compacted matvec columns: only slots that need A x this tick, grouped
+        // by operator
         int nact = 0, nres = 0;
-        for (int s = 0; s < ns; ++s) {
-            hs[s].mpos = -1;
-            hs[s].rpos = -1;
-            if (hs[s].mode == SLOT_RESID) hs[s].rpos = nres++;
-            if ((hs[s].mode == SLOT_START && !hs[s].zero_x) || hs[s].mode == SLOT_ARNOLDI) hs[s].mpos = nact++;
+        for (int s = 0; s < ns; ++s) hs[s].mpos = hs[s].rpos = -1;
+        for (int w = 0; w < nops; ++w) {
+            cnt_m[w] = cnt_r[w] = 0;
+            for (int s = 0; s < ns; ++s) {
+                if (sop[s] != w) continue;
+                if (hs[s].mode == SLOT_RESID) { hs[s].rpos = nres++; ++cnt_r[w]; }
+                if ((hs[s].mode == SLOT_START && !hs[s].zero_x) || hs[s].mode == SLOT_ARNOLDI) {
+                    hs[s].mpos = nact++;
+                    ++cnt_m[w];
+                }
+            }
         }
         cudaMemcpyAsync(bb.slots, hs, sizeof(Slot) * ns, cudaMemcpyHostToDevice, c->st);
         if (mixed) {
@@ -1040,7 +1090,7 @@ int batch_run(scd_ctx *c, ColumnSource &src, double tol, int m, int cycles, int 
             if (upd) k_outer_update<<<g2, 256, 0, c->st>>>(bb.slots, bb.x64, (const cf *)bb.x, n);
             if (resid) {
                 k_stage_resid<<<g2, 256, 0, c->st>>>(bb.slots, bb.x64, bb.Xin64, n);
-                run_matvec(c, (const cd *)bb.Xin64, bb.W64, nres, nullptr);
+                multi_matvec<cd>(c, ops, (const cd *)bb.Xin64, bb.W64, cnt_r);
                 ResidArgs ra;
                 ra.slots = bb.slots; ra.ns = ns; ra.b64 = bb.b64; ra.w64 = bb.W64; ra.rhs32 = (cf *)bb.rhs;
                 ra.x32 = (cf *)bb.x; ra.red = bb.red; ra.bar = c->d_bar; ra.err = c->d_err; ra.n = n; ra.tol = tol;
@@ -1050,9 +1100,9 @@ int batch_run(scd_ctx *c, ColumnSource &src, double tol, int m, int cycles, int 
                 c->launches += 3 + (upd ? 1 : 0);
                 if ((rc = check_cuda(c, e, "residual launch"))) return rc;
             }
-            if ((rc = launch_tick<cf>(c, bb, ns, nact, m, cycles, gm_tol, 1))) return rc;
+            if ((rc = launch_tick<cf>(c, bb, ns, nact, m, cycles, gm_tol, 1, ops, cnt_m))) return rc;
         } else {
-            if ((rc = launch_tick<cd>(c, bb, ns, nact, m, cycles, gm_tol, 0))) return rc;
+            if ((rc = launch_tick<cd>(c, bb, ns, nact, m, cycles, gm_tol, 0, ops, cnt_m))) return rc;
         }
         cudaMemcpyAsync(hs, bb.slots, sizeof(Slot) * ns, cudaMemcpyDeviceToHost, c->st);
         if ((rc = check_cuda(c, cudaStreamSynchronize(c->st), "tick"))) return rc;

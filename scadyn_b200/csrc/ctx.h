@@ -152,6 +152,7 @@ struct scd_ctx {
 
     // timing
     cudaEvent_t ev[8] = {};
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;   // ordering against another context's stream
     double t_matvec = 0, t_near = 0, t_fft = 0, t_gather = 0, t_arn = 0, t_near_k = 0;
     double last_call_ms = 0, accum_ms = 0;
     long long n_matvec = 0, n_arn = 0, launches = 0;
@@ -224,9 +225,16 @@ struct ColumnSource {
     // every slot is idle and the stream drained: block until columns may be
     // ready (true) or no more will come (false, the solver returns)
     virtual bool wait_more() { return false; }
+    // the operator (index into batch_run's ops) that column `tag` is solved with
+    virtual int op_of(int tag) { (void)tag; return 0; }
 };
+// Batched solves on context c's slots and stream.  With ops (contexts of
+// the same device and the same unknowns n, e.g. one per wavelength of one
+// mesh), every column is solved with its own operator ops[op_of(tag)]: the
+// matvecs of a tick run per operator (each on its context's stream, joined
+// back), the Arnoldi steps of all slots in one launch.
 int batch_run(scd_ctx *c, ColumnSource &src, double tol, int m, int cycles, int ns, int precision, double inner_tol,
-              int max_outer);
+              int max_outer, const std::vector<scd_ctx *> *ops = nullptr);
 void batch_free(scd_ctx *c);
 int batch_solve(scd_ctx *c, int ncol, const cd *const *rhs_cols, cd *X, double tol, int m, int cycles, int ns,
                 int *iters, int *conv, int *status, double *relres, int precision, double inner_tol, int max_outer);

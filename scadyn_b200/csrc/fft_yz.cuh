@@ -32,14 +32,35 @@
 
 constexpr int YZ_THREADS = 256;
 
+// Line stride in shared memory: at least the padded line (pidx range), and
+// such that the lines a half-warp transforms together fall in disjoint
+// 8-byte bank pairs: with 8 threads per line a half-warp holds 2 lines, each
+// touching 8 consecutive pairs per access, so the stride is 8 mod 16 pairs;
+// with 4 threads it holds 4 lines of 4 pairs, so 4 or 12 mod 16.
+constexpr int yz_line_stride(int P, int tpl) {
+    int L = P + (P >> 4) + 1;
+    while (tpl == 8 ? (L % 16 != 8) : (L % 16 != 4 && L % 16 != 12)) ++L;
+    return L;
+}
+
 template <int P> struct YzLine {
     static constexpr bool REG = P == 64 || P == 128;
     static constexpr bool MIX = P == 80 || P == 96 || P == 192;
     static constexpr bool OK = REG || MIX;
     static constexpr int TPL = REG ? 8 : (P % 64 == 0 ? 8 : 4);   // threads per line
-    static constexpr int LS = P + (P >> 4) + 1;                     // padded line stride
+    static constexpr int LS = yz_line_stride(P, TPL);               // line stride
     static constexpr int LINES = YZ_THREADS / TPL;                  // lines per round
 };
+
+// Chunk copies between the plane's columns and the z lines run over 4 x 4
+// tiles (4 consecutive lines ky by 4 consecutive z per half-warp): the plane
+// side reads 4 runs of 4 contiguous elements, the chunk side writes 4 runs of
+// 4, instead of 16 elements one line stride apart on one side.
+SCD_HD void yz_tile4(int e, int nl, int &l, int &z) {
+    const int w = e & 15, blk = e >> 4, nbl = nl >> 2;
+    l = ((blk % nbl) << 2) + (w & 3);
+    z = ((blk / nbl) << 2) + (w >> 2);
+}
 
 struct YzDims {
     int Nx, Ny, Nz, NzR;   // grid nodes, Nz rounded up to a multiple of 8
@@ -83,8 +104,11 @@ SCD_HD void yz_store(int tid, const C *A, C *Wp, const YzDims &D) {
 template <int PY, int PZ, typename C>
 SCD_HD void yz_zload(int tid, const C *A, C *B, int ky0, const YzDims &D) {
     constexpr int LSY = YzLine<PY>::LS, LSZ = YzLine<PZ>::LS, KC = YzLine<PZ>::LINES;
+    static_assert(KC % 4 == 0 && PZ % 4 == 0, "4 x 4 tiles");
     for (int e = tid; e < KC * PZ; e += YZ_THREADS) {
-        const int l = e / PZ, z = e - l * PZ, ky = ky0 + l;
+        int l, z;
+        yz_tile4(e, KC, l, z);
+        const int ky = ky0 + l;
         B[l * LSZ + pidx(z)] = (z < D.Nz && ky < PY) ? A[z * LSY + pidx(ky)] : czero<C>();
     }
 }
@@ -93,10 +117,12 @@ SCD_HD void yz_zload(int tid, const C *A, C *B, int ky0, const YzDims &D) {
 template <int PY, int PZ, typename C>
 SCD_HD void yz_zstore(int tid, C *A, const C *B, int ky0, const YzDims &D) {
     constexpr int LSY = YzLine<PY>::LS, LSZ = YzLine<PZ>::LS, KC = YzLine<PZ>::LINES;
-    const int n = KC * D.Nz;
+    const int n = KC * ((D.Nz + 3) & ~3);
     for (int e = tid; e < n; e += YZ_THREADS) {
-        const int l = e / D.Nz, z = e - l * D.Nz, ky = ky0 + l;
-        if (ky < PY) A[z * LSY + pidx(ky)] = B[l * LSZ + pidx(z)];
+        int l, z;
+        yz_tile4(e, KC, l, z);
+        const int ky = ky0 + l;
+        if (ky < PY && z < D.Nz) A[z * LSY + pidx(ky)] = B[l * LSZ + pidx(z)];
     }
 }
 

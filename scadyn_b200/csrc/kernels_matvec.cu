@@ -1007,8 +1007,9 @@ constexpr bool yz_len_ok(int P) { return P == 64 || P == 80 || P == 96 || P == 1
 template <typename C>
 size_t yz_smem_bytes(const scd_ctx *c) {
     const int NzR = yz_round8(c->Nz);
-    auto lines = [](int P) { return (P == 64 || P == 128 || P % 64 == 0) ? YZ_THREADS / 8 : YZ_THREADS / 4; };
-    auto ls = [](int P) { return P + (P >> 4) + 1; };
+    auto tpl = [](int P) { return (P == 64 || P == 128 || P % 64 == 0) ? 8 : 4; };
+    auto lines = [&](int P) { return YZ_THREADS / tpl(P); };
+    auto ls = [&](int P) { return yz_line_stride(P, tpl(P)); };
     return sizeof(C) * (size_t)(c->Py + c->Pz + (long long)NzR * ls(c->Py) + (long long)lines(c->Pz) * ls(c->Pz));
 }
 

@@ -93,7 +93,7 @@ module scadyn_gpu
              scd_set_nearzone, scd_grid_from_mesh, scd_set_mesh, scd_build_projectors, &
              scd_build_nearzone, scd_get_projectors, scd_nearzone_count, scd_get_nearzone, &
              scd_matvec, scd_gmres, scd_set_rhs_matrix, scd_solve_columns, scd_vswf_rhs, scd_compute_T_matrix, &
-             scd_get_timing, scd_profile_matvec, scd_tune_matvec, scd_apply_tuning, &
+             scd_get_timing, scd_profile_matvec, scd_tune_matvec, scd_apply_tuning, scd_solve_sweep, &
              scd_T_assemble_noalloc, scd_column_latency, &
              scd_nearzone_bytes, scd_selftest_waits, scd_last_error_f
    public :: scd_server_create, scd_server_submit, scd_server_estimate, scd_server_poll, &
@@ -249,6 +249,20 @@ module scadyn_gpu
          type(c_ptr), value :: ctx
          type(scd_timing), intent(out) :: t
          integer(c_int32_t), value :: reset
+      end function
+      ! the wavelength loop of calc_T in one batched solve: ctxs(w) = c_ptr of
+      ! wavelength w's context, T(w) = c_loc of its T(2nm_w, 2nm_w), iters(w) =
+      ! c_loc of its iteration counts or c_null_ptr
+      integer(c_int) function scd_solve_sweep(ctxs, nw, Nmax, opts, T, iters, status) &
+            bind(C, name="scd_solve_sweep")
+         import :: c_ptr, c_int, c_int32_t, scd_solve_opts
+         type(c_ptr), intent(in) :: ctxs(*)
+         integer(c_int32_t), value :: nw
+         integer(c_int32_t), intent(in) :: Nmax(*)
+         type(scd_solve_opts), intent(in) :: opts
+         type(c_ptr), intent(in) :: T(*)
+         type(c_ptr), intent(in) :: iters(*)
+         integer(c_int32_t), intent(out) :: status(*)
       end function
       ! autotuner: time the matvec kernel choices, keep and return the fastest
       integer(c_int) function scd_tune_matvec(ctx, nrhs, precision, reps, tuning) bind(C, name="scd_tune_matvec")

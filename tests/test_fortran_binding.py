@@ -176,6 +176,9 @@ def test_interface_matches_prototype(name):
             assert kind == C_SCALAR[ctype], f"{where}: {kind} for C {ctype}"
         elif kind == "type(c_ptr)" and "value" in attrs:
             assert stars == 1, f"{where}: an address stands for a single pointer"
+        elif kind == "type(c_ptr)" and dim == "*":
+            # an array of addresses (scd_ctx *const *, scd_c128 *const *): one c_ptr per element
+            assert stars == 2 and "intent(in)" in attrs, f"{where}: array of c_ptr"
         elif kind == "type(c_ptr)":
             # the address of an opaque handle (scd_ctx **, scd_server **)
             assert stars == 2 and "intent(out)" in attrs, f"{where}: c_ptr by reference"
@@ -187,7 +190,7 @@ def test_interface_matches_prototype(name):
 
 def test_structs_match():
     cs, fs = c_structs(), fortran_types()
-    passed = {"scd_grid_desc", "scd_solve_opts", "scd_timing", "scd_request", "scd_server_stats"}
+    passed = {"scd_grid_desc", "scd_solve_opts", "scd_timing", "scd_request", "scd_server_stats", "scd_tuning"}
     assert passed <= set(cs)
     for name in passed:
         assert name in fs, f"no bind(C) type {name}"
