@@ -224,6 +224,16 @@ SCD_API int scd_vswf_rhs(scd_ctx *ctx, int32_t Nmax, scd_c128 *mat);
 SCD_API int scd_compute_T_matrix(scd_ctx *ctx, int32_t Nmax, const scd_solve_opts *opts, int32_t col0,
                                  int32_t ncol, scd_c128 *T, int32_t *iters);
 
+/* scd_compute_T_matrix over an arbitrary set of columns: cols (ncol) lists
+ * 0-based column indices (each once, any order) of the 2nm columns of the
+ * column loop (src/T_matrix.f90:254-268); T (2nm, ncol) receives
+ * T(:, j) = i k^3 mat^H x_{cols[j]} and iters (ncol) the Arnoldi steps.  For
+ * hosts that deal the columns out to several GPUs round-robin, so that the
+ * slow high-order columns spread evenly; a column gives the same bits as in
+ * scd_compute_T_matrix. */
+SCD_API int scd_compute_T_columns(scd_ctx *ctx, int32_t Nmax, const scd_solve_opts *opts, int32_t ncol,
+                                  const int32_t *cols, scd_c128 *T, int32_t *iters);
+
 /* The wavelength loop of calc_T (src/T_matrix.f90:36-79) in one solve: ctxs[w]
  * holds wavelength w's operator (scd_set_wavenumber, scd_set_mesh with the
  * one mesh, Green spectrum, projectors and near zone, each with its own grid),

@@ -44,7 +44,7 @@ EXPORTS = [
     "scd_get_nearzone", "scd_matvec", "scd_gmres", "scd_set_rhs_matrix", "scd_solve_columns", "scd_vswf_rhs",
     "scd_get_timing", "scd_compute_T_matrix", "scd_profile_matvec", "scd_nearzone_bytes",
     "scd_column_latency", "scd_T_assemble_noalloc", "scd_selftest_waits", "scd_tune_matvec", "scd_apply_tuning",
-    "scd_solve_sweep",
+    "scd_solve_sweep", "scd_compute_T_columns",
 ]
 
 
@@ -115,6 +115,7 @@ def load_library(path: str = LIB_PATH):
         "scd_vswf_rhs": ([vp, i32, vp], C.c_int),
         "scd_get_timing": ([vp, C.POINTER(Timing), i32], C.c_int),
         "scd_compute_T_matrix": ([vp, i32, C.POINTER(SolveOpts), i32, i32, vp, vp], C.c_int),
+        "scd_compute_T_columns": ([vp, i32, C.POINTER(SolveOpts), i32, vp, vp, vp], C.c_int),
         "scd_profile_matvec": ([vp, i32, i32, i32], C.c_int),
         "scd_tune_matvec": ([vp, i32, i32, i32, C.POINTER(Tuning)], C.c_int),
         "scd_apply_tuning": ([vp, C.POINTER(Tuning)], C.c_int),
@@ -409,6 +410,21 @@ class Solver:
         o = SolveOpts(tol, m, cycles, block, precision, inner_tol, max_outer, gram_schmidt)
         self._chk(self.lib.scd_compute_T_matrix(self.ctx, Nmax, C.byref(o), col0, ncol, _p(Tf), _p(iters)),
                   "compute_T_matrix", ok=(SCD_OK, SCD_NOT_CONVERGED))
+        return Tf.T, iters
+
+    def compute_T_columns(self, Nmax, cols, tol=1e-5, m=50, cycles=4, block=1, precision=PREC_FP64,
+                          inner_tol=1e-3, max_outer=10, gram_schmidt=GS_DEFAULT):
+        """compute_T_matrix over the 0-based columns `cols` (any order, each
+        once): returns (T (2nm, len(cols)) with T[:, j] the scaled column
+        cols[j], iters)."""
+        nm = (Nmax + 1) ** 2 - 1
+        cols = np.ascontiguousarray(cols, np.int32)
+        Tf = np.zeros((len(cols), 2 * nm), np.complex128)
+        iters = np.zeros(len(cols), np.int32)
+        o = SolveOpts(tol, m, cycles, block, precision, inner_tol, max_outer, gram_schmidt)
+        self._chk(self.lib.scd_compute_T_columns(self.ctx, Nmax, C.byref(o), len(cols), _p(cols), _p(Tf),
+                                                 _p(iters)),
+                  "compute_T_columns", ok=(SCD_OK, SCD_NOT_CONVERGED))
         return Tf.T, iters
 
     def profile_matvec(self, reps=10, nrhs=1, precision=PREC_FP64):

@@ -896,19 +896,26 @@ static int ensure_vswf(scd_ctx *c, int Nmax) {
     return SCD_OK;
 }
 
-int scd_compute_T_matrix(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int32_t col0, int32_t ncol,
-                         scd_c128 *T, int32_t *iters) {
-    if (!c || !o || !T || Nmax < 1) return SCD_BAD_ARG;
+// compute_T_matrix over the listed columns (0-based, any order, each once);
+// T(:, j) = i k^3 mat^H x_{list[j]}
+static int compute_T_list(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int ncol, const int32_t *list,
+                          scd_c128 *T, int32_t *iters, const char *who) {
     cudaSetDevice(c->dev);
     // the incident columns are constant-basis (vswf2constant); the reference
     // has no linear-basis T-matrix solve (src/T_matrix.f90:250-259)
-    if (c->nb != 1) return set_error(c, SCD_BAD_ARG, "scd_compute_T_matrix: constant basis only");
+    if (c->nb != 1) return set_error(c, SCD_BAD_ARG, "%s: constant basis only", who);
     int rc = ready(c);
     if (rc) return rc;
     if ((rc = check_opts(c, o))) return rc;
     const int nm = (Nmax + 1) * (Nmax + 1) - 1, ntot = 2 * nm;
-    if (col0 < 0 || ncol < 1 || col0 + ncol > ntot)
-        return set_error(c, SCD_BAD_ARG, "columns %d..%d outside 1..%d", col0 + 1, col0 + ncol, ntot);
+    {
+        std::vector<char> seen(ntot, 0);
+        for (int j = 0; j < ncol; ++j) {
+            if (list[j] < 0 || list[j] >= ntot || seen[list[j]])
+                return set_error(c, SCD_BAD_ARG, "%s: column %d outside 1..%d or listed twice", who, list[j] + 1, ntot);
+            seen[list[j]] = 1;
+        }
+    }
     const long long n = c->n;
     if ((rc = ensure_vswf(c, Nmax))) return rc;
     cd *d_X = nullptr, *d_T = nullptr;
@@ -916,7 +923,7 @@ int scd_compute_T_matrix(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int3
     if ((rc = dalloc(c, &d_T, (size_t)ntot * ncol, "T"))) { cudaFree(d_X); return rc; }
     cudaEventRecord(c->ev[4], c->st);
     std::vector<const cd *> cols(ncol);
-    for (int j = 0; j < ncol; ++j) cols[j] = c->d_mat + (size_t)n * (col0 + j);
+    for (int j = 0; j < ncol; ++j) cols[j] = c->d_mat + (size_t)n * list[j];
     const int ns = o->block > 0 ? o->block : ncol;
     std::vector<int> it(ncol, 0);
     int worst = batch_solve(c, ncol, cols.data(), d_X, o->tol, o->m, o->cycles, ns, it.data(), nullptr, nullptr,
@@ -931,7 +938,7 @@ int scd_compute_T_matrix(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int3
         cudaEventRecord(c->ev[5], c->st);
         std::vector<cd> h((size_t)ntot * ncol);
         rc = check_cuda(c, cudaMemcpyAsync(h.data(), d_T, sizeof(cd) * h.size(), cudaMemcpyDeviceToHost, c->st), "T");
-        if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->st), "compute_T_matrix");
+        if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->st), who);
         if (!rc) {
             // T_mat * i k^3 (src/T_matrix.f90:270-275)
             const double k3 = std::pow(c->k, 3.0);
@@ -948,6 +955,23 @@ int scd_compute_T_matrix(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int3
     cudaFree(d_X);
     cudaFree(d_T);
     return worst;
+}
+
+int scd_compute_T_matrix(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int32_t col0, int32_t ncol,
+                         scd_c128 *T, int32_t *iters) {
+    if (!c || !o || !T || Nmax < 1) return SCD_BAD_ARG;
+    const int ntot = 2 * ((Nmax + 1) * (Nmax + 1) - 1);
+    if (col0 < 0 || ncol < 1 || col0 + ncol > ntot)
+        return set_error(c, SCD_BAD_ARG, "columns %d..%d outside 1..%d", col0 + 1, col0 + ncol, ntot);
+    std::vector<int32_t> list(ncol);
+    for (int j = 0; j < ncol; ++j) list[j] = col0 + j;
+    return compute_T_list(c, Nmax, o, ncol, list.data(), T, iters, "scd_compute_T_matrix");
+}
+
+int scd_compute_T_columns(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int32_t ncol, const int32_t *cols,
+                          scd_c128 *T, int32_t *iters) {
+    if (!c || !o || !T || !cols || Nmax < 1 || ncol < 1) return SCD_BAD_ARG;
+    return compute_T_list(c, Nmax, o, ncol, cols, T, iters, "scd_compute_T_columns");
 }
 
 }  // extern "C"

@@ -93,6 +93,7 @@ module scadyn_gpu
              scd_set_nearzone, scd_grid_from_mesh, scd_set_mesh, scd_build_projectors, &
              scd_build_nearzone, scd_get_projectors, scd_nearzone_count, scd_get_nearzone, &
              scd_matvec, scd_gmres, scd_set_rhs_matrix, scd_solve_columns, scd_vswf_rhs, scd_compute_T_matrix, &
+             scd_compute_T_columns, &
              scd_get_timing, scd_profile_matvec, scd_tune_matvec, scd_apply_tuning, scd_solve_sweep, &
              scd_T_assemble_noalloc, scd_column_latency, &
              scd_nearzone_bytes, scd_selftest_waits, scd_last_error_f
@@ -214,6 +215,17 @@ module scadyn_gpu
          type(c_ptr), value :: ctx
          integer(c_int32_t), value :: Nmax, col0, ncol
          type(scd_solve_opts), intent(in) :: opts
+         complex(c_double_complex), intent(out) :: T(*)
+         integer(c_int32_t), intent(out) :: iters(*)
+      end function
+      ! cols(ncol): 0-based column indices, e.g. an MPI rank's round-robin share
+      integer(c_int) function scd_compute_T_columns(ctx, Nmax, opts, ncol, cols, T, iters) &
+            bind(C, name="scd_compute_T_columns")
+         import :: c_ptr, c_int, c_int32_t, c_double_complex, scd_solve_opts
+         type(c_ptr), value :: ctx
+         integer(c_int32_t), value :: Nmax, ncol
+         type(scd_solve_opts), intent(in) :: opts
+         integer(c_int32_t), intent(in) :: cols(*)
          complex(c_double_complex), intent(out) :: T(*)
          integer(c_int32_t), intent(out) :: iters(*)
       end function

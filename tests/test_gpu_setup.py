@@ -114,6 +114,27 @@ def test_full_device_T_matrix_matches_oracle(dev_setup, small_sphere, small_op):
     assert rel(Tpart, Td[:, 2:5]) < 1e-12
 
 
+@pytest.mark.parametrize("block", [1, 3])
+def test_T_columns_round_robin_share(dev_setup, block):
+    """scd_compute_T_columns over a replica's round-robin share, listed out of
+    order, returns the same bits as those columns of scd_compute_T_matrix
+    (columns are batch-invariant); a repeated or out-of-range index is
+    SCD_BAD_ARG."""
+    s, _ = dev_setup
+    Nmax = 2
+    kw = dict(tol=1e-10, m=50, cycles=8, block=block)
+    Tfull, itf = s.compute_T_matrix(Nmax, **kw)
+    cols = np.arange(1, Tfull.shape[1], 3)[::-1].copy()
+    Tc, itc = s.compute_T_columns(Nmax, cols, **kw)
+    assert np.array_equal(Tc, Tfull[:, cols])
+    assert np.array_equal(itc, itf[cols])
+    with pytest.raises(api.ScadynError) as e:
+        s.compute_T_columns(Nmax, [0, 0], **kw)
+    assert e.value.code == api.SCD_BAD_ARG
+    with pytest.raises(api.ScadynError):
+        s.compute_T_columns(Nmax, [Tfull.shape[1]], **kw)
+
+
 @pytest.mark.parametrize("precision", [api.PREC_FP64, api.PREC_MIXED])
 def test_solve_columns_in_blocks_reproduce_T_matrix(dev_setup, small_op, precision):
     """The column loop run by the host in two blocks (scd_solve_columns over
