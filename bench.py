@@ -69,7 +69,7 @@ L2_BYTES = 126 * 1024 * 1024
 # the headline metric, the same string in both arms
 METRIC = "T-matrix columns/sec & p50/p99 solve latency at \u22641e-5 rel err, mixed vs plain FP64"
 # kernel choices of scd_grid_desc / scd_solve_opts (0 = the library's default)
-NEAR_KERNELS = {"default": 0, "cuda": 1, "split": 2, "merged": 3}
+NEAR_KERNELS = {"default": 0, "cuda": 1, "split": 2, "merged": 3, "wide": 4}
 GRAM_SCHMIDT = {"default": 0, "modified": 1, "classical": 2}
 FFT_LENGTHS = {"default": 0, "pow2": 1, "smooth": 2}
 FFT_PASSES = {"default": 0, "fused": 1, "three": 2}
@@ -434,9 +434,9 @@ def main():
         # same mesh, 16 and 32 complex64 right-hand sides, median of 5 profiled loops
         solver.close()
         out = {"config": args.config, "tets": mesh.n_tet, "ms": {}}
-        for label in ("cuda", "split", "merged"):
+        for label in ("cuda", "split", "merged", "wide"):
             sv, _, _, _, _ = build_solver(cfg, mesh, local, choices=dict(choices, near_kernel=NEAR_KERNELS[label]))
-            for nrhs in (16, 32):
+            for nrhs in (16, 32, 64):
                 runs = [sv.profile_matvec(10, nrhs, api.PREC_MIXED) for _ in range(5)]
                 out["ms"][f"{label}_{nrhs}"] = {key: round(float(np.median([r[key] for r in runs])), 4)
                                                 for key in ("nearzone_ms", "near_kernel_ms", "fft_ms", "gather_ms",

@@ -95,6 +95,8 @@ typedef struct scd_grid_desc {
 #define SCD_NEAR_CUDA_CORES     1   /* complex64 FMAs on the CUDA cores */
 #define SCD_NEAR_TENSOR_SPLIT   2   /* tcgen05 MMAs on f16 hi/lo tile planes, 9 MMAs per K step */
 #define SCD_NEAR_TENSOR_MERGED  3   /* the same with x hi/lo merged into one operand, 6 MMAs per K step */
+#define SCD_NEAR_TENSOR_WIDE    4   /* the merged schedule over 32 right-hand sides per pass: each tile is
+                                       read once per 32 instead of 16 (one CTA per SM) */
 
 /* near-zone storage precision */
 #define SCD_STORE_C64   32   /* complex64, as the reference stores sp_mat */
@@ -277,7 +279,7 @@ SCD_API int scd_profile_matvec(scd_ctx *ctx, int32_t reps, int32_t nrhs, int32_t
 typedef struct scd_tuning {
     int32_t nrhs;             /* right-hand sides per matvec the setting was timed at */
     int32_t precision;        /* SCD_PREC_FP64 or SCD_PREC_MIXED (the complex64 matvec) */
-    int32_t near_kernel;      /* SCD_NEAR_CUDA_CORES / _TENSOR_SPLIT / _TENSOR_MERGED (complex64 matvec) */
+    int32_t near_kernel;      /* SCD_NEAR_CUDA_CORES / _TENSOR_SPLIT / _TENSOR_MERGED / _TENSOR_WIDE (complex64 matvec) */
     int32_t fft_passes;       /* SCD_FFT_PASSES_FUSED_YZ or SCD_FFT_PASSES_THREE */
     int32_t scatter_span;     /* right-hand sides per warp of the anterpolation, 0 = all of a call's */
     int32_t gather_span;      /* right-hand sides per warp of the interpolation, 0 = all */
@@ -309,9 +311,8 @@ SCD_API int scd_apply_tuning(scd_ctx *ctx, const scd_tuning *tuning);
  * is a fixed 4 MiB per-device array, held by every GPU that loads the
  * library until the process exits, so ncol*ncb must not exceed 262144
  * (SCD_BAD_ARG otherwise).  The first call on a device looks up that array's
- * device address and keeps it; make it before any stream capture.  The kept
- * address is not valid after cudaDeviceReset, so do not call this after a
- * reset in the same process.  An error left pending by an earlier call of
+ * device address and keeps it.  The kept address is not valid after
+ * cudaDeviceReset, so do not call this after a reset in the same process.  An error left pending by an earlier call of
  * the caller's is returned as SCD_CUDA_ERROR before anything launches, and
  * left pending.  All calls share the array: calls that overlap on the GPU
  * race and must be ordered by the caller (one stream, or events). */

@@ -29,7 +29,7 @@ STORE_C64, STORE_C128 = 32, 64
 PREC_FP64, PREC_MIXED = 0, 1
 SCD_M_MAX = 63
 FFT_DEFAULT, FFT_POW2, FFT_SMOOTH = 0, 1, 2
-NEAR_DEFAULT, NEAR_CUDA_CORES, NEAR_TENSOR_SPLIT, NEAR_TENSOR_MERGED = 0, 1, 2, 3
+NEAR_DEFAULT, NEAR_CUDA_CORES, NEAR_TENSOR_SPLIT, NEAR_TENSOR_MERGED, NEAR_TENSOR_WIDE = 0, 1, 2, 3, 4
 GS_DEFAULT, GS_MODIFIED, GS_CLASSICAL = 0, 1, 2
 FFT_PASSES_DEFAULT, FFT_PASSES_FUSED_YZ, FFT_PASSES_THREE = 0, 1, 2
 

@@ -47,14 +47,20 @@ static int next_pow2(int v) {
 }
 
 // FFT length of an axis with N nodes: the smallest power of two >= 2N, or
-// (opt-in) the smallest length >= 2N among the powers of two and the 5-smooth
-// lengths with register transforms (80, 96, 192)
+// (the default) the smallest length >= 2N among the powers of two and the
+// 5-smooth lengths with register transforms (80, 96, 192)
 static int fft_len(int v, bool smooth) {
     const int p2 = next_pow2(v);
     if (!smooth) return p2;
     for (int p : {80, 96, 192})
         if (p >= v && p < p2) return p;
     return p2;
+}
+
+// instruction schedule of the tensor-core near zone (near_mma.cuh) for a
+// scd_grid_desc.near_kernel / scd_tuning.near_kernel value
+static int nzm_sched_of(int near_kernel) {
+    return near_kernel == SCD_NEAR_TENSOR_SPLIT ? 0 : near_kernel == SCD_NEAR_TENSOR_WIDE ? 2 : 1;
 }
 
 template <typename Tp>
@@ -380,7 +386,7 @@ int scd_create(scd_ctx **out, const scd_grid_desc *d) {
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { cudaGetLastError(); return SCD_NO_DEVICE; }
     if (d->device < 0 || d->device >= ndev) return SCD_BAD_ARG;
     if (d->fft_lengths < SCD_FFT_DEFAULT || d->fft_lengths > SCD_FFT_SMOOTH) return SCD_BAD_ARG;
-    if (d->near_kernel < SCD_NEAR_DEFAULT || d->near_kernel > SCD_NEAR_TENSOR_MERGED) return SCD_BAD_ARG;
+    if (d->near_kernel < SCD_NEAR_DEFAULT || d->near_kernel > SCD_NEAR_TENSOR_WIDE) return SCD_BAD_ARG;
     if (d->near_split < 0 || d->near_split > 2) return SCD_BAD_ARG;
     if (d->fft_passes < SCD_FFT_PASSES_DEFAULT || d->fft_passes > SCD_FFT_PASSES_THREE) return SCD_BAD_ARG;
     scd_ctx *c = new scd_ctx();
@@ -389,7 +395,7 @@ int scd_create(scd_ctx **out, const scd_grid_desc *d) {
     // kernel choices: the tensor-core near zone applies to complex64 storage
     // only (checked when the near zone is set); 0 selects the defaults
     c->nzm_on = d->near_kernel != SCD_NEAR_CUDA_CORES;
-    c->nzm_sched = d->near_kernel == SCD_NEAR_TENSOR_SPLIT ? 0 : 1;
+    c->nzm_sched = nzm_sched_of(d->near_kernel);
     c->near_split = d->near_split == 2 ? 2 : 1;
     c->yz_on = d->fft_passes != SCD_FFT_PASSES_THREE;
     cudaSetDevice(c->dev);
@@ -791,9 +797,9 @@ int scd_profile_matvec(scd_ctx *c, int32_t reps, int32_t nrhs, int32_t precision
 static void put_tuning(scd_ctx *c, const scd_tuning &t) {
     if (t.near_kernel == SCD_NEAR_CUDA_CORES) {
         c->nzm_on = false;
-    } else if (t.near_kernel == SCD_NEAR_TENSOR_SPLIT || t.near_kernel == SCD_NEAR_TENSOR_MERGED) {
+    } else if (t.near_kernel >= SCD_NEAR_TENSOR_SPLIT && t.near_kernel <= SCD_NEAR_TENSOR_WIDE) {
         c->nzm_on = true;
-        c->nzm_sched = t.near_kernel == SCD_NEAR_TENSOR_SPLIT ? 0 : 1;
+        c->nzm_sched = nzm_sched_of(t.near_kernel);
     }
     c->yz_on = t.fft_passes != SCD_FFT_PASSES_THREE;
     c->scatter_span = std::max(0, t.scatter_span);
@@ -804,7 +810,9 @@ static scd_tuning get_tuning(const scd_ctx *c, int nrhs, int precision) {
     scd_tuning t{};
     t.nrhs = nrhs;
     t.precision = precision;
-    t.near_kernel = !c->nzm_on ? SCD_NEAR_CUDA_CORES : c->nzm_sched == 0 ? SCD_NEAR_TENSOR_SPLIT : SCD_NEAR_TENSOR_MERGED;
+    t.near_kernel = !c->nzm_on ? SCD_NEAR_CUDA_CORES
+                    : c->nzm_sched == 0 ? SCD_NEAR_TENSOR_SPLIT
+                    : c->nzm_sched == 2 ? SCD_NEAR_TENSOR_WIDE : SCD_NEAR_TENSOR_MERGED;
     t.fft_passes = c->yz_on ? SCD_FFT_PASSES_FUSED_YZ : SCD_FFT_PASSES_THREE;
     t.scatter_span = c->scatter_span;
     t.gather_span = c->gather_span;
@@ -813,7 +821,7 @@ static scd_tuning get_tuning(const scd_ctx *c, int nrhs, int precision) {
 
 int scd_apply_tuning(scd_ctx *c, const scd_tuning *t) {
     if (!c || !t) return SCD_BAD_ARG;
-    if ((t->near_kernel < SCD_NEAR_DEFAULT || t->near_kernel > SCD_NEAR_TENSOR_MERGED) ||
+    if ((t->near_kernel < SCD_NEAR_DEFAULT || t->near_kernel > SCD_NEAR_TENSOR_WIDE) ||
         (t->fft_passes < SCD_FFT_PASSES_DEFAULT || t->fft_passes > SCD_FFT_PASSES_THREE) || t->scatter_span < 0 ||
         t->gather_span < 0)
         return set_error(c, SCD_BAD_ARG, "tuning out of range");
@@ -853,7 +861,8 @@ int scd_tune_matvec(scd_ctx *c, int32_t nrhs, int32_t precision, int32_t reps, s
         return SCD_OK;
     };
     if (precision == SCD_PREC_MIXED && c->near_prec == SCD_STORE_C64 && c->nb == 1 &&
-        (rc = knob(&scd_tuning::near_kernel, {SCD_NEAR_CUDA_CORES, SCD_NEAR_TENSOR_SPLIT, SCD_NEAR_TENSOR_MERGED})))
+        (rc = knob(&scd_tuning::near_kernel,
+                   {SCD_NEAR_CUDA_CORES, SCD_NEAR_TENSOR_SPLIT, SCD_NEAR_TENSOR_MERGED, SCD_NEAR_TENSOR_WIDE})))
         return rc;
     if ((rc = knob(&scd_tuning::fft_passes, {SCD_FFT_PASSES_FUSED_YZ, SCD_FFT_PASSES_THREE}))) return rc;
     if (nrhs > 8 && (rc = knob(&scd_tuning::scatter_span, {0, 8, 16}))) return rc;

@@ -168,9 +168,9 @@ struct scd_ctx {
     // solve (batch.cu; scd_solve_opts.gram_schmidt)
     bool cgs_on = false;
     // tensor-core near zone of the complex64 matvec (near_mma.cu;
-    // scd_grid_desc.near_kernel, fixed at context creation)
+    // scd_grid_desc.near_kernel at context creation, scd_apply_tuning later)
     bool nzm_on = false, nzm_ready = false;
-    int nzm_sched = 1;                   // instruction schedule (near_mma.cuh): 0 split, 1 merged
+    int nzm_sched = 1;                   // instruction schedule (near_mma.cuh): 0 split, 1 merged, 2 wide
     unsigned char *d_t16 = nullptr;      // f16 hi/lo planes of every tile
     long long *d_t16_off = nullptr;      // per tile byte offset
     unsigned char *d_xb = nullptr;       // x blocks of one pass
@@ -178,7 +178,8 @@ struct scd_ctx {
     unsigned int *d_xmax = nullptr;      // per right-hand side largest |x| (float bits), then the tiles'
     float *d_xinv = nullptr;             // per right-hand side 1 / (sA sx)
     float nzm_sA = 1.f;
-    uint32_t nzm_x1 = 0, nzm_ring = 0, nzm_slack = 0;
+    uint32_t nzm_x1[2] = {0, 0}, nzm_ring[2] = {0, 0};   // per pass width (16, 32): row x block, ring bytes
+    uint32_t nzm_slack = 0;
 
     void *batch = nullptr;               // batch-solver buffers (batch.cu)
     std::vector<double> col_latency_ms;  // admission -> completion, last batch solve

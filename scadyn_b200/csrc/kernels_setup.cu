@@ -170,17 +170,17 @@ extern "C" SCD_API int scd_T_assemble_noalloc(const scd_c128 *mat, int64_t n, in
     if ((int64_t)ncol * ncb > SCD_NOALLOC_SCRATCH) return SCD_BAD_ARG;   // one split must fit the scratch
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return SCD_NO_DEVICE;
+    // an error left pending by an earlier call of the caller's is not this
+    // call's: report it without launching and leave it for the caller to read
+    if (cudaPeekAtLastError() != cudaSuccess) return SCD_CUDA_ERROR;
     if (!g_noalloc_ptr[dev]) {
         cd *p = nullptr;
         if (cudaGetSymbolAddress((void **)&p, g_noalloc_scratch) != cudaSuccess || !p) {
-            cudaGetLastError();
+            cudaGetLastError();   // this lookup's own error
             return SCD_CUDA_ERROR;
         }
         g_noalloc_ptr[dev] = p;
     }
-    // an error left pending by an earlier call of the caller's is not this
-    // call's: report it without launching and leave it for the caller to read
-    if (cudaPeekAtLastError() != cudaSuccess) return SCD_CUDA_ERROR;
     cd *part = g_noalloc_ptr[dev];
     cudaStream_t st = (cudaStream_t)stream;
     // as many K splits as the scratch holds (at most 64); every partial entry

@@ -8,7 +8,8 @@
 // partial slot of g2; k_gather adds the slots in a fixed order.
 //
 // The default near zone of the complex64 matvec when the blocks are stored
-// complex64 (scd_grid_desc.near_kernel: SCD_NEAR_TENSOR_MERGED, or
+// complex64 (scd_grid_desc.near_kernel: SCD_NEAR_TENSOR_MERGED, 16 right-hand
+// sides per pass; SCD_NEAR_TENSOR_WIDE, the same schedule over 32;
 // SCD_NEAR_TENSOR_SPLIT for the split instruction schedule; SCD_NEAR_CUDA_CORES
 // selects k_near_groups instead).
 #include <cuda_fp16.h>
@@ -23,7 +24,8 @@ namespace {
 constexpr int NZM_SLOTS = 8;
 constexpr int NZM_THREADS = 192;          // warp 0 producer, warp 1 MMA issuer, warps 2-5 epilogue
 constexpr uint32_t NZM_META = 256;
-constexpr size_t NZM_SMEM = 113 * 1024;   // two CTAs per SM
+constexpr size_t NZM_SMEM = 113 * 1024;   // two CTAs per SM (schedules 0, 1)
+constexpr size_t NZM_SMEM_WIDE = 224 * 1024;   // one CTA per SM (schedule 2: 384 TMEM columns)
 
 struct NzmArgs {
     const NearTile *tiles;
@@ -111,33 +113,52 @@ __device__ __forceinline__ void issue_product(int use, int n1, int n2, uint32_t 
     }
 }
 
-// a lane's accumulator row of a product (all lanes of the warp take part)
-template <int S>
-__device__ __forceinline__ void load_rows(uint32_t taddr, float (&v)[32], float (&w)[32]) {
-    tc_ld32(taddr, v);
-    if constexpr (S == 1) tc_ld32(taddr + 32, w);
-}
+// a lane's accumulator row of a product as the complex y_r of the pass's R
+// right-hand sides (all lanes of the warp take part).  Schedule 0 holds
+// [Re y | Im y]; schedules 1 and 2 hold [Re (x hi) | Re (x lo) | Im (x hi) |
+// Im (x lo)], each R columns, added pairwise (hi part first).
+template <int S> struct NzmRows { float re[NzmSched<S>::R], im[NzmSched<S>::R]; };
 
-// that row as the complex y_r of the pass's right-hand sides, scaled by
-// xinv, written to part[(r0 + r) * part_len + base + row]
 template <int S>
-__device__ __forceinline__ void store_rows(const NzmArgs &a, const float (&v)[32], const float (&w)[32], int row_ok,
-                                           int row, long long base) {
-    if (!row_ok) return;
+__device__ __forceinline__ void load_rows(uint32_t taddr, NzmRows<S> &y) {
+    constexpr int R = NzmSched<S>::R;
+    float a[32], b[32];
+    if constexpr (S == 0) {
+        tc_ld32(taddr, a);
 #pragma unroll
-    for (int r = 0; r < NZM_R; ++r) {
-        if (r >= a.rg || (a.skip && a.skip[a.r0 + r])) continue;
-        const float sc = a.xinv[r];
-        float re, im;
-        if constexpr (S == 0) { re = v[r]; im = v[NZM_R + r]; }
-        else { re = v[r] + v[NZM_R + r]; im = w[r] + w[NZM_R + r]; }
-        a.part[(long long)(a.r0 + r) * a.part_len + base + row] = make_float2(re * sc, im * sc);
+        for (int r = 0; r < R; ++r) { y.re[r] = a[r]; y.im[r] = a[R + r]; }
+    } else if constexpr (R == 16) {
+        tc_ld32(taddr, a);
+        tc_ld32(taddr + 32, b);
+#pragma unroll
+        for (int r = 0; r < R; ++r) { y.re[r] = a[r] + a[R + r]; y.im[r] = b[r] + b[R + r]; }
+    } else {
+        tc_ld32(taddr, a);
+        tc_ld32(taddr + R, b);
+#pragma unroll
+        for (int r = 0; r < R; ++r) y.re[r] = a[r] + b[r];
+        tc_ld32(taddr + 2 * R, a);
+        tc_ld32(taddr + 3 * R, b);
+#pragma unroll
+        for (int r = 0; r < R; ++r) y.im[r] = a[r] + b[r];
     }
 }
 
-// one CTA per near-zone group, one pass of up to NZM_R right-hand sides
+// that row scaled by xinv, written to part[(r0 + r) * part_len + base + row]
 template <int S>
-__global__ void __launch_bounds__(NZM_THREADS, 2) k_near_mma(NzmArgs a) {
+__device__ __forceinline__ void store_rows(const NzmArgs &a, const NzmRows<S> &y, int row_ok, int row, long long base) {
+    if (!row_ok) return;
+#pragma unroll
+    for (int r = 0; r < NzmSched<S>::R; ++r) {
+        if (r >= a.rg || (a.skip && a.skip[a.r0 + r])) continue;
+        const float sc = a.xinv[r];
+        a.part[(long long)(a.r0 + r) * a.part_len + base + row] = make_float2(y.re[r] * sc, y.im[r] * sc);
+    }
+}
+
+// one CTA per near-zone group, one pass of up to NzmSched<S>::R right-hand sides
+template <int S>
+__global__ void __launch_bounds__(NZM_THREADS, S == 2 ? 1 : 2) k_near_mma(NzmArgs a) {
     constexpr uint32_t NZM_TMEM_COLS = NzmSched<S>::TMEM;   // row product + two transposed buffers
     constexpr uint32_t DC = NzmSched<S>::DCOLS;
     extern __shared__ unsigned char nzm_raw[];
@@ -203,8 +224,8 @@ __global__ void __launch_bounds__(NZM_THREADS, 2) k_near_mma(NzmArgs a) {
             for (int t = t0; t < t1 && ok; ++t, ++ord) {
                 const NearTile &tl = a.tiles[t];
                 const uint32_t mb = nzm_tile_bytes(tl.n1, tl.n2);
-                const uint32_t xb = nzm_xblock_bytes(tl.n2);
-                const uint32_t x1b = t == t0 ? nzm_xblock_bytes(n1) : 0u;
+                const uint32_t xb = nzm_xblock_bytes<S>(tl.n2);
+                const uint32_t x1b = t == t0 ? nzm_xblock_bytes<S>(n1) : 0u;
                 const uint32_t SZ = mb + xb;
                 bool fit = head + SZ <= R;
                 uint32_t res = fit ? SZ : (R - head) + SZ;
@@ -274,21 +295,21 @@ __global__ void __launch_bounds__(NZM_THREADS, 2) k_near_mma(NzmArgs a) {
             const int b = tcount & 1;
             if (!(ok = mbar_wait(&tfull[b], (uint32_t)((tcount >> 1) & 1), a.err))) break;
             tc_fence_after();
-            float v[32], w[32];
-            load_rows<S>(tbase + ((uint32_t)(32 * quarter) << 16) + DC * (1 + b), v, w);
+            NzmRows<S> y;
+            load_rows<S>(tbase + ((uint32_t)(32 * quarter) << 16) + DC * (1 + b), y);
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty[b]);
             const int row = nzm_row_of_lane(nzm_M(1, n1, tl.n2), 32 * quarter + lane);
-            store_rows<S>(a, v, w, row >= 0 && row < 3 * tl.n2, row, tl.col_off);
+            store_rows<S>(a, y, row >= 0 && row < 3 * tl.n2, row, tl.col_off);
             ++tcount;
         }
         if (ok && mbar_wait(rowfull, 0u, a.err)) {
             tc_fence_after();
-            float v[32], w[32];
-            load_rows<S>(tbase + ((uint32_t)(32 * quarter) << 16), v, w);
+            NzmRows<S> y;
+            load_rows<S>(tbase + ((uint32_t)(32 * quarter) << 16), y);
             const int row = nzm_row_of_lane(nzm_M(0, n1, 1), 32 * quarter + lane);
-            store_rows<S>(a, v, w, row >= 0 && row < 3 * n1, row, a.pslot_base[g]);
+            store_rows<S>(a, y, row >= 0 && row < 3 * n1, row, a.pslot_base[g]);
         }
     }
     tc_fence_before();
@@ -319,16 +340,17 @@ template <int S>
 __global__ void k_xblocks(const cf *__restrict__ x, long long n, int r0, int rg, const int *__restrict__ skip,
                           const unsigned int *__restrict__ xmax, float sA, const int *__restrict__ grp_off,
                           const long long *__restrict__ xb_off, unsigned char *__restrict__ xb, float *__restrict__ xinv) {
-    __shared__ float sx[NZM_R];
-    if (threadIdx.x < NZM_R) sx[threadIdx.x] = nzm_scale_for(__uint_as_float(xmax[threadIdx.x]));
+    constexpr int R = NzmSched<S>::R;
+    __shared__ float sx[R];
+    if (threadIdx.x < R) sx[threadIdx.x] = nzm_scale_for(__uint_as_float(xmax[threadIdx.x]));
     __syncthreads();
     const int g = blockIdx.x;
     const int s0 = grp_off[g], ng = grp_off[g + 1] - s0;
     const int K = nzm_xk(ng);
     uint16_t *blk = reinterpret_cast<uint16_t *>(xb + xb_off[g]);
-    const int total = 4 * NZM_R * K;
+    const int total = 4 * R * K;
     for (int e = threadIdx.x; e < total; e += blockDim.x) blk[e] = nzm_xblock_bits<S>(x, n, r0, rg, skip, sx, s0, ng, e);
-    if (g == 0 && threadIdx.x < NZM_R) {
+    if (g == 0 && threadIdx.x < R) {
         const int r = threadIdx.x;
         xinv[r] = r < rg ? 1.f / (sA * sx[r]) : 0.f;
     }
@@ -371,10 +393,11 @@ int near_mma_prepare(scd_ctx *c) {
     for (int t = 0; t < c->ntiles; ++t) {
         const NearTile &tl = c->tiles_h[t];
         toff[t + 1] = toff[t] + nzm_tile_bytes(tl.n1, tl.n2);
-        slack = std::max(slack, std::max(nzm_overrun<0>(tl.n1, tl.n2), nzm_overrun<1>(tl.n1, tl.n2)));
+        slack = std::max({slack, nzm_overrun<0>(tl.n1, tl.n2), nzm_overrun<1>(tl.n1, tl.n2), nzm_overrun<2>(tl.n1, tl.n2)});
     }
+    // x blocks sized for the widest pass (schedule 2), so every schedule fits
     std::vector<long long> xoff(c->ngroups + 1, 0);
-    for (int g = 0; g < c->ngroups; ++g) xoff[g + 1] = xoff[g] + nzm_xblock_bytes(c->grp_off[g + 1] - c->grp_off[g]);
+    for (int g = 0; g < c->ngroups; ++g) xoff[g + 1] = xoff[g] + nzm_xblock_bytes<2>(c->grp_off[g + 1] - c->grp_off[g]);
     auto al = [&](void **p, size_t bytes, const char *what) -> int {
         if (cudaMalloc(p, std::max<size_t>(bytes, 16)) != cudaSuccess) {
             cudaGetLastError();
@@ -387,8 +410,8 @@ int near_mma_prepare(scd_ctx *c) {
         (rc = al((void **)&c->d_t16_off, sizeof(long long) * c->ntiles, "tile offsets")) ||
         (rc = al((void **)&c->d_xb, (size_t)xoff[c->ngroups], "x blocks")) ||
         (rc = al((void **)&c->d_xb_off, sizeof(long long) * c->ngroups, "x-block offsets")) ||
-        (rc = al((void **)&c->d_xmax, sizeof(unsigned int) * (NZM_R + 1), "x scales")) ||
-        (rc = al((void **)&c->d_xinv, sizeof(float) * NZM_R, "x scales")))
+        (rc = al((void **)&c->d_xmax, sizeof(unsigned int) * (NZM_RMAX + 1), "x scales")) ||
+        (rc = al((void **)&c->d_xinv, sizeof(float) * NZM_RMAX, "x scales")))
         return rc;
     if ((rc = check_cuda(c, cudaMemcpy(c->d_t16_off, toff.data(), sizeof(long long) * c->ntiles, cudaMemcpyHostToDevice),
                          "tile offsets")) ||
@@ -397,7 +420,7 @@ int near_mma_prepare(scd_ctx *c) {
         return rc;
     // one power-of-two scale for all tiles
     unsigned int mbits = 0;
-    unsigned int *dm = c->d_xmax + NZM_R;
+    unsigned int *dm = c->d_xmax + NZM_RMAX;
     if ((rc = check_cuda(c, cudaMemsetAsync(dm, 0, sizeof(unsigned int), c->st), "tile scale"))) return rc;
     k_tabsmax<<<4 * c->nsm, 256, 0, c->st>>>((const float *)c->d_tdata, 2 * c->tile_store, dm);
     if ((rc = check_cuda(c, cudaMemcpyAsync(&mbits, dm, sizeof(unsigned int), cudaMemcpyDeviceToHost, c->st), "tile scale")) ||
@@ -412,47 +435,61 @@ int near_mma_prepare(scd_ctx *c) {
     if ((rc = check_cuda(c, cudaGetLastError(), "tile planes")) ||
         (rc = check_cuda(c, cudaStreamSynchronize(c->st), "tile planes")))
         return rc;
-    // shared memory: meta, the row group's x block, the ring, its slack
-    c->nzm_x1 = nzm_xblock_bytes(c->max_per_group);
+    // shared memory per pass width (16: schedules 0 and 1, 32: schedule 2):
+    // meta, the row group's x block, the ring, its slack
     c->nzm_slack = (slack + 127u) & ~127u;
-    uint32_t max_slot = 0;
-    for (int t = 0; t < c->ntiles; ++t) {
-        const NearTile &tl = c->tiles_h[t];
-        max_slot = std::max(max_slot, nzm_tile_bytes(tl.n1, tl.n2) + nzm_xblock_bytes(tl.n2));
+    for (int w = 0; w < 2; ++w) {
+        auto xbytes = [w](int n) { return w ? nzm_xblock_bytes<2>(n) : nzm_xblock_bytes<1>(n); };
+        const uint32_t x1 = xbytes(c->max_per_group);
+        uint32_t max_slot = 0;
+        for (int t = 0; t < c->ntiles; ++t) {
+            const NearTile &tl = c->tiles_h[t];
+            max_slot = std::max(max_slot, nzm_tile_bytes(tl.n1, tl.n2) + xbytes(tl.n2));
+        }
+        const size_t budget = w ? NZM_SMEM_WIDE : NZM_SMEM;
+        const size_t fixed = 128 + NZM_META + x1 + c->nzm_slack;
+        size_t ring = budget > fixed ? (budget - fixed) / 128 * 128 : 0;
+        if (ring < max_slot) ring = (size_t)max_slot;   // one slot at least (then one CTA per SM)
+        if (fixed + ring > 227 * 1024) return set_error(c, SCD_BAD_ARG, "tensor-core near zone: a tile does not fit");
+        c->nzm_x1[w] = x1;
+        c->nzm_ring[w] = (uint32_t)ring;
     }
-    const size_t fixed = 128 + NZM_META + c->nzm_x1 + c->nzm_slack;
-    size_t ring = NZM_SMEM > fixed ? (NZM_SMEM - fixed) / 128 * 128 : 0;
-    if (ring < max_slot) ring = (size_t)max_slot;   // one slot at least (then one CTA per SM)
-    if (fixed + ring > 227 * 1024) return set_error(c, SCD_BAD_ARG, "tensor-core near zone: a tile does not fit");
-    c->nzm_ring = (uint32_t)ring;
     c->nzm_ready = true;
     return SCD_OK;
 }
 
-// near-zone partial slots of nrhs complex64 right-hand sides (columns of stride n)
+// one pass of schedule S over right-hand sides r0 .. r0 + rg - 1
 template <int S>
-static void near_mma_run_s(scd_ctx *c, const cf *x, int nrhs, const int *done) {
-    const size_t sh = 128 + NZM_META + c->nzm_x1 + c->nzm_ring + c->nzm_slack;
+static void near_mma_pass(scd_ctx *c, const cf *x, int r0, int rg, const int *done) {
+    constexpr int R = NzmSched<S>::R;
+    const int w = R == NZM_RMAX ? 1 : 0;
+    const size_t sh = 128 + NZM_META + c->nzm_x1[w] + c->nzm_ring[w] + c->nzm_slack;
     cudaFuncSetAttribute(k_near_mma<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
-    for (int r0 = 0; r0 < nrhs; r0 += NZM_R) {
-        const int rg = std::min(NZM_R, nrhs - r0);
-        cudaMemsetAsync(c->d_xmax, 0, sizeof(unsigned int) * NZM_R, c->st);
-        k_xabsmax<<<dim3((unsigned)c->nsm, (unsigned)rg), 256, 0, c->st>>>(x, c->n, r0, rg, c->d_xmax);
-        k_xblocks<S><<<c->ngroups, 256, 0, c->st>>>(x, c->n, r0, rg, done, c->d_xmax, c->nzm_sA, c->d_grp_off,
-                                                   c->d_xb_off, c->d_xb, c->d_xinv);
-        NzmArgs a;
-        a.tiles = c->d_tiles; a.grp_tile = c->d_grp_tile; a.grp_off = c->d_grp_off; a.pslot_base = c->d_pslot_base;
-        a.t16 = c->d_t16; a.t16_off = c->d_t16_off; a.xb = c->d_xb; a.xb_off = c->d_xb_off;
-        a.part = c->f_nzpart; a.part_len = c->part_len; a.skip = done; a.r0 = r0; a.rg = rg; a.xinv = c->d_xinv;
-        a.x1_bytes = c->nzm_x1; a.ring_bytes = c->nzm_ring; a.slack_bytes = c->nzm_slack; a.err = c->d_kerr;
-        if (c->timing) cudaEventRecord(c->ev[6], c->st);
-        k_near_mma<S><<<c->ngroups, NZM_THREADS, sh, c->st>>>(a);
-        if (c->timing) cudaEventRecord(c->ev[7], c->st);
-        c->launches += 3;
-    }
+    cudaMemsetAsync(c->d_xmax, 0, sizeof(unsigned int) * R, c->st);
+    k_xabsmax<<<dim3((unsigned)c->nsm, (unsigned)rg), 256, 0, c->st>>>(x, c->n, r0, rg, c->d_xmax);
+    k_xblocks<S><<<c->ngroups, 256, 0, c->st>>>(x, c->n, r0, rg, done, c->d_xmax, c->nzm_sA, c->d_grp_off,
+                                               c->d_xb_off, c->d_xb, c->d_xinv);
+    NzmArgs a;
+    a.tiles = c->d_tiles; a.grp_tile = c->d_grp_tile; a.grp_off = c->d_grp_off; a.pslot_base = c->d_pslot_base;
+    a.t16 = c->d_t16; a.t16_off = c->d_t16_off; a.xb = c->d_xb; a.xb_off = c->d_xb_off;
+    a.part = c->f_nzpart; a.part_len = c->part_len; a.skip = done; a.r0 = r0; a.rg = rg; a.xinv = c->d_xinv;
+    a.x1_bytes = c->nzm_x1[w]; a.ring_bytes = c->nzm_ring[w]; a.slack_bytes = c->nzm_slack; a.err = c->d_kerr;
+    if (c->timing) cudaEventRecord(c->ev[6], c->st);
+    k_near_mma<S><<<c->ngroups, NZM_THREADS, sh, c->st>>>(a);
+    if (c->timing) cudaEventRecord(c->ev[7], c->st);
+    c->launches += 3;
 }
 
+// near-zone partial slots of nrhs complex64 right-hand sides (columns of
+// stride n): passes of 16 (schedules 0, 1) or 32 (schedule 2).  A context
+// keeps one schedule for every pass, so a column meets the same instruction
+// shapes alone and in any batch.
 void near_mma_run(scd_ctx *c, const cf *x, int nrhs, const int *done) {
-    if (c->nzm_sched == 1) near_mma_run_s<1>(c, x, nrhs, done);
-    else near_mma_run_s<0>(c, x, nrhs, done);
+    const int R = c->nzm_sched == 2 ? NZM_RMAX : NZM_R;
+    for (int r0 = 0; r0 < nrhs; r0 += R) {
+        const int rg = std::min(R, nrhs - r0);
+        if (c->nzm_sched == 2) near_mma_pass<2>(c, x, r0, rg, done);
+        else if (c->nzm_sched == 0) near_mma_pass<0>(c, x, r0, rg, done);
+        else near_mma_pass<1>(c, x, r0, rg, done);
+    }
 }

@@ -28,12 +28,13 @@
 
 #include "common.cuh"
 
-constexpr int NZM_R = 16;              // right-hand sides per pass
+constexpr int NZM_R = 16;              // right-hand sides per pass of schedules 0 and 1
+constexpr int NZM_RMAX = 32;           // right-hand sides per pass of schedule 2
 constexpr int NZM_N = 2 * NZM_R;       // schedule 0: x-block rows per half (Re x, then Im x)
 constexpr int NZM_SPLITS = 3;          // schedule 0: (hi A, hi x), (hi A, lo x), (lo A, hi x)
 constexpr int NZM_OPS = 3;             // per A part: Re A X, -Im A Im x, Im A Re x
 
-// Two instruction schedules over the same tile planes:
+// Three instruction schedules over the same tile planes:
 //  0 ("split"): the x block is a hi half then a lo half, each of NZM_N rows
 //    (Re x_r, then Im x_r); per K step 3 splits x 3 ops; accumulator
 //    columns [Re y_r | Im y_r].
@@ -42,9 +43,14 @@ constexpr int NZM_OPS = 3;             // per A part: Re A X, -Im A Im x, Im A R
 //    x halves at once (6 instead of 9 instructions; lo A lo x is included);
 //    accumulator columns [Re y (x hi) | Re y (x lo) | Im y (x hi) | Im y (x lo)],
 //    summed pairwise by the epilogue.  Descriptors advance by constant steps.
+//  2 ("wide"): schedule 1 with R = 32 right-hand sides per pass: every tile
+//    crosses HBM once per 32 right-hand sides instead of 16, with N = 128
+//    instructions; its three accumulators take 384 of the SM's 512 TMEM
+//    columns, so it runs one CTA per SM.
 template <int S> struct NzmSched;
-template <> struct NzmSched<0> { static constexpr int PARTS = NZM_SPLITS, DCOLS = 2 * NZM_R, TMEM = 128; };
-template <> struct NzmSched<1> { static constexpr int PARTS = 2, DCOLS = 4 * NZM_R, TMEM = 256; };
+template <> struct NzmSched<0> { static constexpr int R = NZM_R, PARTS = NZM_SPLITS, DCOLS = 2 * R, TMEM = 128; };
+template <> struct NzmSched<1> { static constexpr int R = NZM_R, PARTS = 2, DCOLS = 4 * R, TMEM = 256; };
+template <> struct NzmSched<2> { static constexpr int R = NZM_RMAX, PARTS = 2, DCOLS = 4 * R, TMEM = 512; };
 
 SCD_HD int nzm_ceil8(int v) { return (v + 7) & ~7; }
 SCD_HD int nzm_ceil16(int v) { return (v + 15) & ~15; }
@@ -104,9 +110,11 @@ SCD_HD void nzm_plane_values(const Tile &tl, const float2 *data, float sA, long 
 // ---- x blocks: per group (n tets) and pass, a K-major B operand of NZM_N
 //      rows (Re x_r, r < 16, then Im x_r) by K16 = ceil16(3n) unknowns, hi block
 //      then lo block, zero for unknowns >= 3n and for absent right-hand sides
+//      (schedule 0); 4R rows by K16 (schedules 1 and 2)
 SCD_HD int nzm_xk(int n) { return nzm_ceil16(3 * n); }
 SCD_HD uint32_t nzm_xhalf_bytes(int n) { return 2u * NZM_N * (uint32_t)nzm_xk(n); }
-SCD_HD uint32_t nzm_xblock_bytes(int n) { return 2u * nzm_xhalf_bytes(n); }
+template <int S = 0>
+SCD_HD uint32_t nzm_xblock_bytes(int n) { return 8u * (uint32_t)NzmSched<S>::R * (uint32_t)nzm_xk(n); }
 // element (row, k) of the hi (or lo) block, in halves
 SCD_HD long long nzm_xidx(int row, int k, int n) { return nzm_cidx(row, k, nzm_xk(n)); }
 
@@ -124,7 +132,7 @@ SCD_HD float nzm_xblock_value(const float2 *x, long long n, int r0, int rg, cons
 }
 
 // f16 bits at position e (halves, 0 <= e < 4 R K16) of a group's x block in
-// schedule S's layout
+// schedule S's layout (sx holds the pass's R scales)
 template <int S>
 SCD_HD uint16_t nzm_xblock_bits(const float2 *x, long long n, int r0, int rg, const int *skip, const float *sx, int s0,
                                 int ng, int e) {
@@ -135,9 +143,10 @@ SCD_HD uint16_t nzm_xblock_bits(const float2 *x, long long n, int r0, int rg, co
         nzm_split(nzm_xblock_value(x, n, r0, rg, skip, sx, s0, ng, e - half * NZM_N * K), hi, lo);
         return half ? lo : hi;
     } else {
+        constexpr int R = NzmSched<S>::R;
         int row, k;
         nzm_cpos(e, K, row, k);
-        const int part = row / NZM_R, r = row % NZM_R, im = part >> 1, want_lo = part & 1;
+        const int part = row / R, r = row % R, im = part >> 1, want_lo = part & 1;
         float v = 0.f;
         if (r < rg && k < 3 * ng && !(skip && skip[r0 + r])) {
             const float2 xv = x[(long long)(r0 + r) * n + 3LL * s0 + k];
@@ -161,11 +170,12 @@ struct NzmOp {
     int first;                      // first instruction of the product: overwrite instead of accumulate
 };
 
-// instruction (kk, s, q) of a product in schedule 1: K step kk, A part s
-// (0 hi, 1 lo), op q
+// instruction (kk, s, q) of a product in schedules 1 and 2 (R right-hand
+// sides): K step kk, A part s (0 hi, 1 lo), op q
 //   q 0: D[:, 0:4R)  += Re A * X[0:4R)     (Re and Im of x, hi and lo halves)
 //   q 1: D[:, 0:2R)  += -Im A * X[2R:4R)   (Re y gets -Im A Im x)
 //   q 2: D[:, 2R:4R) += Im A * X[0:2R)     (Im y gets Im A Re x)
+template <int R>
 SCD_HD NzmOp nzm_op_merged(int use, int n1, int n2, int kk, int s, int q) {
     const uint32_t C1 = (uint32_t)nzm_cols8(n2);
     const uint32_t plane = nzm_plane_bytes(n1, n2);
@@ -180,9 +190,9 @@ SCD_HD NzmOp nzm_op_merged(int use, int n1, int n2, int kk, int s, int q) {
     const uint32_t xsbo = 16u * (uint32_t)nzm_xk(use ? n1 : n2);
     const uint32_t xbase = 256u * kk;
     o.b_lbo = 128u; o.b_sbo = xsbo;
-    if (q == 0) { o.b_off = xbase; o.N = 4 * NZM_R; o.d_col = 0; o.a_neg = 0; }
-    else if (q == 1) { o.b_off = xbase + (2 * NZM_R / 8) * xsbo; o.N = 2 * NZM_R; o.d_col = 0; o.a_neg = 1; }
-    else { o.b_off = xbase; o.N = 2 * NZM_R; o.d_col = 2 * NZM_R; o.a_neg = 0; }
+    if (q == 0) { o.b_off = xbase; o.N = 4 * R; o.d_col = 0; o.a_neg = 0; }
+    else if (q == 1) { o.b_off = xbase + (2 * R / 8) * xsbo; o.N = 2 * R; o.d_col = 0; o.a_neg = 1; }
+    else { o.b_off = xbase; o.N = 2 * R; o.d_col = 2 * R; o.a_neg = 0; }
     o.M = nzm_M(use, n1, n2);
     o.first = kk == 0 && s == 0 && q == 0;
     return o;
@@ -222,7 +232,7 @@ SCD_HD NzmOp nzm_op(int use, int n1, int n2, int kk, int s, int q) {
 template <int S>
 SCD_HD NzmOp nzm_op_s(int use, int n1, int n2, int kk, int s, int q) {
     if constexpr (S == 0) return nzm_op(use, n1, n2, kk, s, q);
-    else return nzm_op_merged(use, n1, n2, kk, s, q);
+    else return nzm_op_merged<NzmSched<S>::R>(use, n1, n2, kk, s, q);
 }
 
 // last byte (exclusive) an instruction reads, relative to its operand start

@@ -18,7 +18,8 @@ module scadyn_gpu
    ! kernel choices (0 = the library's default)
    integer(c_int), parameter, public :: SCD_FFT_DEFAULT = 0, SCD_FFT_POW2 = 1, SCD_FFT_SMOOTH = 2
    integer(c_int), parameter, public :: SCD_NEAR_DEFAULT = 0, SCD_NEAR_CUDA_CORES = 1, &
-                                        SCD_NEAR_TENSOR_SPLIT = 2, SCD_NEAR_TENSOR_MERGED = 3
+                                        SCD_NEAR_TENSOR_SPLIT = 2, SCD_NEAR_TENSOR_MERGED = 3, &
+                                        SCD_NEAR_TENSOR_WIDE = 4
    integer(c_int), parameter, public :: SCD_GS_DEFAULT = 0, SCD_GS_MODIFIED = 1, SCD_GS_CLASSICAL = 2
    integer(c_int), parameter, public :: SCD_FFT_PASSES_DEFAULT = 0, SCD_FFT_PASSES_FUSED_YZ = 1, &
                                         SCD_FFT_PASSES_THREE = 2

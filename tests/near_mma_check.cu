@@ -15,6 +15,7 @@
 // and the ring slack the kernel reserves.  Exits non-zero on a failure.
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -43,8 +44,8 @@ struct Image {   // a byte image of shared memory
     }
 };
 
-// D (TMEM [128 lanes][128 columns]) (+)= op(A) op(B) for one instruction
-static void emulate(float (*tm)[128], uint32_t dcol, const Image &A, uint32_t a_start, const Image &B, uint32_t b_start,
+// D (TMEM [128 lanes][256 columns]) (+)= op(A) op(B) for one instruction
+static void emulate(float (*tm)[256], uint32_t dcol, const Image &A, uint32_t a_start, const Image &B, uint32_t b_start,
                     const NzmOp &o, bool acc) {
     for (int m = 0; m < o.M; ++m) {
         const int lane = o.M == 128 ? m : (m % 16) + 32 * (m / 16);
@@ -70,7 +71,7 @@ static double urand() { rs = rs * 1664525u + 1013904223u; return (rs >> 8) / 167
 
 template <int S>
 static int check_tile(int n1, int n2, int rg, bool with_skip) {
-    const int R = NZM_R;
+    constexpr int R = NzmSched<S>::R;
     // complex64 tile in the k_near_groups layout
     NearTile tl{};
     tl.n1 = n1; tl.n2 = n2; tl.data_off = 0;
@@ -94,7 +95,7 @@ static int check_tile(int n1, int n2, int rg, bool with_skip) {
     for (auto &v : x) v = make_float2((float)urand(), (float)urand());
     std::vector<int> skip(R, 0);
     if (with_skip) skip[3] = skip[rg - 1] = 1;
-    float sx[NZM_R], xinv[NZM_R];
+    float sx[R], xinv[R];
     for (int r = 0; r < R; ++r) {
         float m = 0.f;
         for (long long i = 0; i < n; ++i) m = std::max(m, std::max(std::fabs(x[r * n + i].x), std::fabs(x[r * n + i].y)));
@@ -104,9 +105,9 @@ static int check_tile(int n1, int n2, int rg, bool with_skip) {
     // planes, x blocks, images
     const uint32_t tb = nzm_tile_bytes(n1, n2), P = tb / 8;
     auto xblock = [&](int s0, int ng) {
-        std::vector<unsigned char> b(nzm_xblock_bytes(ng));
+        std::vector<unsigned char> b(nzm_xblock_bytes<S>(ng));
         uint16_t *h = (uint16_t *)b.data();
-        for (int e = 0; e < 4 * NZM_R * nzm_xk(ng); ++e)
+        for (int e = 0; e < 4 * R * nzm_xk(ng); ++e)
             h[e] = nzm_xblock_bits<S>(x.data(), n, 0, rg, skip.data(), sx, s0, ng, e);
         return b;
     };
@@ -141,7 +142,7 @@ static int check_tile(int n1, int n2, int rg, bool with_skip) {
                         return 0;
                     }
                 }
-    static float tm[128][128];
+    static float tm[128][256];
     for (auto &row : tm) for (float &v : row) v = NAN;
     // row product into columns 0.., transposed product into columns DCOLS..
     constexpr int DC = NzmSched<S>::DCOLS;
@@ -199,14 +200,15 @@ int main() {
     int bad = 0, n = 0;
     for (auto &sh : shapes)
         for (int v = 0; v < 2; ++v) {
-            n += 2;
+            n += 3;
             bad += !check_tile<0>(sh[0], sh[1], v ? 16 : 7, v == 1);
             bad += !check_tile<1>(sh[0], sh[1], v ? 16 : 7, v == 1);
+            bad += !check_tile<2>(sh[0], sh[1], v ? 32 : 19, v == 1);
         }
     uint32_t slack = 0;
     for (int a = 1; a <= SCD_GROUP_MAX; ++a)
         for (int b = 1; b <= SCD_GROUP_MAX; ++b)
-            slack = std::max(slack, std::max(nzm_overrun<0>(a, b), nzm_overrun<1>(a, b)));
+            slack = std::max({slack, nzm_overrun<0>(a, b), nzm_overrun<1>(a, b), nzm_overrun<2>(a, b)});
     printf("largest overrun over all shapes: %u bytes\n", slack);
     printf("%d of %d tiles ok\n", n - bad, n);
     return bad ? 1 : 0;

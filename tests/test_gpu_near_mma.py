@@ -1,10 +1,12 @@
 """The tensor-core near zone of the complex64 matvec (scd_grid_desc.near_kernel:
-SCD_NEAR_TENSOR_SPLIT, or SCD_NEAR_TENSOR_MERGED, the default with complex64
-storage) against the CUDA-core kernel (SCD_NEAR_CUDA_CORES) on the same
-operator: mixed-precision T-matrices agree to 1e-6 and both meet the FP64
-residual, iteration counts stay within 20%, results are batch-invariant, and
-the pipeline never times out.  Two grid cell sizes give groups below and
-above 64 rows (M = 64 and M = 128 accumulators)."""
+SCD_NEAR_TENSOR_SPLIT, SCD_NEAR_TENSOR_MERGED -- the default with complex64
+storage -- and SCD_NEAR_TENSOR_WIDE, 32 right-hand sides per pass) against the
+CUDA-core kernel (SCD_NEAR_CUDA_CORES) on the same operator: mixed-precision
+T-matrices agree to 1e-6 and both meet the FP64 residual, iteration counts
+stay within 20%, results are batch-invariant, and the pipeline never times
+out.  Two grid cell sizes give groups below and above 64 rows (M = 64 and
+M = 128 accumulators); the wide schedule runs with more than 32 columns in
+flight, so that full and partial passes both occur."""
 import numpy as np
 import pytest
 
@@ -21,8 +23,9 @@ def rel(a, b):
 
 @pytest.fixture(scope="module",
                 params=[(1.8, api.NEAR_TENSOR_SPLIT), (3.2, api.NEAR_TENSOR_SPLIT),
-                        (1.8, api.NEAR_DEFAULT), (3.2, api.NEAR_TENSOR_MERGED)],
-                ids=["1.8", "3.2", "1.8-default", "3.2-merged"])
+                        (1.8, api.NEAR_DEFAULT), (3.2, api.NEAR_TENSOR_MERGED),
+                        (1.8, api.NEAR_TENSOR_WIDE), (3.2, api.NEAR_TENSOR_WIDE)],
+                ids=["1.8", "3.2", "1.8-default", "3.2-merged", "1.8-wide", "3.2-wide"])
 def ops(request, small_sphere):
     grid_size, kernel = request.param
     k = 1.0 / small_sphere.a
@@ -36,8 +39,10 @@ def ops(request, small_sphere):
 
 def test_tensor_near_zone_T_matches_cuda_core(ops, small_sphere):
     op, a, b = ops
-    mat = O.vswf2constant(small_sphere.coord, small_sphere.etopol, op.geom.k, 2)
-    kw = dict(tol=1e-9, block=16, precision=api.PREC_MIXED, inner_tol=1e-4, max_outer=10, want_x=True)
+    wide = b.desc.near_kernel == api.NEAR_TENSOR_WIDE
+    mat = O.vswf2constant(small_sphere.coord, small_sphere.etopol, op.geom.k, 4 if wide else 2)
+    kw = dict(tol=1e-9, block=48 if wide else 16, precision=api.PREC_MIXED, inner_tol=1e-4, max_outer=10,
+              want_x=True)
     Ta, ita, Xa, rca = a.solve_columns(mat, **kw)
     Tb, itb, Xb, rcb = b.solve_columns(mat, **kw)
     assert rca == api.SCD_OK and rcb == api.SCD_OK
@@ -50,17 +55,20 @@ def test_tensor_near_zone_T_matches_cuda_core(ops, small_sphere):
 
 def test_tensor_near_zone_batch_invariant(ops, small_sphere):
     op, _, b = ops
-    mat = O.vswf2constant(small_sphere.coord, small_sphere.etopol, op.geom.k, 1)
+    wide = b.desc.near_kernel == api.NEAR_TENSOR_WIDE
+    mat = O.vswf2constant(small_sphere.coord, small_sphere.etopol, op.geom.k, 4 if wide else 1)
+    if wide:
+        mat = mat[:40]
     kw = dict(tol=1e-8, precision=api.PREC_MIXED, inner_tol=1e-3, want_x=True)
     x1 = b.solve_columns(mat, block=1, **kw)
-    x2 = b.solve_columns(mat, block=6, **kw)
+    x2 = b.solve_columns(mat, block=mat.shape[0], **kw)
     assert np.array_equal(x1[1], x2[1])
     assert np.array_equal(x1[2], x2[2])
 
 
 def test_tensor_near_zone_profile_runs(ops):
     _, _, b = ops
-    t = b.profile_matvec(reps=3, nrhs=16, precision=api.PREC_MIXED)
+    t = b.profile_matvec(reps=3, nrhs=40, precision=api.PREC_MIXED)
     assert t["matvecs"] >= 3 and t["nearzone_ms"] > 0
 
 

@@ -1,5 +1,6 @@
-"""The tensor-core near-zone schedules (scadyn_b200/csrc/near_mma.cuh; split
-and merged, the latter also checked for its constant descriptor steps), run on
+"""The tensor-core near-zone schedules (scadyn_b200/csrc/near_mma.cuh; split,
+merged and wide -- the merged schedule over 32 right-hand sides -- the last
+two also checked for their constant descriptor steps), run on
 the host through an interpreter of the tcgen05 operand descriptors: the f16
 hi/lo planes and x blocks built by the kernels' own element functions give
 the complex products A x and A^T x of a tile to FP32 accuracy (relative error
@@ -21,4 +22,4 @@ def test_near_mma_schedule_reproduces_tile_products(tmp_path):
                            "-o", str(exe)])
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert "40 of 40 tiles ok" in r.stdout
+    assert "60 of 60 tiles ok" in r.stdout
