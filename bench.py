@@ -73,6 +73,7 @@ NEAR_KERNELS = {"default": 0, "cuda": 1, "split": 2, "merged": 3, "wide": 4}
 GRAM_SCHMIDT = {"default": 0, "modified": 1, "classical": 2}
 FFT_LENGTHS = {"default": 0, "pow2": 1, "smooth": 2}
 FFT_PASSES = {"default": 0, "fused": 1, "three": 2}
+NEAR_SPLIT = {"default": 0, "one": 1, "two": 2}
 
 
 def log(*a):
@@ -359,11 +360,11 @@ def main():
                     help="padded FFT lengths (scd_grid_desc.fft_lengths)")
     ap.add_argument("--fft-passes", default="default", choices=sorted(FFT_PASSES),
                     help="fused y-z FFT pass or three separate passes (scd_grid_desc.fft_passes)")
-    ap.add_argument("--near-split", action="store_true",
-                    help="FP64 near-zone row and column sums split in two partial sums (scd_grid_desc.near_split)")
+    ap.add_argument("--near-split", default="default", choices=sorted(NEAR_SPLIT),
+                    help="partial sums per FP64 near-zone row and column sum (scd_grid_desc.near_split)")
     args = ap.parse_args()
     choices = dict(near_kernel=NEAR_KERNELS[args.near_kernel], fft_lengths=FFT_LENGTHS[args.fft_lengths],
-                   near_split=2 if args.near_split else 0, fft_passes=FFT_PASSES[args.fft_passes])
+                   near_split=NEAR_SPLIT[args.near_split], fft_passes=FFT_PASSES[args.fft_passes])
     gs_choice = GRAM_SCHMIDT[args.gram_schmidt]
     if args.serve:
         print(json.dumps(serve_bench(args.serve, args.serve_scale, check_err=args.serve_scale != "small")),
@@ -637,7 +638,7 @@ def main():
                        "l2": "inputs larger than L2 (near-zone tiles %.2f GB per matvec)" % (solver.nearzone_bytes() / 1e9),
                        "near_kernel": args.near_kernel, "gram_schmidt": args.gram_schmidt,
                        "fft_passes": args.fft_passes,
-                       "near_split": bool(args.near_split),
+                       "near_split": args.near_split,
                        "fft_lengths": [fft_len(2 * v, FFT_LENGTHS[args.fft_lengths] != 1) for v in (desc.Nx, desc.Ny, desc.Nz)],
                        "parallelism": f"replicas x{world}"},
             "t_rel_err_vs_fp64": t_err,
@@ -784,10 +785,9 @@ def sweep_bench(nw, nmax_cap):
     columns per wavelength against the FP64 form.
 
     The operators of all wavelengths together can exceed the device: the
-    wavelengths are then taken in groups whose operators, tensor-core tile
-    planes and matvec work for the 64 slots fit the free memory, one
-    scd_solve_sweep per group; the line reports the groups and the summed
-    device time."""
+    wavelengths are then taken in groups whose operators leave a third of the
+    device free for the solve's work buffers, one scd_solve_sweep per group;
+    the line reports the groups and the summed device time."""
     import torch
     from scadyn_b200 import api, geometry, meshgen
     mesh = meshgen.ellipsoid(17.1, (1.0, 0.8, 0.6), seed=1003, eps=2.5 + 0.05j)
@@ -817,38 +817,28 @@ def sweep_bench(nw, nmax_cap):
              "columns": 2 * ((nmax + 1) ** 2 - 1)}
         return s, w
 
-    def solve_bytes(s, w):
-        """Device memory the solve adds to a built context: tile planes (about
-        1.3x the tiles), FFT and result grids and partial sums for every slot,
-        the incident columns and solutions (FP64 and complex64 copies)."""
-        d = s.desc
-        Px, Py = fft_len(2 * d.Nx, True), fft_len(2 * d.Ny, True)
-        grid = 4 * (Px * Py * d.Nz + d.Nx * d.Ny * d.Nz) * 24
-        return int(1.3 * s.nearzone_bytes() + slots * (grid + s.n * 15 * 24) + 2 * s.n * w["columns"] * 16)
-
-    lead_bytes = lambda n: slots * n * ((opts["m"] + 1) * 8 + 10 * 16 + 8 * 8)   # Krylov bases and vectors
+    # the solve builds each wavelength's work buffers and tile planes while it
+    # has columns in flight (a few wavelengths at a time: columns are taken in
+    # wavelength order) and releases them after; keep this much device memory
+    # free for them and for the slots' Krylov bases
+    reserve = 0.35 * torch.cuda.mem_get_info()[1]
     Ts_all, its_all, st_all, waves, groups = [], [], [], [], []
     setup_s = solve_ms = wall = 0.0
     errs = []
     queue = list(pick)
     carry = None
     while queue or carry:
-        ctxs, ws, need = [], [], 0
+        ctxs, ws = [], []
         while queue or carry:
             t0 = time.time()
             s, w = carry if carry else build(queue.pop(0))
             carry = None
             setup_s += time.time() - t0
-            free = torch.cuda.mem_get_info()[0]
-            add = solve_bytes(s, w)
-            if ctxs and need + add + lead_bytes(s.n) > 0.9 * free:
+            if ctxs and torch.cuda.mem_get_info()[0] < reserve:
                 carry = (s, w)        # solve the group first, keep this operator for the next one
                 break
             ctxs.append(s)
             ws.append(w)
-            need += add
-        if carry and not ctxs:
-            raise RuntimeError("one wavelength's operator does not fit the device")
         lead = ctxs[0]
         lead.timing(reset=True)
         t = time.time()

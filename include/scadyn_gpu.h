@@ -73,7 +73,7 @@ typedef struct scd_grid_desc {
      * src/possu.f90:82-89) */
     int32_t fft_lengths;     /* SCD_FFT_*: padded FFT length per axis */
     int32_t near_kernel;     /* SCD_NEAR_*: near-zone kernel of the complex64 matvec */
-    int32_t near_split;      /* partial sums per near-zone row/column sum of the FP64 matvec: 0 or 1 one, 2 two */
+    int32_t near_split;      /* partial sums per near-zone row/column sum of the FP64 matvec: 1 one, 0 or 2 two */
     int32_t fft_passes;      /* SCD_FFT_PASSES_*: how the y and z transforms run */
 } scd_grid_desc;
 

@@ -9,7 +9,9 @@
  * slots, on its own worker thread and CUDA stream.  A request joining a
  * pool that is solving has its incident columns queued at once; they take
  * slots as running columns finish, beside the columns of the other requests
- * (continuous batching across requests).  Pools stay resident when idle, so
+ * (continuous batching across requests).  A pool has 64 slots and keeps
+ * opts.block columns in flight per unfinished request (all 64 for block 0),
+ * the parallelism separate pools would give.  Pools stay resident when idle, so
  * a later request of the same key skips the operator build; idle pools are
  * evicted, least recently used first, when a new pool needs the memory.  A
  * dispatcher admits queued requests in arrival order whenever the estimated

@@ -90,6 +90,24 @@ int ensure_work(scd_ctx *c, int nrhs) {
     return SCD_OK;
 }
 
+// The buffers a solve builds on demand -- the work areas of the right-hand
+// sides in flight, the complex64 operator copies and the tensor-core tile
+// planes -- freed; the next solve builds them again.  A sweep releases a
+// wavelength's once its last column is done.
+void release_work(scd_ctx *c) {
+    auto fr = [](auto *&p) { if (p) { cudaFree(p); p = nullptr; } };
+    fr(c->d_bpart); fr(c->d_W); fr(c->d_R); fr(c->d_nzpart); fr(c->d_x); fr(c->d_y); fr(c->d_io); fr(c->d_rhs);
+    fr(c->d_xT);
+    c->nrhs_cap = 0;
+    fr(c->f_bpart); fr(c->f_W); fr(c->f_R); fr(c->f_nzpart); fr(c->f_xT);
+    c->f_cap = 0;
+    fr(c->f_P); fr(c->f_Fo); fr(c->f_tw[0]); fr(c->f_tw[1]); fr(c->f_tw[2]); fr(c->f_Fyz);
+    c->f_ready = false;
+    c->fyz_ready_f = false;
+    fr(c->d_t16); fr(c->d_t16_off); fr(c->d_xb); fr(c->d_xb_off); fr(c->d_xmax); fr(c->d_xinv);
+    c->nzm_ready = false;
+}
+
 // error word of the near-zone kernel: a bounded wait that ran out
 int near_status(scd_ctx *c) {
     if (c->near_cfg_err) {
@@ -396,7 +414,7 @@ int scd_create(scd_ctx **out, const scd_grid_desc *d) {
     // only (checked when the near zone is set); 0 selects the defaults
     c->nzm_on = d->near_kernel != SCD_NEAR_CUDA_CORES;
     c->nzm_sched = nzm_sched_of(d->near_kernel);
-    c->near_split = d->near_split == 2 ? 2 : 1;
+    c->near_split = d->near_split == 1 ? 1 : 2;
     c->yz_on = d->fft_passes != SCD_FFT_PASSES_THREE;
     cudaSetDevice(c->dev);
     cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, c->dev);
@@ -926,13 +944,47 @@ static int compute_T_list(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int
         }
     }
     const long long n = c->n;
-    if ((rc = ensure_vswf(c, Nmax))) return rc;
-    cd *d_X = nullptr, *d_T = nullptr;
-    if ((rc = dalloc(c, &d_X, (size_t)n * ncol, "X"))) return rc;
-    if ((rc = dalloc(c, &d_T, (size_t)ntot * ncol, "T"))) { cudaFree(d_X); return rc; }
+    // the incident matrix stays resident unless it would take more than a
+    // quarter of the free device memory (C5: 1350 columns of 3.6 M unknowns,
+    // 78 GB): then it is built in chunks of VSWF_CHUNK columns, once for the
+    // listed right-hand sides and once more for the rows of T
+    constexpr int VSWF_CHUNK = 64;
+    size_t dev_free = 0, dev_total = 0;
+    cudaMemGetInfo(&dev_free, &dev_total);
+    const bool resident = (c->d_mat && c->mat_Nmax == Nmax && c->mat_k == c->k) ||
+                          sizeof(cd) * (size_t)n * ntot <= dev_free / 4;
+    cd *d_X = nullptr, *d_T = nullptr, *d_B = nullptr, *d_chunk = nullptr, *d_Tc = nullptr;
+    auto release = [&]() { cudaFree(d_X); cudaFree(d_T); cudaFree(d_B); cudaFree(d_chunk); cudaFree(d_Tc); };
+    if (resident && (rc = ensure_vswf(c, Nmax))) return rc;
+    if ((rc = dalloc(c, &d_X, (size_t)n * ncol, "X")) || (rc = dalloc(c, &d_T, (size_t)ntot * ncol, "T"))) {
+        release();
+        return rc;
+    }
+    if (!resident && ((rc = dalloc(c, &d_B, (size_t)n * ncol, "right-hand sides")) ||
+                      (rc = dalloc(c, &d_chunk, (size_t)n * VSWF_CHUNK, "VSWF chunk")) ||
+                      (rc = dalloc(c, &d_Tc, (size_t)VSWF_CHUNK * ncol, "T chunk")))) {
+        release();
+        return rc;
+    }
     cudaEventRecord(c->ev[4], c->st);
     std::vector<const cd *> cols(ncol);
-    for (int j = 0; j < ncol; ++j) cols[j] = c->d_mat + (size_t)n * list[j];
+    if (resident) {
+        for (int j = 0; j < ncol; ++j) cols[j] = c->d_mat + (size_t)n * list[j];
+    } else {
+        for (int c0 = 0; c0 < ntot && !rc; c0 += VSWF_CHUNK) {
+            const int cw = std::min(VSWF_CHUNK, ntot - c0);
+            bool any = false;
+            for (int j = 0; j < ncol; ++j) any = any || (list[j] >= c0 && list[j] < c0 + cw);
+            if (!any) continue;
+            if ((rc = setup_vswf(c, Nmax, d_chunk, c0, cw))) break;
+            for (int j = 0; j < ncol && !rc; ++j)
+                if (list[j] >= c0 && list[j] < c0 + cw)
+                    rc = check_cuda(c, cudaMemcpyAsync(d_B + (size_t)n * j, d_chunk + (size_t)n * (list[j] - c0),
+                                                       sizeof(cd) * n, cudaMemcpyDeviceToDevice, c->st), "right-hand side");
+        }
+        if (rc) { release(); return rc; }
+        for (int j = 0; j < ncol; ++j) cols[j] = d_B + (size_t)n * j;
+    }
     const int ns = o->block > 0 ? o->block : ncol;
     std::vector<int> it(ncol, 0);
     int worst = batch_solve(c, ncol, cols.data(), d_X, o->tol, o->m, o->cycles, ns, it.data(), nullptr, nullptr,
@@ -943,7 +995,20 @@ static int compute_T_list(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int
     }
     if (iters) for (int j = 0; j < ncol; ++j) iters[j] = it[j];
     if (worst == SCD_OK || worst == SCD_NOT_CONVERGED) {
-        launch_T_assemble(c, c->d_mat, ntot, 0, ncol, d_X, d_T);
+        if (resident) {
+            launch_T_assemble(c, c->d_mat, ntot, 0, ncol, d_X, d_T);
+        } else {
+            // rows c0 .. c0 + cw - 1 of T from the chunk's columns; every
+            // entry is summed as in the resident path (same K split)
+            for (int c0 = 0; c0 < ntot && !rc; c0 += VSWF_CHUNK) {
+                const int cw = std::min(VSWF_CHUNK, ntot - c0);
+                if ((rc = setup_vswf(c, Nmax, d_chunk, c0, cw))) break;
+                launch_T_assemble(c, d_chunk, cw, 0, ncol, d_X, d_Tc);
+                rc = check_cuda(c, cudaMemcpy2DAsync(d_T + c0, sizeof(cd) * ntot, d_Tc, sizeof(cd) * cw, sizeof(cd) * cw,
+                                                     ncol, cudaMemcpyDeviceToDevice, c->st), "T rows");
+            }
+            if (rc) worst = rc;
+        }
         cudaEventRecord(c->ev[5], c->st);
         std::vector<cd> h((size_t)ntot * ncol);
         rc = check_cuda(c, cudaMemcpyAsync(h.data(), d_T, sizeof(cd) * h.size(), cudaMemcpyDeviceToHost, c->st), "T");
@@ -961,8 +1026,7 @@ static int compute_T_list(scd_ctx *c, int32_t Nmax, const scd_solve_opts *o, int
         }
     }
     cudaStreamSynchronize(c->st);
-    cudaFree(d_X);
-    cudaFree(d_T);
+    release();
     return worst;
 }
 
@@ -1013,6 +1077,10 @@ struct SweepSource final : ColumnSource {
         else if (!cv && worst[w] == SCD_OK) worst[w] = SCD_NOT_CONVERGED;
     }
     int op_of(int tag) override { return jobs[tag].first; }
+    // jobs are in wavelength order: w has columns left while the next job is
+    // at or before its last
+    std::vector<size_t> last_job;
+    bool op_pending(int op) override { return next_job <= last_job[op]; }
 };
 }  // namespace
 
@@ -1049,6 +1117,7 @@ int scd_solve_sweep(scd_ctx *const *ctxs, int32_t nw, const int32_t *Nmax, const
         if ((rc = dalloc(c, &X, (size_t)c->n * ncol, "sweep solutions"))) { release(); return rc; }
         src.X.push_back(X);
         for (int j = 0; j < ncol; ++j) src.jobs.emplace_back(w, j);
+        src.last_job.push_back(src.jobs.size() - 1);
     }
     cudaEventRecord(c->ev[4], c->st);
     const int ns = o->block > 0 ? o->block : 64;

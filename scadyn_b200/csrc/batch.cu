@@ -1003,15 +1003,25 @@ int batch_run(scd_ctx *c, ColumnSource &src, double tol, int m, int cycles, int 
             return set_error(c, SCD_BAD_ARG, "operators of one batch need the same device and unknowns");
     int rc = batch_prepare(c, ns, m, mixed, bb);
     if (rc) return rc;
-    for (scd_ctx *o : ops) {
+    // work buffers of operator w for nm complex64 and nr FP64 right-hand
+    // sides (mixed), or nr FP64 ones: one operator is sized for every slot up
+    // front; several grow to the next power of two of their columns in flight
+    auto prepare = [&](int w, int nm, int nr) -> int {
+        scd_ctx *o = ops[w];
+        int r;
         if (mixed) {
-            if ((rc = ensure_single(o)) || (rc = ensure_work_single(o, ns)) || (rc = ensure_work(o, ns)))
-                return o == c ? rc : set_error(c, rc, "operator of the batch: %s", o->err.c_str());
-        } else if ((rc = ensure_work(o, ns))) {
-            return o == c ? rc : set_error(c, rc, "operator of the batch: %s", o->err.c_str());
+            r = ensure_single(o);
+            if (!r && nm > 0) r = ensure_work_single(o, nm);
+            if (!r) r = ensure_work(o, std::max(nr, 1));
+        } else {
+            r = ensure_work(o, std::max(nr, 1));
         }
-    }
+        return r == SCD_OK || o == c ? r : set_error(c, r, "operator of the batch: %s", o->err.c_str());
+    };
+    auto grown = [ns](int v) { int p = 1; while (p < v) p <<= 1; return std::min(p, ns); };
+    if (nops == 1 && (rc = prepare(0, ns, ns))) return rc;
     if (mixed && (rc = ensure_work(c, ns))) return rc;
+    std::vector<char> live(nops, nops == 1 ? 1 : 0);   // operators holding work buffers
     std::vector<int> sop(ns, 0), cnt_m(nops, 0), cnt_r(nops, 0);   // slot operators, columns per operator
     if (!c->d_bar) {
         if (cudaMalloc(&c->d_bar, sizeof(GridBarrier)) != cudaSuccess || cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess)
@@ -1084,6 +1094,14 @@ int batch_run(scd_ctx *c, ColumnSource &src, double tol, int m, int cycles, int 
                 }
             }
         }
+        if (nops > 1) {
+            for (int w = 0; w < nops; ++w) {
+                const int nm = mixed ? cnt_m[w] : 0, nr = mixed ? cnt_r[w] : cnt_m[w];
+                if (nm == 0 && nr == 0) continue;
+                if ((rc = prepare(w, nm ? grown(nm) : 0, nr ? grown(nr) : 0))) return rc;
+                live[w] = 1;
+            }
+        }
         cudaMemcpyAsync(bb.slots, hs, sizeof(Slot) * ns, cudaMemcpyHostToDevice, c->st);
         if (mixed) {
             const dim3 g2(std::min<long long>((n + 255) / 256, 1024), ns);
@@ -1108,6 +1126,18 @@ int batch_run(scd_ctx *c, ColumnSource &src, double tol, int m, int cycles, int 
         if ((rc = check_cuda(c, cudaStreamSynchronize(c->st), "tick"))) return rc;
         for (int s = 0; s < ns; ++s)
             if (hs[s].status == SCD_TIMEOUT) return set_error(c, SCD_TIMEOUT, "grid barrier wait expired in the batch solver");
+        // operators with no column in a slot and none left to hand out give
+        // their work buffers back (every kernel of theirs has finished: the
+        // stream synchronisation above follows the join of their streams)
+        for (int w = 0; w < nops && nops > 1; ++w) {
+            if (!live[w] || ops[w] == c || src.op_pending(w)) continue;
+            bool used = false;
+            for (int s = 0; s < ns && !used; ++s) used = hs[s].mode != SLOT_FREE && sop[s] == w;
+            if (!used) {
+                release_work(ops[w]);
+                live[w] = 0;
+            }
+        }
     }
     return check_cuda(c, cudaStreamSynchronize(c->st), "batch end");
 }

@@ -111,7 +111,7 @@ struct scd_ctx {
     long long tile_store = 0;            // stored elements (tile_elems summed)
     long long max_tile_store = 0;        // largest tile_elems
     long long B_ref = 0;                 // blocks in the reference layout
-    int near_split = 1;                  // partial sums per near-zone row/column sum (scd_grid_desc.near_split)
+    int near_split = 2;                  // partial sums per near-zone row/column sum (scd_grid_desc.near_split)
     int near_cfg_err = 0;                // a near-zone launch was skipped: a tile outgrew the shared-memory ring
     // partial-sum slots per group: slot 0 holds the group's row sums over
     // all its tiles, slots 1.. the M^T x products of the tiles (g', g),
@@ -228,12 +228,16 @@ struct ColumnSource {
     virtual bool wait_more() { return false; }
     // the operator (index into batch_run's ops) that column `tag` is solved with
     virtual int op_of(int tag) { (void)tag; return 0; }
+    // false once operator `op` has no column left to hand out
+    virtual bool op_pending(int op) { (void)op; return true; }
 };
 // Batched solves on context c's slots and stream.  With ops (contexts of
 // the same device and the same unknowns n, e.g. one per wavelength of one
 // mesh), every column is solved with its own operator ops[op_of(tag)]: the
 // matvecs of a tick run per operator (each on its context's stream, joined
-// back), the Arnoldi steps of all slots in one launch.
+// back), the Arnoldi steps of all slots in one launch.  An operator's work
+// buffers then grow with the columns it has in flight, and are released
+// (release_work) once it has none left to solve.
 int batch_run(scd_ctx *c, ColumnSource &src, double tol, int m, int cycles, int ns, int precision, double inner_tol,
               int max_outer, const std::vector<scd_ctx *> *ops = nullptr);
 void batch_free(scd_ctx *c);
@@ -244,7 +248,8 @@ int batch_solve(scd_ctx *c, int ncol, const cd *const *rhs_cols, cd *X, double t
 int setup_green(scd_ctx *c, const scd_c128 *Fg_host);
 int setup_projectors_device(scd_ctx *c);
 int setup_nearzone_device(scd_ctx *c, int prec);
-int setup_vswf(scd_ctx *c, int Nmax, cd *d_mat);   // slot-ordered (n, 2nm)
+// slot-ordered (n, 2nm), or columns c0 .. c0 + cw - 1 of it (n, cw)
+int setup_vswf(scd_ctx *c, int Nmax, cd *d_mat, int c0 = 0, int cw = -1);
 void launch_T_assemble(scd_ctx *c, const cd *d_mat, int ncol_total, int col0, int ncb,
                        const cd *d_X, cd *d_T);
 
@@ -252,6 +257,7 @@ void launch_T_assemble(scd_ctx *c, const cd *d_mat, int ncol_total, int col0, in
 int set_error(scd_ctx *c, int code, const char *fmt, ...);
 int check_cuda(scd_ctx *c, cudaError_t e, const char *what);
 int ensure_work(scd_ctx *c, int nrhs);
+void release_work(scd_ctx *c);
 int near_status(scd_ctx *c);
 // columns of the interleaved matvec input for nrhs right-hand sides: passes
 // of 16, at least 2 (16-byte rows for complex64)

@@ -1142,10 +1142,12 @@ void near_launch(scd_ctx *c, const ST *data, const C *x, int nrhs, const int *do
 
 template <typename ST, typename C>
 void near_dispatch(scd_ctx *c, const ST *data, const C *x, int nrhs, const int *done) {
-    // near_split 2: two partial sums per row and column (two lanes each
-    // at one right-hand side) for the FP64 matvec; the complex64 matvec of the
-    // mixed form keeps one sum per lane (its U = 4 kernel would lose occupancy
-    // to the second set of accumulators)
+    // near_split 2 (the default): two partial sums per row and column (two
+    // lanes each at one right-hand side, both in one lane at four) for the
+    // FP64 matvec, the same arithmetic per sum at U = 1 and U = 4, so a column
+    // keeps its bits alone and in a batch; the complex64 matvec of the mixed
+    // form keeps one sum per lane (its U = 4 kernel would lose occupancy to
+    // the second set of accumulators)
     if (c->near_split == 2 && std::is_same<C, cd>::value) {
         if (nrhs == 1) near_launch<ST, C, 1, 2>(c, data, x, nrhs, done);
         else near_launch<ST, C, 4, 2>(c, data, x, nrhs, done);

@@ -112,7 +112,7 @@ struct Pool {
 void estimate(const scd_request *r, const scd_grid_desc &d, int64_t *pool_bytes, int64_t *req_bytes) {
     const double T = r->T, n = 3.0 * T;
     const int ncol = ncols_of(r->Nmax);
-    const int ns = std::max(1, std::min(r->opts.block > 0 ? r->opts.block : 64, 64));
+    const int ns = 64;   // a pool's slots: `block` columns in flight per request it serves
     const bool mixed = r->opts.precision == SCD_PREC_MIXED;
     auto p2 = [](int v) { int p = 8; while (p < 2 * v) p <<= 1; return (double)p; };
     const double Px = p2(d.Nx), Py = p2(d.Ny);
@@ -195,6 +195,7 @@ struct PoolSource final : ColumnSource {
     std::shared_ptr<Pool> P;
     std::map<int, std::pair<int64_t, int>> inflight;   // tag -> (request, column)
     int next_tag = 0;
+    int block = 64;                                    // columns in flight per request
 
     // set up newly admitted requests: incident columns on the device, room for
     // their solutions, their columns queued
@@ -238,6 +239,9 @@ struct PoolSource final : ColumnSource {
         take_joining();
         std::lock_guard<std::mutex> g(s->m);
         if (P->cols.empty()) return false;
+        // `block` columns in flight per unfinished request of the pool: the
+        // parallelism separate pools would give them, on one operator
+        if ((int)inflight.size() >= block * std::max(1, P->active)) return false;
         const auto job = P->cols.front();
         P->cols.pop_front();
         Req &r = s->reqs[job.first];
@@ -326,8 +330,8 @@ void pool_worker(scd_server *s, std::shared_ptr<Pool> P, Req seed) {
         src.s = s;
         src.P = P;
         const scd_solve_opts &o = seed.opts;
-        const int ns = o.block > 0 ? o.block : 64;
-        rc = batch_run(ctx, src, o.tol, o.m, o.cycles, ns, o.precision, o.inner_tol, o.max_outer);
+        src.block = o.block > 0 ? std::min(o.block, 64) : 64;
+        rc = batch_run(ctx, src, o.tol, o.m, o.cycles, 64, o.precision, o.inner_tol, o.max_outer);
         if (rc) err = scd_last_error(ctx);
         // a solver error fails whatever is still in flight or queued
         std::lock_guard<std::mutex> g(s->m);

@@ -665,7 +665,10 @@ __device__ void legendre_col(int N, double x, double *out, double *diag_scratch)
     }
 }
 
-__global__ void k_vswf(const double *tc, const double *vol, int T, double k, int Nmax, cd *mat, long long ld) {
+// columns c0 .. c0 + cw - 1 of the 2nm (M columns, then N columns) into
+// mat[(col - c0) * ld + 3 s + d]
+__global__ void k_vswf(const double *tc, const double *vol, int T, double k, int Nmax, cd *mat, long long ld, int c0,
+                       int cw) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= T) return;
     const double *p = tc + 12LL * s;
@@ -710,11 +713,12 @@ __global__ void k_vswf(const double *tc, const double *vol, int T, double k, int
             const cd Pv = cscale(e, Yr);
             const cd Mv[3] = {cmk(0, 0), cscale(B3, cc * alpha), cscale(B2, -cc * alpha)};
             const cd Nv[3] = {cscale(Pv, cc * beta), cscale(B2, cc * gamma), cscale(B3, cc * gamma)};
+            const bool mcol = ind >= c0 && ind < c0 + cw, ncol = nm + ind >= c0 && nm + ind < c0 + cw;
             for (int d = 0; d < 3; ++d) {
                 const cd Mc = cadd(cadd(cscale(Mv[0], H[d][0]), cscale(Mv[1], H[d][1])), cscale(Mv[2], H[d][2]));
                 const cd Nc = cadd(cadd(cscale(Nv[0], H[d][0]), cscale(Nv[1], H[d][1])), cscale(Nv[2], H[d][2]));
-                mat[(long long)ind * ld + 3LL * s + d] = cscale(Mc, sv);
-                mat[(long long)(nm + ind) * ld + 3LL * s + d] = cscale(Nc, sv);
+                if (mcol) mat[(long long)(ind - c0) * ld + 3LL * s + d] = cscale(Mc, sv);
+                if (ncol) mat[(long long)(nm + ind - c0) * ld + 3LL * s + d] = cscale(Nc, sv);
             }
         }
     }
@@ -923,12 +927,15 @@ int setup_nearzone_device(scd_ctx *c, int prec) {
     return rc;
 }
 
-int setup_vswf(scd_ctx *c, int Nmax, cd *d_mat) {
+int setup_vswf(scd_ctx *c, int Nmax, cd *d_mat, int c0, int cw) {
     NvtxRange range("VSWF columns");
     if (!c->have_mesh) return set_error(c, SCD_NOT_READY, "VSWF right-hand sides need scd_set_mesh");
     if (!c->have_k) return set_error(c, SCD_NOT_READY, "VSWF right-hand sides need scd_set_wavenumber");
     if (Nmax < 1 || Nmax > VSWF_NMAX - 2) return set_error(c, SCD_BAD_ARG, "Nmax %d outside 1..%d", Nmax, VSWF_NMAX - 2);
-    k_vswf<<<(c->T + 127) / 128, 128, 0, c->st>>>(c->d_tc, c->d_tvol, c->T, c->k, Nmax, d_mat, c->n);
+    const int ntot = 2 * ((Nmax + 1) * (Nmax + 1) - 1);
+    if (cw < 0) { c0 = 0; cw = ntot; }
+    if (c0 < 0 || cw < 1 || c0 + cw > ntot) return set_error(c, SCD_BAD_ARG, "VSWF columns %d..%d outside 1..%d", c0 + 1, c0 + cw, ntot);
+    k_vswf<<<(c->T + 127) / 128, 128, 0, c->st>>>(c->d_tc, c->d_tvol, c->T, c->k, Nmax, d_mat, c->n, c0, cw);
     return check_cuda(c, cudaGetLastError(), "vswf");
 }
 

@@ -1,8 +1,9 @@
 """The FP64 near-zone kernel with split row and column sums
-(scd_grid_desc.near_split = 2: two lanes per sum at one right-hand side, two
-partial sums per lane at four): the FP64 matvec against the oracle, solutions
-against the default kernel, and bit-identical columns alone and in batches
-(the mixed form's complex64 kernels are left unsplit)."""
+(scd_grid_desc.near_split = 2, the default: two lanes per sum at one
+right-hand side, two partial sums per lane at four): the FP64 matvec against
+the oracle, solutions against the one-sum kernel (near_split = 1), and
+bit-identical columns alone and in batches (the mixed form's complex64
+kernels are left unsplit)."""
 import numpy as np
 import pytest
 
