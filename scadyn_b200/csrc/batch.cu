@@ -53,6 +53,7 @@ struct TickArgs {
     double *cpart;  // [NSMAX][NCH][4] chunk partials
     double *ctot;   // [2][NSMAX][4] slot totals
     int *ccnt;      // [NSMAX] chunks published in the current reduction
+    int *qctr;      // [QMAX] work-queue counters, one per phase of the tick
     GridBarrier *bar;
     int *err;
     long long n;
@@ -102,6 +103,30 @@ struct Chunks {
         gw = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
         nw = (int)(((long long)gridDim.x * blockDim.x) >> 5);
         lane = threadIdx.x & 31;
+    }
+};
+
+// Work items (slot, chunk) of a phase are handed to warps in runs of QG by
+// an atomic counter, the slots with the most Krylov vectors first, so that
+// warps finish a phase together instead of all waiting at the next grid
+// barrier for the one whose fixed share held the long slots.  Which warp
+// takes an item does not change any result: every item publishes its partial
+// sums to a fixed place, summed in chunk order.
+constexpr int QG = 4;                          // items per grab
+constexpr int QMAX = 256;                      // phases (counters) per tick
+static_assert(QMAX >= 8 + 3 * (SCD_M_MAX + 1), "one counter per phase of a tick");
+struct WorkQueue {
+    int *ctr;
+    int n, lane, it = 0, end = 0;
+    __device__ WorkQueue(int *c, int nitems, int l) : ctr(c), n(nitems), lane(l) {}
+    __device__ bool next() {
+        if (++it < end) return true;
+        int base = 0;
+        if (lane == 0) base = atomicAdd(ctr, QG);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        it = base;
+        end = min(n, base + QG);
+        return base < n;
     }
 };
 
@@ -224,15 +249,16 @@ __device__ void givens_step(const TickArgs<C> &a, const int *smode, const int *s
 // and the slots' next modes.  Call after the grid barrier that follows
 // givens_step.
 template <typename C>
-__device__ void cycle_end(const TickArgs<C> &a, const Chunks &ch, int nch, const int *smode, cd (*ysm)[SCD_M_MAX + 1]) {
+__device__ void cycle_end(const TickArgs<C> &a, const Chunks &ch, int nch, const int *smode, cd (*ysm)[SCD_M_MAX + 1],
+                          const int *sorder, int *qctr) {
     const long long n = a.n;
     constexpr int TUC = sizeof(C) == 8 ? 2 * TU : TU;
     const int lane = ch.lane;
     const int nitems = a.ns * nch;
     {
         cd *yw = ysm[threadIdx.x >> 5];
-        for (int it = ch.gw; it < nitems; it += ch.nw) {
-            const int s = it / nch, c = it - s * nch;
+        for (WorkQueue q(qctr, nitems, lane); q.next();) {
+            const int s = sorder[q.it / nch], c = q.it % nch;
             if (smode[s] != SLOT_ARNOLDI) continue;
             const Slot *sl = a.slots + s;
             if (!__ldcg(&sl->finish)) continue;      // uniform across the warp (L2 read after the barrier)
@@ -360,10 +386,23 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
         swpos[s] = max(a.slots[s].mpos, 0);   // A v of the slot sits in column mpos of w
     }
     __syncthreads();
+    // slots by cost (Krylov vectors a step reads), largest first, ties by index
+    __shared__ int sorder[NSMAX];
+    if (threadIdx.x == 0) {
+        auto cost = [&](int s) { return smode[s] == SLOT_ARNOLDI ? sstep[s] + 2 : smode[s] == SLOT_START ? 1 : 0; };
+        for (int s = 0; s < a.ns; ++s) {
+            const int cs = cost(s);
+            int j = s - 1;
+            while (j >= 0 && cost(sorder[j]) < cs) { sorder[j + 1] = sorder[j]; --j; }
+            sorder[j + 1] = s;
+        }
+    }
+    __syncthreads();
+    int ph = 0;        // phases so far: each takes the next work-queue counter
     int parity = 0;
     // ---- phase A: first reduction of every active slot
-    for (int it = ch.gw; it < nitems; it += ch.nw) {
-        const int s = it / NCH, c = it - s * NCH;
+    for (WorkQueue q(a.qctr + ph++, nitems, lane); q.next();) {
+        const int s = sorder[q.it / NCH], c = q.it % NCH;
         const int md = smode[s];
         if (md != SLOT_START && md != SLOT_ARNOLDI) continue;
         const long long qa = c * ch.L, qb = min(n, qa + ch.L);
@@ -434,8 +473,8 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
     }
     __syncthreads();
     // cycle starts: normalise V0, set g, b_norm
-    for (int it = ch.gw; it < nitems; it += ch.nw) {
-        const int s = it / NCH, c = it - s * NCH;
+    for (WorkQueue q(a.qctr + ph++, nitems, lane); q.next();) {
+        const int s = sorder[q.it / NCH], c = q.it % NCH;
         if (smode[s] != SLOT_START) continue;
         const double beta = sqrt(tot[s][0]);
         const long long qa = c * ch.L, qb = min(n, qa + ch.L);
@@ -473,8 +512,8 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
     }
     // ---- MGS for the Arnoldi slots: one barrier per term
     for (int k = 1; k <= kmax; ++k) {
-        for (int it = ch.gw; it < nitems; it += ch.nw) {
-            const int s = it / NCH, c = it - s * NCH;
+        for (WorkQueue q(a.qctr + ph++, nitems, lane); q.next();) {
+            const int s = sorder[q.it / NCH], c = q.it % NCH;
             if (smode[s] != SLOT_ARNOLDI) continue;
             const int i = sstep[s] + 1;
             if (k > i) continue;
@@ -529,8 +568,8 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
     // FP64 per element, one rounding to the storage precision), ||w||^2
     if (a.cgs) {
         cd *hs = ysm[threadIdx.x >> 5];
-        for (int it = ch.gw; it < nitems; it += ch.nw) {
-            const int s = it / NCH, c = it - s * NCH;
+        for (WorkQueue q(a.qctr + ph++, nitems, lane); q.next();) {
+            const int s = sorder[q.it / NCH], c = q.it % NCH;
             if (smode[s] != SLOT_ARNOLDI) continue;
             const int i = sstep[s] + 1;
             const double *tt = a.ctm + (size_t)s * CGS_NV;
@@ -588,8 +627,8 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
     for (int s = 0; s < a.ns; ++s)
         if (sro[s]) jmax = max(jmax, sstep[s] + 1);
     for (int j = 1; j <= jmax; ++j) {
-        for (int it = ch.gw; it < nitems; it += ch.nw) {
-            const int s = it / NCH, c = it - s * NCH;
+        for (WorkQueue q(a.qctr + ph++, nitems, lane); q.next();) {
+            const int s = sorder[q.it / NCH], c = q.it % NCH;
             if (!sro[s] || j > sstep[s] + 1) continue;
             const long long qa = c * ch.L, qb = min(n, qa + ch.L);
             const C *vj = a.V + (size_t)s * (a.m + 1) * n + (size_t)(j - 1) * n;
@@ -623,8 +662,8 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
                 Hc[j - 1] = cadd(Hc[j - 1], cmk(tot[s][0], tot[s][1]));
             }
         }
-        for (int it = ch.gw; it < nitems; it += ch.nw) {
-            const int s = it / NCH, c = it - s * NCH;
+        for (WorkQueue q(a.qctr + ph++, nitems, lane); q.next();) {
+            const int s = sorder[q.it / NCH], c = q.it % NCH;
             if (!sact[s]) continue;
             const cd hr = cmk(tot[s][0], tot[s][1]);
             const long long qa = c * ch.L, qb = min(n, qa + ch.L);
@@ -650,8 +689,8 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
         __syncthreads();   // sact / tot are rewritten by the next round
     }
     if (jmax > 0) {
-        for (int it = ch.gw; it < nitems; it += ch.nw) {
-            const int s = it / NCH, c = it - s * NCH;
+        for (WorkQueue q(a.qctr + ph++, nitems, lane); q.next();) {
+            const int s = sorder[q.it / NCH], c = q.it % NCH;
             if (!sro[s]) continue;
             const long long qa = c * ch.L, qb = min(n, qa + ch.L);
             const C *ws = a.w + (size_t)swpos[s] * n;
@@ -678,8 +717,8 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
         __syncthreads();
     }
     // ---- v_i = w / h(i+1,i) and the Givens update
-    for (int it = ch.gw; it < nitems; it += ch.nw) {
-        const int s = it / NCH, c = it - s * NCH;
+    for (WorkQueue q(a.qctr + ph++, nitems, lane); q.next();) {
+        const int s = sorder[q.it / NCH], c = q.it % NCH;
         if (smode[s] != SLOT_ARNOLDI) continue;
         const int i = sstep[s] + 1;
         const double hn = shn[s];
@@ -706,7 +745,7 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
         givens_step(a, smode, sstep, shn, sact);
     }
     grid_barrier(a.bar, gridDim.x, a.err);
-    cycle_end(a, ch, NCH, smode, ysm);
+    cycle_end(a, ch, NCH, smode, ysm, sorder, a.qctr + ph);
 }
 
 // matvec input per slot, compacted: x at a cycle start, v_step during
@@ -904,7 +943,7 @@ int batch_prepare(scd_ctx *c, int ns, int m, int mixed, BatchBuffers &b) {
     if ((rc = al((void **)&b.slots, sizeof(Slot) * ns, "slots"))) return rc;
     if ((rc = al((void **)&b.cpart, sizeof(double) * (size_t)NSMAX * NCH * 4, "chunk partials"))) return rc;
     if ((rc = al((void **)&b.ctot, sizeof(double) * 2 * NSMAX * 4, "slot totals"))) return rc;
-    if ((rc = al((void **)&b.ccnt, sizeof(int) * NSMAX, "chunk counters"))) return rc;
+    if ((rc = al((void **)&b.ccnt, sizeof(int) * (NSMAX + QMAX), "chunk and work-queue counters"))) return rc;
     if (mixed && c->cgs_on) {
         if ((rc = al((void **)&b.cpm, sizeof(double) * (size_t)ns * NCH * CGS_NV, "Gram-Schmidt partials"))) return rc;
         if ((rc = al((void **)&b.ctm, sizeof(double) * (size_t)ns * CGS_NV, "Gram-Schmidt totals"))) return rc;
@@ -964,7 +1003,7 @@ static int launch_tick(scd_ctx *c, BatchBuffers &bb, int ns, int nact, int m, in
     TickArgs<C> a;
     a.slots = bb.slots; a.ns = ns; a.V = (C *)bb.V; a.H = bb.H; a.cs = bb.cs; a.sn = bb.sn; a.g = bb.g; a.y = bb.y;
     a.x = (C *)bb.x; a.rhs = (C *)bb.rhs; a.w = (C *)bb.W; a.red = bb.red; a.bar = c->d_bar; a.err = c->d_err;
-    a.cpart = bb.cpart; a.ctot = bb.ctot; a.ccnt = bb.ccnt;
+    a.cpart = bb.cpart; a.ctot = bb.ctot; a.ccnt = bb.ccnt; a.qctr = bb.ccnt + NSMAX;
     a.n = c->n; a.m = m; a.max_cycles = cycles; a.tol = tol; a.mixed = mixed;
     a.cgs = (mixed && c->cgs_on && bb.cpm) ? 1 : 0;
     a.cpm = bb.cpm; a.ctm = bb.ctm;
@@ -976,7 +1015,7 @@ static int launch_tick(scd_ctx *c, BatchBuffers &bb, int ns, int nact, int m, in
     }
     NvtxRange r("arnoldi tick");
     void *args[] = {&a};
-    cudaMemsetAsync(bb.ccnt, 0, sizeof(int) * NSMAX, c->st);
+    cudaMemsetAsync(bb.ccnt, 0, sizeof(int) * (NSMAX + QMAX), c->st);
     cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_tick<C>, dim3(bb.grid), dim3(BT), args, 0, c->st);
     c->launches += 2;
     return check_cuda(c, e, "tick launch");

@@ -375,14 +375,18 @@ int solving_pools(const scd_server *s) {
 void dispatch_loop(scd_server *s) {
     std::unique_lock<std::mutex> lk(s->m);
     while (true) {
-        // join the workers of retired pools
-        for (auto &p : s->retired) {
-            std::thread t = std::move(p->worker);
+        // join the workers of retired pools: take the list first, since
+        // workers that retire meanwhile append to it (only this thread
+        // creates and joins the worker threads)
+        if (!s->retired.empty()) {
+            std::vector<std::shared_ptr<Pool>> done;
+            done.swap(s->retired);
             lk.unlock();
-            if (t.joinable()) t.join();
+            for (auto &p : done)
+                if (p->worker.joinable()) p->worker.join();
             lk.lock();
+            continue;   // re-check: more may have retired, and memory came back
         }
-        s->retired.clear();
         // admit, in arrival order, every queued request that fits now: into
         // the resident pool of its key, or into a new pool (evicting idle
         // pools, least recently used first, when their memory is needed)
