@@ -106,10 +106,12 @@ struct Chunks {
     }
 };
 
-// Work items (slot, chunk) of a phase are handed to warps in runs of QG by
-// an atomic counter, the slots with the most Krylov vectors first, so that
-// warps finish a phase together instead of all waiting at the next grid
-// barrier for the one whose fixed share held the long slots.  Which warp
+// Work items (slot, chunk) of a phase.  With at least two items per warp
+// they are handed out in runs of QG by an atomic counter, the slots with the
+// most Krylov vectors first, so that warps finish a phase together instead of
+// waiting at the next grid barrier for the one whose fixed share held the
+// long slots; with fewer, warp w takes items w, w + warps, ... (a counter
+// that every warp polls would cost more than the imbalance).  Which warp
 // takes an item does not change any result: every item publishes its partial
 // sums to a fixed place, summed in chunk order.
 constexpr int QG = 4;                          // items per grab
@@ -117,9 +119,17 @@ constexpr int QMAX = 256;                      // phases (counters) per tick
 static_assert(QMAX >= 8 + 3 * (SCD_M_MAX + 1), "one counter per phase of a tick");
 struct WorkQueue {
     int *ctr;
-    int n, lane, it = 0, end = 0;
-    __device__ WorkQueue(int *c, int nitems, int l) : ctr(c), n(nitems), lane(l) {}
+    int n, lane, it, end, step;
+    bool dyn;
+    __device__ WorkQueue(int *c, int nitems, const Chunks &ch)
+        : ctr(c), n(nitems), lane(ch.lane), it(0), end(0), step(ch.nw), dyn(nitems >= 2 * ch.nw) {
+        if (!dyn) it = ch.gw - ch.nw;
+    }
     __device__ bool next() {
+        if (!dyn) {
+            it += step;
+            return it < n;
+        }
         if (++it < end) return true;
         int base = 0;
         if (lane == 0) base = atomicAdd(ctr, QG);
@@ -257,7 +267,7 @@ __device__ void cycle_end(const TickArgs<C> &a, const Chunks &ch, int nch, const
     const int nitems = a.ns * nch;
     {
         cd *yw = ysm[threadIdx.x >> 5];
-        for (WorkQueue q(qctr, nitems, lane); q.next();) {
+        for (WorkQueue q(qctr, nitems, ch); q.next();) {
             const int s = sorder[q.it / nch], c = q.it % nch;
             if (smode[s] != SLOT_ARNOLDI) continue;
             const Slot *sl = a.slots + s;
@@ -401,7 +411,7 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
     int ph = 0;        // phases so far: each takes the next work-queue counter
     int parity = 0;
     // ---- phase A: first reduction of every active slot
-    for (WorkQueue q(a.qctr + ph++, nitems, lane); q.next();) {
+    for (WorkQueue q(a.qctr + ph++, nitems, ch); q.next();) {
         const int s = sorder[q.it / NCH], c = q.it % NCH;
         const int md = smode[s];
         if (md != SLOT_START && md != SLOT_ARNOLDI) continue;
@@ -473,7 +483,7 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
     }
     __syncthreads();
     // cycle starts: normalise V0, set g, b_norm
-    for (WorkQueue q(a.qctr + ph++, nitems, lane); q.next();) {
+    for (WorkQueue q(a.qctr + ph++, nitems, ch); q.next();) {
         const int s = sorder[q.it / NCH], c = q.it % NCH;
         if (smode[s] != SLOT_START) continue;
         const double beta = sqrt(tot[s][0]);
@@ -512,7 +522,7 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
     }
     // ---- MGS for the Arnoldi slots: one barrier per term
     for (int k = 1; k <= kmax; ++k) {
-        for (WorkQueue q(a.qctr + ph++, nitems, lane); q.next();) {
+        for (WorkQueue q(a.qctr + ph++, nitems, ch); q.next();) {
             const int s = sorder[q.it / NCH], c = q.it % NCH;
             if (smode[s] != SLOT_ARNOLDI) continue;
             const int i = sstep[s] + 1;
@@ -568,7 +578,7 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
     // FP64 per element, one rounding to the storage precision), ||w||^2
     if (a.cgs) {
         cd *hs = ysm[threadIdx.x >> 5];
-        for (WorkQueue q(a.qctr + ph++, nitems, lane); q.next();) {
+        for (WorkQueue q(a.qctr + ph++, nitems, ch); q.next();) {
             const int s = sorder[q.it / NCH], c = q.it % NCH;
             if (smode[s] != SLOT_ARNOLDI) continue;
             const int i = sstep[s] + 1;
@@ -627,7 +637,7 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
     for (int s = 0; s < a.ns; ++s)
         if (sro[s]) jmax = max(jmax, sstep[s] + 1);
     for (int j = 1; j <= jmax; ++j) {
-        for (WorkQueue q(a.qctr + ph++, nitems, lane); q.next();) {
+        for (WorkQueue q(a.qctr + ph++, nitems, ch); q.next();) {
             const int s = sorder[q.it / NCH], c = q.it % NCH;
             if (!sro[s] || j > sstep[s] + 1) continue;
             const long long qa = c * ch.L, qb = min(n, qa + ch.L);
@@ -662,7 +672,7 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
                 Hc[j - 1] = cadd(Hc[j - 1], cmk(tot[s][0], tot[s][1]));
             }
         }
-        for (WorkQueue q(a.qctr + ph++, nitems, lane); q.next();) {
+        for (WorkQueue q(a.qctr + ph++, nitems, ch); q.next();) {
             const int s = sorder[q.it / NCH], c = q.it % NCH;
             if (!sact[s]) continue;
             const cd hr = cmk(tot[s][0], tot[s][1]);
@@ -689,7 +699,7 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
         __syncthreads();   // sact / tot are rewritten by the next round
     }
     if (jmax > 0) {
-        for (WorkQueue q(a.qctr + ph++, nitems, lane); q.next();) {
+        for (WorkQueue q(a.qctr + ph++, nitems, ch); q.next();) {
             const int s = sorder[q.it / NCH], c = q.it % NCH;
             if (!sro[s]) continue;
             const long long qa = c * ch.L, qb = min(n, qa + ch.L);
@@ -717,7 +727,7 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
         __syncthreads();
     }
     // ---- v_i = w / h(i+1,i) and the Givens update
-    for (WorkQueue q(a.qctr + ph++, nitems, lane); q.next();) {
+    for (WorkQueue q(a.qctr + ph++, nitems, ch); q.next();) {
         const int s = sorder[q.it / NCH], c = q.it % NCH;
         if (smode[s] != SLOT_ARNOLDI) continue;
         const int i = sstep[s] + 1;

@@ -23,8 +23,8 @@
 namespace {
 
 constexpr int WARPS_PER_CTA = 4;
-// anterpolation and interpolation of eight or more right-hand sides with one
-// CTA per cube / group (k_scatter_cta, k_gather_cta) instead of one warp
+// anterpolation of eight or more right-hand sides with one CTA per cube
+// (k_scatter_cta) instead of one warp
 #ifndef SCD_SG_CTA
 #define SCD_SG_CTA 1
 #endif
@@ -970,87 +970,6 @@ k_gather(const C *__restrict__ Rg, const C *__restrict__ P, int T, const int *__
     }
 }
 
-// The same interpolation and assembly for many right-hand sides, one CTA
-// per (near-zone group, span of right-hand sides): the four warps take GQ
-// right-hand sides each per round over the same group, so the group's
-// projector rows are read from L1 by all four; lane = tet, sums in the
-// order of k_gather (a column gives the same bits through either).
-template <typename C, int GQ>
-__global__ void __launch_bounds__(128)
-k_gather_cta(const C *__restrict__ Rg, const C *__restrict__ P, int T, const int *__restrict__ grp_off,
-             const int *__restrict__ grp_cube, int ngroups, GridDims G, typename CReal<C>::type k2,
-             const C *__restrict__ part, long long part_len, const long long *__restrict__ pslot_base,
-             const int *__restrict__ pslot_cnt, C *__restrict__ y, long long ld, const int *skip, int nrhs, int rspan) {
-    __shared__ C Rs[4][GQ][4][27];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int gq = blockIdx.x;
-    const int s0 = grp_off[gq], nc = grp_off[gq + 1] - s0;
-    const int c = grp_cube[gq];
-    const int bx = c % G.ncx, by = (c / G.ncx) % G.ncy, bz = c / (G.ncx * G.ncy);
-    const long long NN = (long long)G.Nx * G.Ny * G.Nz;
-    const long long pbase = pslot_base[gq];
-    const int nslot = pslot_cnt[gq];
-    long long node = 0;
-    if (lane < 27) {
-        const int a = lane % 3, b = (lane / 3) % 3, cc = lane / 9;
-        node = ((long long)(2 * bz + cc) * G.Ny + (2 * by + b)) * G.Nx + (2 * bx + a);
-    }
-    const int rlo = blockIdx.y * rspan, rhi = min(nrhs, rlo + rspan);
-    for (int r0 = rlo + warp * GQ; r0 < rhi; r0 += 4 * GQ) {
-        if (lane < 27) {
-#pragma unroll
-            for (int q = 0; q < GQ; ++q) {
-                const int r = r0 + q;
-                if (r < rhi) {
-                    const C *Rr = Rg + (long long)r * 4 * NN;
-#pragma unroll
-                    for (int g = 0; g < 4; ++g) Rs[warp][q][g][lane] = Rr[g * NN + node];
-                }
-            }
-        }
-        __syncwarp();
-        for (int sl = lane; sl < nc; sl += 32) {
-            const int s = s0 + sl;
-            C acc[GQ][6];
-#pragma unroll
-            for (int q = 0; q < GQ; ++q)
-#pragma unroll
-                for (int v = 0; v < 6; ++v) acc[q][v] = czero<C>();
-#pragma unroll 3
-            for (int j = 0; j < 27; ++j) {
-                const C p0 = P[(size_t)j * T + s], px = P[(size_t)(27 + j) * T + s];
-                const C py = P[(size_t)(54 + j) * T + s], pz = P[(size_t)(81 + j) * T + s];
-#pragma unroll
-                for (int q = 0; q < GQ; ++q) {
-                    cfma(acc[q][0], p0, Rs[warp][q][0][j]);
-                    cfma(acc[q][1], p0, Rs[warp][q][1][j]);
-                    cfma(acc[q][2], p0, Rs[warp][q][2][j]);
-                    const C r3 = Rs[warp][q][3][j];
-                    cfma(acc[q][3], px, r3);
-                    cfma(acc[q][4], py, r3);
-                    cfma(acc[q][5], pz, r3);
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < GQ; ++q) {
-                const int r = r0 + q;
-                if (r >= rhi || (skip && skip[r])) continue;
-                const C *pr = part + r * part_len + pbase + 3 * sl;
-                C *yr = y + r * ld + 3LL * s;
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    C nz = czero<C>();
-#pragma unroll 8
-                    for (int t = 0; t < nslot; ++t) nz = cadd(nz, pr[(long long)t * 3 * nc + d]);
-                    const C far = csub_scaled(acc[q][3 + d], k2, acc[q][d]);
-                    yr[d] = cadd(nz, far);
-                }
-            }
-        }
-        __syncwarp();
-    }
-}
-
 __global__ void k_twiddles(cd *tw, int P) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < P) {
@@ -1349,14 +1268,7 @@ void gather_t(scd_ctx *c, C *y, int nrhs, const int *done) {
     const R k2 = (R)(c->k * c->k);
     // spans of right-hand sides per warp (c->gather_span, 0 = all of them)
     auto span = [&](int rg) { int sp = c->gather_span > 0 ? c->gather_span : nrhs; return (sp + rg - 1) / rg * rg; };
-    if (nrhs >= 8 && SCD_SG_CTA) {
-        // one CTA per group (its four warps share the projector rows in L1)
-        const int sp = span(4);
-        constexpr int GQ = sizeof(C) == 8 ? 2 : 4;   // complex64: 96 registers, five CTAs per SM
-        k_gather_cta<C, GQ><<<dim3((unsigned)c->ngroups, (nrhs + sp - 1) / sp), 128, 0, c->st>>>(
-            Res<C>::R(c), Res<C>::P(c), c->T, c->d_grp_off, c->d_grp_cube, c->ngroups, G, k2, Res<C>::part(c),
-            c->part_len, c->d_pslot_base, c->d_pslot_cnt, y, c->n, done, nrhs, sp);
-    } else if (nrhs >= 4) {
+    if (nrhs >= 4) {
         const int sp = span(4);
         k_gather<C, 4><<<dim3(gx, (nrhs + sp - 1) / sp), 32 * WARPS_PER_CTA, 0, c->st>>>(
             Res<C>::R(c), Res<C>::P(c), c->T, c->d_grp_off, c->d_grp_cube, c->ngroups, G, k2, Res<C>::part(c),
