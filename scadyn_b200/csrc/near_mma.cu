@@ -144,15 +144,17 @@ __device__ __forceinline__ void load_rows(uint32_t taddr, NzmRows<S> &y) {
     }
 }
 
-// that row scaled by xinv, written to part[(r0 + r) * part_len + base + row]
+// that row scaled by xinv (sc, in shared memory), written to
+// part[(r0 + r) * part_len + base + row] for the right-hand sides whose bit
+// is set in `on` (present and not finished)
 template <int S>
-__device__ __forceinline__ void store_rows(const NzmArgs &a, const NzmRows<S> &y, int row_ok, int row, long long base) {
+__device__ __forceinline__ void store_rows(const NzmArgs &a, const NzmRows<S> &y, int row_ok, int row, long long base,
+                                           const float *sc, unsigned on) {
     if (!row_ok) return;
 #pragma unroll
     for (int r = 0; r < NzmSched<S>::R; ++r) {
-        if (r >= a.rg || (a.skip && a.skip[a.r0 + r])) continue;
-        const float sc = a.xinv[r];
-        a.part[(long long)(a.r0 + r) * a.part_len + base + row] = make_float2(y.re[r] * sc, y.im[r] * sc);
+        if (!((on >> r) & 1u)) continue;
+        a.part[(long long)(a.r0 + r) * a.part_len + base + row] = make_float2(y.re[r] * sc[r], y.im[r] * sc[r]);
     }
 }
 
@@ -200,6 +202,16 @@ __global__ void __launch_bounds__(NZM_THREADS, S == 2 ? 1 : 2) k_near_mma(NzmArg
         mbar_init(rowfull, 1);
         mbar_init(mmadone, 1);
         mbar_fence_init();
+    }
+    // the pass's scales and which right-hand sides to write, read once
+    __shared__ float s_sc[NzmSched<S>::R];
+    __shared__ unsigned s_on;
+    if (warp == 2) {
+        const int r = lane;
+        const bool on = r < NzmSched<S>::R && r < a.rg && !(a.skip && a.skip[a.r0 + r]);
+        if (r < NzmSched<S>::R) s_sc[r] = on ? a.xinv[r] : 0.f;
+        const unsigned m = __ballot_sync(0xffffffffu, on);
+        if (r == 0) s_on = m;
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_addr(tslot)),
@@ -301,7 +313,7 @@ __global__ void __launch_bounds__(NZM_THREADS, S == 2 ? 1 : 2) k_near_mma(NzmArg
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty[b]);
             const int row = nzm_row_of_lane(nzm_M(1, n1, tl.n2), 32 * quarter + lane);
-            store_rows<S>(a, y, row >= 0 && row < 3 * tl.n2, row, tl.col_off);
+            store_rows<S>(a, y, row >= 0 && row < 3 * tl.n2, row, tl.col_off, s_sc, s_on);
             ++tcount;
         }
         if (ok && mbar_wait(rowfull, 0u, a.err)) {
@@ -309,7 +321,7 @@ __global__ void __launch_bounds__(NZM_THREADS, S == 2 ? 1 : 2) k_near_mma(NzmArg
             NzmRows<S> y;
             load_rows<S>(tbase + ((uint32_t)(32 * quarter) << 16), y);
             const int row = nzm_row_of_lane(nzm_M(0, n1, 1), 32 * quarter + lane);
-            store_rows<S>(a, y, row >= 0 && row < 3 * n1, row, a.pslot_base[g]);
+            store_rows<S>(a, y, row >= 0 && row < 3 * n1, row, a.pslot_base[g], s_sc, s_on);
         }
     }
     tc_fence_before();
