@@ -200,33 +200,55 @@ __device__ __forceinline__ void load_totals(const TickArgs<C> &a, int parity, in
 
 // Givens update of the new H column, residual estimate and, when a cycle
 // ends, y = H^-1 g (back substitution) for every Arnoldi slot: CTA 0, one
-// thread per slot.  H column i-1 is complete except H(i, i-1) = shn[s];
-// sreo[s] flags a re-orthogonalised step (counted).
+// warp per slot.  H column i-1 is complete except H(i, i-1) = shn[s];
+// sreo[s] flags a re-orthogonalised step (counted).  The warp stages the
+// column in shared memory (hw) so that lane 0 applies the rotations in their
+// order without a global-memory round trip per step; the back substitution
+// runs column by column over the warp, lane r holding rows r and r + 32.
 template <typename C>
-__device__ void givens_step(const TickArgs<C> &a, const int *smode, const int *sstep, const double *shn, const int *sreo) {
+__device__ void givens_step(const TickArgs<C> &a, const int *smode, const int *sstep, const double *shn, const int *sreo,
+                            cd (*hws)[SCD_M_MAX + 1]) {
     const int ldh = a.m + 1;
-    {
-        for (int s = threadIdx.x; s < a.ns; s += blockDim.x) {
-            if (smode[s] != SLOT_ARNOLDI) continue;
-            Slot &sl = a.slots[s];
-            const int i = sstep[s] + 1;
-            cd *Hc = a.H + (size_t)s * ldh * a.m + (size_t)ldh * (i - 1);
-            cd *cs = a.cs + (size_t)s * (a.m + 1), *sn = a.sn + (size_t)s * (a.m + 1), *g = a.g + (size_t)s * (a.m + 1);
-            Hc[i] = cmk(shn[s], 0.0);
-            for (int k = 1; k <= i - 1; ++k) {
-                const cd c = cs[k - 1], sv = sn[k - 1];
-                const cd tmp = csub(cmul(c, Hc[k - 1]), cmul(sv, Hc[k]));
-                Hc[k] = cadd(cmul(sv, Hc[k - 1]), cmul(cconj(c), Hc[k]));
-                Hc[k - 1] = tmp;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    cd *hw = hws[warp];
+    for (int s = warp; s < a.ns; s += BW) {
+        if (smode[s] != SLOT_ARNOLDI) continue;   // uniform across the warp
+        Slot &sl = a.slots[s];
+        const int i = sstep[s] + 1;
+        cd *Hc = a.H + (size_t)s * ldh * a.m + (size_t)ldh * (i - 1);
+        cd *cs = a.cs + (size_t)s * (a.m + 1), *sn = a.sn + (size_t)s * (a.m + 1), *g = a.g + (size_t)s * (a.m + 1);
+        __syncwarp();
+        for (int k = lane; k < i; k += 32) hw[k] = Hc[k];
+        if (lane == 0) hw[i] = cmk(shn[s], 0.0);
+        // the rotations so far, two per lane (k = lane, lane + 32)
+        cd c0 = cmk(0, 0), s0 = cmk(0, 0), c1 = cmk(0, 0), s1 = cmk(0, 0);
+        if (lane < i - 1) { c0 = cs[lane]; s0 = sn[lane]; }
+        if (lane + 32 < i - 1) { c1 = cs[lane + 32]; s1 = sn[lane + 32]; }
+        __syncwarp();
+        int fin = 0;
+        for (int k = 1; k <= i - 1; ++k) {
+            const int src = (k - 1) & 31;
+            const bool hi = k - 1 >= 32;
+            cd c, sv;
+            c.x = __shfl_sync(0xffffffffu, hi ? c1.x : c0.x, src);
+            c.y = __shfl_sync(0xffffffffu, hi ? c1.y : c0.y, src);
+            sv.x = __shfl_sync(0xffffffffu, hi ? s1.x : s0.x, src);
+            sv.y = __shfl_sync(0xffffffffu, hi ? s1.y : s0.y, src);
+            if (lane == 0) {
+                const cd tmp = csub(cmul(c, hw[k - 1]), cmul(sv, hw[k]));
+                hw[k] = cadd(cmul(sv, hw[k - 1]), cmul(cconj(c), hw[k]));
+                hw[k - 1] = tmp;
             }
-            const double nu = sqrt(cabs2(Hc[i - 1]) + cabs2(Hc[i]));
+        }
+        if (lane == 0) {
+            const double nu = sqrt(cabs2(hw[i - 1]) + cabs2(hw[i]));
             if (nu != 0.0) {
-                const cd c = cconj(cmk(Hc[i - 1].x / nu, Hc[i - 1].y / nu));
-                const cd sv = cmk(-Hc[i].x / nu, -Hc[i].y / nu);
+                const cd c = cconj(cmk(hw[i - 1].x / nu, hw[i - 1].y / nu));
+                const cd sv = cmk(-hw[i].x / nu, -hw[i].y / nu);
                 cs[i - 1] = c;
                 sn[i - 1] = sv;
-                Hc[i - 1] = csub(cmul(c, Hc[i - 1]), cmul(sv, Hc[i]));
-                Hc[i] = cmk(0, 0);
+                hw[i - 1] = csub(cmul(c, hw[i - 1]), cmul(sv, hw[i]));
+                hw[i] = cmk(0, 0);
                 const cd t1 = g[i - 1], t2 = g[i];
                 g[i - 1] = csub(cmul(c, t1), cmul(sv, t2));
                 g[i] = cadd(cmul(sv, t1), cmul(cconj(c), t2));
@@ -241,15 +263,32 @@ __device__ void givens_step(const TickArgs<C> &a, const int *smode, const int *s
             else if (i == a.m) sl.finish = 1;
             if (!(error == error)) { sl.status = SCD_NAN; sl.finish = 0; sl.mode = SLOT_DONE; }
             if (*a.err) { sl.status = SCD_TIMEOUT; sl.finish = 0; sl.mode = SLOT_DONE; }
-            if (sl.finish) {
-                // y = H(1:i,1:i)^-1 g(1:i), back substitution
-                cd *ys = a.y + (size_t)s * (a.m + 1);
-                const cd *Hs = a.H + (size_t)s * ldh * a.m;
-                for (int r = i - 1; r >= 0; --r) {
-                    cd acc = g[r];
-                    for (int cc = r + 1; cc < i; ++cc) acc = csub(acc, cmul(Hs[r + (size_t)ldh * cc], ys[cc]));
-                    ys[r] = cdiv(acc, Hs[r + (size_t)ldh * r]);
-                }
+            fin = sl.finish;
+        }
+        __syncwarp();
+        for (int k = lane; k <= i; k += 32) Hc[k] = hw[k];
+        fin = __shfl_sync(0xffffffffu, fin, 0);
+        if (fin) {
+            // y = H(1:i,1:i)^-1 g(1:i): column cc gives y_cc on the lane of row
+            // cc, then every row above subtracts H(r, cc) y_cc
+            __syncwarp();   // g and column i-1 of H as written by lane 0
+            const cd *Hs = a.H + (size_t)s * ldh * a.m;
+            cd *ys = a.y + (size_t)s * (a.m + 1);
+            const cd *gv = g;
+            cd b0 = lane < i ? gv[lane] : cmk(0, 0), b1 = lane + 32 < i ? gv[lane + 32] : cmk(0, 0);
+            for (int cc = i - 1; cc >= 0; --cc) {
+                const cd *col = Hs + (size_t)ldh * cc;
+                const cd h0 = lane <= cc ? col[lane] : cmk(0, 0);
+                const cd h1 = lane + 32 <= cc ? col[lane + 32] : cmk(0, 0);
+                const int own = cc & 31;
+                const bool hi = cc >= 32;
+                cd yc = cmk(0, 0);
+                if (lane == own) yc = cdiv(hi ? b1 : b0, hi ? h1 : h0);
+                yc.x = __shfl_sync(0xffffffffu, yc.x, own);
+                yc.y = __shfl_sync(0xffffffffu, yc.y, own);
+                if (lane == own) ys[cc] = yc;
+                if (lane < cc) b0 = csub(b0, cmul(h0, yc));
+                if (lane + 32 < cc) b1 = csub(b1, cmul(h1, yc));
             }
         }
     }
@@ -752,7 +791,7 @@ __global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
     if (blockIdx.x == 0) {
         if (threadIdx.x < a.ns) sact[threadIdx.x] = snormav[threadIdx.x] + (double)0.001f * shn[threadIdx.x] == snormav[threadIdx.x];
         __syncthreads();
-        givens_step(a, smode, sstep, shn, sact);
+        givens_step(a, smode, sstep, shn, sact, ysm);
     }
     grid_barrier(a.bar, gridDim.x, a.err);
     cycle_end(a, ch, NCH, smode, ysm, sorder, a.qctr + ph);
