@@ -951,20 +951,40 @@ k_gather(const C *__restrict__ Rg, const C *__restrict__ P, int T, const int *__
                     cfma(acc[q][5], pz, r3);
                 }
             }
+            // far field first (acc dies), then the partial slots of all
+            // right-hand sides of the round in one sweep over the slots, so
+            // that 3 GA_RG independent loads are in flight per slot; each sum
+            // still runs over the slots in order
+            C far[GA_RG][3], nz[GA_RG][3];
+            bool on[GA_RG];
 #pragma unroll
             for (int q = 0; q < GA_RG; ++q) {
                 const int r = r0 + q;
-                if (r >= nrhs || (skip && skip[r])) continue;
-                const C *pr = part + r * part_len + pbase + 3 * sl;
-                C *yr = y + r * ld + 3LL * s;
+                on[q] = r < nrhs && !(skip && skip[r]);
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
-                    C nz = czero<C>();
-#pragma unroll 8
-                    for (int t = 0; t < nslot; ++t) nz = cadd(nz, pr[(long long)t * 3 * nc + d]);
-                    const C far = csub_scaled(acc[q][3 + d], k2, acc[q][d]);
-                    yr[d] = cadd(nz, far);
+                    far[q][d] = csub_scaled(acc[q][3 + d], k2, acc[q][d]);
+                    nz[q][d] = czero<C>();
                 }
+            }
+            const C *pr0 = part + pbase + 3 * sl;
+#pragma unroll 2
+            for (int t = 0; t < nslot; ++t) {
+                const C *pt = pr0 + (long long)t * 3 * nc;
+#pragma unroll
+                for (int q = 0; q < GA_RG; ++q) {
+                    if (!on[q]) continue;
+                    const C *pq = pt + (r0 + q) * part_len;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) nz[q][d] = cadd(nz[q][d], pq[d]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < GA_RG; ++q) {
+                if (!on[q]) continue;
+                C *yr = y + (r0 + q) * ld + 3LL * s;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) yr[d] = cadd(nz[q][d], far[q][d]);
             }
         }
     }
