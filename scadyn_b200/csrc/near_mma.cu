@@ -24,7 +24,10 @@ namespace {
 constexpr int NZM_SLOTS = 8;
 constexpr int NZM_THREADS = 192;          // warp 0 producer, warp 1 MMA issuer, warps 2-5 epilogue
 constexpr uint32_t NZM_META = 256;
-constexpr size_t NZM_SMEM = 113 * 1024;   // two CTAs per SM (schedules 0, 1)
+// two CTAs per SM (schedules 0, 1): 2 x (dynamic + static + 1 KB reserved per
+// CTA) must stay within the SM's 228 KB; 113 KB dynamic plus the kernel's
+// static bytes no longer did, and halved the resident CTAs
+constexpr size_t NZM_SMEM = 112 * 1024;
 constexpr size_t NZM_SMEM_WIDE = 224 * 1024;   // one CTA per SM (schedule 2: 384 TMEM columns)
 
 struct NzmArgs {
@@ -458,7 +461,25 @@ int near_mma_prepare(scd_ctx *c) {
             const NearTile &tl = c->tiles_h[t];
             max_slot = std::max(max_slot, nzm_tile_bytes(tl.n1, tl.n2) + xbytes(tl.n2));
         }
-        const size_t budget = w ? NZM_SMEM_WIDE : NZM_SMEM;
+        size_t budget = w ? NZM_SMEM_WIDE : NZM_SMEM;
+        {
+            // what the SM holds for this many CTAs: per CTA its static bytes
+            // and the reserved kilobyte come out of the SM's shared memory
+            int per_sm = 0, reserved = 0, optin = 0;
+            cudaFuncAttributes fa{};
+            const cudaError_t e1 = cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, c->dev);
+            const cudaError_t e2 = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, c->dev);
+            const cudaError_t e3 = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dev);
+            const cudaError_t e4 = w ? cudaFuncGetAttributes(&fa, k_near_mma<2>) : cudaFuncGetAttributes(&fa, k_near_mma<1>);
+            if (e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess && e4 == cudaSuccess) {
+                const int ctas = w ? 1 : 2;
+                const long long fit = (long long)per_sm / ctas - reserved - (long long)fa.sharedSizeBytes;
+                budget = (size_t)std::max<long long>(0, std::min<long long>(fit, optin - (long long)fa.sharedSizeBytes));
+                budget = budget / 1024 * 1024;
+            } else {
+                cudaGetLastError();
+            }
+        }
         const size_t fixed = 128 + NZM_META + x1 + c->nzm_slack;
         size_t ring = budget > fixed ? (budget - fixed) / 128 * 128 : 0;
         if (ring < max_slot) ring = (size_t)max_slot;   // one slot at least (then one CTA per SM)
