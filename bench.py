@@ -579,20 +579,33 @@ def main():
     Bref = solver.nearzone_count()
     alg_bytes = Bref * (9 * 8 + 8)                 # complex64 blocks + index pair, per pass over the tiles
     # roofline of the headline's dominant kernel: the complex64 near-zone
-    # kernel at 16 right-hand sides per pass (one launch of the batched inner
-    # matvec), live CUDA events on the library's stream
-    prof16 = solver.profile_matvec(20, 16, api.PREC_MIXED)
-    near_ms = prof16["near_kernel_ms"]
+    # kernel the timed steps used, at the right-hand sides of one of its
+    # launches (one pass of the batched inner matvec), live CUDA events on the
+    # library's stream
+    nk = tuning["matvec"]["near_kernel"] if tuning else choices["near_kernel"]
+    nk = nk or NEAR_KERNELS["merged"]
+    per_launch = 32 if nk == NEAR_KERNELS["wide"] else 16
+    kname = {NEAR_KERNELS["wide"]: "k_near_mma<2> (tensor-core near zone, wide schedule)",
+             NEAR_KERNELS["merged"]: "k_near_mma<1> (tensor-core near zone, merged schedule)",
+             NEAR_KERNELS["split"]: "k_near_mma<0> (tensor-core near zone, split schedule)",
+             NEAR_KERNELS["cuda"]: "k_near_groups (near-zone block SpMV on the CUDA cores)"}[nk]
+    profl = solver.profile_matvec(20, per_launch, api.PREC_MIXED)
+    near_ms = profl["near_kernel_ms"]
     achieved = alg_bytes / (near_ms / 1e3) / 1e9
-    traffic = profile_traffic(f"near_mma_{args.config}.txt")
+    traffic = profile_traffic(f"near_mma_{args.config}.txt") if nk == NEAR_KERNELS["merged"] else None
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": kind,
-            "kernel": ("k_near_mma (tensor-core near-zone tile products, 16 complex64 right-hand sides per launch)"
-                       if (tuning["matvec"]["near_kernel"] if tuning else choices["near_kernel"]) != NEAR_KERNELS["cuda"]
-                       else
-                       "k_near_groups (near-zone block SpMV, 16 complex64 right-hand sides per launch)"),
+            "kernel": f"{kname}, {per_launch} complex64 right-hand sides per launch",
             "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": near_ms,
-            "flops_per_launch": Bref * 144 * 16 * 2}
+            "flops_per_launch": Bref * 144 * per_launch * 2}
+    if nk == NEAR_KERNELS["wide"]:
+        # the 16-wide merged pass that takes the last 16 or fewer right-hand sides
+        prof16 = solver.profile_matvec(20, 16, api.PREC_MIXED)
+        roof["merged_16"] = {"kernel": "k_near_mma<1> (16 complex64 right-hand sides)",
+                             "avg_launch_ms": prof16["near_kernel_ms"],
+                             "achieved": round(alg_bytes / (prof16["near_kernel_ms"] / 1e3) / 1e9, 1),
+                             "frac": round(alg_bytes / (prof16["near_kernel_ms"] / 1e3) / 1e9 / peak, 4),
+                             "traffic": profile_traffic(f"near_mma_{args.config}.txt")}
     # secondary: the FP64 one-right-hand-side near zone of the plain form
     prof1 = solver.profile_matvec(20, 1)
     roof["fp64_one_rhs"] = {"kernel": "k_near_groups (FP64, one right-hand side)", "avg_launch_ms": prof1["near_kernel_ms"],

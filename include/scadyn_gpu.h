@@ -91,12 +91,13 @@ typedef struct scd_grid_desc {
 
 /* scd_grid_desc.near_kernel: the near-zone SpMV of the complex64 matvec of the
  * mixed-precision inner solves (the FP64 matvec always runs on the CUDA cores) */
-#define SCD_NEAR_DEFAULT        0   /* SCD_NEAR_TENSOR_MERGED when the blocks are stored complex64, else CUDA cores */
+#define SCD_NEAR_DEFAULT        0   /* SCD_NEAR_TENSOR_WIDE when the blocks are stored complex64, else CUDA cores */
 #define SCD_NEAR_CUDA_CORES     1   /* complex64 FMAs on the CUDA cores */
 #define SCD_NEAR_TENSOR_SPLIT   2   /* tcgen05 MMAs on f16 hi/lo tile planes, 9 MMAs per K step */
 #define SCD_NEAR_TENSOR_MERGED  3   /* the same with x hi/lo merged into one operand, 6 MMAs per K step */
-#define SCD_NEAR_TENSOR_WIDE    4   /* the merged schedule over 32 right-hand sides per pass: each tile is
-                                       read once per 32 instead of 16 (one CTA per SM) */
+#define SCD_NEAR_TENSOR_WIDE    4   /* the merged schedule over 32 right-hand sides per pass while more than
+                                       16 remain (each tile read once per 32, one CTA per SM), 16-wide for
+                                       the rest; the same bits as SCD_NEAR_TENSOR_MERGED */
 
 /* near-zone storage precision */
 #define SCD_STORE_C64   32   /* complex64, as the reference stores sp_mat */

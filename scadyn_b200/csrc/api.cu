@@ -60,7 +60,7 @@ static int fft_len(int v, bool smooth) {
 // instruction schedule of the tensor-core near zone (near_mma.cuh) for a
 // scd_grid_desc.near_kernel / scd_tuning.near_kernel value
 static int nzm_sched_of(int near_kernel) {
-    return near_kernel == SCD_NEAR_TENSOR_SPLIT ? 0 : near_kernel == SCD_NEAR_TENSOR_WIDE ? 2 : 1;
+    return near_kernel == SCD_NEAR_TENSOR_SPLIT ? 0 : near_kernel == SCD_NEAR_TENSOR_MERGED ? 1 : 2;
 }
 
 template <typename Tp>

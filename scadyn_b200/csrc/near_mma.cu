@@ -514,15 +514,25 @@ static void near_mma_pass(scd_ctx *c, const cf *x, int r0, int rg, const int *do
 }
 
 // near-zone partial slots of nrhs complex64 right-hand sides (columns of
-// stride n): passes of 16 (schedules 0, 1) or 32 (schedule 2).  A context
-// keeps one schedule for every pass, so a column meets the same instruction
-// shapes alone and in any batch.
+// stride n): passes of 16 (schedules 0, 1); with schedule 2, passes of 32
+// while more than 16 remain and a last pass of schedule 1 (a 32-wide pass
+// costs twice the tensor work of a 16-wide one).  Schedules 1 and 2 form
+// every output element from the same K = 16 products in the same order (hi
+// part, then lo part, added pairwise) and differ only in how many columns
+// one instruction covers, so a column gets the same bits from either;
+// tests/test_gpu_near_mma.py checks that on the device.
 void near_mma_run(scd_ctx *c, const cf *x, int nrhs, const int *done) {
-    const int R = c->nzm_sched == 2 ? NZM_RMAX : NZM_R;
-    for (int r0 = 0; r0 < nrhs; r0 += R) {
-        const int rg = std::min(R, nrhs - r0);
-        if (c->nzm_sched == 2) near_mma_pass<2>(c, x, r0, rg, done);
-        else if (c->nzm_sched == 0) near_mma_pass<0>(c, x, r0, rg, done);
-        else near_mma_pass<1>(c, x, r0, rg, done);
+    for (int r0 = 0; r0 < nrhs;) {
+        const int left = nrhs - r0;
+        if (c->nzm_sched == 2 && left > NZM_R) {
+            const int rg = std::min(NZM_RMAX, left);
+            near_mma_pass<2>(c, x, r0, rg, done);
+            r0 += rg;
+        } else {
+            const int rg = std::min(NZM_R, left);
+            if (c->nzm_sched == 0) near_mma_pass<0>(c, x, r0, rg, done);
+            else near_mma_pass<1>(c, x, r0, rg, done);
+            r0 += rg;
+        }
     }
 }

@@ -91,3 +91,24 @@ def test_complex128_storage_keeps_cuda_cores(small_sphere):
         assert e.value.code == api.SCD_BAD_ARG
     finally:
         s.close()
+
+
+def test_wide_and_merged_schedules_give_the_same_bits(small_sphere):
+    """The wide schedule (32 right-hand sides per tensor-core pass, 16 for the
+    rest) and the merged one (16 per pass) form every output element from the
+    same products in the same order, so a column solved with either has the
+    same bits: 40 columns at once take a 32-wide and a 16-wide pass, and the
+    batch shrinks through both as columns finish."""
+    k = 1.0 / small_sphere.a
+    op = O.setup(small_sphere, k, grid_size=1.8, nthreads=0)
+    mat = O.vswf2constant(small_sphere.coord, small_sphere.etopol, k, 4)[:40]
+    kw = dict(tol=1e-8, block=40, precision=api.PREC_MIXED, inner_tol=1e-3, want_x=True)
+    out = []
+    for kernel in (api.NEAR_TENSOR_MERGED, api.NEAR_TENSOR_WIDE):
+        s = solver_from_oracle(op, near_kernel=kernel)
+        try:
+            out.append(s.solve_columns(mat, **kw))
+        finally:
+            s.close()
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][2], out[1][2])
