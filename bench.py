@@ -592,7 +592,8 @@ def main():
     profl = solver.profile_matvec(20, per_launch, api.PREC_MIXED)
     near_ms = profl["near_kernel_ms"]
     achieved = alg_bytes / (near_ms / 1e3) / 1e9
-    traffic = profile_traffic(f"near_mma_{args.config}.txt") if nk == NEAR_KERNELS["merged"] else None
+    traffic = {NEAR_KERNELS["merged"]: profile_traffic(f"near_mma_{args.config}.txt"),
+               NEAR_KERNELS["wide"]: profile_traffic(f"near_mma_wide_{args.config}.txt")}.get(nk)
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": kind,
             "kernel": f"{kname}, {per_launch} complex64 right-hand sides per launch",
