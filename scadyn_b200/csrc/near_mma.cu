@@ -28,7 +28,7 @@ constexpr uint32_t NZM_META = 256;
 // CTA) must stay within the SM's 228 KB; 113 KB dynamic plus the kernel's
 // static bytes no longer did, and halved the resident CTAs
 constexpr size_t NZM_SMEM = 112 * 1024;
-constexpr size_t NZM_SMEM_WIDE = 224 * 1024;   // one CTA per SM (schedule 2: 384 TMEM columns)
+constexpr size_t NZM_SMEM_WIDE = NzmSched<2>::CTAS == 2 ? NZM_SMEM : 224 * 1024;   // schedule 2
 
 struct NzmArgs {
     const NearTile *tiles;
@@ -61,6 +61,17 @@ __device__ __forceinline__ void tc_mma(uint32_t d, uint64_t da, uint64_t db, uin
 __device__ __forceinline__ void tc_commit(uint64_t *bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(smem_addr(bar))
                  : "memory");
+}
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 __device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
     uint32_t r[32];
@@ -161,9 +172,48 @@ __device__ __forceinline__ void store_rows(const NzmArgs &a, const NzmRows<S> &y
     }
 }
 
+// a product's accumulator rows into the partial slots; `release` runs once
+// every read of the accumulator is done, so that the buffer can take the
+// next product.  Schedule 2 reads its 32 right-hand sides in two halves of
+// 16 and stores each half at once, which keeps its registers within two CTAs
+// per SM; the sums and stores are those of load_rows / store_rows.
+template <int S, typename Rel>
+__device__ __forceinline__ void drain_rows(const NzmArgs &a, uint32_t taddr, int row_ok, int row, long long base,
+                                           const float *sc, unsigned on, Rel release) {
+    if constexpr (S == 2) {
+        constexpr int R = NzmSched<S>::R;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            float p[16], q[16], re[16], im[16];
+            tc_ld16(taddr + 16 * h, p);
+            tc_ld16(taddr + R + 16 * h, q);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) re[i] = p[i] + q[i];
+            tc_ld16(taddr + 2 * R + 16 * h, p);
+            tc_ld16(taddr + 3 * R + 16 * h, q);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) im[i] = p[i] + q[i];
+            if (h == 1) release();
+            if (row_ok) {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const int r = 16 * h + i;
+                    if (!((on >> r) & 1u)) continue;
+                    a.part[(long long)(a.r0 + r) * a.part_len + base + row] = make_float2(re[i] * sc[r], im[i] * sc[r]);
+                }
+            }
+        }
+    } else {
+        NzmRows<S> y;
+        load_rows<S>(taddr, y);
+        release();
+        store_rows<S>(a, y, row_ok, row, base, sc, on);
+    }
+}
+
 // one CTA per near-zone group, one pass of up to NzmSched<S>::R right-hand sides
 template <int S>
-__global__ void __launch_bounds__(NZM_THREADS, S == 2 ? 1 : 2) k_near_mma(NzmArgs a) {
+__global__ void __launch_bounds__(NZM_THREADS, NzmSched<S>::CTAS) k_near_mma(NzmArgs a) {
     constexpr uint32_t NZM_TMEM_COLS = NzmSched<S>::TMEM;   // row product + two transposed buffers
     constexpr uint32_t DC = NzmSched<S>::DCOLS;
     extern __shared__ unsigned char nzm_raw[];
@@ -284,8 +334,9 @@ __global__ void __launch_bounds__(NZM_THREADS, S == 2 ? 1 : 2) k_near_mma(NzmArg
                 const uint32_t xblk = tile + nzm_tile_bytes(n1, tl.n2);
                 issue_product<S>(0, n1, tl.n2, tile, xblk, tbase, t == t0);
                 if (tl.col_off >= 0) {
-                    const int b = tcount & 1;
-                    if (!(ok = mbar_wait(&tempty[b], (uint32_t)(((tcount >> 1) & 1) ^ 1), a.err))) break;
+                    constexpr int NB = NzmSched<S>::NBUF;
+                    const int b = tcount % NB;
+                    if (!(ok = mbar_wait(&tempty[b], (uint32_t)(((tcount / NB) & 1) ^ 1), a.err))) break;
                     tc_fence_after();
                     issue_product<S>(1, n1, tl.n2, tile, smem_addr(X1), tbase + DC * (1 + b), true);
                     tc_commit(&tfull[b]);
@@ -307,24 +358,24 @@ __global__ void __launch_bounds__(NZM_THREADS, S == 2 ? 1 : 2) k_near_mma(NzmArg
         for (int t = t0; t < t1 && ok; ++t) {
             const NearTile &tl = a.tiles[t];
             if (tl.col_off < 0) continue;
-            const int b = tcount & 1;
-            if (!(ok = mbar_wait(&tfull[b], (uint32_t)((tcount >> 1) & 1), a.err))) break;
+            constexpr int NB = NzmSched<S>::NBUF;
+            const int b = tcount % NB;
+            if (!(ok = mbar_wait(&tfull[b], (uint32_t)((tcount / NB) & 1), a.err))) break;
             tc_fence_after();
-            NzmRows<S> y;
-            load_rows<S>(tbase + ((uint32_t)(32 * quarter) << 16) + DC * (1 + b), y);
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&tempty[b]);
             const int row = nzm_row_of_lane(nzm_M(1, n1, tl.n2), 32 * quarter + lane);
-            store_rows<S>(a, y, row >= 0 && row < 3 * tl.n2, row, tl.col_off, s_sc, s_on);
+            drain_rows<S>(a, tbase + ((uint32_t)(32 * quarter) << 16) + DC * (1 + b), row >= 0 && row < 3 * tl.n2, row,
+                          tl.col_off, s_sc, s_on, [&]() {
+                              tc_fence_before();
+                              __syncwarp();
+                              if (lane == 0) mbar_arrive(&tempty[b]);
+                          });
             ++tcount;
         }
         if (ok && mbar_wait(rowfull, 0u, a.err)) {
             tc_fence_after();
-            NzmRows<S> y;
-            load_rows<S>(tbase + ((uint32_t)(32 * quarter) << 16), y);
             const int row = nzm_row_of_lane(nzm_M(0, n1, 1), 32 * quarter + lane);
-            store_rows<S>(a, y, row >= 0 && row < 3 * n1, row, a.pslot_base[g], s_sc, s_on);
+            drain_rows<S>(a, tbase + ((uint32_t)(32 * quarter) << 16), row >= 0 && row < 3 * n1, row, a.pslot_base[g],
+                          s_sc, s_on, []() {});
         }
     }
     tc_fence_before();
@@ -472,7 +523,7 @@ int near_mma_prepare(scd_ctx *c) {
             const cudaError_t e3 = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dev);
             const cudaError_t e4 = w ? cudaFuncGetAttributes(&fa, k_near_mma<2>) : cudaFuncGetAttributes(&fa, k_near_mma<1>);
             if (e1 == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess && e4 == cudaSuccess) {
-                const int ctas = w ? 1 : 2;
+                const int ctas = w ? NzmSched<2>::CTAS : NzmSched<1>::CTAS;
                 const long long fit = (long long)per_sm / ctas - reserved - (long long)fa.sharedSizeBytes;
                 budget = (size_t)std::max<long long>(0, std::min<long long>(fit, optin - (long long)fa.sharedSizeBytes));
                 budget = budget / 1024 * 1024;

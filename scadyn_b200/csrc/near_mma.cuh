@@ -45,12 +45,25 @@ constexpr int NZM_OPS = 3;             // per A part: Re A X, -Im A Im x, Im A R
 //    summed pairwise by the epilogue.  Descriptors advance by constant steps.
 //  2 ("wide"): schedule 1 with R = 32 right-hand sides per pass: every tile
 //    crosses HBM once per 32 right-hand sides instead of 16, with N = 128
-//    instructions; its three accumulators take 384 of the SM's 512 TMEM
-//    columns, so it runs one CTA per SM.
+//    instructions.  With one buffer for the transposed products (NBUF 1) the
+//    row and transposed accumulators take 256 TMEM columns and two CTAs share
+//    an SM, one overlapping the other's epilogue; with two (NBUF 2) they take
+//    384 of the SM's 512 and one CTA runs per SM.
+// NBUF: accumulator buffers of the transposed products; CTAS: CTAs per SM.
+#ifndef NZM_WIDE_NB
+#define NZM_WIDE_NB 1
+#endif
 template <int S> struct NzmSched;
-template <> struct NzmSched<0> { static constexpr int R = NZM_R, PARTS = NZM_SPLITS, DCOLS = 2 * R, TMEM = 128; };
-template <> struct NzmSched<1> { static constexpr int R = NZM_R, PARTS = 2, DCOLS = 4 * R, TMEM = 256; };
-template <> struct NzmSched<2> { static constexpr int R = NZM_RMAX, PARTS = 2, DCOLS = 4 * R, TMEM = 512; };
+template <> struct NzmSched<0> {
+    static constexpr int R = NZM_R, PARTS = NZM_SPLITS, DCOLS = 2 * R, NBUF = 2, TMEM = 128, CTAS = 2;
+};
+template <> struct NzmSched<1> {
+    static constexpr int R = NZM_R, PARTS = 2, DCOLS = 4 * R, NBUF = 2, TMEM = 256, CTAS = 2;
+};
+template <> struct NzmSched<2> {
+    static constexpr int R = NZM_RMAX, PARTS = 2, DCOLS = 4 * R, NBUF = NZM_WIDE_NB,
+                         TMEM = NZM_WIDE_NB == 1 ? 256 : 512, CTAS = NZM_WIDE_NB == 1 ? 2 : 1;
+};
 
 SCD_HD int nzm_ceil8(int v) { return (v + 7) & ~7; }
 SCD_HD int nzm_ceil16(int v) { return (v + 15) & ~15; }
