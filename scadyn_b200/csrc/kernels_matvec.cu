@@ -28,6 +28,11 @@ constexpr int WARPS_PER_CTA = 4;
 #ifndef SCD_SG_CTA
 #define SCD_SG_CTA 1
 #endif
+// resident CTAs per SM the complex64 interpolation kernel is compiled for
+// (its register cap)
+#ifndef SCD_GATHER_MINB
+#define SCD_GATHER_MINB 1
+#endif
 
 // slot order <-> the reference's unknown order (nb basis functions per tet:
 // 1, or 4 for the linear basis, see linear_basis.h)
@@ -892,7 +897,7 @@ __global__ void __launch_bounds__(NZ_MAX_THREADS, NZ_MIN_CTAS<U>) k_near_groups(
 // slots in slot order and writes Ax = near + (Y2 - k^2 Y).  The spans are the
 // grid's y index; rspan is a multiple of GA_RG.
 template <typename C, int GA_RG>
-__global__ void __launch_bounds__(32 * WARPS_PER_CTA)
+__global__ void __launch_bounds__(32 * WARPS_PER_CTA, sizeof(C) == 8 ? SCD_GATHER_MINB : 1)
 k_gather(const C *__restrict__ Rg, const C *__restrict__ P, int T, const int *__restrict__ grp_off,
          const int *__restrict__ grp_cube, int ngroups, GridDims G, typename CReal<C>::type k2,
          const C *__restrict__ part, long long part_len, const long long *__restrict__ pslot_base,
