@@ -29,9 +29,10 @@ constexpr int WARPS_PER_CTA = 4;
 #define SCD_SG_CTA 1
 #endif
 // resident CTAs per SM the complex64 interpolation kernel is compiled for
-// (its register cap)
+// (its register cap): at C2 with 32 right-hand sides 0.75 ms with 3 (160
+// registers), 0.90 with 1 (174), 1.07 with 4 or 5 (spills)
 #ifndef SCD_GATHER_MINB
-#define SCD_GATHER_MINB 1
+#define SCD_GATHER_MINB 3
 #endif
 
 // slot order <-> the reference's unknown order (nb basis functions per tet:
