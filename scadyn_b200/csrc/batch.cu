@@ -24,6 +24,11 @@ namespace {
 constexpr int BT = 256;             // threads per CTA of the tick kernel
 constexpr int NSMAX = 64;           // slot limit (partial buffer sizing)
 constexpr int BW = BT / 32;         // warps per CTA
+// resident CTAs per SM the complex64 tick is compiled for (its register cap;
+// the cooperative grid follows the occupancy this gives)
+#ifndef SCD_TICK_MINB
+#define SCD_TICK_MINB 2
+#endif
 
 enum { SLOT_FREE = 0, SLOT_START = 1, SLOT_ARNOLDI = 2, SLOT_DONE = 3, SLOT_RESID = 4, SLOT_INNER_DONE = 5 };
 
@@ -416,7 +421,7 @@ __device__ __forceinline__ void cgs_dots(const TickArgs<C> &a, int s, int c, int
 // One tick: cycle starts (r = rhs - A x, V0 = r/||r||) and Arnoldi steps
 // (MGS, normalisation, Givens) for every active slot; cycle ends update x.
 template <typename C>
-__global__ void __launch_bounds__(BT, 2) k_tick(TickArgs<C> a) {
+__global__ void __launch_bounds__(BT, sizeof(C) == 8 ? SCD_TICK_MINB : 2) k_tick(TickArgs<C> a) {
     __shared__ double tot[NSMAX][4];
     __shared__ int smode[NSMAX], sstep[NSMAX], szero[NSMAX], swpos[NSMAX], sact[NSMAX], sro[NSMAX];
     __shared__ double snormav[NSMAX], shn[NSMAX];
@@ -944,7 +949,8 @@ struct BatchBuffers {
     double *cpart = nullptr, *ctot = nullptr;
     double *cpm = nullptr, *ctm = nullptr;   // classical Gram-Schmidt reductions (opt-in)
     int *ccnt = nullptr;
-    int grid = 0;
+    int grid = 0;                        // CTAs of the cooperative FP64 tick and residual kernels
+    int grid_f = 0;                      // CTAs of the complex64 tick
 };
 
 static void free_bb(BatchBuffers &b) {
@@ -1008,6 +1014,11 @@ int batch_prepare(scd_ctx *c, int ns, int m, int mixed, BatchBuffers &b) {
     if (per_sm < 1) return set_error(c, SCD_CUDA_ERROR, "tick kernel cannot be resident");
     per_sm = std::min(per_sm, 2);
     b.grid = per_sm * c->nsm;
+    {
+        int per_f = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_f, k_tick<cf>, BT, 0);
+        b.grid_f = std::max(1, std::min(per_f, SCD_TICK_MINB)) * c->nsm;
+    }
     if ((rc = al((void **)&b.red, sizeof(double) * 2 * (size_t)b.grid * NSMAX * 4, "partials"))) return rc;
     b.ns = ns;
     b.m = m;
@@ -1065,7 +1076,8 @@ static int launch_tick(scd_ctx *c, BatchBuffers &bb, int ns, int nact, int m, in
     NvtxRange r("arnoldi tick");
     void *args[] = {&a};
     cudaMemsetAsync(bb.ccnt, 0, sizeof(int) * (NSMAX + QMAX), c->st);
-    cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_tick<C>, dim3(bb.grid), dim3(BT), args, 0, c->st);
+    const int grid = std::is_same<C, cf>::value ? bb.grid_f : bb.grid;
+    cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_tick<C>, dim3(grid), dim3(BT), args, 0, c->st);
     c->launches += 2;
     return check_cuda(c, e, "tick launch");
 }
