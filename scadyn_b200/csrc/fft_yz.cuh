@@ -126,17 +126,17 @@ SCD_HD void yz_zstore(int tid, C *A, const C *B, int ky0, const YzDims &D) {
     }
 }
 
-// the Green product of a chunk: B[l][kz] *= Fyz(fx, fold(ky), fold(kz))
+// the Green product of a chunk: B[l][kz] *= Fyz(fx, fold(ky), fold(kz)),
+// each line by its own TZ threads (thread t of line l = tid / TZ takes kz = t,
+// t + TZ, ...), so that the line's transforms before and after it need only
+// a warp synchronisation (a warp holds whole lines)
 template <int PY, int PZ, typename C>
 SCD_HD void yz_green(int tid, C *B, const C *Fyz, int fx, int ky0, const YzDims &D) {
-    constexpr int LSZ = YzLine<PZ>::LS, KC = YzLine<PZ>::LINES;
-    for (int e = tid; e < KC * PZ; e += YZ_THREADS) {
-        const int l = e / PZ, kz = e - l * PZ, ky = ky0 + l;
-        if (ky < PY) {
-            const C f = Fyz[((long long)fx * D.Hy + yz_fold(ky, PY)) * D.Hz + yz_fold(kz, PZ)];
-            B[l * LSZ + pidx(kz)] = cmul(f, B[l * LSZ + pidx(kz)]);
-        }
-    }
+    constexpr int LSZ = YzLine<PZ>::LS, TZ = YzLine<PZ>::TPL;
+    const int l = tid / TZ, t = tid - l * TZ, ky = ky0 + l;
+    if (ky >= PY) return;
+    const C *Fr = Fyz + ((long long)fx * D.Hy + yz_fold(ky, PY)) * D.Hz;
+    for (int kz = t; kz < PZ; kz += TZ) B[l * LSZ + pidx(kz)] = cmul(Fr[yz_fold(kz, PZ)], B[l * LSZ + pidx(kz)]);
 }
 
 // one line transform run on the host: every thread of the line, phase by
@@ -226,9 +226,9 @@ k_fft_yz(C *__restrict__ Wt, const C *__restrict__ Fyz, const C *__restrict__ tw
         yz_zload<PY, PZ>(tid, A, B, ky0, D);
         __syncthreads();
         yz_line_dev<PZ, false, C>(B + (tid / TZ) * LSZ, twz, tid % TZ);
-        __syncthreads();
+        __syncwarp();   // a warp holds whole lines (YZ_THREADS / TZ lines, 32 / TZ per warp)
         yz_green<PY, PZ>(tid, B, Fyz, fx, ky0, D);
-        __syncthreads();
+        __syncwarp();
         yz_line_dev<PZ, true, C>(B + (tid / TZ) * LSZ, twz, tid % TZ);
         __syncthreads();
         yz_zstore<PY, PZ>(tid, A, B, ky0, D);
