@@ -337,6 +337,17 @@ SCD_API int64_t scd_nearzone_bytes(scd_ctx *ctx);
  * SCD_CUDA_ERROR otherwise.  The device stays usable. */
 SCD_API int scd_selftest_waits(int32_t device);
 
+/* Determinism self-check of the batched matvec (no counterpart in the
+ * reference): nrhs fixed input columns (different in every column), one
+ * matvec of the current kernel choices as the reference output, then reps
+ * more matvecs of the same inputs, each compared with it bit for bit on the
+ * device.  *bad_reps = repetitions whose output differs in any bit, *bad_words
+ * = differing 32-bit words over all of them.  Every kernel of the matvec sums
+ * in a fixed order, so both are 0; anything else is a race.  precision:
+ * SCD_PREC_FP64 (complex128 columns) or SCD_PREC_MIXED (complex64). */
+SCD_API int scd_check_matvec_repeat(scd_ctx *ctx, int32_t reps, int32_t nrhs, int32_t precision,
+                                    int64_t *bad_reps, int64_t *bad_words);
+
 #ifdef __cplusplus
 }
 #endif

@@ -44,7 +44,7 @@ EXPORTS = [
     "scd_get_nearzone", "scd_matvec", "scd_gmres", "scd_set_rhs_matrix", "scd_solve_columns", "scd_vswf_rhs",
     "scd_get_timing", "scd_compute_T_matrix", "scd_profile_matvec", "scd_nearzone_bytes",
     "scd_column_latency", "scd_T_assemble_noalloc", "scd_selftest_waits", "scd_tune_matvec", "scd_apply_tuning",
-    "scd_solve_sweep", "scd_compute_T_columns",
+    "scd_solve_sweep", "scd_compute_T_columns", "scd_check_matvec_repeat",
 ]
 
 
@@ -124,6 +124,7 @@ def load_library(path: str = LIB_PATH):
         "scd_column_latency": ([vp, i32, vp], C.c_int),
         "scd_T_assemble_noalloc": ([vp, i64, i32, vp, i32, vp, vp], C.c_int),
         "scd_selftest_waits": ([i32], C.c_int),
+        "scd_check_matvec_repeat": ([vp, i32, i32, i32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -430,6 +431,14 @@ class Solver:
     def profile_matvec(self, reps=10, nrhs=1, precision=PREC_FP64):
         self._chk(self.lib.scd_profile_matvec(self.ctx, reps, nrhs, precision), "profile_matvec")
         return self.timing()
+
+    def check_matvec_repeat(self, reps=100, nrhs=1, precision=PREC_MIXED):
+        """scd_check_matvec_repeat: (repetitions whose output differed in any
+        bit from the first matvec of the same inputs, differing 32-bit words)."""
+        br, bw = C.c_int64(0), C.c_int64(0)
+        self._chk(self.lib.scd_check_matvec_repeat(self.ctx, reps, nrhs, precision, C.byref(br), C.byref(bw)),
+                  "check_matvec_repeat")
+        return br.value, bw.value
 
     def tune_matvec(self, nrhs, precision=PREC_MIXED, reps=10):
         """scd_tune_matvec: time the matvec kernel choices, keep the fastest

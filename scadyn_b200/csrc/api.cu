@@ -811,6 +811,77 @@ int scd_profile_matvec(scd_ctx *c, int32_t reps, int32_t nrhs, int32_t precision
     return check_cuda(c, cudaGetLastError(), "profile");
 }
 
+// differing 32-bit words of a and b, added to *cnt
+static __global__ void k_words_differ(const unsigned *a, const unsigned *b, long long nw, unsigned long long *cnt) {
+    unsigned long long d = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nw; i += (long long)gridDim.x * blockDim.x)
+        d += a[i] != b[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+    if ((threadIdx.x & 31) == 0 && d) atomicAdd(cnt, d);
+}
+
+int scd_check_matvec_repeat(scd_ctx *c, int32_t reps, int32_t nrhs, int32_t precision, int64_t *bad_reps,
+                            int64_t *bad_words) {
+    if (!c || reps < 1 || nrhs < 1 || !bad_reps || !bad_words) return SCD_BAD_ARG;
+    if (precision != SCD_PREC_FP64 && precision != SCD_PREC_MIXED)
+        return set_error(c, SCD_BAD_ARG, "precision %d", precision);
+    cudaSetDevice(c->dev);
+    int rc = ready(c);
+    if (rc) return rc;
+    if ((rc = ensure_work(c, nrhs))) return rc;
+    const bool mixed = precision == SCD_PREC_MIXED;
+    if (mixed && ((rc = ensure_single(c)) || (rc = ensure_work_single(c, nrhs)))) return rc;
+    const size_t es = mixed ? sizeof(cf) : sizeof(cd), col = es * (size_t)c->n;
+    void *x = nullptr, *y = nullptr, *y0 = nullptr;
+    unsigned long long *cnt = nullptr;
+    auto release = [&]() { cudaFree(x); cudaFree(y); cudaFree(y0); cudaFree(cnt); };
+    if (cudaMalloc(&x, col * nrhs) != cudaSuccess || cudaMalloc(&y, col * nrhs) != cudaSuccess ||
+        cudaMalloc(&y0, col * nrhs) != cudaSuccess || cudaMalloc(&cnt, sizeof(unsigned long long) * reps) != cudaSuccess) {
+        cudaGetLastError();
+        release();
+        return set_error(c, SCD_OOM, "matvec repeat check: %zu bytes", 3 * col * nrhs);
+    }
+    // column r: a dense vector with an r-dependent phase
+    std::vector<cd> h((size_t)c->n);
+    std::vector<cf> hf(mixed ? (size_t)c->n : 0);
+    for (int r = 0; r < nrhs && !rc; ++r) {
+        for (long long i = 0; i < c->n; ++i) {
+            h[i] = cmk(std::sin(0.37 * (double)i + 0.5 * r), std::cos(0.11 * (double)i + 0.3 * r));
+            if (mixed) hf[i] = make_float2((float)h[i].x, (float)h[i].y);
+        }
+        rc = check_cuda(c, cudaMemcpy((char *)x + col * r, mixed ? (const void *)hf.data() : (const void *)h.data(), col,
+                                      cudaMemcpyHostToDevice), "repeat check x");
+    }
+    auto mv = [&](void *out) {
+        if (mixed) run_matvec(c, (const cf *)x, (cf *)out, nrhs, nullptr);
+        else run_matvec(c, (const cd *)x, (cd *)out, nrhs, nullptr);
+    };
+    if (!rc) rc = check_cuda(c, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long) * reps, c->st), "repeat check");
+    if (!rc) mv(y0);
+    const long long nw = (long long)(col * nrhs / 4);
+    const int blocks = (int)std::min<long long>((nw + 255) / 256, 4 * 148);
+    for (int r = 0; r < reps && !rc; ++r) {
+        mv(y);
+        k_words_differ<<<blocks, 256, 0, c->st>>>((const unsigned *)y0, (const unsigned *)y, nw, cnt + r);
+        c->launches += 1;
+        if (r % 64 == 63 || r == reps - 1) rc = check_cuda(c, cudaStreamSynchronize(c->st), "repeat check");
+    }
+    std::vector<unsigned long long> hc(reps, 0);
+    if (!rc) rc = check_cuda(c, cudaMemcpy(hc.data(), cnt, sizeof(unsigned long long) * reps, cudaMemcpyDeviceToHost),
+                             "repeat check counts");
+    release();
+    if (rc) return rc;
+    *bad_reps = 0;
+    *bad_words = 0;
+    for (unsigned long long v : hc) {
+        *bad_reps += v != 0;
+        *bad_words += (int64_t)v;
+    }
+    if ((rc = near_status(c))) return rc;
+    return check_cuda(c, cudaGetLastError(), "repeat check");
+}
+
 // ---------------------------------------------------------------- autotuner
 static void put_tuning(scd_ctx *c, const scd_tuning &t) {
     if (t.near_kernel == SCD_NEAR_CUDA_CORES) {

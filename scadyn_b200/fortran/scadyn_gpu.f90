@@ -97,7 +97,7 @@ module scadyn_gpu
              scd_compute_T_columns, &
              scd_get_timing, scd_profile_matvec, scd_tune_matvec, scd_apply_tuning, scd_solve_sweep, &
              scd_T_assemble_noalloc, scd_column_latency, &
-             scd_nearzone_bytes, scd_selftest_waits, scd_last_error_f
+             scd_nearzone_bytes, scd_selftest_waits, scd_check_matvec_repeat, scd_last_error_f
    public :: scd_server_create, scd_server_submit, scd_server_estimate, scd_server_poll, &
              scd_server_wait, scd_server_result, scd_server_cancel, scd_server_stats_get, &
              scd_server_destroy, scd_server_error_f
@@ -293,6 +293,13 @@ module scadyn_gpu
          import :: c_ptr, c_int, c_int32_t
          type(c_ptr), value :: ctx
          integer(c_int32_t), value :: reps, nrhs, precision
+      end function
+      integer(c_int) function scd_check_matvec_repeat(ctx, reps, nrhs, precision, bad_reps, bad_words) &
+            bind(C, name="scd_check_matvec_repeat")
+         import :: c_ptr, c_int, c_int32_t, c_int64_t
+         type(c_ptr), value :: ctx
+         integer(c_int32_t), value :: reps, nrhs, precision
+         integer(c_int64_t), intent(out) :: bad_reps, bad_words
       end function
       ! mat, X, T: DEVICE addresses (e.g. c_loc of CUDA Fortran device arrays); stream: a cudaStream_t
       integer(c_int) function scd_T_assemble_noalloc(mat, n, ncol, X, ncb, T, stream) &
