@@ -359,74 +359,41 @@ __device__ void cycle_end(const TickArgs<C> &a, const Chunks &ch, int nch, const
     }
 }
 
-// Classical Gram-Schmidt sweeps take several Krylov vectors per pass over a
-// chunk, TUK elements of each at a time (KBD vectors for the dots, w loaded
-// once per pass; KBU for the update), where one vector per pass left the
-// warp waiting on a round trip per vector.  A lane still takes its elements
-// q = c*L + lane + 32t in ascending t for every vector, so every sum keeps
-// its order (and its bits).  The sizes keep the kernel within 128 registers
-// without spills.
-constexpr int KBD = 3;
-constexpr int KBU = 4;
-constexpr int TUK = 4;
-
-// <v_k, w> for k = k0 .. k0+NK-1 over the lane's elements of one chunk, and
-// ||w||^2 when k0 == 1; the warp's sums of the dots go to pp.
-template <typename C, int NK>
-__device__ __forceinline__ void cgs_dot_pass(const C *Vs, const C *ws, long long n, int k0, long long qa,
-                                             long long qb, int lane, double *pp, double &nw) {
-    double d[NK][2];
-#pragma unroll
-    for (int b = 0; b < NK; ++b) d[b][0] = d[b][1] = 0.0;
-    const C *vk = Vs + (size_t)(k0 - 1) * n;
-    for (long long q = qa + lane; q < qb; q += 32 * TUK) {
-        C w[TUK], z[NK][TUK];
-#pragma unroll
-        for (int e = 0; e < TUK; ++e) {
-            const long long qq = q + 32 * e;
-            w[e] = C{};
-#pragma unroll
-            for (int b = 0; b < NK; ++b) z[b][e] = C{};
-            if (qq < qb) {
-                w[e] = ws[qq];
-#pragma unroll
-                for (int b = 0; b < NK; ++b) z[b][e] = vk[(size_t)b * n + qq];
-            }
-        }
-#pragma unroll
-        for (int e = 0; e < TUK; ++e) {
-            if (q + 32 * e >= qb) break;
-            const cd wv = to_cd(w[e]);
-#pragma unroll
-            for (int b = 0; b < NK; ++b) cdot_acc(d[b][0], d[b][1], to_cd(z[b][e]), wv);
-            if (k0 == 1) nw += cabs2(wv);
-        }
-    }
-#pragma unroll
-    for (int b = 0; b < NK; ++b)
-#pragma unroll
-        for (int h = 0; h < 2; ++h)
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) d[b][h] += __shfl_xor_sync(0xffffffffu, d[b][h], o);
-    if (lane == 0)
-#pragma unroll
-        for (int b = 0; b < NK; ++b) { pp[2 * (k0 - 1 + b)] = d[b][0]; pp[2 * (k0 - 1 + b) + 1] = d[b][1]; }
-}
-
 // Classical Gram-Schmidt, first pass, chunk c of slot s: the dots <v_k, w>,
-// k = 1..i, and ||w||^2, KBD vectors per sweep over the chunk (w is re-read
-// from cache for each sweep), published per chunk; the slot's last warp
-// sums the NCH chunk partials of every value in chunk order into ctm.
-template <typename C>
+// k = 1..i, and ||w||^2 in one sweep over the chunk (w is re-read from cache
+// for each k), published per chunk; the slot's last warp sums the NCH chunk
+// partials of every value in chunk order into ctm.
+template <typename C, int TUC>
 __device__ __forceinline__ void cgs_dots(const TickArgs<C> &a, int s, int c, int i, const C *Vs, const C *ws,
                                          long long qa, long long qb, int lane) {
     const long long n = a.n;
     double *pp = a.cpm + ((size_t)s * NCH + c) * CGS_NV;
     double nw = 0.0;
-    int k = 1;
-    for (; k + KBD - 1 <= i; k += KBD) cgs_dot_pass<C, KBD>(Vs, ws, n, k, qa, qb, lane, pp, nw);
-    if (k + 1 <= i) { cgs_dot_pass<C, 2>(Vs, ws, n, k, qa, qb, lane, pp, nw); k += 2; }
-    for (; k <= i; ++k) cgs_dot_pass<C, 1>(Vs, ws, n, k, qa, qb, lane, pp, nw);
+    for (int k = 1; k <= i; ++k) {
+        const C *vk = Vs + (size_t)(k - 1) * n;
+        double d[2] = {0.0, 0.0};
+        for (long long q = qa + lane; q < qb; q += 32 * TUC) {
+            C w[TUC], z[TUC];
+#pragma unroll
+            for (int e = 0; e < TUC; ++e) {
+                const long long qq = q + 32 * e;
+                w[e] = z[e] = C{};
+                if (qq < qb) { w[e] = ws[qq]; z[e] = vk[qq]; }
+            }
+#pragma unroll
+            for (int e = 0; e < TUC; ++e) {
+                if (q + 32 * e >= qb) break;
+                const cd wv = to_cd(w[e]);
+                cdot_acc(d[0], d[1], to_cd(z[e]), wv);
+                if (k == 1) nw += cabs2(wv);
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) d[h] += __shfl_xor_sync(0xffffffffu, d[h], o);
+        if (lane == 0) { pp[2 * (k - 1)] = d[0]; pp[2 * (k - 1) + 1] = d[1]; }
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) nw += __shfl_xor_sync(0xffffffffu, nw, o);
     int last = 0;
@@ -521,7 +488,7 @@ __global__ void __launch_bounds__(BT, sizeof(C) == 8 ? SCD_TICK_MINB : 2) k_tick
                 }
             }
         } else if (a.cgs) {
-            cgs_dots<C>(a, s, c, sstep[s] + 1, V0, ws, qa, qb, lane);
+            cgs_dots<C, TUC>(a, s, c, sstep[s] + 1, V0, ws, qa, qb, lane);
             continue;
         } else {
             for (long long q = qa + lane; q < qb; q += 32 * TUC) {
@@ -669,46 +636,27 @@ __global__ void __launch_bounds__(BT, sizeof(C) == 8 ? SCD_TICK_MINB : 2) k_tick
             C *ws = a.w + (size_t)swpos[s] * n;
             const C *Vs = a.V + (size_t)s * (a.m + 1) * n;
             double u[1] = {0.0};
-            for (long long q = qa + lane; q < qb; q += 32 * TUK) {
-                cd acc[TUK];
+            for (long long q = qa + lane; q < qb; q += 32 * TUC) {
+                cd acc[TUC];
 #pragma unroll
-                for (int e = 0; e < TUK; ++e) {
+                for (int e = 0; e < TUC; ++e) {
                     const long long qq = q + 32 * e;
                     acc[e] = qq < qb ? to_cd(ws[qq]) : cmk(0, 0);
                 }
-                int k = 0;
-                for (; k + KBU <= i; k += KBU) {   // KBU vectors' loads together, applied in k order
-                    C p[KBU][TUK];
-#pragma unroll
-                    for (int b = 0; b < KBU; ++b) {
-                        const C *vk = Vs + (size_t)(k + b) * n;
-#pragma unroll
-                        for (int e = 0; e < TUK; ++e) {
-                            const long long qq = q + 32 * e;
-                            p[b][e] = qq < qb ? vk[qq] : C{};
-                        }
-                    }
-#pragma unroll
-                    for (int b = 0; b < KBU; ++b) {
-                        const cd hk = hs[k + b];
-#pragma unroll
-                        for (int e = 0; e < TUK; ++e) csub_mul(acc[e], hk, to_cd(p[b][e]));
-                    }
-                }
-                for (; k < i; ++k) {
+                for (int k = 0; k < i; ++k) {
                     const cd hk = hs[k];
                     const C *vk = Vs + (size_t)k * n;
-                    C p[TUK];
+                    C p[TUC];
 #pragma unroll
-                    for (int e = 0; e < TUK; ++e) {
+                    for (int e = 0; e < TUC; ++e) {
                         const long long qq = q + 32 * e;
                         p[e] = qq < qb ? vk[qq] : C{};
                     }
 #pragma unroll
-                    for (int e = 0; e < TUK; ++e) csub_mul(acc[e], hk, to_cd(p[e]));
+                    for (int e = 0; e < TUC; ++e) csub_mul(acc[e], hk, to_cd(p[e]));
                 }
 #pragma unroll
-                for (int e = 0; e < TUK; ++e) {
+                for (int e = 0; e < TUC; ++e) {
                     const long long qq = q + 32 * e;
                     if (qq >= qb) break;
                     store_c(ws[qq], acc[e]);
