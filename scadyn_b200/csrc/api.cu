@@ -116,9 +116,10 @@ int near_status(scd_ctx *c) {
     }
     if (!c->d_kerr) return SCD_OK;
     int h = 0;
-    CK(cudaMemcpy(&h, c->d_kerr, sizeof(int), cudaMemcpyDeviceToHost), "near-zone status");
+    CK(cudaMemcpyAsync(&h, c->d_kerr, sizeof(int), cudaMemcpyDeviceToHost, c->st), "near-zone status");
+    CK(cudaStreamSynchronize(c->st), "near-zone status");
     if (!h) return SCD_OK;
-    CK(cudaMemset(c->d_kerr, 0, sizeof(int)), "near-zone status");
+    CK(cudaMemsetAsync(c->d_kerr, 0, sizeof(int), c->st), "near-zone status");
     return set_error(c, SCD_TIMEOUT, "near-zone kernel: a pipeline wait ran out");
 }
 
@@ -185,11 +186,11 @@ static int set_order(scd_ctx *c, const std::vector<int> &cube_of_tet) {
     if ((rc = dalloc(c, &c->d_cube_off, c->ncubes + 1, "cube offsets"))) return rc;
     if ((rc = dalloc(c, &c->d_grp_off, c->ngroups + 1, "group offsets"))) return rc;
     if ((rc = dalloc(c, &c->d_grp_cube, std::max(c->ngroups, 1), "group boxes"))) return rc;
-    CK(cudaMemcpy(c->d_perm, c->perm.data(), sizeof(int) * T, cudaMemcpyHostToDevice), "perm");
-    CK(cudaMemcpy(c->d_cube_off, c->cube_off.data(), sizeof(int) * (c->ncubes + 1), cudaMemcpyHostToDevice), "cube offsets");
-    CK(cudaMemcpy(c->d_grp_off, c->grp_off.data(), sizeof(int) * (c->ngroups + 1), cudaMemcpyHostToDevice), "groups");
+    CK(cudaMemcpyAsync(c->d_perm, c->perm.data(), sizeof(int) * T, cudaMemcpyHostToDevice, c->st), "perm");
+    CK(cudaMemcpyAsync(c->d_cube_off, c->cube_off.data(), sizeof(int) * (c->ncubes + 1), cudaMemcpyHostToDevice, c->st), "cube offsets");
+    CK(cudaMemcpyAsync(c->d_grp_off, c->grp_off.data(), sizeof(int) * (c->ngroups + 1), cudaMemcpyHostToDevice, c->st), "groups");
     if (c->ngroups)
-        CK(cudaMemcpy(c->d_grp_cube, c->grp_cube.data(), sizeof(int) * c->ngroups, cudaMemcpyHostToDevice), "groups");
+        CK(cudaMemcpyAsync(c->d_grp_cube, c->grp_cube.data(), sizeof(int) * c->ngroups, cudaMemcpyHostToDevice, c->st), "groups");
     c->have_order = true;
     return SCD_OK;
 }
@@ -269,11 +270,11 @@ static int upload_layout(scd_ctx *c, std::vector<NearTile> &tiles, long long off
     if ((rc = dalloc(c, &c->d_pslot_cnt, std::max(ng, 1), "slot counts"))) return rc;
     if ((rc = dalloc(c, &c->d_grp_tile, ng + 1, "group tiles"))) return rc;
     if ((rc = dalloc(c, &c->d_kerr, 1, "error word"))) return rc;
-    CK(cudaMemset(c->d_kerr, 0, sizeof(int)), "error word");
-    if (nt) CK(cudaMemcpy(c->d_tiles, tiles.data(), sizeof(NearTile) * nt, cudaMemcpyHostToDevice), "tile table");
-    CK(cudaMemcpy(c->d_pslot_base, c->pslot_base.data(), sizeof(long long) * (ng + 1), cudaMemcpyHostToDevice), "slots");
-    if (ng) CK(cudaMemcpy(c->d_pslot_cnt, c->pslot_cnt.data(), sizeof(int) * ng, cudaMemcpyHostToDevice), "slots");
-    CK(cudaMemcpy(c->d_grp_tile, c->grp_tile.data(), sizeof(int) * (ng + 1), cudaMemcpyHostToDevice), "group tiles");
+    CK(cudaMemsetAsync(c->d_kerr, 0, sizeof(int), c->st), "error word");
+    if (nt) CK(cudaMemcpyAsync(c->d_tiles, tiles.data(), sizeof(NearTile) * nt, cudaMemcpyHostToDevice, c->st), "tile table");
+    CK(cudaMemcpyAsync(c->d_pslot_base, c->pslot_base.data(), sizeof(long long) * (ng + 1), cudaMemcpyHostToDevice, c->st), "slots");
+    if (ng) CK(cudaMemcpyAsync(c->d_pslot_cnt, c->pslot_cnt.data(), sizeof(int) * ng, cudaMemcpyHostToDevice, c->st), "slots");
+    CK(cudaMemcpyAsync(c->d_grp_tile, c->grp_tile.data(), sizeof(int) * (ng + 1), cudaMemcpyHostToDevice, c->st), "group tiles");
     c->ntiles = nt;
     c->part_len = c->pslot_base[ng];
     c->tiles_h.swap(tiles);
@@ -384,7 +385,7 @@ static int build_tiles(scd_ctx *c, int64_t B, const ST *sp, const int32_t *ind, 
     }
     int rc;
     if ((rc = dalloc(c, (ST **)&c->d_tdata, data.size(), "near-zone tiles"))) return rc;
-    CK(cudaMemcpy(c->d_tdata, data.data(), sizeof(ST) * data.size(), cudaMemcpyHostToDevice), "tiles");
+    CK(cudaMemcpyAsync(c->d_tdata, data.data(), sizeof(ST) * data.size(), cudaMemcpyHostToDevice, c->st), "tiles");
     if ((rc = upload_layout(c, tiles, off))) return rc;
     c->B_ref = B;
     return SCD_OK;
@@ -527,7 +528,7 @@ int scd_set_projectors(scd_ctx *c, int32_t M_box, int32_t T, const scd_c128 *S, 
             for (int j = 0; j < 27; ++j) h[(size_t)(g * 27 + j) * T + s] = cmk(p[j].re, p[j].im);
         }
     if ((rc = dalloc(c, &c->d_P, h.size(), "projectors"))) return rc;
-    CK(cudaMemcpy(c->d_P, h.data(), sizeof(cd) * h.size(), cudaMemcpyHostToDevice), "projectors");
+    CK(cudaMemcpyAsync(c->d_P, h.data(), sizeof(cd) * h.size(), cudaMemcpyHostToDevice, c->st), "projectors");
     c->have_proj = true;
     c->f_ready = false;
     return SCD_OK;
@@ -778,10 +779,12 @@ int scd_profile_matvec(scd_ctx *c, int32_t reps, int32_t nrhs, int32_t precision
         h[i] = cmk(std::sin(0.37 * (double)i), std::cos(0.11 * (double)i));
         hf[i] = make_float2((float)h[i].x, (float)h[i].y);
     }
+    // copies on the context's stream, so that the matvecs below run after them
     for (int r = 0; r < nrhs && !rc; ++r) {
-        if (mixed) rc = check_cuda(c, cudaMemcpy(fx + (size_t)r * c->n, hf.data(), sizeof(cf) * c->n, cudaMemcpyHostToDevice), "profile x");
-        else rc = check_cuda(c, cudaMemcpy(c->d_x + (size_t)r * c->n, h.data(), sizeof(cd) * c->n, cudaMemcpyHostToDevice), "profile x");
+        if (mixed) rc = check_cuda(c, cudaMemcpyAsync(fx + (size_t)r * c->n, hf.data(), sizeof(cf) * c->n, cudaMemcpyHostToDevice, c->st), "profile x");
+        else rc = check_cuda(c, cudaMemcpyAsync(c->d_x + (size_t)r * c->n, h.data(), sizeof(cd) * c->n, cudaMemcpyHostToDevice, c->st), "profile x");
     }
+    if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->st), "profile x");
     double sn = 0, sf = 0, sg = 0, st = 0, sk = 0;
     c->timing = true;
     for (int r = 0; r < reps + 1 && !rc; ++r) {
@@ -842,17 +845,21 @@ int scd_check_matvec_repeat(scd_ctx *c, int32_t reps, int32_t nrhs, int32_t prec
         release();
         return set_error(c, SCD_OOM, "matvec repeat check: %zu bytes", 3 * col * nrhs);
     }
-    // column r: a dense vector with an r-dependent phase
-    std::vector<cd> h((size_t)c->n);
-    std::vector<cf> hf(mixed ? (size_t)c->n : 0);
-    for (int r = 0; r < nrhs && !rc; ++r) {
+    // column r: a dense vector with an r-dependent phase.  The columns go up
+    // in one copy on the context's stream, which orders it before the first
+    // matvec: a blocking cudaMemcpy from pageable memory may return before its
+    // DMA lands, and the non-blocking stream does not wait for it.
+    std::vector<cd> h(mixed ? 0 : (size_t)c->n * nrhs);
+    std::vector<cf> hf(mixed ? (size_t)c->n * nrhs : 0);
+    for (int r = 0; r < nrhs; ++r)
         for (long long i = 0; i < c->n; ++i) {
-            h[i] = cmk(std::sin(0.37 * (double)i + 0.5 * r), std::cos(0.11 * (double)i + 0.3 * r));
-            if (mixed) hf[i] = make_float2((float)h[i].x, (float)h[i].y);
+            const cd v = cmk(std::sin(0.37 * (double)i + 0.5 * r), std::cos(0.11 * (double)i + 0.3 * r));
+            if (mixed) hf[(size_t)r * c->n + i] = make_float2((float)v.x, (float)v.y);
+            else h[(size_t)r * c->n + i] = v;
         }
-        rc = check_cuda(c, cudaMemcpy((char *)x + col * r, mixed ? (const void *)hf.data() : (const void *)h.data(), col,
-                                      cudaMemcpyHostToDevice), "repeat check x");
-    }
+    rc = check_cuda(c, cudaMemcpyAsync(x, mixed ? (const void *)hf.data() : (const void *)h.data(), col * nrhs,
+                                       cudaMemcpyHostToDevice, c->st), "repeat check x");
+    if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->st), "repeat check x");
     auto mv = [&](void *out) {
         if (mixed) run_matvec(c, (const cf *)x, (cf *)out, nrhs, nullptr);
         else run_matvec(c, (const cd *)x, (cd *)out, nrhs, nullptr);

@@ -118,7 +118,7 @@ int setup_green(scd_ctx *c, const scd_c128 *Fg) {
                     const scd_c128 v = Fg[(size_t)x + (size_t)c->Px * ((size_t)y + (size_t)c->Py * z)];
                     h[(size_t)x + (size_t)c->Hx * ((size_t)y + (size_t)c->Hy * z)] = cmk(v.re * scale, v.im * scale);
                 }
-        return check_cuda(c, cudaMemcpy(c->d_Fo, h.data(), sizeof(cd) * oct, cudaMemcpyHostToDevice), "Green octant");
+        return check_cuda(c, cudaMemcpyAsync(c->d_Fo, h.data(), sizeof(cd) * oct, cudaMemcpyHostToDevice, c->st), "Green octant");
     }
     if (cudaMalloc(&tmp, sizeof(cd) * oct) != cudaSuccess) return set_error(c, SCD_OOM, "Green scratch");
     const int blocks = (int)std::min<long long>((oct + 255) / 256, 65535);

@@ -479,9 +479,9 @@ int near_mma_prepare(scd_ctx *c) {
         (rc = al((void **)&c->d_xmax, sizeof(unsigned int) * (NZM_RMAX + 1), "x scales")) ||
         (rc = al((void **)&c->d_xinv, sizeof(float) * NZM_RMAX, "x scales")))
         return rc;
-    if ((rc = check_cuda(c, cudaMemcpy(c->d_t16_off, toff.data(), sizeof(long long) * c->ntiles, cudaMemcpyHostToDevice),
+    if ((rc = check_cuda(c, cudaMemcpyAsync(c->d_t16_off, toff.data(), sizeof(long long) * c->ntiles, cudaMemcpyHostToDevice, c->st),
                          "tile offsets")) ||
-        (rc = check_cuda(c, cudaMemcpy(c->d_xb_off, xoff.data(), sizeof(long long) * c->ngroups, cudaMemcpyHostToDevice),
+        (rc = check_cuda(c, cudaMemcpyAsync(c->d_xb_off, xoff.data(), sizeof(long long) * c->ngroups, cudaMemcpyHostToDevice, c->st),
                          "x-block offsets")))
         return rc;
     // one power-of-two scale for all tiles

@@ -39,9 +39,12 @@ int upload_quadrature(scd_ctx *c) {
     static int done_dev = -1;
     if (done_dev == c->dev) return SCD_OK;
     const HostQuad &q = hq();
-    int rc = check_cuda(c, cudaMemcpyToSymbol(cQT5, q.t5, sizeof q.t5), "quadrature");
-    if (!rc) rc = check_cuda(c, cudaMemcpyToSymbol(cQR5, q.r5, sizeof q.r5), "quadrature");
-    if (!rc) rc = check_cuda(c, cudaMemcpyToSymbol(cPs, q.ps, sizeof q.ps), "quadrature");
+    // copies on the context's stream, finished before any context of the
+    // device may read the tables
+    int rc = check_cuda(c, cudaMemcpyToSymbolAsync(cQT5, q.t5, sizeof q.t5, 0, cudaMemcpyHostToDevice, c->st), "quadrature");
+    if (!rc) rc = check_cuda(c, cudaMemcpyToSymbolAsync(cQR5, q.r5, sizeof q.r5, 0, cudaMemcpyHostToDevice, c->st), "quadrature");
+    if (!rc) rc = check_cuda(c, cudaMemcpyToSymbolAsync(cPs, q.ps, sizeof q.ps, 0, cudaMemcpyHostToDevice, c->st), "quadrature");
+    if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->st), "quadrature");
     if (!rc) done_dev = c->dev;
     return rc;
 }
@@ -842,7 +845,7 @@ int setup_projectors_device(scd_ctx *c) {
         for (int m = 0; m < 98; ++m) WWh[u * 98 + m] = cmk(WW[27 * m + u].real(), WW[27 * m + u].imag());
     cd *dWW = nullptr;
     if (cudaMalloc(&dWW, sizeof(cd) * 27 * 98) != cudaSuccess) return set_error(c, SCD_OOM, "WW");
-    cudaMemcpy(dWW, WWh.data(), sizeof(cd) * 27 * 98, cudaMemcpyHostToDevice);
+    cudaMemcpyAsync(dWW, WWh.data(), sizeof(cd) * 27 * 98, cudaMemcpyHostToDevice, c->st);
     if (!c->d_P && cudaMalloc(&c->d_P, sizeof(cd) * 4 * 27 * (size_t)c->T) != cudaSuccess) {
         cudaFree(dWW);
         return set_error(c, SCD_OOM, "projectors");
@@ -855,12 +858,12 @@ int setup_projectors_device(scd_ctx *c) {
         cudaFree(dcube);
         return set_error(c, SCD_OOM, "projector tables");
     }
-    cudaMemcpy(dcube, c->cube_of_slot.data(), sizeof(int) * c->T, cudaMemcpyHostToDevice);
+    cudaMemcpyAsync(dcube, c->cube_of_slot.data(), sizeof(int) * c->T, cudaMemcpyHostToDevice, c->st);
     if (c->nb == 4) {
         // linear basis: one warp per tet over its four consecutive pseudo-tet slots
         std::vector<int> slot0(ntet);
         for (int q = 0; q < ntet; ++q) slot0[q] = c->slot_of[4 * q];
-        cudaMemcpy(dslot0, slot0.data(), sizeof(int) * ntet, cudaMemcpyHostToDevice);
+        cudaMemcpyAsync(dslot0, slot0.data(), sizeof(int) * ntet, cudaMemcpyHostToDevice, c->st);
         k_projectors_lin<<<ntet, 32, 0, c->st>>>(c->d_tc, c->d_tvol, dcube, dslot0, ntet, c->T, dWW, c->ncx, c->ncy,
                                                   c->d.delta, c->d.min_coord[0], c->d.min_coord[1], c->d.min_coord[2],
                                                   bd, c->k, c->d_P);
@@ -1056,9 +1059,9 @@ int scd_set_mesh(scd_ctx *c, int32_t Nv, const double *coord, const int32_t *eto
         cudaMalloc(&c->d_tvol, sizeof(double) * vol.size()) != cudaSuccess ||
         cudaMalloc(&c->d_eps, sizeof(cd) * eps.size()) != cudaSuccess)
         return set_error(c, SCD_OOM, "mesh arrays");
-    cudaMemcpy(c->d_tc, tc.data(), sizeof(double) * tc.size(), cudaMemcpyHostToDevice);
-    cudaMemcpy(c->d_tvol, vol.data(), sizeof(double) * vol.size(), cudaMemcpyHostToDevice);
-    cudaMemcpy(c->d_eps, eps.data(), sizeof(cd) * eps.size(), cudaMemcpyHostToDevice);
+    cudaMemcpyAsync(c->d_tc, tc.data(), sizeof(double) * tc.size(), cudaMemcpyHostToDevice, c->st);
+    cudaMemcpyAsync(c->d_tvol, vol.data(), sizeof(double) * vol.size(), cudaMemcpyHostToDevice, c->st);
+    cudaMemcpyAsync(c->d_eps, eps.data(), sizeof(cd) * eps.size(), cudaMemcpyHostToDevice, c->st);
     c->have_mesh = true;
     return check_cuda(c, cudaGetLastError(), "set_mesh");
 }
@@ -1081,7 +1084,8 @@ int scd_get_projectors(scd_ctx *c, scd_c128 *S, scd_c128 *Sx, scd_c128 *Sy, scd_
     if (!c->have_proj) return set_error(c, SCD_NOT_READY, "projectors not set");
     const size_t TT = 27 * (size_t)c->T;
     std::vector<cd> h(4 * TT);
-    int rc = check_cuda(c, cudaMemcpy(h.data(), c->d_P, sizeof(cd) * h.size(), cudaMemcpyDeviceToHost), "get_projectors");
+    int rc = check_cuda(c, cudaMemcpyAsync(h.data(), c->d_P, sizeof(cd) * h.size(), cudaMemcpyDeviceToHost, c->st), "get_projectors");
+    if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->st), "get_projectors");
     if (rc) return rc;
     scd_c128 *dst[4] = {S, Sx, Sy, Sz};
     for (int s = 0; s < c->T; ++s) {
@@ -1126,11 +1130,13 @@ int scd_get_nearzone(scd_ctx *c, int64_t B, scd_c128 *sp, int32_t *ind) {
     std::vector<cd> data(nb);
     if (c->near_prec == SCD_STORE_C64) {
         std::vector<cf> f(nb);
-        int rc = check_cuda(c, cudaMemcpy(f.data(), c->d_tdata, sizeof(cf) * nb, cudaMemcpyDeviceToHost), "get_nearzone");
+        int rc = check_cuda(c, cudaMemcpyAsync(f.data(), c->d_tdata, sizeof(cf) * nb, cudaMemcpyDeviceToHost, c->st), "get_nearzone");
+        if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->st), "get_nearzone");
         if (rc) return rc;
         for (size_t i = 0; i < nb; ++i) data[i] = cmk(f[i].x, f[i].y);
     } else {
-        int rc = check_cuda(c, cudaMemcpy(data.data(), c->d_tdata, sizeof(cd) * nb, cudaMemcpyDeviceToHost), "get_nearzone");
+        int rc = check_cuda(c, cudaMemcpyAsync(data.data(), c->d_tdata, sizeof(cd) * nb, cudaMemcpyDeviceToHost, c->st), "get_nearzone");
+        if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->st), "get_nearzone");
         if (rc) return rc;
     }
     if (c->nb == 4) return export_linear_blocks(c, B, data, sp, ind);
