@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <complex>
 #include <cstring>
@@ -36,8 +37,11 @@ const HostQuad &hq() {
 }
 
 int upload_quadrature(scd_ctx *c) {
-    static int done_dev = -1;
-    if (done_dev == c->dev) return SCD_OK;
+    // per device: set once its tables are on the device (contexts of a
+    // server build operators from several host threads)
+    static std::atomic<bool> done[128];
+    const bool tracked = c->dev >= 0 && c->dev < 128;
+    if (tracked && done[c->dev].load(std::memory_order_acquire)) return SCD_OK;
     const HostQuad &q = hq();
     // copies on the context's stream, finished before any context of the
     // device may read the tables
@@ -45,7 +49,7 @@ int upload_quadrature(scd_ctx *c) {
     if (!rc) rc = check_cuda(c, cudaMemcpyToSymbolAsync(cQR5, q.r5, sizeof q.r5, 0, cudaMemcpyHostToDevice, c->st), "quadrature");
     if (!rc) rc = check_cuda(c, cudaMemcpyToSymbolAsync(cPs, q.ps, sizeof q.ps, 0, cudaMemcpyHostToDevice, c->st), "quadrature");
     if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->st), "quadrature");
-    if (!rc) done_dev = c->dev;
+    if (!rc && tracked) done[c->dev].store(true, std::memory_order_release);
     return rc;
 }
 
