@@ -1,8 +1,7 @@
 """Error behaviour of the C ABI without a context: every entry point given a
-NULL context (or server), NULL pointers and zero sizes returns an error code
-(SCD_BAD_ARG) instead of
-crashing, destroying NULL is a no-op, and the error-text getters name the
-missing object.  A Fortran host that calls before scd_create succeeded, or
+NULL context (or server), NULL pointers and zero sizes returns SCD_BAD_ARG
+instead of crashing, destroying NULL is a no-op, and the error-text getters
+name the missing object.  A Fortran host that calls before scd_create succeeded, or
 after it failed, gets a status to test, as the reference's routines return
 to their callers.  The calls run in a child process, so a crash fails this
 test instead of ending the run; none of them reaches the GPU."""
