@@ -845,21 +845,22 @@ int scd_check_matvec_repeat(scd_ctx *c, int32_t reps, int32_t nrhs, int32_t prec
         release();
         return set_error(c, SCD_OOM, "matvec repeat check: %zu bytes", 3 * col * nrhs);
     }
-    // column r: a dense vector with an r-dependent phase.  The columns go up
-    // in one copy on the context's stream, which orders it before the first
-    // matvec: a blocking cudaMemcpy from pageable memory may return before its
-    // DMA lands, and the non-blocking stream does not wait for it.
-    std::vector<cd> h(mixed ? 0 : (size_t)c->n * nrhs);
-    std::vector<cf> hf(mixed ? (size_t)c->n * nrhs : 0);
-    for (int r = 0; r < nrhs; ++r)
+    // column r: a dense vector with an r-dependent phase.  Each column goes up
+    // on the context's stream, which orders it before the first matvec (a
+    // blocking cudaMemcpy from pageable memory may return before its DMA
+    // lands, and the non-blocking stream does not wait for it), and the host
+    // column is refilled only after the copy is done.
+    std::vector<cd> h((size_t)c->n);
+    std::vector<cf> hf(mixed ? (size_t)c->n : 0);
+    for (int r = 0; r < nrhs && !rc; ++r) {
         for (long long i = 0; i < c->n; ++i) {
-            const cd v = cmk(std::sin(0.37 * (double)i + 0.5 * r), std::cos(0.11 * (double)i + 0.3 * r));
-            if (mixed) hf[(size_t)r * c->n + i] = make_float2((float)v.x, (float)v.y);
-            else h[(size_t)r * c->n + i] = v;
+            h[i] = cmk(std::sin(0.37 * (double)i + 0.5 * r), std::cos(0.11 * (double)i + 0.3 * r));
+            if (mixed) hf[i] = make_float2((float)h[i].x, (float)h[i].y);
         }
-    rc = check_cuda(c, cudaMemcpyAsync(x, mixed ? (const void *)hf.data() : (const void *)h.data(), col * nrhs,
-                                       cudaMemcpyHostToDevice, c->st), "repeat check x");
-    if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->st), "repeat check x");
+        rc = check_cuda(c, cudaMemcpyAsync((char *)x + col * r, mixed ? (const void *)hf.data() : (const void *)h.data(),
+                                           col, cudaMemcpyHostToDevice, c->st), "repeat check x");
+        if (!rc) rc = check_cuda(c, cudaStreamSynchronize(c->st), "repeat check x");
+    }
     auto mv = [&](void *out) {
         if (mixed) run_matvec(c, (const cf *)x, (cf *)out, nrhs, nullptr);
         else run_matvec(c, (const cd *)x, (cd *)out, nrhs, nullptr);
