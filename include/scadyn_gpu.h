@@ -313,9 +313,9 @@ SCD_API int scd_apply_tuning(scd_ctx *ctx, const scd_tuning *tuning);
  * library until the process exits, so ncol*ncb must not exceed 262144
  * (SCD_BAD_ARG otherwise).  The first call on a device looks up that array's
  * device address and keeps it.  The kept address is not valid after
- * cudaDeviceReset, so do not call this after a reset in the same process.  An error left pending by an earlier call of
- * the caller's is returned as SCD_CUDA_ERROR before anything launches, and
- * left pending.  All calls share the array: calls that overlap on the GPU
+ * cudaDeviceReset, so do not call this after a reset in the same process.
+ * An error left pending by an earlier call of the caller's is returned as
+ * SCD_CUDA_ERROR before anything launches, and left pending.  All calls share the array: calls that overlap on the GPU
  * race and must be ordered by the caller (one stream, or events). */
 SCD_API int scd_T_assemble_noalloc(const scd_c128 *mat, int64_t n, int32_t ncol, const scd_c128 *X, int32_t ncb,
                                    scd_c128 *T, void *stream);

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <vector>
 
 #include "ctx.h"
@@ -161,8 +162,10 @@ static __device__ __align__(256) cd g_noalloc_scratch[SCD_NOALLOC_SCRATCH];
 
 // device address of g_noalloc_scratch per device; the symbol name in host
 // code is only a host-side stand-in, so the address is looked up once per
-// device with that device current (first call on the device)
-static cd *g_noalloc_ptr[128] = {nullptr};
+// device with that device current (first call on the device).  Atomic, as
+// host threads may make their first calls at the same time; both store the
+// same address.
+static std::atomic<cd *> g_noalloc_ptr[128];
 
 extern "C" SCD_API int scd_T_assemble_noalloc(const scd_c128 *mat, int64_t n, int32_t ncol, const scd_c128 *X,
                                               int32_t ncb, scd_c128 *T, void *stream) {
@@ -173,15 +176,14 @@ extern "C" SCD_API int scd_T_assemble_noalloc(const scd_c128 *mat, int64_t n, in
     // an error left pending by an earlier call of the caller's is not this
     // call's: report it without launching and leave it for the caller to read
     if (cudaPeekAtLastError() != cudaSuccess) return SCD_CUDA_ERROR;
-    if (!g_noalloc_ptr[dev]) {
-        cd *p = nullptr;
-        if (cudaGetSymbolAddress((void **)&p, g_noalloc_scratch) != cudaSuccess || !p) {
+    cd *part = g_noalloc_ptr[dev].load(std::memory_order_acquire);
+    if (!part) {
+        if (cudaGetSymbolAddress((void **)&part, g_noalloc_scratch) != cudaSuccess || !part) {
             cudaGetLastError();   // this lookup's own error
             return SCD_CUDA_ERROR;
         }
-        g_noalloc_ptr[dev] = p;
+        g_noalloc_ptr[dev].store(part, std::memory_order_release);
     }
-    cd *part = g_noalloc_ptr[dev];
     cudaStream_t st = (cudaStream_t)stream;
     // as many K splits as the scratch holds (at most 64); every partial entry
     // is written before it is read, so nothing needs clearing between calls
