@@ -98,7 +98,8 @@ SCD_API int scd_server_cancel(scd_server *srv, int64_t id);
 
 SCD_API int scd_server_stats_get(scd_server *srv, scd_server_stats *st);
 
-/* Text of the last error of a request (empty when none). */
+/* Text of the last error of a request (empty when none).  The text stays
+ * valid until the calling thread's next scd_server_error call. */
 SCD_API const char *scd_server_error(scd_server *srv, int64_t id);
 
 /* Stop admitting, let the running requests finish, free everything. */

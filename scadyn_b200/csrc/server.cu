@@ -159,7 +159,6 @@ struct scd_server {
     bool stop = false;
     std::thread dispatcher;
     std::vector<std::shared_ptr<Pool>> retired;   // pools whose worker returned, to be joined
-    std::string scratch_err;
 };
 
 namespace {
@@ -635,8 +634,11 @@ const char *scd_server_error(scd_server *s, int64_t id) {
     std::lock_guard<std::mutex> g(s->m);
     auto it = s->reqs.find(id);
     if (it == s->reqs.end()) return "unknown request";
-    s->scratch_err = it->second.err;
-    return s->scratch_err.c_str();
+    // a copy per calling thread: valid until this thread's next call, and
+    // not overwritten by another thread's
+    static thread_local std::string text;
+    text = it->second.err;
+    return text.c_str();
 }
 
 int scd_server_destroy(scd_server *s) {
