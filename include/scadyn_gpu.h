@@ -165,7 +165,9 @@ SCD_API int scd_set_nearzone(scd_ctx *ctx, int64_t B, const void *sp_mat, const 
 SCD_API int scd_grid_from_mesh(int32_t Nv, const double *coord, int32_t T, const int32_t *etopol,
                        double grid_size, int32_t M_ex, scd_grid_desc *desc);
 
-/* mesh%coord (3,Nv), mesh%etopol (4,T) 1-based, mesh%param (T) complex eps. */
+/* mesh%coord (3,Nv), mesh%etopol (4,T) 1-based, mesh%param (T) complex eps
+ * (mesh_struct, src/common.f90:63-166); bins the tets into projection boxes
+ * as tetras_in_cubes does (src/geometry.f90:330-377). */
 SCD_API int scd_set_mesh(scd_ctx *ctx, int32_t Nv, const double *coord, const int32_t *etopol,
                  const scd_c128 *param);
 
@@ -179,7 +181,9 @@ SCD_API int scd_build_projectors(scd_ctx *ctx);
 SCD_API int scd_build_nearzone(scd_ctx *ctx, int32_t storage_prec);
 
 /* Copy the device operator back in the reference's layouts (for a Fortran
- * host that keeps its own copy, and for checking).  The near zone comes
+ * host that keeps its own copy, and for checking): matrices%S/Sx/Sy/Sz/indS
+ * (src/projection.f90:155-164) and sp_mat / sp_ind
+ * (src/precorrection.f90:251-254).  The near zone comes
  * back ordered by (tet_T, tet_B): B = scd_nearzone_count blocks, 3x3
  * (sp_mat(3,3,B)), or 12x12 (sp_mat(12,12,B)) with order 1. */
 SCD_API int scd_get_projectors(scd_ctx *ctx, scd_c128 *S, scd_c128 *Sx, scd_c128 *Sy, scd_c128 *Sz,
@@ -252,7 +256,8 @@ SCD_API int scd_compute_T_columns(scd_ctx *ctx, int32_t Nmax, const scd_solve_op
 SCD_API int scd_solve_sweep(scd_ctx *const *ctxs, int32_t nw, const int32_t *Nmax, const scd_solve_opts *opts,
                             scd_c128 *const *T, int32_t *const *iters, int32_t *status);
 
-/* Device timing, milliseconds, from CUDA events on the context's stream. */
+/* Device timing, milliseconds, from CUDA events on the context's stream (no
+ * counterpart in the reference, which times nothing on this path). */
 typedef struct scd_timing {
     double matvec_ms;      /* average matvec (scd_profile_matvec) */
     double nearzone_ms;    /* average near-zone kernel */
@@ -267,12 +272,17 @@ typedef struct scd_timing {
     double near_kernel_ms; /* average duration of the main near-zone kernel launch (the last pass of a
                               matvec: k_near_mma or k_near_groups), scd_profile_matvec */
 } scd_timing;
+/* Read the timing block; reset != 0 then clears the fields counted since the
+ * last reset (accum_ms, launches, matvecs, arnoldi_steps).  No counterpart
+ * in the reference. */
 SCD_API int scd_get_timing(scd_ctx *ctx, scd_timing *t, int32_t reset);
 
-/* Run `reps` device-resident matvecs on `nrhs` fixed vectors at once, in
- * FP64 (SCD_PREC_FP64) or in the complex64 form the mixed-precision inner
- * solves use (SCD_PREC_MIXED), and record per-kernel averages per call in
- * the timing block (matvec_ms, nearzone_ms, fft_ms, gather_ms). */
+/* No counterpart in the reference (a measurement of compute_Ax2,
+ * src/gmres_module.f90:57-176).  Run `reps` device-resident matvecs on
+ * `nrhs` fixed vectors at once, in FP64 (SCD_PREC_FP64) or in the complex64
+ * form the mixed-precision inner solves use (SCD_PREC_MIXED), and record
+ * per-kernel averages per call in the timing block (matvec_ms, nearzone_ms,
+ * fft_ms, gather_ms). */
 SCD_API int scd_profile_matvec(scd_ctx *ctx, int32_t reps, int32_t nrhs, int32_t precision);
 
 /* Matvec kernel settings of a context that can change between calls; the
@@ -299,7 +309,8 @@ typedef struct scd_tuning {
 SCD_API int scd_tune_matvec(scd_ctx *ctx, int32_t nrhs, int32_t precision, int32_t reps, scd_tuning *out);
 
 /* Apply a stored tuning (e.g. a cached scd_tune_matvec result for the same
- * grid, tets and right-hand sides) without timing anything. */
+ * grid, tets and right-hand sides) without timing anything.  No counterpart
+ * in the reference (like reusing an FFTW plan, src/possu.f90:82-89). */
 SCD_API int scd_apply_tuning(scd_ctx *ctx, const scd_tuning *tuning);
 
 /* T = mat^H X without allocating: mat (n, ncol), X (n, ncb) and T (ncol, ncb)
@@ -320,13 +331,15 @@ SCD_API int scd_apply_tuning(scd_ctx *ctx, const scd_tuning *tuning);
 SCD_API int scd_T_assemble_noalloc(const scd_c128 *mat, int64_t n, int32_t ncol, const scd_c128 *X, int32_t ncb,
                                    scd_c128 *T, void *stream);
 
-/* Per-column solve latency (admission to completion, milliseconds on the
- * host clock, each tick ending in a stream synchronisation) of the last
- * scd_solve_columns / scd_compute_T_matrix call; ncol must match it. */
+/* No counterpart in the reference.  Per-column solve latency (admission to
+ * completion, milliseconds on the host clock, each tick ending in a stream
+ * synchronisation) of the last scd_solve_columns / scd_compute_T_matrix
+ * call; ncol must match it. */
 SCD_API int scd_column_latency(scd_ctx *ctx, int32_t ncol, double *ms);
 
-/* Near-zone blocks in the reference layout (tet_B >= tet_T) and the bytes of
- * the device tile storage. */
+/* Near-zone blocks in the reference layout (tet_B >= tet_T; the B of
+ * sp_mat(3,3,B), src/precorrection.f90:251-254) and, with no counterpart in
+ * the reference, the bytes of the device tile storage. */
 SCD_API int64_t scd_nearzone_bytes(scd_ctx *ctx);
 
 /* Failure detection self-test (no counterpart in the reference): runs the
