@@ -8,8 +8,8 @@
  *
  * Parity: UNPINNED by reference golden vectors (the reference ships none and
  * cannot be compiled here).  Cross-checked against an independent numpy/scipy
- * restatement, the Mie series, T-matrix reciprocity and the energy balance
- * (see tests/).
+ * restatement, the Mie series (and convergence to it under mesh
+ * refinement), T-matrix reciprocity and the energy balance (see tests/).
  *
  * Floating-point notes that follow the reference's source literally:
  *  - single-precision literals promoted to double: `(x)**(1.0/3.0)` uses the
